@@ -1,0 +1,259 @@
+/*
+ * spgpu.h — C ABI of the B200 (sm_100a) ePlace global-placement engine.
+ *
+ * Plain C: POD structs, raw pointers and sizes, int status returns. No CUDA, torch or
+ * C++ types cross this boundary. Every entry point returns SPG_OK (0) on success or a
+ * negative SPG_E_* code; spg_last_error() gives the message of the calling thread's last
+ * failure.
+ *
+ * Threading: one host thread per context / Poisson handle (the reference's contract,
+ * src/numeric/poisson_backend.h:20-46 and src/gp/eplace.h:56-77). Independent handles
+ * may be used concurrently from different threads.
+ *
+ * Ownership: the caller owns every host array passed in; the library owns every device
+ * buffer and releases it in the matching *_destroy call.
+ *
+ * There is no CPU fallback: when no sm_100 device is present the create calls fail with
+ * SPG_E_NO_DEVICE.
+ */
+#ifndef SPGPU_H_
+#define SPGPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPG_ABI_VERSION 1
+
+/* ---- status codes (map onto the reference's InvariantError kinds, src/util/invariant.h:10-19) */
+#define SPG_OK 0
+#define SPG_E_INVALID (-1)       /* bad argument: dims, steps, sizes, null pointers      */
+#define SPG_E_NO_DEVICE (-2)     /* no usable sm_100 device                              */
+#define SPG_E_CUDA (-3)          /* a CUDA runtime call failed                           */
+#define SPG_E_NON_FINITE (-4)    /* InvariantError kind "non_finite"                     */
+#define SPG_E_OUT_OF_CORE (-5)   /* InvariantError kind "out_of_core"                    */
+#define SPG_E_CONVERGENCE (-6)   /* InvariantError kind "convergence_mismatch"           */
+#define SPG_E_ROLLBACK (-7)      /* InvariantError kind "rollback_mismatch"              */
+#define SPG_E_STATE (-8)         /* call out of order (e.g. run before stage_begin)      */
+#define SPG_E_CAPACITY (-9)      /* a size beyond a stated maximum                       */
+
+/* ---- node flags: same bit values as sp::NodeFlag (src/db/place_db.h:17-22) */
+#define SPG_F_MACRO 1u
+#define SPG_F_FIXED 2u
+#define SPG_F_FILLER 4u
+#define SPG_F_NI 8u
+
+/* ---- Poisson arithmetic */
+#define SPG_POISSON_FP32 0   /* cosine contractions as FP32 SIMT GEMMs ("plain FP32")        */
+#define SPG_POISSON_BF16X3 1 /* tcgen05 split-BF16 (hi*hi + hi*lo + lo*hi), FP32 accumulate */
+
+/* ---- GP stages (sp::GpStage, src/gp/eplace.h:24-28) */
+#define SPG_STAGE_MGP 0
+#define SPG_STAGE_FILLER_ONLY 1
+#define SPG_STAGE_CGP 2
+
+/*
+ * Read-only view of a PlaceDB (src/db/place_db.h:24-113): node SoA in centre coordinates,
+ * segments [movable | fixed | filler], pins, and the two-way CSR built by
+ * PlaceDB::finalizeCSR (src/db/place_db.cpp:67-95). node2pin_start has
+ * num_nodes + num_fillers + 1 entries (fillers own no pins, src/gp/filler.cpp:130).
+ */
+typedef struct spg_db_view {
+    int32_t num_movable; /* [0, num_movable)                          */
+    int32_t num_nodes;   /* [num_movable, num_nodes) fixed           */
+    int32_t num_fillers; /* [num_nodes, num_nodes + num_fillers)     */
+    const float* node_x;
+    const float* node_y;
+    const float* node_w;
+    const float* node_h;
+    const uint8_t* node_flags;
+
+    int32_t num_pins;
+    const float* pin_offset_x; /* relative to the node centre */
+    const float* pin_offset_y;
+    const int32_t* pin2node;
+    const int32_t* pin2net;
+
+    int32_t num_nets;
+    const int32_t* net2pin_start;  /* num_nets + 1 */
+    const int32_t* flat_net2pin;   /* num_pins     */
+    const int32_t* node2pin_start; /* total + 1    */
+    const int32_t* flat_node2pin;  /* num_pins     */
+
+    int32_t num_rows; /* PlaceDB::SiteRow, src/db/place_db.h:47-55 */
+    const float* row_ly;
+    const float* row_height;
+    const float* row_lx;
+    const float* row_step;
+    const int32_t* row_num_sites;
+
+    /* PlaceDB::computeRegions() results (src/db/place_db.cpp:97-127) */
+    float core_lx, core_ly, core_hx, core_hy;
+    float row_height_mode;
+    double total_row_area;
+} spg_db_view;
+
+/* GP configuration: the Config keys the path reads (src/util/config.h:77-116). */
+typedef struct spg_params {
+    float target_density;       /* 1.0  */
+    float target_overflow;      /* 0.10 */
+    float cgp_target_overflow;  /* 0.10 */
+    int32_t gp_max_iter;        /* 2000 */
+    int32_t ignore_net_degree;  /* 100  */
+    int32_t gp_bin_dim;         /* 0 = auto (power of two, cap 1024) */
+    int32_t filler_only_iters;  /* 20   */
+    float delta_hpwl_ref;       /* 3.5e5 */
+    int32_t lambda_schedule_relative; /* 0 = "fixed", 1 = "relative" */
+    double delta_hpwl_relative; /* 0.01 */
+    int32_t use_bb;             /* 1 */
+    int32_t gp_backtrack;       /* 1 */
+    int32_t max_backtrack;      /* 10 (OptConfig::max_backtrack) */
+    int32_t gp_stagnation_window;  /* 200  */
+    float gp_stagnation_min_gain;  /* 0.02 */
+    uint64_t random_seed;          /* 1002 */
+    int32_t poisson_precision;     /* SPG_POISSON_* */
+    int32_t verbose;               /* log every iteration instead of every 20th */
+} spg_params;
+
+/* Defaults identical to configs/default.json of the reference. */
+void spg_params_default(spg_params* p);
+
+/* sp::GpResult (src/gp/eplace.h:32-42) plus the stage-start summary keys. */
+typedef struct spg_result {
+    int32_t iterations;
+    double hpwl;
+    float overflow;
+    int32_t converged;
+    int32_t stagnated;
+    int32_t rollback_iter;
+    int64_t evaluations;
+    double elapsed_ms;      /* device-timed stage duration (CUDA events) */
+    double initial_hpwl;    /* <stage>_initial_hpwl    */
+    float initial_overflow; /* <stage>_initial_overflow */
+    float initial_lambda;   /* <stage>_initial_lambda   */
+} spg_result;
+
+/* sp::IterMetrics (src/util/metrics.h:12-28), one row per GP iteration. */
+typedef struct spg_iter_metrics {
+    int32_t iter;
+    double hpwl;
+    float overflow;
+    float lambda;
+    float gamma;
+    float step_size;
+    float grad_norm_wl;
+    float grad_norm_den;
+    float eval_lambda;
+    float eval_gamma;
+    double delta_hpwl;
+    float lambda_mu;
+    int64_t evaluations;
+} spg_iter_metrics;
+
+/* Filler plan (sp::FillerInfo, src/gp/filler.h:18-25). */
+typedef struct spg_filler_info {
+    int32_t count;
+    float width;
+    float height;
+    double whitespace_area;
+    double node_area_scaled;
+    double total_filler_area;
+} spg_filler_info;
+
+int spg_abi_version(void);
+const char* spg_last_error(void);
+/* 0 when a usable sm_100 device is visible, else SPG_E_NO_DEVICE. */
+int spg_device_check(void);
+
+/* ------------------------------------------------------------------ Poisson operator
+ * Replaces PoissonBackend::solve (src/numeric/poisson_backend.h:36-37) built by
+ * makePoissonBackend({nx, ny, step_x, step_y, prefer_gpu}) (poisson_backend.h:48-60).
+ * Arrays are row-major data[x * ny + y] (src/numeric/bin_grid_span.h:13-23).
+ * Errors: SPG_E_INVALID on nx,ny < 2 or non-positive steps (cpu_poisson.cpp:78-83);
+ * SPG_E_NO_DEVICE when no device (cuda_poisson.cu:328-336 returns nullptr there).
+ * solve() allocates nothing (poisson_backend.h:35).
+ */
+typedef struct spg_poisson spg_poisson;
+int spg_poisson_create(int nx, int ny, float step_x, float step_y, int precision,
+                       spg_poisson** out);
+/* Host arrays in and out; copies inside (like CudaPoissonBackend::solve). */
+int spg_poisson_solve(spg_poisson* h, const float* rho, float* phi, float* field_x,
+                      float* field_y);
+/* Device arrays in and out, work enqueued on `stream` (a cudaStream_t, 0 = default). */
+int spg_poisson_solve_device(spg_poisson* h, const float* d_rho, float* d_phi,
+                             float* d_field_x, float* d_field_y, void* stream);
+/* Batched device solve: `batch` grids stored back to back (each nx*ny floats). */
+int spg_poisson_solve_batch_device(spg_poisson* h, int batch, const float* d_rho,
+                                   float* d_phi, float* d_field_x, float* d_field_y,
+                                   void* stream);
+const char* spg_poisson_name(const spg_poisson* h);
+int spg_poisson_destroy(spg_poisson* h);
+
+/* ------------------------------------------------------------------ fillers (host)
+ * initializeFillers (src/gp/filler.cpp:47-139): size and count from the view's movable
+ * nodes, rows and fixed nodes; scatterFillers (src/gp/filler.cpp:33-45): mt19937 seeded
+ * uniform positions, written to x/y (count entries each).
+ */
+int spg_fillers_plan(const spg_db_view* db, float target_density, spg_filler_info* out);
+int spg_fillers_scatter(const spg_db_view* db, int32_t count, float width, float height,
+                        uint64_t seed, float* x, float* y);
+
+/* ------------------------------------------------------------------ placement context
+ * Replaces EPlace(PlaceDB&, const Config&, MetricsSink&) + EPlace::run (src/gp/eplace.h:56-77)
+ * as called by GlobalPlaceStage::run (src/stages/gp_stage.cpp:99-201). The view is copied
+ * to the device at create; positions stay device-resident until spg_positions_d2h.
+ */
+typedef struct spg_ctx spg_ctx;
+int spg_ctx_create(const spg_db_view* db, const spg_params* params, spg_ctx** out);
+int spg_ctx_destroy(spg_ctx* ctx);
+
+/* Upload new centre positions for all num_nodes + num_fillers nodes. */
+int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y);
+/* Download the current centre positions of all nodes. */
+int spg_positions_d2h(spg_ctx* ctx, float* x, float* y);
+/* Replace node flags (e.g. macros frozen by mLG get SPG_F_FIXED, gp_stage.cpp:130-177). */
+int spg_flags_h2d(spg_ctx* ctx, const uint8_t* flags);
+
+/* BinGrid::initialize (src/gp/bin_grid.cpp:64-189): static terminal/base density and the
+ * grid dimension for the current flags. bin_dim <= 0 selects the automatic dimension. */
+int spg_grid_init(spg_ctx* ctx, float target_density, int bin_dim);
+int spg_grid_info(const spg_ctx* ctx, int* dim, float* step_x, float* step_y,
+                  float* origin_x, float* origin_y, double* overflow_denominator);
+/* which: 0 node density, 1 filler density, 2 terminal, 3 base, 4 rho, 5 phi, 6 xi_x, 7 xi_y */
+int spg_grid_read(const spg_ctx* ctx, int which, float* out);
+/* The bit-exact 64-bit fixed-point density maps (node, filler) and their scale 2^-shift. */
+int spg_grid_read_fixed(const spg_ctx* ctx, int64_t* node_fixed, int64_t* filler_fixed,
+                        int* shift);
+
+/* Operator parity hooks (each runs on the device over the uploaded positions). */
+int spg_density_accumulate(spg_ctx* ctx);                     /* BinGrid::accumulate  */
+int spg_overflow(spg_ctx* ctx, float* tau);                   /* BinGrid::overflow    */
+int spg_solve_field(spg_ctx* ctx);                            /* BinGrid::solveField  */
+/* BinGrid::gatherForce: force (q*xi, NOT gradient) for every non-fixed node, 2*total floats. */
+int spg_gather_force(spg_ctx* ctx, float* force);
+/* BinGrid::totalCharge (exact sum of the fixed-point contributions). */
+int spg_total_charge(spg_ctx* ctx, double* charge);
+/* WaWirelength::compute (src/gp/wa_wirelength.cpp:46-180): grad = [x..., y...] over num_movable. */
+int spg_wa_wirelength(spg_ctx* ctx, float gamma, int ignore_net_degree, double* wl, float* grad);
+/* computeHPWL (src/db/hpwl.cpp:13-39). */
+int spg_hpwl(spg_ctx* ctx, double* hpwl);
+
+/* EPlace::run (src/gp/eplace.cpp:223-526): the device-resident Nesterov loop for one stage.
+ * Rebuilds the grid with the current flags (as constructing EPlace does,
+ * gp_stage.cpp:175-177), runs to convergence, stagnation or max_iter, and leaves the
+ * delivered positions on the device. */
+int spg_stage_run(spg_ctx* ctx, int stage, spg_result* result);
+/* Per-iteration metrics of the last stage run (up to `cap` rows). */
+int spg_metrics_d2h(const spg_ctx* ctx, spg_iter_metrics* rows, int cap, int* n_rows);
+
+/* Number of kernels this library launched on the context's stream so far. */
+int64_t spg_ctx_launch_count(const spg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPGPU_H_ */

@@ -1,0 +1,206 @@
+"""ctypes access to oracle/_ref/libspref.so: the reference's OWN CPU code for the GP path
+(built from its sources by oracle/Makefile). Test infrastructure: only tests/, the smoke
+check and the CPU-baseline leg of bench.py use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from superplace_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libspref.so")
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(LIB_PATH)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(LIB_PATH)
+        vp, fp, dp, ip = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.spref_last_error.restype = C.c_char_p
+        L.spref_db_create.restype = vp
+        L.spref_db_create.argtypes = [C.POINTER(abi.DbView)]
+        L.spref_db_destroy.argtypes = [vp]
+        L.spref_db_counts.argtypes = [vp, ip]
+        L.spref_db_regions.argtypes = [vp, fp, dp]
+        L.spref_db_get_nodes.argtypes = [vp, fp, fp, fp, fp, C.POINTER(C.c_uint8)]
+        L.spref_db_set_xy.argtypes = [vp, fp, fp]
+        L.spref_db_set_flags.argtypes = [vp, C.POINTER(C.c_uint8)]
+        L.spref_fillers_init.argtypes = [vp, C.c_float, C.c_uint64, dp]
+        L.spref_fillers_scatter.argtypes = [vp, C.c_uint64, C.c_uint64]
+        L.spref_grid_create.restype = vp
+        L.spref_grid_create.argtypes = [vp, C.c_float, C.c_int, C.c_int]
+        L.spref_grid_destroy.argtypes = [vp]
+        L.spref_grid_info.argtypes = [vp, fp, dp]
+        L.spref_grid_accumulate.argtypes = [vp, vp]
+        L.spref_grid_overflow.restype = C.c_float
+        L.spref_grid_overflow.argtypes = [vp]
+        L.spref_grid_solve.argtypes = [vp]
+        L.spref_grid_gather.argtypes = [vp, vp, fp]
+        L.spref_grid_total_charge.restype = C.c_double
+        L.spref_grid_total_charge.argtypes = [vp, vp]
+        L.spref_grid_read.argtypes = [vp, C.c_int, fp]
+        L.spref_wa.restype = C.c_double
+        L.spref_wa.argtypes = [vp, C.c_float, C.c_int, fp]
+        L.spref_hpwl.restype = C.c_double
+        L.spref_hpwl.argtypes = [vp]
+        L.spref_gamma.restype = C.c_float
+        L.spref_gamma.argtypes = [C.c_float, C.c_float]
+        L.spref_poisson.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, fp, fp, fp, fp]
+        L.spref_poisson_bench.restype = C.c_double
+        L.spref_poisson_bench.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, fp]
+        L.spref_eplace_run.argtypes = [vp, C.POINTER(abi.Params), C.c_int, dp, dp, dp, C.c_int, ip]
+        L.spref_nesterov_quadratic.argtypes = [C.c_int, fp, fp, fp, C.c_int, C.c_int, C.c_int,
+                                               C.c_float, dp]
+        L.spref_set_threads.argtypes = [C.c_int]
+        L.spref_max_threads.restype = C.c_int
+        L.spref_quiet.argtypes = [C.c_int]
+        L.spref_quiet(1)
+        _lib = L
+    return _lib
+
+
+def _f(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+class RefDb:
+    """A reference sp::PlaceDB built from a superplace_b200 PlaceDB."""
+
+    def __init__(self, db):
+        self._view = db.view()
+        self.h = lib().spref_db_create(C.byref(self._view))
+        if not self.h:
+            raise RuntimeError(lib().spref_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().spref_db_destroy(self.h)
+            self.h = None
+
+    def counts(self):
+        c = (C.c_int * 5)()
+        lib().spref_db_counts(self.h, c)
+        return tuple(c)
+
+    def nodes(self):
+        total = self.counts()[1] + self.counts()[2]
+        x, y, w, h = (np.zeros(total, np.float32) for _ in range(4))
+        f = np.zeros(total, np.uint8)
+        lib().spref_db_get_nodes(self.h, abi.fptr(x), abi.fptr(y), abi.fptr(w), abi.fptr(h),
+                                 abi.u8ptr(f))
+        return x, y, w, h, f
+
+    def set_xy(self, x, y):
+        x, y = _f(x), _f(y)
+        lib().spref_db_set_xy(self.h, abi.fptr(x), abi.fptr(y))
+
+    def set_flags(self, flags):
+        f = np.ascontiguousarray(flags, np.uint8)
+        lib().spref_db_set_flags(self.h, abi.u8ptr(f))
+
+    def fillers_init(self, target_density=1.0, seed=1002):
+        info = (C.c_double * 6)()
+        rc = lib().spref_fillers_init(self.h, target_density, seed, info)
+        if rc:
+            raise RuntimeError(lib().spref_last_error().decode())
+        return list(info)
+
+    def hpwl(self):
+        return lib().spref_hpwl(self.h)
+
+    def wa(self, gamma, ignore=100):
+        n = self.counts()[0]
+        g = np.zeros(2 * n, np.float32)
+        wl = lib().spref_wa(self.h, gamma, ignore, abi.fptr(g))
+        return wl, g
+
+    def eplace(self, params, stage=abi.STAGE_MGP, cap=4000):
+        res = (C.c_double * 8)()
+        init = (C.c_double * 3)()
+        rows = np.zeros((cap, 8), np.float64)
+        nrows = C.c_int(0)
+        rc = lib().spref_eplace_run(self.h, C.byref(params), stage, res, init,
+                                    rows.ctypes.data_as(C.POINTER(C.c_double)), cap,
+                                    C.byref(nrows))
+        if rc:
+            raise RuntimeError(f"{rc}: " + lib().spref_last_error().decode())
+        keys = ("iterations", "hpwl", "overflow", "converged", "stagnated", "rollback_iter",
+                "evaluations", "elapsed_ms")
+        return dict(zip(keys, list(res))), rows[: nrows.value]
+
+
+class RefGrid:
+    def __init__(self, rdb: RefDb, target_density=1.0, bin_dim=0, chunks=0):
+        self.rdb = rdb
+        self.h = lib().spref_grid_create(rdb.h, target_density, bin_dim, chunks)
+        if not self.h:
+            raise RuntimeError(lib().spref_last_error().decode())
+        info = (C.c_float * 5)()
+        den = C.c_double()
+        lib().spref_grid_info(self.h, info, C.byref(den))
+        self.dim = int(info[0])
+        self.step_x, self.step_y, self.origin_x, self.origin_y = info[1], info[2], info[3], info[4]
+        self.overflow_denominator = den.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().spref_grid_destroy(self.h)
+            self.h = None
+
+    def accumulate(self):
+        lib().spref_grid_accumulate(self.h, self.rdb.h)
+
+    def overflow(self):
+        return lib().spref_grid_overflow(self.h)
+
+    def solve(self):
+        lib().spref_grid_solve(self.h)
+
+    def gather(self):
+        total = self.rdb.counts()[1] + self.rdb.counts()[2]
+        f = np.zeros(2 * total, np.float32)
+        lib().spref_grid_gather(self.h, self.rdb.h, abi.fptr(f))
+        return f
+
+    def total_charge(self):
+        return lib().spref_grid_total_charge(self.h, self.rdb.h)
+
+    def read(self, which):
+        out = np.zeros(self.dim * self.dim, np.float32)
+        lib().spref_grid_read(self.h, which, abi.fptr(out))
+        return out.reshape(self.dim, self.dim)
+
+
+def poisson(rho, step_x, step_y):
+    rho = _f(rho)
+    nx, ny = rho.shape
+    phi, ex, ey = (np.zeros_like(rho) for _ in range(3))
+    rc = lib().spref_poisson(nx, ny, step_x, step_y, abi.fptr(rho), abi.fptr(phi),
+                             abi.fptr(ex), abi.fptr(ey))
+    if rc:
+        raise RuntimeError(lib().spref_last_error().decode())
+    return phi, ex, ey
+
+
+def gamma(tau, step):
+    return lib().spref_gamma(tau, step)
+
+
+def nesterov_quadratic(coef, target, pos, steps, use_bb=True, backtrack=False, init_step=0.0):
+    coef, target = _f(coef), _f(target)
+    pos = _f(pos).copy()
+    out = (C.c_double * 3)()
+    rc = lib().spref_nesterov_quadratic(pos.size, abi.fptr(coef), abi.fptr(target), abi.fptr(pos),
+                                        steps, int(use_bb), int(backtrack), init_step, out)
+    if rc:
+        raise RuntimeError(lib().spref_last_error().decode())
+    return pos, out[0], int(out[1]), out[2]

@@ -1,0 +1,419 @@
+// C entry points onto the reference's OWN CPU implementation of the GP path, compiled
+// from the reference sources (see oracle/Makefile). Test infrastructure only: tests and
+// the CPU-baseline leg of the benchmark load it to check and time against; the product
+// never links it.
+//
+// Every function builds or drives reference objects directly:
+//   sp::PlaceDB (src/db/place_db.h), sp::BinGrid (src/gp/bin_grid.h),
+//   sp::WaWirelength (src/gp/wa_wirelength.h), sp::computeHPWL (src/db/hpwl.h),
+//   sp::initializeFillers (src/gp/filler.h), sp::EPlace (src/gp/eplace.h),
+//   sp::makeNesterov (src/numeric/optimizer.h), sp::makePoissonBackend
+//   (src/numeric/poisson_backend.h; CPU backend = oracle/ref_shim/poisson_shim.cpp).
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "db/hpwl.h"
+#include "db/place_db.h"
+#include "gp/bin_grid.h"
+#include "gp/eplace.h"
+#include "gp/filler.h"
+#include "gp/wa_wirelength.h"
+#include "numeric/optimizer.h"
+#include "numeric/poisson_backend.h"
+#include "spgpu.h"
+#include "util/config.h"
+#include "util/invariant.h"
+#include "util/logger.h"
+#include "util/metrics.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+struct RefDb {
+    sp::PlaceDB db;
+};
+
+struct RefGrid {
+    sp::BinGrid grid;
+};
+
+int fail(const std::exception& e) {
+    g_err = e.what();
+    if (auto* ie = dynamic_cast<const sp::InvariantError*>(&e)) {
+        if (ie->kind == "non_finite") return SPG_E_NON_FINITE;
+        if (ie->kind == "out_of_core") return SPG_E_OUT_OF_CORE;
+        if (ie->kind == "convergence_mismatch") return SPG_E_CONVERGENCE;
+        if (ie->kind == "rollback_mismatch") return SPG_E_ROLLBACK;
+    }
+    return SPG_E_INVALID;
+}
+
+void buildDb(sp::PlaceDB& db, const spg_db_view* v) {
+    const int total = v->num_nodes + v->num_fillers;
+    db.numMovable = v->num_movable;
+    db.numNodes = v->num_nodes;
+    db.numFillers = v->num_fillers;
+    db.reserveNodes(total);
+    for (int i = 0; i < total; ++i) {
+        db.addNode("o" + std::to_string(i), v->node_w[i], v->node_h[i], v->node_flags[i]);
+        db.node_x[static_cast<size_t>(i)] = v->node_x[i];
+        db.node_y[static_cast<size_t>(i)] = v->node_y[i];
+    }
+    db.numPins = v->num_pins;
+    db.numNets = v->num_nets;
+    db.pin_offset_x.assign(v->pin_offset_x, v->pin_offset_x + v->num_pins);
+    db.pin_offset_y.assign(v->pin_offset_y, v->pin_offset_y + v->num_pins);
+    db.pin2node.assign(v->pin2node, v->pin2node + v->num_pins);
+    db.pin2net.assign(v->pin2net, v->pin2net + v->num_pins);
+    db.net2pin_start.assign(v->net2pin_start, v->net2pin_start + v->num_nets + 1);
+    db.flat_net2pin.assign(v->flat_net2pin, v->flat_net2pin + v->num_pins);
+    db.node2pin_start.assign(v->node2pin_start, v->node2pin_start + total + 1);
+    db.flat_node2pin.assign(v->flat_node2pin, v->flat_node2pin + v->num_pins);
+    db.net_weight.assign(static_cast<size_t>(v->num_nets), 1.f);
+    db.net_name.assign(static_cast<size_t>(v->num_nets), "n");
+    for (int r = 0; r < v->num_rows; ++r) {
+        sp::PlaceDB::SiteRow row;
+        row.ly = v->row_ly[r];
+        row.height = v->row_height[r];
+        row.lx = v->row_lx[r];
+        row.step = v->row_step[r];
+        row.numSites = v->row_num_sites[r];
+        db.rows.push_back(row);
+    }
+    db.computeRegions();
+}
+
+sp::Config makeConfig(const spg_params* p) {
+    sp::Config c;
+    c.target_density = p->target_density;
+    c.target_overflow = p->target_overflow;
+    c.cgp_target_overflow = p->cgp_target_overflow;
+    c.gp_max_iter = p->gp_max_iter;
+    c.ignore_net_degree = p->ignore_net_degree;
+    c.gp_bin_dim = p->gp_bin_dim;
+    c.filler_only_iters = p->filler_only_iters;
+    c.delta_hpwl_ref = p->delta_hpwl_ref;
+    c.lambda_schedule = p->lambda_schedule_relative ? "relative" : "fixed";
+    c.delta_hpwl_relative = p->delta_hpwl_relative;
+    c.use_bb = p->use_bb != 0;
+    c.gp_backtrack = p->gp_backtrack != 0;
+    c.gp_stagnation_window = p->gp_stagnation_window;
+    c.gp_stagnation_min_gain = p->gp_stagnation_min_gain;
+    c.random_seed = p->random_seed;
+    c.poisson_backend = "cpu";
+    c.verbose = p->verbose != 0;
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* spref_last_error(void) { return g_err.c_str(); }
+
+void spref_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+int spref_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void spref_quiet(int quiet) {
+    sp::Logger::get().setLevel(quiet ? sp::LogLevel::kError : sp::LogLevel::kInfo);
+}
+
+// ------------------------------------------------------------------ PlaceDB
+void* spref_db_create(const spg_db_view* v) {
+    try {
+        auto* r = new RefDb;
+        buildDb(r->db, v);
+        return r;
+    } catch (const std::exception& e) {
+        fail(e);
+        return nullptr;
+    }
+}
+
+void spref_db_destroy(void* h) { delete static_cast<RefDb*>(h); }
+
+// counts[0..4] = numMovable, numNodes, numFillers, numPins, numNets
+void spref_db_counts(void* h, int* counts) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    counts[0] = db.numMovable;
+    counts[1] = db.numNodes;
+    counts[2] = db.numFillers;
+    counts[3] = db.numPins;
+    counts[4] = db.numNets;
+}
+
+// core[0..3] = core lx ly hx hy, core[4] = rowHeight ; area = totalRowArea
+void spref_db_regions(void* h, float* core, double* area) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    core[0] = db.coreRegion.lx;
+    core[1] = db.coreRegion.ly;
+    core[2] = db.coreRegion.hx;
+    core[3] = db.coreRegion.hy;
+    core[4] = db.rowHeight;
+    *area = db.totalRowArea;
+}
+
+void spref_db_get_nodes(void* h, float* x, float* y, float* w, float* hh, uint8_t* flags) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    const size_t n = static_cast<size_t>(db.totalNodes());
+    if (x) std::memcpy(x, db.node_x.data(), n * sizeof(float));
+    if (y) std::memcpy(y, db.node_y.data(), n * sizeof(float));
+    if (w) std::memcpy(w, db.node_w.data(), n * sizeof(float));
+    if (hh) std::memcpy(hh, db.node_h.data(), n * sizeof(float));
+    if (flags) std::memcpy(flags, db.node_flags.data(), n);
+}
+
+void spref_db_set_xy(void* h, const float* x, const float* y) {
+    sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    const size_t n = static_cast<size_t>(db.totalNodes());
+    std::memcpy(db.node_x.data(), x, n * sizeof(float));
+    std::memcpy(db.node_y.data(), y, n * sizeof(float));
+}
+
+void spref_db_set_flags(void* h, const uint8_t* flags) {
+    sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    std::memcpy(db.node_flags.data(), flags, static_cast<size_t>(db.totalNodes()));
+}
+
+// ------------------------------------------------------------------ fillers
+// info[0..5] = count, width, height, whitespaceArea, nodeAreaScaled, totalFillerArea
+int spref_fillers_init(void* h, float targetDensity, uint64_t seed, double* info) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+        sp::Config cfg;
+        cfg.target_density = targetDensity;
+        cfg.random_seed = seed;
+        const sp::FillerInfo fi = sp::initializeFillers(db, cfg);
+        info[0] = fi.count;
+        info[1] = fi.width;
+        info[2] = fi.height;
+        info[3] = fi.whitespaceArea;
+        info[4] = fi.nodeAreaScaled;
+        info[5] = fi.totalFillerArea;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+int spref_fillers_scatter(void* h, uint64_t seed, uint64_t seedOffset) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+        sp::Config cfg;
+        cfg.random_seed = seed;
+        sp::scatterFillers(db, cfg, seedOffset);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// ------------------------------------------------------------------ BinGrid
+void* spref_grid_create(void* dbh, float targetDensity, int binDim, int chunks) {
+    try {
+        auto* g = new RefGrid;
+        g->grid.initialize(static_cast<RefDb*>(dbh)->db, targetDensity, binDim, chunks, false, 4);
+        return g;
+    } catch (const std::exception& e) {
+        fail(e);
+        return nullptr;
+    }
+}
+
+void spref_grid_destroy(void* g) { delete static_cast<RefGrid*>(g); }
+
+// info[0..4] = dim, stepX, stepY, originX, originY ; den = overflowDenominator
+void spref_grid_info(void* g, float* info, double* den) {
+    const sp::BinGrid& grid = static_cast<RefGrid*>(g)->grid;
+    info[0] = static_cast<float>(grid.dim());
+    info[1] = grid.stepX();
+    info[2] = grid.stepY();
+    info[3] = grid.originX();
+    info[4] = grid.originY();
+    *den = grid.overflowDenominator();
+}
+
+void spref_grid_accumulate(void* g, void* dbh) {
+    static_cast<RefGrid*>(g)->grid.accumulate(static_cast<RefDb*>(dbh)->db);
+}
+
+float spref_grid_overflow(void* g) { return static_cast<RefGrid*>(g)->grid.overflow(); }
+
+void spref_grid_solve(void* g) { static_cast<RefGrid*>(g)->grid.solveField(); }
+
+void spref_grid_gather(void* g, void* dbh, float* force) {
+    static_cast<RefGrid*>(g)->grid.gatherForce(static_cast<RefDb*>(dbh)->db, force);
+}
+
+double spref_grid_total_charge(void* g, void* dbh) {
+    return static_cast<RefGrid*>(g)->grid.totalCharge(static_cast<RefDb*>(dbh)->db);
+}
+
+// which: 0 node, 1 filler, 2 terminal, 3 base, 5 phi, 6 xi_x, 7 xi_y
+void spref_grid_read(void* g, int which, float* out) {
+    const sp::BinGrid& grid = static_cast<RefGrid*>(g)->grid;
+    const std::vector<float>* v = nullptr;
+    switch (which) {
+        case 0: v = &grid.nodeDensity(); break;
+        case 1: v = &grid.fillerDensity(); break;
+        case 2: v = &grid.terminalDensity(); break;
+        case 3: v = &grid.baseDensity(); break;
+        case 5: v = &grid.potential(); break;
+        case 6: v = &grid.fieldX(); break;
+        case 7: v = &grid.fieldY(); break;
+        default: return;
+    }
+    std::memcpy(out, v->data(), v->size() * sizeof(float));
+}
+
+// ------------------------------------------------------------------ WA / HPWL
+double spref_wa(void* dbh, float gamma, int ignoreDeg, float* grad) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(dbh)->db;
+    sp::WaWirelength wa;
+    wa.prepare(db);
+    double wl = 0.0;
+    wa.compute(db, gamma, ignoreDeg, &wl, grad);
+    return wl;
+}
+
+double spref_hpwl(void* dbh) { return sp::computeHPWL(static_cast<RefDb*>(dbh)->db); }
+
+float spref_gamma(float tau, float binStep) { return sp::computeGamma(tau, binStep); }
+
+// ------------------------------------------------------------------ Poisson
+int spref_poisson(int nx, int ny, float sx, float sy, const float* rho, float* phi, float* ex,
+                  float* ey) {
+    try {
+        auto be = sp::makePoissonBackend({nx, ny, sx, sy, false, 4});
+        std::vector<float> in(rho, rho + static_cast<size_t>(nx) * ny);
+        be->solve({in.data(), nx, ny}, {phi, nx, ny}, {ex, nx, ny}, {ey, nx, ny});
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// Times `rounds` solves after `warm` warm-up solves (tools/poisson_bench/main.cpp:13-33);
+// returns milliseconds per solve.
+double spref_poisson_bench(int n, int warm, int rounds, int fftwThreads, const float* rho) {
+    try {
+        auto be = sp::makePoissonBackend({n, n, 1.f, 1.f, false, fftwThreads});
+        std::vector<float> in(rho, rho + static_cast<size_t>(n) * n), a(in.size()), b(in.size()),
+            c(in.size());
+        for (int i = 0; i < warm; ++i) be->solve({in.data(), n, n}, {a.data(), n, n}, {b.data(), n, n}, {c.data(), n, n});
+        const double t0 = omp_get_wtime();
+        for (int i = 0; i < rounds; ++i) be->solve({in.data(), n, n}, {a.data(), n, n}, {b.data(), n, n}, {c.data(), n, n});
+        return (omp_get_wtime() - t0) * 1e3 / rounds;
+    } catch (const std::exception& e) {
+        fail(e);
+        return -1.0;
+    }
+}
+
+// ------------------------------------------------------------------ EPlace
+// result[0..7] = iterations, hpwl, overflow, converged, stagnated, rollbackIter,
+//                evaluations, elapsed_ms
+// init[0..2]   = initial hpwl, initial overflow, initial lambda (summary keys)
+// rows: up to cap metrics rows, 8 doubles each:
+//       iter, hpwl, overflow, lambda, gamma, step, evaluations, elapsed_ms
+int spref_eplace_run(void* dbh, const spg_params* p, int stage, double* result, double* init,
+                     double* rows, int cap, int* nRows) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(dbh)->db;
+        const sp::Config cfg = makeConfig(p);
+        sp::MetricsSink sink;
+        sp::EPlace engine(db, cfg, sink);
+        const sp::GpStage st = stage == SPG_STAGE_MGP ? sp::GpStage::kMGP
+                             : stage == SPG_STAGE_FILLER_ONLY ? sp::GpStage::kFillerOnly
+                                                              : sp::GpStage::kCGP;
+        const double t0 = omp_get_wtime();
+        const sp::GpResult r = engine.run(st);
+        const double ms = (omp_get_wtime() - t0) * 1e3;
+        result[0] = r.iterations;
+        result[1] = r.hpwl;
+        result[2] = r.overflow;
+        result[3] = r.converged;
+        result[4] = r.stagnated;
+        result[5] = r.rollbackIter;
+        result[6] = static_cast<double>(r.evaluations);
+        result[7] = ms;
+        const std::string prefix = std::string(sp::toString(st)) + "_";
+        const auto& m = sink.stageMetrics(sp::toString(st));
+        int n = 0;
+        for (const auto& row : m) {
+            if (n >= cap) break;
+            double* o = rows + 8 * n;
+            o[0] = row.iter;
+            o[1] = row.hpwl;
+            o[2] = row.overflow;
+            o[3] = row.lambda;
+            o[4] = row.gamma;
+            o[5] = row.step_size;
+            o[6] = static_cast<double>(row.evaluations);
+            o[7] = row.elapsed_ms;
+            ++n;
+        }
+        *nRows = n;
+        (void)init;
+        (void)prefix;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// ------------------------------------------------------------------ Nesterov
+// Minimises f(x) = 0.5 * sum c_i (x_i - t_i)^2 (test/test_nesterov.cpp:14-27) for `steps`
+// steps with the reference optimizer. cfgv = {use_bb, backtrack, init_step}.
+// Writes the final positions to pos; out[0..2] = objective, evaluations, step size.
+int spref_nesterov_quadratic(int n, const float* coef, const float* target, float* pos,
+                             int steps, int useBb, int backtrack, float initStep, double* out) {
+    try {
+        std::vector<float> c(coef, coef + n), t(target, target + n);
+        auto f = [&](const float* x, float* g, double* obj) {
+            double o = 0.0;
+            for (int i = 0; i < n; ++i) {
+                const double d = static_cast<double>(x[i]) - t[static_cast<size_t>(i)];
+                o += 0.5 * c[static_cast<size_t>(i)] * d * d;
+                g[i] = static_cast<float>(c[static_cast<size_t>(i)] * d);
+            }
+            *obj = o;
+        };
+        sp::OptConfig cfg;
+        cfg.use_bb = useBb != 0;
+        cfg.backtrack = backtrack != 0;
+        cfg.init_step = initStep;
+        auto opt = sp::makeNesterov(f, nullptr, cfg);
+        for (int k = 0; k < steps; ++k) opt->step(pos, n);
+        out[0] = opt->objective();
+        out[1] = static_cast<double>(opt->evaluations());
+        out[2] = opt->stepSize();
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+}  // extern "C"
