@@ -1,0 +1,333 @@
+"""Benchmark: mGP iterations/s on the 211k-cell synthetic netlist (512x512 bins, tau 0.10).
+
+One "step" is one complete mGP stage (lambda_0 probe, initial-step estimate, Nesterov
+iterations with backtracking until tau < 0.10 or stagnation) from the same initial
+placement. Metric: mGP iterations per second = sum(iterations) / sum(iteration-loop time),
+the reference's own definition (mGP_iterations / durations_ms["mGP"],
+src/gp/eplace.cpp:310,515).
+
+  value  loop time from CUDA events on the engine's stream (inputs resident in HBM)
+  e2e    the same metric through the public API (EPlace.run on a host PlaceDB): H2D of
+         positions/flags, stage set-up, the loop and the D2H of the delivered positions,
+         bracketed by CUDA events on the engine's stream
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                       [--precision fp32|bf16x3] [--workload large|small]
+Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from superplace_b200 import abi, generator  # noqa: E402
+
+WORKLOADS = {
+    "large": dict(desc="mGP to tau<0.10, 211k-cell synthetic netlist (543 fixed macros, 35% "
+                       "blocked), 221k nets, 512x512 bins", bin_dim=512),
+    "small": dict(desc="mGP to tau<0.10, 2k-cell synthetic netlist, 64x64 bins", bin_dim=64),
+}
+METRIC = "mGP iters/s at 211k cells (tau=0.10)"
+
+
+def make_design(workload, seed=1002):
+    if workload == "large":
+        return generator.large_design(seed)
+    return generator.small_design(seed)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.idx)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p["bf16_tflops"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import ref
+
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libspref.so not built"}))
+        return 0
+    db = make_design(args.workload)
+    from superplace_b200 import engine  # host-only filler routines (no device needed)
+
+    engine.initialize_fillers(db, 1.0, 1002)
+    threads = os.cpu_count() or 1
+    ref.lib().spref_set_threads(threads)
+    sample_iters = args.ref_iters
+    params = abi.default_params(gp_bin_dim=WORKLOADS[args.workload]["bin_dim"],
+                                gp_max_iter=sample_iters)
+    iters, ms = [], []
+    for k in range(args.warmup + args.steps):
+        r = ref.RefDb(db)
+        res, rows = r.eplace(params)
+        if k >= args.warmup:
+            iters.append(len(rows))
+            ms.append(rows[-1, 7] if len(rows) else res["elapsed_ms"])
+    value = sum(iters) / (sum(ms) / 1e3)
+    sample = (f"first {sample_iters} mGP iterations of the same instance (reference CPU "
+              f"EPlace built from its sources, FFT stand-in for FFTW)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "iter/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sum(ms) / len(ms), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload]["desc"], "cells": int(db.num_movable),
+                   "fillers": int(db.num_fillers), "pins": int(db.num_pins),
+                   "nets": int(db.num_nets), "bins": WORKLOADS[args.workload]["bin_dim"],
+                   "sample_iterations": sample_iters},
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+def cpu_baseline_sample(db, workload, iters=8):
+    """The reference's CPU EPlace on the same instance, bounded sample, all host cores."""
+    try:
+        from oracle import ref
+
+        if not ref.available():
+            return None
+        threads = os.cpu_count() or 1
+        ref.lib().spref_set_threads(threads)
+        r = ref.RefDb(db)
+        _, rows = r.eplace(abi.default_params(gp_bin_dim=WORKLOADS[workload]["bin_dim"], gp_max_iter=iters))
+        v = len(rows) / (rows[-1, 7] / 1e3)
+        return {"value": v, "unit": "iter/s", "cores": threads, "kind": "reference",
+                "sample": f"first {iters} mGP iterations of this instance on the reference CPU "
+                          f"EPlace built from its sources (FFT stand-in for FFTW)"}
+    except Exception as e:  # the baseline must not hide our number
+        return {"value": None, "unit": "iter/s", "cores": 0, "kind": "reference",
+                "sample": f"failed: {e}"}
+
+
+def time_poisson(dim, step_x, step_y, precision, reps=50):
+    """Average device time of one Poisson solve (the dominant kernel group) with CUDA
+    events on the launching stream; inputs resident."""
+    import torch
+
+    from superplace_b200 import engine
+
+    be = engine.PoissonBackend(dim, dim, step_x, step_y, precision)
+    rng = np.random.default_rng(7)
+    rho = torch.from_numpy(rng.random((dim, dim), dtype=np.float32)).cuda()
+    out = [torch.empty_like(rho) for _ in range(3)]
+    s = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    for _ in range(5):
+        be.solve_device(rho.data_ptr(), *(o.data_ptr() for o in out), stream=s.cuda_stream)
+    times = []
+    for _ in range(reps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        be.solve_device(rho.data_ptr(), *(o.data_ptr() for o in out), stream=s.cuda_stream)
+        e1.record(s)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return statistics.median(times)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from superplace_b200 import engine
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    precision = abi.POISSON_BF16X3 if args.precision == "bf16x3" else abi.POISSON_FP32
+    db = make_design(args.workload)
+    engine.initialize_fillers(db, 1.0, 1002)
+    init_x, init_y = db.node_x.copy(), db.node_y.copy()
+    params = abi.default_params(gp_bin_dim=WORKLOADS[args.workload]["bin_dim"],
+                                poisson_precision=precision)
+    ep = engine.EPlace(db, params)
+    stream = torch.cuda.ExternalStream(ep.ctx.stream())
+
+    def step():
+        db.node_x[:] = init_x
+        db.node_y[:] = init_y
+        return ep.run(abi.STAGE_MGP)
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = engine.launch_count()
+    iters, loop_ms, e2e_ms, hpwl, tau = [], [], [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = step()
+            e1.record(stream)
+            e1.synchronize()
+            e2e_ms.append(e0.elapsed_time(e1))
+            iters.append(r.iterations)
+            loop_ms.append(r.elapsed_ms)
+            hpwl.append(r.hpwl)
+            tau.append(r.overflow)
+    torch.cuda.synchronize()
+    launches = engine.launch_count() - launches0
+    if world > 1:
+        dist.barrier()
+    t_loop = sum(loop_ms) / 1e3
+    t_e2e = sum(e2e_ms) / 1e3
+    if world > 1:
+        tl = torch.tensor([t_loop, t_e2e], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tl, op=dist.ReduceOp.MAX)
+        t_loop, t_e2e = float(tl[0]), float(tl[1])
+    total_iters = sum(iters) * world
+    value = total_iters / t_loop
+    e2e = total_iters / t_e2e
+    if rank == 0:
+        info = ep.ctx.grid_info()
+        dim = info["dim"]
+        hbm, bf16, peak_kind = peaks()
+        t_solve_ms = time_poisson(dim, info["step_x"], info["step_y"], precision)
+        flops = 14.0 * dim ** 3
+        achieved = flops / (t_solve_ms * 1e-3) / 1e12
+        total = db.total_nodes
+        h2d = 2 * 4 * total + total  # positions x, y and flags
+        d2h = 2 * 4 * total
+        line = {
+            "metric": METRIC, "value": value, "unit": "iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sum(loop_ms) / len(loop_ms), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if precision == abi.POISSON_FP32 else "bf16x3+f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOADS[args.workload]["desc"], "cells": int(db.num_movable),
+                       "fillers": int(db.num_fillers), "pins": int(db.num_pins),
+                       "nets": int(db.num_nets), "bins": dim,
+                       "poisson": args.precision, "step": "one full mGP stage run",
+                       "iterations_per_step": iters, "final_hpwl": hpwl, "final_tau": tau,
+                       "l2": "working set (~100 MB) is L2-resident between kernels; the "
+                             "Poisson timing flushes L2 with a 256 MB write between solves",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e, "unit": "iter/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": bf16,
+                         "unit": "TFLOP/s", "frac": achieved / bf16, "traffic": None,
+                         "kernel": f"Poisson solve ({args.precision}, {dim}^2, 14*M^3 flops)",
+                         "peak_kind": peak_kind, "solve_ms": t_solve_ms},
+            "clocks": clk.summary(),
+        }
+        if args.cpu_baseline:
+            db.node_x[:] = init_x
+            db.node_y[:] = init_y
+            line["cpu_baseline"] = cpu_baseline_sample(db, args.workload)
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3"])
+    ap.add_argument("--workload", default="large", choices=list(WORKLOADS))
+    ap.add_argument("--ref-iters", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

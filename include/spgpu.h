@@ -179,6 +179,9 @@ int spg_device_check(void);
 typedef struct spg_poisson spg_poisson;
 int spg_poisson_create(int nx, int ny, float step_x, float step_y, int precision,
                        spg_poisson** out);
+/* As spg_poisson_create, with work buffers for batched solves of up to batch_cap grids. */
+int spg_poisson_create_batched(int nx, int ny, float step_x, float step_y, int precision,
+                               int batch_cap, spg_poisson** out);
 /* Host arrays in and out; copies inside (like CudaPoissonBackend::solve). */
 int spg_poisson_solve(spg_poisson* h, const float* rho, float* phi, float* field_x,
                       float* field_y);
@@ -224,6 +227,9 @@ int spg_grid_info(const spg_ctx* ctx, int* dim, float* step_x, float* step_y,
                   float* origin_x, float* origin_y, double* overflow_denominator);
 /* which: 0 node density, 1 filler density, 2 terminal, 3 base, 4 rho, 5 phi, 6 xi_x, 7 xi_y */
 int spg_grid_read(const spg_ctx* ctx, int which, float* out);
+/* Overwrite a device map (which: 4 rho, 5 phi, 6 xi_x, 7 xi_y) to drive an operator in
+ * isolation, e.g. gather over a given field. */
+int spg_grid_write(spg_ctx* ctx, int which, const float* in);
 /* The bit-exact 64-bit fixed-point density maps (node, filler) and their scale 2^-shift. */
 int spg_grid_read_fixed(const spg_ctx* ctx, int64_t* node_fixed, int64_t* filler_fixed,
                         int* shift);
@@ -249,8 +255,10 @@ int spg_stage_run(spg_ctx* ctx, int stage, spg_result* result);
 /* Per-iteration metrics of the last stage run (up to `cap` rows). */
 int spg_metrics_d2h(const spg_ctx* ctx, spg_iter_metrics* rows, int cap, int* n_rows);
 
-/* Number of kernels this library launched on the context's stream so far. */
+/* Number of kernels this library launched (process-wide) so far. */
 int64_t spg_ctx_launch_count(const spg_ctx* ctx);
+/* The cudaStream_t every call on this context enqueues on (for caller-side CUDA events). */
+void* spg_ctx_stream(const spg_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,110 @@
+// Shared helpers of the sm_100a GP engine: error handling, launch accounting, and the
+// bit-exact float footprint arithmetic of the density operators.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "spgpu.h"
+
+namespace spg {
+
+// A CUDA failure or a bad argument inside the library; converted to an SPG_E_* status at
+// the C ABI boundary.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define SPG_CUDA(call)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            throw ::spg::Error(SPG_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define SPG_CHECK_LAUNCH() SPG_CUDA(cudaGetLastError())
+
+#define SPG_REQUIRE(cond, code, msg)                  \
+    do {                                              \
+        if (!(cond)) throw ::spg::Error((code), (msg)); \
+    } while (0)
+
+// Count of kernels this library launched (process-wide), reported by the benchmark.
+extern int64_t g_launches;
+inline void count_launch(int n = 1) { g_launches += n; }
+
+inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------------------
+// Float arithmetic with explicit round-to-nearest intrinsics: no FMA contraction, so every
+// value equals the reference's un-contracted float expression (src/gp/bin_grid.cpp:22-54,
+// src/db/geometry.h:35-39).
+
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+// std::min / std::max on non-NaN floats
+__device__ __forceinline__ float fmin_(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float fmax_(float a, float b) { return (a < b) ? b : a; }
+
+// Geometry of the bin grid, passed by value to every density kernel.
+struct GridGeom {
+    int dim;
+    float step_x, step_y, origin_x, origin_y;
+    float target_density;
+    int shift;            // fixed-point scale 2^shift
+    double scale;         // 2^shift
+    double inv_scale;     // 2^-shift
+};
+
+// Per density node data fixed for a stage: half extents after local smoothing and the
+// charge weight (footprintOf + chargeWeight, bin_grid.cpp:22-62).
+struct Footprint {
+    int bx0, bx1, by0, by1;
+    float lx, ly, hx, hy;
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// Bin range and smoothed rectangle of a node at centre (x, y). hw/hh are the half extents
+// 0.5f*max(w, step) exactly as footprintOf forms lx = x - 0.5f*W.
+__device__ __forceinline__ Footprint footprint(const GridGeom& g, float x, float y, float hw,
+                                               float hh) {
+    Footprint f;
+    f.lx = fsub(x, hw);
+    f.hx = fadd(x, hw);
+    f.ly = fsub(y, hh);
+    f.hy = fadd(y, hh);
+    const int d = g.dim - 1;
+    f.bx0 = clampi(static_cast<int>(fdiv(fsub(f.lx, g.origin_x), g.step_x)), 0, d);
+    f.bx1 = clampi(static_cast<int>(fdiv(fsub(f.hx, g.origin_x), g.step_x)), 0, d);
+    f.by0 = clampi(static_cast<int>(fdiv(fsub(f.ly, g.origin_y), g.step_y)), 0, d);
+    f.by1 = clampi(static_cast<int>(fdiv(fsub(f.hy, g.origin_y), g.step_y)), 0, d);
+    return f;
+}
+
+// overlapArea(bin(bx,by), rect) * w (bin_grid.cpp:228-233).
+__device__ __forceinline__ float bin_contribution(const GridGeom& g, int bx, int by,
+                                                  const Footprint& f, float w) {
+    const float blx = fadd(g.origin_x, fmul(static_cast<float>(bx), g.step_x));
+    const float bly = fadd(g.origin_y, fmul(static_cast<float>(by), g.step_y));
+    const float bhx = fadd(blx, g.step_x);
+    const float bhy = fadd(bly, g.step_y);
+    const float dx = fsub(fmin_(bhx, f.hx), fmax_(blx, f.lx));
+    const float dy = fsub(fmin_(bhy, f.hy), fmax_(bly, f.ly));
+    const float a = (dx > 0.f && dy > 0.f) ? fmul(dx, dy) : 0.f;
+    return fmul(a, w);
+}
+
+// Fixed-point image of one contribution: round-to-nearest-even of c * 2^shift.
+// (c * 2^shift is exact in double, so this is one rounding.)
+__device__ __forceinline__ unsigned long long to_fixed(float c, double scale) {
+    return static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(c) * scale));
+}
+
+}  // namespace spg

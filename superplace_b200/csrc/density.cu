@@ -1,0 +1,259 @@
+// Density operators of the GP iteration on sm_100a:
+//   * fixed-point charge scatter   (BinGrid::accumulate, src/gp/bin_grid.cpp:191-251)
+//   * rho assembly + overflow tau  (BinGrid::solveField/overflow, bin_grid.cpp:253-285)
+//   * field gather q*xi            (BinGrid::gatherForce, bin_grid.cpp:287-318)
+//
+// Scatter: every contribution overlap(bin, rect) * w is formed with the reference's float
+// operations (no contraction), rounded once to a 64-bit fixed-point integer and added with
+// an integer atomic. Integer addition is associative, so the maps are bit-identical run to
+// run and independent of launch shape; the reference gets the same property from fixed
+// 8-chunk local grids (bin_grid.cpp:196-251). The maps (16 B per bin for node + filler)
+// stay in L2 for every grid size the engine accepts (1024^2 -> 16 MB of the 126 MB L2).
+//
+// Roofline: these kernels are HBM/L2 bound. Algorithmic bytes per evaluation:
+//   scatter 17 B/node + 16 B/bin, rho+tau 28 B/bin, gather 25 B/node.
+#include "engine.h"
+
+namespace spg {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void __launch_bounds__(kThreads) acc_small_kernel(DevPtrs p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= p.n_dens_small) return;
+    const int i = p.dens_small[t];
+    const GridGeom& g = p.geom;
+    const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
+    const float w = p.wgt[i];
+    unsigned long long* map = (p.kind[i] & K_FILLER) ? p.filler_fix : p.node_fix;
+    for (int bx = f.bx0; bx <= f.bx1; ++bx) {
+        unsigned long long* row = map + static_cast<size_t>(bx) * g.dim;
+        for (int by = f.by0; by <= f.by1; ++by) {
+            const float c = bin_contribution(g, bx, by, f, w);
+            if (c <= 0.f) continue;
+            atomicAdd(row + by, to_fixed(c, g.scale));
+        }
+    }
+}
+
+// One block per large node (macros): the block's threads split its footprint's bins.
+__global__ void __launch_bounds__(kThreads) acc_large_kernel(DevPtrs p) {
+    const int i = p.dens_large[blockIdx.x];
+    const GridGeom& g = p.geom;
+    const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
+    const float w = p.wgt[i];
+    unsigned long long* map = (p.kind[i] & K_FILLER) ? p.filler_fix : p.node_fix;
+    const int ny = f.by1 - f.by0 + 1;
+    const int nb = (f.bx1 - f.bx0 + 1) * ny;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int bx = f.bx0 + j / ny, by = f.by0 + j % ny;
+        const float c = bin_contribution(g, bx, by, f, w);
+        if (c <= 0.f) continue;
+        atomicAdd(map + static_cast<size_t>(bx) * g.dim + by, to_fixed(c, g.scale));
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Fixed-order block sum (warp trees, then warp 0 over the warp sums); result in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double ws[32];
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) ws[wid] = v;
+    __syncthreads();
+    const int nw = (blockDim.x + 31) >> 5;
+    double r = 0.0;
+    if (wid == 0) {
+        r = lane < nw ? ws[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+// rho = (node + filler + terminal + base) * (1/binArea) as float (bin_grid.cpp:253-259) and
+// the tau partial sums sum max(rho' - target, 0) * binArea over rho' without fillers
+// (bin_grid.cpp:265-285). Reads the fixed-point maps and clears them for the next
+// evaluation when `zero` is set.
+__global__ void __launch_bounds__(RED_THREADS) rho_overflow_kernel(DevPtrs p, int write_maps,
+                                                                   int zero) {
+    const GridGeom& g = p.geom;
+    const size_t n = static_cast<size_t>(g.dim) * g.dim;
+    const float bin_area_f = fmul(g.step_x, g.step_y);
+    const float inv_area = fdiv(1.0f, bin_area_f);
+    const double area = static_cast<double>(bin_area_f);
+    const double target = static_cast<double>(g.target_density);
+    double over = 0.0;
+    for (size_t b = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; b < n;
+         b += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const long long nfix = static_cast<long long>(p.node_fix[b]);
+        const long long ffix = static_cast<long long>(p.filler_fix[b]);
+        const float nd = static_cast<float>(static_cast<double>(nfix) * g.inv_scale);
+        const float fd = static_cast<float>(static_cast<double>(ffix) * g.inv_scale);
+        const float t = p.terminal[b], bs = p.base[b];
+        p.rho[b] = fmul(fadd(fadd(fadd(nd, fd), t), bs), inv_area);
+        const double r = __dadd_rn(__dadd_rn(static_cast<double>(nd), static_cast<double>(t)),
+                                   static_cast<double>(bs)) / area;
+        const double d = r - target;
+        over += d > 0.0 ? __dmul_rn(d, area) : 0.0;
+        if (write_maps) {
+            p.node_map[b] = nd;
+            p.filler_map[b] = fd;
+        }
+        if (zero) {
+            p.node_fix[b] = 0ull;
+            p.filler_fix[b] = 0ull;
+        }
+    }
+    over = block_sum(over);
+    if (threadIdx.x == 0) p.partials[SLOT_OVERFLOW * RED_BLOCKS + blockIdx.x] = over;
+}
+
+// force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it.
+__device__ __forceinline__ void gather_node(const DevPtrs& p, int i, float& fx, float& fy) {
+    const GridGeom& g = p.geom;
+    const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
+    const float w = p.wgt[i];
+    fx = 0.f;
+    fy = 0.f;
+    for (int bx = f.bx0; bx <= f.bx1; ++bx) {
+        const size_t row = static_cast<size_t>(bx) * g.dim;
+        for (int by = f.by0; by <= f.by1; ++by) {
+            const float q = bin_contribution(g, bx, by, f, w);
+            if (q <= 0.f) continue;
+            fx = fadd(fx, fmul(q, __ldg(p.ex + row + by)));
+            fy = fadd(fy, fmul(q, __ldg(p.ey + row + by)));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) gather_opt_small_kernel(DevPtrs p) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= p.n_opt_small) return;
+    const int k = p.opt_small[t];
+    float fx, fy;
+    gather_node(p, p.opt_idx[k], fx, fy);
+    p.force[k] = fx;
+    p.force[p.n_opt + k] = fy;
+}
+
+// Large nodes: the block splits the footprint; per-thread partial sums are combined in a
+// fixed tree (deterministic, but not the reference's sequential order).
+__device__ __forceinline__ void gather_large(const DevPtrs& p, int i, float& fx, float& fy) {
+    const GridGeom& g = p.geom;
+    const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
+    const float w = p.wgt[i];
+    const int ny = f.by1 - f.by0 + 1;
+    const int nb = (f.bx1 - f.bx0 + 1) * ny;
+    float ax = 0.f, ay = 0.f;
+    for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+        const int bx = f.bx0 + j / ny, by = f.by0 + j % ny;
+        const float q = bin_contribution(g, bx, by, f, w);
+        if (q <= 0.f) continue;
+        const size_t idx = static_cast<size_t>(bx) * g.dim + by;
+        ax = fadd(ax, fmul(q, p.ex[idx]));
+        ay = fadd(ay, fmul(q, p.ey[idx]));
+    }
+    __shared__ float sx[32], sy[32];
+    ax = warp_sum(ax);
+    ay = warp_sum(ay);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        sx[wid] = ax;
+        sy[wid] = ay;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = blockDim.x >> 5;
+        ax = lane < nw ? sx[lane] : 0.f;
+        ay = lane < nw ? sy[lane] : 0.f;
+        ax = warp_sum(ax);
+        ay = warp_sum(ay);
+    }
+    fx = ax;
+    fy = ay;
+}
+
+__global__ void __launch_bounds__(kThreads) gather_opt_large_kernel(DevPtrs p) {
+    const int k = p.opt_large[blockIdx.x];
+    float fx, fy;
+    gather_large(p, p.opt_idx[k], fx, fy);
+    if (threadIdx.x == 0) {
+        p.force[k] = fx;
+        p.force[p.n_opt + k] = fy;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) gather_all_small_kernel(DevPtrs p, float* out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= p.n_dens_small) return;
+    const int i = p.dens_small[t];
+    float fx, fy;
+    gather_node(p, i, fx, fy);
+    out[i] = fx;
+    out[p.total + i] = fy;
+}
+
+__global__ void __launch_bounds__(kThreads) gather_all_large_kernel(DevPtrs p, float* out) {
+    const int i = p.dens_large[blockIdx.x];
+    float fx, fy;
+    gather_large(p, i, fx, fy);
+    if (threadIdx.x == 0) {
+        out[i] = fx;
+        out[p.total + i] = fy;
+    }
+}
+
+}  // namespace
+
+void launch_density_accumulate(const DevPtrs& p, cudaStream_t s) {
+    if (p.n_dens_small > 0) {
+        acc_small_kernel<<<ceil_div(p.n_dens_small, kThreads), kThreads, 0, s>>>(p);
+        count_launch();
+    }
+    if (p.n_dens_large > 0) {
+        acc_large_kernel<<<p.n_dens_large, kThreads, 0, s>>>(p);
+        count_launch();
+    }
+    SPG_CHECK_LAUNCH();
+}
+
+void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s) {
+    rho_overflow_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(p, write_maps, zero);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+}
+
+void launch_gather_opt(const DevPtrs& p, cudaStream_t s) {
+    if (p.n_opt_small > 0) {
+        gather_opt_small_kernel<<<ceil_div(p.n_opt_small, kThreads), kThreads, 0, s>>>(p);
+        count_launch();
+    }
+    if (p.n_opt_large > 0) {
+        gather_opt_large_kernel<<<p.n_opt_large, kThreads, 0, s>>>(p);
+        count_launch();
+    }
+    SPG_CHECK_LAUNCH();
+}
+
+void launch_gather_all(const DevPtrs& p, float* out, cudaStream_t s) {
+    if (p.n_dens_small > 0) {
+        gather_all_small_kernel<<<ceil_div(p.n_dens_small, kThreads), kThreads, 0, s>>>(p, out);
+        count_launch();
+    }
+    if (p.n_dens_large > 0) {
+        gather_all_large_kernel<<<p.n_dens_large, kThreads, 0, s>>>(p, out);
+        count_launch();
+    }
+    SPG_CHECK_LAUNCH();
+}
+
+}  // namespace spg

@@ -1,0 +1,1207 @@
+// Host side of the sm_100a GP engine and the C ABI of include/spgpu.h.
+//
+// The host code here plays the role of the reference's EPlace / BinGrid drivers
+// (src/gp/eplace.cpp, src/gp/bin_grid.cpp): it builds the stage-static data (bin grid
+// dimension, terminal and base density, local-smoothing footprints, optimisation set,
+// clamp boxes) once per stage, then launches the device-resident iteration. It never
+// computes an iteration quantity itself: every schedule scalar lives in DevState and is
+// updated by control kernels. Per iteration it reads a 16-byte status to learn whether
+// to launch a backtracking re-evaluation or the next iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "poisson.h"
+
+namespace spg {
+
+int64_t g_launches = 0;
+
+// optimizer.cu entry points not declared in engine.h
+void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_step(const DevPtrs& p, int reduce_fresh, cudaStream_t s);
+void launch_init_norms(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_init_scale(const DevPtrs& p, float init_perturb, cudaStream_t s);
+void launch_init_diff(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_init_finish(const DevPtrs& p, cudaStream_t s);
+void launch_clamp_role(const DevPtrs& p, int role, cudaStream_t s);
+void launch_stage_clock(const DevPtrs& p, cudaStream_t s);
+void launch_check_geometry(const DevPtrs& p, float lx, float ly, float hx, float hy, const float* w,
+                           const float* h, cudaStream_t s);
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr int kMaxBinDim = 1024;      // bin_grid.cpp:18
+constexpr float kBoundaryEps = 1e-3f;  // eplace.cpp:38
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { reset(); }
+    void reset() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        reset();
+        if (count == 0) count = 1;
+        SPG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void upload(const T* h, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) SPG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+    void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
+    void zero(cudaStream_t s) { SPG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
+};
+
+int clampi_h(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+float hmin(float a, float b) { return (b < a) ? b : a; }
+float hmax(float a, float b) { return (a < b) ? b : a; }
+float overlap_area(float alx, float aly, float ahx, float ahy, float blx, float bly, float bhx,
+                   float bhy) {
+    const float dx = hmin(ahx, bhx) - hmax(alx, blx);
+    const float dy = hmin(ahy, bhy) - hmax(aly, bly);
+    return (dx > 0.f && dy > 0.f) ? dx * dy : 0.f;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------
+struct Context {
+    cudaStream_t stream = nullptr;
+    spg_params prm{};
+    // host copy of the db (flags and sizes change with mLG; positions live on the device)
+    int num_movable = 0, num_nodes = 0, num_fillers = 0, total = 0, num_pins = 0, num_nets = 0;
+    std::vector<float> w, h;
+    std::vector<uint8_t> flags;
+    std::vector<int> node_start;
+    std::vector<float> row_ly, row_hgt, row_lx, row_step;
+    std::vector<int> row_sites;
+    float core_lx = 0, core_ly = 0, core_hx = 0, core_hy = 0;
+
+    DevBuf<float> x, y, dw, dh, hw, hh, wgt;
+    DevBuf<uint8_t> kind;
+    DevBuf<float> pox, poy, gpx, gpy;
+    DevBuf<int> pin2node, pin2net, net_start, net_pins, node_start_d, node_pins, net_order;
+    // grid
+    bool grid_ready = false;
+    GridGeom geom{};
+    double movable_area_scaled = 0.0;
+    DevBuf<unsigned long long> node_fix, filler_fix;
+    DevBuf<float> terminal, base, rho, phi, ex, ey, node_map, filler_map;
+    std::unique_ptr<PoissonPlan> plan;
+    DevBuf<int> dens_small, dens_large;
+    int n_dens_small = 0, n_dens_large = 0;
+    // stage
+    int n_opt = 0;
+    DevBuf<int> opt_idx, opt_deg, opt_small, opt_large;
+    DevBuf<float> opt_lo, opt_hi, force, pool;
+    DevBuf<double> opt_area;
+    int n_opt_small = 0, n_opt_large = 0;
+    size_t vec_stride = 0;
+    DevBuf<double> partials;
+    DevBuf<DevState> st;
+    DevBuf<spg_iter_metrics> metrics;
+    DevBuf<double> scratch_d;
+    int metrics_rows = 0;
+    DevState* hst = nullptr;  // pinned host mirror
+    float step_x_gamma = 1.f;
+
+    ~Context() {
+        if (plan) poisson_plan_destroy(*plan);
+        if (hst) cudaFreeHost(hst);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    DevPtrs ptrs() const {
+        DevPtrs p{};
+        p.num_movable = num_movable;
+        p.num_nodes = num_nodes;
+        p.num_fillers = num_fillers;
+        p.total = total;
+        p.num_pins = num_pins;
+        p.num_nets = num_nets;
+        p.x = x.p;
+        p.y = y.p;
+        p.hw = hw.p;
+        p.hh = hh.p;
+        p.wgt = wgt.p;
+        p.kind = kind.p;
+        p.pox = pox.p;
+        p.poy = poy.p;
+        p.pin2node = pin2node.p;
+        p.pin2net = pin2net.p;
+        p.net_start = net_start.p;
+        p.net_pins = net_pins.p;
+        p.node_start = node_start_d.p;
+        p.node_pins = node_pins.p;
+        p.net_order = net_order.p;
+        p.gpx = gpx.p;
+        p.gpy = gpy.p;
+        p.geom = geom;
+        p.node_fix = node_fix.p;
+        p.filler_fix = filler_fix.p;
+        p.terminal = terminal.p;
+        p.base = base.p;
+        p.rho = rho.p;
+        p.phi = phi.p;
+        p.ex = ex.p;
+        p.ey = ey.p;
+        p.node_map = node_map.p;
+        p.filler_map = filler_map.p;
+        p.movable_area_scaled = movable_area_scaled;
+        p.n_opt = n_opt;
+        p.opt_idx = opt_idx.p;
+        p.opt_lo = opt_lo.p;
+        p.opt_hi = opt_hi.p;
+        p.opt_deg = opt_deg.p;
+        p.opt_area = opt_area.p;
+        p.force = force.p;
+        p.pool = pool.p;
+        p.vec_stride = vec_stride;
+        p.dens_small = dens_small.p;
+        p.dens_large = dens_large.p;
+        p.n_dens_small = n_dens_small;
+        p.n_dens_large = n_dens_large;
+        p.opt_small = opt_small.p;
+        p.opt_large = opt_large.p;
+        p.n_opt_small = n_opt_small;
+        p.n_opt_large = n_opt_large;
+        p.partials = partials.p;
+        p.st = st.p;
+        p.metrics = metrics.p;
+        p.ignore_net_degree = prm.ignore_net_degree;
+        p.use_bb = prm.use_bb;
+        p.backtrack = prm.gp_backtrack;
+        p.max_backtrack = prm.max_backtrack;
+        p.min_gain = std::min(std::max(prm.gp_stagnation_min_gain, 0.f), 0.5f);
+        p.stagnation_window = prm.gp_stagnation_window;
+        p.step_x_gamma = step_x_gamma;
+        return p;
+    }
+
+    bool fixed(int i) const { return (flags[i] & SPG_F_FIXED) != 0; }
+    bool ni(int i) const { return (flags[i] & SPG_F_NI) != 0; }
+    bool macro(int i) const { return (flags[i] & SPG_F_MACRO) != 0; }
+    bool filler(int i) const { return (flags[i] & SPG_F_FILLER) != 0; }
+};
+
+namespace {
+
+// BinGrid::initialize (src/gp/bin_grid.cpp:64-189) for the current flags, plus the
+// per-node footprint data the density kernels read and the fixed-point scale.
+void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& hx_pos,
+               const std::vector<float>& hy_pos) {
+    double cell_area = 0.0, macro_area = 0.0;
+    for (int i = 0; i < c.num_movable; ++i) {
+        if (c.fixed(i) || c.ni(i)) continue;
+        const double a = static_cast<double>(c.w[i]) * static_cast<double>(c.h[i]);
+        if (c.macro(i)) macro_area += a;
+        else cell_area += a;
+    }
+    c.movable_area_scaled = cell_area + macro_area * static_cast<double>(target);
+    int dim;
+    if (bin_dim > 0) {
+        dim = std::min(bin_dim, kMaxBinDim);
+    } else {
+        const double avg = (c.num_movable > 0) ? (cell_area + macro_area) / c.num_movable : 1.0;
+        const double ideal_bin = std::max(avg / target, 1e-9);
+        const float cw = c.core_hx - c.core_lx, ch = c.core_hy - c.core_ly;
+        const double ideal = static_cast<double>(cw) * static_cast<double>(ch) / ideal_bin;
+        dim = 4;
+        while (dim * 2 <= kMaxBinDim && static_cast<double>(dim * 2) * (dim * 2) <= ideal) dim *= 2;
+    }
+    GridGeom& g = c.geom;
+    g.dim = dim;
+    g.origin_x = c.core_lx;
+    g.origin_y = c.core_ly;
+    g.step_x = (c.core_hx - c.core_lx) / static_cast<float>(dim);
+    g.step_y = (c.core_hy - c.core_ly) / static_cast<float>(dim);
+    g.target_density = target;
+    c.step_x_gamma = g.step_x;
+    const size_t n = static_cast<size_t>(dim) * dim;
+
+    // terminal density (bin_grid.cpp:120-137)
+    std::vector<float> term(n, 0.f), base(n, 0.f);
+    for (int i = 0; i < c.num_nodes; ++i) {
+        if (!c.fixed(i) || c.ni(i)) continue;
+        const float lx = hx_pos[i] - 0.5f * c.w[i], hx = hx_pos[i] + 0.5f * c.w[i];
+        const float ly = hy_pos[i] - 0.5f * c.h[i], hy = hy_pos[i] + 0.5f * c.h[i];
+        const int bx0 = clampi_h(static_cast<int>((lx - g.origin_x) / g.step_x), 0, dim - 1);
+        const int bx1 = clampi_h(static_cast<int>((hx - g.origin_x) / g.step_x), 0, dim - 1);
+        const int by0 = clampi_h(static_cast<int>((ly - g.origin_y) / g.step_y), 0, dim - 1);
+        const int by1 = clampi_h(static_cast<int>((hy - g.origin_y) / g.step_y), 0, dim - 1);
+        for (int bx = bx0; bx <= bx1; ++bx) {
+            const float blx = g.origin_x + bx * g.step_x;
+            for (int by = by0; by <= by1; ++by) {
+                const float bly = g.origin_y + by * g.step_y;
+                term[static_cast<size_t>(bx) * dim + by] +=
+                    target * overlap_area(blx, bly, blx + g.step_x, bly + g.step_y, lx, ly, hx, hy);
+            }
+        }
+    }
+    // base density: non-row area of each bin (bin_grid.cpp:144-173)
+    const int nr = static_cast<int>(c.row_ly.size());
+    std::vector<int> order(nr);
+    std::iota(order.begin(), order.end(), 0);
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return c.row_ly[a] < c.row_ly[b]; });
+    std::vector<float> rly(nr), rhy(nr), rlx(nr), rhx(nr);
+    for (int t = 0; t < nr; ++t) {
+        const int r = order[t];
+        rly[t] = c.row_ly[r];
+        rhy[t] = c.row_ly[r] + c.row_hgt[r];
+        rlx[t] = c.row_lx[r];
+        rhx[t] = c.row_lx[r] + c.row_step[r] * static_cast<float>(c.row_sites[r]);
+    }
+    for (int by = 0; by < dim; ++by) {
+        const float bly = g.origin_y + by * g.step_y;
+        const float bhy = bly + g.step_y;
+        size_t lo = 0, hi = static_cast<size_t>(nr);
+        while (lo < hi) {
+            const size_t mid = (lo + hi) / 2;
+            if (rhy[mid] <= bly) lo = mid + 1;
+            else hi = mid;
+        }
+        for (int bx = 0; bx < dim; ++bx) {
+            const float blx = g.origin_x + bx * g.step_x;
+            const float bhx = blx + g.step_x;
+            float covered = 0.f;
+            for (size_t t = lo; t < static_cast<size_t>(nr); ++t) {
+                if (rly[t] >= bhy) break;
+                covered += overlap_area(blx, bly, bhx, bhy, rlx[t], rly[t], rhx[t], rhy[t]);
+            }
+            const float area = (bhx - blx) * (bhy - bly);
+            base[static_cast<size_t>(bx) * dim + by] = target * hmax(0.f, area - covered);
+        }
+    }
+
+    // footprint data: half extents after local smoothing, charge weight, kernel class
+    std::vector<float> hw(c.total), hh(c.total), wgt(c.total);
+    std::vector<uint8_t> kind(c.total, 0);
+    std::vector<int> dsmall, dlarge;
+    double bound = 0.0;
+    for (int i = 0; i < c.total; ++i) {
+        const float w = c.w[i], h = c.h[i];
+        float sx = 1.f, sy = 1.f;
+        hw[i] = 0.5f * w;
+        hh[i] = 0.5f * h;
+        if (w < g.step_x) {
+            sx = w / g.step_x;
+            hw[i] = 0.5f * g.step_x;
+        }
+        if (h < g.step_y) {
+            sy = h / g.step_y;
+            hh[i] = 0.5f * g.step_y;
+        }
+        const float scale = sx * sy;
+        wgt[i] = c.filler(i) ? scale : (c.macro(i) ? scale * target : scale);
+        if (c.fixed(i) || c.ni(i)) continue;
+        bound += static_cast<double>(w) * static_cast<double>(h);
+        uint8_t k = K_DENSITY;
+        if (c.filler(i)) k |= K_FILLER;
+        const double bins = (std::floor(2.0 * hw[i] / g.step_x) + 2.0) * (std::floor(2.0 * hh[i] / g.step_y) + 2.0);
+        if (bins > 16.0) k |= K_LARGE;
+        kind[i] = k;
+        (k & K_LARGE ? dlarge : dsmall).push_back(i);
+    }
+    // fixed-point scale: largest s <= 40 with (total charge bound) * 2^s < 2^62
+    bound *= target > 1.f ? static_cast<double>(target) : 1.0;
+    int s = 40;
+    if (bound > 0.0) {
+        int e = 0;
+        std::frexp(bound, &e);
+        s = std::min(40, 62 - e);
+    }
+    g.shift = s;
+    g.scale = std::ldexp(1.0, s);
+    g.inv_scale = std::ldexp(1.0, -s);
+
+    cudaStream_t st = c.stream;
+    c.terminal.upload(term, st);
+    c.base.upload(base, st);
+    c.hw.upload(hw, st);
+    c.hh.upload(hh, st);
+    c.wgt.upload(wgt, st);
+    c.kind.upload(kind, st);
+    c.dens_small.upload(dsmall, st);
+    c.dens_large.upload(dlarge, st);
+    c.n_dens_small = static_cast<int>(dsmall.size());
+    c.n_dens_large = static_cast<int>(dlarge.size());
+    c.node_fix.alloc(n);
+    c.filler_fix.alloc(n);
+    c.node_fix.zero(st);
+    c.filler_fix.zero(st);
+    for (DevBuf<float>* b : {&c.rho, &c.phi, &c.ex, &c.ey, &c.node_map, &c.filler_map}) {
+        b->alloc(n);
+        b->zero(st);
+    }
+    if (!c.plan || c.plan->nx != dim || c.plan->step_x != g.step_x || c.plan->step_y != g.step_y ||
+        c.plan->precision != c.prm.poisson_precision) {
+        if (c.plan) poisson_plan_destroy(*c.plan);
+        c.plan = std::make_unique<PoissonPlan>();
+        poisson_plan_create(*c.plan, dim, dim, g.step_x, g.step_y, c.prm.poisson_precision, 1);
+    }
+    c.partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_BLOCKS);
+    c.partials.zero(st);
+    SPG_CUDA(cudaStreamSynchronize(st));
+    c.grid_ready = true;
+}
+
+// EPlace::Impl::buildOptSet (eplace.cpp:82-94) and the per-opt-node clamp boxes
+// (eplace.cpp:117-133), degrees and areas (eplace.cpp:176-178).
+void stage_setup(Context& c, int stage) {
+    std::vector<int> opt;
+    opt.reserve(static_cast<size_t>(c.num_movable + c.num_fillers));
+    if (stage != SPG_STAGE_FILLER_ONLY) {
+        for (int i = 0; i < c.num_movable; ++i) {
+            if (c.fixed(i) || c.ni(i)) continue;
+            if (stage == SPG_STAGE_CGP && c.macro(i)) continue;
+            opt.push_back(i);
+        }
+    }
+    for (int i = c.num_nodes; i < c.total; ++i) opt.push_back(i);
+    const int n = static_cast<int>(opt.size());
+    c.n_opt = n;
+    std::vector<float> lo(2 * static_cast<size_t>(n)), hi(2 * static_cast<size_t>(n));
+    std::vector<int> deg(n), osmall, olarge;
+    std::vector<double> area(n);
+    std::vector<uint8_t> kind(c.total);
+    SPG_CUDA(cudaMemcpyAsync(kind.data(), c.kind.p, c.total, cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    for (int k = 0; k < n; ++k) {
+        const int i = opt[k];
+        const float hw = 0.5f * c.w[i], hh = 0.5f * c.h[i];
+        const float xlo = c.core_lx + hw + kBoundaryEps;
+        const float xhi = hmax(xlo, c.core_hx - hw - kBoundaryEps);
+        const float ylo = c.core_ly + hh + kBoundaryEps;
+        const float yhi = hmax(ylo, c.core_hy - hh - kBoundaryEps);
+        lo[k] = xlo;
+        hi[k] = xhi;
+        lo[n + k] = ylo;
+        hi[n + k] = yhi;
+        deg[k] = c.node_start[i + 1] - c.node_start[i];
+        area[k] = static_cast<double>(c.w[i]) * static_cast<double>(c.h[i]);
+        (kind[i] & K_LARGE ? olarge : osmall).push_back(k);
+    }
+    cudaStream_t s = c.stream;
+    c.opt_idx.upload(opt, s);
+    c.opt_lo.upload(lo, s);
+    c.opt_hi.upload(hi, s);
+    c.opt_deg.upload(deg, s);
+    c.opt_area.upload(area, s);
+    c.opt_small.upload(osmall, s);
+    c.opt_large.upload(olarge, s);
+    c.n_opt_small = static_cast<int>(osmall.size());
+    c.n_opt_large = static_cast<int>(olarge.size());
+    c.force.alloc(2 * static_cast<size_t>(std::max(n, 1)));
+    // vectors padded to 64 floats so every role starts 256-byte aligned
+    c.vec_stride = (2 * static_cast<size_t>(std::max(n, 1)) + 63) / 64 * 64;
+    c.pool.alloc(c.vec_stride * (NUM_ROLES + SNAP_MAX));
+    c.pool.zero(s);
+    c.metrics_rows = 0;
+    c.metrics.alloc(static_cast<size_t>(std::max(c.prm.gp_max_iter, c.prm.filler_only_iters) + 1));
+    if (!c.st.p) c.st.alloc(1);
+    if (!c.hst) SPG_CUDA(cudaMallocHost(&c.hst, sizeof(DevState)));
+    if (!c.scratch_d.p) c.scratch_d.alloc(16);
+}
+
+// One objAndGrad evaluation at the positions of `pos_role`, gradient into `grad_role`
+// (eplace.cpp:136-203).
+void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count) {
+    cudaStream_t s = c.stream;
+    launch_scatter(p, pos_role, s);
+    launch_density_accumulate(p, s);
+    launch_rho_overflow(p, 0, 1, s);
+    poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s);
+    launch_gather_opt(p, s);
+    launch_wa_nets(p, &p.st->gamma, 0.f, 1, s);
+    launch_assemble(p, grad_role, s);
+    launch_ctl_eval_done(p, count, s);
+}
+
+void read_state(Context& c) {
+    SPG_CUDA(cudaMemcpyAsync(c.hst, c.st.p, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    if (c.hst->error) {
+        const int e = c.hst->error;
+        throw Error(e, e == SPG_E_NON_FINITE ? "GP/evaluate: non-finite coordinate, gradient or metric"
+                     : e == SPG_E_OUT_OF_CORE ? "GP: node outside core"
+                     : e == SPG_E_CAPACITY ? "GP: stagnation snapshot capacity exceeded"
+                                           : "GP: device error");
+    }
+}
+
+// hpwlReference (src/gp/lambda_schedule.h:11-20)
+double hpwl_reference(const spg_params& p, double initial, bool filler_only) {
+    const bool rel = p.lambda_schedule_relative != 0 && !filler_only;
+    const double ref = rel ? initial * p.delta_hpwl_relative : static_cast<double>(p.delta_hpwl_ref);
+    if (initial == 0.0 && rel) return p.delta_hpwl_ref;
+    if (!(ref > 0.0) || !std::isfinite(ref)) throw Error(SPG_E_INVALID, "invalid effective HPWL reference");
+    return ref;
+}
+
+__global__ void gather_pos_kernel(DevPtrs p) {
+    float* pos = p.pool + static_cast<size_t>(p.st->role[R_POS]) * p.vec_stride;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < p.n_opt; k += gridDim.x * blockDim.x) {
+        const int i = p.opt_idx[k];
+        pos[k] = p.x[i];
+        pos[p.n_opt + k] = p.y[i];
+    }
+}
+
+__global__ void init_state_kernel(DevPtrs p, int stage, int max_iter, float target_tau) {
+    DevState* st = p.st;
+    memset(st, 0, sizeof(DevState));
+    for (int r = 0; r < NUM_ROLES; ++r) st->role[r] = r;
+    st->stage = stage;
+    st->max_iter = max_iter;
+    st->target_tau = target_tau;
+    st->lambda = 1.f;
+    st->a = 1.f;
+    st->alpha = 1.f;
+    st->alpha0 = 1.f;
+    st->tries = 1;
+    st->best_tau = INFINITY;
+    st->ref_tau = INFINITY;
+    st->snap_copy_to = -1;
+    st->rollback_iter = -1;
+    st->deliver = 0;
+}
+
+__global__ void gamma_init_kernel(DevPtrs p) {
+    // computeGamma(1.f, stepX) (eplace.cpp:248): tau = 1 lies in the pow branch
+    float g = __fmul_rn(8.0f, p.step_x_gamma);
+    g = __fmul_rn(g, powf(10.0f, __fsub_rn(__fmul_rn(20.0f / 9.0f, __fsub_rn(1.0f, 0.1f)), 1.0f)));
+    p.st->gamma = fmaxf(g, 1e-4f);
+    p.st->lambda = 1.f;
+}
+
+__global__ void set_hpwl_ref_kernel(DevPtrs p, double ref) { p.st->hpwl_ref = ref; }
+
+// Final metrics at the delivered positions: overflow and HPWL (eplace.cpp:484-488).
+__global__ void final_metrics_kernel(DevPtrs p, double* out) {
+    double over = 0.0, hp = 0.0;
+    for (int j = threadIdx.x; j < RED_BLOCKS; j += blockDim.x) {
+        over += p.partials[SLOT_OVERFLOW * RED_BLOCKS + j];
+        hp += p.partials[SLOT_HPWL * RED_BLOCKS + j];
+    }
+    __shared__ double so[256], sh[256];
+    so[threadIdx.x] = over;
+    sh[threadIdx.x] = hp;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            so[threadIdx.x] += so[threadIdx.x + w];
+            sh[threadIdx.x] += sh[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = p.movable_area_scaled > 0.0 ? static_cast<double>(static_cast<float>(so[0] / p.movable_area_scaled)) : 0.0;
+        out[1] = sh[0];
+    }
+}
+
+void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) {
+    cudaStream_t s = c.stream;
+    launch_scatter(p, R_POS, s);
+    launch_density_accumulate(p, s);
+    launch_rho_overflow(p, 0, 1, s);
+    launch_wa_nets(p, &p.st->gamma, 0.f, 1, s);
+    final_metrics_kernel<<<1, 256, 0, s>>>(p, c.scratch_d.p);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+    double out[2];
+    SPG_CUDA(cudaMemcpyAsync(out, c.scratch_d.p, sizeof(out), cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(cudaStreamSynchronize(s));
+    *overflow = static_cast<float>(out[0]);
+    *hpwl = out[1];
+}
+
+// EPlace::run (eplace.cpp:223-526) for one stage, device-resident.
+void stage_run(Context& c, int stage, spg_result* res) {
+    SPG_REQUIRE(stage >= SPG_STAGE_MGP && stage <= SPG_STAGE_CGP, SPG_E_INVALID, "unknown stage");
+    std::memset(res, 0, sizeof(*res));
+    res->rollback_iter = -1;
+    cudaStream_t s = c.stream;
+    // constructing EPlace rebuilds the grid with the current flags (gp_stage.cpp:175-177)
+    {
+        std::vector<float> hx(c.total), hy(c.total);
+        SPG_CUDA(cudaMemcpyAsync(hx.data(), c.x.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, s));
+        SPG_CUDA(cudaMemcpyAsync(hy.data(), c.y.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, s));
+        SPG_CUDA(cudaStreamSynchronize(s));
+        grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, hx, hy);
+    }
+    stage_setup(c, stage);
+    if (c.n_opt == 0) return;  // "no nodes to optimise" (eplace.cpp:232-236)
+    const bool filler_only = stage == SPG_STAGE_FILLER_ONLY;
+    const float target_tau = stage == SPG_STAGE_CGP ? c.prm.cgp_target_overflow : c.prm.target_overflow;
+    const int max_iter = filler_only ? c.prm.filler_only_iters : c.prm.gp_max_iter;
+    DevPtrs p = c.ptrs();
+    init_state_kernel<<<1, 1, 0, s>>>(p, stage, max_iter, target_tau);
+    gather_pos_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(p);
+    count_launch(2);
+    SPG_CHECK_LAUNCH();
+    launch_clamp_role(p, R_POS, s);
+    // lambda_0 probe (eplace.cpp:248-259)
+    gamma_init_kernel<<<1, 1, 0, s>>>(p);
+    count_launch();
+    evaluate(c, p, R_POS, R_GA, 0);
+    launch_ctl_lambda_init(p, s);
+    read_state(c);
+    const double ref = hpwl_reference(c.prm, c.hst->hpwl, filler_only);
+    res->initial_hpwl = c.hst->hpwl;
+    res->initial_overflow = c.hst->tau;
+    res->initial_lambda = c.hst->lambda;
+    set_hpwl_ref_kernel<<<1, 1, 0, s>>>(p, ref);
+    count_launch();
+
+    if (!filler_only && c.hst->tau < target_tau) {
+        // already converged: take no step (eplace.cpp:278-296)
+        final_metrics(c, p, &res->overflow, &res->hpwl);
+        res->converged = 1;
+        return;
+    }
+
+    cudaEvent_t e0, e1;
+    SPG_CUDA(cudaEventCreate(&e0));
+    SPG_CUDA(cudaEventCreate(&e1));
+    SPG_CUDA(cudaEventRecord(e0, s));
+    launch_stage_clock(p, s);
+    // optimizer init: u = v = uPrev = vPrev = pos, g = gPrevTmp = 0 (nesterov.cpp:174-185)
+    for (int r : {R_U, R_V, R_UPREV, R_VPREV}) launch_copy_role(p, r, R_POS, s);
+    // estimateInitialStep (nesterov.cpp:190-218): two uncounted evaluations
+    evaluate(c, p, R_U, R_GA, 0);
+    launch_init_norms(p, s);
+    launch_ctl_init_scale(p, 0.1f, s);
+    launch_init_perturb(p, s);
+    evaluate(c, p, R_PROBE, R_GB, 0);
+    launch_init_diff(p, s);
+    launch_ctl_init_finish(p, s);
+
+    const bool bt = c.prm.gp_backtrack != 0;
+    int iter = 0;
+    // first evaluation of iteration 0
+    evaluate(c, p, R_U, R_G, 1);
+    launch_reduce_diff(p, s);
+    read_state(c);
+    // host-side bound: the device sets `done` by max_iter; a bound on evaluations guards the
+    // host loop against a control-logic fault
+    const int64_t eval_bound = static_cast<int64_t>(max_iter + 2) * std::max(c.prm.max_backtrack, 1);
+    while (true) {
+        if (c.hst->done) break;
+        if (iter > max_iter || c.hst->evals > eval_bound)
+            throw Error(SPG_E_STATE, "GP loop exceeded its iteration bound");
+        if (c.hst->redo) {  // redoIfOvershot re-evaluation
+            launch_redo_update(p, s);
+            evaluate(c, p, R_U, R_G, 1);
+            launch_reduce_diff(p, s);
+            launch_ctl_redo_check(p, s);
+            read_state(c);
+            continue;
+        }
+        launch_ctl_step(p, (bt && iter > 0) ? 0 : 1, s);
+        launch_nesterov_update(p, s);
+        launch_ctl_iter_end(p, s);
+        launch_snapshot_copy(p, s);
+        ++iter;
+        // first evaluation of the next iteration (harmless if the loop just finished)
+        evaluate(c, p, R_U, R_G, 1);
+        launch_reduce_diff(p, s);
+        if (bt) launch_ctl_redo_check(p, s);
+        read_state(c);
+    }
+    SPG_CUDA(cudaEventRecord(e1, s));
+    launch_deliver(p, s);
+    final_metrics(c, p, &res->overflow, &res->hpwl);
+    launch_check_geometry(p, c.core_lx, c.core_ly, c.core_hx, c.core_hy, c.dw.p, c.dh.p, s);
+    read_state(c);
+    float ms = 0.f;
+    SPG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const DevState& h = *c.hst;
+    res->iterations = h.iter;
+    res->converged = h.converged;
+    res->stagnated = h.stagnated;
+    res->rollback_iter = h.stagnated ? h.rollback_iter : -1;
+    res->evaluations = h.evals;
+    res->elapsed_ms = ms;
+    c.metrics_rows = std::min(h.iter, max_iter);
+    if (res->converged && !(res->overflow < target_tau))
+        throw Error(SPG_E_CONVERGENCE, "delivered overflow disagrees with convergence");
+    if (res->stagnated) {
+        spg_iter_metrics row{};
+        SPG_CUDA(cudaMemcpy(&row, c.metrics.p + res->rollback_iter, sizeof(row), cudaMemcpyDeviceToHost));
+        if (!(std::fabs(double(res->overflow) - row.overflow) <= 1e-7 + 1e-6 * std::fabs(row.overflow) &&
+              std::fabs(res->hpwl - row.hpwl) <= 1e-6 + 1e-10 * std::fabs(row.hpwl)))
+            throw Error(SPG_E_ROLLBACK, "delivered metrics disagree with rollback point");
+    }
+}
+
+int fail(const std::exception& e) {
+    g_last_error = e.what();
+    if (auto* se = dynamic_cast<const Error*>(&e)) return se->code;
+    return SPG_E_INVALID;
+}
+
+bool device_ok() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return false;
+    int dev = 0;
+    cudaDeviceProp prop{};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return false;
+    return prop.major == 10;
+}
+
+}  // namespace
+
+struct PoissonHandle {
+    PoissonPlan plan;
+    DevBuf<float> io;
+    cudaStream_t stream = nullptr;
+};
+
+}  // namespace spg
+
+using spg::Context;
+using spg::Error;
+
+struct spg_ctx {
+    Context c;
+};
+struct spg_poisson {
+    spg::PoissonHandle h;
+};
+
+#define API_TRY try {
+#define API_CATCH \
+    }             \
+    catch (const std::exception& e) { return spg::fail(e); }
+
+extern "C" {
+
+int spg_abi_version(void) { return SPG_ABI_VERSION; }
+const char* spg_last_error(void) { return spg::g_last_error.c_str(); }
+int spg_device_check(void) {
+    if (!spg::device_ok()) {
+        spg::g_last_error = "no usable sm_100 device";
+        return SPG_E_NO_DEVICE;
+    }
+    return SPG_OK;
+}
+
+void spg_params_default(spg_params* p) {
+    std::memset(p, 0, sizeof(*p));
+    p->target_density = 1.0f;
+    p->target_overflow = 0.10f;
+    p->cgp_target_overflow = 0.10f;
+    p->gp_max_iter = 2000;
+    p->ignore_net_degree = 100;
+    p->gp_bin_dim = 0;
+    p->filler_only_iters = 20;
+    p->delta_hpwl_ref = 3.5e5f;
+    p->lambda_schedule_relative = 0;
+    p->delta_hpwl_relative = 0.01;
+    p->use_bb = 1;
+    p->gp_backtrack = 1;
+    p->max_backtrack = 10;
+    p->gp_stagnation_window = 200;
+    p->gp_stagnation_min_gain = 0.02f;
+    p->random_seed = 1002;
+    p->poisson_precision = SPG_POISSON_FP32;
+    p->verbose = 0;
+}
+
+// ------------------------------------------------------------------ Poisson
+int spg_poisson_create_batched(int nx, int ny, float sx, float sy, int precision, int batch_cap,
+                               spg_poisson** out) {
+    API_TRY
+    SPG_REQUIRE(out, SPG_E_INVALID, "null output");
+    *out = nullptr;
+    if (!spg::device_ok()) throw Error(SPG_E_NO_DEVICE, "no usable sm_100 device");
+    auto h = std::make_unique<spg_poisson>();
+    spg::poisson_plan_create(h->h.plan, nx, ny, sx, sy, precision, batch_cap);
+    h->h.io.alloc(4 * static_cast<size_t>(nx) * ny);
+    SPG_CUDA(cudaStreamCreateWithFlags(&h->h.stream, cudaStreamNonBlocking));
+    *out = h.release();
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_poisson_create(int nx, int ny, float sx, float sy, int precision, spg_poisson** out) {
+    return spg_poisson_create_batched(nx, ny, sx, sy, precision, 1, out);
+}
+
+int spg_poisson_solve(spg_poisson* h, const float* rho, float* phi, float* fx, float* fy) {
+    API_TRY
+    SPG_REQUIRE(h && rho && phi && fx && fy, SPG_E_INVALID, "null argument");
+    const size_t n = static_cast<size_t>(h->h.plan.nx) * h->h.plan.ny;
+    float* d = h->h.io.p;
+    cudaStream_t s = h->h.stream;
+    SPG_CUDA(cudaMemcpyAsync(d, rho, n * 4, cudaMemcpyHostToDevice, s));
+    spg::poisson_solve(h->h.plan, 1, d, d + n, d + 2 * n, d + 3 * n, s);
+    SPG_CUDA(cudaMemcpyAsync(phi, d + n, n * 4, cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(cudaMemcpyAsync(fx, d + 2 * n, n * 4, cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(cudaMemcpyAsync(fy, d + 3 * n, n * 4, cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(cudaStreamSynchronize(s));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_poisson_solve_batch_device(spg_poisson* h, int batch, const float* rho, float* phi,
+                                   float* fx, float* fy, void* stream) {
+    API_TRY
+    SPG_REQUIRE(h && rho && phi && fx && fy, SPG_E_INVALID, "null argument");
+    spg::poisson_solve(h->h.plan, batch, rho, phi, fx, fy, static_cast<cudaStream_t>(stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_poisson_solve_device(spg_poisson* h, const float* rho, float* phi, float* fx, float* fy,
+                             void* stream) {
+    return spg_poisson_solve_batch_device(h, 1, rho, phi, fx, fy, stream);
+}
+
+const char* spg_poisson_name(const spg_poisson* h) { return h ? h->h.plan.name.c_str() : "none"; }
+
+int spg_poisson_destroy(spg_poisson* h) {
+    if (!h) return SPG_OK;
+    spg::poisson_plan_destroy(h->h.plan);
+    if (h->h.stream) cudaStreamDestroy(h->h.stream);
+    delete h;
+    return SPG_OK;
+}
+
+// ------------------------------------------------------------------ fillers (host)
+int spg_fillers_plan(const spg_db_view* db, float target, spg_filler_info* out) {
+    API_TRY
+    SPG_REQUIRE(db && out, SPG_E_INVALID, "null argument");
+    // initializeFillers (src/gp/filler.cpp:47-120)
+    spg_filler_info info{};
+    double overlap = 0.0;
+    for (int i = db->num_movable; i < db->num_nodes; ++i) {
+        if (db->node_flags[i] & SPG_F_NI) continue;
+        const float blx = db->node_x[i] - 0.5f * db->node_w[i], bhx = db->node_x[i] + 0.5f * db->node_w[i];
+        const float bly = db->node_y[i] - 0.5f * db->node_h[i], bhy = db->node_y[i] + 0.5f * db->node_h[i];
+        for (int r = 0; r < db->num_rows; ++r) {
+            const float rly = db->row_ly[r], rhy = db->row_ly[r] + db->row_height[r];
+            if (rly >= bhy) break;
+            if (rhy <= bly) continue;
+            const float rlx = db->row_lx[r], rhx = db->row_lx[r] + db->row_step[r] * static_cast<float>(db->row_num_sites[r]);
+            overlap += static_cast<double>(spg::overlap_area(blx, bly, bhx, bhy, rlx, rly, rhx, rhy));
+        }
+    }
+    info.whitespace_area = std::max(0.0, db->total_row_area - overlap);
+    double cell = 0.0, macro = 0.0;
+    for (int i = 0; i < db->num_movable; ++i) {
+        const double a = static_cast<double>(db->node_w[i]) * static_cast<double>(db->node_h[i]);
+        if (db->node_flags[i] & SPG_F_MACRO) macro += a;
+        else cell += a;
+    }
+    info.node_area_scaled = cell + macro * static_cast<double>(target);
+    info.total_filler_area = info.whitespace_area * static_cast<double>(target) - info.node_area_scaled;
+    if (db->num_movable == 0) {
+        *out = info;
+        return SPG_OK;
+    }
+    std::vector<double> areas(static_cast<size_t>(db->num_movable));
+    for (int i = 0; i < db->num_movable; ++i)
+        areas[i] = static_cast<double>(db->node_w[i]) * static_cast<double>(db->node_h[i]);
+    std::sort(areas.begin(), areas.end());
+    const int lo = static_cast<int>(0.10 * db->num_movable), hi = static_cast<int>(0.90 * db->num_movable);
+    double avg = 0.0;
+    if (hi > lo) {
+        for (int i = lo; i < hi; ++i) avg += areas[i];
+        avg /= (hi - lo);
+    } else {
+        avg = areas[db->num_movable / 2];
+    }
+    info.height = db->row_height_mode > 0.f ? db->row_height_mode : 1.f;
+    info.width = static_cast<float>(avg) / info.height;
+    if (!(info.width > 0.f)) info.width = 1.f;
+    const double single = static_cast<double>(info.width) * info.height;
+    const double raw = info.total_filler_area / std::max(single, 1e-9);
+    info.count = std::max(0, static_cast<int>(raw + 0.5));
+    *out = info;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_fillers_scatter(const spg_db_view* db, int32_t count, float width, float height,
+                        uint64_t seed, float* x, float* y) {
+    API_TRY
+    SPG_REQUIRE(db && (count == 0 || (x && y)), SPG_E_INVALID, "null argument");
+    // scatterFillers (src/gp/filler.cpp:33-45): mt19937 seeded with the config seed,
+    // uniform_real_distribution<float> per coordinate, x then y per filler.
+    std::mt19937 eng(static_cast<std::mt19937::result_type>(seed));
+    const float hw = 0.5f * width, hh = 0.5f * height;
+    const float lo_x = db->core_lx + hw, hi_x = db->core_hx - hw;
+    const float lo_y = db->core_ly + hh, hi_y = db->core_hy - hh;
+    const float cx = 0.5f * (db->core_lx + db->core_hx), cy = 0.5f * (db->core_ly + db->core_hy);
+    for (int i = 0; i < count; ++i) {
+        if (hi_x > lo_x) {
+            std::uniform_real_distribution<float> d(lo_x, hi_x);
+            x[i] = d(eng);
+        } else {
+            x[i] = cx;
+        }
+        if (hi_y > lo_y) {
+            std::uniform_real_distribution<float> d(lo_y, hi_y);
+            y[i] = d(eng);
+        } else {
+            y[i] = cy;
+        }
+    }
+    return SPG_OK;
+    API_CATCH
+}
+
+// ------------------------------------------------------------------ context
+int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
+    API_TRY
+    SPG_REQUIRE(v && prm && out, SPG_E_INVALID, "null argument");
+    *out = nullptr;
+    if (!spg::device_ok()) throw Error(SPG_E_NO_DEVICE, "no usable sm_100 device");
+    SPG_REQUIRE(v->num_movable >= 0 && v->num_nodes >= v->num_movable && v->num_fillers >= 0 &&
+                    v->num_pins >= 0 && v->num_nets >= 0,
+                SPG_E_INVALID, "inconsistent db counts");
+    auto h = std::make_unique<spg_ctx>();
+    Context& c = h->c;
+    c.prm = *prm;
+    SPG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.num_movable = v->num_movable;
+    c.num_nodes = v->num_nodes;
+    c.num_fillers = v->num_fillers;
+    c.total = v->num_nodes + v->num_fillers;
+    c.num_pins = v->num_pins;
+    c.num_nets = v->num_nets;
+    const size_t T = static_cast<size_t>(c.total);
+    c.w.assign(v->node_w, v->node_w + T);
+    c.h.assign(v->node_h, v->node_h + T);
+    c.flags.assign(v->node_flags, v->node_flags + T);
+    c.node_start.assign(v->node2pin_start, v->node2pin_start + T + 1);
+    c.row_ly.assign(v->row_ly, v->row_ly + v->num_rows);
+    c.row_hgt.assign(v->row_height, v->row_height + v->num_rows);
+    c.row_lx.assign(v->row_lx, v->row_lx + v->num_rows);
+    c.row_step.assign(v->row_step, v->row_step + v->num_rows);
+    c.row_sites.assign(v->row_num_sites, v->row_num_sites + v->num_rows);
+    c.core_lx = v->core_lx;
+    c.core_ly = v->core_ly;
+    c.core_hx = v->core_hx;
+    c.core_hy = v->core_hy;
+    for (int p = 0; p < c.num_pins; ++p)
+        SPG_REQUIRE(v->pin2node[p] >= 0 && v->pin2node[p] < c.total, SPG_E_INVALID, "pin2node out of range");
+    for (int k = 0; k < c.num_nets; ++k)
+        SPG_REQUIRE(v->net2pin_start[k] <= v->net2pin_start[k + 1], SPG_E_INVALID, "net CSR not monotone");
+    for (size_t i = 0; i < T; ++i)
+        SPG_REQUIRE(c.node_start[i] <= c.node_start[i + 1], SPG_E_INVALID, "node CSR not monotone");
+    SPG_REQUIRE(v->net2pin_start[0] == 0 && c.node_start[0] == 0 &&
+                    v->net2pin_start[c.num_nets] == c.num_pins && c.node_start[T] == c.num_pins,
+                SPG_E_INVALID, "CSR sizes disagree with num_pins");
+    for (int p = 0; p < c.num_pins; ++p) {
+        SPG_REQUIRE(v->flat_net2pin[p] >= 0 && v->flat_net2pin[p] < c.num_pins, SPG_E_INVALID,
+                    "flat_net2pin out of range");
+        SPG_REQUIRE(v->flat_node2pin[p] >= 0 && v->flat_node2pin[p] < c.num_pins, SPG_E_INVALID,
+                    "flat_node2pin out of range");
+        SPG_REQUIRE(v->pin2net[p] < c.num_nets, SPG_E_INVALID, "pin2net out of range");
+    }
+    cudaStream_t s = c.stream;
+    c.x.upload(v->node_x, T, s);
+    c.y.upload(v->node_y, T, s);
+    c.dw.upload(v->node_w, T, s);
+    c.dh.upload(v->node_h, T, s);
+    c.pox.upload(v->pin_offset_x, c.num_pins, s);
+    c.poy.upload(v->pin_offset_y, c.num_pins, s);
+    c.pin2node.upload(v->pin2node, c.num_pins, s);
+    c.pin2net.upload(v->pin2net, c.num_pins, s);
+    c.net_start.upload(v->net2pin_start, c.num_nets + 1, s);
+    c.net_pins.upload(v->flat_net2pin, c.num_pins, s);
+    c.node_start_d.upload(v->node2pin_start, T + 1, s);
+    c.node_pins.upload(v->flat_node2pin, c.num_pins, s);
+    // nets in descending degree (stable): warp-uniform pin loops in the WA kernel
+    std::vector<int> order(c.num_nets);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+        return v->net2pin_start[a + 1] - v->net2pin_start[a] > v->net2pin_start[b + 1] - v->net2pin_start[b];
+    });
+    c.net_order.upload(order, s);
+    c.gpx.alloc(std::max(c.num_pins, 1));
+    c.gpy.alloc(std::max(c.num_pins, 1));
+    c.gpx.zero(s);
+    c.gpy.zero(s);
+    c.st.alloc(1);
+    SPG_CUDA(cudaMallocHost(&c.hst, sizeof(spg::DevState)));
+    c.scratch_d.alloc(16);
+    SPG_CUDA(cudaStreamSynchronize(s));
+    *out = h.release();
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_ctx_destroy(spg_ctx* ctx) {
+    delete ctx;
+    return SPG_OK;
+}
+
+int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y) {
+    API_TRY
+    SPG_REQUIRE(ctx && x && y, SPG_E_INVALID, "null argument");
+    Context& c = ctx->c;
+    SPG_CUDA(cudaMemcpyAsync(c.x.p, x, c.total * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    SPG_CUDA(cudaMemcpyAsync(c.y.p, y, c.total * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_positions_d2h(spg_ctx* ctx, float* x, float* y) {
+    API_TRY
+    SPG_REQUIRE(ctx && x && y, SPG_E_INVALID, "null argument");
+    Context& c = ctx->c;
+    SPG_CUDA(cudaMemcpyAsync(x, c.x.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaMemcpyAsync(y, c.y.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_flags_h2d(spg_ctx* ctx, const uint8_t* flags) {
+    API_TRY
+    SPG_REQUIRE(ctx && flags, SPG_E_INVALID, "null argument");
+    ctx->c.flags.assign(flags, flags + ctx->c.total);
+    ctx->c.grid_ready = false;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_grid_init(spg_ctx* ctx, float target, int bin_dim) {
+    API_TRY
+    SPG_REQUIRE(ctx && target > 0.f, SPG_E_INVALID, "bad argument");
+    Context& c = ctx->c;
+    std::vector<float> hx(c.total), hy(c.total);
+    SPG_CUDA(cudaMemcpyAsync(hx.data(), c.x.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaMemcpyAsync(hy.data(), c.y.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    spg::grid_init(c, target, bin_dim, hx, hy);
+    // parity hooks evaluate over every node: an opt set of all density nodes is not needed
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_grid_info(const spg_ctx* ctx, int* dim, float* sx, float* sy, float* ox, float* oy,
+                  double* den) {
+    API_TRY
+    SPG_REQUIRE(ctx && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    const Context& c = ctx->c;
+    if (dim) *dim = c.geom.dim;
+    if (sx) *sx = c.geom.step_x;
+    if (sy) *sy = c.geom.step_y;
+    if (ox) *ox = c.geom.origin_x;
+    if (oy) *oy = c.geom.origin_y;
+    if (den) *den = c.movable_area_scaled;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_grid_read(const spg_ctx* ctx, int which, float* out) {
+    API_TRY
+    SPG_REQUIRE(ctx && out && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    const Context& c = ctx->c;
+    const spg::DevBuf<float>* b[] = {&c.node_map, &c.filler_map, &c.terminal, &c.base,
+                                     &c.rho, &c.phi, &c.ex, &c.ey};
+    SPG_REQUIRE(which >= 0 && which < 8, SPG_E_INVALID, "unknown map");
+    const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
+    SPG_CUDA(cudaMemcpyAsync(out, b[which]->p, n * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_grid_write(spg_ctx* ctx, int which, const float* in) {
+    API_TRY
+    SPG_REQUIRE(ctx && in && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    Context& c = ctx->c;
+    spg::DevBuf<float>* b[] = {&c.node_map, &c.filler_map, &c.terminal, &c.base,
+                               &c.rho, &c.phi, &c.ex, &c.ey};
+    SPG_REQUIRE(which >= 4 && which < 8, SPG_E_INVALID, "only rho, phi, xi_x, xi_y are writable");
+    const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
+    SPG_CUDA(cudaMemcpyAsync(b[which]->p, in, n * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_grid_read_fixed(const spg_ctx* ctx, int64_t* node, int64_t* filler, int* shift) {
+    API_TRY
+    SPG_REQUIRE(ctx && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    const Context& c = ctx->c;
+    const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
+    if (node) SPG_CUDA(cudaMemcpyAsync(node, c.node_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
+    if (filler) SPG_CUDA(cudaMemcpyAsync(filler, c.filler_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    if (shift) *shift = c.geom.shift;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_density_accumulate(spg_ctx* ctx) {
+    API_TRY
+    SPG_REQUIRE(ctx && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    Context& c = ctx->c;
+    spg::DevPtrs p = c.ptrs();
+    c.node_fix.zero(c.stream);
+    c.filler_fix.zero(c.stream);
+    spg::launch_density_accumulate(p, c.stream);
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_overflow(spg_ctx* ctx, float* tau) {
+    API_TRY
+    SPG_REQUIRE(ctx && tau && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    Context& c = ctx->c;
+    spg::DevPtrs p = c.ptrs();
+    // rho, the float maps and tau from the current fixed-point maps (kept for read_fixed)
+    spg::launch_rho_overflow(p, 1, 0, c.stream);
+    double over = 0.0;
+    spg::launch_finalize_slots(p, spg::SLOT_OVERFLOW, 1, c.scratch_d.p, c.stream);
+    SPG_CUDA(cudaMemcpyAsync(&over, c.scratch_d.p, 8, cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    *tau = c.movable_area_scaled > 0.0 ? static_cast<float>(over / c.movable_area_scaled) : 0.f;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_solve_field(spg_ctx* ctx) {
+    API_TRY
+    SPG_REQUIRE(ctx && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    Context& c = ctx->c;
+    spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, c.stream);
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_gather_force(spg_ctx* ctx, float* force) {
+    API_TRY
+    SPG_REQUIRE(ctx && force && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    Context& c = ctx->c;
+    spg::DevPtrs p = c.ptrs();
+    spg::DevBuf<float> out;
+    out.alloc(2 * static_cast<size_t>(c.total));
+    out.zero(c.stream);
+    spg::launch_gather_all(p, out.p, c.stream);
+    SPG_CUDA(cudaMemcpyAsync(force, out.p, 2 * c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_total_charge(spg_ctx* ctx, double* charge) {
+    API_TRY
+    SPG_REQUIRE(ctx && charge && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
+    Context& c = ctx->c;
+    const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
+    std::vector<long long> a(n), b(n);
+    SPG_CUDA(cudaMemcpyAsync(a.data(), c.node_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaMemcpyAsync(b.data(), c.filler_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    long long s = 0;
+    for (size_t i = 0; i < n; ++i) s += a[i] + b[i];
+    *charge = static_cast<double>(s) * c.geom.inv_scale;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_wa_wirelength(spg_ctx* ctx, float gamma, int ignore, double* wl, float* grad) {
+    API_TRY
+    SPG_REQUIRE(ctx, SPG_E_INVALID, "null context");
+    Context& c = ctx->c;
+    spg::DevPtrs p = c.ptrs();
+    p.ignore_net_degree = ignore;
+    if (!c.partials.p) {
+        c.partials.alloc(static_cast<size_t>(spg::RED_SLOTS) * spg::RED_BLOCKS);
+        c.partials.zero(c.stream);
+        p.partials = c.partials.p;
+    }
+    spg::launch_wa_nets(p, nullptr, gamma, 0, c.stream);
+    spg::DevBuf<float> g;
+    g.alloc(2 * static_cast<size_t>(std::max(c.num_movable, 1)));
+    spg::launch_wa_node_grad(p, g.p, c.stream);
+    spg::launch_finalize_slots(p, spg::SLOT_WL, 1, c.scratch_d.p, c.stream);
+    double v = 0.0;
+    SPG_CUDA(cudaMemcpyAsync(&v, c.scratch_d.p, 8, cudaMemcpyDeviceToHost, c.stream));
+    if (grad)
+        SPG_CUDA(cudaMemcpyAsync(grad, g.p, 2 * c.num_movable * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    if (wl) *wl = v;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_hpwl(spg_ctx* ctx, double* hpwl) {
+    API_TRY
+    SPG_REQUIRE(ctx && hpwl, SPG_E_INVALID, "null argument");
+    Context& c = ctx->c;
+    spg::DevPtrs p = c.ptrs();
+    if (!c.partials.p) {
+        c.partials.alloc(static_cast<size_t>(spg::RED_SLOTS) * spg::RED_BLOCKS);
+        c.partials.zero(c.stream);
+        p.partials = c.partials.p;
+    }
+    spg::launch_wa_nets(p, nullptr, 1.f, 0, c.stream);
+    spg::launch_finalize_slots(p, spg::SLOT_HPWL, 1, c.scratch_d.p, c.stream);
+    SPG_CUDA(cudaMemcpyAsync(hpwl, c.scratch_d.p, 8, cudaMemcpyDeviceToHost, c.stream));
+    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_stage_run(spg_ctx* ctx, int stage, spg_result* result) {
+    API_TRY
+    SPG_REQUIRE(ctx && result, SPG_E_INVALID, "null argument");
+    spg::stage_run(ctx->c, stage, result);
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_metrics_d2h(const spg_ctx* ctx, spg_iter_metrics* rows, int cap, int* n_rows) {
+    API_TRY
+    SPG_REQUIRE(ctx && n_rows, SPG_E_INVALID, "null argument");
+    const Context& c = ctx->c;
+    const int n = std::min(cap, c.metrics_rows);
+    if (n > 0 && rows)
+        SPG_CUDA(cudaMemcpy(rows, c.metrics.p, n * sizeof(spg_iter_metrics), cudaMemcpyDeviceToHost));
+    *n_rows = n;
+    return SPG_OK;
+    API_CATCH
+}
+
+int64_t spg_ctx_launch_count(const spg_ctx* ctx) {
+    (void)ctx;
+    return spg::g_launches;
+}
+
+void* spg_ctx_stream(const spg_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c.stream) : nullptr; }
+
+}  // extern "C"

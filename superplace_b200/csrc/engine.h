@@ -1,0 +1,166 @@
+// Internal interfaces of the sm_100a GP engine (not part of the C ABI).
+//
+// Layout in HBM (one context):
+//   node SoA      x, y, hw, hh, wgt (f32) and kind (u8) over all nodes; hw/hh/wgt/kind are
+//                 rebuilt per stage (local smoothing and charge weight are stage-static)
+//   pins          offsets (f32 x2), pin2node, pin2net, and both CSR directions (i32)
+//   bin maps      node/filler fixed-point maps (i64, M^2 each), terminal, base, rho, phi,
+//                 xi_x, xi_y (f32, M^2 each)
+//   optimizer     a pool of 12 vectors of 2*nOpt f32 whose roles (u, v, uPrev, ...) rotate
+//                 through a role table in DevState, so every launch has fixed arguments
+//   reductions    RED_SLOTS x RED_BLOCKS FP64 partial sums (fixed grid => deterministic)
+//   DevState      every scalar of the Nesterov / lambda / gamma / stagnation logic
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace spg {
+
+constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs; every reducing kernel uses this grid
+constexpr int RED_THREADS = 256;
+
+enum RedSlot : int {
+    SLOT_OVERFLOW = 0,
+    SLOT_WL,
+    SLOT_HPWL,
+    SLOT_SUM_WL,
+    SLOT_SUM_DEN,
+    SLOT_DX,
+    SLOT_DG,
+    SLOT_SY,
+    SLOT_GN,
+    SLOT_PN,
+    SLOT_CHARGE,
+    RED_SLOTS
+};
+
+// node kind bits (stage-static)
+constexpr uint8_t K_DENSITY = 1;  // contributes density (not fixed, not NI)
+constexpr uint8_t K_FILLER = 2;
+constexpr uint8_t K_LARGE = 4;    // footprint may exceed 16 bins: block-per-node kernels
+
+// optimizer vector roles
+enum Role : int {
+    R_U = 0, R_V, R_UPREV, R_VPREV, R_UNEW, R_VNEW, R_G, R_GPREVTMP, R_PROBE, R_GA, R_GB, R_POS,
+    NUM_ROLES
+};
+
+constexpr int SNAP_MAX = 6;  // stagnation snapshots kept (at most ~4 are ever live)
+
+// Every scalar of one stage run. Written by the control kernels, read by the vector
+// kernels and (once per iteration) by the host.
+struct DevState {
+    // schedule (src/gp/eplace.cpp:59-68)
+    float lambda, gamma, tau;
+    float eval_lambda, eval_gamma;
+    double hpwl, wl_obj, sum_wl, sum_den;
+    // Nesterov (src/numeric/cpu/nesterov.cpp:315-324)
+    float a, alpha, alpha0, momentum, momentum_prev, grad_norm;
+    int iter;
+    int64_t evals;
+    double dx, dg, sy, gn, pn;
+    int redo;       // redoIfOvershot decision for the current evaluation
+    int tries;
+    // lambda schedule (eplace.cpp:312-313)
+    double prev_hpwl;
+    int have_prev;
+    double hpwl_ref;
+    // stop / stagnation (eplace.cpp:339-353)
+    float target_tau;
+    float best_tau, ref_tau;
+    int since_improve;
+    int snap_count, snap_head;
+    float snap_tau[SNAP_MAX];
+    double snap_hpwl[SNAP_MAX];
+    int snap_iter[SNAP_MAX];
+    int snap_copy_to;   // slot the snapshot kernel copies lastEval into, or -1
+    int deliver;        // 0 = v, 1 = lastEval (converged), 2 = snapshot slot deliver_slot
+    int deliver_slot;
+    int done, converged, stagnated, rollback_iter;
+    int error;          // SPG_E_* raised on the device (non-finite values)
+    int stage;
+    int max_iter;
+    int role[NUM_ROLES];
+    unsigned long long t0_ns;
+};
+
+// Everything a kernel needs to address the device data, passed by value.
+struct DevPtrs {
+    int num_movable, num_nodes, num_fillers, total, num_pins, num_nets;
+    float *x, *y;
+    float *hw, *hh, *wgt;
+    uint8_t* kind;
+    const float *pox, *poy;
+    const int *pin2node, *pin2net;
+    const int *net_start, *net_pins;
+    const int *node_start, *node_pins;
+    const int* net_order;  // nets sorted by degree (warp-uniform pin loops)
+    // per-pin WA gradient contributions (x, y)
+    float *gpx, *gpy;
+    // grid
+    GridGeom geom;
+    unsigned long long *node_fix, *filler_fix;
+    float *terminal, *base, *rho, *phi, *ex, *ey, *node_map, *filler_map;
+    double movable_area_scaled;
+    // stage / optimizer
+    int n_opt;
+    const int* opt_idx;
+    const float* opt_lo;   // clamp bounds, 2*nOpt (x then y)
+    const float* opt_hi;
+    const int* opt_deg;    // nodeDegree of the opt node
+    const double* opt_area;
+    float* force;          // 2*nOpt, density force q*xi (not gradient)
+    float* pool;           // NUM_ROLES + SNAP_MAX vectors of 2*nOpt
+    size_t vec_stride;
+    // density work lists (node ids)
+    const int *dens_small, *dens_large;
+    int n_dens_small, n_dens_large;
+    const int *opt_small, *opt_large;  // opt positions k
+    int n_opt_small, n_opt_large;
+    double* partials;      // RED_SLOTS * RED_BLOCKS
+    DevState* st;
+    spg_iter_metrics* metrics;
+    int ignore_net_degree;
+    int use_bb, backtrack, max_backtrack;
+    float min_gain;
+    int stagnation_window;
+    float step_x_gamma;   // grid.stepX() used by computeGamma
+};
+
+__device__ __forceinline__ float* role_ptr(const DevPtrs& p, int role) {
+    return p.pool + static_cast<size_t>(p.st->role[role]) * p.vec_stride;
+}
+
+// ---- density.cu
+void launch_density_accumulate(const DevPtrs& p, cudaStream_t s);
+// rho + tau partials; write_maps also stores the float maps, zero clears the fixed maps
+void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s);
+void launch_gather_opt(const DevPtrs& p, cudaStream_t s);
+// gather for every density node into a node-indexed 2*total array (parity hook)
+void launch_gather_all(const DevPtrs& p, float* force_nodes, cudaStream_t s);
+
+// ---- wirelength.cu
+void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, int use_dev_gamma,
+                    cudaStream_t s);
+// node-indexed WA gradient for movable nodes (parity hook)
+void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s);
+
+// ---- optimizer.cu
+void launch_scatter(const DevPtrs& p, int role, cudaStream_t s);
+void launch_assemble(const DevPtrs& p, int grad_role, cudaStream_t s);
+void launch_ctl_eval_done(const DevPtrs& p, int count_eval, cudaStream_t s);
+void launch_reduce_diff(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s);
+void launch_redo_update(const DevPtrs& p, cudaStream_t s);
+void launch_nesterov_update(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_iter_end(const DevPtrs& p, cudaStream_t s);
+void launch_snapshot_copy(const DevPtrs& p, cudaStream_t s);
+void launch_init_perturb(const DevPtrs& p, cudaStream_t s);
+void launch_copy_role(const DevPtrs& p, int dst_role, int src_role, cudaStream_t s);
+void launch_deliver(const DevPtrs& p, cudaStream_t s);
+void launch_finalize_slots(const DevPtrs& p, int first, int count, double* out, cudaStream_t s);
+
+}  // namespace spg

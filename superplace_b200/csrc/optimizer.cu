@@ -1,0 +1,659 @@
+// Gradient assembly, Nesterov update with deferred backtracking, and the per-iteration
+// schedule logic of ePlace, all on the device:
+//   objAndGrad assembly       src/gp/eplace.cpp:136-203
+//   NesterovOptimizer::step   src/numeric/cpu/nesterov.cpp:51-122
+//   redoIfOvershot            nesterov.cpp:146-169
+//   estimateInitialStep       nesterov.cpp:190-218
+//   estimateStep              nesterov.cpp:221-240
+//   EPlace::run loop body     eplace.cpp:356-474 (lambda/gamma schedule, stop test,
+//                             stagnation snapshots and rollback)
+//
+// Vector work (2*nOpt floats) runs on RED_BLOCKS x RED_THREADS grids with grid-stride loops,
+// so every FP64 partial sum has a fixed owner and the reductions are deterministic. The
+// scalar logic runs in single-block "control" kernels that first reduce the partials in a
+// fixed tree and then execute the reference's scalar code on thread 0. The host never
+// computes a schedule value; it only reads the small DevState to decide whether to launch
+// another backtracking evaluation or another iteration.
+#include <cfloat>
+
+#include "engine.h"
+
+namespace spg {
+
+namespace {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double ws[32];
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) ws[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        r = lane < static_cast<int>(blockDim.x >> 5) ? ws[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+// Sum of one slot's RED_BLOCKS partials in a fixed order (valid on thread 0).
+__device__ __forceinline__ double finalize(const DevPtrs& p, int slot) {
+    double v = 0.0;
+    for (int j = threadIdx.x; j < RED_BLOCKS; j += blockDim.x) v += p.partials[slot * RED_BLOCKS + j];
+    return block_sum(v);
+}
+
+__device__ __forceinline__ void raise_error(DevState* st, int code) { atomicCAS(&st->error, 0, code); }
+
+// clamp into [lo, hi] with std::min(std::max(v, lo), hi) semantics (eplace.cpp:130-131)
+__device__ __forceinline__ float clamp_box(float v, float lo, float hi) {
+    const float a = (v < lo) ? lo : v;
+    return (hi < a) ? hi : a;
+}
+
+// computeGamma (wa_wirelength.cpp:18-29)
+__device__ float compute_gamma(float tau, float bin_step) {
+    float gamma = fmul(8.0f, bin_step);
+    if (tau > 1.0f) gamma = fmul(gamma, 10.0f);
+    else if (tau < 0.1f) gamma = fmul(gamma, 0.1f);
+    else gamma = fmul(gamma, powf(10.0f, fsub(fmul(20.0f / 9.0f, fsub(tau, 0.1f)), 1.0f)));
+    return fmax_(gamma, 1e-4f);
+}
+
+// lambdaMultiplier (src/gp/lambda_schedule.h:22-25)
+__device__ float lambda_multiplier(double dh, double ref) {
+    const double mu = pow(1.1, -dh / ref + 1.0);
+    return static_cast<float>(fmin(1.05, fmax(0.95, mu)));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ------------------------------------------------------------------ vector kernels
+
+__global__ void scatter_kernel(DevPtrs p, int role) {
+    const float* u = role_ptr(p, role);
+    const int n = p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float x = u[k], y = u[n + k];
+        // objAndGrad rejects non-finite coordinates (eplace.cpp:140-142)
+        if (!isfinite(x) || !isfinite(y)) raise_error(p.st, SPG_E_NON_FINITE);
+        const int i = p.opt_idx[k];
+        p.x[i] = x;
+        p.y[i] = y;
+    }
+}
+
+// grad_k = precond * (dWL - lambda * q*xi), precond = 1 / max(1, deg + lambda*area)
+// (eplace.cpp:166-189), with the WA pass 2 (per-node sum of per-pin contributions in
+// node->pin order, wa_wirelength.cpp:137-179) fused in.
+__global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int grad_role) {
+    float* grad = role_ptr(p, grad_role);
+    const float lambda = p.st->lambda;
+    const int n = p.n_opt;
+    double acc_wl = 0.0, acc_den = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = p.opt_idx[k];
+        const bool has_wl = i < p.num_movable;
+        float gx = 0.f, gy = 0.f;
+        if (has_wl) {
+            for (int t = p.node_start[i]; t < p.node_start[i + 1]; ++t) {
+                const int pin = p.node_pins[t];
+                if (p.pin2net[pin] < 0) continue;
+                gx = fadd(gx, p.gpx[pin]);
+                gy = fadd(gy, p.gpy[pin]);
+            }
+        }
+        const float fx = p.force[k], fy = p.force[n + k];
+        const double den = __dadd_rn(static_cast<double>(p.opt_deg[k]),
+                                     __dmul_rn(static_cast<double>(lambda), p.opt_area[k]));
+        const float precond = static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
+        const float ox = fmul(precond, fsub(gx, fmul(lambda, fx)));
+        const float oy = fmul(precond, fsub(gy, fmul(lambda, fy)));
+        grad[k] = ox;
+        grad[n + k] = oy;
+        if (!isfinite(ox) || !isfinite(oy)) raise_error(p.st, SPG_E_NON_FINITE);
+        if (has_wl) acc_wl += static_cast<double>(fadd(fabsf(gx), fabsf(gy)));
+        acc_den += static_cast<double>(fadd(fabsf(fx), fabsf(fy)));
+    }
+    acc_wl = block_sum(acc_wl);
+    acc_den = block_sum(acc_den);
+    if (threadIdx.x == 0) {
+        p.partials[SLOT_SUM_WL * RED_BLOCKS + blockIdx.x] = acc_wl;
+        p.partials[SLOT_SUM_DEN * RED_BLOCKS + blockIdx.x] = acc_den;
+    }
+}
+
+// dx^2 = |u - uPrev|^2, dg^2 = |g - gPrevTmp|^2, sy = (u-uPrev).(g-gPrevTmp), gn = |g|^2
+// (l2Diff, dotDiff, l2Norm: nesterov.cpp:25-45), one pass over the four vectors.
+__global__ void __launch_bounds__(RED_THREADS) reduce_diff_kernel(DevPtrs p) {
+    const float* u = role_ptr(p, R_U);
+    const float* up = role_ptr(p, R_UPREV);
+    const float* g = role_ptr(p, R_G);
+    const float* gp = role_ptr(p, R_GPREVTMP);
+    const int n = 2 * p.n_opt;
+    double dx = 0.0, dg = 0.0, sy = 0.0, gn = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const double s = static_cast<double>(u[k]) - static_cast<double>(up[k]);
+        const double y = static_cast<double>(g[k]) - static_cast<double>(gp[k]);
+        const double gv = static_cast<double>(g[k]);
+        dx += __dmul_rn(s, s);
+        dg += __dmul_rn(y, y);
+        sy += __dmul_rn(s, y);
+        gn += __dmul_rn(gv, gv);
+    }
+    dx = block_sum(dx);
+    dg = block_sum(dg);
+    sy = block_sum(sy);
+    gn = block_sum(gn);
+    if (threadIdx.x == 0) {
+        p.partials[SLOT_DX * RED_BLOCKS + blockIdx.x] = dx;
+        p.partials[SLOT_DG * RED_BLOCKS + blockIdx.x] = dg;
+        p.partials[SLOT_SY * RED_BLOCKS + blockIdx.x] = sy;
+        p.partials[SLOT_GN * RED_BLOCKS + blockIdx.x] = gn;
+    }
+}
+
+// v = uPrev - alpha*gPrevTmp ; u = v + momentumPrev*(v - vPrev) ; clamp v, u
+// (redoIfOvershot body, nesterov.cpp:158-163). Runs only when the check asked for it.
+__global__ void redo_update_kernel(DevPtrs p) {
+    if (!p.st->redo) return;
+    float* v = role_ptr(p, R_V);
+    float* u = role_ptr(p, R_U);
+    const float* up = role_ptr(p, R_UPREV);
+    const float* gp = role_ptr(p, R_GPREVTMP);
+    const float* vp = role_ptr(p, R_VPREV);
+    const float alpha = p.st->alpha, m = p.st->momentum_prev;
+    const int n = 2 * p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float vk = fsub(up[k], fmul(alpha, gp[k]));
+        const float uk = fadd(vk, fmul(m, fsub(vk, vp[k])));
+        v[k] = clamp_box(vk, p.opt_lo[k], p.opt_hi[k]);
+        u[k] = clamp_box(uk, p.opt_lo[k], p.opt_hi[k]);
+    }
+}
+
+// vNew = u - alpha*g ; uNew = vNew + momentum*(vNew - v) ; clamp both (nesterov.cpp:97-107)
+__global__ void nesterov_update_kernel(DevPtrs p) {
+    const float* u = role_ptr(p, R_U);
+    const float* v = role_ptr(p, R_V);
+    const float* g = role_ptr(p, R_G);
+    float* vn = role_ptr(p, R_VNEW);
+    float* un = role_ptr(p, R_UNEW);
+    const float alpha = p.st->alpha, m = p.st->momentum;
+    const int n = 2 * p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float vk = fsub(u[k], fmul(alpha, g[k]));
+        const float uk = fadd(vk, fmul(m, fsub(vk, v[k])));
+        vn[k] = clamp_box(vk, p.opt_lo[k], p.opt_hi[k]);
+        un[k] = clamp_box(uk, p.opt_lo[k], p.opt_hi[k]);
+    }
+}
+
+__global__ void copy_role_kernel(DevPtrs p, int dst, int src) {
+    float* d = role_ptr(p, dst);
+    const float* s = role_ptr(p, src);
+    const int n = 2 * p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) d[k] = s[k];
+}
+
+__global__ void clamp_role_kernel(DevPtrs p, int role) {
+    float* d = role_ptr(p, role);
+    const int n = 2 * p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        d[k] = clamp_box(d[k], p.opt_lo[k], p.opt_hi[k]);
+}
+
+// Stagnation snapshot: copy lastEval (= uPrev after the role rotation) into its slot.
+__global__ void snapshot_copy_kernel(DevPtrs p) {
+    const int slot = p.st->snap_copy_to;
+    if (slot < 0) return;
+    float* d = p.pool + static_cast<size_t>(NUM_ROLES + slot) * p.vec_stride;
+    const float* s = role_ptr(p, R_UPREV);
+    const int n = 2 * p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) d[k] = s[k];
+}
+
+// Delivered solution into R_POS: v, lastEval, or the picked snapshot (eplace.cpp:412-485).
+__global__ void deliver_kernel(DevPtrs p) {
+    const DevState* st = p.st;
+    const float* s = st->deliver == 1 ? role_ptr(p, R_UPREV)
+                   : st->deliver == 2 ? p.pool + static_cast<size_t>(NUM_ROLES + st->deliver_slot) * p.vec_stride
+                                      : role_ptr(p, R_V);
+    float* d = role_ptr(p, R_POS);
+    const int n = 2 * p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        d[k] = clamp_box(s[k], p.opt_lo[k], p.opt_hi[k]);
+}
+
+// |u|^2 -> SLOT_PN and |gA|^2 -> SLOT_GN for estimateInitialStep (nesterov.cpp:196-198)
+__global__ void __launch_bounds__(RED_THREADS) init_norms_kernel(DevPtrs p) {
+    const float* u = role_ptr(p, R_U);
+    const float* ga = role_ptr(p, R_GA);
+    const int n = 2 * p.n_opt;
+    double pn = 0.0, gn = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const double a = u[k], b = ga[k];
+        pn += __dmul_rn(a, a);
+        gn += __dmul_rn(b, b);
+    }
+    pn = block_sum(pn);
+    gn = block_sum(gn);
+    if (threadIdx.x == 0) {
+        p.partials[SLOT_PN * RED_BLOCKS + blockIdx.x] = pn;
+        p.partials[SLOT_GN * RED_BLOCKS + blockIdx.x] = gn;
+    }
+}
+
+// probe = clamp(u - (float)scale * gA) (nesterov.cpp:200-205); scale is in st->pn.
+__global__ void init_perturb_kernel(DevPtrs p) {
+    const float* u = role_ptr(p, R_U);
+    const float* ga = role_ptr(p, R_GA);
+    float* pr = role_ptr(p, R_PROBE);
+    const float sc = static_cast<float>(p.st->pn);
+    const int n = 2 * p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        pr[k] = clamp_box(fsub(u[k], fmul(sc, ga[k])), p.opt_lo[k], p.opt_hi[k]);
+}
+
+// dx^2 = |probe - u|^2 -> SLOT_DX, dg^2 = |gB - gA|^2 -> SLOT_DG (nesterov.cpp:207-208)
+__global__ void __launch_bounds__(RED_THREADS) init_diff_kernel(DevPtrs p) {
+    const float* u = role_ptr(p, R_U);
+    const float* pr = role_ptr(p, R_PROBE);
+    const float* ga = role_ptr(p, R_GA);
+    const float* gb = role_ptr(p, R_GB);
+    const int n = 2 * p.n_opt;
+    double dx = 0.0, dg = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const double a = static_cast<double>(pr[k]) - static_cast<double>(u[k]);
+        const double b = static_cast<double>(gb[k]) - static_cast<double>(ga[k]);
+        dx += __dmul_rn(a, a);
+        dg += __dmul_rn(b, b);
+    }
+    dx = block_sum(dx);
+    dg = block_sum(dg);
+    if (threadIdx.x == 0) {
+        p.partials[SLOT_DX * RED_BLOCKS + blockIdx.x] = dx;
+        p.partials[SLOT_DG * RED_BLOCKS + blockIdx.x] = dg;
+    }
+}
+
+// ------------------------------------------------------------------ control kernels
+
+// Results of one objAndGrad evaluation (eplace.cpp:149,154-155,190-197).
+__global__ void ctl_eval_done_kernel(DevPtrs p, int count_eval) {
+    const double over = finalize(p, SLOT_OVERFLOW);
+    const double wl = finalize(p, SLOT_WL);
+    const double hp = finalize(p, SLOT_HPWL);
+    const double swl = finalize(p, SLOT_SUM_WL);
+    const double sden = finalize(p, SLOT_SUM_DEN);
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    st->tau = p.movable_area_scaled > 0.0 ? static_cast<float>(over / p.movable_area_scaled) : 0.f;
+    st->hpwl = hp;
+    st->wl_obj = wl;
+    st->sum_wl = swl;
+    st->sum_den = sden;
+    if (!(isfinite(hp) && isfinite(st->tau) && isfinite(wl) && isfinite(swl) && isfinite(sden)))
+        raise_error(st, SPG_E_NON_FINITE);
+    if (count_eval && !st->done) st->evals += 1;
+}
+
+// lambda_0 = sum|dWL| / sum|q xi|, gamma = computeGamma(tau) (eplace.cpp:254-258)
+__global__ void ctl_lambda_init_kernel(DevPtrs p) {
+    DevState* st = p.st;
+    st->gamma = compute_gamma(st->tau, p.step_x_gamma);
+    float lam = st->sum_den > 0.0 ? static_cast<float>(st->sum_wl / st->sum_den) : 1.f;
+    if (!isfinite(lam) || lam <= 0.f) lam = 1.f;
+    st->lambda = lam;
+}
+
+// estimateInitialStep, first half: perturbation scale into st->pn, or alpha0 = 1.
+__global__ void ctl_init_scale_kernel(DevPtrs p, float init_perturb) {
+    const double pn2 = finalize(p, SLOT_PN);
+    const double gn2 = finalize(p, SLOT_GN);
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    const double pos_norm = sqrt(pn2), g_norm = sqrt(gn2);
+    st->redo = 0;
+    if (!(g_norm > 0.0) || !isfinite(g_norm)) {
+        st->alpha0 = 1.f;
+        st->redo = 1;  // marks "alpha0 decided"
+        st->pn = 0.0;
+        return;
+    }
+    st->pn = static_cast<double>(init_perturb) * (pos_norm > 0.0 ? pos_norm : 1.0) / g_norm;
+}
+
+// estimateInitialStep, second half: alpha0 = |probe-u| / |gB-gA| (nesterov.cpp:207-217).
+__global__ void ctl_init_finish_kernel(DevPtrs p) {
+    const double dx2 = finalize(p, SLOT_DX);
+    const double dg2 = finalize(p, SLOT_DG);
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    if (st->redo) {  // decided in the first half
+        st->redo = 0;
+        return;
+    }
+    const double dx = sqrt(dx2), dg = sqrt(dg2);
+    if (!(dx > 0.0) || !(dg > 0.0) || !isfinite(dg)) {
+        st->alpha0 = 1.f;
+        return;
+    }
+    const double L = dg / dx;
+    const double step = 1.0 / L;
+    st->alpha0 = (isfinite(step) && step > 0.0) ? static_cast<float>(step) : 1.f;
+}
+
+// redoIfOvershot's test (nesterov.cpp:148-157): redo when 1/L at the new point is at most
+// 0.95 of the step just taken, at most max_backtrack-1 times per step.
+__global__ void ctl_redo_check_kernel(DevPtrs p) {
+    const double dx2 = finalize(p, SLOT_DX);
+    const double dg2 = finalize(p, SLOT_DG);
+    const double sy = finalize(p, SLOT_SY);
+    const double gn2 = finalize(p, SLOT_GN);
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    st->dx = sqrt(dx2);
+    st->dg = sqrt(dg2);
+    st->sy = sy;
+    st->gn = gn2;
+    st->redo = 0;
+    if (st->error || st->done || st->tries >= p.max_backtrack) return;
+    const double dx = st->dx, dg = st->dg;
+    if (!(dx > 0.0) || !(dg > 0.0) || !isfinite(dg)) return;
+    const double lip = dx / dg;
+    if (lip > 0.95 * static_cast<double>(st->alpha)) return;
+    st->alpha = static_cast<float>(lip);
+    st->redo = 1;
+    st->tries += 1;
+}
+
+// Step size and momentum of this step (nesterov.cpp:87-96, estimateStep :221-240).
+__global__ void ctl_step_kernel(DevPtrs p, int reduce_fresh) {
+    double dx2 = 0.0, dg2 = 0.0, sy = 0.0, gn2 = 0.0;
+    if (reduce_fresh) {
+        dx2 = finalize(p, SLOT_DX);
+        dg2 = finalize(p, SLOT_DG);
+        sy = finalize(p, SLOT_SY);
+        gn2 = finalize(p, SLOT_GN);
+    }
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    if (reduce_fresh) {
+        st->dx = sqrt(dx2);
+        st->dg = sqrt(dg2);
+        st->sy = sy;
+        st->gn = gn2;
+    }
+    st->grad_norm = static_cast<float>(sqrt(st->gn));
+    if (st->iter == 0) {
+        st->alpha = st->alpha0;
+    } else {
+        const double dx = st->dx, dg = st->dg;
+        if (dx > 0.0 && dg > 0.0) {
+            const double lip = dx / dg;
+            float a = static_cast<float>(lip);
+            if (p.use_bb) {
+                const double yy = dg * dg;
+                bool done = false;
+                if (yy > 0.0) {
+                    const double bb = st->sy / yy;
+                    if (bb > 0.0 && isfinite(bb)) {
+                        a = static_cast<float>(bb);
+                        done = true;
+                    }
+                }
+                if (!done) a = static_cast<float>(fmin(dx / dg, lip));
+            }
+            st->alpha = a;
+        }
+    }
+    const float an = st->a;
+    const float a_next = fmul(0.5f, fadd(1.f, __fsqrt_rn(fadd(fmul(fmul(4.f, an), an), 1.f))));
+    st->momentum = fdiv(fsub(an, 1.f), a_next);
+    st->a = a_next;  // a_{k+1}; the update kernel only reads alpha and momentum
+}
+
+// End of one EPlace iteration: role rotation of the optimizer (nesterov.cpp:110-119),
+// lambda/gamma schedule, metrics row, stop test and stagnation guard (eplace.cpp:362-473).
+__global__ void ctl_iter_end_kernel(DevPtrs p) {
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    int* r = st->role;
+    {   // uPrev <- u <- uNew <- (old uPrev); v <- vNew, vPrev <- v, vNew <- (old vPrev);
+        // gPrevTmp <- g (g's buffer is rewritten by the next evaluation)
+        const int u = r[R_U], up = r[R_UPREV], un = r[R_UNEW];
+        r[R_UPREV] = u;
+        r[R_U] = un;
+        r[R_UNEW] = up;
+        const int v = r[R_V], vp = r[R_VPREV], vn = r[R_VNEW];
+        r[R_V] = vn;
+        r[R_VPREV] = v;
+        r[R_VNEW] = vp;
+        const int g = r[R_G], gp = r[R_GPREVTMP];
+        r[R_GPREVTMP] = g;
+        r[R_G] = gp;
+    }
+    st->momentum_prev = st->momentum;
+    const int iter = st->iter;
+    st->iter = iter + 1;
+    st->tries = 1;
+    st->snap_copy_to = -1;
+    if (!(isfinite(st->hpwl) && isfinite(st->tau) && isfinite(st->alpha))) {
+        raise_error(st, SPG_E_NON_FINITE);
+        st->done = 1;
+        return;
+    }
+    // lambda schedule (eplace.cpp:373-380)
+    const float eval_lambda = st->lambda, eval_gamma = st->gamma;
+    const double dh = st->have_prev ? st->hpwl - st->prev_hpwl : 0.0;
+    const float mu = st->have_prev ? lambda_multiplier(dh, st->hpwl_ref) : 1.f;
+    if (st->have_prev) st->lambda = fmul(st->lambda, mu);
+    st->prev_hpwl = st->hpwl;
+    st->have_prev = 1;
+    st->gamma = compute_gamma(st->tau, p.step_x_gamma);
+    if (!isfinite(st->lambda) || !isfinite(st->gamma)) {
+        raise_error(st, SPG_E_NON_FINITE);
+        st->done = 1;
+        return;
+    }
+    // metrics row (eplace.cpp:384-399)
+    if (iter < st->max_iter) {
+        spg_iter_metrics& m = p.metrics[iter];
+        m.iter = iter;
+        m.hpwl = st->hpwl;
+        m.overflow = st->tau;
+        m.lambda = st->lambda;
+        m.gamma = st->gamma;
+        m.step_size = st->alpha;
+        m.grad_norm_wl = static_cast<float>(st->sum_wl);
+        m.grad_norm_den = static_cast<float>(st->sum_den);
+        m.eval_lambda = eval_lambda;
+        m.eval_gamma = eval_gamma;
+        m.delta_hpwl = dh;
+        m.lambda_mu = mu;
+        m.evaluations = st->evals;
+    }
+    const bool filler_only = st->stage == SPG_STAGE_FILLER_ONLY;
+    // stop test: deliver the evaluated point u (eplace.cpp:412-419)
+    if (!filler_only && st->tau < st->target_tau) {
+        st->converged = 1;
+        st->deliver = 1;
+        st->done = 1;
+        return;
+    }
+    if (!filler_only && p.stagnation_window > 0) {
+        const float g = p.min_gain;
+        if (st->tau < fmul(st->ref_tau, fsub(1.f, g))) {
+            st->ref_tau = st->tau;
+            st->since_improve = 0;
+        } else {
+            st->since_improve += 1;
+        }
+        st->best_tau = fmin_(st->best_tau, st->tau);
+        const float tol = fmul(st->best_tau, fadd(1.f, g));
+        while (st->snap_count > 0 && st->snap_tau[st->snap_head] > tol) {
+            st->snap_head = (st->snap_head + 1) % SNAP_MAX;
+            st->snap_count -= 1;
+        }
+        const int last = (st->snap_head + st->snap_count - 1 + SNAP_MAX) % SNAP_MAX;
+        if (st->snap_count == 0 || fmul(st->tau, fadd(1.f, fmul(0.5f, g))) <= st->snap_tau[last]) {
+            if (st->snap_count == SNAP_MAX) {
+                raise_error(st, SPG_E_CAPACITY);
+                st->done = 1;
+                return;
+            }
+            const int slot = (st->snap_head + st->snap_count) % SNAP_MAX;
+            st->snap_tau[slot] = st->tau;
+            st->snap_hpwl[slot] = st->hpwl;
+            st->snap_iter[slot] = iter;
+            st->snap_count += 1;
+            st->snap_copy_to = slot;
+        }
+        if (st->since_improve >= p.stagnation_window) {
+            int pick = st->snap_head;
+            for (int j = 1; j < st->snap_count; ++j) {
+                const int s = (st->snap_head + j) % SNAP_MAX;
+                if (st->snap_hpwl[s] < st->snap_hpwl[pick]) pick = s;
+            }
+            st->stagnated = 1;
+            st->rollback_iter = st->snap_iter[pick];
+            st->deliver = 2;
+            st->deliver_slot = pick;
+            st->done = 1;
+            return;
+        }
+    }
+    if (st->iter >= st->max_iter) st->done = 1;
+}
+
+__global__ void ctl_stage_start_kernel(DevPtrs p) {
+    p.st->t0_ns = global_ns();
+}
+
+__global__ void ctl_elapsed_kernel(DevPtrs p, double* out_ms) {
+    *out_ms = static_cast<double>(global_ns() - p.st->t0_ns) * 1e-6;
+}
+
+__global__ void check_geometry_kernel(DevPtrs p, float lx, float ly, float hx, float hy,
+                                      const float* w, const float* h) {
+    const int n = p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = p.opt_idx[k];
+        const float x = p.x[i], y = p.y[i];
+        if (!isfinite(x) || !isfinite(y)) {
+            raise_error(p.st, SPG_E_NON_FINITE);
+            continue;
+        }
+        const float hw = fmul(0.5f, w[i]), hh = fmul(0.5f, h[i]);
+        // checkGeometry bounds (src/util/invariant.h:24-30)
+        if (!(fsub(x, hw) >= fsub(lx, .01f) && fsub(y, hh) >= fsub(ly, .01f) &&
+              fadd(x, hw) <= fadd(hx, .01f) && fadd(y, hh) <= fadd(hy, .01f)))
+            raise_error(p.st, SPG_E_OUT_OF_CORE);
+    }
+}
+
+__global__ void finalize_slots_kernel(DevPtrs p, int first, int count, double* out) {
+    for (int s = 0; s < count; ++s) {
+        const double v = finalize(p, first + s);
+        if (threadIdx.x == 0) out[s] = v;
+    }
+}
+
+inline int vec_blocks(const DevPtrs& p) {
+    const int b = ceil_div(2 * static_cast<int64_t>(p.n_opt), RED_THREADS);
+    return b < 1 ? 1 : (b > 4 * RED_BLOCKS ? 4 * RED_BLOCKS : b);
+}
+
+}  // namespace
+
+#define LAUNCH(kernel, grid, block, ...)                      \
+    do {                                                       \
+        kernel<<<(grid), (block), 0, s>>>(__VA_ARGS__);        \
+        count_launch();                                        \
+        SPG_CHECK_LAUNCH();                                    \
+    } while (0)
+
+void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
+    LAUNCH(scatter_kernel, vec_blocks(p), RED_THREADS, p, role);
+}
+void launch_assemble(const DevPtrs& p, int grad_role, cudaStream_t s) {
+    LAUNCH(assemble_kernel, RED_BLOCKS, RED_THREADS, p, grad_role);
+}
+void launch_ctl_eval_done(const DevPtrs& p, int count_eval, cudaStream_t s) {
+    LAUNCH(ctl_eval_done_kernel, 1, RED_THREADS, p, count_eval);
+}
+void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(ctl_lambda_init_kernel, 1, 1, p);
+}
+void launch_reduce_diff(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(reduce_diff_kernel, RED_BLOCKS, RED_THREADS, p);
+}
+void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(ctl_redo_check_kernel, 1, RED_THREADS, p);
+}
+void launch_redo_update(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(redo_update_kernel, vec_blocks(p), RED_THREADS, p);
+}
+void launch_ctl_step(const DevPtrs& p, int reduce_fresh, cudaStream_t s) {
+    LAUNCH(ctl_step_kernel, 1, RED_THREADS, p, reduce_fresh);
+}
+void launch_nesterov_update(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(nesterov_update_kernel, vec_blocks(p), RED_THREADS, p);
+}
+void launch_ctl_iter_end(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(ctl_iter_end_kernel, 1, 32, p);
+}
+void launch_snapshot_copy(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(snapshot_copy_kernel, vec_blocks(p), RED_THREADS, p);
+}
+void launch_init_norms(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(init_norms_kernel, RED_BLOCKS, RED_THREADS, p);
+}
+void launch_ctl_init_scale(const DevPtrs& p, float init_perturb, cudaStream_t s) {
+    LAUNCH(ctl_init_scale_kernel, 1, RED_THREADS, p, init_perturb);
+}
+void launch_init_perturb(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(init_perturb_kernel, vec_blocks(p), RED_THREADS, p);
+}
+void launch_init_diff(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(init_diff_kernel, RED_BLOCKS, RED_THREADS, p);
+}
+void launch_ctl_init_finish(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(ctl_init_finish_kernel, 1, RED_THREADS, p);
+}
+void launch_copy_role(const DevPtrs& p, int dst, int src, cudaStream_t s) {
+    LAUNCH(copy_role_kernel, vec_blocks(p), RED_THREADS, p, dst, src);
+}
+void launch_clamp_role(const DevPtrs& p, int role, cudaStream_t s) {
+    LAUNCH(clamp_role_kernel, vec_blocks(p), RED_THREADS, p, role);
+}
+void launch_deliver(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(deliver_kernel, vec_blocks(p), RED_THREADS, p);
+}
+void launch_stage_clock(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(ctl_stage_start_kernel, 1, 1, p);
+}
+void launch_elapsed(const DevPtrs& p, double* out_ms, cudaStream_t s) {
+    LAUNCH(ctl_elapsed_kernel, 1, 1, p, out_ms);
+}
+void launch_check_geometry(const DevPtrs& p, float lx, float ly, float hx, float hy, const float* w,
+                           const float* h, cudaStream_t s) {
+    LAUNCH(check_geometry_kernel, vec_blocks(p), RED_THREADS, p, lx, ly, hx, hy, w, h);
+}
+void launch_finalize_slots(const DevPtrs& p, int first, int count, double* out, cudaStream_t s) {
+    LAUNCH(finalize_slots_kernel, 1, RED_THREADS, p, first, count, out);
+}
+
+}  // namespace spg

@@ -1,0 +1,226 @@
+// Poisson plan, the plain-FP32 contraction path, and the solve driver.
+// The math and the GEMM chain are described in poisson.h.
+//
+// The FP32 path is a register-tiled SIMT SGEMM (64x64 tile, 4x4 per thread, BK 16,
+// register prefetch of the next K slab). It is the "plain FP32 GPU form" the split-BF16
+// tensor-core path (poisson_tc.cu) is measured against, and the exact-enough reference
+// for the parity tests at 1e-5.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "poisson.h"
+
+namespace spg {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
+
+__global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
+    __shared__ float As[BK][BM + 4];
+    __shared__ float Bs[BK][BN + 4];
+    const int z = blockIdx.z;
+    const float* A = g.A + z * g.sA;
+    const float* B = g.B + z * g.sB;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+    const int lr = tid >> 2, lk = (tid & 3) * 4;  // loader: row, k offset
+    float acc[4][4] = {};
+    float ra[4], rb[4];
+
+    auto load = [&](int k0) {
+        const int am = m0 + lr, bn = n0 + lr, k = k0 + lk;
+        if (vec_ok && k + 3 < g.K) {
+            if (am < g.M) {
+                const float4 v = *reinterpret_cast<const float4*>(A + am * g.lda + k);
+                ra[0] = v.x; ra[1] = v.y; ra[2] = v.z; ra[3] = v.w;
+            } else {
+                ra[0] = ra[1] = ra[2] = ra[3] = 0.f;
+            }
+            if (bn < g.N) {
+                const float4 v = *reinterpret_cast<const float4*>(B + bn * g.ldb + k);
+                rb[0] = v.x; rb[1] = v.y; rb[2] = v.z; rb[3] = v.w;
+            } else {
+                rb[0] = rb[1] = rb[2] = rb[3] = 0.f;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                ra[i] = (am < g.M && k + i < g.K) ? A[am * g.lda + k + i] : 0.f;
+                rb[i] = (bn < g.N && k + i < g.K) ? B[bn * g.ldb + k + i] : 0.f;
+            }
+        }
+    };
+
+    load(0);
+    for (int k0 = 0; k0 < g.K; k0 += BK) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            As[lk + i][lr] = ra[i];
+            Bs[lk + i][lr] = rb[i];
+        }
+        __syncthreads();
+        if (k0 + BK < g.K) load(k0 + BK);
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            const float4 a = *reinterpret_cast<const float4*>(&As[kk][ty * 4]);
+            const float4 b = *reinterpret_cast<const float4*>(&Bs[kk][tx * 4]);
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int m = m0 + ty * 4 + i;
+        if (m >= g.M) continue;
+        float* crow = (m < g.split) ? g.C + z * g.sC + m * g.ldc : g.C2 + z * g.sC + (m - g.split) * g.ldc;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int n = n0 + tx * 4 + j;
+            if (n >= g.N) continue;
+            float v = acc[i][j];
+            if (g.S) v *= g.S[m * g.lds + n];
+            crow[n] = v;
+        }
+    }
+}
+
+// Double-precision basis tables, rounded once to float.
+double cospi_ratio(int64_t num, int64_t den) {
+    // cos(pi * num / den) with exact argument reduction modulo 2
+    const int64_t r = num % (2 * den);
+    return std::cos(M_PI * static_cast<double>(r) / static_cast<double>(den));
+}
+double sinpi_ratio(int64_t num, int64_t den) {
+    const int64_t r = num % (2 * den);
+    return std::sin(M_PI * static_cast<double>(r) / static_cast<double>(den));
+}
+
+template <typename T>
+T* dalloc(size_t n, size_t& bytes) {
+    T* p = nullptr;
+    SPG_CUDA(cudaMalloc(&p, n * sizeof(T)));
+    bytes += n * sizeof(T);
+    return p;
+}
+
+}  // namespace
+
+void sgemm_tn(const GemmArgs& g, int batch, cudaStream_t s) {
+    const bool aligned = (g.lda % 4 == 0) && (g.ldb % 4 == 0) &&
+                         (reinterpret_cast<uintptr_t>(g.A) % 16 == 0) &&
+                         (reinterpret_cast<uintptr_t>(g.B) % 16 == 0) && (g.sA % 4 == 0) &&
+                         (g.sB % 4 == 0);
+    dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), batch);
+    sgemm_tn_kernel<<<grid, NT, 0, s>>>(g, aligned ? 1 : 0);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+}
+
+void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, int precision,
+                         int batch_cap) {
+    SPG_REQUIRE(nx >= 2 && ny >= 2, SPG_E_INVALID, "Poisson: grid must be at least 2x2");
+    SPG_REQUIRE(sx > 0.f && sy > 0.f, SPG_E_INVALID, "Poisson: bin step must be positive");
+    SPG_REQUIRE(precision == SPG_POISSON_FP32 || precision == SPG_POISSON_BF16X3, SPG_E_INVALID,
+                "Poisson: unknown precision");
+    SPG_REQUIRE(batch_cap >= 1, SPG_E_INVALID, "Poisson: batch capacity must be positive");
+    if (precision == SPG_POISSON_BF16X3)
+        SPG_REQUIRE(tc_supported(nx, ny), SPG_E_INVALID,
+                    "Poisson: split-BF16 path needs nx, ny multiples of 128");
+    pl.nx = nx;
+    pl.ny = ny;
+    pl.step_x = sx;
+    pl.step_y = sy;
+    pl.precision = precision;
+    pl.batch_cap = batch_cap;
+    pl.name = precision == SPG_POISSON_FP32 ? "cuda-sm100a-fp32" : "cuda-sm100a-bf16x3";
+
+    const size_t X = nx, Y = ny;
+    std::vector<float> cy(Y * Y), cx(X * X), bcat(2 * Y * Y), acat(2 * X * X), sc(X * Y);
+    std::vector<double> u(X), v(Y);
+    for (size_t j = 0; j < X; ++j) u[j] = M_PI * static_cast<double>(j) / (static_cast<double>(nx) * sx);
+    for (size_t k = 0; k < Y; ++k) v[k] = M_PI * static_cast<double>(k) / (static_cast<double>(ny) * sy);
+    for (size_t k = 0; k < Y; ++k)
+        for (size_t y = 0; y < Y; ++y) {
+            const int64_t num = static_cast<int64_t>(k) * (2 * static_cast<int64_t>(y) + 1);
+            const double c = cospi_ratio(num, 2 * static_cast<int64_t>(ny));
+            const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(ny));
+            cy[k * Y + y] = static_cast<float>(c);
+            bcat[y * Y + k] = static_cast<float>((k == 0 ? 1.0 : 2.0) * c);      // Ay[y][k]
+            bcat[(Y + y) * Y + k] = static_cast<float>(2.0 * v[k] * s);          // Sy[y][k]
+        }
+    for (size_t j = 0; j < X; ++j)
+        for (size_t x = 0; x < X; ++x) {
+            const int64_t num = static_cast<int64_t>(j) * (2 * static_cast<int64_t>(x) + 1);
+            const double c = cospi_ratio(num, 2 * static_cast<int64_t>(nx));
+            const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(nx));
+            cx[j * X + x] = static_cast<float>(c);
+            acat[x * X + j] = static_cast<float>((j == 0 ? 1.0 : 2.0) * c);      // Ax[x][j]
+            acat[(X + x) * X + j] = static_cast<float>(2.0 * u[j] * s);          // Sx[x][j]
+        }
+    const double nn = static_cast<double>(nx) * static_cast<double>(ny);
+    for (size_t j = 0; j < X; ++j)
+        for (size_t k = 0; k < Y; ++k) {
+            const double den = u[j] * u[j] + v[k] * v[k];
+            sc[j * Y + k] = den > 0.0 ? static_cast<float>(1.0 / (nn * den)) : 0.f;
+        }
+
+    size_t& b = pl.bytes;
+    pl.cy = dalloc<float>(Y * Y, b);
+    pl.cx = dalloc<float>(X * X, b);
+    pl.bcat = dalloc<float>(2 * Y * Y, b);
+    pl.acat = dalloc<float>(2 * X * X, b);
+    pl.scale = dalloc<float>(X * Y, b);
+    SPG_CUDA(cudaMemcpy(pl.cy, cy.data(), cy.size() * 4, cudaMemcpyHostToDevice));
+    SPG_CUDA(cudaMemcpy(pl.cx, cx.data(), cx.size() * 4, cudaMemcpyHostToDevice));
+    SPG_CUDA(cudaMemcpy(pl.bcat, bcat.data(), bcat.size() * 4, cudaMemcpyHostToDevice));
+    SPG_CUDA(cudaMemcpy(pl.acat, acat.data(), acat.size() * 4, cudaMemcpyHostToDevice));
+    SPG_CUDA(cudaMemcpy(pl.scale, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice));
+    if (precision == SPG_POISSON_FP32) {
+        const size_t B = static_cast<size_t>(batch_cap);
+        pl.t0t = dalloc<float>(B * X * Y, b);
+        pl.p = dalloc<float>(B * X * Y, b);
+        pl.t12t = dalloc<float>(2 * B * X * Y, b);
+    } else {
+        tc_plan_create(pl);
+    }
+}
+
+void poisson_plan_destroy(PoissonPlan& pl) {
+    if (pl.precision == SPG_POISSON_BF16X3) tc_plan_destroy(pl);
+    for (float* q : {pl.cy, pl.cx, pl.bcat, pl.acat, pl.scale, pl.t0t, pl.p, pl.t12t})
+        if (q) cudaFree(q);
+    pl.cy = pl.cx = pl.bcat = pl.acat = pl.scale = pl.t0t = pl.p = pl.t12t = nullptr;
+}
+
+void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
+                   cudaStream_t s) {
+    SPG_REQUIRE(batch >= 1 && batch <= pl.batch_cap, SPG_E_CAPACITY, "Poisson: batch exceeds plan");
+    if (pl.precision == SPG_POISSON_BF16X3) {
+        tc_solve(pl, batch, rho, phi, ex, ey, s);
+        return;
+    }
+    const int X = pl.nx, Y = pl.ny;
+    const int64_t BX = static_cast<int64_t>(batch) * X;
+    const int64_t XY = static_cast<int64_t>(X) * Y;
+    // G1: T0t (Y x B*X) = Cy . rho_all^T
+    sgemm_tn({pl.cy, rho, pl.t0t, nullptr, nullptr, Y, static_cast<int>(BX), Y, Y, Y, Y, BX, 0, 0, 0, 0}, 1, s);
+    // G2: P_g (X x Y) = Cx . T0t[:, g]^T, times the spectral scale
+    sgemm_tn({pl.cx, pl.t0t, pl.p, nullptr, pl.scale, X, Y, X, X, X, BX, Y, Y, 0, X, XY}, batch, s);
+    // G3: T12t (2Y x B*X) = [Ay; Sy] . P_all^T
+    sgemm_tn({pl.bcat, pl.p, pl.t12t, nullptr, nullptr, 2 * Y, static_cast<int>(BX), Y, 2 * Y, Y, Y, BX, 0, 0, 0, 0}, 1, s);
+    // G4a: [phi_g; xi_x_g] = [Ax; Sx] . T1t[:, g]^T
+    sgemm_tn({pl.acat, pl.t12t, phi, ex, nullptr, 2 * X, Y, X, X, X, BX, Y, 0, 0, X, XY}, batch, s);
+    // G4b: xi_y_g = Ax . T2t[:, g]^T
+    sgemm_tn({pl.acat, pl.t12t + static_cast<int64_t>(Y) * BX, ey, nullptr, nullptr, X, Y, X, X, X, BX, Y, 0, 0, X, XY},
+             batch, s);
+}
+
+}  // namespace spg

@@ -1,0 +1,74 @@
+// Poisson solve on the bin grid as dense cosine-matrix contractions (sm_100a).
+//
+// Math (FFTW r2r definitions, src/numeric/cpu/cpu_poisson.cpp:1-40): with rho[x][y]
+// (x slow, y fast), Cx[j][x] = cos(pi j (x+1/2)/nx), Cy[k][y] = cos(pi k (y+1/2)/ny),
+// c_0 = 1, c_{j>0} = 2, u_j = pi j/(nx sx), v_k = pi k/(ny sy):
+//   P    = (Cx rho Cy^T) / (nx ny (u_j^2 + v_k^2)),  P[0][0] = 0
+//   phi  = Ax P Ay^T             Ax[x][j] = c_j cos(pi j (x+1/2)/nx)
+//   xi_x = Sx P Ay^T             Sx[x][j] = 2 u_j sin(pi j (x+1/2)/nx)
+//   xi_y = Ax P Sy^T             Sy[y][k] = 2 v_k sin(pi k (y+1/2)/ny)
+// The RODFT01 index shift of the reference (cpu_poisson.cpp:182-206) is folded into the
+// sine bases, so no reorder or sign pass is needed.
+//
+// Every contraction is written C[m][n] = sum_k A[m][k] B[n][k] (both operands K-major):
+//   G1  T0t  (ny x nx)  = Cy        . rho^T          K = ny
+//   G2  P    (nx x ny)  = Cx        . T0t^T  (x S)   K = nx   (spectral divide epilogue)
+//   G3  T12t (2ny x nx) = [Ay; Sy]  . P^T            K = ny
+//   G4  [phi; xi_x]     = [Ax; Sx]  . T1t^T          K = nx
+//       xi_y            = Ax        . T2t^T          K = nx
+// 14 nx ny max(nx,ny) flops for a square grid (2+2+4+4+2 M^3).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace spg {
+
+struct PoissonPlan {
+    int nx = 0, ny = 0, batch_cap = 1;
+    float step_x = 1.f, step_y = 1.f;
+    int precision = 0;
+    std::string name;
+    // FP32 bases
+    float *cy = nullptr, *cx = nullptr, *bcat = nullptr, *acat = nullptr, *scale = nullptr;
+    // FP32 work (sized for batch_cap grids)
+    float *t0t = nullptr, *p = nullptr, *t12t = nullptr;
+    // split-BF16 bases and work: hi and lo planes, stored [hi | lo] per matrix
+    uint16_t *cy_s = nullptr, *cx_s = nullptr, *bcat_s = nullptr, *acat_s = nullptr;
+    uint16_t *rho_s = nullptr, *t0t_s = nullptr, *p_s = nullptr, *t12t_s = nullptr;
+    void* tc = nullptr;  // tensor-core launch state (poisson_tc.cu)
+    size_t bytes = 0;    // device memory held
+};
+
+// Allocates bases and work buffers for up to batch_cap grids. precision: SPG_POISSON_*.
+void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float step_x, float step_y,
+                         int precision, int batch_cap);
+void poisson_plan_destroy(PoissonPlan& pl);
+// Device solve of `batch` grids stored back to back.
+void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
+                   cudaStream_t s);
+
+// ---- FP32 SIMT GEMM "TN": C[m][n] = sum_k A[m*lda+k] * B[n*ldb+k] (optionally * S[m][n]).
+// Rows m >= split go to C2 (row m - split) so one launch can fill two outputs.
+struct GemmArgs {
+    const float* A;
+    const float* B;
+    float* C;
+    float* C2;
+    const float* S;
+    int M, N, K, split;
+    int64_t lda, ldb, ldc, lds;
+    int64_t sA, sB, sC;  // per-batch strides (blockIdx.z)
+};
+void sgemm_tn(const GemmArgs& g, int batch, cudaStream_t s);
+
+// ---- tensor-core path (poisson_tc.cu)
+bool tc_supported(int nx, int ny);
+void tc_plan_create(PoissonPlan& pl);
+void tc_plan_destroy(PoissonPlan& pl);
+void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
+              cudaStream_t s);
+
+}  // namespace spg

@@ -1,0 +1,317 @@
+"""Python host over the C ABI (include/spgpu.h), mirroring the reference's operator API
+for the GP path:
+
+* ``make_poisson_backend`` / ``PoissonBackend.solve``  — src/numeric/poisson_backend.h:20-60
+* ``initialize_fillers`` / ``scatter_fillers``        — src/gp/filler.h:29-32
+* ``BinGrid``-style operators on ``GpContext``        — src/gp/bin_grid.h:23-52
+* ``GpContext.wa`` / ``GpContext.hpwl``               — src/gp/wa_wirelength.h:29-33, src/db/hpwl.h:16
+* ``EPlace.run``                                      — src/gp/eplace.h:56-77
+
+There is no CPU fallback: if libspgpu.so is missing or no sm_100 device is visible, the
+constructors raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .placedb import PlaceDB
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libspgpu.so")
+_lib = None
+
+
+class SpgError(RuntimeError):
+    """A failed C-ABI call; ``kind`` is the reference InvariantError kind when it maps to one."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+        self.kind = abi.ERROR_KINDS.get(code)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built (run python -m superplace_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        vp, fp, dp, ip = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int)
+        i64p = C.POINTER(C.c_int64)
+        L.spg_last_error.restype = C.c_char_p
+        L.spg_poisson_name.restype = C.c_char_p
+        L.spg_poisson_name.argtypes = [vp]
+        L.spg_poisson_create_batched.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
+                                                 C.c_int, C.POINTER(vp)]
+        L.spg_poisson_create.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
+                                         C.POINTER(vp)]
+        L.spg_poisson_solve.argtypes = [vp, fp, fp, fp, fp]
+        L.spg_poisson_solve_device.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.spg_poisson_solve_batch_device.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
+        L.spg_poisson_destroy.argtypes = [vp]
+        L.spg_fillers_plan.argtypes = [C.POINTER(abi.DbView), C.c_float, C.POINTER(abi.FillerInfo)]
+        L.spg_fillers_scatter.argtypes = [C.POINTER(abi.DbView), C.c_int32, C.c_float, C.c_float,
+                                          C.c_uint64, fp, fp]
+        L.spg_ctx_create.argtypes = [C.POINTER(abi.DbView), C.POINTER(abi.Params), C.POINTER(vp)]
+        L.spg_ctx_destroy.argtypes = [vp]
+        L.spg_positions_h2d.argtypes = [vp, fp, fp]
+        L.spg_positions_d2h.argtypes = [vp, fp, fp]
+        L.spg_flags_h2d.argtypes = [vp, C.POINTER(C.c_uint8)]
+        L.spg_grid_init.argtypes = [vp, C.c_float, C.c_int]
+        L.spg_grid_info.argtypes = [vp, ip, fp, fp, fp, fp, dp]
+        L.spg_grid_read.argtypes = [vp, C.c_int, fp]
+        L.spg_grid_write.argtypes = [vp, C.c_int, fp]
+        L.spg_grid_read_fixed.argtypes = [vp, i64p, i64p, ip]
+        L.spg_density_accumulate.argtypes = [vp]
+        L.spg_overflow.argtypes = [vp, fp]
+        L.spg_solve_field.argtypes = [vp]
+        L.spg_gather_force.argtypes = [vp, fp]
+        L.spg_total_charge.argtypes = [vp, dp]
+        L.spg_wa_wirelength.argtypes = [vp, C.c_float, C.c_int, dp, fp]
+        L.spg_hpwl.argtypes = [vp, dp]
+        L.spg_stage_run.argtypes = [vp, C.c_int, C.POINTER(abi.Result)]
+        L.spg_metrics_d2h.argtypes = [vp, C.POINTER(abi.IterMetrics), C.c_int, ip]
+        L.spg_ctx_launch_count.restype = C.c_int64
+        L.spg_ctx_launch_count.argtypes = [vp]
+        L.spg_ctx_stream.restype = vp
+        L.spg_ctx_stream.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise SpgError(rc, lib().spg_last_error().decode())
+
+
+def device_available() -> bool:
+    return lib().spg_device_check() == 0
+
+
+def launch_count() -> int:
+    return int(lib().spg_ctx_launch_count(None))
+
+
+# ------------------------------------------------------------------ Poisson operator
+class PoissonBackend:
+    """PoissonBackend (src/numeric/poisson_backend.h:20-46) on the device.
+
+    ``solve(density, phi, field_x, field_y)`` takes and fills host arrays of shape
+    (nx, ny) (row-major, y fast), as the reference's spans."""
+
+    def __init__(self, nx, ny, step_x, step_y, precision=abi.POISSON_FP32, batch=1):
+        self.nx, self.ny = int(nx), int(ny)
+        h = C.c_void_p()
+        check(lib().spg_poisson_create_batched(self.nx, self.ny, step_x, step_y, precision, batch,
+                                               C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.spg_poisson_destroy(self.h)
+            self.h = None
+
+    def name(self) -> str:
+        return lib().spg_poisson_name(self.h).decode()
+
+    def solve(self, density, phi=None, field_x=None, field_y=None):
+        rho = np.ascontiguousarray(density, np.float32).reshape(self.nx, self.ny)
+        phi = np.empty_like(rho) if phi is None else phi
+        fx = np.empty_like(rho) if field_x is None else field_x
+        fy = np.empty_like(rho) if field_y is None else field_y
+        check(lib().spg_poisson_solve(self.h, abi.fptr(rho), abi.fptr(phi), abi.fptr(fx),
+                                      abi.fptr(fy)))
+        return phi, fx, fy
+
+    def solve_device(self, rho_ptr, phi_ptr, fx_ptr, fy_ptr, stream=0, batch=1):
+        """Device-pointer solve (ints are raw device addresses)."""
+        check(lib().spg_poisson_solve_batch_device(self.h, batch, C.c_void_p(rho_ptr),
+                                                   C.c_void_p(phi_ptr), C.c_void_p(fx_ptr),
+                                                   C.c_void_p(fy_ptr), C.c_void_p(stream)))
+
+
+def make_poisson_backend(nx, ny, step_x=1.0, step_y=1.0, precision=abi.POISSON_FP32):
+    return PoissonBackend(nx, ny, step_x, step_y, precision)
+
+
+# ------------------------------------------------------------------ fillers
+def initialize_fillers(db: PlaceDB, target_density=1.0, seed=1002) -> abi.FillerInfo:
+    """initializeFillers (src/gp/filler.cpp:47-139): replaces db's filler segment."""
+    db.num_fillers = 0
+    db.node_x, db.node_y = db.node_x[: db.num_nodes], db.node_y[: db.num_nodes]
+    db.node_w, db.node_h = db.node_w[: db.num_nodes], db.node_h[: db.num_nodes]
+    db.node_flags = db.node_flags[: db.num_nodes]
+    db.extend_node2pin()
+    v = db.view()
+    info = abi.FillerInfo()
+    check(lib().spg_fillers_plan(C.byref(v), target_density, C.byref(info)))
+    if info.count > 0:
+        x = np.zeros(info.count, np.float32)
+        y = np.zeros(info.count, np.float32)
+        check(lib().spg_fillers_scatter(C.byref(v), info.count, info.width, info.height, seed,
+                                        abi.fptr(x), abi.fptr(y)))
+        db.set_fillers(info.count, info.width, info.height, x, y)
+    return info
+
+
+def scatter_fillers(db: PlaceDB, seed=1002, seed_offset=0) -> None:
+    """scatterFillers (src/gp/filler.cpp:33-45) for the existing fillers."""
+    if db.num_fillers == 0:
+        return
+    v = db.view()
+    x = np.zeros(db.num_fillers, np.float32)
+    y = np.zeros(db.num_fillers, np.float32)
+    w = float(db.node_w[db.num_nodes])
+    h = float(db.node_h[db.num_nodes])
+    check(lib().spg_fillers_scatter(C.byref(v), db.num_fillers, w, h, seed + seed_offset,
+                                    abi.fptr(x), abi.fptr(y)))
+    db.node_x[db.num_nodes:] = x
+    db.node_y[db.num_nodes:] = y
+
+
+# ------------------------------------------------------------------ placement context
+MAP_NODE, MAP_FILLER, MAP_TERMINAL, MAP_BASE, MAP_RHO, MAP_PHI, MAP_XI_X, MAP_XI_Y = range(8)
+
+
+class GpContext:
+    """A PlaceDB resident on the device, with the BinGrid / WA / HPWL operators and the
+    stage loop. Positions live on the device between calls."""
+
+    def __init__(self, db: PlaceDB, params: abi.Params | None = None):
+        self.db = db
+        self.params = params or abi.default_params()
+        self._view = db.view()
+        h = C.c_void_p()
+        check(lib().spg_ctx_create(C.byref(self._view), C.byref(self.params), C.byref(h)))
+        self.h = h
+        self.dim = 0
+
+    def close(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.spg_ctx_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def stream(self) -> int:
+        """Raw cudaStream_t of this context (every call enqueues on it)."""
+        return int(lib().spg_ctx_stream(self.h) or 0)
+
+    # positions and flags
+    def set_positions(self, x=None, y=None):
+        x = np.ascontiguousarray(self.db.node_x if x is None else x, np.float32)
+        y = np.ascontiguousarray(self.db.node_y if y is None else y, np.float32)
+        check(lib().spg_positions_h2d(self.h, abi.fptr(x), abi.fptr(y)))
+
+    def positions(self):
+        n = self.db.total_nodes
+        x, y = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        check(lib().spg_positions_d2h(self.h, abi.fptr(x), abi.fptr(y)))
+        return x, y
+
+    def set_flags(self, flags):
+        f = np.ascontiguousarray(flags, np.uint8)
+        check(lib().spg_flags_h2d(self.h, abi.u8ptr(f)))
+
+    # BinGrid
+    def grid_init(self, target_density=None, bin_dim=None):
+        td = self.params.target_density if target_density is None else target_density
+        bd = self.params.gp_bin_dim if bin_dim is None else bin_dim
+        check(lib().spg_grid_init(self.h, td, bd))
+        info = self.grid_info()
+        self.dim = info["dim"]
+        return info
+
+    def grid_info(self):
+        d = C.c_int()
+        sx, sy, ox, oy = C.c_float(), C.c_float(), C.c_float(), C.c_float()
+        den = C.c_double()
+        check(lib().spg_grid_info(self.h, C.byref(d), C.byref(sx), C.byref(sy), C.byref(ox),
+                                  C.byref(oy), C.byref(den)))
+        return dict(dim=d.value, step_x=sx.value, step_y=sy.value, origin_x=ox.value,
+                    origin_y=oy.value, overflow_denominator=den.value)
+
+    def read_map(self, which):
+        out = np.zeros(self.dim * self.dim, np.float32)
+        check(lib().spg_grid_read(self.h, which, abi.fptr(out)))
+        return out.reshape(self.dim, self.dim)
+
+    def write_map(self, which, a):
+        a = np.ascontiguousarray(a, np.float32).ravel()
+        check(lib().spg_grid_write(self.h, which, abi.fptr(a)))
+
+    def read_fixed(self):
+        n = self.dim * self.dim
+        a, b = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        s = C.c_int()
+        check(lib().spg_grid_read_fixed(self.h, a.ctypes.data_as(C.POINTER(C.c_int64)),
+                                        b.ctypes.data_as(C.POINTER(C.c_int64)), C.byref(s)))
+        return a, b, s.value
+
+    def accumulate(self):
+        check(lib().spg_density_accumulate(self.h))
+
+    def overflow(self) -> float:
+        t = C.c_float()
+        check(lib().spg_overflow(self.h, C.byref(t)))
+        return t.value
+
+    def solve_field(self):
+        check(lib().spg_solve_field(self.h))
+
+    def gather_force(self):
+        out = np.zeros(2 * self.db.total_nodes, np.float32)
+        check(lib().spg_gather_force(self.h, abi.fptr(out)))
+        return out
+
+    def total_charge(self) -> float:
+        c = C.c_double()
+        check(lib().spg_total_charge(self.h, C.byref(c)))
+        return c.value
+
+    # wirelength
+    def wa(self, gamma, ignore_net_degree=100):
+        g = np.zeros(2 * self.db.num_movable, np.float32)
+        wl = C.c_double()
+        check(lib().spg_wa_wirelength(self.h, gamma, ignore_net_degree, C.byref(wl), abi.fptr(g)))
+        return wl.value, g
+
+    def hpwl(self) -> float:
+        v = C.c_double()
+        check(lib().spg_hpwl(self.h, C.byref(v)))
+        return v.value
+
+    # EPlace
+    def run(self, stage=abi.STAGE_MGP) -> abi.Result:
+        r = abi.Result()
+        check(lib().spg_stage_run(self.h, stage, C.byref(r)))
+        return r
+
+    def metrics(self, cap=100000):
+        rows = (abi.IterMetrics * cap)()
+        n = C.c_int()
+        check(lib().spg_metrics_d2h(self.h, rows, cap, C.byref(n)))
+        keys = [f[0] for f in abi.IterMetrics._fields_]
+        return {k: np.array([getattr(rows[i], k) for i in range(n.value)]) for k in keys}
+
+
+class EPlace:
+    """EPlace (src/gp/eplace.h:56-77): construct over a PlaceDB + params, then run stages.
+    The PlaceDB's positions are updated from the device after each run."""
+
+    def __init__(self, db: PlaceDB, params: abi.Params | None = None):
+        self.db = db
+        self.ctx = GpContext(db, params)
+
+    def run(self, stage=abi.STAGE_MGP) -> abi.Result:
+        self.ctx.set_positions(self.db.node_x, self.db.node_y)
+        self.ctx.set_flags(self.db.node_flags)
+        r = self.ctx.run(stage)
+        x, y = self.ctx.positions()
+        self.db.node_x[:] = x
+        self.db.node_y[:] = y
+        return r

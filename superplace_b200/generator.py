@@ -17,7 +17,7 @@ so flat_net2pin is the identity, as in a BookShelf .nets file.
 
 Initial placement: the reference starts mGP from a quadratic (B2B) placement, which is
 outside this path. These instances start from a seeded Gaussian cluster around the core
-centre (sigma = core/8), the same "cells piled near the centre" situation the reference's
+centre (sigma = core/20), the same "cells piled near the centre" situation the reference's
 own GP regression fixture uses (test/test_eplace.cpp:45-56).
 """
 from __future__ import annotations
@@ -70,7 +70,7 @@ def _rows(n_rows, row_h, width, ly0=0.0):
             np.ones(n_rows, np.float32), np.full(n_rows, int(width), np.int32))
 
 
-def _cluster_xy(rng, n, core, w, h, sigma_frac=0.125):
+def _cluster_xy(rng, n, core, w, h, sigma_frac=0.05):
     lx, ly, hx, hy = core
     cx, cy = 0.5 * (lx + hx), 0.5 * (ly + hy)
     x = cx + rng.normal(0.0, sigma_frac * (hx - lx), n)
