@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
     const int z = blockIdx.z;
     const float* A = g.A + z * g.sA;
     const float* B = g.B + z * g.sB;
+    const float* boff = g.boff ? g.boff + z * g.sBoff : nullptr;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
@@ -52,6 +53,11 @@ __global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
                 ra[i] = (am < g.M && k + i < g.K) ? A[am * g.lda + k + i] : 0.f;
                 rb[i] = (bn < g.N && k + i < g.K) ? B[bn * g.ldb + k + i] : 0.f;
             }
+        }
+        if (boff && bn < g.N) {  // DC split: B row minus its mean
+            const float o = boff[bn];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) rb[i] = (k + i < g.K) ? rb[i] - o : 0.f;
         }
     };
 
@@ -92,6 +98,34 @@ __global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
     }
 }
 
+// One warp per (row, segment): FP64 sum of `seg` contiguous floats, fixed shuffle tree.
+__global__ void row_stats_kernel(const float* a, int rows, int nseg, int64_t ld, int seg,
+                                 float* mean, float* sum) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= rows * nseg) return;
+    const int r = w % rows, sg = w / rows;
+    const float* p = a + r * ld + static_cast<int64_t>(sg) * seg;
+    double v = 0.0;
+    for (int i = lane; i < seg; i += 32) v += static_cast<double>(p[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) {
+        mean[w] = static_cast<float>(v / seg);
+        sum[w] = static_cast<float>(v);
+    }
+}
+
+__global__ void set_row0_kernel(float* C, int64_t sC, int n, const float* vals, int64_t sv,
+                                const float* scale) {
+    const int z = blockIdx.y;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float v = vals[z * sv + i];
+        if (scale) v *= scale[i];
+        C[z * sC + i] = v;
+    }
+}
+
 // Double-precision basis tables, rounded once to float.
 double cospi_ratio(int64_t num, int64_t den) {
     // cos(pi * num / den) with exact argument reduction modulo 2
@@ -120,6 +154,23 @@ void sgemm_tn(const GemmArgs& g, int batch, cudaStream_t s) {
                          (g.sB % 4 == 0);
     dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), batch);
     sgemm_tn_kernel<<<grid, NT, 0, s>>>(g, aligned ? 1 : 0);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+}
+
+void row_stats(const float* a, int rows, int cols, int64_t ld, int seg, float* mean, float* sum,
+               cudaStream_t s) {
+    const int nseg = cols / seg;
+    const int warps = rows * nseg;
+    row_stats_kernel<<<ceil_div(warps, 8), 256, 0, s>>>(a, rows, nseg, ld, seg, mean, sum);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+}
+
+void set_row0(float* C, int64_t sC, int n, const float* vals, int64_t sv, const float* scale,
+              int batch, cudaStream_t s) {
+    dim3 grid(ceil_div(n, 256), batch);
+    set_row0_kernel<<<grid, 256, 0, s>>>(C, sC, n, vals, sv, scale);
     count_launch();
     SPG_CHECK_LAUNCH();
 }
@@ -183,6 +234,10 @@ void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, in
     SPG_CUDA(cudaMemcpy(pl.bcat, bcat.data(), bcat.size() * 4, cudaMemcpyHostToDevice));
     SPG_CUDA(cudaMemcpy(pl.acat, acat.data(), acat.size() * 4, cudaMemcpyHostToDevice));
     SPG_CUDA(cudaMemcpy(pl.scale, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice));
+    {
+        const size_t B = static_cast<size_t>(batch_cap);
+        pl.dc = dalloc<float>(4 * B * std::max(X, Y), b);  // row means / sums, both splits
+    }
     if (precision == SPG_POISSON_FP32) {
         const size_t B = static_cast<size_t>(batch_cap);
         pl.t0t = dalloc<float>(B * X * Y, b);
@@ -195,9 +250,9 @@ void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, in
 
 void poisson_plan_destroy(PoissonPlan& pl) {
     if (pl.precision == SPG_POISSON_BF16X3) tc_plan_destroy(pl);
-    for (float* q : {pl.cy, pl.cx, pl.bcat, pl.acat, pl.scale, pl.t0t, pl.p, pl.t12t})
+    for (float* q : {pl.cy, pl.cx, pl.bcat, pl.acat, pl.scale, pl.t0t, pl.p, pl.t12t, pl.dc})
         if (q) cudaFree(q);
-    pl.cy = pl.cx = pl.bcat = pl.acat = pl.scale = pl.t0t = pl.p = pl.t12t = nullptr;
+    pl.cy = pl.cx = pl.bcat = pl.acat = pl.scale = pl.t0t = pl.p = pl.t12t = pl.dc = nullptr;
 }
 
 void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
@@ -210,10 +265,25 @@ void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, flo
     const int X = pl.nx, Y = pl.ny;
     const int64_t BX = static_cast<int64_t>(batch) * X;
     const int64_t XY = static_cast<int64_t>(X) * Y;
-    // G1: T0t (Y x B*X) = Cy . rho_all^T
-    sgemm_tn({pl.cy, rho, pl.t0t, nullptr, nullptr, Y, static_cast<int>(BX), Y, Y, Y, Y, BX, 0, 0, 0, 0}, 1, s);
-    // G2: P_g (X x Y) = Cx . T0t[:, g]^T, times the spectral scale
-    sgemm_tn({pl.cx, pl.t0t, pl.p, nullptr, pl.scale, X, Y, X, X, X, BX, Y, Y, 0, X, XY}, batch, s);
+    const int64_t MXY = std::max(X, Y) * static_cast<int64_t>(batch);
+    float* mean_r = pl.dc;
+    float* sum_r = pl.dc + MXY;
+    float* mean_t = pl.dc + 2 * MXY;
+    float* sum_t = pl.dc + 3 * MXY;
+    // G1: T0t (Y x B*X) = Cy . (rho_all - rowmean)^T, DC row from the exact row sums
+    row_stats(rho, static_cast<int>(BX), Y, Y, Y, mean_r, sum_r, s);
+    GemmArgs g1{pl.cy, rho, pl.t0t, nullptr, nullptr, Y, static_cast<int>(BX), Y, Y, Y, Y, BX, 0, 0, 0, 0};
+    g1.boff = mean_r;
+    sgemm_tn(g1, 1, s);
+    set_row0(pl.t0t, 0, static_cast<int>(BX), sum_r, 0, nullptr, 1, s);
+    // G2: P_g (X x Y) = Cx . (T0t[:, g] - rowmean)^T times the spectral scale; row 0 of P_g
+    // (the x-DC row) from the exact sums
+    row_stats(pl.t0t, Y, static_cast<int>(BX), BX, X, mean_t, sum_t, s);
+    GemmArgs g2{pl.cx, pl.t0t, pl.p, nullptr, pl.scale, X, Y, X, X, X, BX, Y, Y, 0, X, XY};
+    g2.boff = mean_t;
+    g2.sBoff = Y;
+    sgemm_tn(g2, batch, s);
+    set_row0(pl.p, XY, Y, sum_t, Y, pl.scale, batch, s);
     // G3: T12t (2Y x B*X) = [Ay; Sy] . P_all^T
     sgemm_tn({pl.bcat, pl.p, pl.t12t, nullptr, nullptr, 2 * Y, static_cast<int>(BX), Y, 2 * Y, Y, Y, BX, 0, 0, 0, 0}, 1, s);
     // G4a: [phi_g; xi_x_g] = [Ax; Sx] . T1t[:, g]^T

@@ -35,6 +35,8 @@ struct PoissonPlan {
     float *cy = nullptr, *cx = nullptr, *bcat = nullptr, *acat = nullptr, *scale = nullptr;
     // FP32 work (sized for batch_cap grids)
     float *t0t = nullptr, *p = nullptr, *t12t = nullptr;
+    float* dc = nullptr;  // DC-split row means and sums
+
     // split-BF16 bases and work: hi and lo planes, stored [hi | lo] per matrix
     uint16_t *cy_s = nullptr, *cx_s = nullptr, *bcat_s = nullptr, *acat_s = nullptr;
     uint16_t *rho_s = nullptr, *t0t_s = nullptr, *p_s = nullptr, *t12t_s = nullptr;
@@ -50,8 +52,16 @@ void poisson_plan_destroy(PoissonPlan& pl);
 void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
                    cudaStream_t s);
 
-// ---- FP32 SIMT GEMM "TN": C[m][n] = sum_k A[m*lda+k] * B[n*ldb+k] (optionally * S[m][n]).
-// Rows m >= split go to C2 (row m - split) so one launch can fill two outputs.
+// ---- FP32 SIMT GEMM "TN": C[m][n] = sum_k A[m*lda+k] * (B[n*ldb+k] - boff[n])
+// (optionally * S[m][n]). Rows m >= split go to C2 (row m - split) so one launch can fill
+// two outputs.
+//
+// DC split: a forward cosine contraction over data with a large mean accumulates long
+// partial sums that cancel, and FP32 sequential accumulation then loses the small
+// low-frequency coefficients the 1/(u^2+v^2) divide amplifies. Subtracting each B row's
+// mean (boff) removes that component; since sum_k cos(pi j (k+1/2)/n) = 0 for j >= 1 only
+// output row 0 (the DC row, whose basis row is all ones) changes, and it is restored
+// exactly from the row sums.
 struct GemmArgs {
     const float* A;
     const float* B;
@@ -61,7 +71,18 @@ struct GemmArgs {
     int M, N, K, split;
     int64_t lda, ldb, ldc, lds;
     int64_t sA, sB, sC;  // per-batch strides (blockIdx.z)
+    const float* boff = nullptr;  // per-B-row offset, batch stride sBoff
+    int64_t sBoff = 0;
 };
+
+// Row statistics for the DC split: for each row r (of `rows`, length `cols` each, leading
+// dimension ld) and each segment of `seg` columns, mean and sum (accumulated in FP64).
+// Output index: segment * rows + r.
+void row_stats(const float* a, int rows, int cols, int64_t ld, int seg, float* mean, float* sum,
+               cudaStream_t s);
+// C[row 0][n] = vals[n] (* scale[n] when scale is given), for `batch` outputs.
+void set_row0(float* C, int64_t sC, int n, const float* vals, int64_t sv, const float* scale,
+              int batch, cudaStream_t s);
 void sgemm_tn(const GemmArgs& g, int batch, cudaStream_t s);
 
 // ---- tensor-core path (poisson_tc.cu)
