@@ -195,6 +195,18 @@ int spg_poisson_solve_batch_device(spg_poisson* h, int batch, const float* d_rho
 const char* spg_poisson_name(const spg_poisson* h);
 int spg_poisson_destroy(spg_poisson* h);
 
+/* Poisson solve that allocates nothing. No counterpart in the reference: it exists for
+ * callers that cannot call cudaMalloc (hosts that reserve all device memory up front in
+ * their own pool and forbid later driver allocations), which therefore cannot create a
+ * spg_poisson plan. Same plain-FP32 solve as a plan's, device arrays in and out, work
+ * enqueued on `stream`. Its bases and work buffers live in one static device array of
+ * 11 MB that every GPU loading this library holds until the process exits; nx and ny must
+ * be at most 512 (larger sizes return SPG_E_CAPACITY). All calls on a device share that
+ * array, so calls that overlap on the GPU race: serialise them. The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress); make it before any stream capture. */
+int spg_poisson_solve_static(int nx, int ny, float step_x, float step_y, const float* d_rho,
+                             float* d_phi, float* d_field_x, float* d_field_y, void* stream);
+
 /* ------------------------------------------------------------------ fillers (host)
  * initializeFillers (src/gp/filler.cpp:47-139): size and count from the view's movable
  * nodes, rows and fixed nodes; scatterFillers (src/gp/filler.cpp:33-45): mt19937 seeded

@@ -674,6 +674,9 @@ bool device_ok() {
 
 }  // namespace
 
+// Records the calling thread's last error for spg_last_error() and returns its status.
+int record_error(const std::exception& e) { return fail(e); }
+
 struct PoissonHandle {
     PoissonPlan plan;
     DevBuf<float> io;

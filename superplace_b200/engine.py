@@ -53,6 +53,8 @@ def lib():
         L.spg_poisson_solve_device.argtypes = [vp, vp, vp, vp, vp, vp]
         L.spg_poisson_solve_batch_device.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
         L.spg_poisson_destroy.argtypes = [vp]
+        L.spg_poisson_solve_static.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, vp, vp, vp,
+                                               vp, vp]
         L.spg_fillers_plan.argtypes = [C.POINTER(abi.DbView), C.c_float, C.POINTER(abi.FillerInfo)]
         L.spg_fillers_scatter.argtypes = [C.POINTER(abi.DbView), C.c_int32, C.c_float, C.c_float,
                                           C.c_uint64, fp, fp]
@@ -136,6 +138,15 @@ class PoissonBackend:
 
 def make_poisson_backend(nx, ny, step_x=1.0, step_y=1.0, precision=abi.POISSON_FP32):
     return PoissonBackend(nx, ny, step_x, step_y, precision)
+
+
+def poisson_solve_static(nx, ny, step_x, step_y, rho_ptr, phi_ptr, fx_ptr, fy_ptr, stream=0):
+    """spg_poisson_solve_static: the FP32 solve with no allocation at all (scratch in a
+    static device array; nx, ny <= 512). Arguments are raw device addresses; for callers
+    that cannot call cudaMalloc and so cannot build a PoissonBackend plan."""
+    check(lib().spg_poisson_solve_static(int(nx), int(ny), step_x, step_y, C.c_void_p(rho_ptr),
+                                         C.c_void_p(phi_ptr), C.c_void_p(fx_ptr),
+                                         C.c_void_p(fy_ptr), C.c_void_p(stream)))
 
 
 # ------------------------------------------------------------------ fillers
