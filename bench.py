@@ -289,6 +289,7 @@ def run_ours(args):
                        "fillers": int(db.num_fillers), "pins": int(db.num_pins),
                        "nets": int(db.num_nets), "bins": dim,
                        "poisson": args.precision, "step": "one full mGP stage run",
+                       "loop": "conditional CUDA graph" if ep.ctx.graph_loop() else "host-driven",
                        "iterations_per_step": iters, "final_hpwl": hpwl, "final_tau": tau,
                        "l2": "working set (~100 MB) is L2-resident between kernels; the "
                              "Poisson timing flushes L2 with a 256 MB write between solves",

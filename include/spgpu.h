@@ -271,6 +271,9 @@ int spg_metrics_d2h(const spg_ctx* ctx, spg_iter_metrics* rows, int cap, int* n_
 int64_t spg_ctx_launch_count(const spg_ctx* ctx);
 /* The cudaStream_t every call on this context enqueues on (for caller-side CUDA events). */
 void* spg_ctx_stream(const spg_ctx* ctx);
+/* 1 when the last stage run executed its iteration loop as one conditional CUDA graph,
+ * 0 when it ran the host-driven loop (SPG_HOST_LOOP set, or conditional nodes refused). */
+int spg_ctx_graph_loop(const spg_ctx* ctx);
 
 #ifdef __cplusplus
 }

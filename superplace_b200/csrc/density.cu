@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(RED_THREADS) rho_overflow_kernel(DevPtrs p, in
         }
     }
     over = block_sum(over);
-    if (threadIdx.x == 0) p.partials[SLOT_OVERFLOW * RED_BLOCKS + blockIdx.x] = over;
+    if (threadIdx.x == 0) p.partials[SLOT_OVERFLOW * RED_CAP + blockIdx.x] = over;
 }
 
 // force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it.

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -58,9 +59,12 @@ struct DevBuf {
         p = nullptr;
         n = 0;
     }
+    // (Re)allocate for `count` elements; an existing buffer of the same size is kept, so
+    // repeated stage runs reuse their device memory and keep their addresses.
     void alloc(size_t count) {
-        reset();
         if (count == 0) count = 1;
+        if (p && n == count) return;
+        reset();
         SPG_CUDA(cudaMalloc(&p, count * sizeof(T)));
         n = count;
     }
@@ -85,6 +89,8 @@ float overlap_area(float alx, float aly, float ahx, float ahy, float blx, float 
 }  // namespace
 
 // ---------------------------------------------------------------------------------------
+struct LoopGraph;
+
 struct Context {
     cudaStream_t stream = nullptr;
     spg_params prm{};
@@ -101,6 +107,7 @@ struct Context {
     DevBuf<uint8_t> kind;
     DevBuf<float> pox, poy, gpx, gpy;
     DevBuf<int> pin2node, pin2net, net_start, net_pins, node_start_d, node_pins, net_order;
+    WaClasses wa_classes{};
     // grid
     bool grid_ready = false;
     GridGeom geom{};
@@ -124,15 +131,22 @@ struct Context {
     int metrics_rows = 0;
     DevState* hst = nullptr;  // pinned host mirror
     float step_x_gamma = 1.f;
+    // the iteration loop as a conditional CUDA graph (engine.cu: build_loop_graph); the
+    // host-driven loop runs instead where the driver refuses conditional nodes
+    bool use_graph = true;
+    bool last_run_graph = false;
+    std::shared_ptr<LoopGraph> loop_graph;
 
     ~Context() {
+        loop_graph.reset();
         if (plan) poisson_plan_destroy(*plan);
         if (hst) cudaFreeHost(hst);
         if (stream) cudaStreamDestroy(stream);
     }
 
     DevPtrs ptrs() const {
-        DevPtrs p{};
+        DevPtrs p;
+        std::memset(&p, 0, sizeof(p));  // padding too: graphs are keyed on the bytes
         p.num_movable = num_movable;
         p.num_nodes = num_nodes;
         p.num_fillers = num_fillers;
@@ -154,6 +168,7 @@ struct Context {
         p.node_start = node_start_d.p;
         p.node_pins = node_pins.p;
         p.net_order = net_order.p;
+        p.wa = wa_classes;
         p.gpx = gpx.p;
         p.gpy = gpy.p;
         p.geom = geom;
@@ -359,7 +374,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         c.plan = std::make_unique<PoissonPlan>();
         poisson_plan_create(*c.plan, dim, dim, g.step_x, g.step_y, c.prm.poisson_precision, 1);
     }
-    c.partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_BLOCKS);
+    c.partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_CAP);
     c.partials.zero(st);
     SPG_CUDA(cudaStreamSynchronize(st));
     c.grid_ready = true;
@@ -499,9 +514,9 @@ __global__ void set_hpwl_ref_kernel(DevPtrs p, double ref) { p.st->hpwl_ref = re
 // Final metrics at the delivered positions: overflow and HPWL (eplace.cpp:484-488).
 __global__ void final_metrics_kernel(DevPtrs p, double* out) {
     double over = 0.0, hp = 0.0;
-    for (int j = threadIdx.x; j < RED_BLOCKS; j += blockDim.x) {
-        over += p.partials[SLOT_OVERFLOW * RED_BLOCKS + j];
-        hp += p.partials[SLOT_HPWL * RED_BLOCKS + j];
+    for (int j = threadIdx.x; j < RED_CAP; j += blockDim.x) {
+        over += p.partials[SLOT_OVERFLOW * RED_CAP + j];
+        hp += p.partials[SLOT_HPWL * RED_CAP + j];
     }
     __shared__ double so[256], sh[256];
     so[threadIdx.x] = over;
@@ -534,6 +549,171 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
     SPG_CUDA(cudaStreamSynchronize(s));
     *overflow = static_cast<float>(out[0]);
     *hpwl = out[1];
+}
+
+// One iteration of the loop body (nesterov.cpp:87-121 then eplace.cpp:362-473), ending
+// with the next iteration's first evaluation and its redo test.
+void enqueue_iteration(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
+    cudaStream_t s = c.stream;
+    launch_ctl_step(p, s);
+    launch_nesterov_update(p, s);
+    launch_ctl_iter_end(p, s);
+    launch_snapshot_copy(p, s);
+    evaluate(c, p, R_U, R_G, 1);
+    launch_reduce_diff(p, s);
+    launch_ctl_redo_check(p, s, use_cond, redo_h);
+}
+
+// One redoIfOvershot re-evaluation (nesterov.cpp:158-166) and the next redo test.
+void enqueue_redo(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
+    cudaStream_t s = c.stream;
+    launch_redo_update(p, s);
+    evaluate(c, p, R_U, R_G, 1);
+    launch_reduce_diff(p, s);
+    launch_ctl_redo_check(p, s, use_cond, redo_h);
+}
+
+// Host-driven loop: one 16-byte state read per iteration (and per re-evaluation).
+void host_loop(Context& c, const DevPtrs& p, int max_iter) {
+    read_state(c);
+    // the device sets `done` by max_iter; this bound guards the host loop itself
+    const int64_t eval_bound = static_cast<int64_t>(max_iter + 2) * std::max(c.prm.max_backtrack, 1);
+    int iter = 0;
+    while (!c.hst->done) {
+        if (iter > max_iter || c.hst->evals > eval_bound)
+            throw Error(SPG_E_STATE, "GP loop exceeded its iteration bound");
+        if (c.hst->redo) {
+            enqueue_redo(c, p, 0, 0);
+        } else {
+            enqueue_iteration(c, p, 0, 0);
+            ++iter;
+        }
+        read_state(c);
+    }
+}
+
+}  // namespace
+
+struct LoopGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    DevPtrs sig{};
+    const void* plan = nullptr;
+    int64_t body_kernels = 0, redo_kernels = 0;
+    ~LoopGraph() { reset(); }
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+};
+
+namespace {
+
+// The whole iteration loop as one CUDA graph:
+//   WHILE (!done) {                      loop_h, set by ctl_loop_cond at the end of a body
+//     step; update; iteration end; snapshot; evaluate; norms; redo test -> redo_h
+//     WHILE (redo) { redo update; evaluate; norms; redo test -> redo_h }
+//     ctl_loop_cond -> loop_h
+//   }
+// Built once per context and stage layout, relaunched on later runs with the same buffers.
+bool build_loop_graph(Context& c, const DevPtrs& p) {
+    LoopGraph& lg = *c.loop_graph;
+    lg.reset();
+    cudaStream_t s = c.stream;
+    const int64_t launches0 = g_launches;
+    auto ok = [](cudaError_t e) { return e == cudaSuccess; };
+    cudaGraph_t g = nullptr;
+    if (!ok(cudaGraphCreate(&g, 0))) return false;
+    lg.graph = g;
+    cudaGraphConditionalHandle loop_h, redo_h;
+    if (!ok(cudaGraphConditionalHandleCreate(&loop_h, g, 1, cudaGraphCondAssignDefault))) return false;
+    cudaGraphNodeParams wp{};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = loop_h;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    if (!ok(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp))) return false;
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    if (!ok(cudaGraphConditionalHandleCreate(&redo_h, body, 0, cudaGraphCondAssignDefault))) return false;
+    // outer body: capture the iteration, insert the inner WHILE, then the loop condition
+    if (!ok(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
+        return false;
+    cudaGraph_t rbody = nullptr;
+    bool fine = true;
+    try {
+        const int64_t k0 = g_launches;
+        enqueue_iteration(c, p, 1, redo_h);
+        cudaStreamCaptureStatus cs;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t ndeps = 0;
+        fine = ok(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps));
+        cudaGraphNodeParams rp{};
+        rp.type = cudaGraphNodeTypeConditional;
+        rp.conditional.handle = redo_h;
+        rp.conditional.type = cudaGraphCondTypeWhile;
+        rp.conditional.size = 1;
+        cudaGraphNode_t rnode;
+        fine = fine && ok(cudaGraphAddNode(&rnode, body, deps, ndeps, &rp));
+        fine = fine && ok(cudaStreamUpdateCaptureDependencies(s, &rnode, 1, cudaStreamSetCaptureDependencies));
+        if (fine) {
+            rbody = rp.conditional.phGraph_out[0];
+            launch_ctl_loop_cond(p, loop_h, s);
+        }
+        lg.body_kernels = g_launches - k0;
+    } catch (const Error&) {
+        fine = false;
+    }
+    cudaGraph_t out = nullptr;
+    const bool ended = ok(cudaStreamEndCapture(s, &out));
+    if (!fine || !ended || !rbody) {
+        cudaGetLastError();
+        g_launches = launches0;
+        return false;
+    }
+    // inner body: one re-evaluation
+    if (!ok(cudaStreamBeginCaptureToGraph(s, rbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
+        return false;
+    try {
+        const int64_t k0 = g_launches;
+        enqueue_redo(c, p, 1, redo_h);
+        lg.redo_kernels = g_launches - k0;
+    } catch (const Error&) {
+        fine = false;
+    }
+    const bool ended2 = ok(cudaStreamEndCapture(s, &out));
+    g_launches = launches0;  // executions are counted after each launch
+    if (!fine || !ended2) {
+        cudaGetLastError();
+        return false;
+    }
+    if (!ok(cudaGraphInstantiate(&lg.exec, g, 0))) {
+        cudaGetLastError();
+        return false;
+    }
+    lg.sig = p;
+    lg.plan = c.plan.get();
+    return true;
+}
+
+bool graph_loop(Context& c, const DevPtrs& p) {
+    if (!c.loop_graph) c.loop_graph = std::make_shared<LoopGraph>();
+    LoopGraph& lg = *c.loop_graph;
+    const bool same = lg.exec && lg.plan == c.plan.get() && std::memcmp(&lg.sig, &p, sizeof(DevPtrs)) == 0;
+    if (!same && !build_loop_graph(c, p)) {
+        lg.reset();
+        c.use_graph = false;  // this device/driver refused the conditional graph: host loop
+        return false;
+    }
+    SPG_CUDA(cudaGraphLaunch(lg.exec, c.stream));
+    read_state(c);
+    // counted evaluations = iteration 0's + one per later iteration + one per re-evaluation
+    const int64_t iters = c.hst->iter;
+    const int64_t redos = std::max<int64_t>(0, c.hst->evals - iters);
+    g_launches += iters * lg.body_kernels + redos * lg.redo_kernels;
+    return true;
 }
 
 // EPlace::run (eplace.cpp:223-526) for one stage, device-resident.
@@ -597,37 +777,14 @@ void stage_run(Context& c, int stage, spg_result* res) {
     launch_init_diff(p, s);
     launch_ctl_init_finish(p, s);
 
-    const bool bt = c.prm.gp_backtrack != 0;
-    int iter = 0;
-    // first evaluation of iteration 0
+    // first evaluation of iteration 0, its norms, and the redo test (a no-op at iteration 0)
     evaluate(c, p, R_U, R_G, 1);
     launch_reduce_diff(p, s);
-    read_state(c);
-    // host-side bound: the device sets `done` by max_iter; a bound on evaluations guards the
-    // host loop against a control-logic fault
-    const int64_t eval_bound = static_cast<int64_t>(max_iter + 2) * std::max(c.prm.max_backtrack, 1);
-    while (true) {
-        if (c.hst->done) break;
-        if (iter > max_iter || c.hst->evals > eval_bound)
-            throw Error(SPG_E_STATE, "GP loop exceeded its iteration bound");
-        if (c.hst->redo) {  // redoIfOvershot re-evaluation
-            launch_redo_update(p, s);
-            evaluate(c, p, R_U, R_G, 1);
-            launch_reduce_diff(p, s);
-            launch_ctl_redo_check(p, s);
-            read_state(c);
-            continue;
-        }
-        launch_ctl_step(p, (bt && iter > 0) ? 0 : 1, s);
-        launch_nesterov_update(p, s);
-        launch_ctl_iter_end(p, s);
-        launch_snapshot_copy(p, s);
-        ++iter;
-        // first evaluation of the next iteration (harmless if the loop just finished)
-        evaluate(c, p, R_U, R_G, 1);
-        launch_reduce_diff(p, s);
-        if (bt) launch_ctl_redo_check(p, s);
-        read_state(c);
+    launch_ctl_redo_check(p, s);
+    c.last_run_graph = false;
+    if (max_iter > 0) {
+        c.last_run_graph = c.use_graph && graph_loop(c, p);
+        if (!c.last_run_graph) host_loop(c, p, max_iter);
     }
     SPG_CUDA(cudaEventRecord(e1, s));
     launch_deliver(p, s);
@@ -890,6 +1047,9 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     auto h = std::make_unique<spg_ctx>();
     Context& c = h->c;
     c.prm = *prm;
+    // SPG_HOST_LOOP=1 selects the host-driven iteration loop (one state read per iteration)
+    // instead of the conditional CUDA graph; both run the same kernels in the same order.
+    c.use_graph = std::getenv("SPG_HOST_LOOP") == nullptr;
     SPG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.num_movable = v->num_movable;
     c.num_nodes = v->num_nodes;
@@ -940,13 +1100,33 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     c.net_pins.upload(v->flat_net2pin, c.num_pins, s);
     c.node_start_d.upload(v->node2pin_start, T + 1, s);
     c.node_pins.upload(v->flat_node2pin, c.num_pins, s);
-    // nets in descending degree (stable): warp-uniform pin loops in the WA kernel
+    // nets in ascending degree (stable), cut into degree classes: a net of degree d is
+    // owned by a lane group of the next power of two >= d (2..32 lanes), nets above 32
+    // pins by a whole warp that loops over its pins (wirelength.cu)
     std::vector<int> order(c.num_nets);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-        return v->net2pin_start[a + 1] - v->net2pin_start[a] > v->net2pin_start[b + 1] - v->net2pin_start[b];
-    });
+    auto deg = [&](int k) { return v->net2pin_start[k + 1] - v->net2pin_start[k]; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return deg(a) < deg(b); });
     c.net_order.upload(order, s);
+    {
+        spg::WaClasses& wc = c.wa_classes;
+        wc = spg::WaClasses{};
+        const int limits[6] = {2, 4, 8, 16, 32, 1 << 30};
+        const int groups[6] = {2, 4, 8, 16, 32, 0};
+        int t = 0, warps = 0;
+        for (int cl = 0; cl < 6; ++cl) {
+            const int begin = t;
+            while (t < c.num_nets && deg(order[t]) <= limits[cl]) ++t;
+            if (t == begin) continue;
+            const int i = wc.n++;
+            wc.group[i] = groups[cl];
+            wc.net_begin[i] = begin;
+            wc.net_end[i] = t;
+            wc.warp_begin[i] = warps;
+            warps += groups[cl] ? spg::ceil_div(t - begin, 32 / groups[cl]) : (t - begin);
+        }
+        wc.warp_begin[wc.n] = warps;
+    }
     c.gpx.alloc(std::max(c.num_pins, 1));
     c.gpy.alloc(std::max(c.num_pins, 1));
     c.gpx.zero(s);
@@ -1143,7 +1323,7 @@ int spg_wa_wirelength(spg_ctx* ctx, float gamma, int ignore, double* wl, float* 
     spg::DevPtrs p = c.ptrs();
     p.ignore_net_degree = ignore;
     if (!c.partials.p) {
-        c.partials.alloc(static_cast<size_t>(spg::RED_SLOTS) * spg::RED_BLOCKS);
+        c.partials.alloc(static_cast<size_t>(spg::RED_SLOTS) * spg::RED_CAP);
         c.partials.zero(c.stream);
         p.partials = c.partials.p;
     }
@@ -1168,7 +1348,7 @@ int spg_hpwl(spg_ctx* ctx, double* hpwl) {
     Context& c = ctx->c;
     spg::DevPtrs p = c.ptrs();
     if (!c.partials.p) {
-        c.partials.alloc(static_cast<size_t>(spg::RED_SLOTS) * spg::RED_BLOCKS);
+        c.partials.alloc(static_cast<size_t>(spg::RED_SLOTS) * spg::RED_CAP);
         c.partials.zero(c.stream);
         p.partials = c.partials.p;
     }
@@ -1206,5 +1386,7 @@ int64_t spg_ctx_launch_count(const spg_ctx* ctx) {
 }
 
 void* spg_ctx_stream(const spg_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c.stream) : nullptr; }
+
+int spg_ctx_graph_loop(const spg_ctx* ctx) { return ctx && ctx->c.last_run_graph ? 1 : 0; }
 
 }  // extern "C"

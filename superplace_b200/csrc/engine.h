@@ -8,7 +8,7 @@
 //                 xi_x, xi_y (f32, M^2 each)
 //   optimizer     a pool of 12 vectors of 2*nOpt f32 whose roles (u, v, uPrev, ...) rotate
 //                 through a role table in DevState, so every launch has fixed arguments
-//   reductions    RED_SLOTS x RED_BLOCKS FP64 partial sums (fixed grid => deterministic)
+//   reductions    RED_SLOTS x RED_CAP FP64 partial sums (fixed grid => deterministic)
 //   DevState      every scalar of the Nesterov / lambda / gamma / stagnation logic
 #pragma once
 
@@ -19,7 +19,10 @@
 
 namespace spg {
 
-constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs; every reducing kernel uses this grid
+constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs: the grid of the vector kernels
+// Partial sums per slot: a reducing kernel writes one per block (at most RED_CAP blocks);
+// entries past its grid stay zero, and the control kernels always sum all RED_CAP.
+constexpr int RED_CAP = 1024;
 constexpr int RED_THREADS = 256;
 
 enum RedSlot : int {
@@ -87,6 +90,16 @@ struct DevState {
     unsigned long long t0_ns;
 };
 
+// Degree classes of the WA kernel over the degree-sorted net order: class i owns nets
+// net_order[net_begin[i] .. net_end[i]) with `group[i]` lanes per net (0: one looping warp
+// per net) and warps [warp_begin[i], warp_begin[i+1]).
+struct WaClasses {
+    int n;
+    int group[8];
+    int net_begin[8], net_end[8];
+    int warp_begin[9];
+};
+
 // Everything a kernel needs to address the device data, passed by value.
 struct DevPtrs {
     int num_movable, num_nodes, num_fillers, total, num_pins, num_nets;
@@ -97,7 +110,8 @@ struct DevPtrs {
     const int *pin2node, *pin2net;
     const int *net_start, *net_pins;
     const int *node_start, *node_pins;
-    const int* net_order;  // nets sorted by degree (warp-uniform pin loops)
+    const int* net_order;  // nets sorted by degree (ascending)
+    WaClasses wa;
     // per-pin WA gradient contributions (x, y)
     float *gpx, *gpy;
     // grid
@@ -120,7 +134,7 @@ struct DevPtrs {
     int n_dens_small, n_dens_large;
     const int *opt_small, *opt_large;  // opt positions k
     int n_opt_small, n_opt_large;
-    double* partials;      // RED_SLOTS * RED_BLOCKS
+    double* partials;      // RED_SLOTS * RED_CAP
     DevState* st;
     spg_iter_metrics* metrics;
     int ignore_net_degree;
@@ -153,7 +167,10 @@ void launch_scatter(const DevPtrs& p, int role, cudaStream_t s);
 void launch_assemble(const DevPtrs& p, int grad_role, cudaStream_t s);
 void launch_ctl_eval_done(const DevPtrs& p, int count_eval, cudaStream_t s);
 void launch_reduce_diff(const DevPtrs& p, cudaStream_t s);
-void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
+                           cudaGraphConditionalHandle redo_cond = 0);
+void launch_ctl_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s);
+void launch_ctl_step(const DevPtrs& p, cudaStream_t s);
 void launch_redo_update(const DevPtrs& p, cudaStream_t s);
 void launch_nesterov_update(const DevPtrs& p, cudaStream_t s);
 void launch_ctl_iter_end(const DevPtrs& p, cudaStream_t s);

@@ -46,7 +46,7 @@ __device__ __forceinline__ double block_sum(double v) {
 // Sum of one slot's RED_BLOCKS partials in a fixed order (valid on thread 0).
 __device__ __forceinline__ double finalize(const DevPtrs& p, int slot) {
     double v = 0.0;
-    for (int j = threadIdx.x; j < RED_BLOCKS; j += blockDim.x) v += p.partials[slot * RED_BLOCKS + j];
+    for (int j = threadIdx.x; j < RED_CAP; j += blockDim.x) v += p.partials[slot * RED_CAP + j];
     return block_sum(v);
 }
 
@@ -129,8 +129,8 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int gr
     acc_wl = block_sum(acc_wl);
     acc_den = block_sum(acc_den);
     if (threadIdx.x == 0) {
-        p.partials[SLOT_SUM_WL * RED_BLOCKS + blockIdx.x] = acc_wl;
-        p.partials[SLOT_SUM_DEN * RED_BLOCKS + blockIdx.x] = acc_den;
+        p.partials[SLOT_SUM_WL * RED_CAP + blockIdx.x] = acc_wl;
+        p.partials[SLOT_SUM_DEN * RED_CAP + blockIdx.x] = acc_den;
     }
 }
 
@@ -157,10 +157,10 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_diff_kernel(DevPtrs p) {
     sy = block_sum(sy);
     gn = block_sum(gn);
     if (threadIdx.x == 0) {
-        p.partials[SLOT_DX * RED_BLOCKS + blockIdx.x] = dx;
-        p.partials[SLOT_DG * RED_BLOCKS + blockIdx.x] = dg;
-        p.partials[SLOT_SY * RED_BLOCKS + blockIdx.x] = sy;
-        p.partials[SLOT_GN * RED_BLOCKS + blockIdx.x] = gn;
+        p.partials[SLOT_DX * RED_CAP + blockIdx.x] = dx;
+        p.partials[SLOT_DG * RED_CAP + blockIdx.x] = dg;
+        p.partials[SLOT_SY * RED_CAP + blockIdx.x] = sy;
+        p.partials[SLOT_GN * RED_CAP + blockIdx.x] = gn;
     }
 }
 
@@ -185,6 +185,7 @@ __global__ void redo_update_kernel(DevPtrs p) {
 
 // vNew = u - alpha*g ; uNew = vNew + momentum*(vNew - v) ; clamp both (nesterov.cpp:97-107)
 __global__ void nesterov_update_kernel(DevPtrs p) {
+    if (p.st->done) return;
     const float* u = role_ptr(p, R_U);
     const float* v = role_ptr(p, R_V);
     const float* g = role_ptr(p, R_G);
@@ -250,8 +251,8 @@ __global__ void __launch_bounds__(RED_THREADS) init_norms_kernel(DevPtrs p) {
     pn = block_sum(pn);
     gn = block_sum(gn);
     if (threadIdx.x == 0) {
-        p.partials[SLOT_PN * RED_BLOCKS + blockIdx.x] = pn;
-        p.partials[SLOT_GN * RED_BLOCKS + blockIdx.x] = gn;
+        p.partials[SLOT_PN * RED_CAP + blockIdx.x] = pn;
+        p.partials[SLOT_GN * RED_CAP + blockIdx.x] = gn;
     }
 }
 
@@ -283,8 +284,8 @@ __global__ void __launch_bounds__(RED_THREADS) init_diff_kernel(DevPtrs p) {
     dx = block_sum(dx);
     dg = block_sum(dg);
     if (threadIdx.x == 0) {
-        p.partials[SLOT_DX * RED_BLOCKS + blockIdx.x] = dx;
-        p.partials[SLOT_DG * RED_BLOCKS + blockIdx.x] = dg;
+        p.partials[SLOT_DX * RED_CAP + blockIdx.x] = dx;
+        p.partials[SLOT_DG * RED_CAP + blockIdx.x] = dg;
     }
 }
 
@@ -355,9 +356,13 @@ __global__ void ctl_init_finish_kernel(DevPtrs p) {
     st->alpha0 = (isfinite(step) && step > 0.0) ? static_cast<float>(step) : 1.f;
 }
 
-// redoIfOvershot's test (nesterov.cpp:148-157): redo when 1/L at the new point is at most
-// 0.95 of the step just taken, at most max_backtrack-1 times per step.
-__global__ void ctl_redo_check_kernel(DevPtrs p) {
+// After every counted evaluation: finalize |u-uPrev|, |g-gPrevTmp|, their dot and |g|^2,
+// then redoIfOvershot's test (nesterov.cpp:148-157): redo when 1/L at the new point is at
+// most 0.95 of the step just taken, at most max_backtrack-1 times per step, and only when
+// backtracking is on and this is not the first step (nesterov.cpp:84).
+// In graph mode it also drives the conditional nodes: redo_cond <- redo, and, when given,
+// loop_cond <- !done && !redo (the iteration loop re-enters once no re-evaluation is due).
+__global__ void ctl_redo_check_kernel(DevPtrs p, int use_cond, cudaGraphConditionalHandle redo_cond) {
     const double dx2 = finalize(p, SLOT_DX);
     const double dg2 = finalize(p, SLOT_DG);
     const double sy = finalize(p, SLOT_SY);
@@ -369,33 +374,34 @@ __global__ void ctl_redo_check_kernel(DevPtrs p) {
     st->sy = sy;
     st->gn = gn2;
     st->redo = 0;
-    if (st->error || st->done || st->tries >= p.max_backtrack) return;
-    const double dx = st->dx, dg = st->dg;
-    if (!(dx > 0.0) || !(dg > 0.0) || !isfinite(dg)) return;
-    const double lip = dx / dg;
-    if (lip > 0.95 * static_cast<double>(st->alpha)) return;
-    st->alpha = static_cast<float>(lip);
-    st->redo = 1;
-    st->tries += 1;
+    const bool eligible = p.backtrack && st->iter > 0 && !st->error && !st->done &&
+                          st->tries < p.max_backtrack;
+    if (eligible) {
+        const double dx = st->dx, dg = st->dg;
+        if (dx > 0.0 && dg > 0.0 && isfinite(dg)) {
+            const double lip = dx / dg;
+            if (!(lip > 0.95 * static_cast<double>(st->alpha))) {
+                st->alpha = static_cast<float>(lip);
+                st->redo = 1;
+                st->tries += 1;
+            }
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(redo_cond, st->redo ? 1u : 0u);
 }
 
-// Step size and momentum of this step (nesterov.cpp:87-96, estimateStep :221-240).
-__global__ void ctl_step_kernel(DevPtrs p, int reduce_fresh) {
-    double dx2 = 0.0, dg2 = 0.0, sy = 0.0, gn2 = 0.0;
-    if (reduce_fresh) {
-        dx2 = finalize(p, SLOT_DX);
-        dg2 = finalize(p, SLOT_DG);
-        sy = finalize(p, SLOT_SY);
-        gn2 = finalize(p, SLOT_GN);
-    }
+// Graph mode: the iteration loop continues while the stage is not done.
+__global__ void ctl_loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond) {
+    const DevState* st = p.st;
+    cudaGraphSetConditional(loop_cond, (st->done || st->error) ? 0u : 1u);
+}
+
+// Step size and momentum of this step (nesterov.cpp:87-96, estimateStep :221-240). The
+// norms were finalized by the redo check that followed the last evaluation.
+__global__ void ctl_step_kernel(DevPtrs p) {
     if (threadIdx.x != 0) return;
     DevState* st = p.st;
-    if (reduce_fresh) {
-        st->dx = sqrt(dx2);
-        st->dg = sqrt(dg2);
-        st->sy = sy;
-        st->gn = gn2;
-    }
+    if (st->done) return;
     st->grad_norm = static_cast<float>(sqrt(st->gn));
     if (st->iter == 0) {
         st->alpha = st->alpha0;
@@ -430,6 +436,7 @@ __global__ void ctl_step_kernel(DevPtrs p, int reduce_fresh) {
 __global__ void ctl_iter_end_kernel(DevPtrs p) {
     if (threadIdx.x != 0) return;
     DevState* st = p.st;
+    if (st->done) return;
     int* r = st->role;
     {   // uPrev <- u <- uNew <- (old uPrev); v <- vNew, vPrev <- v, vNew <- (old vPrev);
         // gPrevTmp <- g (g's buffer is rewritten by the next evaluation)
@@ -600,14 +607,18 @@ void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
 void launch_reduce_diff(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(reduce_diff_kernel, RED_BLOCKS, RED_THREADS, p);
 }
-void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(ctl_redo_check_kernel, 1, RED_THREADS, p);
+void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s, int use_cond,
+                           cudaGraphConditionalHandle redo_cond) {
+    LAUNCH(ctl_redo_check_kernel, 1, RED_THREADS, p, use_cond, redo_cond);
+}
+void launch_ctl_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
+    LAUNCH(ctl_loop_cond_kernel, 1, 1, p, loop_cond);
 }
 void launch_redo_update(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(redo_update_kernel, vec_blocks(p), RED_THREADS, p);
 }
-void launch_ctl_step(const DevPtrs& p, int reduce_fresh, cudaStream_t s) {
-    LAUNCH(ctl_step_kernel, 1, RED_THREADS, p, reduce_fresh);
+void launch_ctl_step(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(ctl_step_kernel, 1, 32, p);
 }
 void launch_nesterov_update(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(nesterov_update_kernel, vec_blocks(p), RED_THREADS, p);

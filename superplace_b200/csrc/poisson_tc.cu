@@ -1,18 +1,519 @@
-// Split-BF16 tensor-core (tcgen05) Poisson path. Placeholder until the kernel lands:
-// tc_supported() reports false, so SPG_POISSON_BF16X3 plans are refused with
-// SPG_E_INVALID rather than silently running another path.
+// Split-BF16 tensor-core Poisson path for sm_100a (tcgen05 + TMA + TMEM).
+//
+// Every contraction of poisson.h's chain, C[m][n] = sum_k A[m][k] B[n][k], runs as a
+// split-BF16 product: each FP32 operand x is stored as two BF16 planes hi = bf16(x),
+// lo = bf16(x - hi), and C = A_hi.B_hi + A_hi.B_lo + A_lo.B_hi accumulated in FP32 in
+// tensor memory (the lo.lo term, ~2^-16 relative, is dropped). The three products are one
+// accumulation over K' = 3K: the producer walks (hi,hi), (hi,lo), (lo,hi) K slabs.
+//
+// Kernel (one 128 x BN output tile per CTA, 128 threads):
+//   warp 0 lane 0   TMA producer: 128x64 A and BNx64 B bf16 tiles (128-byte swizzle)
+//                   into a STAGES-deep shared-memory ring (full/empty mbarriers)
+//   warp 1 lane 0   MMA issuer: 4 x tcgen05.mma.kind::f16 (M=128, N=BN, K=16) per slab,
+//                   tcgen05.commit frees the slab, a final commit publishes the accumulator
+//   warps 0-3       epilogue: tcgen05.ld of the TMEM accumulator (one TMEM lane per
+//                   output row), optional spectral scale, DC-row override, and either an
+//                   FP32 store or a split store of the next contraction's BF16 hi/lo planes
+// Every mbarrier wait is bounded (2 s of %globaltimer); on timeout the kernel records
+// SPG_E_CUDA in the plan's error word, stops issuing, frees its TMEM and returns.
+//
+// DC split (poisson.h): the forward contractions subtract each B row's mean before the
+// split (prep kernels) and restore the DC row exactly in the epilogue.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "common.cuh"
 #include "poisson.h"
 
 namespace spg {
 
-bool tc_supported(int, int) { return false; }
-void tc_plan_create(PoissonPlan&) {
-    throw Error(SPG_E_INVALID, "Poisson: split-BF16 path unavailable");
+namespace {
+
+constexpr int TC_BM = 128;
+constexpr int TC_BK = 64;  // bf16 elements per K slab = one 128-byte swizzle row
+constexpr int TC_THREADS = 128;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // bounded mbarrier waits: 2 s
+
+enum TcMode : int { TC_F32 = 0, TC_SPLIT = 1 };
+
+struct TcArgs {
+    int M, N, K;            // tile-multiple problem dims (K per split pass)
+    int a_row0, a_lo;       // A: first row, rows between hi and lo planes
+    int b_row0, b_lo;       // B: first row, rows between hi and lo planes
+    int b_col_z;            // B column offset per blockIdx.z (batched over grids)
+    int mode;               // TcMode
+    float* out;             // F32: rows < split -> out, else out2 ; SPLIT: hi plane
+    float* out2;
+    int split;
+    int64_t ldc;            // output row pitch (elements)
+    int64_t out_z;          // output offset per blockIdx.z (elements)
+    uint16_t* planes;       // SPLIT: hi plane base (lo plane at + plane_stride)
+    int64_t plane_stride;
+    int64_t plane_z;        // SPLIT: offset per blockIdx.z (elements)
+    const float* scale;     // optional S[m][n] (ld = N of one grid), multiplies the result
+    int64_t lds;
+    const float* row0;      // optional: output row 0 := row0[z*row0_z + n] (* scale[n])
+    int64_t row0_z;
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-void tc_plan_destroy(PoissonPlan&) {}
-void tc_solve(PoissonPlan&, int, const float*, float*, float*, float*, cudaStream_t) {
-    throw Error(SPG_E_INVALID, "Poisson: split-BF16 path unavailable");
+
+__device__ __forceinline__ unsigned long long gtime() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the phase with the given parity to complete; false after kWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = gtime();
+    while (!mbar_try(bar, parity))
+        if (gtime() - t0 > kWaitNs) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int c0, int c1,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(bar)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((addr & 0x3FFFFu) >> 4);  // start address
+    d |= static_cast<uint64_t>(1) << 16;                  // leading byte offset (unused here)
+    d |= static_cast<uint64_t>(1024 >> 4) << 32;          // stride byte offset
+    d |= static_cast<uint64_t>(1) << 46;                  // descriptor version (sm_100)
+    d |= static_cast<uint64_t>(2) << 61;                  // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor of tcgen05.mma.kind::f16: BF16 A and B (K-major), FP32 D.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+    return (1u << 4)                              // D format: F32
+           | (1u << 7)                            // A format: BF16
+           | (1u << 10)                           // B format: BF16
+           | (static_cast<uint32_t>(n >> 3) << 17)  // N / 8
+           | (static_cast<uint32_t>(m >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+          "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+          "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+}
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const TcArgs g) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;
+    constexpr uint32_t B_BYTES = BN * TC_BK * 2;
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = base;
+    uint8_t* sB = base + STAGES * A_BYTES;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + STAGES * B_BYTES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
+    __shared__ int s_fail;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * TC_BM, z = blockIdx.z;
+    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES), accb = smem_u32(bars + 2 * STAGES);
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int i = 0; i < STAGES; ++i) {
+            mbar_init(full0 + 8 * i, 1);
+            mbar_init(empty0 + 8 * i, 1);
+        }
+        mbar_init(accb, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {  // TMEM accumulator: BN fp32 columns x 128 lanes
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(static_cast<uint32_t>(BN)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    const int kpp = g.K / TC_BK;  // slabs per split pass
+    const int nk = 3 * kpp;
+    if (warp == 0 && lane == 0) {
+        // producer: passes (A_hi,B_hi), (A_hi,B_lo), (A_lo,B_hi)
+        for (int s = 0; s < nk; ++s) {
+            const int st = s % STAGES;
+            const uint32_t ph = (s / STAGES) & 1;
+            if (!mbar_wait(empty0 + 8 * st, ph ^ 1)) {
+                s_fail = 1;
+                break;
+            }
+            const int pass = s / kpp, kk = (s % kpp) * TC_BK;
+            const int arow = g.a_row0 + m0 + (pass == 2 ? g.a_lo : 0);
+            const int brow = g.b_row0 + n0 + (pass == 1 ? g.b_lo : 0);
+            mbar_expect_tx(full0 + 8 * st, A_BYTES + B_BYTES);
+            tma_load_2d(smem_u32(sA + st * A_BYTES), &tmA, kk, arow, full0 + 8 * st);
+            tma_load_2d(smem_u32(sB + st * B_BYTES), &tmB, kk + z * g.b_col_z, brow, full0 + 8 * st);
+        }
+    } else if (warp == 1 && lane == 0) {
+        constexpr uint32_t idesc = idesc_bf16(TC_BM, BN);
+        bool ok = true;
+        for (int s = 0; s < nk; ++s) {
+            const int st = s % STAGES;
+            const uint32_t ph = (s / STAGES) & 1;
+            if (!mbar_wait(full0 + 8 * st, ph)) {
+                ok = false;
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t a0 = smem_u32(sA + st * A_BYTES), b0 = smem_u32(sB + st * B_BYTES);
+#pragma unroll
+            for (int k = 0; k < TC_BK / 16; ++k)  // 16 bf16 = 32 bytes per MMA along K
+                umma_bf16(tmem, sw128_desc(a0 + 32 * k), sw128_desc(b0 + 32 * k), idesc,
+                          (s > 0 || k > 0) ? 1u : 0u);
+            umma_commit(empty0 + 8 * st);
+        }
+        if (ok) umma_commit(accb);
+    }
+    __syncwarp();
+
+    // epilogue: TMEM lane = output row (warp w owns rows 32w .. 32w+31)
+    // warp-uniform decision: tcgen05.ld is .sync.aligned
+    const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0) ? 1 : 0) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!acc_ok) {
+        if (threadIdx.x == 0) atomicCAS(g.err, 0, SPG_E_CUDA);
+    } else {
+        const int m = m0 + 32 * warp + lane;
+        const bool row0 = (m == 0) && g.row0;
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 32) {
+            float v[32];
+            tmem_ld32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + c, v);
+            const int nb = n0 + c;
+            if (row0) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[i] = g.row0[z * g.row0_z + nb + i];
+            }
+            if (g.scale) {
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[i] *= g.scale[m * g.lds + nb + i];
+            }
+            if (g.mode == TC_F32) {
+                float* row = (m < g.split) ? g.out + z * g.out_z + m * g.ldc
+                                           : g.out2 + z * g.out_z + (m - g.split) * g.ldc;
+#pragma unroll
+                for (int i = 0; i < 32; i += 4)
+                    *reinterpret_cast<float4*>(row + nb + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+            } else {
+                uint16_t* hi = g.planes + z * g.plane_z + m * g.ldc + nb;
+                uint16_t* lo = hi + g.plane_stride;
+#pragma unroll
+                for (int i = 0; i < 32; i += 8) {
+                    uint16_t h[8], l[8];
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) split_bf16(v[i + j], h[j], l[j]);
+                    *reinterpret_cast<uint4*>(hi + i) = *reinterpret_cast<const uint4*>(h);
+                    *reinterpret_cast<uint4*>(lo + i) = *reinterpret_cast<const uint4*>(l);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(static_cast<uint32_t>(BN)));
+}
+
+// Row means (FP64) of `seg`-long row segments; writes the split BF16 planes of
+// (value - mean) when `center`, else of the value, and the exact segment sums.
+// One warp per (row, segment); outputs planes[row][col] with lo plane at + plane_stride.
+__global__ void prep_split_kernel(const float* src, int rows, int nseg, int64_t ld, int seg,
+                                  int center, uint16_t* planes, int64_t plane_stride, float* sums) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= rows * nseg) return;
+    const int r = w % rows, sg = w / rows;
+    const float* p = src + r * ld + static_cast<int64_t>(sg) * seg;
+    float mean = 0.f;
+    if (center) {
+        double v = 0.0;
+        for (int i = lane; i < seg; i += 32) v += static_cast<double>(p[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        mean = static_cast<float>(v / seg);
+        if (lane == 0 && sums) sums[w] = static_cast<float>(v);
+    }
+    uint16_t* hi = planes + r * ld + static_cast<int64_t>(sg) * seg;
+    uint16_t* lo = hi + plane_stride;
+    for (int i = lane; i < seg; i += 32) {
+        uint16_t h, l;
+        split_bf16(p[i] - mean, h, l);
+        hi[i] = h;
+        lo[i] = l;
+    }
+}
+
+// ------------------------------------------------------------------ host side
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        SPG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        SPG_REQUIRE(q == cudaDriverEntryPointSuccess && p, SPG_E_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 2-D bf16 tensor map over a [rows][cols] plane stack, box 64 (K) x box_rows.
+CUtensorMap make_map(const uint16_t* ptr, int64_t rows, int64_t cols, int box_rows) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+    cuuint64_t strides[1] = {static_cast<cuuint64_t>(cols * 2)};
+    cuuint32_t box[2] = {static_cast<cuuint32_t>(TC_BK), static_cast<cuuint32_t>(box_rows)};
+    cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t*>(ptr), dims,
+                                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    SPG_REQUIRE(r == CUDA_SUCCESS, SPG_E_CUDA, "cuTensorMapEncodeTiled failed");
+    return m;
+}
+
+constexpr int TC_BN = 64;
+constexpr int TC_STAGES = 6;
+constexpr size_t tc_smem_bytes() {
+    // 1024-byte alignment slack + stage ring + mbarriers + TMEM address slot
+    return 1024 + TC_STAGES * (TC_BM * TC_BK * 2 + TC_BN * TC_BK * 2) + (2 * TC_STAGES + 1) * 8 + 128;
+}
+
+struct TcState {
+    // tensor maps: bases (A operands) and data planes (B operands)
+    CUtensorMap cy, cx, bcat, acat;         // A: box rows 128
+    CUtensorMap rho_b, t0t_b, p_b, t12t_b;  // B: box rows TC_BN
+    float* t0t32 = nullptr;                 // FP32 T0t (G1 output, before its DC split)
+    float* sums = nullptr;                  // DC row sums (rho rows, T0t rows per grid)
+    int* err = nullptr;
+};
+
+void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int batch, cudaStream_t s) {
+    SPG_REQUIRE(g.M % TC_BM == 0 && g.N % TC_BN == 0 && g.K % TC_BK == 0, SPG_E_INVALID,
+                "tensor-core GEMM dims must be tile multiples");
+    dim3 grid(g.N / TC_BN, g.M / TC_BM, batch);
+    tc_gemm_kernel<TC_BN, TC_STAGES><<<grid, TC_THREADS, tc_smem_bytes(), s>>>(a, b, g);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+}
+
+void prep_split(const float* src, int rows, int cols, int64_t ld, int seg, int center, uint16_t* planes,
+                int64_t plane_stride, float* sums, cudaStream_t s) {
+    const int warps = rows * (cols / seg);
+    prep_split_kernel<<<ceil_div(warps, 8), 256, 0, s>>>(src, rows, cols / seg, ld, seg, center, planes,
+                                                         plane_stride, sums);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+}
+
+void split_host(const std::vector<float>& v, std::vector<uint16_t>& out) {
+    const size_t n = v.size();
+    out.resize(2 * n);
+    for (size_t i = 0; i < n; ++i) {
+        const __nv_bfloat16 h = __float2bfloat16_rn(v[i]);
+        const __nv_bfloat16 l = __float2bfloat16_rn(v[i] - __bfloat162float(h));
+        out[i] = __bfloat16_as_ushort(h);
+        out[n + i] = __bfloat16_as_ushort(l);
+    }
+}
+
+}  // namespace
+
+bool tc_supported(int nx, int ny) { return nx >= 128 && ny >= 128 && nx % 128 == 0 && ny % 128 == 0; }
+
+void tc_plan_create(PoissonPlan& pl) {
+    const int64_t X = pl.nx, Y = pl.ny, B = pl.batch_cap;
+    auto dl = [&](const float* d, size_t n) {
+        std::vector<float> h(n);
+        SPG_CUDA(cudaMemcpy(h.data(), d, n * 4, cudaMemcpyDeviceToHost));
+        return h;
+    };
+    auto up = [&](uint16_t*& dst, const std::vector<uint16_t>& h) {
+        SPG_CUDA(cudaMalloc(&dst, h.size() * 2));
+        pl.bytes += h.size() * 2;
+        SPG_CUDA(cudaMemcpy(dst, h.data(), h.size() * 2, cudaMemcpyHostToDevice));
+    };
+    std::vector<uint16_t> sp;
+    split_host(dl(pl.cy, Y * Y), sp);
+    up(pl.cy_s, sp);
+    split_host(dl(pl.cx, X * X), sp);
+    up(pl.cx_s, sp);
+    split_host(dl(pl.bcat, 2 * Y * Y), sp);
+    up(pl.bcat_s, sp);
+    split_host(dl(pl.acat, 2 * X * X), sp);
+    up(pl.acat_s, sp);
+    auto al16 = [&](uint16_t*& p, size_t n) {
+        SPG_CUDA(cudaMalloc(&p, n * 2));
+        pl.bytes += n * 2;
+    };
+    al16(pl.rho_s, 2 * B * X * Y);
+    al16(pl.t0t_s, 2 * B * X * Y);
+    al16(pl.p_s, 2 * B * X * Y);
+    al16(pl.t12t_s, 4 * B * X * Y);
+    auto* st = new TcState;
+    pl.tc = st;
+    SPG_CUDA(cudaMalloc(&st->t0t32, B * X * Y * 4));
+    SPG_CUDA(cudaMalloc(&st->sums, 2 * B * std::max(X, Y) * 4));
+    SPG_CUDA(cudaMalloc(&st->err, 4));
+    SPG_CUDA(cudaMemset(st->err, 0, 4));
+    pl.bytes += B * X * Y * 4 + 2 * B * std::max(X, Y) * 4 + 4;
+    st->cy = make_map(pl.cy_s, 2 * Y, Y, TC_BM);
+    st->cx = make_map(pl.cx_s, 2 * X, X, TC_BM);
+    st->bcat = make_map(pl.bcat_s, 4 * Y, Y, TC_BM);
+    st->acat = make_map(pl.acat_s, 4 * X, X, TC_BM);
+    st->rho_b = make_map(pl.rho_s, 2 * B * X, Y, TC_BN);
+    st->t0t_b = make_map(pl.t0t_s, 2 * Y, B * X, TC_BN);
+    st->p_b = make_map(pl.p_s, 2 * B * X, Y, TC_BN);
+    st->t12t_b = make_map(pl.t12t_s, 4 * Y, B * X, TC_BN);
+    static bool attr = false;
+    if (!attr) {
+        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(tc_smem_bytes())));
+        attr = true;
+    }
+}
+
+void tc_plan_destroy(PoissonPlan& pl) {
+    for (uint16_t* q : {pl.cy_s, pl.cx_s, pl.bcat_s, pl.acat_s, pl.rho_s, pl.t0t_s, pl.p_s, pl.t12t_s})
+        if (q) cudaFree(q);
+    pl.cy_s = pl.cx_s = pl.bcat_s = pl.acat_s = pl.rho_s = pl.t0t_s = pl.p_s = pl.t12t_s = nullptr;
+    if (auto* st = static_cast<TcState*>(pl.tc)) {
+        cudaFree(st->t0t32);
+        cudaFree(st->sums);
+        cudaFree(st->err);
+        delete st;
+        pl.tc = nullptr;
+    }
+}
+
+int tc_error(const PoissonPlan& pl) {
+    const auto* st = static_cast<const TcState*>(pl.tc);
+    if (!st) return 0;
+    int e = 0;
+    SPG_CUDA(cudaMemcpy(&e, st->err, 4, cudaMemcpyDeviceToHost));
+    return e;
+}
+
+void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
+              cudaStream_t s) {
+    auto* st = static_cast<TcState*>(pl.tc);
+    const int X = pl.nx, Y = pl.ny;
+    const int64_t Bc = pl.batch_cap, BX = static_cast<int64_t>(batch) * X, XY = static_cast<int64_t>(X) * Y;
+    const int64_t BXc = Bc * X;  // plane row/column extents are sized for the plan's capacity
+    float* sum_r = st->sums;
+    float* sum_t = st->sums + Bc * std::max(X, Y);
+    // rho rows minus their means -> split planes (B operand of G1), exact row sums
+    prep_split(rho, static_cast<int>(BX), Y, Y, Y, 1, pl.rho_s, BXc * Y, sum_r, s);
+    // G1: T0t (Y x BX) = Cy . rho'^T in FP32, DC row from the row sums
+    TcArgs g1{};
+    g1.M = Y; g1.N = static_cast<int>(BX); g1.K = Y;
+    g1.a_row0 = 0; g1.a_lo = Y; g1.b_row0 = 0; g1.b_lo = static_cast<int>(BXc); g1.b_col_z = 0;
+    g1.mode = TC_F32; g1.out = st->t0t32; g1.out2 = st->t0t32; g1.split = Y; g1.ldc = BXc; g1.out_z = 0;
+    g1.row0 = sum_r; g1.row0_z = 0; g1.err = st->err;
+    launch_tc(st->cy, st->rho_b, g1, 1, s);
+    // T0t rows minus their per-grid means -> split planes (B operand of G2), segment sums
+    prep_split(st->t0t32, Y, static_cast<int>(BX), BXc, X, 1, pl.t0t_s, static_cast<int64_t>(Y) * BXc, sum_t, s);
+    // G2: P_z (X x Y) = Cx . T0t'[:, z]^T, times the spectral scale, DC row from the sums
+    TcArgs g2{};
+    g2.M = X; g2.N = Y; g2.K = X;
+    g2.a_row0 = 0; g2.a_lo = X; g2.b_row0 = 0; g2.b_lo = Y; g2.b_col_z = X;
+    g2.mode = TC_SPLIT; g2.planes = pl.p_s; g2.plane_stride = BXc * Y; g2.plane_z = XY; g2.ldc = Y;
+    g2.scale = pl.scale; g2.lds = Y; g2.row0 = sum_t; g2.row0_z = Y; g2.err = st->err;
+    launch_tc(st->cx, st->t0t_b, g2, batch, s);
+    // G3: T12t (2Y x BX) = [Ay; Sy] . P^T  -> split planes
+    TcArgs g3{};
+    g3.M = 2 * Y; g3.N = static_cast<int>(BX); g3.K = Y;
+    g3.a_row0 = 0; g3.a_lo = 2 * Y; g3.b_row0 = 0; g3.b_lo = static_cast<int>(BXc); g3.b_col_z = 0;
+    g3.mode = TC_SPLIT; g3.planes = pl.t12t_s; g3.plane_stride = 2 * static_cast<int64_t>(Y) * BXc;
+    g3.plane_z = 0; g3.ldc = BXc; g3.err = st->err;
+    launch_tc(st->bcat, st->p_b, g3, 1, s);
+    // G4a: [phi; xi_x]_z = [Ax; Sx] . T1t[:, z]^T ; G4b: xi_y_z = Ax . T2t[:, z]^T
+    TcArgs g4{};
+    g4.M = 2 * X; g4.N = Y; g4.K = X;
+    g4.a_row0 = 0; g4.a_lo = 2 * X; g4.b_row0 = 0; g4.b_lo = 2 * Y; g4.b_col_z = X;
+    g4.mode = TC_F32; g4.out = phi; g4.out2 = ex; g4.split = X; g4.ldc = Y; g4.out_z = XY; g4.err = st->err;
+    launch_tc(st->acat, st->t12t_b, g4, batch, s);
+    TcArgs g5 = g4;
+    g5.M = X; g5.b_row0 = Y; g5.out = ey; g5.out2 = ey;
+    launch_tc(st->acat, st->t12t_b, g5, batch, s);
 }
 
 }  // namespace spg

@@ -1,11 +1,13 @@
 // Weighted-average wirelength, its gradient, and HPWL on sm_100a
 // (WaWirelength::compute, src/gp/wa_wirelength.cpp:46-180; computeHPWL, src/db/hpwl.cpp:13-39).
 //
-// Pass 1 runs one thread per net over a degree-sorted net order (so a warp's nets have
-// similar degrees and the pin loops stay converged). Per net it forms the extrema, the
-// shifted exponentials a+- = exp(+-(x - x_ext)/gamma), b+- and the centred c'+- sums
-// (wa_wirelength.cpp:73-127), the WA value and the HPWL term, then writes every pin's
-// gradient contribution termMax - termMin (wa_wirelength.cpp:192-221) to a per-pin array.
+// Pass 1 gives each net a group of lanes sized to its degree (nets sorted by degree and
+// cut into classes of 2, 4, 8, 16, 32 lanes, or a whole looping warp above 32 pins), so
+// a warp's lanes stay converged and the pin loads of a net are issued together. Per net it
+// forms the extrema, the shifted exponentials a+- = exp(+-(x - x_ext)/gamma), b+- and the
+// centred c'+- sums (wa_wirelength.cpp:73-127), the WA value and the HPWL term, and every
+// lane writes its pin's gradient contribution termMax - termMin (wa_wirelength.cpp:192-221)
+// to a per-pin array.
 // Pass 2 (fused into the gradient assembly) sums those contributions per node in
 // node->pin CSR order, which is exactly the reference's accumulation order, so the node
 // gradient equals the reference's whenever the exponentials agree.
@@ -17,6 +19,9 @@
 namespace spg {
 
 namespace {
+
+constexpr int kWaBlocks = 592;
+static_assert(kWaBlocks <= RED_CAP, "WA partials exceed the reduction capacity");
 
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
@@ -48,89 +53,146 @@ __device__ __forceinline__ float wa_pin_term(float dp, float dn, float ap, float
     return fsub(tmax, tmin);
 }
 
+// Width-G lane-group reductions (xor butterfly inside aligned groups of G lanes).
+__device__ __forceinline__ float group_max(float v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v = fmax_(v, __shfl_xor_sync(0xffffffffu, v, o, G));
+    return v;
+}
+__device__ __forceinline__ float group_min(float v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v = fmin_(v, __shfl_xor_sync(0xffffffffu, v, o, G));
+    return v;
+}
+__device__ __forceinline__ float group_sum(float v, int G) {
+    for (int o = G >> 1; o > 0; o >>= 1) v = fadd(v, __shfl_xor_sync(0xffffffffu, v, o, G));
+    return v;
+}
+
+__device__ __forceinline__ void pin_xy(const DevPtrs& p, int pin, float& px, float& py) {
+    const int nd = __ldg(p.pin2node + pin);
+    px = fadd(__ldg(p.x + nd), __ldg(p.pox + pin));
+    py = fadd(__ldg(p.y + nd), __ldg(p.poy + pin));
+}
+
+// WA value of one net from its extrema and sums (wa_wirelength.cpp:122-126).
+__device__ __forceinline__ double wa_value(float mxX, float mnX, float mxY, float mnY,
+                                           const float* s) {
+    return static_cast<double>(fsub(fadd(fsub(mxX, mnX), fdiv(s[1], s[0])), fdiv(s[3], s[2]))) +
+           static_cast<double>(fsub(fadd(fsub(mxY, mnY), fdiv(s[5], s[4])), fdiv(s[7], s[6])));
+}
+
+// One net of more than 32 pins, owned by a whole warp that loops over its pins.
+__device__ void wa_warp_net(const DevPtrs& p, int k, float invG, double& wl, double& hp) {
+    const int lane = threadIdx.x & 31;
+    const int b = p.net_start[k], e = p.net_start[k + 1];
+    float mxX = -FLT_MAX, mnX = FLT_MAX, mxY = -FLT_MAX, mnY = FLT_MAX;
+    for (int q = b + lane; q < e; q += 32) {
+        float px, py;
+        pin_xy(p, p.net_pins[q], px, py);
+        mxX = fmax_(mxX, px);
+        mnX = fmin_(mnX, px);
+        mxY = fmax_(mxY, py);
+        mnY = fmin_(mnY, py);
+    }
+    mxX = group_max(mxX, 32);
+    mnX = group_min(mnX, 32);
+    mxY = group_max(mxY, 32);
+    mnY = group_min(mnY, 32);
+    if (lane == 0) hp += static_cast<double>(fsub(mxX, mnX)) + static_cast<double>(fsub(mxY, mnY));
+    if (e - b > p.ignore_net_degree) {
+        for (int q = b + lane; q < e; q += 32) {
+            p.gpx[p.net_pins[q]] = 0.f;
+            p.gpy[p.net_pins[q]] = 0.f;
+        }
+        return;
+    }
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int q = b + lane; q < e; q += 32) {
+        float px, py;
+        pin_xy(p, p.net_pins[q], px, py);
+        const float dxp = fsub(px, mxX), dxn = fsub(px, mnX), dyp = fsub(py, mxY), dyn = fsub(py, mnY);
+        const float ap = expf(fmul(dxp, invG)), an = expf(fmul(-dxn, invG));
+        const float bp = expf(fmul(dyp, invG)), bn = expf(fmul(-dyn, invG));
+        s[0] = fadd(s[0], ap);
+        s[1] = fadd(s[1], fmul(dxp, ap));
+        s[2] = fadd(s[2], an);
+        s[3] = fadd(s[3], fmul(dxn, an));
+        s[4] = fadd(s[4], bp);
+        s[5] = fadd(s[5], fmul(dyp, bp));
+        s[6] = fadd(s[6], bn);
+        s[7] = fadd(s[7], fmul(dyn, bn));
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s[i] = group_sum(s[i], 32);
+    if (lane == 0) wl += wa_value(mxX, mnX, mxY, mnY, s);
+    for (int q = b + lane; q < e; q += 32) {
+        const int pin = p.net_pins[q];
+        float px, py;
+        pin_xy(p, pin, px, py);
+        const float dxp = fsub(px, mxX), dxn = fsub(px, mnX), dyp = fsub(py, mxY), dyn = fsub(py, mnY);
+        const float ap = expf(fmul(dxp, invG)), an = expf(fmul(-dxn, invG));
+        const float bp = expf(fmul(dyp, invG)), bn = expf(fmul(-dyn, invG));
+        p.gpx[pin] = wa_pin_term(dxp, dxn, ap, an, s[0], s[2], s[1], s[3], invG);
+        p.gpy[pin] = wa_pin_term(dyp, dyn, bp, bn, s[4], s[6], s[5], s[7], invG);
+    }
+}
+
+// Pass 1 of the WA model and HPWL. Nets of degree <= 32 are owned by aligned groups of
+// G = 2..32 lanes (G >= degree), one pin per lane: extrema, exponentials and the b+-/c'+-
+// sums are group butterflies, and every lane writes its own pin's gradient term. The sums
+// are formed in butterfly order rather than the reference's pin order, so values differ
+// from the reference's sequential float sums in the last bits only.
 __global__ void __launch_bounds__(RED_THREADS) wa_net_kernel(DevPtrs p, const float* gamma_dev,
                                                              float gamma_host, int use_dev) {
     __shared__ double ws[32];
     const float gam = use_dev ? *gamma_dev : gamma_host;
     const float g = fmax_(gam, 1e-4f);  // kMinGamma, wa_wirelength.cpp:14
     const float invG = fdiv(1.0f, g);
+    const int lane = threadIdx.x & 31;
+    const int warps_total = p.wa.warp_begin[p.wa.n];
+    const int wstride = gridDim.x * (blockDim.x >> 5);
     double wl = 0.0, hp = 0.0;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < p.num_nets;
-         t += gridDim.x * blockDim.x) {
-        const int k = p.net_order[t];
-        const int b = p.net_start[k], e = p.net_start[k + 1];
-        const int deg = e - b;
-        if (deg < 2) {  // no WA, no HPWL; pass 2 skips these pins (bPos = 0 marker)
-            for (int q = b; q < e; ++q) {
-                p.gpx[p.net_pins[q]] = 0.f;
-                p.gpy[p.net_pins[q]] = 0.f;
-            }
+    for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < warps_total; w += wstride) {
+        int c = 0;
+        while (c + 1 < p.wa.n && w >= p.wa.warp_begin[c + 1]) ++c;
+        const int G = p.wa.group[c];
+        if (G == 0) {
+            wa_warp_net(p, p.net_order[p.wa.net_begin[c] + (w - p.wa.warp_begin[c])], invG, wl, hp);
             continue;
         }
-        float mxX = -FLT_MAX, mnX = FLT_MAX, mxY = -FLT_MAX, mnY = FLT_MAX;
-        for (int q = b; q < e; ++q) {
-            const int pin = p.net_pins[q];
-            const int nd = p.pin2node[pin];
-            const float px = fadd(p.x[nd], p.pox[pin]);
-            const float py = fadd(p.y[nd], p.poy[pin]);
-            mxX = fmax_(mxX, px);
-            mnX = fmin_(mnX, px);
-            mxY = fmax_(mxY, py);
-            mnY = fmin_(mnY, py);
+        const int gi = lane / G, gl = lane % G;
+        const int t = p.wa.net_begin[c] + (w - p.wa.warp_begin[c]) * (32 / G) + gi;
+        const bool net_ok = t < p.wa.net_end[c];
+        const int k = net_ok ? p.net_order[t] : 0;
+        const int b = net_ok ? p.net_start[k] : 0;
+        const int deg = net_ok ? p.net_start[k + 1] - b : 0;
+        const bool act = gl < deg;
+        const int pin = act ? p.net_pins[b + gl] : 0;
+        float px = 0.f, py = 0.f;
+        if (act) pin_xy(p, pin, px, py);
+        const float mxX = group_max(act ? px : -FLT_MAX, G), mnX = group_min(act ? px : FLT_MAX, G);
+        const float mxY = group_max(act ? py : -FLT_MAX, G), mnY = group_min(act ? py : FLT_MAX, G);
+        if (gl == 0 && deg >= 2)  // computeHPWL counts every net of degree >= 2 (hpwl.cpp:18-32)
+            hp += static_cast<double>(fsub(mxX, mnX)) + static_cast<double>(fsub(mxY, mnY));
+        const bool wa_on = deg >= 2 && deg <= p.ignore_net_degree;
+        const bool live = act && wa_on;
+        const float dxp = fsub(px, mxX), dxn = fsub(px, mnX), dyp = fsub(py, mxY), dyn = fsub(py, mnY);
+        const float ap = live ? expf(fmul(dxp, invG)) : 0.f, an = live ? expf(fmul(-dxn, invG)) : 0.f;
+        const float bp = live ? expf(fmul(dyp, invG)) : 0.f, bn = live ? expf(fmul(-dyn, invG)) : 0.f;
+        float s[8] = {ap, live ? fmul(dxp, ap) : 0.f, an, live ? fmul(dxn, an) : 0.f,
+                      bp, live ? fmul(dyp, bp) : 0.f, bn, live ? fmul(dyn, bn) : 0.f};
+#pragma unroll
+        for (int i = 0; i < 8; ++i) s[i] = group_sum(s[i], G);
+        if (act) {
+            p.gpx[pin] = live ? wa_pin_term(dxp, dxn, ap, an, s[0], s[2], s[1], s[3], invG) : 0.f;
+            p.gpy[pin] = live ? wa_pin_term(dyp, dyn, bp, bn, s[4], s[6], s[5], s[7], invG) : 0.f;
         }
-        // computeHPWL: every net of degree >= 2 (hpwl.cpp:18-32)
-        hp += static_cast<double>(fsub(mxX, mnX)) + static_cast<double>(fsub(mxY, mnY));
-        if (deg > p.ignore_net_degree) {
-            for (int q = b; q < e; ++q) {
-                const int pin = p.net_pins[q];
-                p.gpx[pin] = 0.f;
-                p.gpy[pin] = 0.f;
-            }
-            continue;
-        }
-        float bpx = 0.f, bnx = 0.f, cpx = 0.f, cnx = 0.f;
-        float bpy = 0.f, bny = 0.f, cpy = 0.f, cny = 0.f;
-        for (int q = b; q < e; ++q) {
-            const int pin = p.net_pins[q];
-            const int nd = p.pin2node[pin];
-            const float px = fadd(p.x[nd], p.pox[pin]);
-            const float py = fadd(p.y[nd], p.poy[pin]);
-            const float dxp = fsub(px, mxX), dxn = fsub(px, mnX);
-            const float ap = expf(fmul(dxp, invG));
-            const float an = expf(fmul(-dxn, invG));
-            bpx = fadd(bpx, ap);
-            cpx = fadd(cpx, fmul(dxp, ap));
-            bnx = fadd(bnx, an);
-            cnx = fadd(cnx, fmul(dxn, an));
-            const float dyp = fsub(py, mxY), dyn = fsub(py, mnY);
-            const float bp = expf(fmul(dyp, invG));
-            const float bn = expf(fmul(-dyn, invG));
-            bpy = fadd(bpy, bp);
-            cpy = fadd(cpy, fmul(dyp, bp));
-            bny = fadd(bny, bn);
-            cny = fadd(cny, fmul(dyn, bn));
-        }
-        // WA_x = (x_max - x_min) + c'+/b+ - c'-/b-   (wa_wirelength.cpp:122-126)
-        wl += static_cast<double>(fsub(fadd(fsub(mxX, mnX), fdiv(cpx, bpx)), fdiv(cnx, bnx))) +
-              static_cast<double>(fsub(fadd(fsub(mxY, mnY), fdiv(cpy, bpy)), fdiv(cny, bny)));
-        for (int q = b; q < e; ++q) {
-            const int pin = p.net_pins[q];
-            const int nd = p.pin2node[pin];
-            const float px = fadd(p.x[nd], p.pox[pin]);
-            const float py = fadd(p.y[nd], p.poy[pin]);
-            const float dxp = fsub(px, mxX), dxn = fsub(px, mnX);
-            const float dyp = fsub(py, mxY), dyn = fsub(py, mnY);
-            const float ap = expf(fmul(dxp, invG)), an = expf(fmul(-dxn, invG));
-            const float bp = expf(fmul(dyp, invG)), bn = expf(fmul(-dyn, invG));
-            p.gpx[pin] = wa_pin_term(dxp, dxn, ap, an, bpx, bnx, cpx, cnx, invG);
-            p.gpy[pin] = wa_pin_term(dyp, dyn, bp, bn, bpy, bny, cpy, cny, invG);
-        }
+        if (gl == 0 && wa_on) wl += wa_value(mxX, mnX, mxY, mnY, s);
     }
     wl = block_sum_d(wl, ws);
     hp = block_sum_d(hp, ws);
     if (threadIdx.x == 0) {
-        p.partials[SLOT_WL * RED_BLOCKS + blockIdx.x] = wl;
-        p.partials[SLOT_HPWL * RED_BLOCKS + blockIdx.x] = hp;
+        p.partials[SLOT_WL * RED_CAP + blockIdx.x] = wl;
+        p.partials[SLOT_HPWL * RED_CAP + blockIdx.x] = hp;
     }
 }
 
@@ -152,7 +214,8 @@ __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
 
 void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, int use_dev,
                     cudaStream_t s) {
-    wa_net_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(p, gamma_dev, gamma_host, use_dev);
+    // a fixed grid (4 blocks per SM) so the FP64 partials keep a fixed owner per block
+    wa_net_kernel<<<kWaBlocks, RED_THREADS, 0, s>>>(p, gamma_dev, gamma_host, use_dev);
     count_launch();
     SPG_CHECK_LAUNCH();
 }

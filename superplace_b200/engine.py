@@ -81,6 +81,7 @@ def lib():
         L.spg_ctx_launch_count.argtypes = [vp]
         L.spg_ctx_stream.restype = vp
         L.spg_ctx_stream.argtypes = [vp]
+        L.spg_ctx_graph_loop.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -207,6 +208,10 @@ class GpContext:
             self.h = None
 
     __del__ = close
+
+    def graph_loop(self) -> bool:
+        """Whether the last stage run executed its loop as one conditional CUDA graph."""
+        return bool(lib().spg_ctx_graph_loop(self.h))
 
     def stream(self) -> int:
         """Raw cudaStream_t of this context (every call enqueues on it)."""

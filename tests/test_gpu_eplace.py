@@ -81,3 +81,37 @@ def test_non_finite_coordinate_is_reported():
     db.node_x[5] = 300.0
     r = ep.run(abi.STAGE_MGP)
     assert r.converged == 1
+
+
+def test_graph_loop_matches_host_loop():
+    """The conditional-graph iteration loop and the host-driven loop launch the same
+    kernels in the same order: bit-identical placements and metrics."""
+    import os
+    import subprocess
+    import sys
+
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "from tests.conftest import golden_small_db\n"
+        "from superplace_b200 import abi, engine\n"
+        "db, g = golden_small_db(True)\n"
+        "ep = engine.EPlace(db, abi.default_params(gp_bin_dim=64))\n"
+        "r = ep.run(abi.STAGE_MGP)\n"
+        "mode = ep.ctx.graph_loop()\n"
+        "np.save(sys.argv[1], np.concatenate([db.node_x, db.node_y, [r.iterations, r.evaluations, r.hpwl]]))\n"
+        "open(sys.argv[1] + '.mode', 'w').write(str(int(mode)))\n"
+    ) % os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as d:
+        outs = []
+        for host in (False, True):
+            env = dict(os.environ)
+            env.pop("SPG_HOST_LOOP", None)
+            if host:
+                env["SPG_HOST_LOOP"] = "1"
+            f = os.path.join(d, f"o{int(host)}.npy")
+            subprocess.run([sys.executable, "-c", code, f], check=True, env=env)
+            outs.append(np.load(f))
+            assert open(f + ".mode").read() == ("0" if host else "1")
+        assert np.array_equal(outs[0], outs[1])
