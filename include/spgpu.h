@@ -271,6 +271,13 @@ int spg_metrics_d2h(const spg_ctx* ctx, spg_iter_metrics* rows, int cap, int* n_
 int64_t spg_ctx_launch_count(const spg_ctx* ctx);
 /* The cudaStream_t every call on this context enqueues on (for caller-side CUDA events). */
 void* spg_ctx_stream(const spg_ctx* ctx);
+/* Per-kernel device time (microseconds, CUDA events on the context's stream, averaged
+ * over `reps` back-to-back launches, L2 warm as inside the loop) of the iteration's parts
+ * at the current positions, after a stage run. us[] receives up to n values in this order:
+ *   0 update   1 WA pass 1 + HPWL   2 density scatter   3 rho + overflow   4 Poisson solve
+ *   5 assembly (gather + WA pass 2 + gradient)   6 norms + decisions   7 one evaluation
+ * The stage's results are left unchanged (state and delivered positions are restored). */
+int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n);
 /* 1 when the last stage run executed its iteration loop as one conditional CUDA graph,
  * 0 when it ran the host-driven loop (SPG_HOST_LOOP set, or conditional nodes refused). */
 int spg_ctx_graph_loop(const spg_ctx* ctx);

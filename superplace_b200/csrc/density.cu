@@ -135,16 +135,6 @@ __device__ __forceinline__ void gather_node(const DevPtrs& p, int i, float& fx, 
     }
 }
 
-__global__ void __launch_bounds__(kThreads) gather_opt_small_kernel(DevPtrs p) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= p.n_opt_small) return;
-    const int k = p.opt_small[t];
-    float fx, fy;
-    gather_node(p, p.opt_idx[k], fx, fy);
-    p.force[k] = fx;
-    p.force[p.n_opt + k] = fy;
-}
-
 // Large nodes: the block splits the footprint; per-thread partial sums are combined in a
 // fixed tree (deterministic, but not the reference's sequential order).
 __device__ __forceinline__ void gather_large(const DevPtrs& p, int i, float& fx, float& fy) {
@@ -232,11 +222,7 @@ void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_
     SPG_CHECK_LAUNCH();
 }
 
-void launch_gather_opt(const DevPtrs& p, cudaStream_t s) {
-    if (p.n_opt_small > 0) {
-        gather_opt_small_kernel<<<ceil_div(p.n_opt_small, kThreads), kThreads, 0, s>>>(p);
-        count_launch();
-    }
+void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s) {
     if (p.n_opt_large > 0) {
         gather_opt_large_kernel<<<p.n_opt_large, kThreads, 0, s>>>(p);
         count_launch();

@@ -93,6 +93,8 @@ struct LoopGraph;
 
 struct Context {
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // WA pass 1 overlaps the density -> Poisson chain
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     spg_params prm{};
     // host copy of the db (flags and sizes change with mLG; positions live on the device)
     int num_movable = 0, num_nodes = 0, num_fillers = 0, total = 0, num_pins = 0, num_nets = 0;
@@ -139,6 +141,9 @@ struct Context {
 
     ~Context() {
         loop_graph.reset();
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (plan) poisson_plan_destroy(*plan);
         if (hst) cudaFreeHost(hst);
         if (stream) cudaStreamDestroy(stream);
@@ -440,16 +445,23 @@ void stage_setup(Context& c, int stage) {
 
 // One objAndGrad evaluation at the positions of `pos_role`, gradient into `grad_role`
 // (eplace.cpp:136-203).
+// One objAndGrad evaluation (eplace.cpp:136-203) at the current node positions (scattered
+// by the update kernels; pos_role >= 0 scatters that role first), gradient into grad_role.
+// The WA pass 1 depends only on the positions, so it runs on a side stream, overlapping
+// the density -> Poisson chain; the assembly joins both.
 void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count) {
     cudaStream_t s = c.stream;
-    launch_scatter(p, pos_role, s);
+    if (pos_role >= 0) launch_scatter(p, pos_role, s);
+    SPG_CUDA(cudaEventRecord(c.ev_fork, s));
+    SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+    launch_wa_nets(p, &p.st->gamma, 0.f, 1, c.side);
+    SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
     launch_density_accumulate(p, s);
     launch_rho_overflow(p, 0, 1, s);
     poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s);
-    launch_gather_opt(p, s);
-    launch_wa_nets(p, &p.st->gamma, 0.f, 1, s);
-    launch_assemble(p, grad_role, s);
-    launch_ctl_eval_done(p, count, s);
+    launch_gather_opt_large(p, s);
+    SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
+    launch_assemble(p, grad_role, count, s);
 }
 
 void read_state(Context& c) {
@@ -551,26 +563,21 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
     *hpwl = out[1];
 }
 
-// One iteration of the loop body (nesterov.cpp:87-121 then eplace.cpp:362-473), ending
-// with the next iteration's first evaluation and its redo test.
+// One iteration: apply the step decided after the last evaluation (nesterov.cpp:97-119),
+// evaluate at the new u, and run the redo test / next decisions.
 void enqueue_iteration(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
     cudaStream_t s = c.stream;
-    launch_ctl_step(p, s);
-    launch_nesterov_update(p, s);
-    launch_ctl_iter_end(p, s);
-    launch_snapshot_copy(p, s);
-    evaluate(c, p, R_U, R_G, 1);
-    launch_reduce_diff(p, s);
-    launch_ctl_redo_check(p, s, use_cond, redo_h);
+    launch_update(p, s);
+    evaluate(c, p, -1, R_G, 1);
+    launch_reduce(p, s, use_cond, redo_h);
 }
 
 // One redoIfOvershot re-evaluation (nesterov.cpp:158-166) and the next redo test.
 void enqueue_redo(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
     cudaStream_t s = c.stream;
     launch_redo_update(p, s);
-    evaluate(c, p, R_U, R_G, 1);
-    launch_reduce_diff(p, s);
-    launch_ctl_redo_check(p, s, use_cond, redo_h);
+    evaluate(c, p, -1, R_G, 1);
+    launch_reduce(p, s, use_cond, redo_h);
 }
 
 // Host-driven loop: one 16-byte state read per iteration (and per re-evaluation).
@@ -660,7 +667,7 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
         fine = fine && ok(cudaStreamUpdateCaptureDependencies(s, &rnode, 1, cudaStreamSetCaptureDependencies));
         if (fine) {
             rbody = rp.conditional.phGraph_out[0];
-            launch_ctl_loop_cond(p, loop_h, s);
+            launch_loop_cond(p, loop_h, s);
         }
         lg.body_kernels = g_launches - k0;
     } catch (const Error&) {
@@ -709,10 +716,8 @@ bool graph_loop(Context& c, const DevPtrs& p) {
     }
     SPG_CUDA(cudaGraphLaunch(lg.exec, c.stream));
     read_state(c);
-    // counted evaluations = iteration 0's + one per later iteration + one per re-evaluation
-    const int64_t iters = c.hst->iter;
-    const int64_t redos = std::max<int64_t>(0, c.hst->evals - iters);
-    g_launches += iters * lg.body_kernels + redos * lg.redo_kernels;
+    // one outer body per applied update, one inner body per re-evaluation
+    g_launches += static_cast<int64_t>(c.hst->iter) * lg.body_kernels + c.hst->redos * lg.redo_kernels;
     return true;
 }
 
@@ -779,8 +784,7 @@ void stage_run(Context& c, int stage, spg_result* res) {
 
     // first evaluation of iteration 0, its norms, and the redo test (a no-op at iteration 0)
     evaluate(c, p, R_U, R_G, 1);
-    launch_reduce_diff(p, s);
-    launch_ctl_redo_check(p, s);
+    launch_reduce(p, s);
     c.last_run_graph = false;
     if (max_iter > 0) {
         c.last_run_graph = c.use_graph && graph_loop(c, p);
@@ -796,13 +800,13 @@ void stage_run(Context& c, int stage, spg_result* res) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     const DevState& h = *c.hst;
-    res->iterations = h.iter;
+    res->iterations = h.rows;
     res->converged = h.converged;
     res->stagnated = h.stagnated;
     res->rollback_iter = h.stagnated ? h.rollback_iter : -1;
     res->evaluations = h.evals;
     res->elapsed_ms = ms;
-    c.metrics_rows = std::min(h.iter, max_iter);
+    c.metrics_rows = std::min(h.rows, max_iter);
     if (res->converged && !(res->overflow < target_tau))
         throw Error(SPG_E_CONVERGENCE, "delivered overflow disagrees with convergence");
     if (res->stagnated) {
@@ -1051,6 +1055,9 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     // instead of the conditional CUDA graph; both run the same kernels in the same order.
     c.use_graph = std::getenv("SPG_HOST_LOOP") == nullptr;
     SPG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    SPG_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+    SPG_CUDA(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
+    SPG_CUDA(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
     c.num_movable = v->num_movable;
     c.num_nodes = v->num_nodes;
     c.num_fillers = v->num_fillers;
@@ -1388,5 +1395,80 @@ int64_t spg_ctx_launch_count(const spg_ctx* ctx) {
 void* spg_ctx_stream(const spg_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c.stream) : nullptr; }
 
 int spg_ctx_graph_loop(const spg_ctx* ctx) { return ctx && ctx->c.last_run_graph ? 1 : 0; }
+
+int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
+    API_TRY
+    SPG_REQUIRE(ctx && us && reps > 0, SPG_E_INVALID, "bad argument");
+    Context& c = ctx->c;
+    SPG_REQUIRE(c.grid_ready && c.n_opt > 0 && c.plan, SPG_E_STATE, "run a stage before profiling");
+    cudaStream_t s = c.stream;
+    const spg::DevPtrs p = c.ptrs();
+    // keep the stage's state; profiling runs with decisions off (done) except for the update
+    spg::DevState saved;
+    SPG_CUDA(cudaMemcpyAsync(&saved, c.st.p, sizeof(saved), cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(cudaStreamSynchronize(s));
+    spg::DevState probe = saved;
+    probe.done = 1;
+    probe.redo = 0;
+    probe.snap_copy_to = -1;
+    probe.error = 0;
+    probe.tk_update = probe.tk_assemble = probe.tk_reduce = 0;
+    auto set_state = [&](const spg::DevState& st) {
+        SPG_CUDA(cudaMemcpyAsync(c.st.p, &st, sizeof(st), cudaMemcpyHostToDevice, s));
+        SPG_CUDA(cudaStreamSynchronize(s));
+    };
+    cudaEvent_t e0, e1;
+    SPG_CUDA(cudaEventCreate(&e0));
+    SPG_CUDA(cudaEventCreate(&e1));
+    const int64_t launches0 = spg::g_launches;
+    auto time = [&](auto&& body, auto&& before) {
+        double total = 0.0;
+        for (int r = 0; r < reps + 2; ++r) {  // two untimed warm-up launches
+            before();
+            SPG_CUDA(cudaEventRecord(e0, s));
+            body();
+            SPG_CUDA(cudaEventRecord(e1, s));
+            SPG_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            SPG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (r >= 2) total += ms;
+        }
+        return total * 1e3 / reps;
+    };
+    auto nothing = [] {};
+    auto zero_maps = [&] {
+        c.node_fix.zero(s);
+        c.filler_fix.zero(s);
+    };
+    double t[8] = {};
+    spg::DevState upd = probe;
+    upd.done = 0;
+    upd.last = 0;
+    set_state(upd);
+    t[0] = time([&] { spg::launch_update(p, s); }, nothing);
+    set_state(probe);
+    spg::launch_scatter(p, spg::R_POS, s);  // the delivered positions again
+    t[1] = time([&] { spg::launch_wa_nets(p, &p.st->gamma, 0.f, 1, s); }, nothing);
+    t[2] = time([&] { spg::launch_density_accumulate(p, s); }, zero_maps);
+    t[3] = time([&] { spg::launch_rho_overflow(p, 0, 1, s); }, [&] { spg::launch_density_accumulate(p, s); });
+    t[4] = time([&] { spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s); }, nothing);
+    t[5] = time([&] {
+        spg::launch_gather_opt_large(p, s);
+        spg::launch_assemble(p, spg::R_GB, 0, s);
+    }, nothing);
+    t[6] = time([&] { spg::launch_reduce(p, s); }, nothing);
+    t[7] = time([&] { spg::evaluate(c, p, -1, spg::R_GB, 0); }, nothing);
+    spg::g_launches = launches0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    // restore: state, delivered positions, and the evaluation at them
+    set_state(saved);
+    spg::launch_scatter(p, spg::R_POS, s);
+    SPG_CUDA(cudaStreamSynchronize(s));
+    spg::g_launches = launches0;
+    for (int i = 0; i < n && i < 8; ++i) us[i] = t[i];
+    return SPG_OK;
+    API_CATCH
+}
 
 }  // extern "C"

@@ -19,7 +19,9 @@
 
 namespace spg {
 
-constexpr int RED_BLOCKS = 296;  // 2 x 148 SMs: the grid of the vector kernels
+// Grid of the vector and reducing kernels: ~7 blocks of 256 threads per SM (56 warps),
+// enough resident warps to hide the latency of their gathers; at most RED_CAP.
+constexpr int RED_BLOCKS = 1024;
 // Partial sums per slot: a reducing kernel writes one per block (at most RED_CAP blocks);
 // entries past its grid stay zero, and the control kernels always sum all RED_CAP.
 constexpr int RED_CAP = 1024;
@@ -83,7 +85,11 @@ struct DevState {
     int deliver;        // 0 = v, 1 = lastEval (converged), 2 = snapshot slot deliver_slot
     int deliver_slot;
     int done, converged, stagnated, rollback_iter;
+    int last;           // max_iter reached: apply this update, then stop
+    int rows;           // iterations whose loop body ran (metrics rows)
     int error;          // SPG_E_* raised on the device (non-finite values)
+    int64_t redos;      // backtracking re-evaluations
+    unsigned int tk_update, tk_assemble, tk_reduce;  // last-block tickets
     int stage;
     int max_iter;
     int role[NUM_ROLES];
@@ -152,7 +158,8 @@ __device__ __forceinline__ float* role_ptr(const DevPtrs& p, int role) {
 void launch_density_accumulate(const DevPtrs& p, cudaStream_t s);
 // rho + tau partials; write_maps also stores the float maps, zero clears the fixed maps
 void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s);
-void launch_gather_opt(const DevPtrs& p, cudaStream_t s);
+// force of the large (block-per-node) opt nodes; cells are gathered inside the assembly
+void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s);
 // gather for every density node into a node-indexed 2*total array (parity hook)
 void launch_gather_all(const DevPtrs& p, float* force_nodes, cudaStream_t s);
 
@@ -164,20 +171,26 @@ void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s);
 
 // ---- optimizer.cu
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s);
-void launch_assemble(const DevPtrs& p, int grad_role, cudaStream_t s);
-void launch_ctl_eval_done(const DevPtrs& p, int count_eval, cudaStream_t s);
-void launch_reduce_diff(const DevPtrs& p, cudaStream_t s);
-void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
-                           cudaGraphConditionalHandle redo_cond = 0);
-void launch_ctl_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s);
-void launch_ctl_step(const DevPtrs& p, cudaStream_t s);
+// WA pass 2 + cell gather + gradient assembly; its last block finalizes the evaluation
+void launch_assemble(const DevPtrs& p, int grad_role, int count_eval, cudaStream_t s);
+// norms of the last evaluation; its last block runs the redo test and the iteration decisions
+void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
+                   cudaGraphConditionalHandle redo_cond = 0);
+void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s);
+void launch_update(const DevPtrs& p, cudaStream_t s);
 void launch_redo_update(const DevPtrs& p, cudaStream_t s);
-void launch_nesterov_update(const DevPtrs& p, cudaStream_t s);
-void launch_ctl_iter_end(const DevPtrs& p, cudaStream_t s);
-void launch_snapshot_copy(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s);
+void launch_init_norms(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_init_scale(const DevPtrs& p, float init_perturb, cudaStream_t s);
 void launch_init_perturb(const DevPtrs& p, cudaStream_t s);
+void launch_init_diff(const DevPtrs& p, cudaStream_t s);
+void launch_ctl_init_finish(const DevPtrs& p, cudaStream_t s);
 void launch_copy_role(const DevPtrs& p, int dst_role, int src_role, cudaStream_t s);
+void launch_clamp_role(const DevPtrs& p, int role, cudaStream_t s);
 void launch_deliver(const DevPtrs& p, cudaStream_t s);
+void launch_stage_clock(const DevPtrs& p, cudaStream_t s);
+void launch_check_geometry(const DevPtrs& p, float lx, float ly, float hx, float hy, const float* w,
+                           const float* h, cudaStream_t s);
 void launch_finalize_slots(const DevPtrs& p, int first, int count, double* out, cudaStream_t s);
 
 }  // namespace spg

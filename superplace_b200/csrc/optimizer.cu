@@ -8,12 +8,19 @@
 //   EPlace::run loop body     eplace.cpp:356-474 (lambda/gamma schedule, stop test,
 //                             stagnation snapshots and rollback)
 //
-// Vector work (2*nOpt floats) runs on RED_BLOCKS x RED_THREADS grids with grid-stride loops,
-// so every FP64 partial sum has a fixed owner and the reductions are deterministic. The
-// scalar logic runs in single-block "control" kernels that first reduce the partials in a
-// fixed tree and then execute the reference's scalar code on thread 0. The host never
-// computes a schedule value; it only reads the small DevState to decide whether to launch
-// another backtracking evaluation or another iteration.
+// One iteration is three kernels around the objective evaluation:
+//   update_kernel   v' = u - alpha g, u' = v' + m (v' - v), clamp, scatter u' into the node
+//                   positions, copy the last evaluated point into a stagnation snapshot when
+//                   one was decided; its last block rotates the optimizer roles
+//   assemble_kernel WA pass 2 + cell gather + gradient assembly; its last block finalizes
+//                   the evaluation (tau, HPWL, WA value, force sums)
+//   reduce_kernel   |u-uPrev|, |g-gPrevTmp|, their dot, |g|^2; its last block runs the
+//                   backtracking test and, when no re-evaluation is due, every per-iteration
+//                   decision of the reference (step size, momentum, lambda/gamma, metrics row,
+//                   stop test, stagnation and snapshot choice)
+// Vector work runs on fixed grids with grid-stride loops, so every FP64 partial sum has a
+// fixed owner; the "last block" (an atomic ticket) reduces the partials in a fixed tree, so
+// every reduction is deterministic. The host never computes a schedule value.
 #include <cfloat>
 
 #include "engine.h"
@@ -43,11 +50,23 @@ __device__ __forceinline__ double block_sum(double v) {
     return r;
 }
 
-// Sum of one slot's RED_BLOCKS partials in a fixed order (valid on thread 0).
+// Sum of one slot's RED_CAP partials in a fixed order (valid on thread 0). The loads bypass
+// L1 so a last block sees the partials other blocks of the same launch wrote.
 __device__ __forceinline__ double finalize(const DevPtrs& p, int slot) {
     double v = 0.0;
-    for (int j = threadIdx.x; j < RED_CAP; j += blockDim.x) v += p.partials[slot * RED_CAP + j];
+    for (int j = threadIdx.x; j < RED_CAP; j += blockDim.x) v += __ldcg(p.partials + slot * RED_CAP + j);
     return block_sum(v);
+}
+
+// True in exactly one block of the launch: the last to finish its partial sums.
+__device__ __forceinline__ bool last_block(unsigned int* ticket) {
+    __shared__ int is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last != 0;
 }
 
 __device__ __forceinline__ void raise_error(DevState* st, int code) { atomicCAS(&st->error, 0, code); }
@@ -79,6 +98,137 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
+__device__ __forceinline__ float* snap_ptr(const DevPtrs& p, int slot) {
+    return p.pool + static_cast<size_t>(NUM_ROLES + slot) * p.vec_stride;
+}
+
+// Step size and momentum of this step (nesterov.cpp:87-96, estimateStep :221-240), from
+// the norms of the last evaluation.
+__device__ void decide_step(const DevPtrs& p, DevState* st) {
+    st->grad_norm = static_cast<float>(sqrt(st->gn));
+    if (st->iter == 0) {
+        st->alpha = st->alpha0;
+    } else {
+        const double dx = st->dx, dg = st->dg;
+        if (dx > 0.0 && dg > 0.0) {
+            const double lip = dx / dg;
+            float a = static_cast<float>(lip);
+            if (p.use_bb) {
+                const double yy = dg * dg;
+                bool bb_ok = false;
+                if (yy > 0.0) {
+                    const double bb = st->sy / yy;
+                    if (bb > 0.0 && isfinite(bb)) {
+                        a = static_cast<float>(bb);
+                        bb_ok = true;
+                    }
+                }
+                if (!bb_ok) a = static_cast<float>(fmin(dx / dg, lip));
+            }
+            st->alpha = a;
+        }
+    }
+    const float an = st->a;
+    const float a_next = fmul(0.5f, fadd(1.f, __fsqrt_rn(fadd(fmul(fmul(4.f, an), an), 1.f))));
+    st->momentum = fdiv(fsub(an, 1.f), a_next);
+    st->a = a_next;
+}
+
+// EPlace loop body for iteration st->iter after its last evaluation (eplace.cpp:362-473):
+// lambda/gamma schedule, metrics row, stop test, stagnation guard with snapshots. These
+// depend only on the evaluated point's tau and HPWL, so they are decided before the update
+// is applied; the update of a converged or rolled-back iteration is skipped because the
+// delivered point is the evaluated one (or a snapshot).
+__device__ void decide_iteration(const DevPtrs& p, DevState* st) {
+    const int iter = st->iter;
+    if (!(isfinite(st->hpwl) && isfinite(st->tau) && isfinite(st->alpha))) {
+        raise_error(st, SPG_E_NON_FINITE);
+        st->done = 1;
+        return;
+    }
+    const float eval_lambda = st->lambda, eval_gamma = st->gamma;
+    const double dh = st->have_prev ? st->hpwl - st->prev_hpwl : 0.0;
+    const float mu = st->have_prev ? lambda_multiplier(dh, st->hpwl_ref) : 1.f;
+    if (st->have_prev) st->lambda = fmul(st->lambda, mu);
+    st->prev_hpwl = st->hpwl;
+    st->have_prev = 1;
+    st->gamma = compute_gamma(st->tau, p.step_x_gamma);
+    if (!isfinite(st->lambda) || !isfinite(st->gamma)) {
+        raise_error(st, SPG_E_NON_FINITE);
+        st->done = 1;
+        return;
+    }
+    if (iter < st->max_iter) {
+        spg_iter_metrics& m = p.metrics[iter];
+        m.iter = iter;
+        m.hpwl = st->hpwl;
+        m.overflow = st->tau;
+        m.lambda = st->lambda;
+        m.gamma = st->gamma;
+        m.step_size = st->alpha;
+        m.grad_norm_wl = static_cast<float>(st->sum_wl);
+        m.grad_norm_den = static_cast<float>(st->sum_den);
+        m.eval_lambda = eval_lambda;
+        m.eval_gamma = eval_gamma;
+        m.delta_hpwl = dh;
+        m.lambda_mu = mu;
+        m.evaluations = st->evals;
+    }
+    st->rows = iter + 1;
+    const bool filler_only = st->stage == SPG_STAGE_FILLER_ONLY;
+    // stop test: deliver the evaluated point u (eplace.cpp:412-419)
+    if (!filler_only && st->tau < st->target_tau) {
+        st->converged = 1;
+        st->deliver = 1;
+        st->done = 1;
+        return;
+    }
+    if (!filler_only && p.stagnation_window > 0) {
+        const float g = p.min_gain;
+        if (st->tau < fmul(st->ref_tau, fsub(1.f, g))) {
+            st->ref_tau = st->tau;
+            st->since_improve = 0;
+        } else {
+            st->since_improve += 1;
+        }
+        st->best_tau = fmin_(st->best_tau, st->tau);
+        const float tol = fmul(st->best_tau, fadd(1.f, g));
+        while (st->snap_count > 0 && st->snap_tau[st->snap_head] > tol) {
+            st->snap_head = (st->snap_head + 1) % SNAP_MAX;
+            st->snap_count -= 1;
+        }
+        const int last = (st->snap_head + st->snap_count - 1 + SNAP_MAX) % SNAP_MAX;
+        if (st->snap_count == 0 || fmul(st->tau, fadd(1.f, fmul(0.5f, g))) <= st->snap_tau[last]) {
+            if (st->snap_count == SNAP_MAX) {
+                raise_error(st, SPG_E_CAPACITY);
+                st->done = 1;
+                return;
+            }
+            const int slot = (st->snap_head + st->snap_count) % SNAP_MAX;
+            st->snap_tau[slot] = st->tau;
+            st->snap_hpwl[slot] = st->hpwl;
+            st->snap_iter[slot] = iter;
+            st->snap_count += 1;
+            st->snap_copy_to = slot;  // copied from u by the next update (or by deliver)
+        }
+        if (st->since_improve >= p.stagnation_window) {
+            int pick = st->snap_head;
+            for (int j = 1; j < st->snap_count; ++j) {
+                const int s = (st->snap_head + j) % SNAP_MAX;
+                if (st->snap_hpwl[s] < st->snap_hpwl[pick]) pick = s;
+            }
+            st->stagnated = 1;
+            st->rollback_iter = st->snap_iter[pick];
+            st->deliver = 2;
+            st->deliver_slot = pick;
+            st->done = 1;
+            return;
+        }
+    }
+    // the loop runs max_iter steps and delivers v after the last update (eplace.cpp:356,484)
+    if (iter + 1 >= st->max_iter) st->last = 1;
+}
+
 // ------------------------------------------------------------------ vector kernels
 
 __global__ void scatter_kernel(DevPtrs p, int role) {
@@ -94,10 +244,31 @@ __global__ void scatter_kernel(DevPtrs p, int role) {
     }
 }
 
+// force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it
+// (bin_grid.cpp:287-318).
+__device__ __forceinline__ void gather_node(const DevPtrs& p, int i, float& fx, float& fy) {
+    const GridGeom& g = p.geom;
+    const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
+    const float w = p.wgt[i];
+    fx = 0.f;
+    fy = 0.f;
+    for (int bx = f.bx0; bx <= f.bx1; ++bx) {
+        const size_t row = static_cast<size_t>(bx) * g.dim;
+        for (int by = f.by0; by <= f.by1; ++by) {
+            const float q = bin_contribution(g, bx, by, f, w);
+            if (q <= 0.f) continue;
+            fx = fadd(fx, fmul(q, __ldg(p.ex + row + by)));
+            fy = fadd(fy, fmul(q, __ldg(p.ey + row + by)));
+        }
+    }
+}
+
 // grad_k = precond * (dWL - lambda * q*xi), precond = 1 / max(1, deg + lambda*area)
 // (eplace.cpp:166-189), with the WA pass 2 (per-node sum of per-pin contributions in
-// node->pin order, wa_wirelength.cpp:137-179) fused in.
-__global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int grad_role) {
+// node->pin order, wa_wirelength.cpp:137-179) and the field gather of cells fused in (large
+// nodes' force comes from gather_opt_large). The last block finalizes the evaluation
+// (eplace.cpp:149,154-155,190-197).
+__global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int grad_role, int count_eval) {
     float* grad = role_ptr(p, grad_role);
     const float lambda = p.st->lambda;
     const int n = p.n_opt;
@@ -114,7 +285,13 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int gr
                 gy = fadd(gy, p.gpy[pin]);
             }
         }
-        const float fx = p.force[k], fy = p.force[n + k];
+        float fx, fy;
+        if (p.kind[i] & K_LARGE) {
+            fx = p.force[k];
+            fy = p.force[n + k];
+        } else {
+            gather_node(p, i, fx, fy);
+        }
         const double den = __dadd_rn(static_cast<double>(p.opt_deg[k]),
                                      __dmul_rn(static_cast<double>(lambda), p.opt_area[k]));
         const float precond = static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
@@ -132,11 +309,33 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int gr
         p.partials[SLOT_SUM_WL * RED_CAP + blockIdx.x] = acc_wl;
         p.partials[SLOT_SUM_DEN * RED_CAP + blockIdx.x] = acc_den;
     }
+    if (!last_block(&p.st->tk_assemble)) return;
+    const double over = finalize(p, SLOT_OVERFLOW);
+    const double wl = finalize(p, SLOT_WL);
+    const double hp = finalize(p, SLOT_HPWL);
+    const double swl = finalize(p, SLOT_SUM_WL);
+    const double sden = finalize(p, SLOT_SUM_DEN);
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    st->tk_assemble = 0;
+    st->tau = p.movable_area_scaled > 0.0 ? static_cast<float>(over / p.movable_area_scaled) : 0.f;
+    st->hpwl = hp;
+    st->wl_obj = wl;
+    st->sum_wl = swl;
+    st->sum_den = sden;
+    if (!(isfinite(hp) && isfinite(st->tau) && isfinite(wl) && isfinite(swl) && isfinite(sden)))
+        raise_error(st, SPG_E_NON_FINITE);
+    if (count_eval && !st->done) st->evals += 1;
 }
 
-// dx^2 = |u - uPrev|^2, dg^2 = |g - gPrevTmp|^2, sy = (u-uPrev).(g-gPrevTmp), gn = |g|^2
-// (l2Diff, dotDiff, l2Norm: nesterov.cpp:25-45), one pass over the four vectors.
-__global__ void __launch_bounds__(RED_THREADS) reduce_diff_kernel(DevPtrs p) {
+// After every counted evaluation: |u-uPrev|^2, |g-gPrevTmp|^2, their dot and |g|^2
+// (l2Diff, dotDiff, l2Norm: nesterov.cpp:25-45) in one pass; the last block then runs
+// redoIfOvershot's test (nesterov.cpp:148-157) -- redo when 1/L at the new point is at
+// most 0.95 of the step just taken, at most max_backtrack-1 times per step, only with
+// backtracking on and after the first step -- and otherwise decides the iteration. In graph
+// mode it sets the re-evaluation loop's conditional handle.
+__global__ void __launch_bounds__(RED_THREADS) reduce_kernel(DevPtrs p, int use_cond,
+                                                            cudaGraphConditionalHandle redo_cond) {
     const float* u = role_ptr(p, R_U);
     const float* up = role_ptr(p, R_UPREV);
     const float* g = role_ptr(p, R_G);
@@ -162,11 +361,112 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_diff_kernel(DevPtrs p) {
         p.partials[SLOT_SY * RED_CAP + blockIdx.x] = sy;
         p.partials[SLOT_GN * RED_CAP + blockIdx.x] = gn;
     }
+    if (!last_block(&p.st->tk_reduce)) return;
+    const double dx2 = finalize(p, SLOT_DX);
+    const double dg2 = finalize(p, SLOT_DG);
+    const double sy2 = finalize(p, SLOT_SY);
+    const double gn2 = finalize(p, SLOT_GN);
+    if (threadIdx.x != 0) return;
+    DevState* st = p.st;
+    st->tk_reduce = 0;
+    st->dx = sqrt(dx2);
+    st->dg = sqrt(dg2);
+    st->sy = sy2;
+    st->gn = gn2;
+    st->redo = 0;
+    if (!st->done && !st->error) {
+        if (p.backtrack && st->iter > 0 && st->tries < p.max_backtrack) {
+            const double ddx = st->dx, ddg = st->dg;
+            if (ddx > 0.0 && ddg > 0.0 && isfinite(ddg)) {
+                const double lip = ddx / ddg;
+                if (!(lip > 0.95 * static_cast<double>(st->alpha))) {
+                    st->alpha = static_cast<float>(lip);
+                    st->redo = 1;
+                    st->tries += 1;
+                    st->redos += 1;
+                }
+            }
+        }
+        if (!st->redo) {
+            decide_step(p, st);
+            decide_iteration(p, st);
+        }
+    }
+    if (use_cond) cudaGraphSetConditional(redo_cond, st->redo ? 1u : 0u);
+}
+
+// Graph mode: the iteration loop continues while the stage is not done.
+__global__ void loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond) {
+    const DevState* st = p.st;
+    cudaGraphSetConditional(loop_cond, (st->done || st->error) ? 0u : 1u);
+}
+
+// v' = u - alpha g ; u' = v' + momentum (v' - v) ; clamp both (nesterov.cpp:97-107), with
+// u' scattered into the node positions for the next evaluation and, when the iteration
+// decided a stagnation snapshot, the evaluated u copied into its slot. The last block
+// rotates the roles: uPrev <- u <- u' ; vPrev <- v <- v' ; gPrevTmp <- g
+// (nesterov.cpp:110-119).
+__global__ void __launch_bounds__(RED_THREADS) update_kernel(DevPtrs p) {
+    DevState* st = p.st;
+    const int done = st->done;
+    const int slot = st->snap_copy_to;
+    const float* u = role_ptr(p, R_U);
+    const float* v = role_ptr(p, R_V);
+    const float* g = role_ptr(p, R_G);
+    float* vn = role_ptr(p, R_VNEW);
+    float* un = role_ptr(p, R_UNEW);
+    float* snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
+    const float alpha = st->alpha, m = st->momentum;
+    const int n = p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        float nu[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int q = c * n + k;
+            const float uq = u[q];
+            if (snap) snap[q] = uq;
+            const float vk = fsub(uq, fmul(alpha, g[q]));
+            const float uk = fadd(vk, fmul(m, fsub(vk, v[q])));
+            const float lo = p.opt_lo[q], hi = p.opt_hi[q];
+            nu[c] = clamp_box(uk, lo, hi);
+            if (!done) {
+                vn[q] = clamp_box(vk, lo, hi);
+                un[q] = nu[c];
+            }
+        }
+        if (!done) {
+            if (!isfinite(nu[0]) || !isfinite(nu[1])) raise_error(st, SPG_E_NON_FINITE);
+            const int i = p.opt_idx[k];
+            p.x[i] = nu[0];
+            p.y[i] = nu[1];
+        }
+    }
+    if (!last_block(&st->tk_update)) return;
+    if (threadIdx.x != 0) return;
+    st->tk_update = 0;
+    st->snap_copy_to = -1;
+    if (done) return;
+    int* r = st->role;
+    const int ru = r[R_U], rup = r[R_UPREV], run = r[R_UNEW];
+    r[R_UPREV] = ru;
+    r[R_U] = run;
+    r[R_UNEW] = rup;
+    const int rv = r[R_V], rvp = r[R_VPREV], rvn = r[R_VNEW];
+    r[R_V] = rvn;
+    r[R_VPREV] = rv;
+    r[R_VNEW] = rvp;
+    const int rg = r[R_G], rgp = r[R_GPREVTMP];
+    r[R_GPREVTMP] = rg;
+    r[R_G] = rgp;
+    st->momentum_prev = st->momentum;
+    st->iter += 1;
+    st->tries = 1;
+    if (st->last) st->done = 1;
 }
 
 // v = uPrev - alpha*gPrevTmp ; u = v + momentumPrev*(v - vPrev) ; clamp v, u
-// (redoIfOvershot body, nesterov.cpp:158-163). Runs only when the check asked for it.
-__global__ void redo_update_kernel(DevPtrs p) {
+// (redoIfOvershot body, nesterov.cpp:158-163), u scattered into the node positions.
+__global__ void __launch_bounds__(RED_THREADS) redo_update_kernel(DevPtrs p) {
     if (!p.st->redo) return;
     float* v = role_ptr(p, R_V);
     float* u = role_ptr(p, R_U);
@@ -174,30 +474,23 @@ __global__ void redo_update_kernel(DevPtrs p) {
     const float* gp = role_ptr(p, R_GPREVTMP);
     const float* vp = role_ptr(p, R_VPREV);
     const float alpha = p.st->alpha, m = p.st->momentum_prev;
-    const int n = 2 * p.n_opt;
+    const int n = p.n_opt;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const float vk = fsub(up[k], fmul(alpha, gp[k]));
-        const float uk = fadd(vk, fmul(m, fsub(vk, vp[k])));
-        v[k] = clamp_box(vk, p.opt_lo[k], p.opt_hi[k]);
-        u[k] = clamp_box(uk, p.opt_lo[k], p.opt_hi[k]);
-    }
-}
-
-// vNew = u - alpha*g ; uNew = vNew + momentum*(vNew - v) ; clamp both (nesterov.cpp:97-107)
-__global__ void nesterov_update_kernel(DevPtrs p) {
-    if (p.st->done) return;
-    const float* u = role_ptr(p, R_U);
-    const float* v = role_ptr(p, R_V);
-    const float* g = role_ptr(p, R_G);
-    float* vn = role_ptr(p, R_VNEW);
-    float* un = role_ptr(p, R_UNEW);
-    const float alpha = p.st->alpha, m = p.st->momentum;
-    const int n = 2 * p.n_opt;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const float vk = fsub(u[k], fmul(alpha, g[k]));
-        const float uk = fadd(vk, fmul(m, fsub(vk, v[k])));
-        vn[k] = clamp_box(vk, p.opt_lo[k], p.opt_hi[k]);
-        un[k] = clamp_box(uk, p.opt_lo[k], p.opt_hi[k]);
+        float nu[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const int q = c * n + k;
+            const float vk = fsub(up[q], fmul(alpha, gp[q]));
+            const float uk = fadd(vk, fmul(m, fsub(vk, vp[q])));
+            const float lo = p.opt_lo[q], hi = p.opt_hi[q];
+            v[q] = clamp_box(vk, lo, hi);
+            nu[c] = clamp_box(uk, lo, hi);
+            u[q] = nu[c];
+        }
+        if (!isfinite(nu[0]) || !isfinite(nu[1])) raise_error(p.st, SPG_E_NON_FINITE);
+        const int i = p.opt_idx[k];
+        p.x[i] = nu[0];
+        p.y[i] = nu[1];
     }
 }
 
@@ -215,22 +508,15 @@ __global__ void clamp_role_kernel(DevPtrs p, int role) {
         d[k] = clamp_box(d[k], p.opt_lo[k], p.opt_hi[k]);
 }
 
-// Stagnation snapshot: copy lastEval (= uPrev after the role rotation) into its slot.
-__global__ void snapshot_copy_kernel(DevPtrs p) {
-    const int slot = p.st->snap_copy_to;
-    if (slot < 0) return;
-    float* d = p.pool + static_cast<size_t>(NUM_ROLES + slot) * p.vec_stride;
-    const float* s = role_ptr(p, R_UPREV);
-    const int n = 2 * p.n_opt;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) d[k] = s[k];
-}
-
-// Delivered solution into R_POS: v, lastEval, or the picked snapshot (eplace.cpp:412-485).
+// Delivered solution into R_POS (eplace.cpp:412-485): v after the last update, the last
+// evaluated point u (converged), or the picked snapshot (stagnated; when the pick is the
+// snapshot decided in the final iteration, its copy is still pending and u is it).
 __global__ void deliver_kernel(DevPtrs p) {
     const DevState* st = p.st;
-    const float* s = st->deliver == 1 ? role_ptr(p, R_UPREV)
-                   : st->deliver == 2 ? p.pool + static_cast<size_t>(NUM_ROLES + st->deliver_slot) * p.vec_stride
-                                      : role_ptr(p, R_V);
+    const float* s = role_ptr(p, R_V);
+    if (st->deliver == 1) s = role_ptr(p, R_U);
+    if (st->deliver == 2)
+        s = (st->deliver_slot == st->snap_copy_to) ? role_ptr(p, R_U) : snap_ptr(p, st->deliver_slot);
     float* d = role_ptr(p, R_POS);
     const int n = 2 * p.n_opt;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
@@ -291,25 +577,6 @@ __global__ void __launch_bounds__(RED_THREADS) init_diff_kernel(DevPtrs p) {
 
 // ------------------------------------------------------------------ control kernels
 
-// Results of one objAndGrad evaluation (eplace.cpp:149,154-155,190-197).
-__global__ void ctl_eval_done_kernel(DevPtrs p, int count_eval) {
-    const double over = finalize(p, SLOT_OVERFLOW);
-    const double wl = finalize(p, SLOT_WL);
-    const double hp = finalize(p, SLOT_HPWL);
-    const double swl = finalize(p, SLOT_SUM_WL);
-    const double sden = finalize(p, SLOT_SUM_DEN);
-    if (threadIdx.x != 0) return;
-    DevState* st = p.st;
-    st->tau = p.movable_area_scaled > 0.0 ? static_cast<float>(over / p.movable_area_scaled) : 0.f;
-    st->hpwl = hp;
-    st->wl_obj = wl;
-    st->sum_wl = swl;
-    st->sum_den = sden;
-    if (!(isfinite(hp) && isfinite(st->tau) && isfinite(wl) && isfinite(swl) && isfinite(sden)))
-        raise_error(st, SPG_E_NON_FINITE);
-    if (count_eval && !st->done) st->evals += 1;
-}
-
 // lambda_0 = sum|dWL| / sum|q xi|, gamma = computeGamma(tau) (eplace.cpp:254-258)
 __global__ void ctl_lambda_init_kernel(DevPtrs p) {
     DevState* st = p.st;
@@ -356,202 +623,7 @@ __global__ void ctl_init_finish_kernel(DevPtrs p) {
     st->alpha0 = (isfinite(step) && step > 0.0) ? static_cast<float>(step) : 1.f;
 }
 
-// After every counted evaluation: finalize |u-uPrev|, |g-gPrevTmp|, their dot and |g|^2,
-// then redoIfOvershot's test (nesterov.cpp:148-157): redo when 1/L at the new point is at
-// most 0.95 of the step just taken, at most max_backtrack-1 times per step, and only when
-// backtracking is on and this is not the first step (nesterov.cpp:84).
-// In graph mode it also drives the conditional nodes: redo_cond <- redo, and, when given,
-// loop_cond <- !done && !redo (the iteration loop re-enters once no re-evaluation is due).
-__global__ void ctl_redo_check_kernel(DevPtrs p, int use_cond, cudaGraphConditionalHandle redo_cond) {
-    const double dx2 = finalize(p, SLOT_DX);
-    const double dg2 = finalize(p, SLOT_DG);
-    const double sy = finalize(p, SLOT_SY);
-    const double gn2 = finalize(p, SLOT_GN);
-    if (threadIdx.x != 0) return;
-    DevState* st = p.st;
-    st->dx = sqrt(dx2);
-    st->dg = sqrt(dg2);
-    st->sy = sy;
-    st->gn = gn2;
-    st->redo = 0;
-    const bool eligible = p.backtrack && st->iter > 0 && !st->error && !st->done &&
-                          st->tries < p.max_backtrack;
-    if (eligible) {
-        const double dx = st->dx, dg = st->dg;
-        if (dx > 0.0 && dg > 0.0 && isfinite(dg)) {
-            const double lip = dx / dg;
-            if (!(lip > 0.95 * static_cast<double>(st->alpha))) {
-                st->alpha = static_cast<float>(lip);
-                st->redo = 1;
-                st->tries += 1;
-            }
-        }
-    }
-    if (use_cond) cudaGraphSetConditional(redo_cond, st->redo ? 1u : 0u);
-}
-
-// Graph mode: the iteration loop continues while the stage is not done.
-__global__ void ctl_loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond) {
-    const DevState* st = p.st;
-    cudaGraphSetConditional(loop_cond, (st->done || st->error) ? 0u : 1u);
-}
-
-// Step size and momentum of this step (nesterov.cpp:87-96, estimateStep :221-240). The
-// norms were finalized by the redo check that followed the last evaluation.
-__global__ void ctl_step_kernel(DevPtrs p) {
-    if (threadIdx.x != 0) return;
-    DevState* st = p.st;
-    if (st->done) return;
-    st->grad_norm = static_cast<float>(sqrt(st->gn));
-    if (st->iter == 0) {
-        st->alpha = st->alpha0;
-    } else {
-        const double dx = st->dx, dg = st->dg;
-        if (dx > 0.0 && dg > 0.0) {
-            const double lip = dx / dg;
-            float a = static_cast<float>(lip);
-            if (p.use_bb) {
-                const double yy = dg * dg;
-                bool done = false;
-                if (yy > 0.0) {
-                    const double bb = st->sy / yy;
-                    if (bb > 0.0 && isfinite(bb)) {
-                        a = static_cast<float>(bb);
-                        done = true;
-                    }
-                }
-                if (!done) a = static_cast<float>(fmin(dx / dg, lip));
-            }
-            st->alpha = a;
-        }
-    }
-    const float an = st->a;
-    const float a_next = fmul(0.5f, fadd(1.f, __fsqrt_rn(fadd(fmul(fmul(4.f, an), an), 1.f))));
-    st->momentum = fdiv(fsub(an, 1.f), a_next);
-    st->a = a_next;  // a_{k+1}; the update kernel only reads alpha and momentum
-}
-
-// End of one EPlace iteration: role rotation of the optimizer (nesterov.cpp:110-119),
-// lambda/gamma schedule, metrics row, stop test and stagnation guard (eplace.cpp:362-473).
-__global__ void ctl_iter_end_kernel(DevPtrs p) {
-    if (threadIdx.x != 0) return;
-    DevState* st = p.st;
-    if (st->done) return;
-    int* r = st->role;
-    {   // uPrev <- u <- uNew <- (old uPrev); v <- vNew, vPrev <- v, vNew <- (old vPrev);
-        // gPrevTmp <- g (g's buffer is rewritten by the next evaluation)
-        const int u = r[R_U], up = r[R_UPREV], un = r[R_UNEW];
-        r[R_UPREV] = u;
-        r[R_U] = un;
-        r[R_UNEW] = up;
-        const int v = r[R_V], vp = r[R_VPREV], vn = r[R_VNEW];
-        r[R_V] = vn;
-        r[R_VPREV] = v;
-        r[R_VNEW] = vp;
-        const int g = r[R_G], gp = r[R_GPREVTMP];
-        r[R_GPREVTMP] = g;
-        r[R_G] = gp;
-    }
-    st->momentum_prev = st->momentum;
-    const int iter = st->iter;
-    st->iter = iter + 1;
-    st->tries = 1;
-    st->snap_copy_to = -1;
-    if (!(isfinite(st->hpwl) && isfinite(st->tau) && isfinite(st->alpha))) {
-        raise_error(st, SPG_E_NON_FINITE);
-        st->done = 1;
-        return;
-    }
-    // lambda schedule (eplace.cpp:373-380)
-    const float eval_lambda = st->lambda, eval_gamma = st->gamma;
-    const double dh = st->have_prev ? st->hpwl - st->prev_hpwl : 0.0;
-    const float mu = st->have_prev ? lambda_multiplier(dh, st->hpwl_ref) : 1.f;
-    if (st->have_prev) st->lambda = fmul(st->lambda, mu);
-    st->prev_hpwl = st->hpwl;
-    st->have_prev = 1;
-    st->gamma = compute_gamma(st->tau, p.step_x_gamma);
-    if (!isfinite(st->lambda) || !isfinite(st->gamma)) {
-        raise_error(st, SPG_E_NON_FINITE);
-        st->done = 1;
-        return;
-    }
-    // metrics row (eplace.cpp:384-399)
-    if (iter < st->max_iter) {
-        spg_iter_metrics& m = p.metrics[iter];
-        m.iter = iter;
-        m.hpwl = st->hpwl;
-        m.overflow = st->tau;
-        m.lambda = st->lambda;
-        m.gamma = st->gamma;
-        m.step_size = st->alpha;
-        m.grad_norm_wl = static_cast<float>(st->sum_wl);
-        m.grad_norm_den = static_cast<float>(st->sum_den);
-        m.eval_lambda = eval_lambda;
-        m.eval_gamma = eval_gamma;
-        m.delta_hpwl = dh;
-        m.lambda_mu = mu;
-        m.evaluations = st->evals;
-    }
-    const bool filler_only = st->stage == SPG_STAGE_FILLER_ONLY;
-    // stop test: deliver the evaluated point u (eplace.cpp:412-419)
-    if (!filler_only && st->tau < st->target_tau) {
-        st->converged = 1;
-        st->deliver = 1;
-        st->done = 1;
-        return;
-    }
-    if (!filler_only && p.stagnation_window > 0) {
-        const float g = p.min_gain;
-        if (st->tau < fmul(st->ref_tau, fsub(1.f, g))) {
-            st->ref_tau = st->tau;
-            st->since_improve = 0;
-        } else {
-            st->since_improve += 1;
-        }
-        st->best_tau = fmin_(st->best_tau, st->tau);
-        const float tol = fmul(st->best_tau, fadd(1.f, g));
-        while (st->snap_count > 0 && st->snap_tau[st->snap_head] > tol) {
-            st->snap_head = (st->snap_head + 1) % SNAP_MAX;
-            st->snap_count -= 1;
-        }
-        const int last = (st->snap_head + st->snap_count - 1 + SNAP_MAX) % SNAP_MAX;
-        if (st->snap_count == 0 || fmul(st->tau, fadd(1.f, fmul(0.5f, g))) <= st->snap_tau[last]) {
-            if (st->snap_count == SNAP_MAX) {
-                raise_error(st, SPG_E_CAPACITY);
-                st->done = 1;
-                return;
-            }
-            const int slot = (st->snap_head + st->snap_count) % SNAP_MAX;
-            st->snap_tau[slot] = st->tau;
-            st->snap_hpwl[slot] = st->hpwl;
-            st->snap_iter[slot] = iter;
-            st->snap_count += 1;
-            st->snap_copy_to = slot;
-        }
-        if (st->since_improve >= p.stagnation_window) {
-            int pick = st->snap_head;
-            for (int j = 1; j < st->snap_count; ++j) {
-                const int s = (st->snap_head + j) % SNAP_MAX;
-                if (st->snap_hpwl[s] < st->snap_hpwl[pick]) pick = s;
-            }
-            st->stagnated = 1;
-            st->rollback_iter = st->snap_iter[pick];
-            st->deliver = 2;
-            st->deliver_slot = pick;
-            st->done = 1;
-            return;
-        }
-    }
-    if (st->iter >= st->max_iter) st->done = 1;
-}
-
-__global__ void ctl_stage_start_kernel(DevPtrs p) {
-    p.st->t0_ns = global_ns();
-}
-
-__global__ void ctl_elapsed_kernel(DevPtrs p, double* out_ms) {
-    *out_ms = static_cast<double>(global_ns() - p.st->t0_ns) * 1e-6;
-}
+__global__ void ctl_stage_start_kernel(DevPtrs p) { p.st->t0_ns = global_ns(); }
 
 __global__ void check_geometry_kernel(DevPtrs p, float lx, float ly, float hx, float hy,
                                       const float* w, const float* h) {
@@ -580,7 +652,7 @@ __global__ void finalize_slots_kernel(DevPtrs p, int first, int count, double* o
 
 inline int vec_blocks(const DevPtrs& p) {
     const int b = ceil_div(2 * static_cast<int64_t>(p.n_opt), RED_THREADS);
-    return b < 1 ? 1 : (b > 4 * RED_BLOCKS ? 4 * RED_BLOCKS : b);
+    return b < 1 ? 1 : (b > RED_BLOCKS ? RED_BLOCKS : b);
 }
 
 }  // namespace
@@ -595,39 +667,23 @@ inline int vec_blocks(const DevPtrs& p) {
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
     LAUNCH(scatter_kernel, vec_blocks(p), RED_THREADS, p, role);
 }
-void launch_assemble(const DevPtrs& p, int grad_role, cudaStream_t s) {
-    LAUNCH(assemble_kernel, RED_BLOCKS, RED_THREADS, p, grad_role);
+void launch_assemble(const DevPtrs& p, int grad_role, int count_eval, cudaStream_t s) {
+    LAUNCH(assemble_kernel, RED_BLOCKS, RED_THREADS, p, grad_role, count_eval);
 }
-void launch_ctl_eval_done(const DevPtrs& p, int count_eval, cudaStream_t s) {
-    LAUNCH(ctl_eval_done_kernel, 1, RED_THREADS, p, count_eval);
+void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond, cudaGraphConditionalHandle redo_cond) {
+    LAUNCH(reduce_kernel, RED_BLOCKS, RED_THREADS, p, use_cond, redo_cond);
+}
+void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
+    LAUNCH(loop_cond_kernel, 1, 1, p, loop_cond);
+}
+void launch_update(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(update_kernel, RED_BLOCKS, RED_THREADS, p);
+}
+void launch_redo_update(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(redo_update_kernel, RED_BLOCKS, RED_THREADS, p);
 }
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_lambda_init_kernel, 1, 1, p);
-}
-void launch_reduce_diff(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(reduce_diff_kernel, RED_BLOCKS, RED_THREADS, p);
-}
-void launch_ctl_redo_check(const DevPtrs& p, cudaStream_t s, int use_cond,
-                           cudaGraphConditionalHandle redo_cond) {
-    LAUNCH(ctl_redo_check_kernel, 1, RED_THREADS, p, use_cond, redo_cond);
-}
-void launch_ctl_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
-    LAUNCH(ctl_loop_cond_kernel, 1, 1, p, loop_cond);
-}
-void launch_redo_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(redo_update_kernel, vec_blocks(p), RED_THREADS, p);
-}
-void launch_ctl_step(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(ctl_step_kernel, 1, 32, p);
-}
-void launch_nesterov_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(nesterov_update_kernel, vec_blocks(p), RED_THREADS, p);
-}
-void launch_ctl_iter_end(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(ctl_iter_end_kernel, 1, 32, p);
-}
-void launch_snapshot_copy(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(snapshot_copy_kernel, vec_blocks(p), RED_THREADS, p);
 }
 void launch_init_norms(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(init_norms_kernel, RED_BLOCKS, RED_THREADS, p);
@@ -655,9 +711,6 @@ void launch_deliver(const DevPtrs& p, cudaStream_t s) {
 }
 void launch_stage_clock(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_stage_start_kernel, 1, 1, p);
-}
-void launch_elapsed(const DevPtrs& p, double* out_ms, cudaStream_t s) {
-    LAUNCH(ctl_elapsed_kernel, 1, 1, p, out_ms);
 }
 void launch_check_geometry(const DevPtrs& p, float lx, float ly, float hx, float hy, const float* w,
                            const float* h, cudaStream_t s) {

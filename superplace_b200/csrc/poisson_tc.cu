@@ -6,14 +6,15 @@
 // tensor memory (the lo.lo term, ~2^-16 relative, is dropped). The three products are one
 // accumulation over K' = 3K: the producer walks (hi,hi), (hi,lo), (lo,hi) K slabs.
 //
-// Kernel (one 128 x BN output tile per CTA, 128 threads):
+// Kernel (one 128 x BN output tile per cluster of S split-K CTAs, 128 threads each):
 //   warp 0 lane 0   TMA producer: 128x64 A and BNx64 B bf16 tiles (128-byte swizzle)
 //                   into a STAGES-deep shared-memory ring (full/empty mbarriers)
 //   warp 1 lane 0   MMA issuer: 4 x tcgen05.mma.kind::f16 (M=128, N=BN, K=16) per slab,
 //                   tcgen05.commit frees the slab, a final commit publishes the accumulator
-//   warps 0-3       epilogue: tcgen05.ld of the TMEM accumulator (one TMEM lane per
-//                   output row), optional spectral scale, DC-row override, and either an
-//                   FP32 store or a split store of the next contraction's BF16 hi/lo planes
+//   warps 0-3       epilogue: tcgen05.ld of the TMEM partial into shared memory, a
+//                   cluster-wide reduction of the S partials over DSMEM (rank order), the
+//                   optional spectral scale and DC-row override, and either an FP32 store
+//                   or a split store of the next contraction's BF16 hi/lo planes
 // Every mbarrier wait is bounded (2 s of %globaltimer); on timeout the kernel records
 // SPG_E_CUDA in the plan's error word, stops issuing, frees its TMEM and returns.
 //
@@ -165,6 +166,31 @@ __device__ __forceinline__ void split_bf16(float v, uint16_t& hi, uint16_t& lo) 
     lo = __bfloat16_as_ushort(l);
 }
 
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t map_rank(uint32_t local_addr, uint32_t rank) {
+    uint32_t remote;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(local_addr), "r"(rank));
+    return remote;
+}
+
+// 16-byte load from another CTA's shared memory (volatile keeps it after the cluster barrier).
+__device__ __forceinline__ float4 ld_dsmem4(uint32_t addr) {
+    float4 v;
+    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(addr));
+    return v;
+}
+
+// Grid (S, N/BN, (M/128) * batch), cluster (S, 1, 1): the S CTAs of a cluster share one
+// 128 x BN output tile and split its 3K/64 K slabs evenly (split-K). Each accumulates its
+// slice in TMEM and stages it in shared memory; then CTA r reduces rows
+// [r*128/S, (r+1)*128/S) over the cluster's S partials through distributed shared memory,
+// in rank order (deterministic), and runs the epilogue for those rows with consecutive
+// threads on consecutive columns (coalesced stores).
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -172,19 +198,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;
     constexpr uint32_t B_BYTES = BN * TC_BK * 2;
+    constexpr int RED_LD = BN + 4;  // staged partial tile row pitch (floats, 16-byte rows)
+    static_assert(TC_BM * RED_LD * 4 <= STAGES * (A_BYTES + B_BYTES), "partial tile must fit the ring");
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = base;
     uint8_t* sB = base + STAGES * A_BYTES;
     uint64_t* bars = reinterpret_cast<uint64_t*>(sB + STAGES * B_BYTES);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
-    __shared__ int s_fail;
+    float* red = reinterpret_cast<float*>(base);  // reuses the ring after the main loop
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * TC_BM, z = blockIdx.z;
+    const int S = gridDim.x, rank = blockIdx.x;
+    const int tiles_m = g.M / TC_BM;
+    const int n0 = blockIdx.y * BN, m0 = (blockIdx.z % tiles_m) * TC_BM, z = blockIdx.z / tiles_m;
     const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES), accb = smem_u32(bars + 2 * STAGES);
 
     if (threadIdx.x == 0) {
-        s_fail = 0;
         for (int i = 0; i < STAGES; ++i) {
             mbar_init(full0 + 8 * i, 1);
             mbar_init(empty0 + 8 * i, 1);
@@ -205,15 +234,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
     const int kpp = g.K / TC_BK;  // slabs per split pass
     const int nk = 3 * kpp;
+    const int s0 = rank * nk / S, s1 = (rank + 1) * nk / S;
     if (warp == 0 && lane == 0) {
-        // producer: passes (A_hi,B_hi), (A_hi,B_lo), (A_lo,B_hi)
-        for (int s = 0; s < nk; ++s) {
-            const int st = s % STAGES;
-            const uint32_t ph = (s / STAGES) & 1;
-            if (!mbar_wait(empty0 + 8 * st, ph ^ 1)) {
-                s_fail = 1;
-                break;
-            }
+        // producer: passes (A_hi,B_hi), (A_hi,B_lo), (A_lo,B_hi) over this CTA's slabs
+        for (int s = s0; s < s1; ++s) {
+            const int i = s - s0, st = i % STAGES;
+            const uint32_t ph = (i / STAGES) & 1;
+            if (!mbar_wait(empty0 + 8 * st, ph ^ 1)) break;
             const int pass = s / kpp, kk = (s % kpp) * TC_BK;
             const int arow = g.a_row0 + m0 + (pass == 2 ? g.a_lo : 0);
             const int brow = g.b_row0 + n0 + (pass == 1 ? g.b_lo : 0);
@@ -224,12 +251,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else if (warp == 1 && lane == 0) {
         constexpr uint32_t idesc = idesc_bf16(TC_BM, BN);
         bool ok = true;
-        for (int s = 0; s < nk; ++s) {
-            const int st = s % STAGES;
-            const uint32_t ph = (s / STAGES) & 1;
+        for (int s = s0; s < s1; ++s) {
+            const int i = s - s0, st = i % STAGES;
+            const uint32_t ph = (i / STAGES) & 1;
             if (!mbar_wait(full0 + 8 * st, ph)) {
                 ok = false;
-                s_fail = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -237,55 +263,76 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
             for (int k = 0; k < TC_BK / 16; ++k)  // 16 bf16 = 32 bytes per MMA along K
                 umma_bf16(tmem, sw128_desc(a0 + 32 * k), sw128_desc(b0 + 32 * k), idesc,
-                          (s > 0 || k > 0) ? 1u : 0u);
+                          (i > 0 || k > 0) ? 1u : 0u);
             umma_commit(empty0 + 8 * st);
         }
         if (ok) umma_commit(accb);
     }
     __syncwarp();
 
-    // epilogue: TMEM lane = output row (warp w owns rows 32w .. 32w+31)
-    // warp-uniform decision: tcgen05.ld is .sync.aligned
+    // stage this CTA's partial tile (TMEM lane = tile row; warp w owns rows 32w..32w+31)
     const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0) ? 1 : 0) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!acc_ok) {
-        if (threadIdx.x == 0) atomicCAS(g.err, 0, SPG_E_CUDA);
-    } else {
-        const int m = m0 + 32 * warp + lane;
-        const bool row0 = (m == 0) && g.row0;
+    if (acc_ok) {
+        const int r = 32 * warp + lane;
 #pragma unroll 1
         for (int c = 0; c < BN; c += 32) {
             float v[32];
             tmem_ld32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + c, v);
-            const int nb = n0 + c;
-            if (row0) {
 #pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] = g.row0[z * g.row0_z + nb + i];
+            for (int i = 0; i < 32; ++i) red[r * RED_LD + c + i] = v[i];
+        }
+    } else if (threadIdx.x == 0) {
+        atomicCAS(g.err, 0, SPG_E_CUDA);
+    }
+    const int ok_cta = __syncthreads_and(acc_ok ? 1 : 0);
+    cluster_sync_all();  // every CTA of the cluster has staged its partial
+
+    // reduce rows [rank*R, rank*R + R) over the S partials (4 columns per thread, rank
+    // order) and write them
+    const int R = TC_BM / S;
+    if (ok_cta) {
+        const uint32_t red_addr = smem_u32(red);
+        uint32_t rbase[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) rbase[q] = q < S ? map_rank(red_addr, static_cast<uint32_t>(q)) : 0u;
+        for (int e = threadIdx.x; e < R * (BN / 4); e += TC_THREADS) {
+            const int row = rank * R + e / (BN / 4), col = (e % (BN / 4)) * 4;
+            const uint32_t off = 4u * static_cast<uint32_t>(row * RED_LD + col);
+            float4 parts[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (q < S) parts[q] = ld_dsmem4(rbase[q] + off);
+            float v[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                if (q >= S) break;
+                v[0] += parts[q].x;
+                v[1] += parts[q].y;
+                v[2] += parts[q].z;
+                v[3] += parts[q].w;
             }
-            if (g.scale) {
+            const int m = m0 + row, n = n0 + col;
 #pragma unroll
-                for (int i = 0; i < 32; ++i) v[i] *= g.scale[m * g.lds + nb + i];
+            for (int i = 0; i < 4; ++i) {
+                if (m == 0 && g.row0) v[i] = g.row0[z * g.row0_z + n + i];
+                if (g.scale) v[i] *= g.scale[m * g.lds + n + i];
             }
             if (g.mode == TC_F32) {
-                float* row = (m < g.split) ? g.out + z * g.out_z + m * g.ldc
+                float* dst = (m < g.split) ? g.out + z * g.out_z + m * g.ldc
                                            : g.out2 + z * g.out_z + (m - g.split) * g.ldc;
-#pragma unroll
-                for (int i = 0; i < 32; i += 4)
-                    *reinterpret_cast<float4*>(row + nb + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                *reinterpret_cast<float4*>(dst + n) = make_float4(v[0], v[1], v[2], v[3]);
             } else {
-                uint16_t* hi = g.planes + z * g.plane_z + m * g.ldc + nb;
-                uint16_t* lo = hi + g.plane_stride;
+                uint16_t h[4], l[4];
 #pragma unroll
-                for (int i = 0; i < 32; i += 8) {
-                    uint16_t h[8], l[8];
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) split_bf16(v[i + j], h[j], l[j]);
-                    *reinterpret_cast<uint4*>(hi + i) = *reinterpret_cast<const uint4*>(h);
-                    *reinterpret_cast<uint4*>(lo + i) = *reinterpret_cast<const uint4*>(l);
-                }
+                for (int i = 0; i < 4; ++i) split_bf16(v[i], h[i], l[i]);
+                uint16_t* hi = g.planes + z * g.plane_z + m * g.ldc + n;
+                *reinterpret_cast<uint2*>(hi) = *reinterpret_cast<const uint2*>(h);
+                *reinterpret_cast<uint2*>(hi + g.plane_stride) = *reinterpret_cast<const uint2*>(l);
             }
         }
     }
+    cluster_sync_all();  // no CTA leaves while another may still read its shared memory
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
@@ -365,13 +412,35 @@ struct TcState {
     int* err = nullptr;
 };
 
-void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int batch, cudaStream_t s) {
+// Split-K factor: the largest S in {8, 4, 2} (S divides the 128 tile rows, which the
+// reduction splits into S bands) dividing the slab count, with one grid's tiles * S CTAs
+// in one wave over the 148 SMs (1 CTA per SM), else 1. It depends on one grid's problem
+// only, so a grid's result does not depend on the batch it is solved in.
+int pick_splits(int tiles, int slabs) {
+    for (int s : {8, 4, 2})
+        if (slabs % s == 0 && tiles * s <= 148) return s;
+    return 1;
+}
+
+void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int batch, int grid_tiles,
+               cudaStream_t s) {
     SPG_REQUIRE(g.M % TC_BM == 0 && g.N % TC_BN == 0 && g.K % TC_BK == 0, SPG_E_INVALID,
                 "tensor-core GEMM dims must be tile multiples");
-    dim3 grid(g.N / TC_BN, g.M / TC_BM, batch);
-    tc_gemm_kernel<TC_BN, TC_STAGES><<<grid, TC_THREADS, tc_smem_bytes(), s>>>(a, b, g);
+    const int S = pick_splits(grid_tiles, 3 * (g.K / TC_BK));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(S, g.N / TC_BN, (g.M / TC_BM) * batch);
+    cfg.blockDim = dim3(TC_THREADS);
+    cfg.dynamicSmemBytes = tc_smem_bytes();
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = S;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES>, a, b, g));
     count_launch();
-    SPG_CHECK_LAUNCH();
 }
 
 void prep_split(const float* src, int rows, int cols, int64_t ld, int seg, int center, uint16_t* planes,
@@ -488,7 +557,7 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
     g1.a_row0 = 0; g1.a_lo = Y; g1.b_row0 = 0; g1.b_lo = static_cast<int>(BXc); g1.b_col_z = 0;
     g1.mode = TC_F32; g1.out = st->t0t32; g1.out2 = st->t0t32; g1.split = Y; g1.ldc = BXc; g1.out_z = 0;
     g1.row0 = sum_r; g1.row0_z = 0; g1.err = st->err;
-    launch_tc(st->cy, st->rho_b, g1, 1, s);
+    launch_tc(st->cy, st->rho_b, g1, 1, (X / TC_BN) * (Y / TC_BM), s);
     // T0t rows minus their per-grid means -> split planes (B operand of G2), segment sums
     prep_split(st->t0t32, Y, static_cast<int>(BX), BXc, X, 1, pl.t0t_s, static_cast<int64_t>(Y) * BXc, sum_t, s);
     // G2: P_z (X x Y) = Cx . T0t'[:, z]^T, times the spectral scale, DC row from the sums
@@ -497,23 +566,23 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
     g2.a_row0 = 0; g2.a_lo = X; g2.b_row0 = 0; g2.b_lo = Y; g2.b_col_z = X;
     g2.mode = TC_SPLIT; g2.planes = pl.p_s; g2.plane_stride = BXc * Y; g2.plane_z = XY; g2.ldc = Y;
     g2.scale = pl.scale; g2.lds = Y; g2.row0 = sum_t; g2.row0_z = Y; g2.err = st->err;
-    launch_tc(st->cx, st->t0t_b, g2, batch, s);
+    launch_tc(st->cx, st->t0t_b, g2, batch, (Y / TC_BN) * (X / TC_BM), s);
     // G3: T12t (2Y x BX) = [Ay; Sy] . P^T  -> split planes
     TcArgs g3{};
     g3.M = 2 * Y; g3.N = static_cast<int>(BX); g3.K = Y;
     g3.a_row0 = 0; g3.a_lo = 2 * Y; g3.b_row0 = 0; g3.b_lo = static_cast<int>(BXc); g3.b_col_z = 0;
     g3.mode = TC_SPLIT; g3.planes = pl.t12t_s; g3.plane_stride = 2 * static_cast<int64_t>(Y) * BXc;
     g3.plane_z = 0; g3.ldc = BXc; g3.err = st->err;
-    launch_tc(st->bcat, st->p_b, g3, 1, s);
+    launch_tc(st->bcat, st->p_b, g3, 1, (X / TC_BN) * (2 * Y / TC_BM), s);
     // G4a: [phi; xi_x]_z = [Ax; Sx] . T1t[:, z]^T ; G4b: xi_y_z = Ax . T2t[:, z]^T
     TcArgs g4{};
     g4.M = 2 * X; g4.N = Y; g4.K = X;
     g4.a_row0 = 0; g4.a_lo = 2 * X; g4.b_row0 = 0; g4.b_lo = 2 * Y; g4.b_col_z = X;
     g4.mode = TC_F32; g4.out = phi; g4.out2 = ex; g4.split = X; g4.ldc = Y; g4.out_z = XY; g4.err = st->err;
-    launch_tc(st->acat, st->t12t_b, g4, batch, s);
+    launch_tc(st->acat, st->t12t_b, g4, batch, (Y / TC_BN) * (2 * X / TC_BM), s);
     TcArgs g5 = g4;
     g5.M = X; g5.b_row0 = Y; g5.out = ey; g5.out2 = ey;
-    launch_tc(st->acat, st->t12t_b, g5, batch, s);
+    launch_tc(st->acat, st->t12t_b, g5, batch, (Y / TC_BN) * (X / TC_BM), s);
 }
 
 }  // namespace spg

@@ -20,7 +20,7 @@ namespace spg {
 
 namespace {
 
-constexpr int kWaBlocks = 592;
+constexpr int kWaBlocks = 1024;
 static_assert(kWaBlocks <= RED_CAP, "WA partials exceed the reduction capacity");
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -214,7 +214,7 @@ __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
 
 void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, int use_dev,
                     cudaStream_t s) {
-    // a fixed grid (4 blocks per SM) so the FP64 partials keep a fixed owner per block
+    // a fixed grid (RED_CAP blocks) so the FP64 partials keep a fixed owner per block
     wa_net_kernel<<<kWaBlocks, RED_THREADS, 0, s>>>(p, gamma_dev, gamma_host, use_dev);
     count_launch();
     SPG_CHECK_LAUNCH();

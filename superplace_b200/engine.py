@@ -82,6 +82,7 @@ def lib():
         L.spg_ctx_stream.restype = vp
         L.spg_ctx_stream.argtypes = [vp]
         L.spg_ctx_graph_loop.argtypes = [vp]
+        L.spg_ctx_profile.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int]
         _lib = L
     return _lib
 
@@ -212,6 +213,15 @@ class GpContext:
     def graph_loop(self) -> bool:
         """Whether the last stage run executed its loop as one conditional CUDA graph."""
         return bool(lib().spg_ctx_graph_loop(self.h))
+
+    PROFILE_PARTS = ("update", "wa", "scatter", "rho", "poisson", "assemble", "reduce", "evaluation")
+
+    def profile(self, reps=20) -> dict:
+        """Warm-L2 device time (us) of each iteration part at the current positions,
+        CUDA events on the context's stream; the stage's results are left unchanged."""
+        out = (C.c_double * 8)()
+        check(lib().spg_ctx_profile(self.h, reps, out, 8))
+        return dict(zip(self.PROFILE_PARTS, list(out)))
 
     def stream(self) -> int:
         """Raw cudaStream_t of this context (every call enqueues on it)."""
