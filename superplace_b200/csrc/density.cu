@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(RED_THREADS) rho_overflow_kernel(DevPtrs p, in
         }
     }
     over = block_sum(over);
-    if (threadIdx.x == 0) p.partials[SLOT_OVERFLOW * RED_CAP + blockIdx.x] = over;
+    put_partial(p, SLOT_OVERFLOW, over);
 }
 
 // force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it.
@@ -217,7 +217,8 @@ void launch_density_accumulate(const DevPtrs& p, cudaStream_t s) {
 }
 
 void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s) {
-    rho_overflow_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(p, write_maps, zero);
+    const int grid = wave_grid(reinterpret_cast<const void*>(rho_overflow_kernel), RED_THREADS, RED_CAP);
+    rho_overflow_kernel<<<grid, RED_THREADS, 0, s>>>(p, write_maps, zero);
     count_launch();
     SPG_CHECK_LAUNCH();
 }

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <random>
 #include <string>
@@ -26,6 +27,36 @@
 namespace spg {
 
 int64_t g_launches = 0;
+
+int wave_grid(const void* kernel, int threads, int cap) {
+    struct Entry {
+        const void* kernel;
+        int device, threads, blocks;
+    };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    int dev = 0;
+    SPG_CUDA(cudaGetDevice(&dev));
+    int blocks = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (const Entry& e : cache)
+            if (e.kernel == kernel && e.device == dev && e.threads == threads) blocks = e.blocks;
+    }
+    if (blocks == 0) {
+        int sms = 0, per_sm = 0;
+        SPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        SPG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0));
+        blocks = std::max(1, sms) * std::max(1, per_sm);
+        std::lock_guard<std::mutex> lock(mu);
+        cache.push_back(Entry{kernel, dev, threads, blocks});
+    }
+    if (blocks <= cap) return blocks;
+    int sms = 0;
+    SPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // whole blocks per SM under the cap, so the wave stays even
+    return sms > 0 && cap >= sms ? (cap / sms) * sms : cap;
+}
 
 // optimizer.cu entry points not declared in engine.h
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s);
@@ -97,7 +128,7 @@ struct Context {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     spg_params prm{};
     // host copy of the db (flags and sizes change with mLG; positions live on the device)
-    int num_movable = 0, num_nodes = 0, num_fillers = 0, total = 0, num_pins = 0, num_nets = 0;
+    int num_movable = 0, num_nodes = 0, num_fillers = 0, total = 0, num_pins = 0, num_nets = 0, num_slots = 0;
     std::vector<float> w, h;
     std::vector<uint8_t> flags;
     std::vector<int> node_start;
@@ -109,6 +140,7 @@ struct Context {
     DevBuf<uint8_t> kind;
     DevBuf<float> pox, poy, gpx, gpy;
     DevBuf<int> pin2node, pin2net, net_start, net_pins, node_start_d, node_pins, net_order;
+    DevBuf<int> slot_start, net_slot;
     WaClasses wa_classes{};
     // grid
     bool grid_ready = false;
@@ -176,6 +208,8 @@ struct Context {
         p.wa = wa_classes;
         p.gpx = gpx.p;
         p.gpy = gpy.p;
+        p.slot_start = slot_start.p;
+        p.net_slot = net_slot.p;
         p.geom = geom;
         p.node_fix = node_fix.p;
         p.filler_fix = filler_fix.p;
@@ -742,7 +776,8 @@ void stage_run(Context& c, int stage, spg_result* res) {
     const int max_iter = filler_only ? c.prm.filler_only_iters : c.prm.gp_max_iter;
     DevPtrs p = c.ptrs();
     init_state_kernel<<<1, 1, 0, s>>>(p, stage, max_iter, target_tau);
-    gather_pos_kernel<<<RED_BLOCKS, RED_THREADS, 0, s>>>(p);
+    gather_pos_kernel<<<wave_grid(reinterpret_cast<const void*>(gather_pos_kernel), RED_THREADS, RED_CAP),
+                        RED_THREADS, 0, s>>>(p);
     count_launch(2);
     SPG_CHECK_LAUNCH();
     launch_clamp_role(p, R_POS, s);
@@ -1134,8 +1169,33 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
         }
         wc.warp_begin[wc.n] = warps;
     }
-    c.gpx.alloc(std::max(c.num_pins, 1));
-    c.gpy.alloc(std::max(c.num_pins, 1));
+    // node-order slots of the pins that belong to a net; the last slot is never read
+    {
+        for (int k = 0; k < c.num_nets; ++k)
+            for (int q = v->net2pin_start[k]; q < v->net2pin_start[k + 1]; ++q)
+                SPG_REQUIRE(v->pin2net[v->flat_net2pin[q]] == k, SPG_E_INVALID,
+                            "pin2net disagrees with the net CSR");
+        std::vector<int> slot_of_pin(c.num_pins, -1), slot_start(T + 1);
+        int slots = 0;
+        for (size_t i = 0; i < T; ++i) {
+            slot_start[i] = slots;
+            for (int t = c.node_start[i]; t < c.node_start[i + 1]; ++t) {
+                const int pin = v->flat_node2pin[t];
+                if (v->pin2net[pin] >= 0) slot_of_pin[pin] = slots++;
+            }
+        }
+        slot_start[T] = slots;
+        std::vector<int> net_slot(c.num_pins);
+        for (int q = 0; q < c.num_pins; ++q) {
+            const int sl = slot_of_pin[v->flat_net2pin[q]];
+            net_slot[q] = sl >= 0 ? sl : slots;
+        }
+        c.slot_start.upload(slot_start, s);
+        c.net_slot.upload(net_slot, s);
+        c.num_slots = slots;
+    }
+    c.gpx.alloc(c.num_slots + 1);
+    c.gpy.alloc(c.num_slots + 1);
     c.gpx.zero(s);
     c.gpy.zero(s);
     c.st.alloc(1);

@@ -19,13 +19,16 @@
 
 namespace spg {
 
-// Grid of the vector and reducing kernels: ~7 blocks of 256 threads per SM (56 warps),
-// enough resident warps to hide the latency of their gathers; at most RED_CAP.
-constexpr int RED_BLOCKS = 1024;
-// Partial sums per slot: a reducing kernel writes one per block (at most RED_CAP blocks);
-// entries past its grid stay zero, and the control kernels always sum all RED_CAP.
+// Partial sums per slot: a reducing kernel writes one per block (at most RED_CAP blocks)
+// and clears the entries past its grid; the finalizing code always sums all RED_CAP in a
+// fixed tree. The vector and reducing kernels run one full wave (wave_grid), so no SM
+// idles behind a partial second wave.
 constexpr int RED_CAP = 1024;
 constexpr int RED_THREADS = 256;
+
+// Blocks of `threads` threads that fill every SM once at the kernel's occupancy, at most
+// `cap`; cached per kernel and device (engine.cu).
+int wave_grid(const void* kernel, int threads, int cap);
 
 enum RedSlot : int {
     SLOT_OVERFLOW = 0,
@@ -118,8 +121,11 @@ struct DevPtrs {
     const int *node_start, *node_pins;
     const int* net_order;  // nets sorted by degree (ascending)
     WaClasses wa;
-    // per-pin WA gradient contributions (x, y)
+    // per-pin WA gradient contributions (x, y), stored in node order: the pins of node i
+    // that belong to a net own slots [slot_start[i], slot_start[i+1]) in node->pin order;
+    // net_slot[q] is the slot of net-CSR entry q
     float *gpx, *gpy;
+    const int *slot_start, *net_slot;
     // grid
     GridGeom geom;
     unsigned long long *node_fix, *filler_fix;
@@ -152,6 +158,15 @@ struct DevPtrs {
 
 __device__ __forceinline__ float* role_ptr(const DevPtrs& p, int role) {
     return p.pool + static_cast<size_t>(p.st->role[role]) * p.vec_stride;
+}
+
+// Thread 0 of every block stores the block's partial of `slot`; block 0 also clears the
+// entries past the grid, so the slot sums exactly this launch's partials.
+__device__ __forceinline__ void put_partial(const DevPtrs& p, int slot, double v) {
+    double* d = p.partials + static_cast<size_t>(slot) * RED_CAP;
+    if (threadIdx.x == 0) d[blockIdx.x] = v;
+    if (blockIdx.x == 0)
+        for (int j = gridDim.x + threadIdx.x; j < RED_CAP; j += blockDim.x) d[j] = 0.0;
 }
 
 // ---- density.cu

@@ -58,6 +58,62 @@ __device__ __forceinline__ double finalize(const DevPtrs& p, int slot) {
     return block_sum(v);
 }
 
+// block_sum of N values at once (RED_THREADS-thread blocks), each in block_sum's tree, with
+// one pair of barriers for all N; results on thread 0.
+template <int N>
+__device__ __forceinline__ void block_sums(double (&v)[N]) {
+    __shared__ double ws[N][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        v[i] = warp_sum(v[i]);
+        if (lane == 0) ws[i][wid] = v[i];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        double r = 0.0;
+        if (wid == 0) {
+            r = lane < RED_THREADS / 32 ? ws[i][lane] : 0.0;
+            r = warp_sum(r);
+        }
+        v[i] = r;
+    }
+    __syncthreads();
+}
+
+// finalize of N slots at once, each in finalize's tree: all the partial loads are issued
+// together and the N block reductions share their barriers.
+template <int N>
+__device__ __forceinline__ void finalize_n(const DevPtrs& p, const int (&slots)[N], double (&out)[N]) {
+    static_assert(RED_CAP % RED_THREADS == 0, "partials must split evenly over the block");
+#pragma unroll
+    for (int i = 0; i < N; ++i) out[i] = 0.0;
+#pragma unroll
+    for (int j = 0; j < RED_CAP / RED_THREADS; ++j)
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+            out[i] += __ldcg(p.partials + slots[i] * RED_CAP + j * RED_THREADS + threadIdx.x);
+    block_sums(out);
+}
+
+// Whole-state copies between global and shared memory (all threads of the block). The
+// serial decision code of a last block is a chain of dependent reads and writes of the
+// state; on a shared copy each link costs a shared-memory access instead of an L2 trip.
+__device__ __forceinline__ void state_copy_in(DevState* dst, const DevState* src) {
+    static_assert(sizeof(DevState) % 8 == 0, "DevState is copied as 8-byte words");
+    const auto* s = reinterpret_cast<const unsigned long long*>(src);
+    auto* d = reinterpret_cast<unsigned long long*>(dst);
+    for (int j = threadIdx.x; j < static_cast<int>(sizeof(DevState) / 8); j += blockDim.x) d[j] = __ldcg(s + j);
+    __syncthreads();
+}
+__device__ __forceinline__ void state_copy_out(DevState* dst, const DevState* src) {
+    __syncthreads();
+    const auto* s = reinterpret_cast<const unsigned long long*>(src);
+    auto* d = reinterpret_cast<unsigned long long*>(dst);
+    for (int j = threadIdx.x; j < static_cast<int>(sizeof(DevState) / 8); j += blockDim.x) d[j] = s[j];
+}
+
 // True in exactly one block of the launch: the last to finish its partial sums.
 __device__ __forceinline__ bool last_block(unsigned int* ticket) {
     __shared__ int is_last;
@@ -246,12 +302,35 @@ __global__ void scatter_kernel(DevPtrs p, int role) {
 
 // force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it
 // (bin_grid.cpp:287-318).
+// Footprints of at most 2x2 bins (every cell no wider than one bin) issue their eight field
+// loads before the sums, which keep the reference's order.
 __device__ __forceinline__ void gather_node(const DevPtrs& p, int i, float& fx, float& fy) {
     const GridGeom& g = p.geom;
     const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
     const float w = p.wgt[i];
     fx = 0.f;
     fy = 0.f;
+    if (f.bx1 - f.bx0 <= 1 && f.by1 - f.by0 <= 1) {
+        float q[4], ex[4], ey[4];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const int bx = f.bx0 + a, by = f.by0 + b;
+                const bool in = bx <= f.bx1 && by <= f.by1;
+                const size_t o = static_cast<size_t>(in ? bx : f.bx0) * g.dim + (in ? by : f.by0);
+                q[2 * a + b] = in ? bin_contribution(g, bx, by, f, w) : 0.f;
+                ex[2 * a + b] = __ldg(p.ex + o);
+                ey[2 * a + b] = __ldg(p.ey + o);
+            }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (q[j] <= 0.f) continue;
+            fx = fadd(fx, fmul(q[j], ex[j]));
+            fy = fadd(fy, fmul(q[j], ey[j]));
+        }
+        return;
+    }
     for (int bx = f.bx0; bx <= f.bx1; ++bx) {
         const size_t row = static_cast<size_t>(bx) * g.dim;
         for (int by = f.by0; by <= f.by1; ++by) {
@@ -278,11 +357,10 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int gr
         const bool has_wl = i < p.num_movable;
         float gx = 0.f, gy = 0.f;
         if (has_wl) {
-            for (int t = p.node_start[i]; t < p.node_start[i + 1]; ++t) {
-                const int pin = p.node_pins[t];
-                if (p.pin2net[pin] < 0) continue;
-                gx = fadd(gx, p.gpx[pin]);
-                gy = fadd(gy, p.gpy[pin]);
+            const int s1 = p.slot_start[i + 1];
+            for (int t = p.slot_start[i]; t < s1; ++t) {
+                gx = fadd(gx, p.gpx[t]);
+                gy = fadd(gy, p.gpy[t]);
             }
         }
         float fx, fy;
@@ -303,18 +381,15 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int gr
         if (has_wl) acc_wl += static_cast<double>(fadd(fabsf(gx), fabsf(gy)));
         acc_den += static_cast<double>(fadd(fabsf(fx), fabsf(fy)));
     }
-    acc_wl = block_sum(acc_wl);
-    acc_den = block_sum(acc_den);
-    if (threadIdx.x == 0) {
-        p.partials[SLOT_SUM_WL * RED_CAP + blockIdx.x] = acc_wl;
-        p.partials[SLOT_SUM_DEN * RED_CAP + blockIdx.x] = acc_den;
-    }
+    double v2[2] = {acc_wl, acc_den};
+    block_sums(v2);
+    put_partial(p, SLOT_SUM_WL, v2[0]);
+    put_partial(p, SLOT_SUM_DEN, v2[1]);
     if (!last_block(&p.st->tk_assemble)) return;
-    const double over = finalize(p, SLOT_OVERFLOW);
-    const double wl = finalize(p, SLOT_WL);
-    const double hp = finalize(p, SLOT_HPWL);
-    const double swl = finalize(p, SLOT_SUM_WL);
-    const double sden = finalize(p, SLOT_SUM_DEN);
+    constexpr int kSlots[5] = {SLOT_OVERFLOW, SLOT_WL, SLOT_HPWL, SLOT_SUM_WL, SLOT_SUM_DEN};
+    double sums[5];
+    finalize_n(p, kSlots, sums);
+    const double over = sums[0], wl = sums[1], hp = sums[2], swl = sums[3], sden = sums[4];
     if (threadIdx.x != 0) return;
     DevState* st = p.st;
     st->tk_assemble = 0;
@@ -326,6 +401,34 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int gr
     if (!(isfinite(hp) && isfinite(st->tau) && isfinite(wl) && isfinite(swl) && isfinite(sden)))
         raise_error(st, SPG_E_NON_FINITE);
     if (count_eval && !st->done) st->evals += 1;
+}
+
+// The reduce kernel's last-block decisions on the state `st` (a shared-memory copy).
+__device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, double sy2, double gn2) {
+    st->tk_reduce = 0;
+    st->dx = sqrt(dx2);
+    st->dg = sqrt(dg2);
+    st->sy = sy2;
+    st->gn = gn2;
+    st->redo = 0;
+    if (!st->done && !st->error) {
+        if (p.backtrack && st->iter > 0 && st->tries < p.max_backtrack) {
+            const double ddx = st->dx, ddg = st->dg;
+            if (ddx > 0.0 && ddg > 0.0 && isfinite(ddg)) {
+                const double lip = ddx / ddg;
+                if (!(lip > 0.95 * static_cast<double>(st->alpha))) {
+                    st->alpha = static_cast<float>(lip);
+                    st->redo = 1;
+                    st->tries += 1;
+                    st->redos += 1;
+                }
+            }
+        }
+        if (!st->redo) {
+            decide_step(p, st);
+            decide_iteration(p, st);
+        }
+    }
 }
 
 // After every counted evaluation: |u-uPrev|^2, |g-gPrevTmp|^2, their dot and |g|^2
@@ -351,48 +454,25 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(DevPtrs p, int use_
         sy += __dmul_rn(s, y);
         gn += __dmul_rn(gv, gv);
     }
-    dx = block_sum(dx);
-    dg = block_sum(dg);
-    sy = block_sum(sy);
-    gn = block_sum(gn);
-    if (threadIdx.x == 0) {
-        p.partials[SLOT_DX * RED_CAP + blockIdx.x] = dx;
-        p.partials[SLOT_DG * RED_CAP + blockIdx.x] = dg;
-        p.partials[SLOT_SY * RED_CAP + blockIdx.x] = sy;
-        p.partials[SLOT_GN * RED_CAP + blockIdx.x] = gn;
-    }
+    double v4[4] = {dx, dg, sy, gn};
+    block_sums(v4);
+    dx = v4[0];
+    dg = v4[1];
+    sy = v4[2];
+    gn = v4[3];
+    put_partial(p, SLOT_DX, dx);
+    put_partial(p, SLOT_DG, dg);
+    put_partial(p, SLOT_SY, sy);
+    put_partial(p, SLOT_GN, gn);
     if (!last_block(&p.st->tk_reduce)) return;
-    const double dx2 = finalize(p, SLOT_DX);
-    const double dg2 = finalize(p, SLOT_DG);
-    const double sy2 = finalize(p, SLOT_SY);
-    const double gn2 = finalize(p, SLOT_GN);
-    if (threadIdx.x != 0) return;
-    DevState* st = p.st;
-    st->tk_reduce = 0;
-    st->dx = sqrt(dx2);
-    st->dg = sqrt(dg2);
-    st->sy = sy2;
-    st->gn = gn2;
-    st->redo = 0;
-    if (!st->done && !st->error) {
-        if (p.backtrack && st->iter > 0 && st->tries < p.max_backtrack) {
-            const double ddx = st->dx, ddg = st->dg;
-            if (ddx > 0.0 && ddg > 0.0 && isfinite(ddg)) {
-                const double lip = ddx / ddg;
-                if (!(lip > 0.95 * static_cast<double>(st->alpha))) {
-                    st->alpha = static_cast<float>(lip);
-                    st->redo = 1;
-                    st->tries += 1;
-                    st->redos += 1;
-                }
-            }
-        }
-        if (!st->redo) {
-            decide_step(p, st);
-            decide_iteration(p, st);
-        }
-    }
-    if (use_cond) cudaGraphSetConditional(redo_cond, st->redo ? 1u : 0u);
+    constexpr int kSlots[4] = {SLOT_DX, SLOT_DG, SLOT_SY, SLOT_GN};
+    double sums[4];
+    finalize_n(p, kSlots, sums);
+    __shared__ DevState sst;
+    state_copy_in(&sst, p.st);
+    if (threadIdx.x == 0) decide(p, &sst, sums[0], sums[1], sums[2], sums[3]);
+    state_copy_out(p.st, &sst);
+    if (threadIdx.x == 0 && use_cond) cudaGraphSetConditional(redo_cond, sst.redo ? 1u : 0u);
 }
 
 // Graph mode: the iteration loop continues while the stage is not done.
@@ -536,10 +616,8 @@ __global__ void __launch_bounds__(RED_THREADS) init_norms_kernel(DevPtrs p) {
     }
     pn = block_sum(pn);
     gn = block_sum(gn);
-    if (threadIdx.x == 0) {
-        p.partials[SLOT_PN * RED_CAP + blockIdx.x] = pn;
-        p.partials[SLOT_GN * RED_CAP + blockIdx.x] = gn;
-    }
+    put_partial(p, SLOT_PN, pn);
+    put_partial(p, SLOT_GN, gn);
 }
 
 // probe = clamp(u - (float)scale * gA) (nesterov.cpp:200-205); scale is in st->pn.
@@ -569,10 +647,8 @@ __global__ void __launch_bounds__(RED_THREADS) init_diff_kernel(DevPtrs p) {
     }
     dx = block_sum(dx);
     dg = block_sum(dg);
-    if (threadIdx.x == 0) {
-        p.partials[SLOT_DX * RED_CAP + blockIdx.x] = dx;
-        p.partials[SLOT_DG * RED_CAP + blockIdx.x] = dg;
-    }
+    put_partial(p, SLOT_DX, dx);
+    put_partial(p, SLOT_DG, dg);
 }
 
 // ------------------------------------------------------------------ control kernels
@@ -650,9 +726,18 @@ __global__ void finalize_slots_kernel(DevPtrs p, int first, int count, double* o
     }
 }
 
-inline int vec_blocks(const DevPtrs& p) {
-    const int b = ceil_div(2 * static_cast<int64_t>(p.n_opt), RED_THREADS);
-    return b < 1 ? 1 : (b > RED_BLOCKS ? RED_BLOCKS : b);
+// One full wave of RED_THREADS-thread blocks (reducing kernels: the partials' owners).
+template <typename K>
+inline int wave(K kernel) {
+    return wave_grid(reinterpret_cast<const void*>(kernel), RED_THREADS, RED_CAP);
+}
+
+// Element-wise kernels over 2*nOpt values: one thread per value up to one full wave.
+template <typename K>
+inline int vec_blocks(const DevPtrs& p, K kernel) {
+    const int64_t b = ceil_div(2 * static_cast<int64_t>(p.n_opt), RED_THREADS);
+    const int w = wave(kernel);
+    return b < 1 ? 1 : (b > w ? w : static_cast<int>(b));
 }
 
 }  // namespace
@@ -665,56 +750,56 @@ inline int vec_blocks(const DevPtrs& p) {
     } while (0)
 
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
-    LAUNCH(scatter_kernel, vec_blocks(p), RED_THREADS, p, role);
+    LAUNCH(scatter_kernel, vec_blocks(p, scatter_kernel), RED_THREADS, p, role);
 }
 void launch_assemble(const DevPtrs& p, int grad_role, int count_eval, cudaStream_t s) {
-    LAUNCH(assemble_kernel, RED_BLOCKS, RED_THREADS, p, grad_role, count_eval);
+    LAUNCH(assemble_kernel, wave(assemble_kernel), RED_THREADS, p, grad_role, count_eval);
 }
 void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond, cudaGraphConditionalHandle redo_cond) {
-    LAUNCH(reduce_kernel, RED_BLOCKS, RED_THREADS, p, use_cond, redo_cond);
+    LAUNCH(reduce_kernel, wave(reduce_kernel), RED_THREADS, p, use_cond, redo_cond);
 }
 void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
     LAUNCH(loop_cond_kernel, 1, 1, p, loop_cond);
 }
 void launch_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(update_kernel, RED_BLOCKS, RED_THREADS, p);
+    LAUNCH(update_kernel, wave(update_kernel), RED_THREADS, p);
 }
 void launch_redo_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(redo_update_kernel, RED_BLOCKS, RED_THREADS, p);
+    LAUNCH(redo_update_kernel, wave(redo_update_kernel), RED_THREADS, p);
 }
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_lambda_init_kernel, 1, 1, p);
 }
 void launch_init_norms(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(init_norms_kernel, RED_BLOCKS, RED_THREADS, p);
+    LAUNCH(init_norms_kernel, wave(init_norms_kernel), RED_THREADS, p);
 }
 void launch_ctl_init_scale(const DevPtrs& p, float init_perturb, cudaStream_t s) {
     LAUNCH(ctl_init_scale_kernel, 1, RED_THREADS, p, init_perturb);
 }
 void launch_init_perturb(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(init_perturb_kernel, vec_blocks(p), RED_THREADS, p);
+    LAUNCH(init_perturb_kernel, vec_blocks(p, init_perturb_kernel), RED_THREADS, p);
 }
 void launch_init_diff(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(init_diff_kernel, RED_BLOCKS, RED_THREADS, p);
+    LAUNCH(init_diff_kernel, wave(init_diff_kernel), RED_THREADS, p);
 }
 void launch_ctl_init_finish(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_init_finish_kernel, 1, RED_THREADS, p);
 }
 void launch_copy_role(const DevPtrs& p, int dst, int src, cudaStream_t s) {
-    LAUNCH(copy_role_kernel, vec_blocks(p), RED_THREADS, p, dst, src);
+    LAUNCH(copy_role_kernel, vec_blocks(p, copy_role_kernel), RED_THREADS, p, dst, src);
 }
 void launch_clamp_role(const DevPtrs& p, int role, cudaStream_t s) {
-    LAUNCH(clamp_role_kernel, vec_blocks(p), RED_THREADS, p, role);
+    LAUNCH(clamp_role_kernel, vec_blocks(p, clamp_role_kernel), RED_THREADS, p, role);
 }
 void launch_deliver(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(deliver_kernel, vec_blocks(p), RED_THREADS, p);
+    LAUNCH(deliver_kernel, vec_blocks(p, deliver_kernel), RED_THREADS, p);
 }
 void launch_stage_clock(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_stage_start_kernel, 1, 1, p);
 }
 void launch_check_geometry(const DevPtrs& p, float lx, float ly, float hx, float hy, const float* w,
                            const float* h, cudaStream_t s) {
-    LAUNCH(check_geometry_kernel, vec_blocks(p), RED_THREADS, p, lx, ly, hx, hy, w, h);
+    LAUNCH(check_geometry_kernel, vec_blocks(p, check_geometry_kernel), RED_THREADS, p, lx, ly, hx, hy, w, h);
 }
 void launch_finalize_slots(const DevPtrs& p, int first, int count, double* out, cudaStream_t s) {
     LAUNCH(finalize_slots_kernel, 1, RED_THREADS, p, first, count, out);

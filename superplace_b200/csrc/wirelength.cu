@@ -20,9 +20,6 @@ namespace spg {
 
 namespace {
 
-constexpr int kWaBlocks = 1024;
-static_assert(kWaBlocks <= RED_CAP, "WA partials exceed the reduction capacity");
-
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -100,8 +97,8 @@ __device__ void wa_warp_net(const DevPtrs& p, int k, float invG, double& wl, dou
     if (lane == 0) hp += static_cast<double>(fsub(mxX, mnX)) + static_cast<double>(fsub(mxY, mnY));
     if (e - b > p.ignore_net_degree) {
         for (int q = b + lane; q < e; q += 32) {
-            p.gpx[p.net_pins[q]] = 0.f;
-            p.gpy[p.net_pins[q]] = 0.f;
+            p.gpx[p.net_slot[q]] = 0.f;
+            p.gpy[p.net_slot[q]] = 0.f;
         }
         return;
     }
@@ -125,14 +122,14 @@ __device__ void wa_warp_net(const DevPtrs& p, int k, float invG, double& wl, dou
     for (int i = 0; i < 8; ++i) s[i] = group_sum(s[i], 32);
     if (lane == 0) wl += wa_value(mxX, mnX, mxY, mnY, s);
     for (int q = b + lane; q < e; q += 32) {
-        const int pin = p.net_pins[q];
         float px, py;
-        pin_xy(p, pin, px, py);
+        pin_xy(p, p.net_pins[q], px, py);
         const float dxp = fsub(px, mxX), dxn = fsub(px, mnX), dyp = fsub(py, mxY), dyn = fsub(py, mnY);
         const float ap = expf(fmul(dxp, invG)), an = expf(fmul(-dxn, invG));
         const float bp = expf(fmul(dyp, invG)), bn = expf(fmul(-dyn, invG));
-        p.gpx[pin] = wa_pin_term(dxp, dxn, ap, an, s[0], s[2], s[1], s[3], invG);
-        p.gpy[pin] = wa_pin_term(dyp, dyn, bp, bn, s[4], s[6], s[5], s[7], invG);
+        const int sl = p.net_slot[q];
+        p.gpx[sl] = wa_pin_term(dxp, dxn, ap, an, s[0], s[2], s[1], s[3], invG);
+        p.gpy[sl] = wa_pin_term(dyp, dyn, bp, bn, s[4], s[6], s[5], s[7], invG);
     }
 }
 
@@ -167,6 +164,7 @@ __global__ void __launch_bounds__(RED_THREADS) wa_net_kernel(DevPtrs p, const fl
         const int deg = net_ok ? p.net_start[k + 1] - b : 0;
         const bool act = gl < deg;
         const int pin = act ? p.net_pins[b + gl] : 0;
+        const int sl = act ? p.net_slot[b + gl] : 0;
         float px = 0.f, py = 0.f;
         if (act) pin_xy(p, pin, px, py);
         const float mxX = group_max(act ? px : -FLT_MAX, G), mnX = group_min(act ? px : FLT_MAX, G);
@@ -183,28 +181,24 @@ __global__ void __launch_bounds__(RED_THREADS) wa_net_kernel(DevPtrs p, const fl
 #pragma unroll
         for (int i = 0; i < 8; ++i) s[i] = group_sum(s[i], G);
         if (act) {
-            p.gpx[pin] = live ? wa_pin_term(dxp, dxn, ap, an, s[0], s[2], s[1], s[3], invG) : 0.f;
-            p.gpy[pin] = live ? wa_pin_term(dyp, dyn, bp, bn, s[4], s[6], s[5], s[7], invG) : 0.f;
+            p.gpx[sl] = live ? wa_pin_term(dxp, dxn, ap, an, s[0], s[2], s[1], s[3], invG) : 0.f;
+            p.gpy[sl] = live ? wa_pin_term(dyp, dyn, bp, bn, s[4], s[6], s[5], s[7], invG) : 0.f;
         }
         if (gl == 0 && wa_on) wl += wa_value(mxX, mnX, mxY, mnY, s);
     }
     wl = block_sum_d(wl, ws);
     hp = block_sum_d(hp, ws);
-    if (threadIdx.x == 0) {
-        p.partials[SLOT_WL * RED_CAP + blockIdx.x] = wl;
-        p.partials[SLOT_HPWL * RED_CAP + blockIdx.x] = hp;
-    }
+    put_partial(p, SLOT_WL, wl);
+    put_partial(p, SLOT_HPWL, hp);
 }
 
 __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.num_movable) return;
     float gx = 0.f, gy = 0.f;
-    for (int t = p.node_start[i]; t < p.node_start[i + 1]; ++t) {
-        const int pin = p.node_pins[t];
-        if (p.pin2net[pin] < 0) continue;
-        gx = fadd(gx, p.gpx[pin]);
-        gy = fadd(gy, p.gpy[pin]);
+    for (int t = p.slot_start[i]; t < p.slot_start[i + 1]; ++t) {
+        gx = fadd(gx, p.gpx[t]);
+        gy = fadd(gy, p.gpy[t]);
     }
     grad[i] = gx;
     grad[p.num_movable + i] = gy;
@@ -214,8 +208,9 @@ __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
 
 void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, int use_dev,
                     cudaStream_t s) {
-    // a fixed grid (RED_CAP blocks) so the FP64 partials keep a fixed owner per block
-    wa_net_kernel<<<kWaBlocks, RED_THREADS, 0, s>>>(p, gamma_dev, gamma_host, use_dev);
+    // one full wave, fixed per device, so the FP64 partials keep a fixed owner per block
+    const int grid = wave_grid(reinterpret_cast<const void*>(wa_net_kernel), RED_THREADS, RED_CAP);
+    wa_net_kernel<<<grid, RED_THREADS, 0, s>>>(p, gamma_dev, gamma_host, use_dev);
     count_launch();
     SPG_CHECK_LAUNCH();
 }
