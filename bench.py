@@ -12,7 +12,8 @@ src/gp/eplace.cpp:310,515).
          bracketed by CUDA events on the engine's stream
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                       [--precision fp32|bf16x3] [--workload large|small]
+                       [--precision bf16x3|fp32] [--workload large|small]
+The default Poisson arithmetic is split-BF16 on tcgen05 (bf16x3); fp32 is the plain FP32 form.
 Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
 """
 from __future__ import annotations
@@ -355,7 +356,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16x3"])
+    ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16x3"])
     ap.add_argument("--workload", default="large", choices=list(WORKLOADS))
     ap.add_argument("--ref-iters", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
