@@ -194,14 +194,14 @@ def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision):
       scatter    25 B per density node + 16 B per bin (two 64-bit maps)
       rho        44 B per bin (maps, terminal, base in; rho out; maps cleared)
       poisson    14 M^3 flops (16 B per bin of I/O)
-      assemble   60 B per optimised node + 16 B per pin
-      reduce     32 B per optimised node (u, uPrev, g, gPrevTmp)
+      assemble   76 B per optimised node + 16 B per pin (WA pass 2, gather, gradient, and
+                 the step's norms over uPrev and gPrevTmp)
     """
     n_opt = db.num_movable + db.num_fillers
     n_dens = n_opt
     pins, nets, bins = db.num_pins, db.num_nets, dim * dim
     by = {"update": 68 * n_opt, "wa": 32 * pins + 8 * nets, "scatter": 25 * n_dens + 16 * bins,
-          "rho": 44 * bins, "assemble": 60 * n_opt + 16 * pins, "reduce": 32 * n_opt}
+          "rho": 44 * bins, "assemble": 76 * n_opt + 16 * pins}
     out = {}
     for k, us in parts.items():
         if k == "poisson":

@@ -7,6 +7,7 @@
 
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 #include "spgpu.h"
 
@@ -38,6 +39,36 @@ extern int64_t g_launches;
 inline void count_launch(int n = 1) { g_launches += n; }
 
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------------------
+// Programmatic dependent launch. A kernel launched by launch_pdl may begin while the kernel
+// before it on the stream is still finishing: its blocks get scheduled (and may run a
+// prologue that touches no global data) as soon as every block of the earlier kernel has
+// called pdl_trigger() or exited. pdl_wait() then blocks until the earlier kernel has
+// completed and its memory is visible, so every kernel calls it before its first global
+// access. In a kernel launched without the attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// False when SPG_PDL=0 (every launch then waits for the previous kernel as usual).
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SPG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+    count_launch();
+}
 
 // ---------------------------------------------------------------------------------------
 // Float arithmetic with explicit round-to-nearest intrinsics: no FMA contraction, so every

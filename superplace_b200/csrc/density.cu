@@ -21,6 +21,8 @@ namespace {
 constexpr int kThreads = 256;
 
 __global__ void __launch_bounds__(kThreads) acc_small_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= p.n_dens_small) return;
     const int i = p.dens_small[t];
@@ -40,6 +42,8 @@ __global__ void __launch_bounds__(kThreads) acc_small_kernel(DevPtrs p) {
 
 // One block per large node (macros): the block's threads split its footprint's bins.
 __global__ void __launch_bounds__(kThreads) acc_large_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const int i = p.dens_large[blockIdx.x];
     const GridGeom& g = p.geom;
     const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
@@ -85,6 +89,8 @@ __device__ __forceinline__ double block_sum(double v) {
 // evaluation when `zero` is set.
 __global__ void __launch_bounds__(RED_THREADS) rho_overflow_kernel(DevPtrs p, int write_maps,
                                                                    int zero) {
+    pdl_wait();
+    pdl_trigger();
     const GridGeom& g = p.geom;
     const size_t n = static_cast<size_t>(g.dim) * g.dim;
     const float bin_area_f = fmul(g.step_x, g.step_y);
@@ -173,6 +179,8 @@ __device__ __forceinline__ void gather_large(const DevPtrs& p, int i, float& fx,
 }
 
 __global__ void __launch_bounds__(kThreads) gather_opt_large_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const int k = p.opt_large[blockIdx.x];
     float fx, fy;
     gather_large(p, p.opt_idx[k], fx, fy);
@@ -183,6 +191,8 @@ __global__ void __launch_bounds__(kThreads) gather_opt_large_kernel(DevPtrs p) {
 }
 
 __global__ void __launch_bounds__(kThreads) gather_all_small_kernel(DevPtrs p, float* out) {
+    pdl_wait();
+    pdl_trigger();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= p.n_dens_small) return;
     const int i = p.dens_small[t];
@@ -193,6 +203,8 @@ __global__ void __launch_bounds__(kThreads) gather_all_small_kernel(DevPtrs p, f
 }
 
 __global__ void __launch_bounds__(kThreads) gather_all_large_kernel(DevPtrs p, float* out) {
+    pdl_wait();
+    pdl_trigger();
     const int i = p.dens_large[blockIdx.x];
     float fx, fy;
     gather_large(p, i, fx, fy);
@@ -206,41 +218,31 @@ __global__ void __launch_bounds__(kThreads) gather_all_large_kernel(DevPtrs p, f
 
 void launch_density_accumulate(const DevPtrs& p, cudaStream_t s) {
     if (p.n_dens_small > 0) {
-        acc_small_kernel<<<ceil_div(p.n_dens_small, kThreads), kThreads, 0, s>>>(p);
-        count_launch();
+        launch_pdl(acc_small_kernel, dim3(ceil_div(p.n_dens_small, kThreads)), dim3(kThreads), 0, s, p);
     }
     if (p.n_dens_large > 0) {
-        acc_large_kernel<<<p.n_dens_large, kThreads, 0, s>>>(p);
-        count_launch();
+        launch_pdl(acc_large_kernel, dim3(p.n_dens_large), dim3(kThreads), 0, s, p);
     }
-    SPG_CHECK_LAUNCH();
 }
 
 void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s) {
     const int grid = wave_grid(reinterpret_cast<const void*>(rho_overflow_kernel), RED_THREADS, RED_CAP);
-    rho_overflow_kernel<<<grid, RED_THREADS, 0, s>>>(p, write_maps, zero);
-    count_launch();
-    SPG_CHECK_LAUNCH();
+    launch_pdl(rho_overflow_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, write_maps, zero);
 }
 
 void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s) {
     if (p.n_opt_large > 0) {
-        gather_opt_large_kernel<<<p.n_opt_large, kThreads, 0, s>>>(p);
-        count_launch();
+        launch_pdl(gather_opt_large_kernel, dim3(p.n_opt_large), dim3(kThreads), 0, s, p);
     }
-    SPG_CHECK_LAUNCH();
 }
 
 void launch_gather_all(const DevPtrs& p, float* out, cudaStream_t s) {
     if (p.n_dens_small > 0) {
-        gather_all_small_kernel<<<ceil_div(p.n_dens_small, kThreads), kThreads, 0, s>>>(p, out);
-        count_launch();
+        launch_pdl(gather_all_small_kernel, dim3(ceil_div(p.n_dens_small, kThreads)), dim3(kThreads), 0, s, p, out);
     }
     if (p.n_dens_large > 0) {
-        gather_all_large_kernel<<<p.n_dens_large, kThreads, 0, s>>>(p, out);
-        count_launch();
+        launch_pdl(gather_all_large_kernel, dim3(p.n_dens_large), dim3(kThreads), 0, s, p, out);
     }
-    SPG_CHECK_LAUNCH();
 }
 
 }  // namespace spg

@@ -28,6 +28,14 @@ namespace spg {
 
 int64_t g_launches = 0;
 
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("SPG_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 int wave_grid(const void* kernel, int threads, int cap) {
     struct Entry {
         const void* kernel;
@@ -154,6 +162,10 @@ struct Context {
     // stage
     int n_opt = 0;
     DevBuf<int> opt_idx, opt_deg, opt_small, opt_large;
+    DevBuf<float4> opt_geom;
+    DevBuf<int4> opt_meta;
+    std::vector<float> hw_h, hh_h, wgt_h;  // per-node footprint data of the current grid
+    std::vector<int> slot_start_h;         // node-order pin slots (see DevPtrs::slot_start)
     DevBuf<float> opt_lo, opt_hi, force, pool;
     DevBuf<double> opt_area;
     int n_opt_small = 0, n_opt_large = 0;
@@ -224,6 +236,8 @@ struct Context {
         p.movable_area_scaled = movable_area_scaled;
         p.n_opt = n_opt;
         p.opt_idx = opt_idx.p;
+        p.opt_geom = opt_geom.p;
+        p.opt_meta = opt_meta.p;
         p.opt_lo = opt_lo.p;
         p.opt_hi = opt_hi.p;
         p.opt_deg = opt_deg.p;
@@ -394,6 +408,9 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     c.hw.upload(hw, st);
     c.hh.upload(hh, st);
     c.wgt.upload(wgt, st);
+    c.hw_h = hw;
+    c.hh_h = hh;
+    c.wgt_h = wgt;
     c.kind.upload(kind, st);
     c.dens_small.upload(dsmall, st);
     c.dens_large.upload(dlarge, st);
@@ -437,6 +454,8 @@ void stage_setup(Context& c, int stage) {
     std::vector<float> lo(2 * static_cast<size_t>(n)), hi(2 * static_cast<size_t>(n));
     std::vector<int> deg(n), osmall, olarge;
     std::vector<double> area(n);
+    std::vector<float4> geom(n);
+    std::vector<int4> meta(n);
     std::vector<uint8_t> kind(c.total);
     SPG_CUDA(cudaMemcpyAsync(kind.data(), c.kind.p, c.total, cudaMemcpyDeviceToHost, c.stream));
     SPG_CUDA(cudaStreamSynchronize(c.stream));
@@ -454,6 +473,10 @@ void stage_setup(Context& c, int stage) {
         deg[k] = c.node_start[i + 1] - c.node_start[i];
         area[k] = static_cast<double>(c.w[i]) * static_cast<double>(c.h[i]);
         (kind[i] & K_LARGE ? olarge : osmall).push_back(k);
+        geom[k] = make_float4(c.hw_h[i], c.hh_h[i], c.wgt_h[i], 0.f);
+        const bool has_wl = i < c.num_movable;
+        meta[k] = make_int4(c.slot_start_h[i], has_wl ? c.slot_start_h[i + 1] : c.slot_start_h[i], deg[k],
+                            static_cast<int>(kind[i]) | (has_wl ? OPT_HAS_WL : 0));
     }
     cudaStream_t s = c.stream;
     c.opt_idx.upload(opt, s);
@@ -461,6 +484,8 @@ void stage_setup(Context& c, int stage) {
     c.opt_hi.upload(hi, s);
     c.opt_deg.upload(deg, s);
     c.opt_area.upload(area, s);
+    c.opt_geom.upload(geom, s);
+    c.opt_meta.upload(meta, s);
     c.opt_small.upload(osmall, s);
     c.opt_large.upload(olarge, s);
     c.n_opt_small = static_cast<int>(osmall.size());
@@ -483,7 +508,8 @@ void stage_setup(Context& c, int stage) {
 // by the update kernels; pos_role >= 0 scatters that role first), gradient into grad_role.
 // The WA pass 1 depends only on the positions, so it runs on a side stream, overlapping
 // the density -> Poisson chain; the assembly joins both.
-void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count) {
+void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count, bool fused_reduce = false,
+              int use_cond = 0, cudaGraphConditionalHandle redo_h = 0) {
     cudaStream_t s = c.stream;
     if (pos_role >= 0) launch_scatter(p, pos_role, s);
     SPG_CUDA(cudaEventRecord(c.ev_fork, s));
@@ -495,7 +521,8 @@ void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int cou
     poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s);
     launch_gather_opt_large(p, s);
     SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
-    launch_assemble(p, grad_role, count, s);
+    if (fused_reduce) launch_assemble_reduce(p, s, use_cond, redo_h);
+    else launch_assemble(p, pos_role >= 0 ? pos_role : R_U, grad_role, count, s);
 }
 
 void read_state(Context& c) {
@@ -602,16 +629,14 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
 void enqueue_iteration(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
     cudaStream_t s = c.stream;
     launch_update(p, s);
-    evaluate(c, p, -1, R_G, 1);
-    launch_reduce(p, s, use_cond, redo_h);
+    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h);
 }
 
 // One redoIfOvershot re-evaluation (nesterov.cpp:158-166) and the next redo test.
 void enqueue_redo(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
     cudaStream_t s = c.stream;
     launch_redo_update(p, s);
-    evaluate(c, p, -1, R_G, 1);
-    launch_reduce(p, s, use_cond, redo_h);
+    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h);
 }
 
 // Host-driven loop: one 16-byte state read per iteration (and per re-evaluation).
@@ -818,8 +843,7 @@ void stage_run(Context& c, int stage, spg_result* res) {
     launch_ctl_init_finish(p, s);
 
     // first evaluation of iteration 0, its norms, and the redo test (a no-op at iteration 0)
-    evaluate(c, p, R_U, R_G, 1);
-    launch_reduce(p, s);
+    evaluate(c, p, R_U, R_G, 1, true);
     c.last_run_graph = false;
     if (max_iter > 0) {
         c.last_run_graph = c.use_graph && graph_loop(c, p);
@@ -1191,6 +1215,7 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
             net_slot[q] = sl >= 0 ? sl : slots;
         }
         c.slot_start.upload(slot_start, s);
+        c.slot_start_h = slot_start;
         c.net_slot.upload(net_slot, s);
         c.num_slots = slots;
     }
@@ -1512,12 +1537,13 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     t[2] = time([&] { spg::launch_density_accumulate(p, s); }, zero_maps);
     t[3] = time([&] { spg::launch_rho_overflow(p, 0, 1, s); }, [&] { spg::launch_density_accumulate(p, s); });
     t[4] = time([&] { spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s); }, nothing);
+    // the loop's assembly carries the norms and decisions of the reduce step (part 6 = 0)
     t[5] = time([&] {
         spg::launch_gather_opt_large(p, s);
-        spg::launch_assemble(p, spg::R_GB, 0, s);
+        spg::launch_assemble_reduce(p, s);
     }, nothing);
-    t[6] = time([&] { spg::launch_reduce(p, s); }, nothing);
-    t[7] = time([&] { spg::evaluate(c, p, -1, spg::R_GB, 0); }, nothing);
+    t[6] = 0.0;
+    t[7] = time([&] { spg::evaluate(c, p, -1, spg::R_G, 1, true); }, nothing);
     spg::g_launches = launches0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -49,6 +49,7 @@ enum RedSlot : int {
 constexpr uint8_t K_DENSITY = 1;  // contributes density (not fixed, not NI)
 constexpr uint8_t K_FILLER = 2;
 constexpr uint8_t K_LARGE = 4;    // footprint may exceed 16 bins: block-per-node kernels
+constexpr int OPT_HAS_WL = 0x100;  // opt_meta flag: a movable node (it owns the WA gradient)
 
 // optimizer vector roles
 enum Role : int {
@@ -138,6 +139,11 @@ struct DevPtrs {
     const float* opt_hi;
     const int* opt_deg;    // nodeDegree of the opt node
     const double* opt_area;
+    // stage-static attributes of opt node k packed for one load each:
+    //   opt_geom[k] = {hw, hh, wgt, 0} of its node (smoothed half extents, charge weight)
+    //   opt_meta[k] = {first pin slot, end pin slot, nodeDegree, kind | OPT_HAS_WL}
+    const float4* opt_geom;
+    const int4* opt_meta;
     float* force;          // 2*nOpt, density force q*xi (not gradient)
     float* pool;           // NUM_ROLES + SNAP_MAX vectors of 2*nOpt
     size_t vec_stride;
@@ -187,7 +193,11 @@ void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s);
 // ---- optimizer.cu
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s);
 // WA pass 2 + cell gather + gradient assembly; its last block finalizes the evaluation
-void launch_assemble(const DevPtrs& p, int grad_role, int count_eval, cudaStream_t s);
+void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s);
+// the loop's evaluation tail: the assembly at u = R_U into g = R_G fused with the reduce
+// kernel's norms and decisions (one launch instead of two)
+void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
+                            cudaGraphConditionalHandle redo_cond = 0);
 // norms of the last evaluation; its last block runs the redo test and the iteration decisions
 void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
                    cudaGraphConditionalHandle redo_cond = 0);

@@ -288,6 +288,8 @@ __device__ void decide_iteration(const DevPtrs& p, DevState* st) {
 // ------------------------------------------------------------------ vector kernels
 
 __global__ void scatter_kernel(DevPtrs p, int role) {
+    pdl_wait();
+    pdl_trigger();
     const float* u = role_ptr(p, role);
     const int n = p.n_opt;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -302,12 +304,14 @@ __global__ void scatter_kernel(DevPtrs p, int role) {
 
 // force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it
 // (bin_grid.cpp:287-318).
-// Footprints of at most 2x2 bins (every cell no wider than one bin) issue their eight field
-// loads before the sums, which keep the reference's order.
-__device__ __forceinline__ void gather_node(const DevPtrs& p, int i, float& fx, float& fy) {
+// force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it
+// (bin_grid.cpp:287-318), for a node at (x, y) with smoothed half extents hw, hh and charge
+// weight w. Footprints of at most 2x2 bins (every cell no wider than one bin) issue their
+// eight field loads before the sums, which keep the reference's order.
+__device__ __forceinline__ void gather_at(const DevPtrs& p, float x, float y, float hw, float hh,
+                                          float w, float& fx, float& fy) {
     const GridGeom& g = p.geom;
-    const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
-    const float w = p.wgt[i];
+    const Footprint f = footprint(g, x, y, hw, hh);
     fx = 0.f;
     fy = 0.f;
     if (f.bx1 - f.bx0 <= 1 && f.by1 - f.by0 <= 1) {
@@ -342,68 +346,23 @@ __device__ __forceinline__ void gather_node(const DevPtrs& p, int i, float& fx, 
     }
 }
 
-// grad_k = precond * (dWL - lambda * q*xi), precond = 1 / max(1, deg + lambda*area)
-// (eplace.cpp:166-189), with the WA pass 2 (per-node sum of per-pin contributions in
-// node->pin order, wa_wirelength.cpp:137-179) and the field gather of cells fused in (large
-// nodes' force comes from gather_opt_large). The last block finalizes the evaluation
-// (eplace.cpp:149,154-155,190-197).
-__global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int grad_role, int count_eval) {
-    float* grad = role_ptr(p, grad_role);
-    const float lambda = p.st->lambda;
-    const int n = p.n_opt;
-    double acc_wl = 0.0, acc_den = 0.0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int i = p.opt_idx[k];
-        const bool has_wl = i < p.num_movable;
-        float gx = 0.f, gy = 0.f;
-        if (has_wl) {
-            const int s1 = p.slot_start[i + 1];
-            for (int t = p.slot_start[i]; t < s1; ++t) {
-                gx = fadd(gx, p.gpx[t]);
-                gy = fadd(gy, p.gpy[t]);
-            }
-        }
-        float fx, fy;
-        if (p.kind[i] & K_LARGE) {
-            fx = p.force[k];
-            fy = p.force[n + k];
-        } else {
-            gather_node(p, i, fx, fy);
-        }
-        const double den = __dadd_rn(static_cast<double>(p.opt_deg[k]),
-                                     __dmul_rn(static_cast<double>(lambda), p.opt_area[k]));
-        const float precond = static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
-        const float ox = fmul(precond, fsub(gx, fmul(lambda, fx)));
-        const float oy = fmul(precond, fsub(gy, fmul(lambda, fy)));
-        grad[k] = ox;
-        grad[n + k] = oy;
-        if (!isfinite(ox) || !isfinite(oy)) raise_error(p.st, SPG_E_NON_FINITE);
-        if (has_wl) acc_wl += static_cast<double>(fadd(fabsf(gx), fabsf(gy)));
-        acc_den += static_cast<double>(fadd(fabsf(fx), fabsf(fy)));
-    }
-    double v2[2] = {acc_wl, acc_den};
-    block_sums(v2);
-    put_partial(p, SLOT_SUM_WL, v2[0]);
-    put_partial(p, SLOT_SUM_DEN, v2[1]);
-    if (!last_block(&p.st->tk_assemble)) return;
-    constexpr int kSlots[5] = {SLOT_OVERFLOW, SLOT_WL, SLOT_HPWL, SLOT_SUM_WL, SLOT_SUM_DEN};
-    double sums[5];
-    finalize_n(p, kSlots, sums);
-    const double over = sums[0], wl = sums[1], hp = sums[2], swl = sums[3], sden = sums[4];
-    if (threadIdx.x != 0) return;
-    DevState* st = p.st;
+// The finalized evaluation (eplace.cpp:149,154-155,190-197) into the state: tau from the
+// overflow sum, HPWL, WA value and the two gradient-norm sums; s = {overflow, WA, HPWL,
+// sum|dWL|, sum|q xi|}.
+__device__ void finish_evaluation(const DevPtrs& p, DevState* st, const double* s, int count_eval) {
     st->tk_assemble = 0;
-    st->tau = p.movable_area_scaled > 0.0 ? static_cast<float>(over / p.movable_area_scaled) : 0.f;
-    st->hpwl = hp;
-    st->wl_obj = wl;
-    st->sum_wl = swl;
-    st->sum_den = sden;
-    if (!(isfinite(hp) && isfinite(st->tau) && isfinite(wl) && isfinite(swl) && isfinite(sden)))
+    st->tau = p.movable_area_scaled > 0.0 ? static_cast<float>(s[0] / p.movable_area_scaled) : 0.f;
+    st->hpwl = s[2];
+    st->wl_obj = s[1];
+    st->sum_wl = s[3];
+    st->sum_den = s[4];
+    if (!(isfinite(s[2]) && isfinite(st->tau) && isfinite(s[1]) && isfinite(s[3]) && isfinite(s[4])))
         raise_error(st, SPG_E_NON_FINITE);
     if (count_eval && !st->done) st->evals += 1;
 }
 
-// The reduce kernel's last-block decisions on the state `st` (a shared-memory copy).
+// The decisions after a counted evaluation, on the state `st` (a shared-memory copy): the
+// redo test and, when no re-evaluation is due, the step and iteration decisions.
 __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, double sy2, double gn2) {
     st->tk_reduce = 0;
     st->dx = sqrt(dx2);
@@ -431,6 +390,115 @@ __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, d
     }
 }
 
+// grad_k = precond * (dWL - lambda * q*xi), precond = 1 / max(1, deg + lambda*area)
+// (eplace.cpp:166-189), with the WA pass 2 (per-node sum of per-pin contributions in
+// node->pin order, wa_wirelength.cpp:137-179) and the field gather of cells fused in (large
+// nodes' force comes from gather_opt_large). The last block finalizes the evaluation
+// (eplace.cpp:149,154-155,190-197).
+//
+// FUSE (the iteration loop's evaluations, at u = R_U into g = R_G): the same pass also forms
+// reduce_kernel's four norms |u-uPrev|^2, |g-gPrevTmp|^2, (u-uPrev).(g-gPrevTmp), |g|^2 from
+// the values it holds, and its last block runs the decisions after the evaluation's
+// finalize, as the separate reduce kernel would.
+template <bool FUSE>
+__global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int pos_role, int grad_role,
+                                                              int count_eval, int use_cond,
+                                                              cudaGraphConditionalHandle redo_cond) {
+    pdl_wait();
+    pdl_trigger();
+    // the evaluated positions, by opt index: the role the update (or scatter) wrote the
+    // node coordinates from, so pos[k] == x[opt_idx[k]] bit for bit
+    const float* __restrict__ pos = role_ptr(p, pos_role);
+    float* __restrict__ grad = role_ptr(p, grad_role);
+    const float* __restrict__ up = FUSE ? role_ptr(p, R_UPREV) : nullptr;
+    const float* __restrict__ gp = FUSE ? role_ptr(p, R_GPREVTMP) : nullptr;
+    const float lambda = p.st->lambda;
+    const int n = p.n_opt;
+    double acc_wl = 0.0, acc_den = 0.0;
+    double dx = 0.0, dg = 0.0, sy = 0.0, gn = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int4 meta = p.opt_meta[k];
+        const float4 geo = p.opt_geom[k];
+        const float x = pos[k], y = pos[n + k];
+        const double area = p.opt_area[k];
+        float upx = 0.f, upy = 0.f, gpx = 0.f, gpy = 0.f;
+        if (FUSE) {
+            upx = up[k];
+            upy = up[n + k];
+            gpx = gp[k];
+            gpy = gp[n + k];
+        }
+        float gx = 0.f, gy = 0.f;
+        for (int t = meta.x; t < meta.y; ++t) {
+            gx = fadd(gx, p.gpx[t]);
+            gy = fadd(gy, p.gpy[t]);
+        }
+        float fx, fy;
+        if (meta.w & K_LARGE) {
+            fx = p.force[k];
+            fy = p.force[n + k];
+        } else {
+            gather_at(p, x, y, geo.x, geo.y, geo.z, fx, fy);
+        }
+        const double den = __dadd_rn(static_cast<double>(meta.z), __dmul_rn(static_cast<double>(lambda), area));
+        const float precond = static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
+        const float ox = fmul(precond, fsub(gx, fmul(lambda, fx)));
+        const float oy = fmul(precond, fsub(gy, fmul(lambda, fy)));
+        grad[k] = ox;
+        grad[n + k] = oy;
+        if (!isfinite(ox) || !isfinite(oy)) raise_error(p.st, SPG_E_NON_FINITE);
+        if (meta.w & OPT_HAS_WL) acc_wl += static_cast<double>(fadd(fabsf(gx), fabsf(gy)));
+        acc_den += static_cast<double>(fadd(fabsf(fx), fabsf(fy)));
+        if (FUSE) {
+            // l2Diff, dotDiff, l2Norm terms (nesterov.cpp:25-45), x then y
+            const double sxd = static_cast<double>(x) - static_cast<double>(upx);
+            const double syd = static_cast<double>(y) - static_cast<double>(upy);
+            const double yx = static_cast<double>(ox) - static_cast<double>(gpx);
+            const double yy = static_cast<double>(oy) - static_cast<double>(gpy);
+            dx += __dmul_rn(sxd, sxd) + __dmul_rn(syd, syd);
+            dg += __dmul_rn(yx, yx) + __dmul_rn(yy, yy);
+            sy += __dmul_rn(sxd, yx) + __dmul_rn(syd, yy);
+            gn += __dmul_rn(static_cast<double>(ox), static_cast<double>(ox)) +
+                  __dmul_rn(static_cast<double>(oy), static_cast<double>(oy));
+        }
+    }
+    if (FUSE) {
+        double v6[6] = {acc_wl, acc_den, dx, dg, sy, gn};
+        block_sums(v6);
+        put_partial(p, SLOT_SUM_WL, v6[0]);
+        put_partial(p, SLOT_SUM_DEN, v6[1]);
+        put_partial(p, SLOT_DX, v6[2]);
+        put_partial(p, SLOT_DG, v6[3]);
+        put_partial(p, SLOT_SY, v6[4]);
+        put_partial(p, SLOT_GN, v6[5]);
+    } else {
+        double v2[2] = {acc_wl, acc_den};
+        block_sums(v2);
+        put_partial(p, SLOT_SUM_WL, v2[0]);
+        put_partial(p, SLOT_SUM_DEN, v2[1]);
+    }
+    if (!last_block(&p.st->tk_assemble)) return;
+    if (!FUSE) {
+        constexpr int kSlots[5] = {SLOT_OVERFLOW, SLOT_WL, SLOT_HPWL, SLOT_SUM_WL, SLOT_SUM_DEN};
+        double sums[5];
+        finalize_n(p, kSlots, sums);
+        if (threadIdx.x == 0) finish_evaluation(p, p.st, sums, count_eval);
+        return;
+    }
+    constexpr int kSlots[9] = {SLOT_OVERFLOW, SLOT_WL, SLOT_HPWL, SLOT_SUM_WL, SLOT_SUM_DEN,
+                               SLOT_DX, SLOT_DG, SLOT_SY, SLOT_GN};
+    double sums[9];
+    finalize_n(p, kSlots, sums);
+    __shared__ DevState sst;
+    state_copy_in(&sst, p.st);
+    if (threadIdx.x == 0) {
+        finish_evaluation(p, &sst, sums, count_eval);
+        decide(p, &sst, sums[5], sums[6], sums[7], sums[8]);
+    }
+    state_copy_out(p.st, &sst);
+    if (threadIdx.x == 0 && use_cond) cudaGraphSetConditional(redo_cond, sst.redo ? 1u : 0u);
+}
+
 // After every counted evaluation: |u-uPrev|^2, |g-gPrevTmp|^2, their dot and |g|^2
 // (l2Diff, dotDiff, l2Norm: nesterov.cpp:25-45) in one pass; the last block then runs
 // redoIfOvershot's test (nesterov.cpp:148-157) -- redo when 1/L at the new point is at
@@ -439,21 +507,36 @@ __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, d
 // mode it sets the re-evaluation loop's conditional handle.
 __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(DevPtrs p, int use_cond,
                                                             cudaGraphConditionalHandle redo_cond) {
-    const float* u = role_ptr(p, R_U);
-    const float* up = role_ptr(p, R_UPREV);
-    const float* g = role_ptr(p, R_G);
-    const float* gp = role_ptr(p, R_GPREVTMP);
-    const int n = 2 * p.n_opt;
+    pdl_wait();
+    pdl_trigger();
+    const float* __restrict__ u = role_ptr(p, R_U);
+    const float* __restrict__ up = role_ptr(p, R_UPREV);
+    const float* __restrict__ g = role_ptr(p, R_G);
+    const float* __restrict__ gp = role_ptr(p, R_GPREVTMP);
+    const int n = 2 * p.n_opt, n4 = n >> 2;
     double dx = 0.0, dg = 0.0, sy = 0.0, gn = 0.0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const double s = static_cast<double>(u[k]) - static_cast<double>(up[k]);
-        const double y = static_cast<double>(g[k]) - static_cast<double>(gp[k]);
-        const double gv = static_cast<double>(g[k]);
+    auto term = [&](float a, float b, float c, float d) {
+        const double s = static_cast<double>(a) - static_cast<double>(b);
+        const double y = static_cast<double>(c) - static_cast<double>(d);
+        const double gv = static_cast<double>(c);
         dx += __dmul_rn(s, s);
         dg += __dmul_rn(y, y);
         sy += __dmul_rn(s, y);
         gn += __dmul_rn(gv, gv);
+    };
+    // float4 groups of the flat 2n values (256-byte aligned role vectors), then the tail
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += gridDim.x * blockDim.x) {
+        const float4 a = reinterpret_cast<const float4*>(u)[t];
+        const float4 b = reinterpret_cast<const float4*>(up)[t];
+        const float4 c = reinterpret_cast<const float4*>(g)[t];
+        const float4 d = reinterpret_cast<const float4*>(gp)[t];
+        term(a.x, b.x, c.x, d.x);
+        term(a.y, b.y, c.y, d.y);
+        term(a.z, b.z, c.z, d.z);
+        term(a.w, b.w, c.w, d.w);
     }
+    for (int k = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        term(u[k], up[k], g[k], gp[k]);
     double v4[4] = {dx, dg, sy, gn};
     block_sums(v4);
     dx = v4[0];
@@ -477,6 +560,8 @@ __global__ void __launch_bounds__(RED_THREADS) reduce_kernel(DevPtrs p, int use_
 
 // Graph mode: the iteration loop continues while the stage is not done.
 __global__ void loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond) {
+    pdl_wait();
+    pdl_trigger();
     const DevState* st = p.st;
     cudaGraphSetConditional(loop_cond, (st->done || st->error) ? 0u : 1u);
 }
@@ -487,40 +572,70 @@ __global__ void loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond
 // rotates the roles: uPrev <- u <- u' ; vPrev <- v <- v' ; gPrevTmp <- g
 // (nesterov.cpp:110-119).
 __global__ void __launch_bounds__(RED_THREADS) update_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     DevState* st = p.st;
     const int done = st->done;
     const int slot = st->snap_copy_to;
-    const float* u = role_ptr(p, R_U);
-    const float* v = role_ptr(p, R_V);
-    const float* g = role_ptr(p, R_G);
-    float* vn = role_ptr(p, R_VNEW);
-    float* un = role_ptr(p, R_UNEW);
-    float* snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
+    const float* __restrict__ u = role_ptr(p, R_U);
+    const float* __restrict__ v = role_ptr(p, R_V);
+    const float* __restrict__ g = role_ptr(p, R_G);
+    float* __restrict__ vn = role_ptr(p, R_VNEW);
+    float* __restrict__ un = role_ptr(p, R_UNEW);
+    float* __restrict__ snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
     const float alpha = st->alpha, m = st->momentum;
     const int n = p.n_opt;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        float nu[2];
+    // The x and y halves are one flat array of 2n values, processed as float4 groups (every
+    // role vector and clamp box starts on a 256-byte boundary); value q < n is node
+    // opt_idx[q]'s x, q >= n its y.
+    const int n2 = 2 * n, n4 = n2 >> 2;
+    bool bad = false;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += gridDim.x * blockDim.x) {
+        const float4 u4 = reinterpret_cast<const float4*>(u)[t];
+        const float4 v4 = reinterpret_cast<const float4*>(v)[t];
+        const float4 g4 = reinterpret_cast<const float4*>(g)[t];
+        const float4 lo4 = reinterpret_cast<const float4*>(p.opt_lo)[t];
+        const float4 hi4 = reinterpret_cast<const float4*>(p.opt_hi)[t];
+        if (snap) reinterpret_cast<float4*>(snap)[t] = u4;
+        const float uq[4] = {u4.x, u4.y, u4.z, u4.w}, vq[4] = {v4.x, v4.y, v4.z, v4.w};
+        const float gq[4] = {g4.x, g4.y, g4.z, g4.w};
+        const float lo[4] = {lo4.x, lo4.y, lo4.z, lo4.w}, hi[4] = {hi4.x, hi4.y, hi4.z, hi4.w};
+        float vo[4], uo[4];
 #pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int q = c * n + k;
-            const float uq = u[q];
-            if (snap) snap[q] = uq;
-            const float vk = fsub(uq, fmul(alpha, g[q]));
-            const float uk = fadd(vk, fmul(m, fsub(vk, v[q])));
-            const float lo = p.opt_lo[q], hi = p.opt_hi[q];
-            nu[c] = clamp_box(uk, lo, hi);
-            if (!done) {
-                vn[q] = clamp_box(vk, lo, hi);
-                un[q] = nu[c];
-            }
+        for (int c = 0; c < 4; ++c) {
+            const float vk = fsub(uq[c], fmul(alpha, gq[c]));
+            const float uk = fadd(vk, fmul(m, fsub(vk, vq[c])));
+            vo[c] = clamp_box(vk, lo[c], hi[c]);
+            uo[c] = clamp_box(uk, lo[c], hi[c]);
         }
         if (!done) {
-            if (!isfinite(nu[0]) || !isfinite(nu[1])) raise_error(st, SPG_E_NON_FINITE);
-            const int i = p.opt_idx[k];
-            p.x[i] = nu[0];
-            p.y[i] = nu[1];
+            reinterpret_cast<float4*>(vn)[t] = make_float4(vo[0], vo[1], vo[2], vo[3]);
+            reinterpret_cast<float4*>(un)[t] = make_float4(uo[0], uo[1], uo[2], uo[3]);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const int q = 4 * t + c;
+                bad |= !isfinite(uo[c]);
+                if (q < n) p.x[p.opt_idx[q]] = uo[c];
+                else p.y[p.opt_idx[q - n]] = uo[c];
+            }
         }
     }
+    for (int q = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += gridDim.x * blockDim.x) {
+        const float uq = u[q];
+        if (snap) snap[q] = uq;
+        const float vk = fsub(uq, fmul(alpha, g[q]));
+        const float uk = fadd(vk, fmul(m, fsub(vk, v[q])));
+        const float lo = p.opt_lo[q], hi = p.opt_hi[q];
+        const float uo = clamp_box(uk, lo, hi);
+        if (!done) {
+            vn[q] = clamp_box(vk, lo, hi);
+            un[q] = uo;
+            bad |= !isfinite(uo);
+            if (q < n) p.x[p.opt_idx[q]] = uo;
+            else p.y[p.opt_idx[q - n]] = uo;
+        }
+    }
+    if (bad) raise_error(st, SPG_E_NON_FINITE);
     if (!last_block(&st->tk_update)) return;
     if (threadIdx.x != 0) return;
     st->tk_update = 0;
@@ -547,6 +662,8 @@ __global__ void __launch_bounds__(RED_THREADS) update_kernel(DevPtrs p) {
 // v = uPrev - alpha*gPrevTmp ; u = v + momentumPrev*(v - vPrev) ; clamp v, u
 // (redoIfOvershot body, nesterov.cpp:158-163), u scattered into the node positions.
 __global__ void __launch_bounds__(RED_THREADS) redo_update_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     if (!p.st->redo) return;
     float* v = role_ptr(p, R_V);
     float* u = role_ptr(p, R_U);
@@ -575,6 +692,8 @@ __global__ void __launch_bounds__(RED_THREADS) redo_update_kernel(DevPtrs p) {
 }
 
 __global__ void copy_role_kernel(DevPtrs p, int dst, int src) {
+    pdl_wait();
+    pdl_trigger();
     float* d = role_ptr(p, dst);
     const float* s = role_ptr(p, src);
     const int n = 2 * p.n_opt;
@@ -582,6 +701,8 @@ __global__ void copy_role_kernel(DevPtrs p, int dst, int src) {
 }
 
 __global__ void clamp_role_kernel(DevPtrs p, int role) {
+    pdl_wait();
+    pdl_trigger();
     float* d = role_ptr(p, role);
     const int n = 2 * p.n_opt;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
@@ -592,6 +713,8 @@ __global__ void clamp_role_kernel(DevPtrs p, int role) {
 // evaluated point u (converged), or the picked snapshot (stagnated; when the pick is the
 // snapshot decided in the final iteration, its copy is still pending and u is it).
 __global__ void deliver_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const DevState* st = p.st;
     const float* s = role_ptr(p, R_V);
     if (st->deliver == 1) s = role_ptr(p, R_U);
@@ -605,6 +728,8 @@ __global__ void deliver_kernel(DevPtrs p) {
 
 // |u|^2 -> SLOT_PN and |gA|^2 -> SLOT_GN for estimateInitialStep (nesterov.cpp:196-198)
 __global__ void __launch_bounds__(RED_THREADS) init_norms_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const float* u = role_ptr(p, R_U);
     const float* ga = role_ptr(p, R_GA);
     const int n = 2 * p.n_opt;
@@ -622,6 +747,8 @@ __global__ void __launch_bounds__(RED_THREADS) init_norms_kernel(DevPtrs p) {
 
 // probe = clamp(u - (float)scale * gA) (nesterov.cpp:200-205); scale is in st->pn.
 __global__ void init_perturb_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const float* u = role_ptr(p, R_U);
     const float* ga = role_ptr(p, R_GA);
     float* pr = role_ptr(p, R_PROBE);
@@ -633,6 +760,8 @@ __global__ void init_perturb_kernel(DevPtrs p) {
 
 // dx^2 = |probe - u|^2 -> SLOT_DX, dg^2 = |gB - gA|^2 -> SLOT_DG (nesterov.cpp:207-208)
 __global__ void __launch_bounds__(RED_THREADS) init_diff_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const float* u = role_ptr(p, R_U);
     const float* pr = role_ptr(p, R_PROBE);
     const float* ga = role_ptr(p, R_GA);
@@ -655,6 +784,8 @@ __global__ void __launch_bounds__(RED_THREADS) init_diff_kernel(DevPtrs p) {
 
 // lambda_0 = sum|dWL| / sum|q xi|, gamma = computeGamma(tau) (eplace.cpp:254-258)
 __global__ void ctl_lambda_init_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     DevState* st = p.st;
     st->gamma = compute_gamma(st->tau, p.step_x_gamma);
     float lam = st->sum_den > 0.0 ? static_cast<float>(st->sum_wl / st->sum_den) : 1.f;
@@ -664,6 +795,8 @@ __global__ void ctl_lambda_init_kernel(DevPtrs p) {
 
 // estimateInitialStep, first half: perturbation scale into st->pn, or alpha0 = 1.
 __global__ void ctl_init_scale_kernel(DevPtrs p, float init_perturb) {
+    pdl_wait();
+    pdl_trigger();
     const double pn2 = finalize(p, SLOT_PN);
     const double gn2 = finalize(p, SLOT_GN);
     if (threadIdx.x != 0) return;
@@ -681,6 +814,8 @@ __global__ void ctl_init_scale_kernel(DevPtrs p, float init_perturb) {
 
 // estimateInitialStep, second half: alpha0 = |probe-u| / |gB-gA| (nesterov.cpp:207-217).
 __global__ void ctl_init_finish_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
     const double dx2 = finalize(p, SLOT_DX);
     const double dg2 = finalize(p, SLOT_DG);
     if (threadIdx.x != 0) return;
@@ -699,10 +834,16 @@ __global__ void ctl_init_finish_kernel(DevPtrs p) {
     st->alpha0 = (isfinite(step) && step > 0.0) ? static_cast<float>(step) : 1.f;
 }
 
-__global__ void ctl_stage_start_kernel(DevPtrs p) { p.st->t0_ns = global_ns(); }
+__global__ void ctl_stage_start_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
+    p.st->t0_ns = global_ns();
+}
 
 __global__ void check_geometry_kernel(DevPtrs p, float lx, float ly, float hx, float hy,
                                       const float* w, const float* h) {
+    pdl_wait();
+    pdl_trigger();
     const int n = p.n_opt;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const int i = p.opt_idx[k];
@@ -720,6 +861,8 @@ __global__ void check_geometry_kernel(DevPtrs p, float lx, float ly, float hx, f
 }
 
 __global__ void finalize_slots_kernel(DevPtrs p, int first, int count, double* out) {
+    pdl_wait();
+    pdl_trigger();
     for (int s = 0; s < count; ++s) {
         const double v = finalize(p, first + s);
         if (threadIdx.x == 0) out[s] = v;
@@ -742,18 +885,18 @@ inline int vec_blocks(const DevPtrs& p, K kernel) {
 
 }  // namespace
 
-#define LAUNCH(kernel, grid, block, ...)                      \
-    do {                                                       \
-        kernel<<<(grid), (block), 0, s>>>(__VA_ARGS__);        \
-        count_launch();                                        \
-        SPG_CHECK_LAUNCH();                                    \
-    } while (0)
+#define LAUNCH(kernel, grid, block, ...) launch_pdl(kernel, dim3(grid), dim3(block), 0, s, __VA_ARGS__)
 
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
     LAUNCH(scatter_kernel, vec_blocks(p, scatter_kernel), RED_THREADS, p, role);
 }
-void launch_assemble(const DevPtrs& p, int grad_role, int count_eval, cudaStream_t s) {
-    LAUNCH(assemble_kernel, wave(assemble_kernel), RED_THREADS, p, grad_role, count_eval);
+void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s) {
+    LAUNCH(assemble_kernel<false>, wave(assemble_kernel<false>), RED_THREADS, p, pos_role, grad_role,
+           count_eval, 0, cudaGraphConditionalHandle{});
+}
+void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, int use_cond, cudaGraphConditionalHandle redo_cond) {
+    LAUNCH(assemble_kernel<true>, wave(assemble_kernel<true>), RED_THREADS, p, static_cast<int>(R_U),
+           static_cast<int>(R_G), 1, use_cond, redo_cond);
 }
 void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond, cudaGraphConditionalHandle redo_cond) {
     LAUNCH(reduce_kernel, wave(reduce_kernel), RED_THREADS, p, use_cond, redo_cond);

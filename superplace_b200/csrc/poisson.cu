@@ -19,6 +19,8 @@ namespace {
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
 __global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ float As[BK][BM + 4];
     __shared__ float Bs[BK][BN + 4];
     const int z = blockIdx.z;
@@ -101,6 +103,8 @@ __global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
 // One warp per (row, segment): FP64 sum of `seg` contiguous floats, fixed shuffle tree.
 __global__ void row_stats_kernel(const float* a, int rows, int nseg, int64_t ld, int seg,
                                  float* mean, float* sum) {
+    pdl_wait();
+    pdl_trigger();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= rows * nseg) return;
@@ -118,6 +122,8 @@ __global__ void row_stats_kernel(const float* a, int rows, int nseg, int64_t ld,
 
 __global__ void set_row0_kernel(float* C, int64_t sC, int n, const float* vals, int64_t sv,
                                 const float* scale) {
+    pdl_wait();
+    pdl_trigger();
     const int z = blockIdx.y;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float v = vals[z * sv + i];
@@ -153,26 +159,20 @@ void sgemm_tn(const GemmArgs& g, int batch, cudaStream_t s) {
                          (reinterpret_cast<uintptr_t>(g.B) % 16 == 0) && (g.sA % 4 == 0) &&
                          (g.sB % 4 == 0);
     dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), batch);
-    sgemm_tn_kernel<<<grid, NT, 0, s>>>(g, aligned ? 1 : 0);
-    count_launch();
-    SPG_CHECK_LAUNCH();
+    launch_pdl(sgemm_tn_kernel, grid, dim3(NT), 0, s, g, aligned ? 1 : 0);
 }
 
 void row_stats(const float* a, int rows, int cols, int64_t ld, int seg, float* mean, float* sum,
                cudaStream_t s) {
     const int nseg = cols / seg;
     const int warps = rows * nseg;
-    row_stats_kernel<<<ceil_div(warps, 8), 256, 0, s>>>(a, rows, nseg, ld, seg, mean, sum);
-    count_launch();
-    SPG_CHECK_LAUNCH();
+    launch_pdl(row_stats_kernel, dim3(ceil_div(warps, 8)), dim3(256), 0, s, a, rows, nseg, ld, seg, mean, sum);
 }
 
 void set_row0(float* C, int64_t sC, int n, const float* vals, int64_t sv, const float* scale,
               int batch, cudaStream_t s) {
     dim3 grid(ceil_div(n, 256), batch);
-    set_row0_kernel<<<grid, 256, 0, s>>>(C, sC, n, vals, sv, scale);
-    count_launch();
-    SPG_CHECK_LAUNCH();
+    launch_pdl(set_row0_kernel, grid, dim3(256), 0, s, C, sC, n, vals, sv, scale);
 }
 
 void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, int precision,

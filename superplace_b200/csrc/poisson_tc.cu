@@ -231,6 +231,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    // everything above touched only this CTA's shared memory and TMEM: wait for the kernel
+    // that produced the operands only now
+    pdl_wait();
+    pdl_trigger();
 
     const int kpp = g.K / TC_BK;  // slabs per split pass
     const int nk = 3 * kpp;
@@ -344,6 +348,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // One warp per (row, segment); outputs planes[row][col] with lo plane at + plane_stride.
 __global__ void prep_split_kernel(const float* src, int rows, int nseg, int64_t ld, int seg,
                                   int center, uint16_t* planes, int64_t plane_stride, float* sums) {
+    pdl_wait();
+    pdl_trigger();
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= rows * nseg) return;
@@ -432,13 +438,15 @@ void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int 
     cfg.blockDim = dim3(TC_THREADS);
     cfg.dynamicSmemBytes = tc_smem_bytes();
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = S;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES>, a, b, g));
     count_launch();
 }
@@ -446,10 +454,8 @@ void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int 
 void prep_split(const float* src, int rows, int cols, int64_t ld, int seg, int center, uint16_t* planes,
                 int64_t plane_stride, float* sums, cudaStream_t s) {
     const int warps = rows * (cols / seg);
-    prep_split_kernel<<<ceil_div(warps, 8), 256, 0, s>>>(src, rows, cols / seg, ld, seg, center, planes,
-                                                         plane_stride, sums);
-    count_launch();
-    SPG_CHECK_LAUNCH();
+    launch_pdl(prep_split_kernel, dim3(ceil_div(warps, 8)), dim3(256), 0, s, src, rows, cols / seg, ld, seg,
+               center, planes, plane_stride, sums);
 }
 
 void split_host(const std::vector<float>& v, std::vector<uint16_t>& out) {

@@ -140,6 +140,8 @@ __device__ void wa_warp_net(const DevPtrs& p, int k, float invG, double& wl, dou
 // from the reference's sequential float sums in the last bits only.
 __global__ void __launch_bounds__(RED_THREADS) wa_net_kernel(DevPtrs p, const float* gamma_dev,
                                                              float gamma_host, int use_dev) {
+    pdl_wait();
+    pdl_trigger();
     __shared__ double ws[32];
     const float gam = use_dev ? *gamma_dev : gamma_host;
     const float g = fmax_(gam, 1e-4f);  // kMinGamma, wa_wirelength.cpp:14
@@ -193,6 +195,8 @@ __global__ void __launch_bounds__(RED_THREADS) wa_net_kernel(DevPtrs p, const fl
 }
 
 __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
+    pdl_wait();
+    pdl_trigger();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= p.num_movable) return;
     float gx = 0.f, gy = 0.f;
@@ -210,16 +214,12 @@ void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, 
                     cudaStream_t s) {
     // one full wave, fixed per device, so the FP64 partials keep a fixed owner per block
     const int grid = wave_grid(reinterpret_cast<const void*>(wa_net_kernel), RED_THREADS, RED_CAP);
-    wa_net_kernel<<<grid, RED_THREADS, 0, s>>>(p, gamma_dev, gamma_host, use_dev);
-    count_launch();
-    SPG_CHECK_LAUNCH();
+    launch_pdl(wa_net_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, gamma_dev, gamma_host, use_dev);
 }
 
 void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s) {
     if (p.num_movable <= 0) return;
-    wa_node_grad_kernel<<<ceil_div(p.num_movable, 256), 256, 0, s>>>(p, grad);
-    count_launch();
-    SPG_CHECK_LAUNCH();
+    launch_pdl(wa_node_grad_kernel, dim3(ceil_div(p.num_movable, 256)), dim3(256), 0, s, p, grad);
 }
 
 }  // namespace spg
