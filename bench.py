@@ -189,9 +189,11 @@ def cpu_baseline_sample(db, workload, iters=8):
 def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision):
     """Algorithmic bytes (or flops) of each iteration part per launch, divided by its
     warm-L2 device time. Bytes count every array the part must touch once (FP32/int32):
-      update     68 B per optimised node (u, v, g, clamp box, index in; v', u', x, y out)
+      update     80 B per optimised node (u, v, g, clamp box, index, hw/hh/weight in; v', u',
+                 x, y out) + 16 B per bin (the two fixed-point maps it scatters into)
       wa         32 B per pin + 8 B per net (pin ids, offsets, positions in; 2 terms out)
-      scatter    25 B per density node + 16 B per bin (two 64-bit maps)
+      scatter    25 B per density node outside the opt set + 16 B per bin (only FILLERONLY
+                 and cGP have such nodes)
       rho        44 B per bin (maps, terminal, base in; rho out; maps cleared)
       poisson    14 M^3 flops (16 B per bin of I/O)
       assemble   76 B per optimised node + 16 B per pin (WA pass 2, gather, gradient, and
@@ -200,7 +202,7 @@ def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision):
     n_opt = db.num_movable + db.num_fillers
     n_dens = n_opt
     pins, nets, bins = db.num_pins, db.num_nets, dim * dim
-    by = {"update": 68 * n_opt, "wa": 32 * pins + 8 * nets, "scatter": 25 * n_dens + 16 * bins,
+    by = {"update": 80 * n_opt + 16 * bins, "wa": 32 * pins + 8 * nets, "scatter": 25 * n_dens + 16 * bins,
           "rho": 44 * bins, "assemble": 76 * n_opt + 16 * pins}
     out = {}
     for k, us in parts.items():

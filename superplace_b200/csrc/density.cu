@@ -20,31 +20,20 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__global__ void __launch_bounds__(kThreads) acc_small_kernel(DevPtrs p) {
+__global__ void __launch_bounds__(kThreads) acc_small_kernel(DevPtrs p, const int* list, int count) {
     pdl_wait();
     pdl_trigger();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= p.n_dens_small) return;
-    const int i = p.dens_small[t];
-    const GridGeom& g = p.geom;
-    const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
-    const float w = p.wgt[i];
-    unsigned long long* map = (p.kind[i] & K_FILLER) ? p.filler_fix : p.node_fix;
-    for (int bx = f.bx0; bx <= f.bx1; ++bx) {
-        unsigned long long* row = map + static_cast<size_t>(bx) * g.dim;
-        for (int by = f.by0; by <= f.by1; ++by) {
-            const float c = bin_contribution(g, bx, by, f, w);
-            if (c <= 0.f) continue;
-            atomicAdd(row + by, to_fixed(c, g.scale));
-        }
-    }
+    if (t >= count) return;
+    const int i = list[t];
+    rasterize(p, p.x[i], p.y[i], p.hw[i], p.hh[i], p.wgt[i], (p.kind[i] & K_FILLER) != 0);
 }
 
 // One block per large node (macros): the block's threads split its footprint's bins.
-__global__ void __launch_bounds__(kThreads) acc_large_kernel(DevPtrs p) {
+__global__ void __launch_bounds__(kThreads) acc_large_kernel(DevPtrs p, const int* list) {
     pdl_wait();
     pdl_trigger();
-    const int i = p.dens_large[blockIdx.x];
+    const int i = list[blockIdx.x];
     const GridGeom& g = p.geom;
     const Footprint f = footprint(g, p.x[i], p.y[i], p.hw[i], p.hh[i]);
     const float w = p.wgt[i];
@@ -218,10 +207,21 @@ __global__ void __launch_bounds__(kThreads) gather_all_large_kernel(DevPtrs p, f
 
 void launch_density_accumulate(const DevPtrs& p, cudaStream_t s) {
     if (p.n_dens_small > 0) {
-        launch_pdl(acc_small_kernel, dim3(ceil_div(p.n_dens_small, kThreads)), dim3(kThreads), 0, s, p);
+        launch_pdl(acc_small_kernel, dim3(ceil_div(p.n_dens_small, kThreads)), dim3(kThreads), 0, s, p,
+                   p.dens_small, p.n_dens_small);
     }
     if (p.n_dens_large > 0) {
-        launch_pdl(acc_large_kernel, dim3(p.n_dens_large), dim3(kThreads), 0, s, p);
+        launch_pdl(acc_large_kernel, dim3(p.n_dens_large), dim3(kThreads), 0, s, p, p.dens_large);
+    }
+}
+
+void launch_density_rest(const DevPtrs& p, cudaStream_t s) {
+    if (p.n_rest_small > 0) {
+        launch_pdl(acc_small_kernel, dim3(ceil_div(p.n_rest_small, kThreads)), dim3(kThreads), 0, s, p,
+                   p.rest_small, p.n_rest_small);
+    }
+    if (p.n_rest_large > 0) {
+        launch_pdl(acc_large_kernel, dim3(p.n_rest_large), dim3(kThreads), 0, s, p, p.rest_large);
     }
 }
 

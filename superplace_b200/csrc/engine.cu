@@ -159,6 +159,9 @@ struct Context {
     std::unique_ptr<PoissonPlan> plan;
     DevBuf<int> dens_small, dens_large;
     int n_dens_small = 0, n_dens_large = 0;
+    std::vector<int> dens_small_h, dens_large_h;  // host copies, for the per-stage rest lists
+    DevBuf<int> rest_small, rest_large;
+    int n_rest_small = 0, n_rest_large = 0;
     // stage
     int n_opt = 0;
     DevBuf<int> opt_idx, opt_deg, opt_small, opt_large;
@@ -249,6 +252,10 @@ struct Context {
         p.dens_large = dens_large.p;
         p.n_dens_small = n_dens_small;
         p.n_dens_large = n_dens_large;
+        p.rest_small = rest_small.p;
+        p.rest_large = rest_large.p;
+        p.n_rest_small = n_rest_small;
+        p.n_rest_large = n_rest_large;
         p.opt_small = opt_small.p;
         p.opt_large = opt_large.p;
         p.n_opt_small = n_opt_small;
@@ -416,6 +423,8 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     c.dens_large.upload(dlarge, st);
     c.n_dens_small = static_cast<int>(dsmall.size());
     c.n_dens_large = static_cast<int>(dlarge.size());
+    c.dens_small_h = dsmall;
+    c.dens_large_h = dlarge;
     c.node_fix.alloc(n);
     c.filler_fix.alloc(n);
     c.node_fix.zero(st);
@@ -486,6 +495,19 @@ void stage_setup(Context& c, int stage) {
     c.opt_area.upload(area, s);
     c.opt_geom.upload(geom, s);
     c.opt_meta.upload(meta, s);
+    // density nodes the loop's step kernel does not rasterize: small ones outside the opt
+    // set (the cells of FILLERONLY, the macros of cGP) and every large node
+    {
+        std::vector<uint8_t> in_opt(c.total, 0);
+        for (int i : opt) in_opt[i] = 1;
+        std::vector<int> rs;
+        for (int i : c.dens_small_h)
+            if (!in_opt[i]) rs.push_back(i);
+        c.rest_small.upload(rs, s);
+        c.n_rest_small = static_cast<int>(rs.size());
+        c.rest_large.upload(c.dens_large_h, s);
+        c.n_rest_large = static_cast<int>(c.dens_large_h.size());
+    }
     c.opt_small.upload(osmall, s);
     c.opt_large.upload(olarge, s);
     c.n_opt_small = static_cast<int>(osmall.size());
@@ -508,15 +530,17 @@ void stage_setup(Context& c, int stage) {
 // by the update kernels; pos_role >= 0 scatters that role first), gradient into grad_role.
 // The WA pass 1 depends only on the positions, so it runs on a side stream, overlapping
 // the density -> Poisson chain; the assembly joins both.
+// `stepped`: the step kernel already added the opt nodes' charge (loop evaluations).
 void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count, bool fused_reduce = false,
-              int use_cond = 0, cudaGraphConditionalHandle redo_h = 0) {
+              int use_cond = 0, cudaGraphConditionalHandle redo_h = 0, bool stepped = false) {
     cudaStream_t s = c.stream;
     if (pos_role >= 0) launch_scatter(p, pos_role, s);
     SPG_CUDA(cudaEventRecord(c.ev_fork, s));
     SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
     launch_wa_nets(p, &p.st->gamma, 0.f, 1, c.side);
     SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
-    launch_density_accumulate(p, s);
+    if (stepped) launch_density_rest(p, s);
+    else launch_density_accumulate(p, s);
     launch_rho_overflow(p, 0, 1, s);
     poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s);
     launch_gather_opt_large(p, s);
@@ -629,14 +653,14 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
 void enqueue_iteration(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
     cudaStream_t s = c.stream;
     launch_update(p, s);
-    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h);
+    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h, true);
 }
 
 // One redoIfOvershot re-evaluation (nesterov.cpp:158-166) and the next redo test.
 void enqueue_redo(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
     cudaStream_t s = c.stream;
     launch_redo_update(p, s);
-    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h);
+    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h, true);
 }
 
 // Host-driven loop: one 16-byte state read per iteration (and per re-evaluation).
@@ -1113,8 +1137,13 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     // SPG_HOST_LOOP=1 selects the host-driven iteration loop (one state read per iteration)
     // instead of the conditional CUDA graph; both run the same kernels in the same order.
     c.use_graph = std::getenv("SPG_HOST_LOOP") == nullptr;
-    SPG_CUDA(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
-    SPG_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+    // The main stream carries the latency-bound chain (scatter -> rho -> Poisson -> assembly)
+    // at the highest priority; the WA pass on the side stream is throughput work that fills
+    // whatever SMs the chain leaves free.
+    int prio_low = 0, prio_high = 0;
+    SPG_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    SPG_CUDA(cudaStreamCreateWithPriority(&c.stream, cudaStreamNonBlocking, prio_high));
+    SPG_CUDA(cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, prio_low));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
     c.num_movable = v->num_movable;
@@ -1530,11 +1559,12 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     upd.done = 0;
     upd.last = 0;
     set_state(upd);
-    t[0] = time([&] { spg::launch_update(p, s); }, nothing);
+    // the step carries the density scatter of the opt nodes (part 2 is the rest list only)
+    t[0] = time([&] { spg::launch_update(p, s); }, zero_maps);
     set_state(probe);
     spg::launch_scatter(p, spg::R_POS, s);  // the delivered positions again
     t[1] = time([&] { spg::launch_wa_nets(p, &p.st->gamma, 0.f, 1, s); }, nothing);
-    t[2] = time([&] { spg::launch_density_accumulate(p, s); }, zero_maps);
+    t[2] = (c.n_rest_small + c.n_rest_large) > 0 ? time([&] { spg::launch_density_rest(p, s); }, zero_maps) : 0.0;
     t[3] = time([&] { spg::launch_rho_overflow(p, 0, 1, s); }, [&] { spg::launch_density_accumulate(p, s); });
     t[4] = time([&] { spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s); }, nothing);
     // the loop's assembly carries the norms and decisions of the reduce step (part 6 = 0)
@@ -1543,7 +1573,7 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
         spg::launch_assemble_reduce(p, s);
     }, nothing);
     t[6] = 0.0;
-    t[7] = time([&] { spg::evaluate(c, p, -1, spg::R_G, 1, true); }, nothing);
+    t[7] = time([&] { spg::evaluate(c, p, -1, spg::R_G, 1, true, 0, 0, true); }, nothing);
     spg::g_launches = launches0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

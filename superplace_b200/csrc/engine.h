@@ -94,6 +94,11 @@ struct DevState {
     int error;          // SPG_E_* raised on the device (non-finite values)
     int64_t redos;      // backtracking re-evaluations
     unsigned int tk_update, tk_assemble, tk_reduce;  // last-block tickets
+    // bookkeeping of the last step kernel, applied by the next assembly's last block (the step
+    // kernel has no last block: a fence per block would wait on its atomics): 0 none,
+    // 1 clear the snapshot copy, 2 also rotate the roles and advance the iteration
+    int step_pending;
+    int step_pending_pad;
     int stage;
     int max_iter;
     int role[NUM_ROLES];
@@ -147,9 +152,13 @@ struct DevPtrs {
     float* force;          // 2*nOpt, density force q*xi (not gradient)
     float* pool;           // NUM_ROLES + SNAP_MAX vectors of 2*nOpt
     size_t vec_stride;
-    // density work lists (node ids)
+    // density work lists (node ids): every density node, and the "rest" the loop's step
+    // kernel does not rasterize itself (density nodes outside the opt set, and every node
+    // whose footprint may exceed 16 bins)
     const int *dens_small, *dens_large;
     int n_dens_small, n_dens_large;
+    const int *rest_small, *rest_large;
+    int n_rest_small, n_rest_large;
     const int *opt_small, *opt_large;  // opt positions k
     int n_opt_small, n_opt_large;
     double* partials;      // RED_SLOTS * RED_CAP
@@ -166,6 +175,25 @@ __device__ __forceinline__ float* role_ptr(const DevPtrs& p, int role) {
     return p.pool + static_cast<size_t>(p.st->role[role]) * p.vec_stride;
 }
 
+// Fixed-point charge of one node with at most 16 footprint bins (BinGrid::accumulate,
+// bin_grid.cpp:191-251): every overlap x weight formed with the reference's float
+// operations, rounded once to 64-bit fixed point and added with an integer atomic, so the
+// maps do not depend on the order of the adds.
+__device__ __forceinline__ void rasterize(const DevPtrs& p, float x, float y, float hw, float hh, float w,
+                                          bool filler) {
+    const GridGeom& g = p.geom;
+    const Footprint f = footprint(g, x, y, hw, hh);
+    unsigned long long* map = filler ? p.filler_fix : p.node_fix;
+    for (int bx = f.bx0; bx <= f.bx1; ++bx) {
+        unsigned long long* row = map + static_cast<size_t>(bx) * g.dim;
+        for (int by = f.by0; by <= f.by1; ++by) {
+            const float c = bin_contribution(g, bx, by, f, w);
+            if (c <= 0.f) continue;
+            atomicAdd(row + by, to_fixed(c, g.scale));
+        }
+    }
+}
+
 // Thread 0 of every block stores the block's partial of `slot`; block 0 also clears the
 // entries past the grid, so the slot sums exactly this launch's partials.
 __device__ __forceinline__ void put_partial(const DevPtrs& p, int slot, double v) {
@@ -177,6 +205,8 @@ __device__ __forceinline__ void put_partial(const DevPtrs& p, int slot, double v
 
 // ---- density.cu
 void launch_density_accumulate(const DevPtrs& p, cudaStream_t s);
+// the density nodes the loop's step kernel does not rasterize (rest_small, rest_large)
+void launch_density_rest(const DevPtrs& p, cudaStream_t s);
 // rho + tau partials; write_maps also stores the float maps, zero clears the fixed maps
 void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s);
 // force of the large (block-per-node) opt nodes; cells are gathered inside the assembly
@@ -202,6 +232,8 @@ void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
 void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
                    cudaGraphConditionalHandle redo_cond = 0);
 void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s);
+// the loop's Nesterov step (and its redo variant) with the density scatter of the new
+// positions fused in; the evaluation that follows accumulates only the rest list
 void launch_update(const DevPtrs& p, cudaStream_t s);
 void launch_redo_update(const DevPtrs& p, cudaStream_t s);
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s);

@@ -346,6 +346,54 @@ __device__ __forceinline__ void gather_at(const DevPtrs& p, float x, float y, fl
     }
 }
 
+// Physical pool slot of a logical role while a step's role rotation is pending: uPrev <- u
+// <- u' ; vPrev <- v <- v' ; gPrevTmp <- g <- (old gPrevTmp buffer) (nesterov.cpp:110-119).
+__device__ __forceinline__ int role_slot(const DevState* st, int role, int pending) {
+    const int* r = st->role;
+    if (pending != 2) return r[role];
+    switch (role) {
+        case R_U: return r[R_UNEW];
+        case R_UPREV: return r[R_U];
+        case R_UNEW: return r[R_UPREV];
+        case R_V: return r[R_VNEW];
+        case R_VPREV: return r[R_V];
+        case R_VNEW: return r[R_VPREV];
+        case R_G: return r[R_GPREVTMP];
+        case R_GPREVTMP: return r[R_G];
+        default: return r[role];
+    }
+}
+__device__ __forceinline__ float* role_ptr_pending(const DevPtrs& p, int role, int pending) {
+    return p.pool + static_cast<size_t>(role_slot(p.st, role, pending)) * p.vec_stride;
+}
+
+// The end of the last step kernel (nesterov.cpp:110-119 and the loop counter): the snapshot
+// copy it made is done; when it applied a step, the roles rotate, momentumPrev takes the
+// step's momentum, the iteration advances, and max_iter marks the stage done.
+__device__ void apply_pending_step(DevState* st) {
+    const int pending = st->step_pending;
+    if (pending == 0) return;
+    st->step_pending = 0;
+    st->snap_copy_to = -1;
+    if (pending != 2) return;
+    int* r = st->role;
+    const int ru = r[R_U], rup = r[R_UPREV], run = r[R_UNEW];
+    r[R_UPREV] = ru;
+    r[R_U] = run;
+    r[R_UNEW] = rup;
+    const int rv = r[R_V], rvp = r[R_VPREV], rvn = r[R_VNEW];
+    r[R_V] = rvn;
+    r[R_VPREV] = rv;
+    r[R_VNEW] = rvp;
+    const int rg = r[R_G], rgp = r[R_GPREVTMP];
+    r[R_GPREVTMP] = rg;
+    r[R_G] = rgp;
+    st->momentum_prev = st->momentum;
+    st->iter += 1;
+    st->tries = 1;
+    if (st->last) st->done = 1;
+}
+
 // The finalized evaluation (eplace.cpp:149,154-155,190-197) into the state: tau from the
 // overflow sum, HPWL, WA value and the two gradient-norm sums; s = {overflow, WA, HPWL,
 // sum|dWL|, sum|q xi|}.
@@ -408,10 +456,12 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
     pdl_trigger();
     // the evaluated positions, by opt index: the role the update (or scatter) wrote the
     // node coordinates from, so pos[k] == x[opt_idx[k]] bit for bit
-    const float* __restrict__ pos = role_ptr(p, pos_role);
-    float* __restrict__ grad = role_ptr(p, grad_role);
-    const float* __restrict__ up = FUSE ? role_ptr(p, R_UPREV) : nullptr;
-    const float* __restrict__ gp = FUSE ? role_ptr(p, R_GPREVTMP) : nullptr;
+    // (through a step's pending role rotation, which the last block then applies)
+    const int pending = p.st->step_pending;
+    const float* __restrict__ pos = role_ptr_pending(p, pos_role, pending);
+    float* __restrict__ grad = role_ptr_pending(p, grad_role, pending);
+    const float* __restrict__ up = FUSE ? role_ptr_pending(p, R_UPREV, pending) : nullptr;
+    const float* __restrict__ gp = FUSE ? role_ptr_pending(p, R_GPREVTMP, pending) : nullptr;
     const float lambda = p.st->lambda;
     const int n = p.n_opt;
     double acc_wl = 0.0, acc_den = 0.0;
@@ -482,7 +532,10 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
         constexpr int kSlots[5] = {SLOT_OVERFLOW, SLOT_WL, SLOT_HPWL, SLOT_SUM_WL, SLOT_SUM_DEN};
         double sums[5];
         finalize_n(p, kSlots, sums);
-        if (threadIdx.x == 0) finish_evaluation(p, p.st, sums, count_eval);
+        if (threadIdx.x == 0) {
+            apply_pending_step(p.st);
+            finish_evaluation(p, p.st, sums, count_eval);
+        }
         return;
     }
     constexpr int kSlots[9] = {SLOT_OVERFLOW, SLOT_WL, SLOT_HPWL, SLOT_SUM_WL, SLOT_SUM_DEN,
@@ -492,6 +545,7 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
     __shared__ DevState sst;
     state_copy_in(&sst, p.st);
     if (threadIdx.x == 0) {
+        apply_pending_step(&sst);
         finish_evaluation(p, &sst, sums, count_eval);
         decide(p, &sst, sums[5], sums[6], sums[7], sums[8]);
     }
@@ -566,129 +620,72 @@ __global__ void loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond
     cudaGraphSetConditional(loop_cond, (st->done || st->error) ? 0u : 1u);
 }
 
-// v' = u - alpha g ; u' = v' + momentum (v' - v) ; clamp both (nesterov.cpp:97-107), with
-// u' scattered into the node positions for the next evaluation and, when the iteration
-// decided a stagnation snapshot, the evaluated u copied into its slot. The last block
-// rotates the roles: uPrev <- u <- u' ; vPrev <- v <- v' ; gPrevTmp <- g
-// (nesterov.cpp:110-119).
-__global__ void __launch_bounds__(RED_THREADS) update_kernel(DevPtrs p) {
+// The loop's position step with the density scatter of the new positions fused in.
+//
+//   REDO = false (NesterovOptimizer::step, nesterov.cpp:97-119):
+//     v' = u - alpha g ; u' = v' + momentum (v' - v) ; clamp both (nesterov.cpp:97-107); when
+//     the iteration decided a stagnation snapshot, the evaluated u is copied into its slot.
+//     The last block rotates the roles: uPrev <- u <- u' ; vPrev <- v <- v' ; gPrevTmp <- g.
+//   REDO = true (redoIfOvershot body, nesterov.cpp:158-163):
+//     v = uPrev - alpha gPrevTmp ; u = v + momentumPrev (v - vPrev) ; clamp v, u.
+//
+// The new u is written into the node positions (for the WA pass) and its fixed-point charge
+// is added to the density maps right here (BinGrid::accumulate, bin_grid.cpp:191-251), so
+// the evaluation needs no separate pass over the cells; nodes whose footprint may exceed 16
+// bins are left to the block-per-node kernel of the rest list. When no step applies (the
+// stage is done, or no re-evaluation was decided) the current u is rasterized unchanged.
+template <bool REDO>
+__global__ void __launch_bounds__(RED_THREADS) step_kernel(DevPtrs p) {
     pdl_wait();
     pdl_trigger();
     DevState* st = p.st;
-    const int done = st->done;
-    const int slot = st->snap_copy_to;
-    const float* __restrict__ u = role_ptr(p, R_U);
-    const float* __restrict__ v = role_ptr(p, R_V);
-    const float* __restrict__ g = role_ptr(p, R_G);
-    float* __restrict__ vn = role_ptr(p, R_VNEW);
-    float* __restrict__ un = role_ptr(p, R_UNEW);
-    float* __restrict__ snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
-    const float alpha = st->alpha, m = st->momentum;
+    const int apply = REDO ? st->redo : !st->done;
+    const int slot = REDO ? -1 : st->snap_copy_to;
+    const float* u = role_ptr(p, REDO ? R_UPREV : R_U);
+    const float* v = role_ptr(p, REDO ? R_VPREV : R_V);
+    const float* g = role_ptr(p, REDO ? R_GPREVTMP : R_G);
+    float* vn = role_ptr(p, REDO ? R_V : R_VNEW);
+    float* un = role_ptr(p, REDO ? R_U : R_UNEW);
+    const float* cur = role_ptr(p, R_U);
+    float* snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
+    const float alpha = st->alpha, m = REDO ? st->momentum_prev : st->momentum;
     const int n = p.n_opt;
-    // The x and y halves are one flat array of 2n values, processed as float4 groups (every
-    // role vector and clamp box starts on a 256-byte boundary); value q < n is node
-    // opt_idx[q]'s x, q >= n its y.
-    const int n2 = 2 * n, n4 = n2 >> 2;
     bool bad = false;
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += gridDim.x * blockDim.x) {
-        const float4 u4 = reinterpret_cast<const float4*>(u)[t];
-        const float4 v4 = reinterpret_cast<const float4*>(v)[t];
-        const float4 g4 = reinterpret_cast<const float4*>(g)[t];
-        const float4 lo4 = reinterpret_cast<const float4*>(p.opt_lo)[t];
-        const float4 hi4 = reinterpret_cast<const float4*>(p.opt_hi)[t];
-        if (snap) reinterpret_cast<float4*>(snap)[t] = u4;
-        const float uq[4] = {u4.x, u4.y, u4.z, u4.w}, vq[4] = {v4.x, v4.y, v4.z, v4.w};
-        const float gq[4] = {g4.x, g4.y, g4.z, g4.w};
-        const float lo[4] = {lo4.x, lo4.y, lo4.z, lo4.w}, hi[4] = {hi4.x, hi4.y, hi4.z, hi4.w};
-        float vo[4], uo[4];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int4 meta = p.opt_meta[k];
+        const float4 geo = p.opt_geom[k];
+        float nu[2];
+        if (apply) {
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            const float vk = fsub(uq[c], fmul(alpha, gq[c]));
-            const float uk = fadd(vk, fmul(m, fsub(vk, vq[c])));
-            vo[c] = clamp_box(vk, lo[c], hi[c]);
-            uo[c] = clamp_box(uk, lo[c], hi[c]);
-        }
-        if (!done) {
-            reinterpret_cast<float4*>(vn)[t] = make_float4(vo[0], vo[1], vo[2], vo[3]);
-            reinterpret_cast<float4*>(un)[t] = make_float4(uo[0], uo[1], uo[2], uo[3]);
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int q = 4 * t + c;
-                bad |= !isfinite(uo[c]);
-                if (q < n) p.x[p.opt_idx[q]] = uo[c];
-                else p.y[p.opt_idx[q - n]] = uo[c];
+            for (int c = 0; c < 2; ++c) {
+                const int q = c * n + k;
+                const float uq = u[q];
+                if (snap) snap[q] = uq;
+                const float vk = fsub(uq, fmul(alpha, g[q]));
+                const float uk = fadd(vk, fmul(m, fsub(vk, v[q])));
+                const float lo = p.opt_lo[q], hi = p.opt_hi[q];
+                vn[q] = clamp_box(vk, lo, hi);
+                nu[c] = clamp_box(uk, lo, hi);
+                un[q] = nu[c];
+            }
+            bad |= !isfinite(nu[0]) || !isfinite(nu[1]);
+            const int i = p.opt_idx[k];
+            p.x[i] = nu[0];
+            p.y[i] = nu[1];
+        } else {
+            nu[0] = cur[k];
+            nu[1] = cur[n + k];
+            if (snap) {
+                snap[k] = nu[0];
+                snap[n + k] = nu[1];
             }
         }
-    }
-    for (int q = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; q < n2; q += gridDim.x * blockDim.x) {
-        const float uq = u[q];
-        if (snap) snap[q] = uq;
-        const float vk = fsub(uq, fmul(alpha, g[q]));
-        const float uk = fadd(vk, fmul(m, fsub(vk, v[q])));
-        const float lo = p.opt_lo[q], hi = p.opt_hi[q];
-        const float uo = clamp_box(uk, lo, hi);
-        if (!done) {
-            vn[q] = clamp_box(vk, lo, hi);
-            un[q] = uo;
-            bad |= !isfinite(uo);
-            if (q < n) p.x[p.opt_idx[q]] = uo;
-            else p.y[p.opt_idx[q - n]] = uo;
-        }
+        if (!(meta.w & K_LARGE)) rasterize(p, nu[0], nu[1], geo.x, geo.y, geo.z, (meta.w & K_FILLER) != 0);
     }
     if (bad) raise_error(st, SPG_E_NON_FINITE);
-    if (!last_block(&st->tk_update)) return;
-    if (threadIdx.x != 0) return;
-    st->tk_update = 0;
-    st->snap_copy_to = -1;
-    if (done) return;
-    int* r = st->role;
-    const int ru = r[R_U], rup = r[R_UPREV], run = r[R_UNEW];
-    r[R_UPREV] = ru;
-    r[R_U] = run;
-    r[R_UNEW] = rup;
-    const int rv = r[R_V], rvp = r[R_VPREV], rvn = r[R_VNEW];
-    r[R_V] = rvn;
-    r[R_VPREV] = rv;
-    r[R_VNEW] = rvp;
-    const int rg = r[R_G], rgp = r[R_GPREVTMP];
-    r[R_GPREVTMP] = rg;
-    r[R_G] = rgp;
-    st->momentum_prev = st->momentum;
-    st->iter += 1;
-    st->tries = 1;
-    if (st->last) st->done = 1;
-}
-
-// v = uPrev - alpha*gPrevTmp ; u = v + momentumPrev*(v - vPrev) ; clamp v, u
-// (redoIfOvershot body, nesterov.cpp:158-163), u scattered into the node positions.
-__global__ void __launch_bounds__(RED_THREADS) redo_update_kernel(DevPtrs p) {
-    pdl_wait();
-    pdl_trigger();
-    if (!p.st->redo) return;
-    float* v = role_ptr(p, R_V);
-    float* u = role_ptr(p, R_U);
-    const float* up = role_ptr(p, R_UPREV);
-    const float* gp = role_ptr(p, R_GPREVTMP);
-    const float* vp = role_ptr(p, R_VPREV);
-    const float alpha = p.st->alpha, m = p.st->momentum_prev;
-    const int n = p.n_opt;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        float nu[2];
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const int q = c * n + k;
-            const float vk = fsub(up[q], fmul(alpha, gp[q]));
-            const float uk = fadd(vk, fmul(m, fsub(vk, vp[q])));
-            const float lo = p.opt_lo[q], hi = p.opt_hi[q];
-            v[q] = clamp_box(vk, lo, hi);
-            nu[c] = clamp_box(uk, lo, hi);
-            u[q] = nu[c];
-        }
-        if (!isfinite(nu[0]) || !isfinite(nu[1])) raise_error(p.st, SPG_E_NON_FINITE);
-        const int i = p.opt_idx[k];
-        p.x[i] = nu[0];
-        p.y[i] = nu[1];
-    }
+    // the rest of the step (apply_pending_step) runs in the next assembly's last block; every
+    // block read the state above before this store can matter to anyone
+    if (!REDO && blockIdx.x == 0 && threadIdx.x == 0) st->step_pending = apply ? 2 : 1;
 }
 
 __global__ void copy_role_kernel(DevPtrs p, int dst, int src) {
@@ -904,11 +901,18 @@ void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond, cudaGraphCond
 void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
     LAUNCH(loop_cond_kernel, 1, 1, p, loop_cond);
 }
+// One opt node per thread: the step ends in four fixed-point atomics per node, and a grid
+// of many short blocks keeps enough of them in flight (the step writes no partial sums, so
+// its grid need not be one wave).
+inline int node_blocks(const DevPtrs& p) {
+    const int b = ceil_div(static_cast<int64_t>(p.n_opt), RED_THREADS);
+    return b < 1 ? 1 : b;
+}
 void launch_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(update_kernel, wave(update_kernel), RED_THREADS, p);
+    LAUNCH(step_kernel<false>, node_blocks(p), RED_THREADS, p);
 }
 void launch_redo_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(redo_update_kernel, wave(redo_update_kernel), RED_THREADS, p);
+    LAUNCH(step_kernel<true>, node_blocks(p), RED_THREADS, p);
 }
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_lambda_init_kernel, 1, 1, p);

@@ -12,13 +12,18 @@
 // node->pin CSR order, which is exactly the reference's accumulation order, so the node
 // gradient equals the reference's whenever the exponentials agree.
 // HPWL is fused into pass 1 (the reference re-walks all pins for it every evaluation).
+#include <algorithm>
 #include <cfloat>
+#include <cstdlib>
 
 #include "engine.h"
 
 namespace spg {
 
 namespace {
+
+// WA blocks per SM (0: one full wave); SPG_WA_BLOCKS_PER_SM overrides it.
+constexpr int kWaBlocksPerSm = 0;
 
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
@@ -212,8 +217,16 @@ __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
 
 void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, int use_dev,
                     cudaStream_t s) {
-    // one full wave, fixed per device, so the FP64 partials keep a fixed owner per block
-    const int grid = wave_grid(reinterpret_cast<const void*>(wa_net_kernel), RED_THREADS, RED_CAP);
+    // A fixed grid per device, so the FP64 partials keep a fixed owner per block. WA runs
+    // beside the scatter -> rho -> Poisson chain; at most kWaBlocksPerSm blocks per SM leave
+    // each SM room for a Poisson GEMM block (its registers and ~150 KB of shared memory).
+    int per_sm = kWaBlocksPerSm;
+    if (const char* e = std::getenv("SPG_WA_BLOCKS_PER_SM")) per_sm = std::atoi(e);
+    int dev = 0, sms = 0;
+    SPG_CUDA(cudaGetDevice(&dev));
+    SPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int full = wave_grid(reinterpret_cast<const void*>(wa_net_kernel), RED_THREADS, RED_CAP);
+    const int grid = per_sm > 0 ? std::min(full, std::min(per_sm * sms, RED_CAP)) : full;
     launch_pdl(wa_net_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, gamma_dev, gamma_host, use_dev);
 }
 

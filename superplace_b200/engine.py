@@ -221,7 +221,8 @@ class GpContext:
         CUDA events on the context's stream; the stage's results are left unchanged."""
         out = (C.c_double * 8)()
         check(lib().spg_ctx_profile(self.h, reps, out, 8))
-        # "reduce" reports 0: the loop runs the norms and decisions inside the assembly
+        # "reduce" reports 0 (the norms and decisions run inside the assembly), and so does
+        # "scatter" when every density node is in the opt set (the update scatters them)
         return {k: v for k, v in zip(self.PROFILE_PARTS, list(out)) if v > 0.0}
 
     def stream(self) -> int:
