@@ -53,21 +53,34 @@ __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.lau
 // False when SPG_PDL=0 (every launch then waits for the previous kernel as usual).
 bool pdl_enabled();
 
+// Scheduling priority of a launch (a kernel-node attribute, kept by graph capture): the
+// latency-bound chain of an iteration runs at the device's greatest priority, the WA pass
+// beside it at the least, so blocks of the chain get SMs first as blocks retire.
+int launch_priority(bool high);
+
 template <typename... KArgs, typename... Args>
-inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                       Args&&... args) {
+inline void launch_prio(bool high, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                        Args&&... args) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    attr[1].id = cudaLaunchAttributePriority;
+    attr[1].val.priority = launch_priority(high);
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = 2;
     SPG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
     count_launch();
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+    launch_prio(true, kernel, grid, block, smem, s, std::forward<Args>(args)...);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -34,6 +35,17 @@ bool pdl_enabled() {
         return !(e && e[0] == '0');
     }();
     return on;
+}
+
+int launch_priority(bool high) {
+    static int lo = 1, hi = 1;
+    if (lo > 0) {
+        int l = 0, h = 0;
+        SPG_CUDA(cudaDeviceGetStreamPriorityRange(&l, &h));
+        hi = h;
+        lo = l;
+    }
+    return high ? hi : lo;
 }
 
 int wave_grid(const void* kernel, int threads, int cap) {
@@ -532,20 +544,28 @@ void stage_setup(Context& c, int stage) {
 // the density -> Poisson chain; the assembly joins both.
 // `stepped`: the step kernel already added the opt nodes' charge (loop evaluations).
 void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count, bool fused_reduce = false,
-              int use_cond = 0, cudaGraphConditionalHandle redo_h = 0, bool stepped = false) {
+              bool stepped = false) {
     cudaStream_t s = c.stream;
     if (pos_role >= 0) launch_scatter(p, pos_role, s);
-    SPG_CUDA(cudaEventRecord(c.ev_fork, s));
-    SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
-    launch_wa_nets(p, &p.st->gamma, 0.f, 1, c.side);
-    SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
+    static const bool wa_serial = [] {
+        const char* e = std::getenv("SPG_WA_SERIAL");
+        return e && e[0] == '1';
+    }();
+    if (wa_serial) {
+        launch_wa_nets(p, &p.st->gamma, 0.f, 1, s);
+    } else {
+        SPG_CUDA(cudaEventRecord(c.ev_fork, s));
+        SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+        launch_wa_nets(p, &p.st->gamma, 0.f, 1, c.side);
+        SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
+    }
     if (stepped) launch_density_rest(p, s);
     else launch_density_accumulate(p, s);
     launch_rho_overflow(p, 0, 1, s);
     poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s);
     launch_gather_opt_large(p, s);
-    SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
-    if (fused_reduce) launch_assemble_reduce(p, s, use_cond, redo_h);
+    if (!wa_serial) SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
+    if (fused_reduce) launch_assemble_reduce(p, s);
     else launch_assemble(p, pos_role >= 0 ? pos_role : R_U, grad_role, count, s);
 }
 
@@ -648,36 +668,25 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
     *hpwl = out[1];
 }
 
-// One iteration: apply the step decided after the last evaluation (nesterov.cpp:97-119),
-// evaluate at the new u, and run the redo test / next decisions.
-void enqueue_iteration(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
+// One loop pass: the step the last decisions asked for (the next Nesterov step, or a
+// redoIfOvershot re-evaluation step, nesterov.cpp:97-119,158-166), the evaluation at the new
+// u, and the redo test / next decisions. A re-evaluation takes a pass of its own, so the loop
+// body is the same for both.
+void enqueue_iteration(Context& c, const DevPtrs& p) {
     cudaStream_t s = c.stream;
     launch_update(p, s);
-    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h, true);
+    evaluate(c, p, -1, R_G, 1, true, true);
 }
 
-// One redoIfOvershot re-evaluation (nesterov.cpp:158-166) and the next redo test.
-void enqueue_redo(Context& c, const DevPtrs& p, int use_cond, cudaGraphConditionalHandle redo_h) {
-    cudaStream_t s = c.stream;
-    launch_redo_update(p, s);
-    evaluate(c, p, -1, R_G, 1, true, use_cond, redo_h, true);
-}
-
-// Host-driven loop: one 16-byte state read per iteration (and per re-evaluation).
+// Host-driven loop: one state read per pass.
 void host_loop(Context& c, const DevPtrs& p, int max_iter) {
     read_state(c);
     // the device sets `done` by max_iter; this bound guards the host loop itself
-    const int64_t eval_bound = static_cast<int64_t>(max_iter + 2) * std::max(c.prm.max_backtrack, 1);
-    int iter = 0;
+    const int64_t pass_bound = static_cast<int64_t>(max_iter + 2) * std::max(c.prm.max_backtrack, 1);
+    int64_t passes = 0;
     while (!c.hst->done) {
-        if (iter > max_iter || c.hst->evals > eval_bound)
-            throw Error(SPG_E_STATE, "GP loop exceeded its iteration bound");
-        if (c.hst->redo) {
-            enqueue_redo(c, p, 0, 0);
-        } else {
-            enqueue_iteration(c, p, 0, 0);
-            ++iter;
-        }
+        if (++passes > pass_bound) throw Error(SPG_E_STATE, "GP loop exceeded its iteration bound");
+        enqueue_iteration(c, p);
         read_state(c);
     }
 }
@@ -689,7 +698,7 @@ struct LoopGraph {
     cudaGraphExec_t exec = nullptr;
     DevPtrs sig{};
     const void* plan = nullptr;
-    int64_t body_kernels = 0, redo_kernels = 0;
+    int64_t body_kernels = 0;
     ~LoopGraph() { reset(); }
     void reset() {
         if (exec) cudaGraphExecDestroy(exec);
@@ -702,12 +711,30 @@ struct LoopGraph {
 namespace {
 
 // The whole iteration loop as one CUDA graph:
-//   WHILE (!done) {                      loop_h, set by ctl_loop_cond at the end of a body
-//     step; update; iteration end; snapshot; evaluate; norms; redo test -> redo_h
-//     WHILE (redo) { redo update; evaluate; norms; redo test -> redo_h }
-//     ctl_loop_cond -> loop_h
+//   WHILE (!done) {                      loop_h, set by loop_cond_kernel at the end of a body
+//     step (Nesterov or re-evaluation); evaluate; norms and decisions; loop_cond -> loop_h
 //   }
 // Built once per context and stage layout, relaunched on later runs with the same buffers.
+// SPG_GRAPH_STATS=1: print a body graph's node and edge counts, and how many edges are
+// programmatic (PDL) ones, to stderr.
+void graph_stats(const char* name, cudaGraph_t g) {
+    static const bool on = [] {
+        const char* e = std::getenv("SPG_GRAPH_STATS");
+        return e && e[0] == '1';
+    }();
+    if (!on || !g) return;
+    size_t nodes = 0, edges = 0;
+    cudaGraphGetNodes(g, nullptr, &nodes);
+    cudaGraphGetEdges_v2(g, nullptr, nullptr, nullptr, &edges);
+    std::vector<cudaGraphNode_t> from(edges), to(edges);
+    std::vector<cudaGraphEdgeData> data(edges);
+    size_t n = edges;
+    int prog = 0;
+    if (edges && cudaGraphGetEdges_v2(g, from.data(), to.data(), data.data(), &n) == cudaSuccess)
+        for (size_t i = 0; i < n; ++i) prog += data[i].type == cudaGraphDependencyTypeProgrammatic;
+    std::fprintf(stderr, "[spg graph] %s: %zu nodes, %zu edges, %d programmatic\n", name, nodes, edges, prog);
+}
+
 bool build_loop_graph(Context& c, const DevPtrs& p) {
     LoopGraph& lg = *c.loop_graph;
     lg.reset();
@@ -717,7 +744,7 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
     cudaGraph_t g = nullptr;
     if (!ok(cudaGraphCreate(&g, 0))) return false;
     lg.graph = g;
-    cudaGraphConditionalHandle loop_h, redo_h;
+    cudaGraphConditionalHandle loop_h;
     if (!ok(cudaGraphConditionalHandleCreate(&loop_h, g, 1, cudaGraphCondAssignDefault))) return false;
     cudaGraphNodeParams wp{};
     wp.type = cudaGraphNodeTypeConditional;
@@ -727,58 +754,25 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
     cudaGraphNode_t wnode;
     if (!ok(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp))) return false;
     cudaGraph_t body = wp.conditional.phGraph_out[0];
-    if (!ok(cudaGraphConditionalHandleCreate(&redo_h, body, 0, cudaGraphCondAssignDefault))) return false;
-    // outer body: capture the iteration, insert the inner WHILE, then the loop condition
     if (!ok(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
         return false;
-    cudaGraph_t rbody = nullptr;
     bool fine = true;
     try {
         const int64_t k0 = g_launches;
-        enqueue_iteration(c, p, 1, redo_h);
-        cudaStreamCaptureStatus cs;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t ndeps = 0;
-        fine = ok(cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &deps, &ndeps));
-        cudaGraphNodeParams rp{};
-        rp.type = cudaGraphNodeTypeConditional;
-        rp.conditional.handle = redo_h;
-        rp.conditional.type = cudaGraphCondTypeWhile;
-        rp.conditional.size = 1;
-        cudaGraphNode_t rnode;
-        fine = fine && ok(cudaGraphAddNode(&rnode, body, deps, ndeps, &rp));
-        fine = fine && ok(cudaStreamUpdateCaptureDependencies(s, &rnode, 1, cudaStreamSetCaptureDependencies));
-        if (fine) {
-            rbody = rp.conditional.phGraph_out[0];
-            launch_loop_cond(p, loop_h, s);
-        }
+        enqueue_iteration(c, p);
+        launch_loop_cond(p, loop_h, s);
         lg.body_kernels = g_launches - k0;
     } catch (const Error&) {
         fine = false;
     }
     cudaGraph_t out = nullptr;
     const bool ended = ok(cudaStreamEndCapture(s, &out));
-    if (!fine || !ended || !rbody) {
-        cudaGetLastError();
-        g_launches = launches0;
-        return false;
-    }
-    // inner body: one re-evaluation
-    if (!ok(cudaStreamBeginCaptureToGraph(s, rbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
-        return false;
-    try {
-        const int64_t k0 = g_launches;
-        enqueue_redo(c, p, 1, redo_h);
-        lg.redo_kernels = g_launches - k0;
-    } catch (const Error&) {
-        fine = false;
-    }
-    const bool ended2 = ok(cudaStreamEndCapture(s, &out));
     g_launches = launches0;  // executions are counted after each launch
-    if (!fine || !ended2) {
+    if (!fine || !ended) {
         cudaGetLastError();
         return false;
     }
+    graph_stats("loop body", body);
     if (!ok(cudaGraphInstantiate(&lg.exec, g, 0))) {
         cudaGetLastError();
         return false;
@@ -799,8 +793,8 @@ bool graph_loop(Context& c, const DevPtrs& p) {
     }
     SPG_CUDA(cudaGraphLaunch(lg.exec, c.stream));
     read_state(c);
-    // one outer body per applied update, one inner body per re-evaluation
-    g_launches += static_cast<int64_t>(c.hst->iter) * lg.body_kernels + c.hst->redos * lg.redo_kernels;
+    // one body per pass: per applied update and per re-evaluation
+    g_launches += (static_cast<int64_t>(c.hst->iter) + c.hst->redos) * lg.body_kernels;
     return true;
 }
 
@@ -1573,7 +1567,7 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
         spg::launch_assemble_reduce(p, s);
     }, nothing);
     t[6] = 0.0;
-    t[7] = time([&] { spg::evaluate(c, p, -1, spg::R_G, 1, true, 0, 0, true); }, nothing);
+    t[7] = time([&] { spg::evaluate(c, p, -1, spg::R_G, 1, true, true); }, nothing);
     spg::g_launches = launches0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

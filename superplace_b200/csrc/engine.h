@@ -224,18 +224,14 @@ void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s);
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s);
 // WA pass 2 + cell gather + gradient assembly; its last block finalizes the evaluation
 void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s);
-// the loop's evaluation tail: the assembly at u = R_U into g = R_G fused with the reduce
-// kernel's norms and decisions (one launch instead of two)
-void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
-                            cudaGraphConditionalHandle redo_cond = 0);
-// norms of the last evaluation; its last block runs the redo test and the iteration decisions
-void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond = 0,
-                   cudaGraphConditionalHandle redo_cond = 0);
+// the loop's evaluation tail: the assembly at u = R_U into g = R_G with the step's norms
+// and the per-iteration decisions in the same launch
+void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s);
 void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s);
-// the loop's Nesterov step (and its redo variant) with the density scatter of the new
-// positions fused in; the evaluation that follows accumulates only the rest list
+// the loop pass's position step (the Nesterov step, or the re-evaluation step when the last
+// decisions asked for one) with the density scatter of the new positions fused in; the
+// evaluation that follows accumulates only the rest list
 void launch_update(const DevPtrs& p, cudaStream_t s);
-void launch_redo_update(const DevPtrs& p, cudaStream_t s);
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s);
 void launch_init_norms(const DevPtrs& p, cudaStream_t s);
 void launch_ctl_init_scale(const DevPtrs& p, float init_perturb, cudaStream_t s);

@@ -8,16 +8,16 @@
 //   EPlace::run loop body     eplace.cpp:356-474 (lambda/gamma schedule, stop test,
 //                             stagnation snapshots and rollback)
 //
-// One iteration is three kernels around the objective evaluation:
-//   update_kernel   v' = u - alpha g, u' = v' + m (v' - v), clamp, scatter u' into the node
-//                   positions, copy the last evaluated point into a stagnation snapshot when
-//                   one was decided; its last block rotates the optimizer roles
-//   assemble_kernel WA pass 2 + cell gather + gradient assembly; its last block finalizes
-//                   the evaluation (tau, HPWL, WA value, force sums)
-//   reduce_kernel   |u-uPrev|, |g-gPrevTmp|, their dot, |g|^2; its last block runs the
-//                   backtracking test and, when no re-evaluation is due, every per-iteration
-//                   decision of the reference (step size, momentum, lambda/gamma, metrics row,
-//                   stop test, stagnation and snapshot choice)
+// One loop pass is the step kernel, the evaluation, and the assembly that closes it:
+//   step_kernel     v' = u - alpha g, u' = v' + m (v' - v), clamp (or the re-evaluation step
+//                   when the last decisions asked for one), u' into the node positions and
+//                   its fixed-point charge into the density maps; stagnation snapshot copy
+//   assemble_kernel WA pass 2 + cell gather + gradient assembly and, in the same pass, the
+//                   norms |u-uPrev|, |g-gPrevTmp|, their dot and |g|^2; its last block applies
+//                   the step's role rotation, finalizes the evaluation (tau, HPWL, WA value,
+//                   force sums) and runs the backtracking test and every per-iteration decision
+//                   of the reference (step size, momentum, lambda/gamma, metrics row, stop test,
+//                   stagnation and snapshot choice)
 // Vector work runs on fixed grids with grid-stride loops, so every FP64 partial sum has a
 // fixed owner; the "last block" (an atomic ticket) reduces the partials in a fixed tree, so
 // every reduction is deterministic. The host never computes a schedule value.
@@ -445,13 +445,12 @@ __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, d
 // (eplace.cpp:149,154-155,190-197).
 //
 // FUSE (the iteration loop's evaluations, at u = R_U into g = R_G): the same pass also forms
-// reduce_kernel's four norms |u-uPrev|^2, |g-gPrevTmp|^2, (u-uPrev).(g-gPrevTmp), |g|^2 from
-// the values it holds, and its last block runs the decisions after the evaluation's
-// finalize, as the separate reduce kernel would.
+// the four norms |u-uPrev|^2, |g-gPrevTmp|^2, (u-uPrev).(g-gPrevTmp), |g|^2 (l2Diff, dotDiff,
+// l2Norm: nesterov.cpp:25-45) from the values it holds, and its last block runs the redo test
+// (nesterov.cpp:148-157) and the decisions after the evaluation's finalize.
 template <bool FUSE>
 __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int pos_role, int grad_role,
-                                                              int count_eval, int use_cond,
-                                                              cudaGraphConditionalHandle redo_cond) {
+                                                              int count_eval) {
     pdl_wait();
     pdl_trigger();
     // the evaluated positions, by opt index: the role the update (or scatter) wrote the
@@ -550,66 +549,6 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
         decide(p, &sst, sums[5], sums[6], sums[7], sums[8]);
     }
     state_copy_out(p.st, &sst);
-    if (threadIdx.x == 0 && use_cond) cudaGraphSetConditional(redo_cond, sst.redo ? 1u : 0u);
-}
-
-// After every counted evaluation: |u-uPrev|^2, |g-gPrevTmp|^2, their dot and |g|^2
-// (l2Diff, dotDiff, l2Norm: nesterov.cpp:25-45) in one pass; the last block then runs
-// redoIfOvershot's test (nesterov.cpp:148-157) -- redo when 1/L at the new point is at
-// most 0.95 of the step just taken, at most max_backtrack-1 times per step, only with
-// backtracking on and after the first step -- and otherwise decides the iteration. In graph
-// mode it sets the re-evaluation loop's conditional handle.
-__global__ void __launch_bounds__(RED_THREADS) reduce_kernel(DevPtrs p, int use_cond,
-                                                            cudaGraphConditionalHandle redo_cond) {
-    pdl_wait();
-    pdl_trigger();
-    const float* __restrict__ u = role_ptr(p, R_U);
-    const float* __restrict__ up = role_ptr(p, R_UPREV);
-    const float* __restrict__ g = role_ptr(p, R_G);
-    const float* __restrict__ gp = role_ptr(p, R_GPREVTMP);
-    const int n = 2 * p.n_opt, n4 = n >> 2;
-    double dx = 0.0, dg = 0.0, sy = 0.0, gn = 0.0;
-    auto term = [&](float a, float b, float c, float d) {
-        const double s = static_cast<double>(a) - static_cast<double>(b);
-        const double y = static_cast<double>(c) - static_cast<double>(d);
-        const double gv = static_cast<double>(c);
-        dx += __dmul_rn(s, s);
-        dg += __dmul_rn(y, y);
-        sy += __dmul_rn(s, y);
-        gn += __dmul_rn(gv, gv);
-    };
-    // float4 groups of the flat 2n values (256-byte aligned role vectors), then the tail
-    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n4; t += gridDim.x * blockDim.x) {
-        const float4 a = reinterpret_cast<const float4*>(u)[t];
-        const float4 b = reinterpret_cast<const float4*>(up)[t];
-        const float4 c = reinterpret_cast<const float4*>(g)[t];
-        const float4 d = reinterpret_cast<const float4*>(gp)[t];
-        term(a.x, b.x, c.x, d.x);
-        term(a.y, b.y, c.y, d.y);
-        term(a.z, b.z, c.z, d.z);
-        term(a.w, b.w, c.w, d.w);
-    }
-    for (int k = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-        term(u[k], up[k], g[k], gp[k]);
-    double v4[4] = {dx, dg, sy, gn};
-    block_sums(v4);
-    dx = v4[0];
-    dg = v4[1];
-    sy = v4[2];
-    gn = v4[3];
-    put_partial(p, SLOT_DX, dx);
-    put_partial(p, SLOT_DG, dg);
-    put_partial(p, SLOT_SY, sy);
-    put_partial(p, SLOT_GN, gn);
-    if (!last_block(&p.st->tk_reduce)) return;
-    constexpr int kSlots[4] = {SLOT_DX, SLOT_DG, SLOT_SY, SLOT_GN};
-    double sums[4];
-    finalize_n(p, kSlots, sums);
-    __shared__ DevState sst;
-    state_copy_in(&sst, p.st);
-    if (threadIdx.x == 0) decide(p, &sst, sums[0], sums[1], sums[2], sums[3]);
-    state_copy_out(p.st, &sst);
-    if (threadIdx.x == 0 && use_cond) cudaGraphSetConditional(redo_cond, sst.redo ? 1u : 0u);
 }
 
 // Graph mode: the iteration loop continues while the stage is not done.
@@ -620,35 +559,37 @@ __global__ void loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond
     cudaGraphSetConditional(loop_cond, (st->done || st->error) ? 0u : 1u);
 }
 
-// The loop's position step with the density scatter of the new positions fused in.
+// The loop's position step with the density scatter of the new positions fused in. One
+// launch per loop pass; the pass applies whichever step the last decisions asked for:
 //
-//   REDO = false (NesterovOptimizer::step, nesterov.cpp:97-119):
+//   a re-evaluation (st->redo; redoIfOvershot body, nesterov.cpp:158-163):
+//     v = uPrev - alpha gPrevTmp ; u = v + momentumPrev (v - vPrev) ; clamp v, u.
+//   otherwise the next step (NesterovOptimizer::step, nesterov.cpp:97-119):
 //     v' = u - alpha g ; u' = v' + momentum (v' - v) ; clamp both (nesterov.cpp:97-107); when
 //     the iteration decided a stagnation snapshot, the evaluated u is copied into its slot.
-//     The last block rotates the roles: uPrev <- u <- u' ; vPrev <- v <- v' ; gPrevTmp <- g.
-//   REDO = true (redoIfOvershot body, nesterov.cpp:158-163):
-//     v = uPrev - alpha gPrevTmp ; u = v + momentumPrev (v - vPrev) ; clamp v, u.
+//     The role rotation uPrev <- u <- u' ; vPrev <- v <- v' ; gPrevTmp <- g and the loop
+//     counter follow in the next assembly's last block (apply_pending_step).
 //
 // The new u is written into the node positions (for the WA pass) and its fixed-point charge
 // is added to the density maps right here (BinGrid::accumulate, bin_grid.cpp:191-251), so
 // the evaluation needs no separate pass over the cells; nodes whose footprint may exceed 16
 // bins are left to the block-per-node kernel of the rest list. When no step applies (the
-// stage is done, or no re-evaluation was decided) the current u is rasterized unchanged.
-template <bool REDO>
+// stage is done) the current u is rasterized unchanged.
 __global__ void __launch_bounds__(RED_THREADS) step_kernel(DevPtrs p) {
     pdl_wait();
     pdl_trigger();
     DevState* st = p.st;
-    const int apply = REDO ? st->redo : !st->done;
-    const int slot = REDO ? -1 : st->snap_copy_to;
-    const float* u = role_ptr(p, REDO ? R_UPREV : R_U);
-    const float* v = role_ptr(p, REDO ? R_VPREV : R_V);
-    const float* g = role_ptr(p, REDO ? R_GPREVTMP : R_G);
-    float* vn = role_ptr(p, REDO ? R_V : R_VNEW);
-    float* un = role_ptr(p, REDO ? R_U : R_UNEW);
+    const bool redo = st->redo != 0;
+    const int apply = redo ? 1 : !st->done;
+    const int slot = redo ? -1 : st->snap_copy_to;
+    const float* u = role_ptr(p, redo ? R_UPREV : R_U);
+    const float* v = role_ptr(p, redo ? R_VPREV : R_V);
+    const float* g = role_ptr(p, redo ? R_GPREVTMP : R_G);
+    float* vn = role_ptr(p, redo ? R_V : R_VNEW);
+    float* un = role_ptr(p, redo ? R_U : R_UNEW);
     const float* cur = role_ptr(p, R_U);
     float* snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
-    const float alpha = st->alpha, m = REDO ? st->momentum_prev : st->momentum;
+    const float alpha = st->alpha, m = redo ? st->momentum_prev : st->momentum;
     const int n = p.n_opt;
     bool bad = false;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -685,7 +626,7 @@ __global__ void __launch_bounds__(RED_THREADS) step_kernel(DevPtrs p) {
     if (bad) raise_error(st, SPG_E_NON_FINITE);
     // the rest of the step (apply_pending_step) runs in the next assembly's last block; every
     // block read the state above before this store can matter to anyone
-    if (!REDO && blockIdx.x == 0 && threadIdx.x == 0) st->step_pending = apply ? 2 : 1;
+    if (!redo && blockIdx.x == 0 && threadIdx.x == 0) st->step_pending = apply ? 2 : 1;
 }
 
 __global__ void copy_role_kernel(DevPtrs p, int dst, int src) {
@@ -889,14 +830,11 @@ void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
 }
 void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s) {
     LAUNCH(assemble_kernel<false>, wave(assemble_kernel<false>), RED_THREADS, p, pos_role, grad_role,
-           count_eval, 0, cudaGraphConditionalHandle{});
+           count_eval);
 }
-void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, int use_cond, cudaGraphConditionalHandle redo_cond) {
+void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(assemble_kernel<true>, wave(assemble_kernel<true>), RED_THREADS, p, static_cast<int>(R_U),
-           static_cast<int>(R_G), 1, use_cond, redo_cond);
-}
-void launch_reduce(const DevPtrs& p, cudaStream_t s, int use_cond, cudaGraphConditionalHandle redo_cond) {
-    LAUNCH(reduce_kernel, wave(reduce_kernel), RED_THREADS, p, use_cond, redo_cond);
+           static_cast<int>(R_G), 1);
 }
 void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
     LAUNCH(loop_cond_kernel, 1, 1, p, loop_cond);
@@ -909,10 +847,7 @@ inline int node_blocks(const DevPtrs& p) {
     return b < 1 ? 1 : b;
 }
 void launch_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(step_kernel<false>, node_blocks(p), RED_THREADS, p);
-}
-void launch_redo_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(step_kernel<true>, node_blocks(p), RED_THREADS, p);
+    LAUNCH(step_kernel, node_blocks(p), RED_THREADS, p);
 }
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_lambda_init_kernel, 1, 1, p);

@@ -4,12 +4,13 @@
 // split-BF16 product: each FP32 operand x is stored as two BF16 planes hi = bf16(x),
 // lo = bf16(x - hi), and C = A_hi.B_hi + A_hi.B_lo + A_lo.B_hi accumulated in FP32 in
 // tensor memory (the lo.lo term, ~2^-16 relative, is dropped). The three products are one
-// accumulation over K' = 3K: the producer walks (hi,hi), (hi,lo), (lo,hi) K slabs.
+// accumulation: each K slab's four planes arrive in one ring stage and the MMA thread issues
+// hi.hi, hi.lo and lo.hi for every 16-wide K step.
 //
 // Kernel (one 128 x BN output tile per cluster of S split-K CTAs, 128 threads each):
-//   warp 0 lane 0   TMA producer: 128x64 A and BNx64 B bf16 tiles (128-byte swizzle)
-//                   into a STAGES-deep shared-memory ring (full/empty mbarriers)
-//   warp 1 lane 0   MMA issuer: 4 x tcgen05.mma.kind::f16 (M=128, N=BN, K=16) per slab,
+//   warp 0 lane 0   TMA producer: 128x64 A hi/lo and BNx64 B hi/lo bf16 tiles (128-byte
+//                   swizzle) into a STAGES-deep shared-memory ring (full/empty mbarriers)
+//   warp 1 lane 0   MMA issuer: 12 x tcgen05.mma.kind::f16 (M=128, N=BN, K=16) per slab,
 //                   tcgen05.commit frees the slab, a final commit publishes the accumulator
 //   warps 0-3       epilogue: tcgen05.ld of the TMEM partial into shared memory, a
 //                   cluster-wide reduction of the S partials over DSMEM (rank order), the
@@ -186,29 +187,33 @@ __device__ __forceinline__ float4 ld_dsmem4(uint32_t addr) {
 }
 
 // Grid (S, N/BN, (M/128) * batch), cluster (S, 1, 1): the S CTAs of a cluster share one
-// 128 x BN output tile and split its 3K/64 K slabs evenly (split-K). Each accumulates its
-// slice in TMEM and stages it in shared memory; then CTA r reduces rows
-// [r*128/S, (r+1)*128/S) over the cluster's S partials through distributed shared memory,
-// in rank order (deterministic), and runs the epilogue for those rows with consecutive
-// threads on consecutive columns (coalesced stores).
-template <int BN, int STAGES>
+// 128 x BN output tile and split its K/64 K slabs evenly (split-K). A ring stage holds one K
+// slab of all four operand planes (A hi, A lo, B hi, B lo), from which the MMA thread issues
+// the three products, so every plane crosses L2 once per slab. Each CTA accumulates its slice
+// in TMEM and stages it in shared memory; then CTA r reduces rows [r*128/S, (r+1)*128/S)
+// over the cluster's S partials through distributed shared memory, in rank order
+// (deterministic), with all of its remote loads in flight at once, and runs the epilogue for
+// those rows with consecutive threads on consecutive columns (coalesced stores).
+template <int BN, int STAGES, int S>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const TcArgs g) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;
+    constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;  // one plane
     constexpr uint32_t B_BYTES = BN * TC_BK * 2;
+    constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
     constexpr int RED_LD = BN + 4;  // staged partial tile row pitch (floats, 16-byte rows)
-    static_assert(TC_BM * RED_LD * 4 <= STAGES * (A_BYTES + B_BYTES), "partial tile must fit the ring");
+    constexpr int R = TC_BM / S;    // output rows this CTA reduces
+    constexpr int GPT = R * (BN / 4) / TC_THREADS;  // float4 groups per thread
+    static_assert(GPT >= 1 && R * (BN / 4) % TC_THREADS == 0, "reduction must split evenly");
+    static_assert(TC_BM * RED_LD * 4 <= STAGES * STAGE_BYTES, "partial tile must fit the ring");
     uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sA = base;
-    uint8_t* sB = base + STAGES * A_BYTES;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + STAGES * B_BYTES);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
     float* red = reinterpret_cast<float*>(base);  // reuses the ring after the main loop
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int S = gridDim.x, rank = blockIdx.x;
+    const int rank = blockIdx.x;
     const int tiles_m = g.M / TC_BM;
     const int n0 = blockIdx.y * BN, m0 = (blockIdx.z % tiles_m) * TC_BM, z = blockIdx.z / tiles_m;
     const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES), accb = smem_u32(bars + 2 * STAGES);
@@ -236,21 +241,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     pdl_wait();
     pdl_trigger();
 
-    const int kpp = g.K / TC_BK;  // slabs per split pass
-    const int nk = 3 * kpp;
+    const int nk = g.K / TC_BK;
     const int s0 = rank * nk / S, s1 = (rank + 1) * nk / S;
     if (warp == 0 && lane == 0) {
-        // producer: passes (A_hi,B_hi), (A_hi,B_lo), (A_lo,B_hi) over this CTA's slabs
+        // producer: one stage = K slab kk of A hi, A lo, B hi, B lo
         for (int s = s0; s < s1; ++s) {
             const int i = s - s0, st = i % STAGES;
             const uint32_t ph = (i / STAGES) & 1;
             if (!mbar_wait(empty0 + 8 * st, ph ^ 1)) break;
-            const int pass = s / kpp, kk = (s % kpp) * TC_BK;
-            const int arow = g.a_row0 + m0 + (pass == 2 ? g.a_lo : 0);
-            const int brow = g.b_row0 + n0 + (pass == 1 ? g.b_lo : 0);
-            mbar_expect_tx(full0 + 8 * st, A_BYTES + B_BYTES);
-            tma_load_2d(smem_u32(sA + st * A_BYTES), &tmA, kk, arow, full0 + 8 * st);
-            tma_load_2d(smem_u32(sB + st * B_BYTES), &tmB, kk + z * g.b_col_z, brow, full0 + 8 * st);
+            const int kk = s * TC_BK;
+            const uint32_t sa = smem_u32(base + st * STAGE_BYTES);
+            const int arow = g.a_row0 + m0, brow = g.b_row0 + n0, bcol = kk + z * g.b_col_z;
+            mbar_expect_tx(full0 + 8 * st, STAGE_BYTES);
+            tma_load_2d(sa, &tmA, kk, arow, full0 + 8 * st);
+            tma_load_2d(sa + A_BYTES, &tmA, kk, arow + g.a_lo, full0 + 8 * st);
+            tma_load_2d(sa + 2 * A_BYTES, &tmB, bcol, brow, full0 + 8 * st);
+            tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tmB, bcol, brow + g.b_lo, full0 + 8 * st);
         }
     } else if (warp == 1 && lane == 0) {
         constexpr uint32_t idesc = idesc_bf16(TC_BM, BN);
@@ -263,16 +269,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t a0 = smem_u32(sA + st * A_BYTES), b0 = smem_u32(sB + st * B_BYTES);
+            const uint32_t ahi = smem_u32(base + st * STAGE_BYTES), alo = ahi + A_BYTES;
+            const uint32_t bhi = ahi + 2 * A_BYTES, blo = bhi + B_BYTES;
 #pragma unroll
-            for (int k = 0; k < TC_BK / 16; ++k)  // 16 bf16 = 32 bytes per MMA along K
-                umma_bf16(tmem, sw128_desc(a0 + 32 * k), sw128_desc(b0 + 32 * k), idesc,
-                          (i > 0 || k > 0) ? 1u : 0u);
+            for (int k = 0; k < TC_BK / 16; ++k) {  // 16 bf16 = 32 bytes per MMA along K
+                const uint32_t o = 32 * k;
+                umma_bf16(tmem, sw128_desc(ahi + o), sw128_desc(bhi + o), idesc, (i > 0 || k > 0) ? 1u : 0u);
+                umma_bf16(tmem, sw128_desc(ahi + o), sw128_desc(blo + o), idesc, 1u);
+                umma_bf16(tmem, sw128_desc(alo + o), sw128_desc(bhi + o), idesc, 1u);
+            }
             umma_commit(empty0 + 8 * st);
         }
         if (ok) umma_commit(accb);
     }
     __syncwarp();
+
+    // epilogue inputs that do not depend on the partials, fetched while the MMAs run: this
+    // thread's output groups (row, 4 columns), the spectral scale and the exact DC row
+    int grow[GPT], gcol[GPT];
+    float4 sc[GPT];
+#pragma unroll
+    for (int j = 0; j < GPT; ++j) {
+        const int e = threadIdx.x + j * TC_THREADS;
+        grow[j] = rank * R + e / (BN / 4);
+        gcol[j] = (e % (BN / 4)) * 4;
+        const int m = m0 + grow[j], n = n0 + gcol[j];
+        sc[j] = g.scale ? __ldg(reinterpret_cast<const float4*>(g.scale + m * g.lds + n)) : make_float4(1.f, 1.f, 1.f, 1.f);
+        if (m == 0 && g.row0) {
+            const float4 r0 = __ldg(reinterpret_cast<const float4*>(g.row0 + z * g.row0_z + n));
+            sc[j] = make_float4(r0.x * sc[j].x, r0.y * sc[j].y, r0.z * sc[j].z, r0.w * sc[j].w);
+        }
+    }
 
     // stage this CTA's partial tile (TMEM lane = tile row; warp w owns rows 32w..32w+31)
     const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0) ? 1 : 0) != 0;
@@ -284,7 +311,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             float v[32];
             tmem_ld32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + c, v);
 #pragma unroll
-            for (int i = 0; i < 32; ++i) red[r * RED_LD + c + i] = v[i];
+            for (int i = 0; i < 32; i += 4)
+                *reinterpret_cast<float4*>(red + r * RED_LD + c + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
         }
     } else if (threadIdx.x == 0) {
         atomicCAS(g.err, 0, SPG_E_CUDA);
@@ -292,35 +320,36 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int ok_cta = __syncthreads_and(acc_ok ? 1 : 0);
     cluster_sync_all();  // every CTA of the cluster has staged its partial
 
-    // reduce rows [rank*R, rank*R + R) over the S partials (4 columns per thread, rank
-    // order) and write them
-    const int R = TC_BM / S;
     if (ok_cta) {
         const uint32_t red_addr = smem_u32(red);
-        uint32_t rbase[8];
+        float4 parts[GPT][S];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) rbase[q] = q < S ? map_rank(red_addr, static_cast<uint32_t>(q)) : 0u;
-        for (int e = threadIdx.x; e < R * (BN / 4); e += TC_THREADS) {
-            const int row = rank * R + e / (BN / 4), col = (e % (BN / 4)) * 4;
-            const uint32_t off = 4u * static_cast<uint32_t>(row * RED_LD + col);
-            float4 parts[8];
+        for (int j = 0; j < GPT; ++j) {
+            const uint32_t off = 4u * static_cast<uint32_t>(grow[j] * RED_LD + gcol[j]);
 #pragma unroll
-            for (int q = 0; q < 8; ++q)
-                if (q < S) parts[q] = ld_dsmem4(rbase[q] + off);
+            for (int q = 0; q < S; ++q) parts[j][q] = ld_dsmem4(map_rank(red_addr, static_cast<uint32_t>(q)) + off);
+        }
+#pragma unroll
+        for (int j = 0; j < GPT; ++j) {
             float v[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                if (q >= S) break;
-                v[0] += parts[q].x;
-                v[1] += parts[q].y;
-                v[2] += parts[q].z;
-                v[3] += parts[q].w;
+            for (int q = 0; q < S; ++q) {
+                v[0] += parts[j][q].x;
+                v[1] += parts[j][q].y;
+                v[2] += parts[j][q].z;
+                v[3] += parts[j][q].w;
             }
-            const int m = m0 + row, n = n0 + col;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-                if (m == 0 && g.row0) v[i] = g.row0[z * g.row0_z + n + i];
-                if (g.scale) v[i] *= g.scale[m * g.lds + n + i];
+            const int m = m0 + grow[j], n = n0 + gcol[j];
+            if (m == 0 && g.row0) {  // the DC row: the exact sums (times the scale), in sc
+                v[0] = sc[j].x;
+                v[1] = sc[j].y;
+                v[2] = sc[j].z;
+                v[3] = sc[j].w;
+            } else if (g.scale) {
+                v[0] *= sc[j].x;
+                v[1] *= sc[j].y;
+                v[2] *= sc[j].z;
+                v[3] *= sc[j].w;
             }
             if (g.mode == TC_F32) {
                 float* dst = (m < g.split) ? g.out + z * g.out_z + m * g.ldc
@@ -403,11 +432,12 @@ CUtensorMap make_map(const uint16_t* ptr, int64_t rows, int64_t cols, int box_ro
 }
 
 constexpr int TC_BN = 64;
-constexpr int TC_STAGES = 6;
+constexpr int TC_STAGES = 4;
 constexpr size_t tc_smem_bytes() {
-    // 1024-byte alignment slack + stage ring + mbarriers + TMEM address slot
-    return 1024 + TC_STAGES * (TC_BM * TC_BK * 2 + TC_BN * TC_BK * 2) + (2 * TC_STAGES + 1) * 8 + 128;
+    // 1024-byte alignment slack + stage ring (four planes per stage) + mbarriers + TMEM slot
+    return 1024 + TC_STAGES * 2 * (TC_BM * TC_BK * 2 + TC_BN * TC_BK * 2) + (2 * TC_STAGES + 1) * 8 + 128;
 }
+static_assert(tc_smem_bytes() <= 227 * 1024, "ring exceeds the shared memory of one CTA");
 
 struct TcState {
     // tensor maps: bases (A operands) and data planes (B operands)
@@ -432,22 +462,29 @@ void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int 
                cudaStream_t s) {
     SPG_REQUIRE(g.M % TC_BM == 0 && g.N % TC_BN == 0 && g.K % TC_BK == 0, SPG_E_INVALID,
                 "tensor-core GEMM dims must be tile multiples");
-    const int S = pick_splits(grid_tiles, 3 * (g.K / TC_BK));
+    const int S = pick_splits(grid_tiles, g.K / TC_BK);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(S, g.N / TC_BN, (g.M / TC_BM) * batch);
     cfg.blockDim = dim3(TC_THREADS);
     cfg.dynamicSmemBytes = tc_smem_bytes();
     cfg.stream = s;
-    cudaLaunchAttribute attr[2];
+    cudaLaunchAttribute attr[3];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = S;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    attr[2].id = cudaLaunchAttributePriority;
+    attr[2].val.priority = launch_priority(true);
     cfg.attrs = attr;
-    cfg.numAttrs = 2;
-    SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES>, a, b, g));
+    cfg.numAttrs = 3;
+    switch (S) {
+        case 8: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 8>, a, b, g)); break;
+        case 4: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 4>, a, b, g)); break;
+        case 2: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 2>, a, b, g)); break;
+        default: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 1>, a, b, g)); break;
+    }
     count_launch();
 }
 
@@ -519,9 +556,11 @@ void tc_plan_create(PoissonPlan& pl) {
     st->t12t_b = make_map(pl.t12t_s, 4 * Y, B * X, TC_BN);
     static bool attr = false;
     if (!attr) {
-        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(tc_smem_bytes())));
+        const int bytes = static_cast<int>(tc_smem_bytes());
+        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         attr = true;
     }
 }

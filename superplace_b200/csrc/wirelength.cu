@@ -227,7 +227,7 @@ void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, 
     SPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int full = wave_grid(reinterpret_cast<const void*>(wa_net_kernel), RED_THREADS, RED_CAP);
     const int grid = per_sm > 0 ? std::min(full, std::min(per_sm * sms, RED_CAP)) : full;
-    launch_pdl(wa_net_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, gamma_dev, gamma_host, use_dev);
+    launch_prio(false, wa_net_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, gamma_dev, gamma_host, use_dev);
 }
 
 void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s) {
