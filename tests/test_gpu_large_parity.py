@@ -1,0 +1,57 @@
+"""End-to-end parity at full size (GPU only): the 211k-cell netlist at 512x512 bins, tau 0.10.
+
+The reference's CPU EPlace (its own sources, compiled in oracle/_ref; the Poisson solve is the
+FFT stand-in for FFTW) places the same instance from the same initial positions on all host
+cores; the device runs the same stage with the plain FP32 and the split-BF16 Poisson. The bar
+is the one set for this path: the device run reaches tau < 0.10 and its final HPWL lies within
+0.5% of the CPU run's. Iteration counts must agree within 25%, and the first iteration (same
+instance, same positions) must report the same HPWL.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from superplace_b200 import abi, engine, generator
+
+pytestmark = pytest.mark.gpu
+
+HPWL_TOL = 0.005
+BINS = 512
+
+
+@pytest.fixture(scope="module")
+def instance():
+    db = generator.large_design(1002)
+    engine.initialize_fillers(db, 1.0, 1002)
+    return db
+
+
+@pytest.fixture(scope="module")
+def reference(instance):
+    from oracle import ref
+
+    if not ref.available():
+        pytest.skip("oracle/_ref/libspref.so not built")
+    ref.lib().spref_set_threads(os.cpu_count() or 1)
+    res, rows = ref.RefDb(instance).eplace(abi.default_params(gp_bin_dim=BINS))
+    return res, rows
+
+
+def run_device(db0, precision):
+    db = db0.copy()
+    ep = engine.EPlace(db, abi.default_params(gp_bin_dim=BINS, poisson_precision=precision))
+    r = ep.run(abi.STAGE_MGP)
+    return r, ep.ctx.metrics()
+
+
+@pytest.mark.parametrize("precision", [abi.POISSON_BF16X3, abi.POISSON_FP32], ids=["bf16x3", "fp32"])
+def test_final_hpwl_within_half_percent_of_cpu(instance, reference, precision):
+    res, rows = reference
+    r, m = run_device(instance, precision)
+    assert r.converged == 1 and r.overflow < 0.10
+    assert abs(r.hpwl - res["hpwl"]) <= HPWL_TOL * res["hpwl"], (r.hpwl, res["hpwl"])
+    assert abs(r.iterations - res["iterations"]) <= 0.25 * res["iterations"]
+    # iteration 0 sees the same instance at the same positions
+    assert abs(m["hpwl"][0] - rows[0, 1]) <= 1e-9 * rows[0, 1]
+    assert abs(m["overflow"][0] - rows[0, 2]) <= 1e-5
