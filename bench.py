@@ -13,6 +13,7 @@ src/gp/eplace.cpp:310,515).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision bf16x3|fp32] [--workload large|small]
+       python bench.py --poisson-sweep | --precision-study   (studies: JSON lines of their own)
 The default Poisson arithmetic is split-BF16 on tcgen05 (bf16x3); fp32 is the plain FP32 form.
 Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
 """
@@ -352,6 +353,124 @@ def run_ours(args):
     return 0
 
 
+# ------------------------------------------------------------------ extra studies
+def blob_density(m, seed):
+    """The operator sweep's density: 50 seeded Gaussian blobs (sigma U[2,40] bins, amplitude
+    U[0.5,3]) on a 0.3 floor, clipped at 0 and mean-removed."""
+    rng = np.random.default_rng(seed)
+    c = np.arange(m, dtype=np.float64) + 0.5
+    v = np.full((m, m), 0.3)
+    for _ in range(50):
+        cx, cy = rng.uniform(0, m, 2)
+        sig = rng.uniform(2, 40)
+        amp = rng.uniform(0.5, 3)
+        gx = np.exp(-((c - cx) ** 2) / (2 * sig * sig))
+        gy = np.exp(-((c - cy) ** 2) / (2 * sig * sig))
+        v += amp * np.outer(gx, gy)
+    v = np.clip(v, 0, None)
+    return (v - v.mean()).astype(np.float32)
+
+
+def rel_errors(ref, got):
+    ref = np.asarray(ref, np.float64)
+    d = np.asarray(got, np.float64) - ref
+    scale = max(np.abs(ref).max(), 1e-300)
+    return [float(np.abs(d).max() / scale), float(np.sqrt(np.mean(d * d)) / scale)]
+
+
+def run_poisson_sweep(args):
+    """Operator sweep over grid sizes and batches: device time per solve of the FP32 and the
+    split-BF16 forms (L2 flushed before every timed call), algorithmic TFLOP/s (14 M^3 per
+    grid) against the measured bf16 peak, and max/RMS error of phi, xi_x, xi_y against the
+    FP64 form; the reference's CPU solve (FFT stand-in for FFTW) timed beside them."""
+    import torch
+
+    from superplace_b200 import engine
+
+    _, bf16, peak_kind = peaks()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    s = torch.cuda.current_stream()
+    for m in (128, 512, 1024, 2048):
+        rho1 = blob_density(m, 1000 + m)
+        ref64 = engine.PoissonBackend(m, m, 1.0, 1.0, abi.POISSON_FP64).solve(rho1)
+        cpu = None
+        try:
+            from oracle import ref
+
+            if ref.available():
+                ref.lib().spref_set_threads(os.cpu_count() or 1)
+                ref.poisson(rho1, 1.0, 1.0)
+                t0 = time.perf_counter()
+                for _ in range(3):
+                    ref.poisson(rho1, 1.0, 1.0)
+                cpu = (time.perf_counter() - t0) / 3 * 1e6
+        except Exception:  # the CPU column must not hide the device numbers
+            cpu = None
+        for prec, name in ((abi.POISSON_FP32, "fp32"), (abi.POISSON_BF16X3, "bf16x3")):
+            got = engine.PoissonBackend(m, m, 1.0, 1.0, prec).solve(rho1)
+            err = {k: rel_errors(r, g) for k, r, g in zip(("phi", "xi_x", "xi_y"), ref64, got)}
+            for batch in (1, 64):
+                be = engine.PoissonBackend(m, m, 1.0, 1.0, prec, batch=batch)
+                rho = torch.from_numpy(np.ascontiguousarray(np.broadcast_to(rho1, (batch, m, m)))).cuda()
+                out = [torch.empty_like(rho) for _ in range(3)]
+                call = lambda: be.solve_device(rho.data_ptr(), *(o.data_ptr() for o in out),
+                                               stream=s.cuda_stream, batch=batch)
+                for _ in range(3):
+                    call()
+                times = []
+                for _ in range(10 if batch == 1 else 3):
+                    flush.zero_()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(s)
+                    call()
+                    e1.record(s)
+                    e1.synchronize()
+                    times.append(e0.elapsed_time(e1) * 1e3)
+                us = statistics.median(times)
+                tflops = 14.0 * m ** 3 * batch / (us * 1e-6) / 1e12
+                print(json.dumps({"study": "poisson-sweep", "grid": m, "batch": batch, "precision": name,
+                                  "us_per_call": us, "us_per_grid": us / batch, "grids_per_s": batch / (us * 1e-6),
+                                  "tflops_algorithmic": tflops, "frac_of_bf16_peak": tflops / bf16,
+                                  "peak_kind": peak_kind, "err_vs_fp64": err,
+                                  "cpu_reference_us_per_grid": cpu, "cpu_cores": os.cpu_count()}), flush=True)
+                del be, rho, out
+                torch.cuda.empty_cache()
+    return 0
+
+
+def run_precision_study(args):
+    """The 211k-cell mGP stage with the FP64, FP32 and split-BF16 Poisson forms and the
+    reference's CPU run: iterations, final tau and HPWL, and HPWL against FP64 and CPU."""
+    from superplace_b200 import engine
+
+    db = make_design("large")
+    engine.initialize_fillers(db, 1.0, 1002)
+    out = {}
+    for prec, name in ((abi.POISSON_FP64, "fp64"), (abi.POISSON_FP32, "fp32"), (abi.POISSON_BF16X3, "bf16x3")):
+        d = db.copy()
+        r = engine.EPlace(d, abi.default_params(gp_bin_dim=512, poisson_precision=prec)).run(abi.STAGE_MGP)
+        out[name] = {"iterations": r.iterations, "hpwl": r.hpwl, "tau": r.overflow, "converged": r.converged,
+                     "loop_ms": r.elapsed_ms}
+    cpu = None
+    try:
+        from oracle import ref
+
+        if ref.available():
+            ref.lib().spref_set_threads(os.cpu_count() or 1)
+            res, _ = ref.RefDb(db).eplace(abi.default_params(gp_bin_dim=512))
+            cpu = {"iterations": int(res["iterations"]), "hpwl": res["hpwl"], "tau": res["overflow"],
+                   "converged": int(res["converged"]), "loop_ms": res["elapsed_ms"]}
+    except Exception as e:
+        cpu = {"failed": str(e)}
+    for name, v in out.items():
+        v["hpwl_vs_fp64"] = v["hpwl"] / out["fp64"]["hpwl"] - 1.0
+        if cpu and "hpwl" in cpu:
+            v["hpwl_vs_cpu"] = v["hpwl"] / cpu["hpwl"] - 1.0
+    print(json.dumps({"study": "precision", "workload": WORKLOADS["large"]["desc"], "device": out,
+                      "cpu_reference": cpu, "cpu_cores": os.cpu_count()}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -362,7 +481,15 @@ def main():
     ap.add_argument("--workload", default="large", choices=list(WORKLOADS))
     ap.add_argument("--ref-iters", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--poisson-sweep", action="store_true",
+                    help="operator sweep (grids 128..2048, batch 1 and 64): JSON lines, not the bench line")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="211k mGP with FP64 / FP32 / BF16x3 Poisson and the CPU reference: one JSON line")
     args = ap.parse_args()
+    if args.poisson_sweep:
+        return run_poisson_sweep(args)
+    if args.precision_study:
+        return run_precision_study(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -49,6 +49,7 @@ extern "C" {
 /* ---- Poisson arithmetic */
 #define SPG_POISSON_FP32 0   /* cosine contractions as FP32 SIMT GEMMs ("plain FP32")        */
 #define SPG_POISSON_BF16X3 1 /* tcgen05 split-BF16 (hi*hi + hi*lo + lo*hi), FP32 accumulate */
+#define SPG_POISSON_FP64 2   /* the same contractions in FP64 (accuracy reference, slow)      */
 
 /* ---- GP stages (sp::GpStage, src/gp/eplace.h:24-28) */
 #define SPG_STAGE_MGP 0

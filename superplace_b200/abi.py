@@ -20,6 +20,7 @@ F_MACRO, F_FIXED, F_FILLER, F_NI = 1, 2, 4, 8
 
 POISSON_FP32 = 0
 POISSON_BF16X3 = 1
+POISSON_FP64 = 2
 
 STAGE_MGP, STAGE_FILLER_ONLY, STAGE_CGP = 0, 1, 2
 

@@ -4,7 +4,9 @@
 // The FP32 path is a register-tiled SIMT SGEMM (64x64 tile, 4x4 per thread, BK 16,
 // register prefetch of the next K slab). It is the "plain FP32 GPU form" the split-BF16
 // tensor-core path (poisson_tc.cu) is measured against, and the exact-enough reference
-// for the parity tests at 1e-5.
+// for the parity tests at 1e-5. The FP64 path runs the same kernel in double: the accuracy
+// reference of the precision study (potential, field and final HPWL against FP32 and
+// split-BF16), not a production form.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -18,48 +20,56 @@ namespace {
 
 constexpr int BM = 64, BN = 64, BK = 16, NT = 256;
 
-__global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
+// C[m][n] = sum_k A[m][k] (B[n][k] - boff[n]) (* S[m][n]) in T, stored as TO. The float4 load
+// path serves the FP32 form; the FP64 form loads scalars.
+template <typename T, typename TO>
+__global__ void __launch_bounds__(NT) gemm_tn_kernel(GemmArgsT<T, TO> g, int vec_ok) {
     pdl_wait();
     pdl_trigger();
-    __shared__ float As[BK][BM + 4];
-    __shared__ float Bs[BK][BN + 4];
+    __shared__ T As[BK][BM + 4];
+    __shared__ T Bs[BK][BN + 4];
     const int z = blockIdx.z;
-    const float* A = g.A + z * g.sA;
-    const float* B = g.B + z * g.sB;
-    const float* boff = g.boff ? g.boff + z * g.sBoff : nullptr;
+    const T* A = g.A + z * g.sA;
+    const T* B = g.B + z * g.sB;
+    const T* boff = g.boff ? g.boff + z * g.sBoff : nullptr;
     const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
     const int lr = tid >> 2, lk = (tid & 3) * 4;  // loader: row, k offset
-    float acc[4][4] = {};
-    float ra[4], rb[4];
+    T acc[4][4] = {};
+    T ra[4], rb[4];
 
     auto load = [&](int k0) {
         const int am = m0 + lr, bn = n0 + lr, k = k0 + lk;
-        if (vec_ok && k + 3 < g.K) {
-            if (am < g.M) {
-                const float4 v = *reinterpret_cast<const float4*>(A + am * g.lda + k);
-                ra[0] = v.x; ra[1] = v.y; ra[2] = v.z; ra[3] = v.w;
-            } else {
-                ra[0] = ra[1] = ra[2] = ra[3] = 0.f;
+        bool done = false;
+        if constexpr (sizeof(T) == 4) {
+            if (vec_ok && k + 3 < g.K) {
+                if (am < g.M) {
+                    const float4 v = *reinterpret_cast<const float4*>(A + am * g.lda + k);
+                    ra[0] = v.x; ra[1] = v.y; ra[2] = v.z; ra[3] = v.w;
+                } else {
+                    ra[0] = ra[1] = ra[2] = ra[3] = T(0);
+                }
+                if (bn < g.N) {
+                    const float4 v = *reinterpret_cast<const float4*>(B + bn * g.ldb + k);
+                    rb[0] = v.x; rb[1] = v.y; rb[2] = v.z; rb[3] = v.w;
+                } else {
+                    rb[0] = rb[1] = rb[2] = rb[3] = T(0);
+                }
+                done = true;
             }
-            if (bn < g.N) {
-                const float4 v = *reinterpret_cast<const float4*>(B + bn * g.ldb + k);
-                rb[0] = v.x; rb[1] = v.y; rb[2] = v.z; rb[3] = v.w;
-            } else {
-                rb[0] = rb[1] = rb[2] = rb[3] = 0.f;
-            }
-        } else {
+        }
+        if (!done) {
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-                ra[i] = (am < g.M && k + i < g.K) ? A[am * g.lda + k + i] : 0.f;
-                rb[i] = (bn < g.N && k + i < g.K) ? B[bn * g.ldb + k + i] : 0.f;
+                ra[i] = (am < g.M && k + i < g.K) ? A[am * g.lda + k + i] : T(0);
+                rb[i] = (bn < g.N && k + i < g.K) ? B[bn * g.ldb + k + i] : T(0);
             }
         }
         if (boff && bn < g.N) {  // DC split: B row minus its mean
-            const float o = boff[bn];
+            const T o = boff[bn];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) rb[i] = (k + i < g.K) ? rb[i] - o : 0.f;
+            for (int i = 0; i < 4; ++i) rb[i] = (k + i < g.K) ? rb[i] - o : T(0);
         }
     };
 
@@ -74,13 +84,16 @@ __global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
         if (k0 + BK < g.K) load(k0 + BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
-            const float4 a = *reinterpret_cast<const float4*>(&As[kk][ty * 4]);
-            const float4 b = *reinterpret_cast<const float4*>(&Bs[kk][tx * 4]);
-            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+            T av[4], bv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                av[i] = As[kk][ty * 4 + i];
+                bv[i] = Bs[kk][tx * 4 + i];
+            }
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
         }
         __syncthreads();
     }
@@ -88,16 +101,25 @@ __global__ void __launch_bounds__(NT) sgemm_tn_kernel(GemmArgs g, int vec_ok) {
     for (int i = 0; i < 4; ++i) {
         const int m = m0 + ty * 4 + i;
         if (m >= g.M) continue;
-        float* crow = (m < g.split) ? g.C + z * g.sC + m * g.ldc : g.C2 + z * g.sC + (m - g.split) * g.ldc;
+        TO* crow = (m < g.split) ? g.C + z * g.sC + m * g.ldc : g.C2 + z * g.sC + (m - g.split) * g.ldc;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int n = n0 + tx * 4 + j;
             if (n >= g.N) continue;
-            float v = acc[i][j];
+            T v = acc[i][j];
             if (g.S) v *= g.S[m * g.lds + n];
-            crow[n] = v;
+            crow[n] = static_cast<TO>(v);
         }
     }
+}
+
+// FP32 -> FP64 copy of the density (the FP64 form's B operand of G1).
+__global__ void widen_kernel(const float* src, double* dst, int64_t n) {
+    pdl_wait();
+    pdl_trigger();
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        dst[i] = static_cast<double>(src[i]);
 }
 
 // One warp per (row, segment): FP64 sum of `seg` contiguous floats, fixed shuffle tree.
@@ -159,7 +181,13 @@ void sgemm_tn(const GemmArgs& g, int batch, cudaStream_t s) {
                          (reinterpret_cast<uintptr_t>(g.B) % 16 == 0) && (g.sA % 4 == 0) &&
                          (g.sB % 4 == 0);
     dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), batch);
-    launch_pdl(sgemm_tn_kernel, grid, dim3(NT), 0, s, g, aligned ? 1 : 0);
+    launch_pdl(gemm_tn_kernel<float, float>, grid, dim3(NT), 0, s, g, aligned ? 1 : 0);
+}
+
+template <typename TO>
+void dgemm_tn(const GemmArgsT<double, TO>& g, int batch, cudaStream_t s) {
+    dim3 grid(ceil_div(g.N, BN), ceil_div(g.M, BM), batch);
+    launch_pdl(gemm_tn_kernel<double, TO>, grid, dim3(NT), 0, s, g, 0);
 }
 
 void row_stats(const float* a, int rows, int cols, int64_t ld, int seg, float* mean, float* sum,
@@ -179,8 +207,8 @@ void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, in
                          int batch_cap) {
     SPG_REQUIRE(nx >= 2 && ny >= 2, SPG_E_INVALID, "Poisson: grid must be at least 2x2");
     SPG_REQUIRE(sx > 0.f && sy > 0.f, SPG_E_INVALID, "Poisson: bin step must be positive");
-    SPG_REQUIRE(precision == SPG_POISSON_FP32 || precision == SPG_POISSON_BF16X3, SPG_E_INVALID,
-                "Poisson: unknown precision");
+    SPG_REQUIRE(precision == SPG_POISSON_FP32 || precision == SPG_POISSON_BF16X3 || precision == SPG_POISSON_FP64,
+                SPG_E_INVALID, "Poisson: unknown precision");
     SPG_REQUIRE(batch_cap >= 1, SPG_E_INVALID, "Poisson: batch capacity must be positive");
     if (precision == SPG_POISSON_BF16X3)
         SPG_REQUIRE(tc_supported(nx, ny), SPG_E_INVALID,
@@ -191,10 +219,12 @@ void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, in
     pl.step_y = sy;
     pl.precision = precision;
     pl.batch_cap = batch_cap;
-    pl.name = precision == SPG_POISSON_FP32 ? "cuda-sm100a-fp32" : "cuda-sm100a-bf16x3";
+    pl.name = precision == SPG_POISSON_FP32   ? "cuda-sm100a-fp32"
+              : precision == SPG_POISSON_FP64 ? "cuda-sm100a-fp64"
+                                              : "cuda-sm100a-bf16x3";
 
     const size_t X = nx, Y = ny;
-    std::vector<float> cy(Y * Y), cx(X * X), bcat(2 * Y * Y), acat(2 * X * X), sc(X * Y);
+    std::vector<double> cy(Y * Y), cx(X * X), bcat(2 * Y * Y), acat(2 * X * X), sc(X * Y);
     std::vector<double> u(X), v(Y);
     for (size_t j = 0; j < X; ++j) u[j] = M_PI * static_cast<double>(j) / (static_cast<double>(nx) * sx);
     for (size_t k = 0; k < Y; ++k) v[k] = M_PI * static_cast<double>(k) / (static_cast<double>(ny) * sy);
@@ -203,43 +233,57 @@ void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, in
             const int64_t num = static_cast<int64_t>(k) * (2 * static_cast<int64_t>(y) + 1);
             const double c = cospi_ratio(num, 2 * static_cast<int64_t>(ny));
             const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(ny));
-            cy[k * Y + y] = static_cast<float>(c);
-            bcat[y * Y + k] = static_cast<float>((k == 0 ? 1.0 : 2.0) * c);      // Ay[y][k]
-            bcat[(Y + y) * Y + k] = static_cast<float>(2.0 * v[k] * s);          // Sy[y][k]
+            cy[k * Y + y] = c;
+            bcat[y * Y + k] = (k == 0 ? 1.0 : 2.0) * c;      // Ay[y][k]
+            bcat[(Y + y) * Y + k] = 2.0 * v[k] * s;          // Sy[y][k]
         }
     for (size_t j = 0; j < X; ++j)
         for (size_t x = 0; x < X; ++x) {
             const int64_t num = static_cast<int64_t>(j) * (2 * static_cast<int64_t>(x) + 1);
             const double c = cospi_ratio(num, 2 * static_cast<int64_t>(nx));
             const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(nx));
-            cx[j * X + x] = static_cast<float>(c);
-            acat[x * X + j] = static_cast<float>((j == 0 ? 1.0 : 2.0) * c);      // Ax[x][j]
-            acat[(X + x) * X + j] = static_cast<float>(2.0 * u[j] * s);          // Sx[x][j]
+            cx[j * X + x] = c;
+            acat[x * X + j] = (j == 0 ? 1.0 : 2.0) * c;      // Ax[x][j]
+            acat[(X + x) * X + j] = 2.0 * u[j] * s;          // Sx[x][j]
         }
     const double nn = static_cast<double>(nx) * static_cast<double>(ny);
     for (size_t j = 0; j < X; ++j)
         for (size_t k = 0; k < Y; ++k) {
             const double den = u[j] * u[j] + v[k] * v[k];
-            sc[j * Y + k] = den > 0.0 ? static_cast<float>(1.0 / (nn * den)) : 0.f;
+            sc[j * Y + k] = den > 0.0 ? 1.0 / (nn * den) : 0.0;
         }
 
     size_t& b = pl.bytes;
-    pl.cy = dalloc<float>(Y * Y, b);
-    pl.cx = dalloc<float>(X * X, b);
-    pl.bcat = dalloc<float>(2 * Y * Y, b);
-    pl.acat = dalloc<float>(2 * X * X, b);
-    pl.scale = dalloc<float>(X * Y, b);
-    SPG_CUDA(cudaMemcpy(pl.cy, cy.data(), cy.size() * 4, cudaMemcpyHostToDevice));
-    SPG_CUDA(cudaMemcpy(pl.cx, cx.data(), cx.size() * 4, cudaMemcpyHostToDevice));
-    SPG_CUDA(cudaMemcpy(pl.bcat, bcat.data(), bcat.size() * 4, cudaMemcpyHostToDevice));
-    SPG_CUDA(cudaMemcpy(pl.acat, acat.data(), acat.size() * 4, cudaMemcpyHostToDevice));
-    SPG_CUDA(cudaMemcpy(pl.scale, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice));
-    {
-        const size_t B = static_cast<size_t>(batch_cap);
-        pl.dc = dalloc<float>(4 * B * std::max(X, Y), b);  // row means / sums, both splits
+    const size_t B = static_cast<size_t>(batch_cap);
+    if (precision == SPG_POISSON_FP64) {
+        auto up64 = [&](double*& dst, const std::vector<double>& h) {
+            dst = dalloc<double>(h.size(), b);
+            SPG_CUDA(cudaMemcpy(dst, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+        };
+        up64(pl.cy64, cy);
+        up64(pl.cx64, cx);
+        up64(pl.bcat64, bcat);
+        up64(pl.acat64, acat);
+        up64(pl.scale64, sc);
+        pl.rho64 = dalloc<double>(B * X * Y, b);
+        pl.t0t64 = dalloc<double>(B * X * Y, b);
+        pl.p64 = dalloc<double>(B * X * Y, b);
+        pl.t12t64 = dalloc<double>(2 * B * X * Y, b);
+        return;
     }
+    // the FP32 forms: bases rounded once to float
+    auto up32 = [&](float*& dst, const std::vector<double>& h) {
+        std::vector<float> f(h.begin(), h.end());
+        dst = dalloc<float>(f.size(), b);
+        SPG_CUDA(cudaMemcpy(dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    };
+    up32(pl.cy, cy);
+    up32(pl.cx, cx);
+    up32(pl.bcat, bcat);
+    up32(pl.acat, acat);
+    up32(pl.scale, sc);
+    pl.dc = dalloc<float>(4 * B * std::max(X, Y), b);  // row means / sums, both splits
     if (precision == SPG_POISSON_FP32) {
-        const size_t B = static_cast<size_t>(batch_cap);
         pl.t0t = dalloc<float>(B * X * Y, b);
         pl.p = dalloc<float>(B * X * Y, b);
         pl.t12t = dalloc<float>(2 * B * X * Y, b);
@@ -253,6 +297,10 @@ void poisson_plan_destroy(PoissonPlan& pl) {
     for (float* q : {pl.cy, pl.cx, pl.bcat, pl.acat, pl.scale, pl.t0t, pl.p, pl.t12t, pl.dc})
         if (q) cudaFree(q);
     pl.cy = pl.cx = pl.bcat = pl.acat = pl.scale = pl.t0t = pl.p = pl.t12t = pl.dc = nullptr;
+    for (double* q : {pl.cy64, pl.cx64, pl.bcat64, pl.acat64, pl.scale64, pl.rho64, pl.t0t64, pl.p64, pl.t12t64})
+        if (q) cudaFree(q);
+    pl.cy64 = pl.cx64 = pl.bcat64 = pl.acat64 = pl.scale64 = nullptr;
+    pl.rho64 = pl.t0t64 = pl.p64 = pl.t12t64 = nullptr;
 }
 
 void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
@@ -263,6 +311,21 @@ void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, flo
         return;
     }
     const int X = pl.nx, Y = pl.ny;
+    if (pl.precision == SPG_POISSON_FP64) {
+        // the same chain in FP64 (no DC split needed), results rounded once to float
+        const int64_t BX = static_cast<int64_t>(batch) * X, XY = static_cast<int64_t>(X) * Y;
+        launch_pdl(widen_kernel, dim3(std::min<int64_t>(ceil_div(BX * Y, 256), 4096)), dim3(256), 0, s, rho,
+                   pl.rho64, BX * Y);
+        dgemm_tn<double>({pl.cy64, pl.rho64, pl.t0t64, nullptr, nullptr, Y, static_cast<int>(BX), Y, Y, Y, Y, BX, 0,
+                          0, 0, 0}, 1, s);
+        dgemm_tn<double>({pl.cx64, pl.t0t64, pl.p64, nullptr, pl.scale64, X, Y, X, X, X, BX, Y, Y, 0, X, XY}, batch, s);
+        dgemm_tn<double>({pl.bcat64, pl.p64, pl.t12t64, nullptr, nullptr, 2 * Y, static_cast<int>(BX), Y, 2 * Y, Y, Y,
+                          BX, 0, 0, 0, 0}, 1, s);
+        dgemm_tn<float>({pl.acat64, pl.t12t64, phi, ex, nullptr, 2 * X, Y, X, X, X, BX, Y, 0, 0, X, XY}, batch, s);
+        dgemm_tn<float>({pl.acat64, pl.t12t64 + static_cast<int64_t>(Y) * BX, ey, nullptr, nullptr, X, Y, X, X, X, BX,
+                         Y, 0, 0, X, XY}, batch, s);
+        return;
+    }
     const int64_t BX = static_cast<int64_t>(batch) * X;
     const int64_t XY = static_cast<int64_t>(X) * Y;
     const int64_t MXY = std::max(X, Y) * static_cast<int64_t>(batch);

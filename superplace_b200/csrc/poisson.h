@@ -37,6 +37,10 @@ struct PoissonPlan {
     float *t0t = nullptr, *p = nullptr, *t12t = nullptr;
     float* dc = nullptr;  // DC-split row means and sums
 
+    // FP64 bases and work (the FP64 reference form)
+    double *cy64 = nullptr, *cx64 = nullptr, *bcat64 = nullptr, *acat64 = nullptr, *scale64 = nullptr;
+    double *rho64 = nullptr, *t0t64 = nullptr, *p64 = nullptr, *t12t64 = nullptr;
+
     // split-BF16 bases and work: hi and lo planes, stored [hi | lo] per matrix
     uint16_t *cy_s = nullptr, *cx_s = nullptr, *bcat_s = nullptr, *acat_s = nullptr;
     uint16_t *rho_s = nullptr, *t0t_s = nullptr, *p_s = nullptr, *t12t_s = nullptr;
@@ -62,18 +66,20 @@ void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, flo
 // mean (boff) removes that component; since sum_k cos(pi j (k+1/2)/n) = 0 for j >= 1 only
 // output row 0 (the DC row, whose basis row is all ones) changes, and it is restored
 // exactly from the row sums.
-struct GemmArgs {
-    const float* A;
-    const float* B;
-    float* C;
-    float* C2;
-    const float* S;
+template <typename T, typename TO>
+struct GemmArgsT {
+    const T* A;
+    const T* B;
+    TO* C;
+    TO* C2;
+    const T* S;
     int M, N, K, split;
     int64_t lda, ldb, ldc, lds;
     int64_t sA, sB, sC;  // per-batch strides (blockIdx.z)
-    const float* boff = nullptr;  // per-B-row offset, batch stride sBoff
+    const T* boff = nullptr;  // per-B-row offset, batch stride sBoff
     int64_t sBoff = 0;
 };
+using GemmArgs = GemmArgsT<float, float>;
 
 // Row statistics for the DC split: for each row r (of `rows`, length `cols` each, leading
 // dimension ld) and each segment of `seg` columns, mean and sum (accumulated in FP64).

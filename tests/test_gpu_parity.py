@@ -54,6 +54,22 @@ def test_poisson_fp32_parity(nx, ny, sx, sy):
             assert np.array_equal(g, h)  # bitwise repeatable
 
 
+FP64_TOL = 1e-6  # outputs are rounded once to float: ~6e-8 of max|ref|
+
+
+@pytest.mark.parametrize("nx,ny,sx,sy", [(64, 64, 2.5, 2.5), (512, 512, 20.88, 20.86), (96, 160, 3.0, 1.7)])
+def test_poisson_fp64_parity(nx, ny, sx, sy):
+    """The FP64 form (the precision study's reference) agrees with the FP64 oracle to the
+    rounding of its float outputs, on tile and non-tile grids."""
+    be = engine.PoissonBackend(nx, ny, sx, sy, abi.POISSON_FP64)
+    rng = np.random.default_rng(7 + nx * 31 + ny)
+    for rho in (rng.random((nx, ny)).astype(np.float32), gaussians(nx, ny)):
+        got = be.solve(rho)
+        want = orc.poisson_f64(rho, sx, sy)
+        for g, w in zip(got, want):
+            assert rel_err(w, g) < FP64_TOL
+
+
 def test_poisson_fp32_analytic():
     be = {}
 
