@@ -13,7 +13,7 @@ src/gp/eplace.cpp:310,515).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision bf16x3|fp32] [--workload large|small]
-       python bench.py --poisson-sweep | --precision-study   (studies: JSON lines of their own)
+       python bench.py --poisson-sweep | --precision-study | --serve   (studies: JSON lines of their own)
 The default Poisson arithmetic is split-BF16 on tcgen05 (bf16x3); fp32 is the plain FP32 form.
 Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
 """
@@ -471,6 +471,51 @@ def run_precision_study(args):
     return 0
 
 
+def run_serve(args):
+    """The serving loop on arrival traces: requests from the small generator (cells log-uniform
+    in 1k..100k, nets 1.05x cells, grid the next power of two in 64..512 at ~4 cells per bin),
+    Poisson arrivals at 10, 50 and 200 req/s, admitted against a 150 GB budget. The server
+    (`--slots` slots, split-BF16 where the grid tiles by 128) is compared with one-at-a-time
+    plain-FP32 solves on the same trace: placements/s and p50/p99 latency from arrival to the
+    converged placement. Distinct designs are generated once and reused across the trace."""
+    from superplace_b200 import engine, generator, serving
+
+    rng = np.random.default_rng(11)
+    n_distinct = args.serve_designs
+    designs = []
+    for i in range(n_distinct):
+        n = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e5)))))
+        db, grid = generator.scaled_design(5000 + i, n)
+        engine.initialize_fillers(db, 1.0, 1002)
+        designs.append((db, grid))
+    # warm the library (plans, pool, kernels) on a few requests
+    with serving.PlacementServer(slots=2) as srv:
+        for f in [srv.submit(db, g) for db, g in designs[:4]]:
+            f.result()
+    # single-solve latency of each form, alone on an idle device
+    single = {}
+    for prec in ("fp32", "auto"):
+        with serving.PlacementServer(slots=1, precision=prec) as srv:
+            lat = [srv.submit(db, g).result().latency for db, g in designs[:16]]
+        single[prec] = float(np.median(lat) * 1e3)
+    for rate in args.serve_rates:
+        n = min(512, max(16, int(rate * args.serve_seconds)))
+        arrivals = serving.poisson_arrivals(rate, n, seed=int(rate))
+        reqs = [designs[i % n_distinct] for i in range(n)]
+        with serving.PlacementServer(slots=args.slots, hbm_budget_bytes=150e9) as srv:
+            ours = serving.summarize(serving.replay(srv, reqs, arrivals))
+            ours["peak_running"] = srv.peak_running
+        with serving.PlacementServer(slots=1, precision="fp32") as srv:
+            base = serving.summarize(serving.replay(srv, reqs, arrivals))
+        print(json.dumps({"study": "serve", "rate_per_s": rate, "requests": n, "slots": args.slots,
+                          "ours": ours, "one_at_a_time_fp32": base,
+                          "throughput_ratio": ours["placements_per_s"] / base["placements_per_s"],
+                          "single_solve_ms": single,
+                          "p99_over_single_fp32": ours["p99_ms"] / single["fp32"],
+                          "designs": n_distinct, "data": "synthetic"}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -485,7 +530,15 @@ def main():
                     help="operator sweep (grids 128..2048, batch 1 and 64): JSON lines, not the bench line")
     ap.add_argument("--precision-study", action="store_true",
                     help="211k mGP with FP64 / FP32 / BF16x3 Poisson and the CPU reference: one JSON line")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving loop on Poisson arrival traces: JSON lines, not the bench line")
+    ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
+    ap.add_argument("--serve-seconds", type=float, default=8.0)
+    ap.add_argument("--serve-designs", type=int, default=48)
     args = ap.parse_args()
+    if args.serve:
+        return run_serve(args)
     if args.poisson_sweep:
         return run_poisson_sweep(args)
     if args.precision_study:

@@ -224,6 +224,12 @@ int spg_fillers_scatter(const spg_db_view* db, int32_t count, float width, float
  */
 typedef struct spg_ctx spg_ctx;
 int spg_ctx_create(const spg_db_view* db, const spg_params* params, spg_ctx** out);
+/* Replace the context's netlist and parameters with another instance (the next request of a
+ * placement server): the context keeps its streams, staging memory and device buffers where
+ * their capacity suffices, so no device memory is allocated or freed for an instance of no
+ * larger size. Equivalent to destroying and creating the context. No counterpart in the
+ * reference, which builds one EPlace per instance. */
+int spg_ctx_load(spg_ctx* ctx, const spg_db_view* db, const spg_params* params);
 int spg_ctx_destroy(spg_ctx* ctx);
 
 /* Upload new centre positions for all num_nodes + num_fillers nodes. */

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -35,10 +36,37 @@ struct Error : std::runtime_error {
     } while (0)
 
 // Count of kernels this library launched (process-wide), reported by the benchmark.
-extern int64_t g_launches;
+extern std::atomic<int64_t> g_launches;
 inline void count_launch(int n = 1) { g_launches += n; }
 
 inline int ceil_div(int64_t a, int64_t b) { return static_cast<int>((a + b - 1) / b); }
+
+// ---------------------------------------------------------------------------------------
+// Device memory. Buffers come from a library-owned stream-ordered pool per device: they are
+// allocated on the stream of the context (or Poisson plan) being set up and freed in order on
+// that same stream, so creating or destroying one context never waits for the work of
+// another (a plain cudaFree would synchronize the device). Entry points that (re)allocate
+// open an AllocScope with their stream; outside any scope the calls fall back to
+// cudaMalloc / cudaFree.
+extern thread_local cudaStream_t t_alloc_stream;
+struct AllocScope {
+    cudaStream_t prev;
+    explicit AllocScope(cudaStream_t s) : prev(t_alloc_stream) { t_alloc_stream = s; }
+    ~AllocScope() { t_alloc_stream = prev; }
+    AllocScope(const AllocScope&) = delete;
+    AllocScope& operator=(const AllocScope&) = delete;
+};
+// `bytes` of device memory, usable on every stream when this returns; *owner receives the
+// stream its free must be ordered on (nullptr: plain cudaMalloc).
+void* dev_alloc(size_t bytes, cudaStream_t* owner);
+void dev_free(void* p, cudaStream_t owner);
+// Host -> device copy queued on `s` (through the current context's pinned staging memory
+// when `s` is its stream); the source may be reused on return.
+void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// Device -> host copy, complete on return.
+void download_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// Host wait for the work queued on `s`, sleeping rather than spinning.
+cudaError_t host_wait(cudaStream_t s);
 
 // ---------------------------------------------------------------------------------------
 // Programmatic dependent launch. A kernel launched by launch_pdl may begin while the kernel

@@ -226,7 +226,8 @@ void launch_density_rest(const DevPtrs& p, cudaStream_t s) {
 }
 
 void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s) {
-    const int grid = wave_grid(reinterpret_cast<const void*>(rho_overflow_kernel), RED_THREADS, RED_CAP);
+    const int grid = work_grid(reinterpret_cast<const void*>(rho_overflow_kernel),
+                               static_cast<int64_t>(p.geom.dim) * p.geom.dim, RED_THREADS);
     launch_pdl(rho_overflow_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, write_maps, zero);
 }
 

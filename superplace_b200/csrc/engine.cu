@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -27,7 +28,7 @@
 
 namespace spg {
 
-int64_t g_launches = 0;
+std::atomic<int64_t> g_launches{0};
 
 bool pdl_enabled() {
     static const bool on = [] {
@@ -37,15 +38,92 @@ bool pdl_enabled() {
     return on;
 }
 
-int launch_priority(bool high) {
-    static int lo = 1, hi = 1;
-    if (lo > 0) {
-        int l = 0, h = 0;
-        SPG_CUDA(cudaDeviceGetStreamPriorityRange(&l, &h));
-        hi = h;
-        lo = l;
+thread_local cudaStream_t t_alloc_stream = nullptr;
+
+namespace {
+cudaMemPool_t library_pool(int dev) {
+    static std::mutex mu;
+    static std::vector<std::pair<int, cudaMemPool_t>> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto& e : pools)
+        if (e.first == dev) return e.second;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    SPG_CUDA(cudaMemPoolCreate(&pool, &props));
+    // keep freed memory in the pool for the next context instead of returning it at every sync
+    uint64_t keep = ~0ull;
+    SPG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    // Reuse memory freed on another stream only once that free has completed: never make one
+    // context's stream wait on another's (which the pool would do to hand out memory freed
+    // ahead in another stream, serializing independent placements).
+    int off = 0, on = 1;
+    SPG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseFollowEventDependencies, &off));
+    SPG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &off));
+    SPG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowOpportunistic, &on));
+    pools.emplace_back(dev, pool);
+    return pool;
+}
+}  // namespace
+
+// Waits on the host for the work queued on `s` so far, sleeping instead of spinning: a
+// thread-local event created with cudaEventBlockingSync. Many host threads (one per context
+// of a placement server) then wait without taking the CPU from threads with host work.
+cudaError_t host_wait(cudaStream_t s) {
+    struct Ev {
+        int dev = -1;
+        cudaEvent_t ev = nullptr;
+        ~Ev() {
+            if (ev) cudaEventDestroy(ev);
+        }
+    };
+    static thread_local Ev e;
+    int dev = 0;
+    cudaError_t r = cudaGetDevice(&dev);
+    if (r != cudaSuccess) return r;
+    if (!e.ev || e.dev != dev) {
+        if (e.ev) cudaEventDestroy(e.ev);
+        e.ev = nullptr;
+        r = cudaEventCreateWithFlags(&e.ev, cudaEventBlockingSync | cudaEventDisableTiming);
+        if (r != cudaSuccess) return r;
+        e.dev = dev;
     }
-    return high ? hi : lo;
+    r = cudaEventRecord(e.ev, s);
+    return r == cudaSuccess ? cudaEventSynchronize(e.ev) : r;
+}
+
+void* dev_alloc(size_t bytes, cudaStream_t* owner) {
+    void* p = nullptr;
+    const cudaStream_t s = t_alloc_stream;
+    *owner = s;
+    if (!s) {
+        SPG_CUDA(cudaMalloc(&p, bytes));
+        return p;
+    }
+    int dev = 0;
+    SPG_CUDA(cudaGetDevice(&dev));
+    SPG_CUDA(cudaMallocFromPoolAsync(&p, bytes, library_pool(dev), s));
+    // complete before return: callers copy into it from the host or use it on other streams
+    SPG_CUDA(host_wait(s));
+    return p;
+}
+
+void dev_free(void* p, cudaStream_t owner) {
+    if (!p) return;
+    if (owner) cudaFreeAsync(p, owner);
+    else cudaFree(p);
+}
+
+int launch_priority(bool high) {
+    static const std::pair<int, int> range = [] {
+        int l = 0, h = 0;
+        if (cudaDeviceGetStreamPriorityRange(&l, &h) != cudaSuccess) l = h = 0;
+        return std::make_pair(l, h);
+    }();
+    return high ? range.second : range.first;
 }
 
 int wave_grid(const void* kernel, int threads, int cap) {
@@ -97,31 +175,102 @@ thread_local std::string g_last_error;
 constexpr int kMaxBinDim = 1024;      // bin_grid.cpp:18
 constexpr float kBoundaryEps = 1e-3f;  // eplace.cpp:38
 
+}  // namespace
+
+// Pinned staging memory for the host <-> device copies of one context: a copy from pageable
+// memory is staged by the driver through a shared buffer (serialized across threads and
+// synchronous), one from pinned memory is a plain DMA on the context's stream. Regions are
+// handed out in order and recycled after the stream has been synchronized.
+struct Staging {
+    char* buf = nullptr;
+    size_t cap = 0, used = 0;
+    cudaStream_t s = nullptr;
+    Staging() = default;
+    Staging(const Staging&) = delete;
+    Staging& operator=(const Staging&) = delete;
+    ~Staging() {
+        if (buf) cudaFreeHost(buf);
+    }
+    void* reserve(size_t bytes) {
+        const size_t need = (bytes + 255) & ~static_cast<size_t>(255);
+        if (used + need > cap) {
+            SPG_CUDA(host_wait(s));  // every earlier region has been consumed
+            used = 0;
+            if (need > cap) {
+                if (buf) cudaFreeHost(buf);
+                buf = nullptr;
+                cap = 0;
+                const size_t grown = std::max(need, static_cast<size_t>(8) << 20);
+                SPG_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&buf), grown, cudaHostAllocDefault));
+                cap = grown;
+            }
+        }
+        void* d = buf + used;
+        used += need;
+        return d;
+    }
+};
+// The staging memory of the context the calling thread is working on (see CtxScope).
+thread_local Staging* t_staging = nullptr;
+
+void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (!bytes) return;
+    if (t_staging && t_staging->s == s) {
+        void* d = t_staging->reserve(bytes);
+        std::memcpy(d, src, bytes);
+        src = d;
+    }
+    SPG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+}
+
+// Device -> host copy, complete on return.
+void download_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (!bytes) return;
+    if (t_staging && t_staging->s == s) {
+        void* d = t_staging->reserve(bytes);
+        SPG_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToHost, s));
+        SPG_CUDA(host_wait(s));
+        std::memcpy(dst, d, bytes);
+        return;
+    }
+    SPG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(host_wait(s));
+}
+
+namespace {
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
-    size_t n = 0;
+    size_t n = 0, cap = 0;
+    cudaStream_t owner = nullptr;  // the stream its free is ordered on
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { reset(); }
     void reset() {
-        if (p) cudaFree(p);
+        dev_free(p, owner);
         p = nullptr;
-        n = 0;
+        n = cap = 0;
     }
-    // (Re)allocate for `count` elements; an existing buffer of the same size is kept, so
-    // repeated stage runs reuse their device memory and keep their addresses.
+    // Size the buffer for `count` elements. An allocation with enough capacity is kept, so
+    // repeated stage runs, and a context reloaded with another netlist of no larger size,
+    // reuse their device memory and keep their addresses; a larger size grows it by half.
     void alloc(size_t count) {
         if (count == 0) count = 1;
-        if (p && n == count) return;
+        if (p && count <= cap) {
+            n = count;
+            return;
+        }
+        const size_t grown = p ? std::max(count, cap + cap / 2) : count;
         reset();
-        SPG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        p = static_cast<T*>(dev_alloc(grown * sizeof(T), &owner));
         n = count;
+        cap = grown;
     }
     void upload(const T* h, size_t count, cudaStream_t s) {
         alloc(count);
-        if (count) SPG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+        upload_bytes(p, h, count * sizeof(T), s);
     }
     void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
     void zero(cudaStream_t s) { SPG_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s)); }
@@ -142,9 +291,19 @@ float overlap_area(float alx, float aly, float ahx, float ahy, float blx, float 
 // ---------------------------------------------------------------------------------------
 struct LoopGraph;
 
-struct Context {
+// The context's streams live in a base class: the members' device buffers are freed (in
+// order on `stream`) before the streams are destroyed.
+struct ContextStreams {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // WA pass 1 overlaps the density -> Poisson chain
+    ~ContextStreams() {
+        if (stream) host_wait(stream);
+        if (side) cudaStreamDestroy(side);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+struct Context : ContextStreams {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     spg_params prm{};
     // host copy of the db (flags and sizes change with mLG; positions live on the device)
@@ -168,7 +327,8 @@ struct Context {
     double movable_area_scaled = 0.0;
     DevBuf<unsigned long long> node_fix, filler_fix;
     DevBuf<float> terminal, base, rho, phi, ex, ey, node_map, filler_map;
-    std::unique_ptr<PoissonPlan> plan;
+    std::unique_ptr<PoissonPlan> plan;                      // the current grid's Poisson plan
+    std::vector<std::unique_ptr<PoissonPlan>> spare_plans;  // other grid sizes seen (reused)
     DevBuf<int> dens_small, dens_large;
     int n_dens_small = 0, n_dens_large = 0;
     std::vector<int> dens_small_h, dens_large_h;  // host copies, for the per-stage rest lists
@@ -181,6 +341,7 @@ struct Context {
     DevBuf<int4> opt_meta;
     std::vector<float> hw_h, hh_h, wgt_h;  // per-node footprint data of the current grid
     std::vector<int> slot_start_h;         // node-order pin slots (see DevPtrs::slot_start)
+    std::vector<uint8_t> kind_h;           // host copy of the per-node kernel classes
     DevBuf<float> opt_lo, opt_hi, force, pool;
     DevBuf<double> opt_area;
     int n_opt_small = 0, n_opt_large = 0;
@@ -191,21 +352,24 @@ struct Context {
     DevBuf<double> scratch_d;
     int metrics_rows = 0;
     DevState* hst = nullptr;  // pinned host mirror
+    Staging staging;          // pinned staging of this context's host <-> device copies
     float step_x_gamma = 1.f;
     // the iteration loop as a conditional CUDA graph (engine.cu: build_loop_graph); the
     // host-driven loop runs instead where the driver refuses conditional nodes
     bool use_graph = true;
     bool last_run_graph = false;
+    double last_graph_build_ms = 0.0;
     std::shared_ptr<LoopGraph> loop_graph;
 
     ~Context() {
+        if (side) host_wait(side);
+        if (stream) host_wait(stream);
         loop_graph.reset();
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
-        if (side) cudaStreamDestroy(side);
         if (plan) poisson_plan_destroy(*plan);
+        for (auto& q : spare_plans) poisson_plan_destroy(*q);
         if (hst) cudaFreeHost(hst);
-        if (stream) cudaStreamDestroy(stream);
     }
 
     DevPtrs ptrs() const {
@@ -295,8 +459,32 @@ namespace {
 
 // BinGrid::initialize (src/gp/bin_grid.cpp:64-189) for the current flags, plus the
 // per-node footprint data the density kernels read and the fixed-point scale.
+// SPG_HOST_TIMING=1: stage_run (and grid_init) print the host time of their phases to stderr.
+struct HostTimer {
+    bool on;
+    std::chrono::steady_clock::time_point t0;
+    std::string line;
+    const char* tag;
+    explicit HostTimer(const char* t = "") : tag(t) {
+        const char* e = std::getenv("SPG_HOST_TIMING");
+        on = e && e[0] == '1';
+        t0 = std::chrono::steady_clock::now();
+    }
+    void mark(const char* name) {
+        if (!on) return;
+        const auto t = std::chrono::steady_clock::now();
+        line += std::string(" ") + name + "=" +
+                std::to_string(std::chrono::duration<double, std::milli>(t - t0).count()).substr(0, 6);
+        t0 = t;
+    }
+    ~HostTimer() {
+        if (on) std::fprintf(stderr, "[spg host ms%s]%s\n", tag, line.c_str());
+    }
+};
+
 void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& hx_pos,
                const std::vector<float>& hy_pos) {
+    HostTimer ht(" grid");
     double cell_area = 0.0, macro_area = 0.0;
     for (int i = 0; i < c.num_movable; ++i) {
         if (c.fixed(i) || c.ni(i)) continue;
@@ -380,6 +568,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         }
     }
 
+    ht.mark("statics");
     // footprint data: half extents after local smoothing, charge weight, kernel class
     std::vector<float> hw(c.total), hh(c.total), wgt(c.total);
     std::vector<uint8_t> kind(c.total, 0);
@@ -421,6 +610,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     g.scale = std::ldexp(1.0, s);
     g.inv_scale = std::ldexp(1.0, -s);
 
+    ht.mark("footprints");
     cudaStream_t st = c.stream;
     c.terminal.upload(term, st);
     c.base.upload(base, st);
@@ -431,6 +621,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     c.hh_h = hh;
     c.wgt_h = wgt;
     c.kind.upload(kind, st);
+    c.kind_h = kind;
     c.dens_small.upload(dsmall, st);
     c.dens_large.upload(dlarge, st);
     c.n_dens_small = static_cast<int>(dsmall.size());
@@ -445,15 +636,35 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         b->alloc(n);
         b->zero(st);
     }
-    if (!c.plan || c.plan->nx != dim || c.plan->step_x != g.step_x || c.plan->step_y != g.step_y ||
-        c.plan->precision != c.prm.poisson_precision) {
-        if (c.plan) poisson_plan_destroy(*c.plan);
-        c.plan = std::make_unique<PoissonPlan>();
-        poisson_plan_create(*c.plan, dim, dim, g.step_x, g.step_y, c.prm.poisson_precision, 1);
+    ht.mark("uploads");
+    // a plan per grid size and precision is kept; new bin steps only rewrite its tables
+    auto fits = [&](const std::unique_ptr<PoissonPlan>& q) {
+        return q && q->nx == dim && q->ny == dim && q->precision == c.prm.poisson_precision;
+    };
+    if (!fits(c.plan)) {
+        auto it = std::find_if(c.spare_plans.begin(), c.spare_plans.end(), fits);
+        std::unique_ptr<PoissonPlan> next;
+        if (it != c.spare_plans.end()) {
+            next = std::move(*it);
+            c.spare_plans.erase(it);
+        } else {
+            next = std::make_unique<PoissonPlan>();
+            poisson_plan_create(*next, dim, dim, g.step_x, g.step_y, c.prm.poisson_precision, 1);
+        }
+        if (c.plan) c.spare_plans.push_back(std::move(c.plan));
+        c.plan = std::move(next);
+        constexpr size_t kSparePlans = 4;
+        while (c.spare_plans.size() > kSparePlans) {
+            poisson_plan_destroy(*c.spare_plans.front());
+            c.spare_plans.erase(c.spare_plans.begin());
+        }
     }
+    poisson_plan_set_steps(*c.plan, g.step_x, g.step_y);
+    ht.mark("plan");
     c.partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_CAP);
     c.partials.zero(st);
-    SPG_CUDA(cudaStreamSynchronize(st));
+    SPG_CUDA(host_wait(st));
+    ht.mark("wait");
     c.grid_ready = true;
 }
 
@@ -477,9 +688,7 @@ void stage_setup(Context& c, int stage) {
     std::vector<double> area(n);
     std::vector<float4> geom(n);
     std::vector<int4> meta(n);
-    std::vector<uint8_t> kind(c.total);
-    SPG_CUDA(cudaMemcpyAsync(kind.data(), c.kind.p, c.total, cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    const std::vector<uint8_t>& kind = c.kind_h;
     for (int k = 0; k < n; ++k) {
         const int i = opt[k];
         const float hw = 0.5f * c.w[i], hh = 0.5f * c.h[i];
@@ -571,7 +780,7 @@ void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int cou
 
 void read_state(Context& c) {
     SPG_CUDA(cudaMemcpyAsync(c.hst, c.st.p, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(host_wait(c.stream));
     if (c.hst->error) {
         const int e = c.hst->error;
         throw Error(e, e == SPG_E_NON_FINITE ? "GP/evaluate: non-finite coordinate, gradient or metric"
@@ -663,7 +872,7 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
     SPG_CHECK_LAUNCH();
     double out[2];
     SPG_CUDA(cudaMemcpyAsync(out, c.scratch_d.p, sizeof(out), cudaMemcpyDeviceToHost, s));
-    SPG_CUDA(cudaStreamSynchronize(s));
+    SPG_CUDA(host_wait(s));
     *overflow = static_cast<float>(out[0]);
     *hpwl = out[1];
 }
@@ -692,6 +901,23 @@ void host_loop(Context& c, const DevPtrs& p, int max_iter) {
 }
 
 }  // namespace
+
+// Binds the calling thread's device allocations and host copies to one context: buffers come
+// from the pool on its stream and copies go through its pinned staging memory. The
+// context's earlier work is waited for first, so the staging memory can be reused.
+struct CtxScope {
+    AllocScope alloc;
+    Staging* prev;
+    explicit CtxScope(Context& c) : alloc(c.stream), prev(t_staging) {
+        SPG_CUDA(host_wait(c.stream));
+        c.staging.s = c.stream;
+        c.staging.used = 0;
+        t_staging = &c.staging;
+    }
+    ~CtxScope() { t_staging = prev; }
+    CtxScope(const CtxScope&) = delete;
+    CtxScope& operator=(const CtxScope&) = delete;
+};
 
 struct LoopGraph {
     cudaGraph_t graph = nullptr;
@@ -735,9 +961,31 @@ void graph_stats(const char* name, cudaGraph_t g) {
     std::fprintf(stderr, "[spg graph] %s: %zu nodes, %zu edges, %d programmatic\n", name, nodes, edges, prog);
 }
 
+void graph_note(const char* what) {
+    static const bool on = [] {
+        const char* e = std::getenv("SPG_GRAPH_STATS");
+        return e && e[0] == '1';
+    }();
+    if (on) std::fprintf(stderr, "[spg graph] %s\n", what);
+}
+
 bool build_loop_graph(Context& c, const DevPtrs& p) {
     LoopGraph& lg = *c.loop_graph;
-    lg.reset();
+    // an executable graph of an earlier netlist is updated in place when the new capture
+    // allows it (same topology, new kernel arguments), which costs far less than a new
+    // instantiation; otherwise it is replaced
+    cudaGraphExec_t old_exec = lg.exec;
+    cudaGraph_t old_graph = lg.graph;
+    lg.exec = nullptr;
+    lg.graph = nullptr;
+    struct DropOld {
+        cudaGraphExec_t& e;
+        cudaGraph_t& g;
+        ~DropOld() {
+            if (e) cudaGraphExecDestroy(e);
+            if (g) cudaGraphDestroy(g);
+        }
+    } drop_old{old_exec, old_graph};
     cudaStream_t s = c.stream;
     const int64_t launches0 = g_launches;
     auto ok = [](cudaError_t e) { return e == cudaSuccess; };
@@ -773,7 +1021,17 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
         return false;
     }
     graph_stats("loop body", body);
-    if (!ok(cudaGraphInstantiate(&lg.exec, g, 0))) {
+    if (old_exec) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(old_exec, g, &info) == cudaSuccess) {
+            lg.exec = old_exec;
+            old_exec = nullptr;
+        } else {
+            cudaGetLastError();
+        }
+        graph_note(lg.exec ? "loop graph updated in place" : "loop graph re-instantiated");
+    }
+    if (!lg.exec && !ok(cudaGraphInstantiate(&lg.exec, g, 0))) {
         cudaGetLastError();
         return false;
     }
@@ -786,7 +1044,10 @@ bool graph_loop(Context& c, const DevPtrs& p) {
     if (!c.loop_graph) c.loop_graph = std::make_shared<LoopGraph>();
     LoopGraph& lg = *c.loop_graph;
     const bool same = lg.exec && lg.plan == c.plan.get() && std::memcmp(&lg.sig, &p, sizeof(DevPtrs)) == 0;
-    if (!same && !build_loop_graph(c, p)) {
+    const auto tb = std::chrono::steady_clock::now();
+    const bool built = !same && build_loop_graph(c, p);
+    if (!same) c.last_graph_build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+    if (!same && !built) {
         lg.reset();
         c.use_graph = false;  // this device/driver refused the conditional graph: host loop
         return false;
@@ -801,25 +1062,27 @@ bool graph_loop(Context& c, const DevPtrs& p) {
 // EPlace::run (eplace.cpp:223-526) for one stage, device-resident.
 void stage_run(Context& c, int stage, spg_result* res) {
     SPG_REQUIRE(stage >= SPG_STAGE_MGP && stage <= SPG_STAGE_CGP, SPG_E_INVALID, "unknown stage");
+    HostTimer ht;
     std::memset(res, 0, sizeof(*res));
     res->rollback_iter = -1;
     cudaStream_t s = c.stream;
     // constructing EPlace rebuilds the grid with the current flags (gp_stage.cpp:175-177)
     {
         std::vector<float> hx(c.total), hy(c.total);
-        SPG_CUDA(cudaMemcpyAsync(hx.data(), c.x.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, s));
-        SPG_CUDA(cudaMemcpyAsync(hy.data(), c.y.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, s));
-        SPG_CUDA(cudaStreamSynchronize(s));
+        download_bytes(hx.data(), c.x.p, c.total * sizeof(float), s);
+        download_bytes(hy.data(), c.y.p, c.total * sizeof(float), s);
         grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, hx, hy);
     }
+    ht.mark("grid_init");
     stage_setup(c, stage);
+    ht.mark("stage_setup");
     if (c.n_opt == 0) return;  // "no nodes to optimise" (eplace.cpp:232-236)
     const bool filler_only = stage == SPG_STAGE_FILLER_ONLY;
     const float target_tau = stage == SPG_STAGE_CGP ? c.prm.cgp_target_overflow : c.prm.target_overflow;
     const int max_iter = filler_only ? c.prm.filler_only_iters : c.prm.gp_max_iter;
     DevPtrs p = c.ptrs();
     init_state_kernel<<<1, 1, 0, s>>>(p, stage, max_iter, target_tau);
-    gather_pos_kernel<<<wave_grid(reinterpret_cast<const void*>(gather_pos_kernel), RED_THREADS, RED_CAP),
+    gather_pos_kernel<<<work_grid(reinterpret_cast<const void*>(gather_pos_kernel), p.n_opt, RED_THREADS),
                         RED_THREADS, 0, s>>>(p);
     count_launch(2);
     SPG_CHECK_LAUNCH();
@@ -836,6 +1099,7 @@ void stage_run(Context& c, int stage, spg_result* res) {
     res->initial_lambda = c.hst->lambda;
     set_hpwl_ref_kernel<<<1, 1, 0, s>>>(p, ref);
     count_launch();
+    ht.mark("lambda_probe");
 
     if (!filler_only && c.hst->tau < target_tau) {
         // already converged: take no step (eplace.cpp:278-296)
@@ -862,16 +1126,21 @@ void stage_run(Context& c, int stage, spg_result* res) {
 
     // first evaluation of iteration 0, its norms, and the redo test (a no-op at iteration 0)
     evaluate(c, p, R_U, R_G, 1, true);
+    ht.mark("init_enqueue");
     c.last_run_graph = false;
+    c.last_graph_build_ms = 0.0;
     if (max_iter > 0) {
         c.last_run_graph = c.use_graph && graph_loop(c, p);
         if (!c.last_run_graph) host_loop(c, p, max_iter);
     }
+    ht.mark("loop");
+    if (ht.on) ht.line += " (graph_build=" + std::to_string(c.last_graph_build_ms).substr(0, 6) + ")";
     SPG_CUDA(cudaEventRecord(e1, s));
     launch_deliver(p, s);
     final_metrics(c, p, &res->overflow, &res->hpwl);
     launch_check_geometry(p, c.core_lx, c.core_ly, c.core_hx, c.core_hy, c.dw.p, c.dh.p, s);
     read_state(c);
+    ht.mark("final");
     float ms = 0.f;
     SPG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     cudaEventDestroy(e0);
@@ -919,6 +1188,13 @@ struct PoissonHandle {
     PoissonPlan plan;
     DevBuf<float> io;
     cudaStream_t stream = nullptr;
+    ~PoissonHandle() {
+        // the buffers' frees are ordered on `stream`, so it goes last
+        if (stream) host_wait(stream);
+        poisson_plan_destroy(plan);
+        io.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
 };
 
 }  // namespace spg
@@ -932,6 +1208,132 @@ struct spg_ctx {
 struct spg_poisson {
     spg::PoissonHandle h;
 };
+
+namespace spg {
+
+// Uploads a netlist into the context, replacing any earlier one (spg_ctx_create and
+// spg_ctx_load): host copies, device arrays, the degree-ordered net classes of the WA kernel
+// and the node-order pin slots. Device buffers with enough capacity are reused. The grid
+// and the stage state are rebuilt by the next stage run.
+void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
+    SPG_REQUIRE(v->num_movable >= 0 && v->num_nodes >= v->num_movable && v->num_fillers >= 0 &&
+                    v->num_pins >= 0 && v->num_nets >= 0,
+                SPG_E_INVALID, "inconsistent db counts");
+    c.prm = *prm;
+    c.grid_ready = false;
+    c.metrics_rows = 0;
+    c.num_movable = v->num_movable;
+    c.num_nodes = v->num_nodes;
+    c.num_fillers = v->num_fillers;
+    c.total = v->num_nodes + v->num_fillers;
+    c.num_pins = v->num_pins;
+    c.num_nets = v->num_nets;
+    const size_t T = static_cast<size_t>(c.total);
+    c.w.assign(v->node_w, v->node_w + T);
+    c.h.assign(v->node_h, v->node_h + T);
+    c.flags.assign(v->node_flags, v->node_flags + T);
+    c.node_start.assign(v->node2pin_start, v->node2pin_start + T + 1);
+    c.row_ly.assign(v->row_ly, v->row_ly + v->num_rows);
+    c.row_hgt.assign(v->row_height, v->row_height + v->num_rows);
+    c.row_lx.assign(v->row_lx, v->row_lx + v->num_rows);
+    c.row_step.assign(v->row_step, v->row_step + v->num_rows);
+    c.row_sites.assign(v->row_num_sites, v->row_num_sites + v->num_rows);
+    c.core_lx = v->core_lx;
+    c.core_ly = v->core_ly;
+    c.core_hx = v->core_hx;
+    c.core_hy = v->core_hy;
+    for (int p = 0; p < c.num_pins; ++p)
+        SPG_REQUIRE(v->pin2node[p] >= 0 && v->pin2node[p] < c.total, SPG_E_INVALID, "pin2node out of range");
+    for (int k = 0; k < c.num_nets; ++k)
+        SPG_REQUIRE(v->net2pin_start[k] <= v->net2pin_start[k + 1], SPG_E_INVALID, "net CSR not monotone");
+    for (size_t i = 0; i < T; ++i)
+        SPG_REQUIRE(c.node_start[i] <= c.node_start[i + 1], SPG_E_INVALID, "node CSR not monotone");
+    SPG_REQUIRE(v->net2pin_start[0] == 0 && c.node_start[0] == 0 &&
+                    v->net2pin_start[c.num_nets] == c.num_pins && c.node_start[T] == c.num_pins,
+                SPG_E_INVALID, "CSR sizes disagree with num_pins");
+    for (int p = 0; p < c.num_pins; ++p) {
+        SPG_REQUIRE(v->flat_net2pin[p] >= 0 && v->flat_net2pin[p] < c.num_pins, SPG_E_INVALID,
+                    "flat_net2pin out of range");
+        SPG_REQUIRE(v->flat_node2pin[p] >= 0 && v->flat_node2pin[p] < c.num_pins, SPG_E_INVALID,
+                    "flat_node2pin out of range");
+        SPG_REQUIRE(v->pin2net[p] < c.num_nets, SPG_E_INVALID, "pin2net out of range");
+    }
+    cudaStream_t s = c.stream;
+    c.x.upload(v->node_x, T, s);
+    c.y.upload(v->node_y, T, s);
+    c.dw.upload(v->node_w, T, s);
+    c.dh.upload(v->node_h, T, s);
+    c.pox.upload(v->pin_offset_x, c.num_pins, s);
+    c.poy.upload(v->pin_offset_y, c.num_pins, s);
+    c.pin2node.upload(v->pin2node, c.num_pins, s);
+    c.pin2net.upload(v->pin2net, c.num_pins, s);
+    c.net_start.upload(v->net2pin_start, c.num_nets + 1, s);
+    c.net_pins.upload(v->flat_net2pin, c.num_pins, s);
+    c.node_start_d.upload(v->node2pin_start, T + 1, s);
+    c.node_pins.upload(v->flat_node2pin, c.num_pins, s);
+    // nets in ascending degree (stable), cut into degree classes: a net of degree d is
+    // owned by a lane group of the next power of two >= d (2..32 lanes), nets above 32
+    // pins by a whole warp that loops over its pins (wirelength.cu)
+    std::vector<int> order(c.num_nets);
+    std::iota(order.begin(), order.end(), 0);
+    auto deg = [&](int k) { return v->net2pin_start[k + 1] - v->net2pin_start[k]; };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return deg(a) < deg(b); });
+    c.net_order.upload(order, s);
+    {
+        WaClasses& wc = c.wa_classes;
+        wc = WaClasses{};
+        const int limits[6] = {2, 4, 8, 16, 32, 1 << 30};
+        const int groups[6] = {2, 4, 8, 16, 32, 0};
+        int t = 0, warps = 0;
+        for (int cl = 0; cl < 6; ++cl) {
+            const int begin = t;
+            while (t < c.num_nets && deg(order[t]) <= limits[cl]) ++t;
+            if (t == begin) continue;
+            const int i = wc.n++;
+            wc.group[i] = groups[cl];
+            wc.net_begin[i] = begin;
+            wc.net_end[i] = t;
+            wc.warp_begin[i] = warps;
+            warps += groups[cl] ? ceil_div(t - begin, 32 / groups[cl]) : (t - begin);
+        }
+        wc.warp_begin[wc.n] = warps;
+    }
+    // node-order slots of the pins that belong to a net; the last slot is never read
+    {
+        for (int k = 0; k < c.num_nets; ++k)
+            for (int q = v->net2pin_start[k]; q < v->net2pin_start[k + 1]; ++q)
+                SPG_REQUIRE(v->pin2net[v->flat_net2pin[q]] == k, SPG_E_INVALID,
+                            "pin2net disagrees with the net CSR");
+        std::vector<int> slot_of_pin(c.num_pins, -1), slot_start(T + 1);
+        int slots = 0;
+        for (size_t i = 0; i < T; ++i) {
+            slot_start[i] = slots;
+            for (int t = c.node_start[i]; t < c.node_start[i + 1]; ++t) {
+                const int pin = v->flat_node2pin[t];
+                if (v->pin2net[pin] >= 0) slot_of_pin[pin] = slots++;
+            }
+        }
+        slot_start[T] = slots;
+        std::vector<int> net_slot(c.num_pins);
+        for (int q = 0; q < c.num_pins; ++q) {
+            const int sl = slot_of_pin[v->flat_net2pin[q]];
+            net_slot[q] = sl >= 0 ? sl : slots;
+        }
+        c.slot_start.upload(slot_start, s);
+        c.slot_start_h = slot_start;
+        c.net_slot.upload(net_slot, s);
+        c.num_slots = slots;
+    }
+    c.gpx.alloc(c.num_slots + 1);
+    c.gpy.alloc(c.num_slots + 1);
+    c.gpx.zero(s);
+    c.gpy.zero(s);
+    c.st.alloc(1);
+    if (!c.hst) SPG_CUDA(cudaMallocHost(&c.hst, sizeof(DevState)));
+    c.scratch_d.alloc(16);
+}
+
+}  // namespace spg
 
 #define API_TRY try {
 #define API_CATCH \
@@ -980,9 +1382,10 @@ int spg_poisson_create_batched(int nx, int ny, float sx, float sy, int precision
     *out = nullptr;
     if (!spg::device_ok()) throw Error(SPG_E_NO_DEVICE, "no usable sm_100 device");
     auto h = std::make_unique<spg_poisson>();
+    SPG_CUDA(cudaStreamCreateWithFlags(&h->h.stream, cudaStreamNonBlocking));
+    spg::AllocScope alloc_scope(h->h.stream);
     spg::poisson_plan_create(h->h.plan, nx, ny, sx, sy, precision, batch_cap);
     h->h.io.alloc(4 * static_cast<size_t>(nx) * ny);
-    SPG_CUDA(cudaStreamCreateWithFlags(&h->h.stream, cudaStreamNonBlocking));
     *out = h.release();
     return SPG_OK;
     API_CATCH
@@ -1003,7 +1406,7 @@ int spg_poisson_solve(spg_poisson* h, const float* rho, float* phi, float* fx, f
     SPG_CUDA(cudaMemcpyAsync(phi, d + n, n * 4, cudaMemcpyDeviceToHost, s));
     SPG_CUDA(cudaMemcpyAsync(fx, d + 2 * n, n * 4, cudaMemcpyDeviceToHost, s));
     SPG_CUDA(cudaMemcpyAsync(fy, d + 3 * n, n * 4, cudaMemcpyDeviceToHost, s));
-    SPG_CUDA(cudaStreamSynchronize(s));
+    SPG_CUDA(spg::host_wait(s));
     return SPG_OK;
     API_CATCH
 }
@@ -1025,9 +1428,6 @@ int spg_poisson_solve_device(spg_poisson* h, const float* rho, float* phi, float
 const char* spg_poisson_name(const spg_poisson* h) { return h ? h->h.plan.name.c_str() : "none"; }
 
 int spg_poisson_destroy(spg_poisson* h) {
-    if (!h) return SPG_OK;
-    spg::poisson_plan_destroy(h->h.plan);
-    if (h->h.stream) cudaStreamDestroy(h->h.stream);
     delete h;
     return SPG_OK;
 }
@@ -1122,12 +1522,8 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     SPG_REQUIRE(v && prm && out, SPG_E_INVALID, "null argument");
     *out = nullptr;
     if (!spg::device_ok()) throw Error(SPG_E_NO_DEVICE, "no usable sm_100 device");
-    SPG_REQUIRE(v->num_movable >= 0 && v->num_nodes >= v->num_movable && v->num_fillers >= 0 &&
-                    v->num_pins >= 0 && v->num_nets >= 0,
-                SPG_E_INVALID, "inconsistent db counts");
     auto h = std::make_unique<spg_ctx>();
     Context& c = h->c;
-    c.prm = *prm;
     // SPG_HOST_LOOP=1 selects the host-driven iteration loop (one state read per iteration)
     // instead of the conditional CUDA graph; both run the same kernels in the same order.
     c.use_graph = std::getenv("SPG_HOST_LOOP") == nullptr;
@@ -1140,117 +1536,22 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     SPG_CUDA(cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, prio_low));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
-    c.num_movable = v->num_movable;
-    c.num_nodes = v->num_nodes;
-    c.num_fillers = v->num_fillers;
-    c.total = v->num_nodes + v->num_fillers;
-    c.num_pins = v->num_pins;
-    c.num_nets = v->num_nets;
-    const size_t T = static_cast<size_t>(c.total);
-    c.w.assign(v->node_w, v->node_w + T);
-    c.h.assign(v->node_h, v->node_h + T);
-    c.flags.assign(v->node_flags, v->node_flags + T);
-    c.node_start.assign(v->node2pin_start, v->node2pin_start + T + 1);
-    c.row_ly.assign(v->row_ly, v->row_ly + v->num_rows);
-    c.row_hgt.assign(v->row_height, v->row_height + v->num_rows);
-    c.row_lx.assign(v->row_lx, v->row_lx + v->num_rows);
-    c.row_step.assign(v->row_step, v->row_step + v->num_rows);
-    c.row_sites.assign(v->row_num_sites, v->row_num_sites + v->num_rows);
-    c.core_lx = v->core_lx;
-    c.core_ly = v->core_ly;
-    c.core_hx = v->core_hx;
-    c.core_hy = v->core_hy;
-    for (int p = 0; p < c.num_pins; ++p)
-        SPG_REQUIRE(v->pin2node[p] >= 0 && v->pin2node[p] < c.total, SPG_E_INVALID, "pin2node out of range");
-    for (int k = 0; k < c.num_nets; ++k)
-        SPG_REQUIRE(v->net2pin_start[k] <= v->net2pin_start[k + 1], SPG_E_INVALID, "net CSR not monotone");
-    for (size_t i = 0; i < T; ++i)
-        SPG_REQUIRE(c.node_start[i] <= c.node_start[i + 1], SPG_E_INVALID, "node CSR not monotone");
-    SPG_REQUIRE(v->net2pin_start[0] == 0 && c.node_start[0] == 0 &&
-                    v->net2pin_start[c.num_nets] == c.num_pins && c.node_start[T] == c.num_pins,
-                SPG_E_INVALID, "CSR sizes disagree with num_pins");
-    for (int p = 0; p < c.num_pins; ++p) {
-        SPG_REQUIRE(v->flat_net2pin[p] >= 0 && v->flat_net2pin[p] < c.num_pins, SPG_E_INVALID,
-                    "flat_net2pin out of range");
-        SPG_REQUIRE(v->flat_node2pin[p] >= 0 && v->flat_node2pin[p] < c.num_pins, SPG_E_INVALID,
-                    "flat_node2pin out of range");
-        SPG_REQUIRE(v->pin2net[p] < c.num_nets, SPG_E_INVALID, "pin2net out of range");
-    }
-    cudaStream_t s = c.stream;
-    c.x.upload(v->node_x, T, s);
-    c.y.upload(v->node_y, T, s);
-    c.dw.upload(v->node_w, T, s);
-    c.dh.upload(v->node_h, T, s);
-    c.pox.upload(v->pin_offset_x, c.num_pins, s);
-    c.poy.upload(v->pin_offset_y, c.num_pins, s);
-    c.pin2node.upload(v->pin2node, c.num_pins, s);
-    c.pin2net.upload(v->pin2net, c.num_pins, s);
-    c.net_start.upload(v->net2pin_start, c.num_nets + 1, s);
-    c.net_pins.upload(v->flat_net2pin, c.num_pins, s);
-    c.node_start_d.upload(v->node2pin_start, T + 1, s);
-    c.node_pins.upload(v->flat_node2pin, c.num_pins, s);
-    // nets in ascending degree (stable), cut into degree classes: a net of degree d is
-    // owned by a lane group of the next power of two >= d (2..32 lanes), nets above 32
-    // pins by a whole warp that loops over its pins (wirelength.cu)
-    std::vector<int> order(c.num_nets);
-    std::iota(order.begin(), order.end(), 0);
-    auto deg = [&](int k) { return v->net2pin_start[k + 1] - v->net2pin_start[k]; };
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return deg(a) < deg(b); });
-    c.net_order.upload(order, s);
-    {
-        spg::WaClasses& wc = c.wa_classes;
-        wc = spg::WaClasses{};
-        const int limits[6] = {2, 4, 8, 16, 32, 1 << 30};
-        const int groups[6] = {2, 4, 8, 16, 32, 0};
-        int t = 0, warps = 0;
-        for (int cl = 0; cl < 6; ++cl) {
-            const int begin = t;
-            while (t < c.num_nets && deg(order[t]) <= limits[cl]) ++t;
-            if (t == begin) continue;
-            const int i = wc.n++;
-            wc.group[i] = groups[cl];
-            wc.net_begin[i] = begin;
-            wc.net_end[i] = t;
-            wc.warp_begin[i] = warps;
-            warps += groups[cl] ? spg::ceil_div(t - begin, 32 / groups[cl]) : (t - begin);
-        }
-        wc.warp_begin[wc.n] = warps;
-    }
-    // node-order slots of the pins that belong to a net; the last slot is never read
-    {
-        for (int k = 0; k < c.num_nets; ++k)
-            for (int q = v->net2pin_start[k]; q < v->net2pin_start[k + 1]; ++q)
-                SPG_REQUIRE(v->pin2net[v->flat_net2pin[q]] == k, SPG_E_INVALID,
-                            "pin2net disagrees with the net CSR");
-        std::vector<int> slot_of_pin(c.num_pins, -1), slot_start(T + 1);
-        int slots = 0;
-        for (size_t i = 0; i < T; ++i) {
-            slot_start[i] = slots;
-            for (int t = c.node_start[i]; t < c.node_start[i + 1]; ++t) {
-                const int pin = v->flat_node2pin[t];
-                if (v->pin2net[pin] >= 0) slot_of_pin[pin] = slots++;
-            }
-        }
-        slot_start[T] = slots;
-        std::vector<int> net_slot(c.num_pins);
-        for (int q = 0; q < c.num_pins; ++q) {
-            const int sl = slot_of_pin[v->flat_net2pin[q]];
-            net_slot[q] = sl >= 0 ? sl : slots;
-        }
-        c.slot_start.upload(slot_start, s);
-        c.slot_start_h = slot_start;
-        c.net_slot.upload(net_slot, s);
-        c.num_slots = slots;
-    }
-    c.gpx.alloc(c.num_slots + 1);
-    c.gpy.alloc(c.num_slots + 1);
-    c.gpx.zero(s);
-    c.gpy.zero(s);
-    c.st.alloc(1);
-    SPG_CUDA(cudaMallocHost(&c.hst, sizeof(spg::DevState)));
-    c.scratch_d.alloc(16);
-    SPG_CUDA(cudaStreamSynchronize(s));
+    spg::CtxScope scope(c);
+    spg::load_netlist(c, v, prm);
+    SPG_CUDA(spg::host_wait(c.stream));
     *out = h.release();
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_ctx_load(spg_ctx* ctx, const spg_db_view* v, const spg_params* prm) {
+    API_TRY
+    SPG_REQUIRE(ctx && v && prm, SPG_E_INVALID, "null argument");
+    Context& c = ctx->c;
+    spg::CtxScope scope(c);
+    if (c.side) SPG_CUDA(spg::host_wait(c.side));
+    spg::load_netlist(c, v, prm);
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1264,9 +1565,10 @@ int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y) {
     API_TRY
     SPG_REQUIRE(ctx && x && y, SPG_E_INVALID, "null argument");
     Context& c = ctx->c;
-    SPG_CUDA(cudaMemcpyAsync(c.x.p, x, c.total * sizeof(float), cudaMemcpyHostToDevice, c.stream));
-    SPG_CUDA(cudaMemcpyAsync(c.y.p, y, c.total * sizeof(float), cudaMemcpyHostToDevice, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    spg::CtxScope scope(c);
+    spg::upload_bytes(c.x.p, x, c.total * sizeof(float), c.stream);
+    spg::upload_bytes(c.y.p, y, c.total * sizeof(float), c.stream);
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1275,9 +1577,9 @@ int spg_positions_d2h(spg_ctx* ctx, float* x, float* y) {
     API_TRY
     SPG_REQUIRE(ctx && x && y, SPG_E_INVALID, "null argument");
     Context& c = ctx->c;
-    SPG_CUDA(cudaMemcpyAsync(x, c.x.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaMemcpyAsync(y, c.y.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    spg::CtxScope scope(c);
+    spg::download_bytes(x, c.x.p, c.total * sizeof(float), c.stream);
+    spg::download_bytes(y, c.y.p, c.total * sizeof(float), c.stream);
     return SPG_OK;
     API_CATCH
 }
@@ -1295,10 +1597,10 @@ int spg_grid_init(spg_ctx* ctx, float target, int bin_dim) {
     API_TRY
     SPG_REQUIRE(ctx && target > 0.f, SPG_E_INVALID, "bad argument");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     std::vector<float> hx(c.total), hy(c.total);
-    SPG_CUDA(cudaMemcpyAsync(hx.data(), c.x.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaMemcpyAsync(hy.data(), c.y.p, c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    spg::download_bytes(hx.data(), c.x.p, c.total * sizeof(float), c.stream);
+    spg::download_bytes(hy.data(), c.y.p, c.total * sizeof(float), c.stream);
     spg::grid_init(c, target, bin_dim, hx, hy);
     // parity hooks evaluate over every node: an opt set of all density nodes is not needed
     return SPG_OK;
@@ -1329,7 +1631,7 @@ int spg_grid_read(const spg_ctx* ctx, int which, float* out) {
     SPG_REQUIRE(which >= 0 && which < 8, SPG_E_INVALID, "unknown map");
     const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
     SPG_CUDA(cudaMemcpyAsync(out, b[which]->p, n * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1338,12 +1640,13 @@ int spg_grid_write(spg_ctx* ctx, int which, const float* in) {
     API_TRY
     SPG_REQUIRE(ctx && in && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     spg::DevBuf<float>* b[] = {&c.node_map, &c.filler_map, &c.terminal, &c.base,
                                &c.rho, &c.phi, &c.ex, &c.ey};
     SPG_REQUIRE(which >= 4 && which < 8, SPG_E_INVALID, "only rho, phi, xi_x, xi_y are writable");
     const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
     SPG_CUDA(cudaMemcpyAsync(b[which]->p, in, n * sizeof(float), cudaMemcpyHostToDevice, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1355,7 +1658,7 @@ int spg_grid_read_fixed(const spg_ctx* ctx, int64_t* node, int64_t* filler, int*
     const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
     if (node) SPG_CUDA(cudaMemcpyAsync(node, c.node_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
     if (filler) SPG_CUDA(cudaMemcpyAsync(filler, c.filler_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     if (shift) *shift = c.geom.shift;
     return SPG_OK;
     API_CATCH
@@ -1365,11 +1668,12 @@ int spg_density_accumulate(spg_ctx* ctx) {
     API_TRY
     SPG_REQUIRE(ctx && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     spg::DevPtrs p = c.ptrs();
     c.node_fix.zero(c.stream);
     c.filler_fix.zero(c.stream);
     spg::launch_density_accumulate(p, c.stream);
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1378,13 +1682,14 @@ int spg_overflow(spg_ctx* ctx, float* tau) {
     API_TRY
     SPG_REQUIRE(ctx && tau && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     spg::DevPtrs p = c.ptrs();
     // rho, the float maps and tau from the current fixed-point maps (kept for read_fixed)
     spg::launch_rho_overflow(p, 1, 0, c.stream);
     double over = 0.0;
     spg::launch_finalize_slots(p, spg::SLOT_OVERFLOW, 1, c.scratch_d.p, c.stream);
     SPG_CUDA(cudaMemcpyAsync(&over, c.scratch_d.p, 8, cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     *tau = c.movable_area_scaled > 0.0 ? static_cast<float>(over / c.movable_area_scaled) : 0.f;
     return SPG_OK;
     API_CATCH
@@ -1394,8 +1699,9 @@ int spg_solve_field(spg_ctx* ctx) {
     API_TRY
     SPG_REQUIRE(ctx && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, c.stream);
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1404,13 +1710,14 @@ int spg_gather_force(spg_ctx* ctx, float* force) {
     API_TRY
     SPG_REQUIRE(ctx && force && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     spg::DevPtrs p = c.ptrs();
     spg::DevBuf<float> out;
     out.alloc(2 * static_cast<size_t>(c.total));
     out.zero(c.stream);
     spg::launch_gather_all(p, out.p, c.stream);
     SPG_CUDA(cudaMemcpyAsync(force, out.p, 2 * c.total * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1419,11 +1726,12 @@ int spg_total_charge(spg_ctx* ctx, double* charge) {
     API_TRY
     SPG_REQUIRE(ctx && charge && ctx->c.grid_ready, SPG_E_STATE, "grid not initialised");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     const size_t n = static_cast<size_t>(c.geom.dim) * c.geom.dim;
     std::vector<long long> a(n), b(n);
     SPG_CUDA(cudaMemcpyAsync(a.data(), c.node_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
     SPG_CUDA(cudaMemcpyAsync(b.data(), c.filler_fix.p, n * 8, cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     long long s = 0;
     for (size_t i = 0; i < n; ++i) s += a[i] + b[i];
     *charge = static_cast<double>(s) * c.geom.inv_scale;
@@ -1435,6 +1743,7 @@ int spg_wa_wirelength(spg_ctx* ctx, float gamma, int ignore, double* wl, float* 
     API_TRY
     SPG_REQUIRE(ctx, SPG_E_INVALID, "null context");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     spg::DevPtrs p = c.ptrs();
     p.ignore_net_degree = ignore;
     if (!c.partials.p) {
@@ -1451,7 +1760,7 @@ int spg_wa_wirelength(spg_ctx* ctx, float gamma, int ignore, double* wl, float* 
     SPG_CUDA(cudaMemcpyAsync(&v, c.scratch_d.p, 8, cudaMemcpyDeviceToHost, c.stream));
     if (grad)
         SPG_CUDA(cudaMemcpyAsync(grad, g.p, 2 * c.num_movable * sizeof(float), cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     if (wl) *wl = v;
     return SPG_OK;
     API_CATCH
@@ -1461,6 +1770,7 @@ int spg_hpwl(spg_ctx* ctx, double* hpwl) {
     API_TRY
     SPG_REQUIRE(ctx && hpwl, SPG_E_INVALID, "null argument");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     spg::DevPtrs p = c.ptrs();
     if (!c.partials.p) {
         c.partials.alloc(static_cast<size_t>(spg::RED_SLOTS) * spg::RED_CAP);
@@ -1470,7 +1780,7 @@ int spg_hpwl(spg_ctx* ctx, double* hpwl) {
     spg::launch_wa_nets(p, nullptr, 1.f, 0, c.stream);
     spg::launch_finalize_slots(p, spg::SLOT_HPWL, 1, c.scratch_d.p, c.stream);
     SPG_CUDA(cudaMemcpyAsync(hpwl, c.scratch_d.p, 8, cudaMemcpyDeviceToHost, c.stream));
-    SPG_CUDA(cudaStreamSynchronize(c.stream));
+    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1508,13 +1818,14 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     API_TRY
     SPG_REQUIRE(ctx && us && reps > 0, SPG_E_INVALID, "bad argument");
     Context& c = ctx->c;
+    spg::CtxScope scope(c);
     SPG_REQUIRE(c.grid_ready && c.n_opt > 0 && c.plan, SPG_E_STATE, "run a stage before profiling");
     cudaStream_t s = c.stream;
     const spg::DevPtrs p = c.ptrs();
     // keep the stage's state; profiling runs with decisions off (done) except for the update
     spg::DevState saved;
     SPG_CUDA(cudaMemcpyAsync(&saved, c.st.p, sizeof(saved), cudaMemcpyDeviceToHost, s));
-    SPG_CUDA(cudaStreamSynchronize(s));
+    SPG_CUDA(spg::host_wait(s));
     spg::DevState probe = saved;
     probe.done = 1;
     probe.redo = 0;
@@ -1523,7 +1834,7 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     probe.tk_update = probe.tk_assemble = probe.tk_reduce = 0;
     auto set_state = [&](const spg::DevState& st) {
         SPG_CUDA(cudaMemcpyAsync(c.st.p, &st, sizeof(st), cudaMemcpyHostToDevice, s));
-        SPG_CUDA(cudaStreamSynchronize(s));
+        SPG_CUDA(spg::host_wait(s));
     };
     cudaEvent_t e0, e1;
     SPG_CUDA(cudaEventCreate(&e0));
@@ -1574,7 +1885,7 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     // restore: state, delivered positions, and the evaluation at them
     set_state(saved);
     spg::launch_scatter(p, spg::R_POS, s);
-    SPG_CUDA(cudaStreamSynchronize(s));
+    SPG_CUDA(spg::host_wait(s));
     spg::g_launches = launches0;
     for (int i = 0; i < n && i < 8; ++i) us[i] = t[i];
     return SPG_OK;

@@ -29,6 +29,15 @@ constexpr int RED_THREADS = 256;
 // Blocks of `threads` threads that fill every SM once at the kernel's occupancy, at most
 // `cap`; cached per kernel and device (engine.cu).
 int wave_grid(const void* kernel, int threads, int cap);
+// The grid of a grid-stride kernel over `items` work items, `per_block` per block and pass:
+// enough blocks for one item per thread, at most one wave (wave_grid). Small problems launch
+// only the blocks they fill, so concurrent contexts share the device; the grid is fixed per
+// device and problem size, so reductions keep their fixed order.
+inline int work_grid(const void* kernel, int64_t items, int per_block, int threads = RED_THREADS) {
+    const int64_t need = (items + per_block - 1) / per_block;
+    const int w = wave_grid(kernel, threads, RED_CAP);
+    return need < 1 ? 1 : (need < w ? static_cast<int>(need) : w);
+}
 
 enum RedSlot : int {
     SLOT_OVERFLOW = 0,

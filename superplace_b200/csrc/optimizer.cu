@@ -829,11 +829,13 @@ void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
     LAUNCH(scatter_kernel, vec_blocks(p, scatter_kernel), RED_THREADS, p, role);
 }
 void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s) {
-    LAUNCH(assemble_kernel<false>, wave(assemble_kernel<false>), RED_THREADS, p, pos_role, grad_role,
+    LAUNCH(assemble_kernel<false>, work_grid(reinterpret_cast<const void*>(assemble_kernel<false>), p.n_opt, RED_THREADS),
+           RED_THREADS, p, pos_role, grad_role,
            count_eval);
 }
 void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(assemble_kernel<true>, wave(assemble_kernel<true>), RED_THREADS, p, static_cast<int>(R_U),
+    LAUNCH(assemble_kernel<true>, work_grid(reinterpret_cast<const void*>(assemble_kernel<true>), p.n_opt, RED_THREADS),
+           RED_THREADS, p, static_cast<int>(R_U),
            static_cast<int>(R_G), 1);
 }
 void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
@@ -853,7 +855,8 @@ void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_lambda_init_kernel, 1, 1, p);
 }
 void launch_init_norms(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(init_norms_kernel, wave(init_norms_kernel), RED_THREADS, p);
+    LAUNCH(init_norms_kernel, work_grid(reinterpret_cast<const void*>(init_norms_kernel), 2 * static_cast<int64_t>(p.n_opt), RED_THREADS),
+           RED_THREADS, p);
 }
 void launch_ctl_init_scale(const DevPtrs& p, float init_perturb, cudaStream_t s) {
     LAUNCH(ctl_init_scale_kernel, 1, RED_THREADS, p, init_perturb);
@@ -862,7 +865,8 @@ void launch_init_perturb(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(init_perturb_kernel, vec_blocks(p, init_perturb_kernel), RED_THREADS, p);
 }
 void launch_init_diff(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(init_diff_kernel, wave(init_diff_kernel), RED_THREADS, p);
+    LAUNCH(init_diff_kernel, work_grid(reinterpret_cast<const void*>(init_diff_kernel), 2 * static_cast<int64_t>(p.n_opt), RED_THREADS),
+           RED_THREADS, p);
 }
 void launch_ctl_init_finish(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_init_finish_kernel, 1, RED_THREADS, p);

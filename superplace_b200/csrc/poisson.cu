@@ -166,11 +166,83 @@ double sinpi_ratio(int64_t num, int64_t den) {
 }
 
 template <typename T>
-T* dalloc(size_t n, size_t& bytes) {
-    T* p = nullptr;
-    SPG_CUDA(cudaMalloc(&p, n * sizeof(T)));
-    bytes += n * sizeof(T);
+T* dalloc(size_t n, PoissonPlan& pl) {
+    T* p = static_cast<T*>(dev_alloc(n * sizeof(T), &pl.stream));
+    pl.bytes += n * sizeof(T);
     return p;
+}
+
+// The basis tables of the chain (FFTW r2r definitions, poisson.h) in FP64.
+struct Tables {
+    std::vector<double> cy, cx, bcat, acat, sc;
+    std::vector<double> sin_x, sin_y;  // sin(pi j (x+1/2)/nx) [j][x], sin(pi k (y+1/2)/ny) [k][y]
+};
+
+// The step-dependent tables from the cached sines: Sy (rows ny..2ny of [Ay; Sy]), Sx (rows
+// nx..2nx of [Ax; Sx]) and the spectral scale, with the same expressions as make_tables.
+void step_tables(int nx, int ny, float sx, float sy, const std::vector<double>& sin_x,
+                 const std::vector<double>& sin_y, std::vector<double>& sy_rows, std::vector<double>& sx_rows,
+                 std::vector<double>& sc) {
+    const size_t X = nx, Y = ny;
+    std::vector<double> u(X), v(Y);
+    for (size_t j = 0; j < X; ++j) u[j] = M_PI * static_cast<double>(j) / (static_cast<double>(nx) * sx);
+    for (size_t k = 0; k < Y; ++k) v[k] = M_PI * static_cast<double>(k) / (static_cast<double>(ny) * sy);
+    sy_rows.resize(Y * Y);
+    sx_rows.resize(X * X);
+    sc.resize(X * Y);
+    for (size_t k = 0; k < Y; ++k)
+        for (size_t y = 0; y < Y; ++y) sy_rows[y * Y + k] = 2.0 * v[k] * sin_y[k * Y + y];
+    for (size_t j = 0; j < X; ++j)
+        for (size_t x = 0; x < X; ++x) sx_rows[x * X + j] = 2.0 * u[j] * sin_x[j * X + x];
+    const double nn = static_cast<double>(nx) * static_cast<double>(ny);
+    for (size_t j = 0; j < X; ++j)
+        for (size_t k = 0; k < Y; ++k) {
+            const double den = u[j] * u[j] + v[k] * v[k];
+            sc[j * Y + k] = den > 0.0 ? 1.0 / (nn * den) : 0.0;
+        }
+}
+Tables make_tables(int nx, int ny, float sx, float sy) {
+    const size_t X = nx, Y = ny;
+    Tables t;
+    t.cy.resize(Y * Y);
+    t.cx.resize(X * X);
+    t.bcat.resize(2 * Y * Y);
+    t.acat.resize(2 * X * X);
+    t.sc.resize(X * Y);
+    std::vector<double>&cy = t.cy, &cx = t.cx, &bcat = t.bcat, &acat = t.acat, &sc = t.sc;
+    t.sin_x.resize(X * X);
+    t.sin_y.resize(Y * Y);
+    std::vector<double> u(X), v(Y);
+    for (size_t j = 0; j < X; ++j) u[j] = M_PI * static_cast<double>(j) / (static_cast<double>(nx) * sx);
+    for (size_t k = 0; k < Y; ++k) v[k] = M_PI * static_cast<double>(k) / (static_cast<double>(ny) * sy);
+    for (size_t k = 0; k < Y; ++k)
+        for (size_t y = 0; y < Y; ++y) {
+            const int64_t num = static_cast<int64_t>(k) * (2 * static_cast<int64_t>(y) + 1);
+            const double c = cospi_ratio(num, 2 * static_cast<int64_t>(ny));
+            const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(ny));
+            cy[k * Y + y] = c;
+            t.sin_y[k * Y + y] = s;
+            bcat[y * Y + k] = (k == 0 ? 1.0 : 2.0) * c;      // Ay[y][k]
+            bcat[(Y + y) * Y + k] = 2.0 * v[k] * s;          // Sy[y][k]
+        }
+    for (size_t j = 0; j < X; ++j)
+        for (size_t x = 0; x < X; ++x) {
+            const int64_t num = static_cast<int64_t>(j) * (2 * static_cast<int64_t>(x) + 1);
+            const double c = cospi_ratio(num, 2 * static_cast<int64_t>(nx));
+            const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(nx));
+            cx[j * X + x] = c;
+            t.sin_x[j * X + x] = s;
+            acat[x * X + j] = (j == 0 ? 1.0 : 2.0) * c;      // Ax[x][j]
+            acat[(X + x) * X + j] = 2.0 * u[j] * s;          // Sx[x][j]
+        }
+    const double nn = static_cast<double>(nx) * static_cast<double>(ny);
+    for (size_t j = 0; j < X; ++j)
+        for (size_t k = 0; k < Y; ++k) {
+            const double den = u[j] * u[j] + v[k] * v[k];
+            sc[j * Y + k] = den > 0.0 ? 1.0 / (nn * den) : 0.0;
+        }
+
+    return t;
 }
 
 }  // namespace
@@ -224,81 +296,76 @@ void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float sx, float sy, in
                                               : "cuda-sm100a-bf16x3";
 
     const size_t X = nx, Y = ny;
-    std::vector<double> cy(Y * Y), cx(X * X), bcat(2 * Y * Y), acat(2 * X * X), sc(X * Y);
-    std::vector<double> u(X), v(Y);
-    for (size_t j = 0; j < X; ++j) u[j] = M_PI * static_cast<double>(j) / (static_cast<double>(nx) * sx);
-    for (size_t k = 0; k < Y; ++k) v[k] = M_PI * static_cast<double>(k) / (static_cast<double>(ny) * sy);
-    for (size_t k = 0; k < Y; ++k)
-        for (size_t y = 0; y < Y; ++y) {
-            const int64_t num = static_cast<int64_t>(k) * (2 * static_cast<int64_t>(y) + 1);
-            const double c = cospi_ratio(num, 2 * static_cast<int64_t>(ny));
-            const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(ny));
-            cy[k * Y + y] = c;
-            bcat[y * Y + k] = (k == 0 ? 1.0 : 2.0) * c;      // Ay[y][k]
-            bcat[(Y + y) * Y + k] = 2.0 * v[k] * s;          // Sy[y][k]
-        }
-    for (size_t j = 0; j < X; ++j)
-        for (size_t x = 0; x < X; ++x) {
-            const int64_t num = static_cast<int64_t>(j) * (2 * static_cast<int64_t>(x) + 1);
-            const double c = cospi_ratio(num, 2 * static_cast<int64_t>(nx));
-            const double s = sinpi_ratio(num, 2 * static_cast<int64_t>(nx));
-            cx[j * X + x] = c;
-            acat[x * X + j] = (j == 0 ? 1.0 : 2.0) * c;      // Ax[x][j]
-            acat[(X + x) * X + j] = 2.0 * u[j] * s;          // Sx[x][j]
-        }
-    const double nn = static_cast<double>(nx) * static_cast<double>(ny);
-    for (size_t j = 0; j < X; ++j)
-        for (size_t k = 0; k < Y; ++k) {
-            const double den = u[j] * u[j] + v[k] * v[k];
-            sc[j * Y + k] = den > 0.0 ? 1.0 / (nn * den) : 0.0;
-        }
+    const Tables t = make_tables(nx, ny, sx, sy);
+    const std::vector<double>&cy = t.cy, &cx = t.cx, &bcat = t.bcat, &acat = t.acat, &sc = t.sc;
+    pl.sin_x = t.sin_x;
+    pl.sin_y = t.sin_y;
 
-    size_t& b = pl.bytes;
     const size_t B = static_cast<size_t>(batch_cap);
     if (precision == SPG_POISSON_FP64) {
         auto up64 = [&](double*& dst, const std::vector<double>& h) {
-            dst = dalloc<double>(h.size(), b);
-            SPG_CUDA(cudaMemcpy(dst, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+            dst = dalloc<double>(h.size(), pl);
+            upload_bytes(dst, h.data(), h.size() * 8, pl.stream);
         };
         up64(pl.cy64, cy);
         up64(pl.cx64, cx);
         up64(pl.bcat64, bcat);
         up64(pl.acat64, acat);
         up64(pl.scale64, sc);
-        pl.rho64 = dalloc<double>(B * X * Y, b);
-        pl.t0t64 = dalloc<double>(B * X * Y, b);
-        pl.p64 = dalloc<double>(B * X * Y, b);
-        pl.t12t64 = dalloc<double>(2 * B * X * Y, b);
+        pl.rho64 = dalloc<double>(B * X * Y, pl);
+        pl.t0t64 = dalloc<double>(B * X * Y, pl);
+        pl.p64 = dalloc<double>(B * X * Y, pl);
+        pl.t12t64 = dalloc<double>(2 * B * X * Y, pl);
         return;
     }
     // the FP32 forms: bases rounded once to float
     auto up32 = [&](float*& dst, const std::vector<double>& h) {
         std::vector<float> f(h.begin(), h.end());
-        dst = dalloc<float>(f.size(), b);
-        SPG_CUDA(cudaMemcpy(dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+        dst = dalloc<float>(f.size(), pl);
+        upload_bytes(dst, f.data(), f.size() * 4, pl.stream);
+        return f;
     };
-    up32(pl.cy, cy);
-    up32(pl.cx, cx);
-    up32(pl.bcat, bcat);
-    up32(pl.acat, acat);
+    const std::vector<float> fcy = up32(pl.cy, cy), fcx = up32(pl.cx, cx);
+    const std::vector<float> fbcat = up32(pl.bcat, bcat), facat = up32(pl.acat, acat);
     up32(pl.scale, sc);
-    pl.dc = dalloc<float>(4 * B * std::max(X, Y), b);  // row means / sums, both splits
+    pl.dc = dalloc<float>(4 * B * std::max(X, Y), pl);  // row means / sums, both splits
     if (precision == SPG_POISSON_FP32) {
-        pl.t0t = dalloc<float>(B * X * Y, b);
-        pl.p = dalloc<float>(B * X * Y, b);
-        pl.t12t = dalloc<float>(2 * B * X * Y, b);
+        pl.t0t = dalloc<float>(B * X * Y, pl);
+        pl.p = dalloc<float>(B * X * Y, pl);
+        pl.t12t = dalloc<float>(2 * B * X * Y, pl);
     } else {
-        tc_plan_create(pl);
+        tc_plan_create(pl, fcy, fcx, fbcat, facat);
     }
+}
+
+void poisson_plan_set_steps(PoissonPlan& pl, float sx, float sy) {
+    if (sx == pl.step_x && sy == pl.step_y) return;
+    SPG_REQUIRE(sx > 0.f && sy > 0.f, SPG_E_INVALID, "Poisson: bin step must be positive");
+    const size_t X = pl.nx, Y = pl.ny;
+    std::vector<double> sy_rows, sx_rows, sc;
+    step_tables(pl.nx, pl.ny, sx, sy, pl.sin_x, pl.sin_y, sy_rows, sx_rows, sc);
+    if (pl.precision == SPG_POISSON_FP64) {
+        upload_bytes(pl.bcat64 + Y * Y, sy_rows.data(), Y * Y * 8, pl.stream);
+        upload_bytes(pl.acat64 + X * X, sx_rows.data(), X * X * 8, pl.stream);
+        upload_bytes(pl.scale64, sc.data(), sc.size() * 8, pl.stream);
+    } else {
+        const std::vector<float> fsy(sy_rows.begin(), sy_rows.end()), fsx(sx_rows.begin(), sx_rows.end());
+        const std::vector<float> fsc(sc.begin(), sc.end());
+        upload_bytes(pl.bcat + Y * Y, fsy.data(), Y * Y * 4, pl.stream);
+        upload_bytes(pl.acat + X * X, fsx.data(), X * X * 4, pl.stream);
+        upload_bytes(pl.scale, fsc.data(), fsc.size() * 4, pl.stream);
+        if (pl.precision == SPG_POISSON_BF16X3) tc_plan_refill_sines(pl, fsy, fsx);
+    }
+    pl.step_x = sx;
+    pl.step_y = sy;
 }
 
 void poisson_plan_destroy(PoissonPlan& pl) {
     if (pl.precision == SPG_POISSON_BF16X3) tc_plan_destroy(pl);
-    for (float* q : {pl.cy, pl.cx, pl.bcat, pl.acat, pl.scale, pl.t0t, pl.p, pl.t12t, pl.dc})
-        if (q) cudaFree(q);
+    for (float* q : {pl.cy, pl.cx, pl.bcat, pl.acat, pl.scale, pl.t0t, pl.p, pl.t12t, pl.dc}) dev_free(q, pl.stream);
     pl.cy = pl.cx = pl.bcat = pl.acat = pl.scale = pl.t0t = pl.p = pl.t12t = pl.dc = nullptr;
     for (double* q : {pl.cy64, pl.cx64, pl.bcat64, pl.acat64, pl.scale64, pl.rho64, pl.t0t64, pl.p64, pl.t12t64})
-        if (q) cudaFree(q);
+        dev_free(q, pl.stream);
     pl.cy64 = pl.cx64 = pl.bcat64 = pl.acat64 = pl.scale64 = nullptr;
     pl.rho64 = pl.t0t64 = pl.p64 = pl.t12t64 = nullptr;
 }

@@ -23,6 +23,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 namespace spg {
 
@@ -45,13 +46,18 @@ struct PoissonPlan {
     uint16_t *cy_s = nullptr, *cx_s = nullptr, *bcat_s = nullptr, *acat_s = nullptr;
     uint16_t *rho_s = nullptr, *t0t_s = nullptr, *p_s = nullptr, *t12t_s = nullptr;
     void* tc = nullptr;  // tensor-core launch state (poisson_tc.cu)
+    std::vector<double> sin_x, sin_y;  // host sine tables, for new bin steps (set_steps)
     size_t bytes = 0;    // device memory held
+    cudaStream_t stream = nullptr;  // the stream its buffers' frees are ordered on
 };
 
 // Allocates bases and work buffers for up to batch_cap grids. precision: SPG_POISSON_*.
 void poisson_plan_create(PoissonPlan& pl, int nx, int ny, float step_x, float step_y,
                          int precision, int batch_cap);
 void poisson_plan_destroy(PoissonPlan& pl);
+// New bin steps for an existing plan: the tables are rebuilt on the host and written into the
+// plan's buffers on its stream (no allocation; the tensor maps stay valid).
+void poisson_plan_set_steps(PoissonPlan& pl, float step_x, float step_y);
 // Device solve of `batch` grids stored back to back.
 void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
                    cudaStream_t s);
@@ -93,8 +99,14 @@ void sgemm_tn(const GemmArgs& g, int batch, cudaStream_t s);
 
 // ---- tensor-core path (poisson_tc.cu)
 bool tc_supported(int nx, int ny);
-void tc_plan_create(PoissonPlan& pl);
+// split-BF16 planes of the FP32 bases (given as the host tables the plan uploaded), work
+// buffers and tensor maps
+void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::vector<float>& cx,
+                    const std::vector<float>& bcat, const std::vector<float>& acat);
 void tc_plan_destroy(PoissonPlan& pl);
+// rewrite the split-BF16 planes of the step-dependent rows in place: Sy (rows ny..2ny of
+// [Ay; Sy]) and Sx (rows nx..2nx of [Ax; Sx]); same buffers, same tensor maps
+void tc_plan_refill_sines(PoissonPlan& pl, const std::vector<float>& sy_rows, const std::vector<float>& sx_rows);
 void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
               cudaStream_t s);
 

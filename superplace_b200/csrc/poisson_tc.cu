@@ -405,14 +405,13 @@ __global__ void prep_split_kernel(const float* src, int rows, int nseg, int64_t 
 
 // ------------------------------------------------------------------ host side
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         cudaDriverEntryPointQueryResult q;
         void* p = nullptr;
         SPG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
         SPG_REQUIRE(q == cudaDriverEntryPointSuccess && p, SPG_E_CUDA, "cuTensorMapEncodeTiled unavailable");
-        fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
     return fn;
 }
 
@@ -510,29 +509,25 @@ void split_host(const std::vector<float>& v, std::vector<uint16_t>& out) {
 
 bool tc_supported(int nx, int ny) { return nx >= 128 && ny >= 128 && nx % 128 == 0 && ny % 128 == 0; }
 
-void tc_plan_create(PoissonPlan& pl) {
+void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::vector<float>& cx,
+                    const std::vector<float>& bcat, const std::vector<float>& acat) {
     const int64_t X = pl.nx, Y = pl.ny, B = pl.batch_cap;
-    auto dl = [&](const float* d, size_t n) {
-        std::vector<float> h(n);
-        SPG_CUDA(cudaMemcpy(h.data(), d, n * 4, cudaMemcpyDeviceToHost));
-        return h;
-    };
     auto up = [&](uint16_t*& dst, const std::vector<uint16_t>& h) {
-        SPG_CUDA(cudaMalloc(&dst, h.size() * 2));
+        dst = static_cast<uint16_t*>(dev_alloc(h.size() * 2, &pl.stream));
         pl.bytes += h.size() * 2;
-        SPG_CUDA(cudaMemcpy(dst, h.data(), h.size() * 2, cudaMemcpyHostToDevice));
+        upload_bytes(dst, h.data(), h.size() * 2, pl.stream);
     };
     std::vector<uint16_t> sp;
-    split_host(dl(pl.cy, Y * Y), sp);
+    split_host(cy, sp);
     up(pl.cy_s, sp);
-    split_host(dl(pl.cx, X * X), sp);
+    split_host(cx, sp);
     up(pl.cx_s, sp);
-    split_host(dl(pl.bcat, 2 * Y * Y), sp);
+    split_host(bcat, sp);
     up(pl.bcat_s, sp);
-    split_host(dl(pl.acat, 2 * X * X), sp);
+    split_host(acat, sp);
     up(pl.acat_s, sp);
     auto al16 = [&](uint16_t*& p, size_t n) {
-        SPG_CUDA(cudaMalloc(&p, n * 2));
+        p = static_cast<uint16_t*>(dev_alloc(n * 2, &pl.stream));
         pl.bytes += n * 2;
     };
     al16(pl.rho_s, 2 * B * X * Y);
@@ -541,10 +536,10 @@ void tc_plan_create(PoissonPlan& pl) {
     al16(pl.t12t_s, 4 * B * X * Y);
     auto* st = new TcState;
     pl.tc = st;
-    SPG_CUDA(cudaMalloc(&st->t0t32, B * X * Y * 4));
-    SPG_CUDA(cudaMalloc(&st->sums, 2 * B * std::max(X, Y) * 4));
-    SPG_CUDA(cudaMalloc(&st->err, 4));
-    SPG_CUDA(cudaMemset(st->err, 0, 4));
+    st->t0t32 = static_cast<float*>(dev_alloc(B * X * Y * 4, &pl.stream));
+    st->sums = static_cast<float*>(dev_alloc(2 * B * std::max(X, Y) * 4, &pl.stream));
+    st->err = static_cast<int*>(dev_alloc(4, &pl.stream));
+    SPG_CUDA(cudaMemsetAsync(st->err, 0, 4, pl.stream));
     pl.bytes += B * X * Y * 4 + 2 * B * std::max(X, Y) * 4 + 4;
     st->cy = make_map(pl.cy_s, 2 * Y, Y, TC_BM);
     st->cx = make_map(pl.cx_s, 2 * X, X, TC_BM);
@@ -554,25 +549,35 @@ void tc_plan_create(PoissonPlan& pl) {
     st->t0t_b = make_map(pl.t0t_s, 2 * Y, B * X, TC_BN);
     st->p_b = make_map(pl.p_s, 2 * B * X, Y, TC_BN);
     st->t12t_b = make_map(pl.t12t_s, 4 * Y, B * X, TC_BN);
-    static bool attr = false;
-    if (!attr) {
-        const int bytes = static_cast<int>(tc_smem_bytes());
-        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
-        attr = true;
-    }
+    // per device (the attribute is a property of the kernel on the current device)
+    const int bytes = static_cast<int>(tc_smem_bytes());
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+}
+
+void tc_plan_refill_sines(PoissonPlan& pl, const std::vector<float>& sy_rows, const std::vector<float>& sx_rows) {
+    // plane stacks are [hi | lo] of the whole [A; S] matrix: the S rows start half-way into
+    // each plane
+    const size_t X = pl.nx, Y = pl.ny;
+    std::vector<uint16_t> sp;
+    split_host(sy_rows, sp);  // sp = [hi(Y*Y) | lo(Y*Y)]
+    upload_bytes(pl.bcat_s + Y * Y, sp.data(), Y * Y * 2, pl.stream);
+    upload_bytes(pl.bcat_s + 2 * Y * Y + Y * Y, sp.data() + Y * Y, Y * Y * 2, pl.stream);
+    split_host(sx_rows, sp);
+    upload_bytes(pl.acat_s + X * X, sp.data(), X * X * 2, pl.stream);
+    upload_bytes(pl.acat_s + 2 * X * X + X * X, sp.data() + X * X, X * X * 2, pl.stream);
 }
 
 void tc_plan_destroy(PoissonPlan& pl) {
     for (uint16_t* q : {pl.cy_s, pl.cx_s, pl.bcat_s, pl.acat_s, pl.rho_s, pl.t0t_s, pl.p_s, pl.t12t_s})
-        if (q) cudaFree(q);
+        dev_free(q, pl.stream);
     pl.cy_s = pl.cx_s = pl.bcat_s = pl.acat_s = pl.rho_s = pl.t0t_s = pl.p_s = pl.t12t_s = nullptr;
     if (auto* st = static_cast<TcState*>(pl.tc)) {
-        cudaFree(st->t0t32);
-        cudaFree(st->sums);
-        cudaFree(st->err);
+        dev_free(st->t0t32, pl.stream);
+        dev_free(st->sums, pl.stream);
+        dev_free(st->err, pl.stream);
         delete st;
         pl.tc = nullptr;
     }

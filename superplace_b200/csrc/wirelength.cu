@@ -225,7 +225,8 @@ void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, 
     int dev = 0, sms = 0;
     SPG_CUDA(cudaGetDevice(&dev));
     SPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int full = wave_grid(reinterpret_cast<const void*>(wa_net_kernel), RED_THREADS, RED_CAP);
+    // one warp per lane group of nets: the grid the work fills, at most one wave
+    const int full = work_grid(reinterpret_cast<const void*>(wa_net_kernel), p.wa.warp_begin[p.wa.n], RED_THREADS / 32);
     const int grid = per_sm > 0 ? std::min(full, std::min(per_sm * sms, RED_CAP)) : full;
     launch_prio(false, wa_net_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, gamma_dev, gamma_host, use_dev);
 }

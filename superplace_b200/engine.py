@@ -60,6 +60,7 @@ def lib():
                                           C.c_uint64, fp, fp]
         L.spg_ctx_create.argtypes = [C.POINTER(abi.DbView), C.POINTER(abi.Params), C.POINTER(vp)]
         L.spg_ctx_destroy.argtypes = [vp]
+        L.spg_ctx_load.argtypes = [vp, C.POINTER(abi.DbView), C.POINTER(abi.Params)]
         L.spg_positions_h2d.argtypes = [vp, fp, fp]
         L.spg_positions_d2h.argtypes = [vp, fp, fp]
         L.spg_flags_h2d.argtypes = [vp, C.POINTER(C.c_uint8)]
@@ -201,6 +202,15 @@ class GpContext:
         h = C.c_void_p()
         check(lib().spg_ctx_create(C.byref(self._view), C.byref(self.params), C.byref(h)))
         self.h = h
+        self.dim = 0
+
+    def load(self, db: PlaceDB, params: abi.Params | None = None):
+        """Replace the netlist (and parameters) with another instance, keeping the context's
+        streams and device buffers (spg_ctx_load): what a placement server does per request."""
+        self.db = db
+        self.params = params or self.params
+        self._view = db.view()
+        check(lib().spg_ctx_load(self.h, C.byref(self._view), C.byref(self.params)))
         self.dim = 0
 
     def close(self):
