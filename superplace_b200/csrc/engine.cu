@@ -342,6 +342,9 @@ struct Context : ContextStreams {
     std::vector<float> hw_h, hh_h, wgt_h;  // per-node footprint data of the current grid
     std::vector<int> slot_start_h;         // node-order pin slots (see DevPtrs::slot_start)
     std::vector<uint8_t> kind_h;           // host copy of the per-node kernel classes
+    // host copy of the node positions as last uploaded, while the device copy is unchanged
+    std::vector<float> x_mirror, y_mirror;
+    bool mirror_valid = false;
     DevBuf<float> opt_lo, opt_hi, force, pool;
     DevBuf<double> opt_area;
     int n_opt_small = 0, n_opt_large = 0;
@@ -1068,10 +1071,14 @@ void stage_run(Context& c, int stage, spg_result* res) {
     cudaStream_t s = c.stream;
     // constructing EPlace rebuilds the grid with the current flags (gp_stage.cpp:175-177)
     {
-        std::vector<float> hx(c.total), hy(c.total);
-        download_bytes(hx.data(), c.x.p, c.total * sizeof(float), s);
-        download_bytes(hy.data(), c.y.p, c.total * sizeof(float), s);
-        grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, hx, hy);
+        if (!c.mirror_valid) {
+            c.x_mirror.resize(c.total);
+            c.y_mirror.resize(c.total);
+            download_bytes(c.x_mirror.data(), c.x.p, c.total * sizeof(float), s);
+            download_bytes(c.y_mirror.data(), c.y.p, c.total * sizeof(float), s);
+        }
+        grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, c.x_mirror, c.y_mirror);
+        c.mirror_valid = false;  // the stage moves the positions
     }
     ht.mark("grid_init");
     stage_setup(c, stage);
@@ -1261,6 +1268,9 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
     cudaStream_t s = c.stream;
     c.x.upload(v->node_x, T, s);
     c.y.upload(v->node_y, T, s);
+    c.x_mirror.assign(v->node_x, v->node_x + T);
+    c.y_mirror.assign(v->node_y, v->node_y + T);
+    c.mirror_valid = true;
     c.dw.upload(v->node_w, T, s);
     c.dh.upload(v->node_h, T, s);
     c.pox.upload(v->pin_offset_x, c.num_pins, s);
@@ -1568,6 +1578,9 @@ int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y) {
     spg::CtxScope scope(c);
     spg::upload_bytes(c.x.p, x, c.total * sizeof(float), c.stream);
     spg::upload_bytes(c.y.p, y, c.total * sizeof(float), c.stream);
+    c.x_mirror.assign(x, x + c.total);
+    c.y_mirror.assign(y, y + c.total);
+    c.mirror_valid = true;
     SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
@@ -1820,6 +1833,7 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     Context& c = ctx->c;
     spg::CtxScope scope(c);
     SPG_REQUIRE(c.grid_ready && c.n_opt > 0 && c.plan, SPG_E_STATE, "run a stage before profiling");
+    c.mirror_valid = false;  // the parts below write the node positions
     cudaStream_t s = c.stream;
     const spg::DevPtrs p = c.ptrs();
     // keep the stage's state; profiling runs with decisions off (done) except for the update
