@@ -339,6 +339,12 @@ struct Context : ContextStreams {
     DevBuf<int> opt_idx, opt_deg, opt_small, opt_large;
     DevBuf<float4> opt_geom;
     DevBuf<int4> opt_meta;
+    // the fillers' shared attributes (see DevPtrs::filler_k0)
+    int filler_k0 = 0;
+    float4 filler_geom{};
+    int4 filler_meta{};
+    double filler_area = 0.0;
+    float filler_lo_x = 0.f, filler_hi_x = 0.f, filler_lo_y = 0.f, filler_hi_y = 0.f;
     std::vector<float> hw_h, hh_h, wgt_h;  // per-node footprint data of the current grid
     std::vector<int> slot_start_h;         // node-order pin slots (see DevPtrs::slot_start)
     std::vector<uint8_t> kind_h;           // host copy of the per-node kernel classes
@@ -420,6 +426,15 @@ struct Context : ContextStreams {
         p.opt_idx = opt_idx.p;
         p.opt_geom = opt_geom.p;
         p.opt_meta = opt_meta.p;
+        p.filler_k0 = filler_k0;
+        p.filler_node0 = num_nodes - filler_k0;
+        p.filler_geom = filler_geom;
+        p.filler_meta = filler_meta;
+        p.filler_area = filler_area;
+        p.filler_lo_x = filler_lo_x;
+        p.filler_hi_x = filler_hi_x;
+        p.filler_lo_y = filler_lo_y;
+        p.filler_hi_y = filler_hi_y;
         p.opt_lo = opt_lo.p;
         p.opt_hi = opt_hi.p;
         p.opt_deg = opt_deg.p;
@@ -719,6 +734,31 @@ void stage_setup(Context& c, int stage) {
     c.opt_area.upload(area, s);
     c.opt_geom.upload(geom, s);
     c.opt_meta.upload(meta, s);
+    // the fillers close the opt set (one run, nodes num_nodes..total-1); when they all share
+    // every attribute the kernels read, pass those once instead of per node
+    {
+        const int nf = c.total - c.num_nodes;
+        const int k0 = n - nf;
+        bool same = nf > 0 && k0 >= 0 && opt[k0] == c.num_nodes;
+        for (int k = k0; same && k < n; ++k) {
+            same = opt[k] == c.num_nodes + (k - k0) && geom[k].x == geom[k0].x && geom[k].y == geom[k0].y &&
+                   geom[k].z == geom[k0].z && meta[k].x == meta[k].y && meta[k].z == meta[k0].z &&
+                   meta[k].w == meta[k0].w && area[k] == area[k0] && lo[k] == lo[k0] && hi[k] == hi[k0] &&
+                   lo[n + k] == lo[n + k0] && hi[n + k] == hi[n + k0];
+        }
+        if (same) {
+            c.filler_k0 = k0;
+            c.filler_geom = geom[k0];
+            c.filler_meta = make_int4(0, 0, meta[k0].z, meta[k0].w);
+            c.filler_area = area[k0];
+            c.filler_lo_x = lo[k0];
+            c.filler_hi_x = hi[k0];
+            c.filler_lo_y = lo[n + k0];
+            c.filler_hi_y = hi[n + k0];
+        } else {
+            c.filler_k0 = n;
+        }
+    }
     // density nodes the loop's step kernel does not rasterize: small ones outside the opt
     // set (the cells of FILLERONLY, the macros of cGP) and every large node
     {

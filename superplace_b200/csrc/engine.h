@@ -158,6 +158,14 @@ struct DevPtrs {
     //   opt_meta[k] = {first pin slot, end pin slot, nodeDegree, kind | OPT_HAS_WL}
     const float4* opt_geom;
     const int4* opt_meta;
+    // Fillers (opt indices k >= filler_k0, nodes filler_node0 + k) all share one size and
+    // carry no pins, so their per-node attributes are these constants instead of loads;
+    // filler_k0 = n_opt when the fillers differ (then every node reads the arrays).
+    int filler_k0, filler_node0;
+    float4 filler_geom;
+    int4 filler_meta;
+    double filler_area;
+    float filler_lo_x, filler_hi_x, filler_lo_y, filler_hi_y;
     float* force;          // 2*nOpt, density force q*xi (not gradient)
     float* pool;           // NUM_ROLES + SNAP_MAX vectors of 2*nOpt
     size_t vec_stride;

@@ -466,10 +466,11 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
     double acc_wl = 0.0, acc_den = 0.0;
     double dx = 0.0, dg = 0.0, sy = 0.0, gn = 0.0;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int4 meta = p.opt_meta[k];
-        const float4 geo = p.opt_geom[k];
+        const bool fill = k >= p.filler_k0;  // a filler: attributes are the shared constants
+        const int4 meta = fill ? p.filler_meta : p.opt_meta[k];
+        const float4 geo = fill ? p.filler_geom : p.opt_geom[k];
         const float x = pos[k], y = pos[n + k];
-        const double area = p.opt_area[k];
+        const double area = fill ? p.filler_area : p.opt_area[k];
         float upx = 0.f, upy = 0.f, gpx = 0.f, gpy = 0.f;
         if (FUSE) {
             upx = up[k];
@@ -593,8 +594,9 @@ __global__ void __launch_bounds__(RED_THREADS) step_kernel(DevPtrs p) {
     const int n = p.n_opt;
     bool bad = false;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const int4 meta = p.opt_meta[k];
-        const float4 geo = p.opt_geom[k];
+        const bool fill = k >= p.filler_k0;  // a filler: attributes are the shared constants
+        const int4 meta = fill ? p.filler_meta : p.opt_meta[k];
+        const float4 geo = fill ? p.filler_geom : p.opt_geom[k];
         float nu[2];
         if (apply) {
 #pragma unroll
@@ -604,13 +606,14 @@ __global__ void __launch_bounds__(RED_THREADS) step_kernel(DevPtrs p) {
                 if (snap) snap[q] = uq;
                 const float vk = fsub(uq, fmul(alpha, g[q]));
                 const float uk = fadd(vk, fmul(m, fsub(vk, v[q])));
-                const float lo = p.opt_lo[q], hi = p.opt_hi[q];
+                const float lo = fill ? (c ? p.filler_lo_y : p.filler_lo_x) : p.opt_lo[q];
+                const float hi = fill ? (c ? p.filler_hi_y : p.filler_hi_x) : p.opt_hi[q];
                 vn[q] = clamp_box(vk, lo, hi);
                 nu[c] = clamp_box(uk, lo, hi);
                 un[q] = nu[c];
             }
             bad |= !isfinite(nu[0]) || !isfinite(nu[1]);
-            const int i = p.opt_idx[k];
+            const int i = fill ? p.filler_node0 + k : p.opt_idx[k];
             p.x[i] = nu[0];
             p.y[i] = nu[1];
         } else {
