@@ -438,6 +438,62 @@ __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, d
     }
 }
 
+// One node of the assembly (see assemble_kernel). FILL: a filler, whose attributes are the
+// shared constants (no pins, so no WA term).
+template <bool FUSE, bool FILL>
+__device__ __forceinline__ void assemble_node(const DevPtrs& p, int k, float lambda, const float* __restrict__ pos,
+                                              float* __restrict__ grad, const float* __restrict__ up,
+                                              const float* __restrict__ gp, double& acc_wl, double& acc_den,
+                                              double& dx, double& dg, double& sy, double& gn) {
+    const int n = p.n_opt;
+    const int4 meta = FILL ? p.filler_meta : p.opt_meta[k];
+    const float4 geo = FILL ? p.filler_geom : p.opt_geom[k];
+    const float x = pos[k], y = pos[n + k];
+    const double area = FILL ? p.filler_area : p.opt_area[k];
+    float upx = 0.f, upy = 0.f, gpx = 0.f, gpy = 0.f;
+    if (FUSE) {
+        upx = up[k];
+        upy = up[n + k];
+        gpx = gp[k];
+        gpy = gp[n + k];
+    }
+    float gx = 0.f, gy = 0.f;
+    if (!FILL) {
+        for (int t = meta.x; t < meta.y; ++t) {
+            gx = fadd(gx, p.gpx[t]);
+            gy = fadd(gy, p.gpy[t]);
+        }
+    }
+    float fx, fy;
+    if (meta.w & K_LARGE) {
+        fx = p.force[k];
+        fy = p.force[n + k];
+    } else {
+        gather_at(p, x, y, geo.x, geo.y, geo.z, fx, fy);
+    }
+    const double den = __dadd_rn(static_cast<double>(meta.z), __dmul_rn(static_cast<double>(lambda), area));
+    const float precond = static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
+    const float ox = fmul(precond, fsub(gx, fmul(lambda, fx)));
+    const float oy = fmul(precond, fsub(gy, fmul(lambda, fy)));
+    grad[k] = ox;
+    grad[n + k] = oy;
+    if (!isfinite(ox) || !isfinite(oy)) raise_error(p.st, SPG_E_NON_FINITE);
+    if (!FILL && (meta.w & OPT_HAS_WL)) acc_wl += static_cast<double>(fadd(fabsf(gx), fabsf(gy)));
+    acc_den += static_cast<double>(fadd(fabsf(fx), fabsf(fy)));
+    if (FUSE) {
+        // l2Diff, dotDiff, l2Norm terms (nesterov.cpp:25-45), x then y
+        const double sxd = static_cast<double>(x) - static_cast<double>(upx);
+        const double syd = static_cast<double>(y) - static_cast<double>(upy);
+        const double yx = static_cast<double>(ox) - static_cast<double>(gpx);
+        const double yy = static_cast<double>(oy) - static_cast<double>(gpy);
+        dx += __dmul_rn(sxd, sxd) + __dmul_rn(syd, syd);
+        dg += __dmul_rn(yx, yx) + __dmul_rn(yy, yy);
+        sy += __dmul_rn(sxd, yx) + __dmul_rn(syd, yy);
+        gn += __dmul_rn(static_cast<double>(ox), static_cast<double>(ox)) +
+              __dmul_rn(static_cast<double>(oy), static_cast<double>(oy));
+    }
+}
+
 // grad_k = precond * (dWL - lambda * q*xi), precond = 1 / max(1, deg + lambda*area)
 // (eplace.cpp:166-189), with the WA pass 2 (per-node sum of per-pin contributions in
 // node->pin order, wa_wirelength.cpp:137-179) and the field gather of cells fused in (large
@@ -465,53 +521,15 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
     const int n = p.n_opt;
     double acc_wl = 0.0, acc_den = 0.0;
     double dx = 0.0, dg = 0.0, sy = 0.0, gn = 0.0;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const bool fill = k >= p.filler_k0;  // a filler: attributes are the shared constants
-        const int4 meta = fill ? p.filler_meta : p.opt_meta[k];
-        const float4 geo = fill ? p.filler_geom : p.opt_geom[k];
-        const float x = pos[k], y = pos[n + k];
-        const double area = fill ? p.filler_area : p.opt_area[k];
-        float upx = 0.f, upy = 0.f, gpx = 0.f, gpy = 0.f;
-        if (FUSE) {
-            upx = up[k];
-            upy = up[n + k];
-            gpx = gp[k];
-            gpy = gp[n + k];
-        }
-        float gx = 0.f, gy = 0.f;
-        for (int t = meta.x; t < meta.y; ++t) {
-            gx = fadd(gx, p.gpx[t]);
-            gy = fadd(gy, p.gpy[t]);
-        }
-        float fx, fy;
-        if (meta.w & K_LARGE) {
-            fx = p.force[k];
-            fy = p.force[n + k];
-        } else {
-            gather_at(p, x, y, geo.x, geo.y, geo.z, fx, fy);
-        }
-        const double den = __dadd_rn(static_cast<double>(meta.z), __dmul_rn(static_cast<double>(lambda), area));
-        const float precond = static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
-        const float ox = fmul(precond, fsub(gx, fmul(lambda, fx)));
-        const float oy = fmul(precond, fsub(gy, fmul(lambda, fy)));
-        grad[k] = ox;
-        grad[n + k] = oy;
-        if (!isfinite(ox) || !isfinite(oy)) raise_error(p.st, SPG_E_NON_FINITE);
-        if (meta.w & OPT_HAS_WL) acc_wl += static_cast<double>(fadd(fabsf(gx), fabsf(gy)));
-        acc_den += static_cast<double>(fadd(fabsf(fx), fabsf(fy)));
-        if (FUSE) {
-            // l2Diff, dotDiff, l2Norm terms (nesterov.cpp:25-45), x then y
-            const double sxd = static_cast<double>(x) - static_cast<double>(upx);
-            const double syd = static_cast<double>(y) - static_cast<double>(upy);
-            const double yx = static_cast<double>(ox) - static_cast<double>(gpx);
-            const double yy = static_cast<double>(oy) - static_cast<double>(gpy);
-            dx += __dmul_rn(sxd, sxd) + __dmul_rn(syd, syd);
-            dg += __dmul_rn(yx, yx) + __dmul_rn(yy, yy);
-            sy += __dmul_rn(sxd, yx) + __dmul_rn(syd, yy);
-            gn += __dmul_rn(static_cast<double>(ox), static_cast<double>(ox)) +
-                  __dmul_rn(static_cast<double>(oy), static_cast<double>(oy));
-        }
-    }
+    // cells, then the fillers (their attributes the shared constants); every thread keeps the
+    // nodes k = t0 (mod stride) of a single grid-stride pass, in increasing k
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+    const int k0 = p.filler_k0 < n ? p.filler_k0 : n;
+    int k = t0;
+    for (; k < k0; k += stride)
+        assemble_node<FUSE, false>(p, k, lambda, pos, grad, up, gp, acc_wl, acc_den, dx, dg, sy, gn);
+    for (; k < n; k += stride)
+        assemble_node<FUSE, true>(p, k, lambda, pos, grad, up, gp, acc_wl, acc_den, dx, dg, sy, gn);
     if (FUSE) {
         double v6[6] = {acc_wl, acc_den, dx, dg, sy, gn};
         block_sums(v6);
