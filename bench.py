@@ -187,24 +187,42 @@ def cpu_baseline_sample(db, workload, iters=8):
                 "sample": f"failed: {e}"}
 
 
-def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision):
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each part, from one
+# ncu --set full capture of the 211k-cell workload with the split-BF16 Poisson (caches flushed
+# before each replayed launch, so these are cold-L2 figures; writes that stay in L2 at the end
+# of a launch are not counted). The Poisson part is its seven launches of one solve.
+PROFILED_DRAM_BYTES = {
+    ("large", "bf16x3"): {"update": 41.87e6, "wa": 20.69e6, "rho": 6.31e6, "poisson": 15.87e6,
+                          "assemble": 44.38e6,
+                          "source": "profiles/mgp_211k_bf16x3_kernels.md"},
+}
+
+
+def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision, traffic=None):
     """Algorithmic bytes (or flops) of each iteration part per launch, divided by its
-    warm-L2 device time. Bytes count every array the part must touch once (FP32/int32):
-      update     80 B per optimised node (u, v, g, clamp box, index, hw/hh/weight in; v', u',
-                 x, y out) + 16 B per bin (the two fixed-point maps it scatters into)
+    warm-L2 device time. Bytes count every array the part must touch once (FP32/int32);
+    fillers share their attributes as launch constants, so only cells read per-node ones:
+      update     48 B per optimised node (u, v, g in; v', u' out; x, y into the node arrays)
+                 + 52 B per cell (meta, geometry, clamp box, node index) + 16 B per bin (the
+                 two fixed-point maps it scatters into)
       wa         32 B per pin + 8 B per net (pin ids, offsets, positions in; 2 terms out)
       scatter    25 B per density node outside the opt set + 16 B per bin (only FILLERONLY
                  and cGP have such nodes)
       rho        44 B per bin (maps, terminal, base in; rho out; maps cleared)
       poisson    14 M^3 flops (16 B per bin of I/O)
-      assemble   76 B per optimised node + 16 B per pin (WA pass 2, gather, gradient, and
-                 the step's norms over uPrev and gPrevTmp)
+      assemble   32 B per optimised node (u, uPrev, gPrevTmp in; g out) + 40 B per cell
+                 (meta, geometry, area) + 8 B per pin (the WA pass-1 terms) + 8 B per bin
+                 (the field maps it gathers from)
+    traffic: measured DRAM bytes per launch by part (PROFILED_DRAM_BYTES), when known.
     """
     n_opt = db.num_movable + db.num_fillers
+    cells = db.num_movable
     n_dens = n_opt
     pins, nets, bins = db.num_pins, db.num_nets, dim * dim
-    by = {"update": 80 * n_opt + 16 * bins, "wa": 32 * pins + 8 * nets, "scatter": 25 * n_dens + 16 * bins,
-          "rho": 44 * bins, "assemble": 76 * n_opt + 16 * pins}
+    by = {"update": 48 * n_opt + 52 * cells + 16 * bins, "wa": 32 * pins + 8 * nets,
+          "scatter": 25 * n_dens + 16 * bins, "rho": 44 * bins,
+          "assemble": 32 * n_opt + 40 * cells + 8 * pins + 8 * bins}
+    traffic = traffic or {}
     out = {}
     for k, us in parts.items():
         if k == "poisson":
@@ -219,6 +237,7 @@ def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision):
                       "frac": ach / hbm_gbs, "bytes": by[k]}
         else:
             out[k] = {"us": us}
+        out[k]["traffic"] = traffic.get(k)
     return out
 
 
@@ -310,7 +329,8 @@ def run_ours(args):
         dim = info["dim"]
         hbm, bf16, peak_kind = peaks()
         parts = ep.ctx.profile(reps=20)
-        kern = part_rooflines(parts, db, dim, hbm, bf16, precision)
+        traffic = PROFILED_DRAM_BYTES.get((args.workload, args.precision), {})
+        kern = part_rooflines(parts, db, dim, hbm, bf16, precision, traffic)
         dom = max((k for k in kern if k != "evaluation"), key=lambda k: kern[k]["us"])
         d = kern[dom]
         total = db.total_nodes
@@ -337,7 +357,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": {"bound": d["bound"], "achieved": d["achieved"], "peak": d["peak"],
-                         "unit": d["unit"], "frac": d["frac"], "traffic": None,
+                         "unit": d["unit"], "frac": d["frac"], "traffic": d["traffic"],
+                         "traffic_source": traffic.get("source"),
                          "kernel": dom, "us_per_launch": d["us"], "peak_kind": peak_kind},
             "kernels": kern,
             "clocks": clk.summary(),

@@ -319,7 +319,9 @@ struct Context : ContextStreams {
     DevBuf<uint8_t> kind;
     DevBuf<float> pox, poy, gpx, gpy;
     DevBuf<int> pin2node, pin2net, net_start, net_pins, node_start_d, node_pins, net_order;
-    DevBuf<int> slot_start, net_slot;
+    DevBuf<int> slot_start, net_slot, wa_start;
+    DevBuf<int2> wa_node_slot;
+    DevBuf<float2> wa_off;
     WaClasses wa_classes{};
     // grid
     bool grid_ready = false;
@@ -410,6 +412,9 @@ struct Context : ContextStreams {
         p.gpy = gpy.p;
         p.slot_start = slot_start.p;
         p.net_slot = net_slot.p;
+        p.wa_start = wa_start.p;
+        p.wa_node_slot = wa_node_slot.p;
+        p.wa_off = wa_off.p;
         p.geom = geom;
         p.node_fix = node_fix.p;
         p.filler_fix = filler_fix.p;
@@ -1321,9 +1326,10 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
     c.net_pins.upload(v->flat_net2pin, c.num_pins, s);
     c.node_start_d.upload(v->node2pin_start, T + 1, s);
     c.node_pins.upload(v->flat_node2pin, c.num_pins, s);
-    // nets in ascending degree (stable), cut into degree classes: a net of degree d is
-    // owned by a lane group of the next power of two >= d (2..32 lanes), nets above 32
-    // pins by a whole warp that loops over its pins (wirelength.cu)
+    // nets in ascending degree (stable), cut into degree classes: a net of degree d <=
+    // kWaThreadNetDegree is owned by one thread, a larger one by a lane group of the next
+    // power of two >= d (up to 32 lanes), nets above 32 pins by a whole warp that loops over
+    // its pins (wirelength.cu)
     std::vector<int> order(c.num_nets);
     std::iota(order.begin(), order.end(), 0);
     auto deg = [&](int k) { return v->net2pin_start[k + 1] - v->net2pin_start[k]; };
@@ -1332,19 +1338,25 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
     {
         WaClasses& wc = c.wa_classes;
         wc = WaClasses{};
-        const int limits[6] = {2, 4, 8, 16, 32, 1 << 30};
-        const int groups[6] = {2, 4, 8, 16, 32, 0};
+        int thread_deg = kWaThreadNetDegree;
+        if (const char* e = std::getenv("SPG_WA_THREAD_DEGREE")) thread_deg = std::atoi(e);
+        SPG_REQUIRE(thread_deg >= 0 && thread_deg <= kWaThreadNetDegree, SPG_E_INVALID,
+                    "SPG_WA_THREAD_DEGREE out of range");
+        const int limits[7] = {thread_deg, 2, 4, 8, 16, 32, 1 << 30};
+        const int groups[7] = {1, 2, 4, 8, 16, 32, 0};
         int t = 0, warps = 0;
-        for (int cl = 0; cl < 6; ++cl) {
+        for (int cl = 0; cl < 7; ++cl) {
             const int begin = t;
             while (t < c.num_nets && deg(order[t]) <= limits[cl]) ++t;
             if (t == begin) continue;
             const int i = wc.n++;
-            wc.group[i] = groups[cl];
+            const int g = groups[cl];
+            wc.group[i] = g;
+            wc.shift[i] = g > 0 ? __builtin_ctz(g) : 0;
             wc.net_begin[i] = begin;
             wc.net_end[i] = t;
             wc.warp_begin[i] = warps;
-            warps += groups[cl] ? ceil_div(t - begin, 32 / groups[cl]) : (t - begin);
+            warps += g ? ceil_div(t - begin, 32 / g) : (t - begin);
         }
         wc.warp_begin[wc.n] = warps;
     }
@@ -1373,6 +1385,24 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
         c.slot_start_h = slot_start;
         c.net_slot.upload(net_slot, s);
         c.num_slots = slots;
+        // the WA pass-1 copy of each pin's data, in the degree-sorted net order
+        std::vector<int> wa_start(c.num_nets + 1);
+        std::vector<int2> node_slot(c.num_pins);
+        std::vector<float2> off(c.num_pins);
+        int q = 0;
+        for (int t = 0; t < c.num_nets; ++t) {
+            const int k = order[t];
+            wa_start[t] = q;
+            for (int e = v->net2pin_start[k]; e < v->net2pin_start[k + 1]; ++e, ++q) {
+                const int pin = v->flat_net2pin[e];
+                node_slot[q] = make_int2(v->pin2node[pin], net_slot[e]);
+                off[q] = make_float2(v->pin_offset_x[pin], v->pin_offset_y[pin]);
+            }
+        }
+        wa_start[c.num_nets] = q;
+        c.wa_start.upload(wa_start, s);
+        c.wa_node_slot.upload(node_slot, s);
+        c.wa_off.upload(off, s);
     }
     c.gpx.alloc(c.num_slots + 1);
     c.gpy.alloc(c.num_slots + 1);

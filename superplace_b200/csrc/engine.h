@@ -114,12 +114,17 @@ struct DevState {
     unsigned long long t0_ns;
 };
 
+// Nets of at most this degree get one thread each in WA pass 1 (SPG_WA_THREAD_DEGREE
+// lowers it; 0 gives every net a lane group).
+constexpr int kWaThreadNetDegree = 4;
+
 // Degree classes of the WA kernel over the degree-sorted net order: class i owns nets
 // net_order[net_begin[i] .. net_end[i]) with `group[i]` lanes per net (0: one looping warp
 // per net) and warps [warp_begin[i], warp_begin[i+1]).
 struct WaClasses {
     int n;
-    int group[8];
+    int group[8];  // lanes per net: 1 (one thread per net), 2..32 (a lane group), 0 (a whole warp)
+    int shift[8];  // log2(group[c]) for the lane-group classes
     int net_begin[8], net_end[8];
     int warp_begin[9];
 };
@@ -136,6 +141,12 @@ struct DevPtrs {
     const int *node_start, *node_pins;
     const int* net_order;  // nets sorted by degree (ascending)
     WaClasses wa;
+    // WA pass 1 pin data in the degree-sorted net order: the pins of net net_order[t] are
+    // entries [wa_start[t], wa_start[t+1]) in net-CSR order, each with its node and gradient
+    // slot (wa_node_slot) and its pin offset (wa_off)
+    const int* wa_start;
+    const int2* wa_node_slot;
+    const float2* wa_off;
     // per-pin WA gradient contributions (x, y), stored in node order: the pins of node i
     // that belong to a net own slots [slot_start[i], slot_start[i+1]) in node->pin order;
     // net_slot[q] is the slot of net-CSR entry q

@@ -1,9 +1,11 @@
 // Weighted-average wirelength, its gradient, and HPWL on sm_100a
 // (WaWirelength::compute, src/gp/wa_wirelength.cpp:46-180; computeHPWL, src/db/hpwl.cpp:13-39).
 //
-// Pass 1 gives each net a group of lanes sized to its degree (nets sorted by degree and
-// cut into classes of 2, 4, 8, 16, 32 lanes, or a whole looping warp above 32 pins), so
-// a warp's lanes stay converged and the pin loads of a net are issued together. Per net it
+// Pass 1 sorts nets by degree and cuts them into classes: a net of at most
+// kWaThreadNetDegree pins is owned by one thread (its pins in registers, its sums in the
+// reference's pin order), a larger one by a group of 8, 16 or 32 lanes, and a net above 32
+// pins by a whole warp that loops over its pins. A warp's lanes stay converged and the pin
+// loads of a net are issued together. Per net it
 // forms the extrema, the shifted exponentials a+- = exp(+-(x - x_ext)/gamma), b+- and the
 // centred c'+- sums (wa_wirelength.cpp:73-127), the WA value and the HPWL term, and every
 // lane writes its pin's gradient contribution termMax - termMin (wa_wirelength.cpp:192-221)
@@ -69,10 +71,14 @@ __device__ __forceinline__ float group_sum(float v, int G) {
     return v;
 }
 
-__device__ __forceinline__ void pin_xy(const DevPtrs& p, int pin, float& px, float& py) {
-    const int nd = __ldg(p.pin2node + pin);
-    px = fadd(__ldg(p.x + nd), __ldg(p.pox + pin));
-    py = fadd(__ldg(p.y + nd), __ldg(p.poy + pin));
+// Position and gradient slot of entry q of the sorted WA pin order (pinX/pinY: node position
+// plus pin offset).
+__device__ __forceinline__ void wa_pin(const DevPtrs& p, int q, float& px, float& py, int& slot) {
+    const int2 ns = __ldg(p.wa_node_slot + q);
+    const float2 o = __ldg(p.wa_off + q);
+    px = fadd(__ldg(p.x + ns.x), o.x);
+    py = fadd(__ldg(p.y + ns.x), o.y);
+    slot = ns.y;
 }
 
 // WA value of one net from its extrema and sums (wa_wirelength.cpp:122-126).
@@ -82,14 +88,16 @@ __device__ __forceinline__ double wa_value(float mxX, float mnX, float mxY, floa
            static_cast<double>(fsub(fadd(fsub(mxY, mnY), fdiv(s[5], s[4])), fdiv(s[7], s[6])));
 }
 
-// One net of more than 32 pins, owned by a whole warp that loops over its pins.
-__device__ void wa_warp_net(const DevPtrs& p, int k, float invG, double& wl, double& hp) {
+// One net of more than 32 pins (sorted position t), owned by a whole warp that loops over
+// its pins.
+__device__ void wa_warp_net(const DevPtrs& p, int t, float invG, double& wl, double& hp) {
     const int lane = threadIdx.x & 31;
-    const int b = p.net_start[k], e = p.net_start[k + 1];
+    const int b = p.wa_start[t], e = p.wa_start[t + 1];
     float mxX = -FLT_MAX, mnX = FLT_MAX, mxY = -FLT_MAX, mnY = FLT_MAX;
     for (int q = b + lane; q < e; q += 32) {
         float px, py;
-        pin_xy(p, p.net_pins[q], px, py);
+        int sl;
+        wa_pin(p, q, px, py, sl);
         mxX = fmax_(mxX, px);
         mnX = fmin_(mnX, px);
         mxY = fmax_(mxY, py);
@@ -102,15 +110,17 @@ __device__ void wa_warp_net(const DevPtrs& p, int k, float invG, double& wl, dou
     if (lane == 0) hp += static_cast<double>(fsub(mxX, mnX)) + static_cast<double>(fsub(mxY, mnY));
     if (e - b > p.ignore_net_degree) {
         for (int q = b + lane; q < e; q += 32) {
-            p.gpx[p.net_slot[q]] = 0.f;
-            p.gpy[p.net_slot[q]] = 0.f;
+            const int sl = __ldg(p.wa_node_slot + q).y;
+            p.gpx[sl] = 0.f;
+            p.gpy[sl] = 0.f;
         }
         return;
     }
     float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (int q = b + lane; q < e; q += 32) {
         float px, py;
-        pin_xy(p, p.net_pins[q], px, py);
+        int sl;
+        wa_pin(p, q, px, py, sl);
         const float dxp = fsub(px, mxX), dxn = fsub(px, mnX), dyp = fsub(py, mxY), dyn = fsub(py, mnY);
         const float ap = expf(fmul(dxp, invG)), an = expf(fmul(-dxn, invG));
         const float bp = expf(fmul(dyp, invG)), bn = expf(fmul(-dyn, invG));
@@ -128,22 +138,95 @@ __device__ void wa_warp_net(const DevPtrs& p, int k, float invG, double& wl, dou
     if (lane == 0) wl += wa_value(mxX, mnX, mxY, mnY, s);
     for (int q = b + lane; q < e; q += 32) {
         float px, py;
-        pin_xy(p, p.net_pins[q], px, py);
+        int sl;
+        wa_pin(p, q, px, py, sl);
         const float dxp = fsub(px, mxX), dxn = fsub(px, mnX), dyp = fsub(py, mxY), dyn = fsub(py, mnY);
         const float ap = expf(fmul(dxp, invG)), an = expf(fmul(-dxn, invG));
         const float bp = expf(fmul(dyp, invG)), bn = expf(fmul(-dyn, invG));
-        const int sl = p.net_slot[q];
         p.gpx[sl] = wa_pin_term(dxp, dxn, ap, an, s[0], s[2], s[1], s[3], invG);
         p.gpy[sl] = wa_pin_term(dyp, dyn, bp, bn, s[4], s[6], s[5], s[7], invG);
     }
 }
 
-// Pass 1 of the WA model and HPWL. Nets of degree <= 32 are owned by aligned groups of
-// G = 2..32 lanes (G >= degree), one pin per lane: extrema, exponentials and the b+-/c'+-
-// sums are group butterflies, and every lane writes its own pin's gradient term. The sums
-// are formed in butterfly order rather than the reference's pin order, so values differ
-// from the reference's sequential float sums in the last bits only.
-__global__ void __launch_bounds__(RED_THREADS) wa_net_kernel(DevPtrs p, const float* gamma_dev,
+// One net of D pins (2 <= D <= kWaThreadNetDegree), owned by one thread: the extrema, the
+// exponentials and the sums in pin order, as wa_wirelength.cpp:84-127 forms them, then the
+// pins' gradient terms.
+template <int D>
+__device__ __forceinline__ void wa_thread_net(const DevPtrs& p, int b, float invG, double& wl, double& hp) {
+    float px[D], py[D];
+    int sl[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) wa_pin(p, b + j, px[j], py[j], sl[j]);
+    float mxX = -FLT_MAX, mnX = FLT_MAX, mxY = -FLT_MAX, mnY = FLT_MAX;
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        mxX = fmax_(mxX, px[j]);
+        mnX = fmin_(mnX, px[j]);
+        mxY = fmax_(mxY, py[j]);
+        mnY = fmin_(mnY, py[j]);
+    }
+    hp += static_cast<double>(fsub(mxX, mnX)) + static_cast<double>(fsub(mxY, mnY));
+    if (D > p.ignore_net_degree) {
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+            p.gpx[sl[j]] = 0.f;
+            p.gpy[sl[j]] = 0.f;
+        }
+        return;
+    }
+    float ap[D], an[D], bp[D], bn[D];
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        const float dxp = fsub(px[j], mxX), dxn = fsub(px[j], mnX);
+        const float dyp = fsub(py[j], mxY), dyn = fsub(py[j], mnY);
+        ap[j] = expf(fmul(dxp, invG));
+        an[j] = expf(fmul(-dxn, invG));
+        bp[j] = expf(fmul(dyp, invG));
+        bn[j] = expf(fmul(-dyn, invG));
+        s[0] = fadd(s[0], ap[j]);
+        s[1] = fadd(s[1], fmul(dxp, ap[j]));
+        s[2] = fadd(s[2], an[j]);
+        s[3] = fadd(s[3], fmul(dxn, an[j]));
+        s[4] = fadd(s[4], bp[j]);
+        s[5] = fadd(s[5], fmul(dyp, bp[j]));
+        s[6] = fadd(s[6], bn[j]);
+        s[7] = fadd(s[7], fmul(dyn, bn[j]));
+    }
+    wl += wa_value(mxX, mnX, mxY, mnY, s);
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        p.gpx[sl[j]] = wa_pin_term(fsub(px[j], mxX), fsub(px[j], mnX), ap[j], an[j], s[0], s[2], s[1], s[3], invG);
+        p.gpy[sl[j]] = wa_pin_term(fsub(py[j], mxY), fsub(py[j], mnY), bp[j], bn[j], s[4], s[6], s[5], s[7], invG);
+    }
+}
+
+// The net at sorted position t, of degree 0..kWaThreadNetDegree, in the one-thread class.
+// Degree 0 and 1 nets have no WA term and no HPWL; a 1-pin net's gradient slot is written 0.
+__device__ __forceinline__ void wa_thread_class_net(const DevPtrs& p, int t, float invG, double& wl, double& hp) {
+    const int b = p.wa_start[t];
+    switch (p.wa_start[t + 1] - b) {
+        case 1: {
+            const int sl = __ldg(p.wa_node_slot + b).y;
+            p.gpx[sl] = 0.f;
+            p.gpy[sl] = 0.f;
+            break;
+        }
+        case 2: wa_thread_net<2>(p, b, invG, wl, hp); break;
+        case 3: wa_thread_net<3>(p, b, invG, wl, hp); break;
+        case 4: wa_thread_net<4>(p, b, invG, wl, hp); break;
+        default: break;
+    }
+}
+static_assert(kWaThreadNetDegree == 4, "wa_thread_class_net covers degrees up to 4");
+
+// Pass 1 of the WA model and HPWL. Nets of the one-thread class are formed in pin order
+// (wa_thread_net). Other nets of degree <= 32 are owned by aligned groups of G = 2..32 lanes
+// (G >= degree), one pin per lane: extrema, exponentials and the b+-/c'+- sums are group
+// butterflies, and every lane writes its own pin's gradient term. Those sums are formed in
+// butterfly order rather than the reference's pin order, so values differ from the
+// reference's sequential float sums in the last bits only.
+__global__ void __launch_bounds__(RED_THREADS, 4) wa_net_kernel(DevPtrs p, const float* gamma_dev,
                                                              float gamma_host, int use_dev) {
     pdl_wait();
     pdl_trigger();
@@ -155,25 +238,29 @@ __global__ void __launch_bounds__(RED_THREADS) wa_net_kernel(DevPtrs p, const fl
     const int warps_total = p.wa.warp_begin[p.wa.n];
     const int wstride = gridDim.x * (blockDim.x >> 5);
     double wl = 0.0, hp = 0.0;
+    int c = 0;  // the class of warp w (w only grows)
     for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < warps_total; w += wstride) {
-        int c = 0;
         while (c + 1 < p.wa.n && w >= p.wa.warp_begin[c + 1]) ++c;
         const int G = p.wa.group[c];
         if (G == 0) {
-            wa_warp_net(p, p.net_order[p.wa.net_begin[c] + (w - p.wa.warp_begin[c])], invG, wl, hp);
+            wa_warp_net(p, p.wa.net_begin[c] + (w - p.wa.warp_begin[c]), invG, wl, hp);
             continue;
         }
-        const int gi = lane / G, gl = lane % G;
-        const int t = p.wa.net_begin[c] + (w - p.wa.warp_begin[c]) * (32 / G) + gi;
+        if (G == 1) {
+            const int t = p.wa.net_begin[c] + (w - p.wa.warp_begin[c]) * 32 + lane;
+            if (t < p.wa.net_end[c]) wa_thread_class_net(p, t, invG, wl, hp);
+            continue;
+        }
+        const int sh = p.wa.shift[c];
+        const int gi = lane >> sh, gl = lane & (G - 1);
+        const int t = p.wa.net_begin[c] + ((w - p.wa.warp_begin[c]) << (5 - sh)) + gi;
         const bool net_ok = t < p.wa.net_end[c];
-        const int k = net_ok ? p.net_order[t] : 0;
-        const int b = net_ok ? p.net_start[k] : 0;
-        const int deg = net_ok ? p.net_start[k + 1] - b : 0;
+        const int b = net_ok ? p.wa_start[t] : 0;
+        const int deg = net_ok ? p.wa_start[t + 1] - b : 0;
         const bool act = gl < deg;
-        const int pin = act ? p.net_pins[b + gl] : 0;
-        const int sl = act ? p.net_slot[b + gl] : 0;
         float px = 0.f, py = 0.f;
-        if (act) pin_xy(p, pin, px, py);
+        int sl = 0;
+        if (act) wa_pin(p, b + gl, px, py, sl);
         const float mxX = group_max(act ? px : -FLT_MAX, G), mnX = group_min(act ? px : FLT_MAX, G);
         const float mxY = group_max(act ? py : -FLT_MAX, G), mnY = group_min(act ? py : FLT_MAX, G);
         if (gl == 0 && deg >= 2)  // computeHPWL counts every net of degree >= 2 (hpwl.cpp:18-32)
