@@ -407,7 +407,6 @@ struct Context : ContextStreams {
         p.node_start = node_start_d.p;
         p.node_pins = node_pins.p;
         p.net_order = net_order.p;
-        p.wa = wa_classes;
         p.gpx = gpx.p;
         p.gpy = gpy.p;
         p.slot_start = slot_start.p;
@@ -809,11 +808,11 @@ void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int cou
         return e && e[0] == '1';
     }();
     if (wa_serial) {
-        launch_wa_nets(p, &p.st->gamma, 0.f, 1, s);
+        launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s);
     } else {
         SPG_CUDA(cudaEventRecord(c.ev_fork, s));
         SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
-        launch_wa_nets(p, &p.st->gamma, 0.f, 1, c.side);
+        launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, c.side);
         SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
     }
     if (stepped) launch_density_rest(p, s);
@@ -914,7 +913,7 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
     launch_scatter(p, R_POS, s);
     launch_density_accumulate(p, s);
     launch_rho_overflow(p, 0, 1, s);
-    launch_wa_nets(p, &p.st->gamma, 0.f, 1, s);
+    launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s);
     final_metrics_kernel<<<1, 256, 0, s>>>(p, c.scratch_d.p);
     count_launch();
     SPG_CHECK_LAUNCH();
@@ -1326,10 +1325,10 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
     c.net_pins.upload(v->flat_net2pin, c.num_pins, s);
     c.node_start_d.upload(v->node2pin_start, T + 1, s);
     c.node_pins.upload(v->flat_node2pin, c.num_pins, s);
-    // nets in ascending degree (stable), cut into degree classes: a net of degree d <=
-    // kWaThreadNetDegree is owned by one thread, a larger one by a lane group of the next
-    // power of two >= d (up to 32 lanes), nets above 32 pins by a whole warp that loops over
-    // its pins (wirelength.cu)
+    // nets in ascending degree (stable), cut into classes of one degree each: a net of degree
+    // d <= kWaThreadNetDegree is owned by one thread, a larger one by a lane group of the next
+    // power of two >= d, and the nets above 32 pins by one warp each that loops over its pins
+    // (wirelength.cu)
     std::vector<int> order(c.num_nets);
     std::iota(order.begin(), order.end(), 0);
     auto deg = [&](int k) { return v->net2pin_start[k + 1] - v->net2pin_start[k]; };
@@ -1342,21 +1341,35 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
         if (const char* e = std::getenv("SPG_WA_THREAD_DEGREE")) thread_deg = std::atoi(e);
         SPG_REQUIRE(thread_deg >= 0 && thread_deg <= kWaThreadNetDegree, SPG_E_INVALID,
                     "SPG_WA_THREAD_DEGREE out of range");
-        const int limits[7] = {thread_deg, 2, 4, 8, 16, 32, 1 << 30};
-        const int groups[7] = {1, 2, 4, 8, 16, 32, 0};
-        int t = 0, warps = 0;
-        for (int cl = 0; cl < 7; ++cl) {
-            const int begin = t;
-            while (t < c.num_nets && deg(order[t]) <= limits[cl]) ++t;
-            if (t == begin) continue;
+        int warps = 0, pins = 0;
+        auto add = [&](int g, int d, int begin, int end) {
+            SPG_REQUIRE(wc.n < WA_MAX_CLASSES, SPG_E_INVALID, "too many WA degree classes");
             const int i = wc.n++;
-            const int g = groups[cl];
             wc.group[i] = g;
             wc.shift[i] = g > 0 ? __builtin_ctz(g) : 0;
+            wc.deg[i] = d;
             wc.net_begin[i] = begin;
-            wc.net_end[i] = t;
+            wc.net_end[i] = end;
+            wc.pin_begin[i] = pins;
             wc.warp_begin[i] = warps;
-            warps += g ? ceil_div(t - begin, 32 / g) : (t - begin);
+            warps += g ? ceil_div(end - begin, 32 / g) : (end - begin);
+        };
+        for (int t = 0; t < c.num_nets;) {
+            const int d = deg(order[t]);
+            if (d > 32) {  // the sorted tail: every remaining net is above 32 pins
+                add(0, -1, t, c.num_nets);
+                break;
+            }
+            int e = t;
+            while (e < c.num_nets && deg(order[e]) == d) ++e;
+            if (d > 0) {
+                int g = 1;
+                if (d > thread_deg)
+                    while (g < d || g < 2) g <<= 1;
+                add(g, d, t, e);
+            }
+            pins += d * (e - t);
+            t = e;
         }
         wc.warp_begin[wc.n] = warps;
     }
@@ -1834,7 +1847,7 @@ int spg_wa_wirelength(spg_ctx* ctx, float gamma, int ignore, double* wl, float* 
         c.partials.zero(c.stream);
         p.partials = c.partials.p;
     }
-    spg::launch_wa_nets(p, nullptr, gamma, 0, c.stream);
+    spg::launch_wa_nets(p, c.wa_classes, nullptr, gamma, 0, c.stream);
     spg::DevBuf<float> g;
     g.alloc(2 * static_cast<size_t>(std::max(c.num_movable, 1)));
     spg::launch_wa_node_grad(p, g.p, c.stream);
@@ -1860,7 +1873,7 @@ int spg_hpwl(spg_ctx* ctx, double* hpwl) {
         c.partials.zero(c.stream);
         p.partials = c.partials.p;
     }
-    spg::launch_wa_nets(p, nullptr, 1.f, 0, c.stream);
+    spg::launch_wa_nets(p, c.wa_classes, nullptr, 1.f, 0, c.stream);
     spg::launch_finalize_slots(p, spg::SLOT_HPWL, 1, c.scratch_d.p, c.stream);
     SPG_CUDA(cudaMemcpyAsync(hpwl, c.scratch_d.p, 8, cudaMemcpyDeviceToHost, c.stream));
     SPG_CUDA(spg::host_wait(c.stream));
@@ -1952,7 +1965,7 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     t[0] = time([&] { spg::launch_update(p, s); }, zero_maps);
     set_state(probe);
     spg::launch_scatter(p, spg::R_POS, s);  // the delivered positions again
-    t[1] = time([&] { spg::launch_wa_nets(p, &p.st->gamma, 0.f, 1, s); }, nothing);
+    t[1] = time([&] { spg::launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s); }, nothing);
     t[2] = (c.n_rest_small + c.n_rest_large) > 0 ? time([&] { spg::launch_density_rest(p, s); }, zero_maps) : 0.0;
     t[3] = time([&] { spg::launch_rho_overflow(p, 0, 1, s); }, [&] { spg::launch_density_accumulate(p, s); });
     t[4] = time([&] { spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s); }, nothing);

@@ -116,17 +116,23 @@ struct DevState {
 
 // Nets of at most this degree get one thread each in WA pass 1 (SPG_WA_THREAD_DEGREE
 // lowers it; 0 gives every net a lane group).
-constexpr int kWaThreadNetDegree = 4;
+constexpr int kWaThreadNetDegree = 5;
 
-// Degree classes of the WA kernel over the degree-sorted net order: class i owns nets
-// net_order[net_begin[i] .. net_end[i]) with `group[i]` lanes per net (0: one looping warp
-// per net) and warps [warp_begin[i], warp_begin[i+1]).
+// Degree classes of the WA kernel over the degree-sorted net order. Class i owns the nets at
+// sorted positions [net_begin[i], net_end[i]), all of degree deg[i] (the last class, of the
+// nets above 32 pins, has mixed degrees: deg -1), whose pins start at entry pin_begin[i] of
+// the sorted pin order, with group[i] lanes per net (1: one thread; 2..32: a lane group,
+// shift = log2 of it; 0: one warp that loops over the pins) and warps
+// [warp_begin[i], warp_begin[i+1]). Passed by value to the WA kernel only.
+constexpr int WA_MAX_CLASSES = 40;
 struct WaClasses {
     int n;
-    int group[8];  // lanes per net: 1 (one thread per net), 2..32 (a lane group), 0 (a whole warp)
-    int shift[8];  // log2(group[c]) for the lane-group classes
-    int net_begin[8], net_end[8];
-    int warp_begin[9];
+    int group[WA_MAX_CLASSES];
+    int shift[WA_MAX_CLASSES];
+    int deg[WA_MAX_CLASSES];
+    int net_begin[WA_MAX_CLASSES], net_end[WA_MAX_CLASSES];
+    int pin_begin[WA_MAX_CLASSES];
+    int warp_begin[WA_MAX_CLASSES + 1];
 };
 
 // Everything a kernel needs to address the device data, passed by value.
@@ -140,7 +146,6 @@ struct DevPtrs {
     const int *net_start, *net_pins;
     const int *node_start, *node_pins;
     const int* net_order;  // nets sorted by degree (ascending)
-    WaClasses wa;
     // WA pass 1 pin data in the degree-sorted net order: the pins of net net_order[t] are
     // entries [wa_start[t], wa_start[t+1]) in net-CSR order, each with its node and gradient
     // slot (wa_node_slot) and its pin offset (wa_off)
@@ -243,7 +248,7 @@ void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s);
 void launch_gather_all(const DevPtrs& p, float* force_nodes, cudaStream_t s);
 
 // ---- wirelength.cu
-void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, int use_dev_gamma,
+void launch_wa_nets(const DevPtrs& p, const WaClasses& wa, const float* gamma_dev, float gamma_host, int use_dev_gamma,
                     cudaStream_t s);
 // node-indexed WA gradient for movable nodes (parity hook)
 void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s);

@@ -201,11 +201,11 @@ __device__ __forceinline__ void wa_thread_net(const DevPtrs& p, int b, float inv
     }
 }
 
-// The net at sorted position t, of degree 0..kWaThreadNetDegree, in the one-thread class.
-// Degree 0 and 1 nets have no WA term and no HPWL; a 1-pin net's gradient slot is written 0.
-__device__ __forceinline__ void wa_thread_class_net(const DevPtrs& p, int t, float invG, double& wl, double& hp) {
-    const int b = p.wa_start[t];
-    switch (p.wa_start[t + 1] - b) {
+// A net of degree D (1..kWaThreadNetDegree, the same for the whole warp) whose pins start at
+// entry b of the sorted pin order, in the one-thread class. A 1-pin net has no WA term and
+// no HPWL; its gradient slot is written 0.
+__device__ __forceinline__ void wa_thread_class_net(const DevPtrs& p, int D, int b, float invG, double& wl, double& hp) {
+    switch (D) {
         case 1: {
             const int sl = __ldg(p.wa_node_slot + b).y;
             p.gpx[sl] = 0.f;
@@ -215,10 +215,11 @@ __device__ __forceinline__ void wa_thread_class_net(const DevPtrs& p, int t, flo
         case 2: wa_thread_net<2>(p, b, invG, wl, hp); break;
         case 3: wa_thread_net<3>(p, b, invG, wl, hp); break;
         case 4: wa_thread_net<4>(p, b, invG, wl, hp); break;
+        case 5: wa_thread_net<5>(p, b, invG, wl, hp); break;
         default: break;
     }
 }
-static_assert(kWaThreadNetDegree == 4, "wa_thread_class_net covers degrees up to 4");
+static_assert(kWaThreadNetDegree == 5, "wa_thread_class_net covers degrees up to 5");
 
 // Pass 1 of the WA model and HPWL. Nets of the one-thread class are formed in pin order
 // (wa_thread_net). Other nets of degree <= 32 are owned by aligned groups of G = 2..32 lanes
@@ -226,8 +227,8 @@ static_assert(kWaThreadNetDegree == 4, "wa_thread_class_net covers degrees up to
 // butterflies, and every lane writes its own pin's gradient term. Those sums are formed in
 // butterfly order rather than the reference's pin order, so values differ from the
 // reference's sequential float sums in the last bits only.
-__global__ void __launch_bounds__(RED_THREADS, 4) wa_net_kernel(DevPtrs p, const float* gamma_dev,
-                                                             float gamma_host, int use_dev) {
+__global__ void __launch_bounds__(RED_THREADS, 4) wa_net_kernel(DevPtrs p, WaClasses wa, const float* gamma_dev,
+                                                                float gamma_host, int use_dev) {
     pdl_wait();
     pdl_trigger();
     __shared__ double ws[32];
@@ -235,28 +236,28 @@ __global__ void __launch_bounds__(RED_THREADS, 4) wa_net_kernel(DevPtrs p, const
     const float g = fmax_(gam, 1e-4f);  // kMinGamma, wa_wirelength.cpp:14
     const float invG = fdiv(1.0f, g);
     const int lane = threadIdx.x & 31;
-    const int warps_total = p.wa.warp_begin[p.wa.n];
+    const int warps_total = wa.warp_begin[wa.n];
     const int wstride = gridDim.x * (blockDim.x >> 5);
     double wl = 0.0, hp = 0.0;
     int c = 0;  // the class of warp w (w only grows)
     for (int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < warps_total; w += wstride) {
-        while (c + 1 < p.wa.n && w >= p.wa.warp_begin[c + 1]) ++c;
-        const int G = p.wa.group[c];
+        while (c + 1 < wa.n && w >= wa.warp_begin[c + 1]) ++c;
+        const int G = wa.group[c], D = wa.deg[c];
+        const int wi = w - wa.warp_begin[c];
         if (G == 0) {
-            wa_warp_net(p, p.wa.net_begin[c] + (w - p.wa.warp_begin[c]), invG, wl, hp);
+            wa_warp_net(p, wa.net_begin[c] + wi, invG, wl, hp);
             continue;
         }
         if (G == 1) {
-            const int t = p.wa.net_begin[c] + (w - p.wa.warp_begin[c]) * 32 + lane;
-            if (t < p.wa.net_end[c]) wa_thread_class_net(p, t, invG, wl, hp);
+            const int i = wi * 32 + lane;
+            if (wa.net_begin[c] + i < wa.net_end[c]) wa_thread_class_net(p, D, wa.pin_begin[c] + i * D, invG, wl, hp);
             continue;
         }
-        const int sh = p.wa.shift[c];
+        const int sh = wa.shift[c];
         const int gi = lane >> sh, gl = lane & (G - 1);
-        const int t = p.wa.net_begin[c] + ((w - p.wa.warp_begin[c]) << (5 - sh)) + gi;
-        const bool net_ok = t < p.wa.net_end[c];
-        const int b = net_ok ? p.wa_start[t] : 0;
-        const int deg = net_ok ? p.wa_start[t + 1] - b : 0;
+        const int i = (wi << (5 - sh)) + gi;
+        const int deg = wa.net_begin[c] + i < wa.net_end[c] ? D : 0;
+        const int b = wa.pin_begin[c] + i * D;
         const bool act = gl < deg;
         float px = 0.f, py = 0.f;
         int sl = 0;
@@ -302,7 +303,7 @@ __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
 
 }  // namespace
 
-void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, int use_dev,
+void launch_wa_nets(const DevPtrs& p, const WaClasses& wa, const float* gamma_dev, float gamma_host, int use_dev,
                     cudaStream_t s) {
     // A fixed grid per device, so the FP64 partials keep a fixed owner per block. WA runs
     // beside the scatter -> rho -> Poisson chain; at most kWaBlocksPerSm blocks per SM leave
@@ -313,9 +314,9 @@ void launch_wa_nets(const DevPtrs& p, const float* gamma_dev, float gamma_host, 
     SPG_CUDA(cudaGetDevice(&dev));
     SPG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // one warp per lane group of nets: the grid the work fills, at most one wave
-    const int full = work_grid(reinterpret_cast<const void*>(wa_net_kernel), p.wa.warp_begin[p.wa.n], RED_THREADS / 32);
+    const int full = work_grid(reinterpret_cast<const void*>(wa_net_kernel), wa.warp_begin[wa.n], RED_THREADS / 32);
     const int grid = per_sm > 0 ? std::min(full, std::min(per_sm * sms, RED_CAP)) : full;
-    launch_prio(false, wa_net_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, gamma_dev, gamma_host, use_dev);
+    launch_prio(false, wa_net_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, wa, gamma_dev, gamma_host, use_dev);
 }
 
 void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s) {
