@@ -546,7 +546,11 @@ def run_serve(args):
             ours = serving.summarize(res)
             ours["peak_running"] = srv.peak_running
             slow = np.array([r.latency / alone[i] for r, i in zip(res, idx)])
+            solo = np.array([alone[i] for i in idx])
             ours["slowdown_vs_alone"] = {"p50": float(np.percentile(slow, 50)), "p99": float(np.percentile(slow, 99))}
+            # the trace's p99 latency against the p99 of the same requests' solo latencies
+            ours["p99_over_solo_p99"] = float(np.percentile([r.latency for r in res], 99) /
+                                             np.percentile(solo, 99))
         with serving.PlacementServer(slots=1, precision="fp32") as srv:
             warm(srv, 1)
             base = serving.summarize(serving.replay(srv, reqs, arrivals))
@@ -581,6 +585,9 @@ def main():
     ap.add_argument("--serve-designs", type=int, default=48)
     args = ap.parse_args()
     if args.serve:
+        # two streams per slot: give the device as many hardware work queues (read when the
+        # CUDA context is created, which has not happened yet in this process)
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "16")
         return run_serve(args)
     if args.poisson_sweep:
         return run_poisson_sweep(args)

@@ -6,8 +6,13 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <utility>
 
 #include "spgpu.h"
@@ -21,8 +26,38 @@ struct Error : std::runtime_error {
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// Diagnostics: with SPG_SLOW_CALLS=<ms> set, every checked CUDA call that takes longer than
+// that on the host is reported on stderr (time, source line, start time in microseconds,
+// thread, expression), so calls that stall behind other threads can be told apart.
+inline double slow_call_ms() {
+    static const double ms = [] {
+        const char* e = std::getenv("SPG_SLOW_CALLS");
+        return e ? std::atof(e) : 0.0;
+    }();
+    return ms;
+}
+struct CallClock {
+    const char* what;
+    int line;
+    std::chrono::steady_clock::time_point t0;
+    CallClock(const char* w, int l) : what(w), line(l) {
+        if (slow_call_ms() > 0.0) t0 = std::chrono::steady_clock::now();
+    }
+    ~CallClock() {
+        const double lim = slow_call_ms();
+        if (lim <= 0.0) return;
+        const double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        if (ms > lim)
+            std::fprintf(stderr, "[spg slow call] %.2f ms line %d t0 %lld tid %zu: %s\n", ms, line,
+                         static_cast<long long>(std::chrono::duration_cast<std::chrono::microseconds>(
+                                                    t0.time_since_epoch()).count()),
+                         std::hash<std::thread::id>{}(std::this_thread::get_id()) % 100000, what);
+    }
+};
+
 #define SPG_CUDA(call)                                                                   \
     do {                                                                                 \
+        const ::spg::CallClock clk_(#call, __LINE__);                                    \
         cudaError_t e_ = (call);                                                         \
         if (e_ != cudaSuccess)                                                           \
             throw ::spg::Error(SPG_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \

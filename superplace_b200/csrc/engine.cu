@@ -305,6 +305,7 @@ struct ContextStreams {
 
 struct Context : ContextStreams {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // the stage loop's timing events
     spg_params prm{};
     // host copy of the db (flags and sizes change with mLG; positions live on the device)
     int num_movable = 0, num_nodes = 0, num_fillers = 0, total = 0, num_pins = 0, num_nets = 0, num_slots = 0;
@@ -365,19 +366,29 @@ struct Context : ContextStreams {
     DevState* hst = nullptr;  // pinned host mirror
     Staging staging;          // pinned staging of this context's host <-> device copies
     float step_x_gamma = 1.f;
-    // the iteration loop as a conditional CUDA graph (engine.cu: build_loop_graph); the
-    // host-driven loop runs instead where the driver refuses conditional nodes
+    // the iteration loop as a conditional CUDA graph (engine.cu: build_loop_graph), one per
+    // Poisson plan held (the kernel sequence differs between grid sizes); the host-driven
+    // loop runs instead where the driver refuses conditional nodes
     bool use_graph = true;
     bool last_run_graph = false;
     double last_graph_build_ms = 0.0;
-    std::shared_ptr<LoopGraph> loop_graph;
+    std::vector<std::pair<const PoissonPlan*, std::shared_ptr<LoopGraph>>> loop_graphs;
+    void drop_loop_graph(const PoissonPlan* pl) {
+        for (auto it = loop_graphs.begin(); it != loop_graphs.end(); ++it)
+            if (it->first == pl) {
+                loop_graphs.erase(it);
+                return;
+            }
+    }
 
     ~Context() {
         if (side) host_wait(side);
         if (stream) host_wait(stream);
-        loop_graph.reset();
+        loop_graphs.clear();
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
+        if (ev_t0) cudaEventDestroy(ev_t0);
+        if (ev_t1) cudaEventDestroy(ev_t1);
         if (plan) poisson_plan_destroy(*plan);
         for (auto& q : spare_plans) poisson_plan_destroy(*q);
         if (hst) cudaFreeHost(hst);
@@ -677,6 +688,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         c.plan = std::move(next);
         constexpr size_t kSparePlans = 4;
         while (c.spare_plans.size() > kSparePlans) {
+            c.drop_loop_graph(c.spare_plans.front().get());
             poisson_plan_destroy(*c.spare_plans.front());
             c.spare_plans.erase(c.spare_plans.begin());
         }
@@ -825,7 +837,21 @@ void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int cou
     else launch_assemble(p, pos_role >= 0 ? pos_role : R_U, grad_role, count, s);
 }
 
+// A tensor-core Poisson solve that gave up a bounded pipeline wait leaves its code in the
+// plan's flag; it becomes the stage's error, so the state read below raises it.
+__global__ void fold_error_kernel(DevState* st, const int* flag) {
+    const int e = *flag;
+    if (e) atomicCAS(&st->error, 0, e);
+}
+
 void read_state(Context& c) {
+    if (c.plan) {
+        if (const int* f = tc_error_flag(*c.plan)) {
+            fold_error_kernel<<<1, 1, 0, c.stream>>>(c.st.p, f);
+            count_launch();
+            SPG_CHECK_LAUNCH();
+        }
+    }
     SPG_CUDA(cudaMemcpyAsync(c.hst, c.st.p, sizeof(DevState), cudaMemcpyDeviceToHost, c.stream));
     SPG_CUDA(host_wait(c.stream));
     if (c.hst->error) {
@@ -833,6 +859,7 @@ void read_state(Context& c) {
         throw Error(e, e == SPG_E_NON_FINITE ? "GP/evaluate: non-finite coordinate, gradient or metric"
                      : e == SPG_E_OUT_OF_CORE ? "GP: node outside core"
                      : e == SPG_E_CAPACITY ? "GP: stagnation snapshot capacity exceeded"
+                     : e == SPG_E_CUDA ? "GP: a tensor-core Poisson solve gave up a bounded pipeline wait"
                                            : "GP: device error");
     }
 }
@@ -967,8 +994,11 @@ struct CtxScope {
 };
 
 struct LoopGraph {
-    cudaGraph_t graph = nullptr;
+    cudaGraph_t graph = nullptr;  // the template the executable was made from (kept with it)
     cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle loop_h{};
+    std::vector<cudaGraphNode_t> body_nodes;  // the WHILE body's kernel nodes, in launch order
+    bool patchable = true;                    // the last patch attempt worked (or none was made)
     DevPtrs sig{};
     const void* plan = nullptr;
     int64_t body_kernels = 0;
@@ -978,6 +1008,8 @@ struct LoopGraph {
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
         graph = nullptr;
+        body_nodes.clear();
+        patchable = true;
     }
 };
 
@@ -1016,8 +1048,85 @@ void graph_note(const char* what) {
     if (on) std::fprintf(stderr, "[spg graph] %s\n", what);
 }
 
-bool build_loop_graph(Context& c, const DevPtrs& p) {
-    LoopGraph& lg = *c.loop_graph;
+// The kernel nodes of a graph in creation (launch) order, or false when it holds any other
+// kind of node.
+bool kernel_nodes(cudaGraph_t g, std::vector<cudaGraphNode_t>& out) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess) return false;
+    out.resize(n);
+    if (n && cudaGraphGetNodes(g, out.data(), &n) != cudaSuccess) return false;
+    for (cudaGraphNode_t nd : out) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) != cudaSuccess || t != cudaGraphNodeTypeKernel) return false;
+    }
+    return true;
+}
+
+// A new netlist's loop with the same kernel sequence: capture the body alone (a plain graph,
+// cheap to build and to destroy) and write its kernel arguments and launch shapes into the
+// executable's body nodes. Keeping the template avoids destroying a graph that holds a
+// conditional node per request, which is slow and stalls other threads' CUDA calls.
+// Returns false (the executable is then rebuilt) when the sequences differ in length,
+// kernels or dependency counts.
+bool patch_loop_graph(Context& c, const DevPtrs& p, LoopGraph& lg) {
+    cudaStream_t s = c.stream;
+    const int64_t launches0 = g_launches;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    bool fine = true;
+    try {
+        enqueue_iteration(c, p);
+        launch_loop_cond(p, lg.loop_h, s);
+    } catch (const Error&) {
+        fine = false;
+    }
+    cudaGraph_t nb = nullptr;
+    const bool ended = cudaStreamEndCapture(s, &nb) == cudaSuccess;
+    g_launches = launches0;
+    struct Drop {
+        cudaGraph_t g;
+        ~Drop() {
+            if (g) cudaGraphDestroy(g);
+        }
+    } drop{nb};
+    std::vector<cudaGraphNode_t> nodes;
+    if (!fine || !ended || !nb || !kernel_nodes(nb, nodes) || nodes.size() != lg.body_nodes.size()) {
+        cudaGetLastError();
+        return false;
+    }
+    std::vector<cudaKernelNodeParams> kp(nodes.size());
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        cudaKernelNodeParams old{};
+        size_t da = 0, db = 0;
+        if (cudaGraphKernelNodeGetParams(nodes[i], &kp[i]) != cudaSuccess ||
+            cudaGraphKernelNodeGetParams(lg.body_nodes[i], &old) != cudaSuccess || kp[i].func != old.func ||
+            cudaGraphNodeGetDependencies(nodes[i], nullptr, &da) != cudaSuccess ||
+            cudaGraphNodeGetDependencies(lg.body_nodes[i], nullptr, &db) != cudaSuccess || da != db) {
+            cudaGetLastError();
+            return false;
+        }
+    }
+    for (size_t i = 0; i < nodes.size(); ++i)
+        if (cudaGraphExecKernelNodeSetParams(lg.exec, lg.body_nodes[i], &kp[i]) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+    return true;
+}
+
+bool build_loop_graph(Context& c, const DevPtrs& p, LoopGraph& lg) {
+    const CallClock clk_all("build_loop_graph (capture, update or instantiate, destroy)", __LINE__);
+    if (lg.exec && lg.patchable && !lg.body_nodes.empty()) {
+        if (patch_loop_graph(c, p, lg)) {
+            graph_note("loop graph patched in place");
+            lg.sig = p;
+            lg.plan = c.plan.get();
+            return true;
+        }
+        lg.patchable = false;
+    }
     // an executable graph of an earlier netlist is updated in place when the new capture
     // allows it (same topology, new kernel arguments), which costs far less than a new
     // instantiation; otherwise it is replaced
@@ -1029,6 +1138,7 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
         cudaGraphExec_t& e;
         cudaGraph_t& g;
         ~DropOld() {
+            const CallClock clk_("cudaGraphExecDestroy / cudaGraphDestroy", __LINE__);
             if (e) cudaGraphExecDestroy(e);
             if (g) cudaGraphDestroy(g);
         }
@@ -1049,6 +1159,7 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
     cudaGraphNode_t wnode;
     if (!ok(cudaGraphAddNode(&wnode, g, nullptr, 0, &wp))) return false;
     cudaGraph_t body = wp.conditional.phGraph_out[0];
+    lg.loop_h = loop_h;
     if (!ok(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal)))
         return false;
     bool fine = true;
@@ -1068,11 +1179,18 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
         return false;
     }
     graph_stats("loop body", body);
+    bool updated_in_place = false;
     if (old_exec) {
         cudaGraphExecUpdateResultInfo info{};
-        if (cudaGraphExecUpdate(old_exec, g, &info) == cudaSuccess) {
+        cudaError_t ue;
+        {
+            const CallClock clk_("cudaGraphExecUpdate", __LINE__);
+            ue = cudaGraphExecUpdate(old_exec, g, &info);
+        }
+        if (ue == cudaSuccess) {
             lg.exec = old_exec;
             old_exec = nullptr;
+            updated_in_place = true;
         } else {
             cudaGetLastError();
         }
@@ -1082,17 +1200,28 @@ bool build_loop_graph(Context& c, const DevPtrs& p) {
         cudaGetLastError();
         return false;
     }
+    // node-level patches address the nodes of the graph the executable was instantiated
+    // from: not this template after an update in place
+    lg.patchable = !updated_in_place && kernel_nodes(body, lg.body_nodes);
+    if (!lg.patchable) lg.body_nodes.clear();
+    cudaGetLastError();
     lg.sig = p;
     lg.plan = c.plan.get();
     return true;
 }
 
 bool graph_loop(Context& c, const DevPtrs& p) {
-    if (!c.loop_graph) c.loop_graph = std::make_shared<LoopGraph>();
-    LoopGraph& lg = *c.loop_graph;
+    std::shared_ptr<LoopGraph> lgp;
+    for (auto& e : c.loop_graphs)
+        if (e.first == c.plan.get()) lgp = e.second;
+    if (!lgp) {
+        lgp = std::make_shared<LoopGraph>();
+        c.loop_graphs.emplace_back(c.plan.get(), lgp);
+    }
+    LoopGraph& lg = *lgp;
     const bool same = lg.exec && lg.plan == c.plan.get() && std::memcmp(&lg.sig, &p, sizeof(DevPtrs)) == 0;
     const auto tb = std::chrono::steady_clock::now();
-    const bool built = !same && build_loop_graph(c, p);
+    const bool built = !same && build_loop_graph(c, p, lg);
     if (!same) c.last_graph_build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
     if (!same && !built) {
         lg.reset();
@@ -1159,9 +1288,7 @@ void stage_run(Context& c, int stage, spg_result* res) {
         return;
     }
 
-    cudaEvent_t e0, e1;
-    SPG_CUDA(cudaEventCreate(&e0));
-    SPG_CUDA(cudaEventCreate(&e1));
+    cudaEvent_t e0 = c.ev_t0, e1 = c.ev_t1;
     SPG_CUDA(cudaEventRecord(e0, s));
     launch_stage_clock(p, s);
     // optimizer init: u = v = uPrev = vPrev = pos, g = gPrevTmp = 0 (nesterov.cpp:174-185)
@@ -1194,8 +1321,6 @@ void stage_run(Context& c, int stage, spg_result* res) {
     ht.mark("final");
     float ms = 0.f;
     SPG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     const DevState& h = *c.hst;
     res->iterations = h.rows;
     res->converged = h.converged;
@@ -1267,6 +1392,7 @@ namespace spg {
 // and the node-order pin slots. Device buffers with enough capacity are reused. The grid
 // and the stage state are rebuilt by the next stage run.
 void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
+    HostTimer ht(" load");
     SPG_REQUIRE(v->num_movable >= 0 && v->num_nodes >= v->num_movable && v->num_fillers >= 0 &&
                     v->num_pins >= 0 && v->num_nets >= 0,
                 SPG_E_INVALID, "inconsistent db counts");
@@ -1309,6 +1435,7 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
                     "flat_node2pin out of range");
         SPG_REQUIRE(v->pin2net[p] < c.num_nets, SPG_E_INVALID, "pin2net out of range");
     }
+    ht.mark("validate");
     cudaStream_t s = c.stream;
     c.x.upload(v->node_x, T, s);
     c.y.upload(v->node_y, T, s);
@@ -1329,6 +1456,7 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
     // d <= kWaThreadNetDegree is owned by one thread, a larger one by a lane group of the next
     // power of two >= d, and the nets above 32 pins by one warp each that loops over its pins
     // (wirelength.cu)
+    ht.mark("uploads");
     std::vector<int> order(c.num_nets);
     std::iota(order.begin(), order.end(), 0);
     auto deg = [&](int k) { return v->net2pin_start[k + 1] - v->net2pin_start[k]; };
@@ -1373,6 +1501,7 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
         }
         wc.warp_begin[wc.n] = warps;
     }
+    ht.mark("classes");
     // node-order slots of the pins that belong to a net; the last slot is never read
     {
         for (int k = 0; k < c.num_nets; ++k)
@@ -1417,6 +1546,7 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
         c.wa_node_slot.upload(node_slot, s);
         c.wa_off.upload(off, s);
     }
+    ht.mark("slots");
     c.gpx.alloc(c.num_slots + 1);
     c.gpy.alloc(c.num_slots + 1);
     c.gpx.zero(s);
@@ -1424,6 +1554,7 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
     c.st.alloc(1);
     if (!c.hst) SPG_CUDA(cudaMallocHost(&c.hst, sizeof(DevState)));
     c.scratch_d.alloc(16);
+    ht.mark("alloc");
 }
 
 }  // namespace spg
@@ -1500,6 +1631,12 @@ int spg_poisson_solve(spg_poisson* h, const float* rho, float* phi, float* fx, f
     SPG_CUDA(cudaMemcpyAsync(fx, d + 2 * n, n * 4, cudaMemcpyDeviceToHost, s));
     SPG_CUDA(cudaMemcpyAsync(fy, d + 3 * n, n * 4, cudaMemcpyDeviceToHost, s));
     SPG_CUDA(spg::host_wait(s));
+    if (const int* f = spg::tc_error_flag(h->h.plan)) {
+        int e = 0;
+        SPG_CUDA(cudaMemcpyAsync(&e, f, sizeof(e), cudaMemcpyDeviceToHost, s));
+        SPG_CUDA(spg::host_wait(s));
+        if (e) throw spg::Error(e, "Poisson tensor-core solve gave up a bounded pipeline wait");
+    }
     return SPG_OK;
     API_CATCH
 }
@@ -1629,6 +1766,8 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     SPG_CUDA(cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, prio_low));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
+    SPG_CUDA(cudaEventCreate(&c.ev_t0));
+    SPG_CUDA(cudaEventCreate(&c.ev_t1));
     spg::CtxScope scope(c);
     spg::load_netlist(c, v, prm);
     SPG_CUDA(spg::host_wait(c.stream));
@@ -1884,6 +2023,7 @@ int spg_hpwl(spg_ctx* ctx, double* hpwl) {
 int spg_stage_run(spg_ctx* ctx, int stage, spg_result* result) {
     API_TRY
     SPG_REQUIRE(ctx && result, SPG_E_INVALID, "null argument");
+    spg::CtxScope scope(ctx->c);
     spg::stage_run(ctx->c, stage, result);
     return SPG_OK;
     API_CATCH

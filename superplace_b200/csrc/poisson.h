@@ -104,6 +104,9 @@ bool tc_supported(int nx, int ny);
 void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::vector<float>& cx,
                     const std::vector<float>& bcat, const std::vector<float>& acat);
 void tc_plan_destroy(PoissonPlan& pl);
+// The plan's device error flag (0, or SPG_E_CUDA after a tensor-core solve gave up a bounded
+// pipeline wait), or nullptr for plans without tensor-core GEMMs.
+const int* tc_error_flag(const PoissonPlan& pl);
 // rewrite the split-BF16 planes of the step-dependent rows in place: Sy (rows ny..2ny of
 // [Ay; Sy]) and Sx (rows nx..2nx of [Ax; Sx]); same buffers, same tensor maps
 void tc_plan_refill_sines(PoissonPlan& pl, const std::vector<float>& sy_rows, const std::vector<float>& sx_rows);

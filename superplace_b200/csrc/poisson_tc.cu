@@ -583,12 +583,9 @@ void tc_plan_destroy(PoissonPlan& pl) {
     }
 }
 
-int tc_error(const PoissonPlan& pl) {
+const int* tc_error_flag(const PoissonPlan& pl) {
     const auto* st = static_cast<const TcState*>(pl.tc);
-    if (!st) return 0;
-    int e = 0;
-    SPG_CUDA(cudaMemcpy(&e, st->err, 4, cudaMemcpyDeviceToHost));
-    return e;
+    return st ? st->err : nullptr;
 }
 
 void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
