@@ -14,6 +14,9 @@ keeps up to `slots` requests on the device at once:
   its own inputs, and every reduction in the engine has a fixed order.
 
 `PlacementServer(slots=1, precision="fp32")` is the one-at-a-time plain-FP32 baseline.
+Each slot's context uses two CUDA streams; a serving process with many slots should set
+CUDA_DEVICE_MAX_CONNECTIONS to twice the slot count before CUDA starts (bench.py --serve does),
+so that the slots' streams do not share hardware work queues.
 """
 from __future__ import annotations
 
