@@ -339,7 +339,8 @@ struct Context : ContextStreams {
     int n_rest_small = 0, n_rest_large = 0;
     // stage
     int n_opt = 0;
-    DevBuf<int> opt_idx, opt_deg, opt_small, opt_large;
+    DevBuf<int> opt_idx, opt_deg, opt_large, opt_cells;
+    std::vector<int> opt_cells_h;  // the stage's opt cells (host), ascending
     DevBuf<float4> opt_geom;
     DevBuf<int4> opt_meta;
     // the fillers' shared attributes (see DevPtrs::filler_k0)
@@ -356,7 +357,7 @@ struct Context : ContextStreams {
     bool mirror_valid = false;
     DevBuf<float> opt_lo, opt_hi, force, pool;
     DevBuf<double> opt_area;
-    int n_opt_small = 0, n_opt_large = 0;
+    int n_opt_large = 0;
     size_t vec_stride = 0;
     DevBuf<double> partials;
     DevBuf<DevState> st;
@@ -465,9 +466,7 @@ struct Context : ContextStreams {
         p.rest_large = rest_large.p;
         p.n_rest_small = n_rest_small;
         p.n_rest_large = n_rest_large;
-        p.opt_small = opt_small.p;
         p.opt_large = opt_large.p;
-        p.n_opt_small = n_opt_small;
         p.n_opt_large = n_opt_large;
         p.partials = partials.p;
         p.st = st.p;
@@ -602,34 +601,60 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     }
 
     ht.mark("statics");
-    // footprint data: half extents after local smoothing, charge weight, kernel class
-    std::vector<float> hw(c.total), hh(c.total), wgt(c.total);
-    std::vector<uint8_t> kind(c.total, 0);
-    std::vector<int> dsmall, dlarge;
+    // footprint data: half extents after local smoothing, charge weight, kernel class (host
+    // copies kept in the context, so their memory is reused stage after stage)
+    std::vector<float>& hw = c.hw_h;
+    std::vector<float>& hh = c.hh_h;
+    std::vector<float>& wgt = c.wgt_h;
+    std::vector<uint8_t>& kind = c.kind_h;
+    std::vector<int>& dsmall = c.dens_small_h;
+    std::vector<int>& dlarge = c.dens_large_h;
+    hw.resize(c.total);
+    hh.resize(c.total);
+    wgt.resize(c.total);
+    kind.assign(c.total, 0);
+    dsmall.clear();
+    dlarge.clear();
     double bound = 0.0;
+    // a node's footprint is a function of its size and flags alone: runs of identical nodes
+    // (the fillers above all) reuse the previous node's values instead of recomputing them
+    float pw = -1.f, ph = -1.f, phw = 0.f, phh = 0.f, pwgt = 0.f;
+    uint8_t pflags = 0, pkind = 0;
     for (int i = 0; i < c.total; ++i) {
         const float w = c.w[i], h = c.h[i];
-        float sx = 1.f, sy = 1.f;
-        hw[i] = 0.5f * w;
-        hh[i] = 0.5f * h;
-        if (w < g.step_x) {
-            sx = w / g.step_x;
-            hw[i] = 0.5f * g.step_x;
+        if (!(w == pw && h == ph && c.flags[i] == pflags)) {
+            float sx = 1.f, sy = 1.f;
+            phw = 0.5f * w;
+            phh = 0.5f * h;
+            if (w < g.step_x) {
+                sx = w / g.step_x;
+                phw = 0.5f * g.step_x;
+            }
+            if (h < g.step_y) {
+                sy = h / g.step_y;
+                phh = 0.5f * g.step_y;
+            }
+            const float scale = sx * sy;
+            pwgt = c.filler(i) ? scale : (c.macro(i) ? scale * target : scale);
+            pkind = 0;
+            if (!(c.fixed(i) || c.ni(i))) {
+                pkind = K_DENSITY;
+                if (c.filler(i)) pkind |= K_FILLER;
+                const double bins =
+                    (std::floor(2.0 * phw / g.step_x) + 2.0) * (std::floor(2.0 * phh / g.step_y) + 2.0);
+                if (bins > 16.0) pkind |= K_LARGE;
+            }
+            pw = w;
+            ph = h;
+            pflags = c.flags[i];
         }
-        if (h < g.step_y) {
-            sy = h / g.step_y;
-            hh[i] = 0.5f * g.step_y;
-        }
-        const float scale = sx * sy;
-        wgt[i] = c.filler(i) ? scale : (c.macro(i) ? scale * target : scale);
-        if (c.fixed(i) || c.ni(i)) continue;
+        hw[i] = phw;
+        hh[i] = phh;
+        wgt[i] = pwgt;
+        if (!pkind) continue;  // fixed or NI: no density
         bound += static_cast<double>(w) * static_cast<double>(h);
-        uint8_t k = K_DENSITY;
-        if (c.filler(i)) k |= K_FILLER;
-        const double bins = (std::floor(2.0 * hw[i] / g.step_x) + 2.0) * (std::floor(2.0 * hh[i] / g.step_y) + 2.0);
-        if (bins > 16.0) k |= K_LARGE;
-        kind[i] = k;
-        (k & K_LARGE ? dlarge : dsmall).push_back(i);
+        kind[i] = pkind;
+        (pkind & K_LARGE ? dlarge : dsmall).push_back(i);
     }
     // fixed-point scale: largest s <= 40 with (total charge bound) * 2^s < 2^62
     bound *= target > 1.f ? static_cast<double>(target) : 1.0;
@@ -650,17 +675,11 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     c.hw.upload(hw, st);
     c.hh.upload(hh, st);
     c.wgt.upload(wgt, st);
-    c.hw_h = hw;
-    c.hh_h = hh;
-    c.wgt_h = wgt;
     c.kind.upload(kind, st);
-    c.kind_h = kind;
     c.dens_small.upload(dsmall, st);
     c.dens_large.upload(dlarge, st);
     c.n_dens_small = static_cast<int>(dsmall.size());
     c.n_dens_large = static_cast<int>(dlarge.size());
-    c.dens_small_h = dsmall;
-    c.dens_large_h = dlarge;
     c.node_fix.alloc(n);
     c.filler_fix.alloc(n);
     c.node_fix.zero(st);
@@ -702,95 +721,141 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     c.grid_ready = true;
 }
 
+// Per-opt-node arrays of a stage, built on the device from the node arrays already there:
+// opt k is node cells[k] (k < k0) or filler num_nodes + (k - k0). Clamp box, degree, area,
+// footprint and slot range use the same IEEE single and double operations as the reference
+// (eplace.cpp:117-133,176-178), so every value equals a host computation bit for bit.
+struct StageOptArgs {
+    const int* cells;
+    int k0, n, num_nodes, num_movable;
+    const float *w, *h, *hw, *hh, *wgt;
+    const int *node_start, *slot_start;
+    const uint8_t* kind;
+    float core_lx, core_ly, core_hx, core_hy;
+    int* opt_idx;
+    float *lo, *hi;
+    int* deg;
+    double* area;
+    float4* geom;
+    int4* meta;
+};
+
+__device__ __forceinline__ float dmax_f(float a, float b) { return (a < b) ? b : a; }
+
+__global__ void stage_opt_kernel(StageOptArgs a) {
+    const int n = a.n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = k < a.k0 ? a.cells[k] : a.num_nodes + (k - a.k0);
+        a.opt_idx[k] = i;
+        const float w = a.w[i], h = a.h[i];
+        const float hw = fmul(0.5f, w), hh = fmul(0.5f, h);
+        const float xlo = fadd(fadd(a.core_lx, hw), kBoundaryEps);
+        const float ylo = fadd(fadd(a.core_ly, hh), kBoundaryEps);
+        a.lo[k] = xlo;
+        a.hi[k] = dmax_f(xlo, fsub(fsub(a.core_hx, hw), kBoundaryEps));
+        a.lo[n + k] = ylo;
+        a.hi[n + k] = dmax_f(ylo, fsub(fsub(a.core_hy, hh), kBoundaryEps));
+        const int d = a.node_start[i + 1] - a.node_start[i];
+        a.deg[k] = d;
+        a.area[k] = __dmul_rn(static_cast<double>(w), static_cast<double>(h));
+        a.geom[k] = make_float4(a.hw[i], a.hh[i], a.wgt[i], 0.f);
+        const bool has_wl = i < a.num_movable;
+        a.meta[k] = make_int4(a.slot_start[i], has_wl ? a.slot_start[i + 1] : a.slot_start[i], d,
+                              static_cast<int>(a.kind[i]) | (has_wl ? OPT_HAS_WL : 0));
+    }
+}
+
 // EPlace::Impl::buildOptSet (eplace.cpp:82-94) and the per-opt-node clamp boxes
-// (eplace.cpp:117-133), degrees and areas (eplace.cpp:176-178).
+// (eplace.cpp:117-133), degrees and areas (eplace.cpp:176-178). The host picks the opt cells,
+// checks whether the fillers share every attribute and lists the large opt nodes; the
+// per-node arrays are written by stage_opt_kernel.
 void stage_setup(Context& c, int stage) {
-    std::vector<int> opt;
-    opt.reserve(static_cast<size_t>(c.num_movable + c.num_fillers));
+    std::vector<int>& cells = c.opt_cells_h;
+    cells.clear();
     if (stage != SPG_STAGE_FILLER_ONLY) {
         for (int i = 0; i < c.num_movable; ++i) {
             if (c.fixed(i) || c.ni(i)) continue;
             if (stage == SPG_STAGE_CGP && c.macro(i)) continue;
-            opt.push_back(i);
+            cells.push_back(i);
         }
     }
-    for (int i = c.num_nodes; i < c.total; ++i) opt.push_back(i);
-    const int n = static_cast<int>(opt.size());
+    const int k0 = static_cast<int>(cells.size());
+    const int nf = c.total - c.num_nodes;
+    const int n = k0 + nf;
     c.n_opt = n;
-    std::vector<float> lo(2 * static_cast<size_t>(n)), hi(2 * static_cast<size_t>(n));
-    std::vector<int> deg(n), osmall, olarge;
-    std::vector<double> area(n);
-    std::vector<float4> geom(n);
-    std::vector<int4> meta(n);
     const std::vector<uint8_t>& kind = c.kind_h;
-    for (int k = 0; k < n; ++k) {
-        const int i = opt[k];
+    // opt k's clamp box (eplace.cpp:117-133), for the filler constants
+    auto box = [&](int i, float& xlo, float& xhi, float& ylo, float& yhi) {
         const float hw = 0.5f * c.w[i], hh = 0.5f * c.h[i];
-        const float xlo = c.core_lx + hw + kBoundaryEps;
-        const float xhi = hmax(xlo, c.core_hx - hw - kBoundaryEps);
-        const float ylo = c.core_ly + hh + kBoundaryEps;
-        const float yhi = hmax(ylo, c.core_hy - hh - kBoundaryEps);
-        lo[k] = xlo;
-        hi[k] = xhi;
-        lo[n + k] = ylo;
-        hi[n + k] = yhi;
-        deg[k] = c.node_start[i + 1] - c.node_start[i];
-        area[k] = static_cast<double>(c.w[i]) * static_cast<double>(c.h[i]);
-        (kind[i] & K_LARGE ? olarge : osmall).push_back(k);
-        geom[k] = make_float4(c.hw_h[i], c.hh_h[i], c.wgt_h[i], 0.f);
-        const bool has_wl = i < c.num_movable;
-        meta[k] = make_int4(c.slot_start_h[i], has_wl ? c.slot_start_h[i + 1] : c.slot_start_h[i], deg[k],
-                            static_cast<int>(kind[i]) | (has_wl ? OPT_HAS_WL : 0));
-    }
-    cudaStream_t s = c.stream;
-    c.opt_idx.upload(opt, s);
-    c.opt_lo.upload(lo, s);
-    c.opt_hi.upload(hi, s);
-    c.opt_deg.upload(deg, s);
-    c.opt_area.upload(area, s);
-    c.opt_geom.upload(geom, s);
-    c.opt_meta.upload(meta, s);
-    // the fillers close the opt set (one run, nodes num_nodes..total-1); when they all share
-    // every attribute the kernels read, pass those once instead of per node
+        xlo = c.core_lx + hw + kBoundaryEps;
+        xhi = hmax(xlo, c.core_hx - hw - kBoundaryEps);
+        ylo = c.core_ly + hh + kBoundaryEps;
+        yhi = hmax(ylo, c.core_hy - hh - kBoundaryEps);
+    };
+    std::vector<int> olarge;
+    for (int k = 0; k < k0; ++k)
+        if (kind[cells[k]] & K_LARGE) olarge.push_back(k);
+    // the fillers close the opt set (nodes num_nodes..total-1); when they all share every
+    // attribute the kernels read (size, so clamp box, area and footprint; degree; kind; no
+    // pin slots), pass those once instead of per node
+    bool same = nf > 0;
     {
-        const int nf = c.total - c.num_nodes;
-        const int k0 = n - nf;
-        bool same = nf > 0 && k0 >= 0 && opt[k0] == c.num_nodes;
-        for (int k = k0; same && k < n; ++k) {
-            same = opt[k] == c.num_nodes + (k - k0) && geom[k].x == geom[k0].x && geom[k].y == geom[k0].y &&
-                   geom[k].z == geom[k0].z && meta[k].x == meta[k].y && meta[k].z == meta[k0].z &&
-                   meta[k].w == meta[k0].w && area[k] == area[k0] && lo[k] == lo[k0] && hi[k] == hi[k0] &&
-                   lo[n + k] == lo[n + k0] && hi[n + k] == hi[n + k0];
+        const int f0 = c.num_nodes;
+        for (int i = f0; i < c.total; ++i) {
+            if (kind[i] & K_LARGE) olarge.push_back(k0 + (i - f0));
+            if (same)
+                same = c.w[i] == c.w[f0] && c.h[i] == c.h[f0] && kind[i] == kind[f0] &&
+                       c.node_start[i + 1] - c.node_start[i] == c.node_start[f0 + 1] - c.node_start[f0] &&
+                       c.slot_start_h[i] == c.slot_start_h[i + 1] && c.hw_h[i] == c.hw_h[f0] &&
+                       c.hh_h[i] == c.hh_h[f0] && c.wgt_h[i] == c.wgt_h[f0];
         }
         if (same) {
             c.filler_k0 = k0;
-            c.filler_geom = geom[k0];
-            c.filler_meta = make_int4(0, 0, meta[k0].z, meta[k0].w);
-            c.filler_area = area[k0];
-            c.filler_lo_x = lo[k0];
-            c.filler_hi_x = hi[k0];
-            c.filler_lo_y = lo[n + k0];
-            c.filler_hi_y = hi[n + k0];
+            c.filler_geom = make_float4(c.hw_h[f0], c.hh_h[f0], c.wgt_h[f0], 0.f);
+            c.filler_meta = make_int4(0, 0, c.node_start[f0 + 1] - c.node_start[f0], static_cast<int>(kind[f0]));
+            c.filler_area = static_cast<double>(c.w[f0]) * static_cast<double>(c.h[f0]);
+            box(f0, c.filler_lo_x, c.filler_hi_x, c.filler_lo_y, c.filler_hi_y);
         } else {
             c.filler_k0 = n;
         }
     }
+    cudaStream_t s = c.stream;
+    c.opt_cells.upload(cells, s);
+    const size_t nn = static_cast<size_t>(std::max(n, 1));
+    c.opt_idx.alloc(nn);
+    c.opt_lo.alloc(2 * nn);
+    c.opt_hi.alloc(2 * nn);
+    c.opt_deg.alloc(nn);
+    c.opt_area.alloc(nn);
+    c.opt_geom.alloc(nn);
+    c.opt_meta.alloc(nn);
+    if (n > 0) {
+        StageOptArgs a{c.opt_cells.p, k0, n, c.num_nodes, c.num_movable, c.dw.p, c.dh.p, c.hw.p, c.hh.p,
+                       c.wgt.p, c.node_start_d.p, c.slot_start.p, c.kind.p, c.core_lx, c.core_ly, c.core_hx,
+                       c.core_hy, c.opt_idx.p, c.opt_lo.p, c.opt_hi.p, c.opt_deg.p, c.opt_area.p, c.opt_geom.p,
+                       c.opt_meta.p};
+        stage_opt_kernel<<<work_grid(reinterpret_cast<const void*>(stage_opt_kernel), n, RED_THREADS),
+                           RED_THREADS, 0, s>>>(a);
+        count_launch();
+        SPG_CHECK_LAUNCH();
+    }
     // density nodes the loop's step kernel does not rasterize: small ones outside the opt
-    // set (the cells of FILLERONLY, the macros of cGP) and every large node
+    // set (the cells of FILLERONLY, the macros of cGP) and every large node. Every density
+    // node is movable (or a filler, always in the opt set).
     {
-        std::vector<uint8_t> in_opt(c.total, 0);
-        for (int i : opt) in_opt[i] = 1;
         std::vector<int> rs;
-        for (int i : c.dens_small_h)
-            if (!in_opt[i]) rs.push_back(i);
+        for (int i : c.dens_small_h) {
+            if (i >= c.num_nodes) break;  // the list is ascending; fillers are in the opt set
+            const bool in_opt = i < c.num_movable && !c.fixed(i) && !c.ni(i) && stage != SPG_STAGE_FILLER_ONLY &&
+                                !(stage == SPG_STAGE_CGP && c.macro(i));
+            if (!in_opt) rs.push_back(i);
+        }
         c.rest_small.upload(rs, s);
         c.n_rest_small = static_cast<int>(rs.size());
         c.rest_large.upload(c.dens_large_h, s);
         c.n_rest_large = static_cast<int>(c.dens_large_h.size());
     }
-    c.opt_small.upload(osmall, s);
     c.opt_large.upload(olarge, s);
-    c.n_opt_small = static_cast<int>(osmall.size());
     c.n_opt_large = static_cast<int>(olarge.size());
     c.force.alloc(2 * static_cast<size_t>(std::max(n, 1)));
     // vectors padded to 64 floats so every role starts 256-byte aligned

@@ -192,8 +192,8 @@ struct DevPtrs {
     int n_dens_small, n_dens_large;
     const int *rest_small, *rest_large;
     int n_rest_small, n_rest_large;
-    const int *opt_small, *opt_large;  // opt positions k
-    int n_opt_small, n_opt_large;
+    const int* opt_large;  // opt positions k of the large nodes
+    int n_opt_large;
     double* partials;      // RED_SLOTS * RED_CAP
     DevState* st;
     spg_iter_metrics* metrics;

@@ -245,9 +245,17 @@ class GpContext:
         y = np.ascontiguousarray(self.db.node_y if y is None else y, np.float32)
         check(lib().spg_positions_h2d(self.h, abi.fptr(x), abi.fptr(y)))
 
-    def positions(self):
+    def positions(self, out=None):
+        """Node positions (x, y) from the device; into `out` = (x, y) when given (float32,
+        contiguous, one entry per node), else into new arrays."""
         n = self.db.total_nodes
-        x, y = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        if out is None:
+            x, y = np.empty(n, np.float32), np.empty(n, np.float32)
+        else:
+            x, y = out
+            for a in (x, y):
+                if a.dtype != np.float32 or a.shape != (n,) or not a.flags.c_contiguous or not a.flags.writeable:
+                    raise ValueError("positions(out=...): float32 contiguous writable arrays of one entry per node")
         check(lib().spg_positions_d2h(self.h, abi.fptr(x), abi.fptr(y)))
         return x, y
 
@@ -349,7 +357,10 @@ class EPlace:
         self.ctx.set_positions(self.db.node_x, self.db.node_y)
         self.ctx.set_flags(self.db.node_flags)
         r = self.ctx.run(stage)
-        x, y = self.ctx.positions()
-        self.db.node_x[:] = x
-        self.db.node_y[:] = y
+        x, y = self.db.node_x, self.db.node_y
+        if (x.dtype == np.float32 and y.dtype == np.float32 and x.flags.c_contiguous and y.flags.c_contiguous
+                and x.flags.writeable and y.flags.writeable):
+            self.ctx.positions(out=(x, y))
+        else:
+            x[:], y[:] = self.ctx.positions()
         return r
