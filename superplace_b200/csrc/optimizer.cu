@@ -594,7 +594,9 @@ __global__ void loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond
 // the evaluation needs no separate pass over the cells; nodes whose footprint may exceed 16
 // bins are left to the block-per-node kernel of the rest list. When no step applies (the
 // stage is done) the current u is rasterized unchanged.
-__global__ void __launch_bounds__(RED_THREADS) step_kernel(DevPtrs p) {
+// 40 registers (6 blocks of 256 per SM, no spills): the kernel is latency-bound, one node
+// per thread, so occupancy is what hides its loads and atomics
+__global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
     pdl_wait();
     pdl_trigger();
     DevState* st = p.st;
