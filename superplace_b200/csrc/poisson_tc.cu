@@ -63,6 +63,11 @@ struct TcArgs {
     const float* row0;      // optional: output row 0 := row0[z*row0_z + n] (* scale[n])
     int64_t row0_z;
     int* err;
+    // optional alternate region (m_alt > 0): output rows m >= m_alt read A from row
+    // a_alt_row0 + (m - m_alt) and B from row b_alt_row0 + n, and go to out3 row m - m_alt
+    // (F32 mode), so two products sharing A's layout run as one launch
+    int m_alt, a_alt_row0, b_alt_row0;
+    float* out3;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -251,7 +256,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (!mbar_wait(empty0 + 8 * st, ph ^ 1)) break;
             const int kk = s * TC_BK;
             const uint32_t sa = smem_u32(base + st * STAGE_BYTES);
-            const int arow = g.a_row0 + m0, brow = g.b_row0 + n0, bcol = kk + z * g.b_col_z;
+            const bool alt = g.m_alt > 0 && m0 >= g.m_alt;
+            const int arow = alt ? g.a_alt_row0 + (m0 - g.m_alt) : g.a_row0 + m0;
+            const int brow = (alt ? g.b_alt_row0 : g.b_row0) + n0, bcol = kk + z * g.b_col_z;
             mbar_expect_tx(full0 + 8 * st, STAGE_BYTES);
             tma_load_2d(sa, &tmA, kk, arow, full0 + 8 * st);
             tma_load_2d(sa + A_BYTES, &tmA, kk, arow + g.a_lo, full0 + 8 * st);
@@ -352,8 +359,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 v[3] *= sc[j].w;
             }
             if (g.mode == TC_F32) {
-                float* dst = (m < g.split) ? g.out + z * g.out_z + m * g.ldc
-                                           : g.out2 + z * g.out_z + (m - g.split) * g.ldc;
+                float* dst = (g.m_alt > 0 && m >= g.m_alt) ? g.out3 + z * g.out_z + (m - g.m_alt) * g.ldc
+                             : (m < g.split) ? g.out + z * g.out_z + m * g.ldc
+                                             : g.out2 + z * g.out_z + (m - g.split) * g.ldc;
                 *reinterpret_cast<float4*>(dst + n) = make_float4(v[0], v[1], v[2], v[3]);
             } else {
                 uint16_t h[4], l[4];
@@ -621,15 +629,14 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
     g3.mode = TC_SPLIT; g3.planes = pl.t12t_s; g3.plane_stride = 2 * static_cast<int64_t>(Y) * BXc;
     g3.plane_z = 0; g3.ldc = BXc; g3.err = st->err;
     launch_tc(st->bcat, st->p_b, g3, 1, (X / TC_BN) * (2 * Y / TC_BM), s);
-    // G4a: [phi; xi_x]_z = [Ax; Sx] . T1t[:, z]^T ; G4b: xi_y_z = Ax . T2t[:, z]^T
+    // G4 in one launch of 3X rows: [phi; xi_x]_z = [Ax; Sx] . T1t[:, z]^T (rows < 2X) and
+    // xi_y_z = Ax . T2t[:, z]^T (the alternate region, rows >= 2X)
     TcArgs g4{};
-    g4.M = 2 * X; g4.N = Y; g4.K = X;
+    g4.M = 3 * X; g4.N = Y; g4.K = X;
     g4.a_row0 = 0; g4.a_lo = 2 * X; g4.b_row0 = 0; g4.b_lo = 2 * Y; g4.b_col_z = X;
     g4.mode = TC_F32; g4.out = phi; g4.out2 = ex; g4.split = X; g4.ldc = Y; g4.out_z = XY; g4.err = st->err;
-    launch_tc(st->acat, st->t12t_b, g4, batch, (Y / TC_BN) * (2 * X / TC_BM), s);
-    TcArgs g5 = g4;
-    g5.M = X; g5.b_row0 = Y; g5.out = ey; g5.out2 = ey;
-    launch_tc(st->acat, st->t12t_b, g5, batch, (Y / TC_BN) * (X / TC_BM), s);
+    g4.m_alt = 2 * X; g4.a_alt_row0 = 0; g4.b_alt_row0 = Y; g4.out3 = ey;
+    launch_tc(st->acat, st->t12t_b, g4, batch, (Y / TC_BN) * (3 * X / TC_BM), s);
 }
 
 }  // namespace spg
