@@ -877,7 +877,7 @@ void stage_setup(Context& c, int stage) {
 // the density -> Poisson chain; the assembly joins both.
 // `stepped`: the step kernel already added the opt nodes' charge (loop evaluations).
 void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count, bool fused_reduce = false,
-              bool stepped = false) {
+              bool stepped = false, cudaGraphConditionalHandle loop_cond = 0) {
     cudaStream_t s = c.stream;
     if (pos_role >= 0) launch_scatter(p, pos_role, s);
     static const bool wa_serial = [] {
@@ -898,7 +898,7 @@ void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int cou
     poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s);
     launch_gather_opt_large(p, s);
     if (!wa_serial) SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
-    if (fused_reduce) launch_assemble_reduce(p, s);
+    if (fused_reduce) launch_assemble_reduce(p, s, loop_cond);
     else launch_assemble(p, pos_role >= 0 ? pos_role : R_U, grad_role, count, s);
 }
 
@@ -1020,10 +1020,12 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
 // redoIfOvershot re-evaluation step, nesterov.cpp:97-119,158-166), the evaluation at the new
 // u, and the redo test / next decisions. A re-evaluation takes a pass of its own, so the loop
 // body is the same for both.
-void enqueue_iteration(Context& c, const DevPtrs& p) {
+// One loop pass; in a captured body the assembly's last block also sets the WHILE node's
+// condition (loop_cond), so the body needs no kernel of its own for it.
+void enqueue_iteration(Context& c, const DevPtrs& p, cudaGraphConditionalHandle loop_cond = 0) {
     cudaStream_t s = c.stream;
     launch_update(p, s);
-    evaluate(c, p, -1, R_G, 1, true, true);
+    evaluate(c, p, -1, R_G, 1, true, true, loop_cond);
 }
 
 // Host-driven loop: one state read per pass.
@@ -1081,8 +1083,8 @@ struct LoopGraph {
 namespace {
 
 // The whole iteration loop as one CUDA graph:
-//   WHILE (!done) {                      loop_h, set by loop_cond_kernel at the end of a body
-//     step (Nesterov or re-evaluation); evaluate; norms and decisions; loop_cond -> loop_h
+//   WHILE (!done) {                      loop_h, set by the assembly's last block
+//     step (Nesterov or re-evaluation); evaluate; norms, decisions and loop_h in the assembly
 //   }
 // Built once per context and stage layout, relaunched on later runs with the same buffers.
 // SPG_GRAPH_STATS=1: print a body graph's node and edge counts, and how many edges are
@@ -1142,8 +1144,7 @@ bool patch_loop_graph(Context& c, const DevPtrs& p, LoopGraph& lg) {
     }
     bool fine = true;
     try {
-        enqueue_iteration(c, p);
-        launch_loop_cond(p, lg.loop_h, s);
+        enqueue_iteration(c, p, lg.loop_h);
     } catch (const Error&) {
         fine = false;
     }
@@ -1230,8 +1231,7 @@ bool build_loop_graph(Context& c, const DevPtrs& p, LoopGraph& lg) {
     bool fine = true;
     try {
         const int64_t k0 = g_launches;
-        enqueue_iteration(c, p);
-        launch_loop_cond(p, loop_h, s);
+        enqueue_iteration(c, p, loop_h);
         lg.body_kernels = g_launches - k0;
     } catch (const Error&) {
         fine = false;

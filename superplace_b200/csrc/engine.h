@@ -259,8 +259,8 @@ void launch_scatter(const DevPtrs& p, int role, cudaStream_t s);
 void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s);
 // the loop's evaluation tail: the assembly at u = R_U into g = R_G with the step's norms
 // and the per-iteration decisions in the same launch
-void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s);
-void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s);
+// the loop's fused assembly; in graph mode it also sets the WHILE node's condition
+void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, cudaGraphConditionalHandle loop_cond = 0);
 // the loop pass's position step (the Nesterov step, or the re-evaluation step when the last
 // decisions asked for one) with the density scatter of the new positions fused in; the
 // evaluation that follows accumulates only the rest list

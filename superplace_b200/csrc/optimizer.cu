@@ -505,8 +505,10 @@ __device__ __forceinline__ void assemble_node(const DevPtrs& p, int k, float lam
 // l2Norm: nesterov.cpp:25-45) from the values it holds, and its last block runs the redo test
 // (nesterov.cpp:148-157) and the decisions after the evaluation's finalize.
 template <bool FUSE>
+// loop_cond (graph mode, FUSE): the enclosing WHILE node's handle; the last block sets it
+// from the decisions (continue while the stage is neither done nor failed). 0: host loop.
 __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int pos_role, int grad_role,
-                                                              int count_eval) {
+                                                              int count_eval, cudaGraphConditionalHandle loop_cond) {
     pdl_wait();
     pdl_trigger();
     // the evaluated positions, by opt index: the role the update (or scatter) wrote the
@@ -566,16 +568,9 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
         apply_pending_step(&sst);
         finish_evaluation(p, &sst, sums, count_eval);
         decide(p, &sst, sums[5], sums[6], sums[7], sums[8]);
+        if (loop_cond) cudaGraphSetConditional(loop_cond, (sst.done || sst.error) ? 0u : 1u);
     }
     state_copy_out(p.st, &sst);
-}
-
-// Graph mode: the iteration loop continues while the stage is not done.
-__global__ void loop_cond_kernel(DevPtrs p, cudaGraphConditionalHandle loop_cond) {
-    pdl_wait();
-    pdl_trigger();
-    const DevState* st = p.st;
-    cudaGraphSetConditional(loop_cond, (st->done || st->error) ? 0u : 1u);
 }
 
 // The loop's position step with the density scatter of the new positions fused in. One
@@ -854,15 +849,12 @@ void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
 void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s) {
     LAUNCH(assemble_kernel<false>, work_grid(reinterpret_cast<const void*>(assemble_kernel<false>), p.n_opt, RED_THREADS),
            RED_THREADS, p, pos_role, grad_role,
-           count_eval);
+           count_eval, cudaGraphConditionalHandle{0});
 }
-void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s) {
+void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, cudaGraphConditionalHandle loop_cond) {
     LAUNCH(assemble_kernel<true>, work_grid(reinterpret_cast<const void*>(assemble_kernel<true>), p.n_opt, RED_THREADS),
            RED_THREADS, p, static_cast<int>(R_U),
-           static_cast<int>(R_G), 1);
-}
-void launch_loop_cond(const DevPtrs& p, cudaGraphConditionalHandle loop_cond, cudaStream_t s) {
-    LAUNCH(loop_cond_kernel, 1, 1, p, loop_cond);
+           static_cast<int>(R_G), 1, loop_cond);
 }
 // One opt node per thread: the step ends in four fixed-point atomics per node, and a grid
 // of many short blocks keeps enough of them in flight (the step writes no partial sums, so
