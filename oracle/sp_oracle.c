@@ -232,11 +232,13 @@ void spo_accumulate_chunks(const spg_db_view* db, const spo_grid* g, int chunks,
 int spo_fixed_shift(const spg_db_view* db, const spo_grid* g) {
     const int total = db->num_nodes + db->num_fillers;
     const double tw = g->target_density > 1.f ? (double)g->target_density : 1.0;
-    double bound = 0.0;
+    /* four partial sums, node i into acc[i % 4], combined as (0 + 1) + (2 + 3) */
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int i = 0; i < total; ++i) {
         if (is_fixed(db, i) || is_ni(db, i)) continue;
-        bound += (double)db->node_w[i] * (double)db->node_h[i];
+        acc[i & 3] += (double)db->node_w[i] * (double)db->node_h[i];
     }
+    double bound = (acc[0] + acc[1]) + (acc[2] + acc[3]);
     bound *= tw;
     if (!(bound > 0.0)) return 40;
     int e = 0;

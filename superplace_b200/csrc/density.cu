@@ -20,13 +20,17 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// The small density nodes of `list` (count entries), or, with no list, every node i < count
+// whose kind marks it a small density node. The fixed-point sums do not depend on the order.
 __global__ void __launch_bounds__(kThreads) acc_small_kernel(DevPtrs p, const int* list, int count) {
     pdl_wait();
     pdl_trigger();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count) return;
-    const int i = list[t];
-    rasterize(p, p.x[i], p.y[i], p.hw[i], p.hh[i], p.wgt[i], (p.kind[i] & K_FILLER) != 0);
+    const int i = list ? list[t] : t;
+    const uint8_t k = p.kind[i];
+    if (!list && (k & (K_DENSITY | K_LARGE)) != K_DENSITY) return;
+    rasterize(p, p.x[i], p.y[i], p.hw[i], p.hh[i], p.wgt[i], (k & K_FILLER) != 0);
 }
 
 // One block per large node (macros): the block's threads split its footprint's bins.
@@ -182,9 +186,8 @@ __global__ void __launch_bounds__(kThreads) gather_opt_large_kernel(DevPtrs p) {
 __global__ void __launch_bounds__(kThreads) gather_all_small_kernel(DevPtrs p, float* out) {
     pdl_wait();
     pdl_trigger();
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= p.n_dens_small) return;
-    const int i = p.dens_small[t];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= p.total || (p.kind[i] & (K_DENSITY | K_LARGE)) != K_DENSITY) return;  // small density nodes
     float fx, fy;
     gather_node(p, i, fx, fy);
     out[i] = fx;
@@ -207,8 +210,8 @@ __global__ void __launch_bounds__(kThreads) gather_all_large_kernel(DevPtrs p, f
 
 void launch_density_accumulate(const DevPtrs& p, cudaStream_t s) {
     if (p.n_dens_small > 0) {
-        launch_pdl(acc_small_kernel, dim3(ceil_div(p.n_dens_small, kThreads)), dim3(kThreads), 0, s, p,
-                   p.dens_small, p.n_dens_small);
+        launch_pdl(acc_small_kernel, dim3(ceil_div(p.total, kThreads)), dim3(kThreads), 0, s, p,
+                   static_cast<const int*>(nullptr), p.total);
     }
     if (p.n_dens_large > 0) {
         launch_pdl(acc_large_kernel, dim3(p.n_dens_large), dim3(kThreads), 0, s, p, p.dens_large);
@@ -239,7 +242,7 @@ void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s) {
 
 void launch_gather_all(const DevPtrs& p, float* out, cudaStream_t s) {
     if (p.n_dens_small > 0) {
-        launch_pdl(gather_all_small_kernel, dim3(ceil_div(p.n_dens_small, kThreads)), dim3(kThreads), 0, s, p, out);
+        launch_pdl(gather_all_small_kernel, dim3(ceil_div(p.total, kThreads)), dim3(kThreads), 0, s, p, out);
     }
     if (p.n_dens_large > 0) {
         launch_pdl(gather_all_large_kernel, dim3(p.n_dens_large), dim3(kThreads), 0, s, p, out);

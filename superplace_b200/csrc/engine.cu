@@ -332,9 +332,9 @@ struct Context : ContextStreams {
     DevBuf<float> terminal, base, rho, phi, ex, ey, node_map, filler_map;
     std::unique_ptr<PoissonPlan> plan;                      // the current grid's Poisson plan
     std::vector<std::unique_ptr<PoissonPlan>> spare_plans;  // other grid sizes seen (reused)
-    DevBuf<int> dens_small, dens_large;
+    DevBuf<int> dens_large;
     int n_dens_small = 0, n_dens_large = 0;
-    std::vector<int> dens_small_h, dens_large_h;  // host copies, for the per-stage rest lists
+    std::vector<int> dens_large_h;  // host copy (ascending), for the per-stage lists
     DevBuf<int> rest_small, rest_large;
     int n_rest_small = 0, n_rest_large = 0;
     // stage
@@ -349,9 +349,9 @@ struct Context : ContextStreams {
     int4 filler_meta{};
     double filler_area = 0.0;
     float filler_lo_x = 0.f, filler_hi_x = 0.f, filler_lo_y = 0.f, filler_hi_y = 0.f;
-    std::vector<float> hw_h, hh_h, wgt_h;  // per-node footprint data of the current grid
+    DevBuf<uint8_t> flags_d;  // the node flags the current grid was built with
     std::vector<int> slot_start_h;         // node-order pin slots (see DevPtrs::slot_start)
-    std::vector<uint8_t> kind_h;           // host copy of the per-node kernel classes
+
     // host copy of the node positions as last uploaded, while the device copy is unchanged
     std::vector<float> x_mirror, y_mirror;
     bool mirror_valid = false;
@@ -458,7 +458,6 @@ struct Context : ContextStreams {
         p.force = force.p;
         p.pool = pool.p;
         p.vec_stride = vec_stride;
-        p.dens_small = dens_small.p;
         p.dens_large = dens_large.p;
         p.n_dens_small = n_dens_small;
         p.n_dens_large = n_dens_large;
@@ -513,6 +512,77 @@ struct HostTimer {
         if (on) std::fprintf(stderr, "[spg host ms%s]%s\n", tag, line.c_str());
     }
 };
+
+// footprintOf + chargeWeight (bin_grid.cpp:22-62) of one node: half extents after local
+// smoothing (a node narrower or shorter than a bin is widened to it, with scale w/step), the
+// charge weight (the scale, times the target density for macros) and the kernel class
+// (density node, filler, large: a footprint of more than 16 bins). footprint_kernel writes
+// the same values for every node with the same single and double operations.
+struct NodeFootprint {
+    float hw, hh, wgt;
+    uint8_t kind;
+};
+
+NodeFootprint node_footprint(const Context& c, const GridGeom& g, float target, int i) {
+    const float w = c.w[i], h = c.h[i];
+    NodeFootprint r{0.5f * w, 0.5f * h, 0.f, 0};
+    float sx = 1.f, sy = 1.f;
+    if (w < g.step_x) {
+        sx = w / g.step_x;
+        r.hw = 0.5f * g.step_x;
+    }
+    if (h < g.step_y) {
+        sy = h / g.step_y;
+        r.hh = 0.5f * g.step_y;
+    }
+    const float scale = sx * sy;
+    r.wgt = c.filler(i) ? scale : (c.macro(i) ? scale * target : scale);
+    if (!(c.fixed(i) || c.ni(i))) {
+        r.kind = K_DENSITY;
+        if (c.filler(i)) r.kind |= K_FILLER;
+        const double bins = (std::floor(2.0 * r.hw / g.step_x) + 2.0) * (std::floor(2.0 * r.hh / g.step_y) + 2.0);
+        if (bins > 16.0) r.kind |= K_LARGE;
+    }
+    return r;
+}
+
+struct FootprintArgs {
+    const float *w, *h;
+    const uint8_t* flags;
+    int total;
+    float step_x, step_y, target;
+    float *hw, *hh, *wgt;
+    uint8_t* kind;
+};
+
+__global__ void footprint_kernel(FootprintArgs a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.total; i += gridDim.x * blockDim.x) {
+        const float w = a.w[i], h = a.h[i];
+        const uint8_t f = a.flags[i];
+        float sx = 1.f, sy = 1.f, hw = fmul(0.5f, w), hh = fmul(0.5f, h);
+        if (w < a.step_x) {
+            sx = fdiv(w, a.step_x);
+            hw = fmul(0.5f, a.step_x);
+        }
+        if (h < a.step_y) {
+            sy = fdiv(h, a.step_y);
+            hh = fmul(0.5f, a.step_y);
+        }
+        const float scale = fmul(sx, sy);
+        const bool filler = (f & SPG_F_FILLER) != 0;
+        a.wgt[i] = filler ? scale : ((f & SPG_F_MACRO) ? fmul(scale, a.target) : scale);
+        a.hw[i] = hw;
+        a.hh[i] = hh;
+        uint8_t k = 0;
+        if (!(f & (SPG_F_FIXED | SPG_F_NI))) {
+            k = K_DENSITY | (filler ? K_FILLER : 0);
+            const double bx = floor(__ddiv_rn(__dmul_rn(2.0, static_cast<double>(hw)), static_cast<double>(a.step_x)));
+            const double by = floor(__ddiv_rn(__dmul_rn(2.0, static_cast<double>(hh)), static_cast<double>(a.step_y)));
+            if (__dmul_rn(__dadd_rn(bx, 2.0), __dadd_rn(by, 2.0)) > 16.0) k |= K_LARGE;
+        }
+        a.kind[i] = k;
+    }
+}
 
 void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& hx_pos,
                const std::vector<float>& hy_pos) {
@@ -601,62 +671,23 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     }
 
     ht.mark("statics");
-    // footprint data: half extents after local smoothing, charge weight, kernel class (host
-    // copies kept in the context, so their memory is reused stage after stage)
-    std::vector<float>& hw = c.hw_h;
-    std::vector<float>& hh = c.hh_h;
-    std::vector<float>& wgt = c.wgt_h;
-    std::vector<uint8_t>& kind = c.kind_h;
-    std::vector<int>& dsmall = c.dens_small_h;
+    // footprint data (half extents after local smoothing, charge weight, kernel class) is
+    // written on the device by footprint_kernel; the host keeps the fixed-point bound, the
+    // large nodes (only nodes at least a bin wide or tall can be) and the small-node count
     std::vector<int>& dlarge = c.dens_large_h;
-    hw.resize(c.total);
-    hh.resize(c.total);
-    wgt.resize(c.total);
-    kind.assign(c.total, 0);
-    dsmall.clear();
     dlarge.clear();
-    double bound = 0.0;
-    // a node's footprint is a function of its size and flags alone: runs of identical nodes
-    // (the fillers above all) reuse the previous node's values instead of recomputing them
-    float pw = -1.f, ph = -1.f, phw = 0.f, phh = 0.f, pwgt = 0.f;
-    uint8_t pflags = 0, pkind = 0;
+    int n_small = 0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};  // bound partials: node i adds into acc[i % 4]
     for (int i = 0; i < c.total; ++i) {
+        if (c.fixed(i) || c.ni(i)) continue;
         const float w = c.w[i], h = c.h[i];
-        if (!(w == pw && h == ph && c.flags[i] == pflags)) {
-            float sx = 1.f, sy = 1.f;
-            phw = 0.5f * w;
-            phh = 0.5f * h;
-            if (w < g.step_x) {
-                sx = w / g.step_x;
-                phw = 0.5f * g.step_x;
-            }
-            if (h < g.step_y) {
-                sy = h / g.step_y;
-                phh = 0.5f * g.step_y;
-            }
-            const float scale = sx * sy;
-            pwgt = c.filler(i) ? scale : (c.macro(i) ? scale * target : scale);
-            pkind = 0;
-            if (!(c.fixed(i) || c.ni(i))) {
-                pkind = K_DENSITY;
-                if (c.filler(i)) pkind |= K_FILLER;
-                const double bins =
-                    (std::floor(2.0 * phw / g.step_x) + 2.0) * (std::floor(2.0 * phh / g.step_y) + 2.0);
-                if (bins > 16.0) pkind |= K_LARGE;
-            }
-            pw = w;
-            ph = h;
-            pflags = c.flags[i];
-        }
-        hw[i] = phw;
-        hh[i] = phh;
-        wgt[i] = pwgt;
-        if (!pkind) continue;  // fixed or NI: no density
-        bound += static_cast<double>(w) * static_cast<double>(h);
-        kind[i] = pkind;
-        (pkind & K_LARGE ? dlarge : dsmall).push_back(i);
+        acc[i & 3] += static_cast<double>(w) * static_cast<double>(h);
+        const bool large = !(w < g.step_x && h < g.step_y) && (node_footprint(c, g, target, i).kind & K_LARGE);
+        if (large) dlarge.push_back(i);
+        else ++n_small;
     }
     // fixed-point scale: largest s <= 40 with (total charge bound) * 2^s < 2^62
+    double bound = (acc[0] + acc[1]) + (acc[2] + acc[3]);
     bound *= target > 1.f ? static_cast<double>(target) : 1.0;
     int s = 40;
     if (bound > 0.0) {
@@ -672,13 +703,21 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     cudaStream_t st = c.stream;
     c.terminal.upload(term, st);
     c.base.upload(base, st);
-    c.hw.upload(hw, st);
-    c.hh.upload(hh, st);
-    c.wgt.upload(wgt, st);
-    c.kind.upload(kind, st);
-    c.dens_small.upload(dsmall, st);
+    c.flags_d.upload(c.flags, st);
+    c.hw.alloc(c.total);
+    c.hh.alloc(c.total);
+    c.wgt.alloc(c.total);
+    c.kind.alloc(c.total);
+    if (c.total > 0) {
+        FootprintArgs fa{c.dw.p, c.dh.p, c.flags_d.p, c.total, g.step_x, g.step_y, target,
+                         c.hw.p, c.hh.p, c.wgt.p, c.kind.p};
+        footprint_kernel<<<work_grid(reinterpret_cast<const void*>(footprint_kernel), c.total, RED_THREADS),
+                           RED_THREADS, 0, st>>>(fa);
+        count_launch();
+        SPG_CHECK_LAUNCH();
+    }
     c.dens_large.upload(dlarge, st);
-    c.n_dens_small = static_cast<int>(dsmall.size());
+    c.n_dens_small = n_small;
     c.n_dens_large = static_cast<int>(dlarge.size());
     c.node_fix.alloc(n);
     c.filler_fix.alloc(n);
@@ -783,7 +822,6 @@ void stage_setup(Context& c, int stage) {
     const int nf = c.total - c.num_nodes;
     const int n = k0 + nf;
     c.n_opt = n;
-    const std::vector<uint8_t>& kind = c.kind_h;
     // opt k's clamp box (eplace.cpp:117-133), for the filler constants
     auto box = [&](int i, float& xlo, float& xhi, float& ylo, float& yhi) {
         const float hw = 0.5f * c.w[i], hh = 0.5f * c.h[i];
@@ -792,27 +830,35 @@ void stage_setup(Context& c, int stage) {
         ylo = c.core_ly + hh + kBoundaryEps;
         yhi = hmax(ylo, c.core_hy - hh - kBoundaryEps);
     };
+    // the large opt nodes: the large density nodes (ascending) matched against the opt cells
+    // (ascending) and the filler run
     std::vector<int> olarge;
-    for (int k = 0; k < k0; ++k)
-        if (kind[cells[k]] & K_LARGE) olarge.push_back(k);
+    {
+        size_t q = 0;
+        for (int i : c.dens_large_h) {
+            if (i >= c.num_nodes) {
+                olarge.push_back(k0 + (i - c.num_nodes));
+                continue;
+            }
+            while (q < cells.size() && cells[q] < i) ++q;
+            if (q < cells.size() && cells[q] == i) olarge.push_back(static_cast<int>(q));
+        }
+    }
     // the fillers close the opt set (nodes num_nodes..total-1); when they all share every
-    // attribute the kernels read (size, so clamp box, area and footprint; degree; kind; no
-    // pin slots), pass those once instead of per node
+    // attribute the kernels read (size and flags, so clamp box, area, footprint and kind;
+    // degree; no pin slots), pass those once instead of per node
     bool same = nf > 0;
     {
         const int f0 = c.num_nodes;
-        for (int i = f0; i < c.total; ++i) {
-            if (kind[i] & K_LARGE) olarge.push_back(k0 + (i - f0));
-            if (same)
-                same = c.w[i] == c.w[f0] && c.h[i] == c.h[f0] && kind[i] == kind[f0] &&
-                       c.node_start[i + 1] - c.node_start[i] == c.node_start[f0 + 1] - c.node_start[f0] &&
-                       c.slot_start_h[i] == c.slot_start_h[i + 1] && c.hw_h[i] == c.hw_h[f0] &&
-                       c.hh_h[i] == c.hh_h[f0] && c.wgt_h[i] == c.wgt_h[f0];
-        }
+        for (int i = f0; same && i < c.total; ++i)
+            same = c.w[i] == c.w[f0] && c.h[i] == c.h[f0] && c.flags[i] == c.flags[f0] &&
+                   c.node_start[i + 1] - c.node_start[i] == c.node_start[f0 + 1] - c.node_start[f0] &&
+                   c.slot_start_h[i] == c.slot_start_h[i + 1];
         if (same) {
+            const NodeFootprint fp = node_footprint(c, c.geom, c.geom.target_density, f0);
             c.filler_k0 = k0;
-            c.filler_geom = make_float4(c.hw_h[f0], c.hh_h[f0], c.wgt_h[f0], 0.f);
-            c.filler_meta = make_int4(0, 0, c.node_start[f0 + 1] - c.node_start[f0], static_cast<int>(kind[f0]));
+            c.filler_geom = make_float4(fp.hw, fp.hh, fp.wgt, 0.f);
+            c.filler_meta = make_int4(0, 0, c.node_start[f0 + 1] - c.node_start[f0], static_cast<int>(fp.kind));
             c.filler_area = static_cast<double>(c.w[f0]) * static_cast<double>(c.h[f0]);
             box(f0, c.filler_lo_x, c.filler_hi_x, c.filler_lo_y, c.filler_hi_y);
         } else {
@@ -844,11 +890,15 @@ void stage_setup(Context& c, int stage) {
     // node is movable (or a filler, always in the opt set).
     {
         std::vector<int> rs;
-        for (int i : c.dens_small_h) {
-            if (i >= c.num_nodes) break;  // the list is ascending; fillers are in the opt set
-            const bool in_opt = i < c.num_movable && !c.fixed(i) && !c.ni(i) && stage != SPG_STAGE_FILLER_ONLY &&
+        const GridGeom& g = c.geom;
+        for (int i = 0; i < c.num_nodes; ++i) {  // fillers are always in the opt set
+            if (c.fixed(i) || c.ni(i)) continue;  // not a density node
+            const bool in_opt = i < c.num_movable && stage != SPG_STAGE_FILLER_ONLY &&
                                 !(stage == SPG_STAGE_CGP && c.macro(i));
-            if (!in_opt) rs.push_back(i);
+            if (in_opt) continue;
+            const bool large = !(c.w[i] < g.step_x && c.h[i] < g.step_y) &&
+                               (node_footprint(c, g, g.target_density, i).kind & K_LARGE);
+            if (!large) rs.push_back(i);
         }
         c.rest_small.upload(rs, s);
         c.n_rest_small = static_cast<int>(rs.size());

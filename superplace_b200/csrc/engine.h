@@ -188,7 +188,7 @@ struct DevPtrs {
     // density work lists (node ids): every density node, and the "rest" the loop's step
     // kernel does not rasterize itself (density nodes outside the opt set, and every node
     // whose footprint may exceed 16 bins)
-    const int *dens_small, *dens_large;
+    const int* dens_large;  // the large density nodes (the small ones are found by kind)
     int n_dens_small, n_dens_large;
     const int *rest_small, *rest_large;
     int n_rest_small, n_rest_large;
