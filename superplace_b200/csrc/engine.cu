@@ -335,6 +335,7 @@ struct Context : ContextStreams {
     DevBuf<int> dens_large;
     int n_dens_small = 0, n_dens_large = 0;
     std::vector<int> dens_large_h;  // host copy (ascending), for the per-stage lists
+    bool fillers_alike = false;     // every filler has the same size and degree and no pin slots
     DevBuf<int> rest_small, rest_large;
     int n_rest_small = 0, n_rest_large = 0;
     // stage
@@ -850,10 +851,8 @@ void stage_setup(Context& c, int stage) {
     bool same = nf > 0;
     {
         const int f0 = c.num_nodes;
-        for (int i = f0; same && i < c.total; ++i)
-            same = c.w[i] == c.w[f0] && c.h[i] == c.h[f0] && c.flags[i] == c.flags[f0] &&
-                   c.node_start[i + 1] - c.node_start[i] == c.node_start[f0 + 1] - c.node_start[f0] &&
-                   c.slot_start_h[i] == c.slot_start_h[i + 1];
+        same = same && c.fillers_alike;  // sizes, degrees and pin slots: fixed per netlist
+        for (int i = f0; same && i < c.total; ++i) same = c.flags[i] == c.flags[f0];
         if (same) {
             const NodeFootprint fp = node_footprint(c, c.geom, c.geom.target_density, f0);
             c.filler_k0 = k0;
@@ -1662,6 +1661,15 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
         c.wa_off.upload(off, s);
     }
     ht.mark("slots");
+    {
+        const int f0 = c.num_nodes;
+        bool alike = c.total > f0;
+        for (int i = f0; alike && i < c.total; ++i)
+            alike = c.w[i] == c.w[f0] && c.h[i] == c.h[f0] &&
+                    c.node_start[i + 1] - c.node_start[i] == c.node_start[f0 + 1] - c.node_start[f0] &&
+                    c.slot_start_h[i] == c.slot_start_h[i + 1];
+        c.fillers_alike = alike;
+    }
     c.gpx.alloc(c.num_slots + 1);
     c.gpy.alloc(c.num_slots + 1);
     c.gpx.zero(s);
