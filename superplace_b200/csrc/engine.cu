@@ -21,6 +21,7 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "engine.h"
@@ -514,6 +515,17 @@ struct HostTimer {
     }
 };
 
+// Runs fn(t) for t = 0..n-1, t = 0 on the calling thread and the others on threads of their
+// own; returns once all have finished. Used for host passes whose parts write disjoint data.
+template <typename F>
+void run_parts(int n, F&& fn) {
+    std::vector<std::thread> th;
+    th.reserve(static_cast<size_t>(n > 1 ? n - 1 : 0));
+    for (int t = 1; t < n; ++t) th.emplace_back(fn, t);
+    fn(0);
+    for (auto& x : th) x.join();
+}
+
 // footprintOf + chargeWeight (bin_grid.cpp:22-62) of one node: half extents after local
 // smoothing (a node narrower or shorter than a bin is widened to it, with scale w/step), the
 // charge weight (the scale, times the target density for macros) and the kernel class
@@ -649,7 +661,9 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         rlx[t] = c.row_lx[r];
         rhx[t] = c.row_lx[r] + c.row_step[r] * static_cast<float>(c.row_sites[r]);
     }
-    for (int by = 0; by < dim; ++by) {
+    // bin rows are independent: four threads take every fourth one
+    run_parts(4, [&](int part) {
+    for (int by = part; by < dim; by += 4) {
         const float bly = g.origin_y + by * g.step_y;
         const float bhy = bly + g.step_y;
         size_t lo = 0, hi = static_cast<size_t>(nr);
@@ -670,6 +684,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
             base[static_cast<size_t>(bx) * dim + by] = target * hmax(0.f, area - covered);
         }
     }
+    });
 
     ht.mark("statics");
     // footprint data (half extents after local smoothing, charge weight, kernel class) is
