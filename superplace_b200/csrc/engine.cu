@@ -178,6 +178,32 @@ constexpr float kBoundaryEps = 1e-3f;  // eplace.cpp:38
 
 }  // namespace
 
+// Runs fn(t) for t = 0..n-1, t = 0 on the calling thread and the others on threads of their
+// own; returns once all have finished. Used for host passes whose parts write disjoint data.
+template <typename F>
+void run_parts(int n, F&& fn) {
+    std::vector<std::thread> th;
+    th.reserve(static_cast<size_t>(n > 1 ? n - 1 : 0));
+    for (int t = 1; t < n; ++t) th.emplace_back(fn, t);
+    fn(0);
+    for (auto& x : th) x.join();
+}
+
+// memcpy of a large host buffer split over four threads (a single thread copies a few GB/s,
+// well below what the host link and the host's memory sustain).
+void host_copy(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kSplit = size_t(4) << 20;
+    if (bytes < kSplit) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes / 4 + 4095) & ~size_t(4095);
+    run_parts(4, [&](int t) {
+        const size_t b0 = std::min(bytes, part * t), b1 = std::min(bytes, part * (t + 1));
+        if (b1 > b0) std::memcpy(static_cast<char*>(dst) + b0, static_cast<const char*>(src) + b0, b1 - b0);
+    });
+}
+
 // Pinned staging memory for the host <-> device copies of one context: a copy from pageable
 // memory is staged by the driver through a shared buffer (serialized across threads and
 // synchronous), one from pinned memory is a plain DMA on the context's stream. Regions are
@@ -218,7 +244,7 @@ void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (!bytes) return;
     if (t_staging && t_staging->s == s) {
         void* d = t_staging->reserve(bytes);
-        std::memcpy(d, src, bytes);
+        host_copy(d, src, bytes);
         src = d;
     }
     SPG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
@@ -231,7 +257,7 @@ void download_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s) {
         void* d = t_staging->reserve(bytes);
         SPG_CUDA(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToHost, s));
         SPG_CUDA(host_wait(s));
-        std::memcpy(dst, d, bytes);
+        host_copy(dst, d, bytes);
         return;
     }
     SPG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s));
@@ -355,7 +381,7 @@ struct Context : ContextStreams {
     std::vector<int> slot_start_h;         // node-order pin slots (see DevPtrs::slot_start)
 
     // host copy of the node positions as last uploaded, while the device copy is unchanged
-    std::vector<float> x_mirror, y_mirror;
+    std::vector<float> x_mirror, y_mirror;  // host copy of the non-filler positions (fixed nodes' terminal density)
     bool mirror_valid = false;
     DevBuf<float> opt_lo, opt_hi, force, pool;
     DevBuf<double> opt_area;
@@ -514,17 +540,6 @@ struct HostTimer {
         if (on) std::fprintf(stderr, "[spg host ms%s]%s\n", tag, line.c_str());
     }
 };
-
-// Runs fn(t) for t = 0..n-1, t = 0 on the calling thread and the others on threads of their
-// own; returns once all have finished. Used for host passes whose parts write disjoint data.
-template <typename F>
-void run_parts(int n, F&& fn) {
-    std::vector<std::thread> th;
-    th.reserve(static_cast<size_t>(n > 1 ? n - 1 : 0));
-    for (int t = 1; t < n; ++t) th.emplace_back(fn, t);
-    fn(0);
-    for (auto& x : th) x.join();
-}
 
 // footprintOf + chargeWeight (bin_grid.cpp:22-62) of one node: half extents after local
 // smoothing (a node narrower or shorter than a bin is widened to it, with scale w/step), the
@@ -1374,10 +1389,10 @@ void stage_run(Context& c, int stage, spg_result* res) {
     // constructing EPlace rebuilds the grid with the current flags (gp_stage.cpp:175-177)
     {
         if (!c.mirror_valid) {
-            c.x_mirror.resize(c.total);
-            c.y_mirror.resize(c.total);
-            download_bytes(c.x_mirror.data(), c.x.p, c.total * sizeof(float), s);
-            download_bytes(c.y_mirror.data(), c.y.p, c.total * sizeof(float), s);
+            c.x_mirror.resize(c.num_nodes);
+            c.y_mirror.resize(c.num_nodes);
+            download_bytes(c.x_mirror.data(), c.x.p, c.num_nodes * sizeof(float), s);
+            download_bytes(c.y_mirror.data(), c.y.p, c.num_nodes * sizeof(float), s);
         }
         grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, c.x_mirror, c.y_mirror);
         c.mirror_valid = false;  // the stage moves the positions
@@ -1568,8 +1583,8 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
     cudaStream_t s = c.stream;
     c.x.upload(v->node_x, T, s);
     c.y.upload(v->node_y, T, s);
-    c.x_mirror.assign(v->node_x, v->node_x + T);
-    c.y_mirror.assign(v->node_y, v->node_y + T);
+    c.x_mirror.assign(v->node_x, v->node_x + v->num_nodes);
+    c.y_mirror.assign(v->node_y, v->node_y + v->num_nodes);
     c.mirror_valid = true;
     c.dw.upload(v->node_w, T, s);
     c.dh.upload(v->node_h, T, s);
@@ -1938,8 +1953,8 @@ int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y) {
     spg::CtxScope scope(c);
     spg::upload_bytes(c.x.p, x, c.total * sizeof(float), c.stream);
     spg::upload_bytes(c.y.p, y, c.total * sizeof(float), c.stream);
-    c.x_mirror.assign(x, x + c.total);
-    c.y_mirror.assign(y, y + c.total);
+    c.x_mirror.assign(x, x + c.num_nodes);
+    c.y_mirror.assign(y, y + c.num_nodes);
     c.mirror_valid = true;
     SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
