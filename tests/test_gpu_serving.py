@@ -61,6 +61,41 @@ def test_reloaded_context_matches_a_fresh_one(requests):
         assert np.array_equal(x, xf) and np.array_equal(y, yf)
 
 
+def test_context_alternating_grid_sizes_matches_fresh_contexts(requests):
+    """One context places a 64x64-grid request, a 128x128 one, then the first again: each grid
+    size keeps its own Poisson plan and loop graph, and a later netlist patches the kept
+    graph's kernel arguments. Every placement equals a fresh context's bit for bit."""
+    from superplace_b200 import abi
+
+    order = [requests[0], requests[2], requests[1], requests[0]]
+    assert [g for _, g in order] == [64, 128, 64, 64]
+
+    def run(ctx, db):
+        ctx.set_positions(db.node_x, db.node_y)
+        ctx.set_flags(db.node_flags)
+        r = ctx.run(abi.STAGE_MGP)
+        return r, ctx.positions()
+
+    def params(g):
+        return abi.default_params(gp_bin_dim=g, poisson_precision=serving.choose_precision(g, "auto"))
+
+    fresh = []
+    for db, g in order:
+        c = engine.GpContext(db, params(g))
+        fresh.append(run(c, db))
+        c.close()
+    ctx = None
+    for (db, g), (rf, (xf, yf)) in zip(order, fresh):
+        if ctx is None:
+            ctx = engine.GpContext(db, params(g))
+        else:
+            ctx.load(db, params(g))
+        r, (x, y) = run(ctx, db)
+        assert r.converged == 1 and r.iterations == rf.iterations and r.hpwl == rf.hpwl
+        assert np.array_equal(x, xf) and np.array_equal(y, yf)
+    ctx.close()
+
+
 def test_same_result_alone_and_in_the_mix(requests):
     alone, _ = place_all(requests, 1)
     mix, peak = place_all(requests, 4)
