@@ -717,8 +717,8 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         if (large) dlarge.push_back(i);
         else ++n_small;
     }
-    // fixed-point scale: largest s <= 40 with (total charge bound) * 2^s < 2^62
     double bound = (acc[0] + acc[1]) + (acc[2] + acc[3]);
+    // fixed-point scale: largest s <= 40 with (total charge bound) * 2^s < 2^62
     bound *= target > 1.f ? static_cast<double>(target) : 1.0;
     int s = 40;
     if (bound > 0.0) {
@@ -786,8 +786,6 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     ht.mark("plan");
     c.partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_CAP);
     c.partials.zero(st);
-    SPG_CUDA(host_wait(st));
-    ht.mark("wait");
     c.grid_ready = true;
 }
 
