@@ -100,6 +100,8 @@ void dev_free(void* p, cudaStream_t owner);
 void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s);
 // Device -> host copy, complete on return.
 void download_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s);
+// Two device -> host copies of `bytes` each, complete on return, with one wait.
+void download_pair(void* dst0, const void* src0, void* dst1, const void* src1, size_t bytes, cudaStream_t s);
 // Host wait for the work queued on `s`, sleeping rather than spinning.
 cudaError_t host_wait(cudaStream_t s);
 

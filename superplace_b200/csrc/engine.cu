@@ -250,6 +250,26 @@ void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     SPG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
 }
 
+// Two device -> host copies of `bytes` each, complete on return, with one wait.
+void download_pair(void* dst0, const void* src0, void* dst1, const void* src1, size_t bytes, cudaStream_t s) {
+    if (!bytes) return;
+    if (t_staging && t_staging->s == s) {
+        // one region for both (a second reservation could recycle the first's memory)
+        const size_t half = (bytes + 255) & ~static_cast<size_t>(255);
+        char* d0 = static_cast<char*>(t_staging->reserve(2 * half));
+        char* d1 = d0 + half;
+        SPG_CUDA(cudaMemcpyAsync(d0, src0, bytes, cudaMemcpyDeviceToHost, s));
+        SPG_CUDA(cudaMemcpyAsync(d1, src1, bytes, cudaMemcpyDeviceToHost, s));
+        SPG_CUDA(host_wait(s));
+        host_copy(dst0, d0, bytes);
+        host_copy(dst1, d1, bytes);
+        return;
+    }
+    SPG_CUDA(cudaMemcpyAsync(dst0, src0, bytes, cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(cudaMemcpyAsync(dst1, src1, bytes, cudaMemcpyDeviceToHost, s));
+    SPG_CUDA(host_wait(s));
+}
+
 // Device -> host copy, complete on return.
 void download_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     if (!bytes) return;
@@ -1949,12 +1969,13 @@ int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y) {
     SPG_REQUIRE(ctx && x && y, SPG_E_INVALID, "null argument");
     Context& c = ctx->c;
     spg::CtxScope scope(c);
+    // staged copies: the caller's arrays are free once this returns, and the copies run on
+    // the context's stream ahead of its next work (no wait here)
     spg::upload_bytes(c.x.p, x, c.total * sizeof(float), c.stream);
     spg::upload_bytes(c.y.p, y, c.total * sizeof(float), c.stream);
     c.x_mirror.assign(x, x + c.num_nodes);
     c.y_mirror.assign(y, y + c.num_nodes);
     c.mirror_valid = true;
-    SPG_CUDA(spg::host_wait(c.stream));
     return SPG_OK;
     API_CATCH
 }
@@ -1964,8 +1985,7 @@ int spg_positions_d2h(spg_ctx* ctx, float* x, float* y) {
     SPG_REQUIRE(ctx && x && y, SPG_E_INVALID, "null argument");
     Context& c = ctx->c;
     spg::CtxScope scope(c);
-    spg::download_bytes(x, c.x.p, c.total * sizeof(float), c.stream);
-    spg::download_bytes(y, c.y.p, c.total * sizeof(float), c.stream);
+    spg::download_pair(x, c.x.p, y, c.y.p, c.total * sizeof(float), c.stream);
     return SPG_OK;
     API_CATCH
 }
