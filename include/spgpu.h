@@ -232,7 +232,9 @@ int spg_ctx_create(const spg_db_view* db, const spg_params* params, spg_ctx** ou
 int spg_ctx_load(spg_ctx* ctx, const spg_db_view* db, const spg_params* params);
 int spg_ctx_destroy(spg_ctx* ctx);
 
-/* Upload new centre positions for all num_nodes + num_fillers nodes. */
+/* Upload new centre positions for all num_nodes + num_fillers nodes. The arrays are copied
+ * before the call returns (into the context's pinned staging memory); the device copy runs
+ * on the context's stream ahead of its next work. */
 int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y);
 /* Download the current centre positions of all nodes. */
 int spg_positions_d2h(spg_ctx* ctx, float* x, float* y);
