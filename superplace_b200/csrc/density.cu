@@ -12,6 +12,8 @@
 //
 // Roofline: these kernels are HBM/L2 bound. Algorithmic bytes per evaluation:
 //   scatter 17 B/node + 16 B/bin, rho+tau 28 B/bin, gather 25 B/node.
+#include <cuda_bf16.h>
+
 #include "engine.h"
 
 namespace spg {
@@ -111,6 +113,89 @@ __global__ void __launch_bounds__(RED_THREADS) rho_overflow_kernel(DevPtrs p, in
             p.node_fix[b] = 0ull;
             p.filler_fix[b] = 0ull;
         }
+    }
+    over = block_sum(over);
+    put_partial(p, SLOT_OVERFLOW, over);
+}
+
+// hi/lo BF16 split of v (v = hi + lo to about 16 bits), as the tensor-core solve splits its
+// operands
+__device__ __forceinline__ void split_bf16_pair(float v, uint16_t& hi, uint16_t& lo) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    hi = __bfloat16_as_ushort(h);
+    lo = __bfloat16_as_ushort(l);
+}
+
+// rho and the tau partials (as rho_overflow_kernel, clearing the fixed maps) fused with the
+// first operand split of a one-grid tensor-core Poisson solve (prep_split_kernel with
+// centring): one block per bin row bx. Each thread keeps its bins' rho in registers; the
+// row's FP64 sum is a fixed-order block reduction (thread partials in bin order, warp trees,
+// then the warp sums in order), so the mean, the split planes of rho - mean and the exact
+// row sum are deterministic.
+constexpr int kRhoPrepThreads = 256;
+constexpr int kRhoPrepPer = 4;  // bins per thread: rows up to 1024 bins
+__global__ void __launch_bounds__(kRhoPrepThreads) rho_prep_kernel(DevPtrs p, uint16_t* planes,
+                                                                   int64_t plane_stride, int64_t ld,
+                                                                   float* sums) {
+    pdl_wait();
+    pdl_trigger();
+    __shared__ double wsum[kRhoPrepThreads / 32];
+    __shared__ double row_total;
+    const GridGeom& g = p.geom;
+    const int dim = g.dim;
+    const int row = blockIdx.x, tid = threadIdx.x;
+    const float bin_area_f = fmul(g.step_x, g.step_y);
+    const float inv_area = fdiv(1.0f, bin_area_f);
+    const double area = static_cast<double>(bin_area_f);
+    const double target = static_cast<double>(g.target_density);
+    const size_t base = static_cast<size_t>(row) * dim;
+    double over = 0.0, v = 0.0;
+    float rho[kRhoPrepPer];
+#pragma unroll
+    for (int j = 0; j < kRhoPrepPer; ++j) {
+        const int i = tid + j * kRhoPrepThreads;
+        rho[j] = 0.f;
+        if (i >= dim) continue;
+        const size_t b = base + i;
+        const long long nfix = static_cast<long long>(p.node_fix[b]);
+        const long long ffix = static_cast<long long>(p.filler_fix[b]);
+        const float nd = static_cast<float>(static_cast<double>(nfix) * g.inv_scale);
+        const float fd = static_cast<float>(static_cast<double>(ffix) * g.inv_scale);
+        const float t = p.terminal[b], bs = p.base[b];
+        rho[j] = fmul(fadd(fadd(fadd(nd, fd), t), bs), inv_area);
+        p.rho[b] = rho[j];
+        const double r = __dadd_rn(__dadd_rn(static_cast<double>(nd), static_cast<double>(t)),
+                                   static_cast<double>(bs)) / area;
+        const double d = r - target;
+        over += d > 0.0 ? __dmul_rn(d, area) : 0.0;
+        p.node_fix[b] = 0ull;
+        p.filler_fix[b] = 0ull;
+        v += static_cast<double>(rho[j]);
+    }
+    // the row sum: warp trees, then the warp sums in warp order
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((tid & 31) == 0) wsum[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kRhoPrepThreads / 32; ++w) s += wsum[w];
+        row_total = s;
+        sums[row] = static_cast<float>(s);
+    }
+    __syncthreads();
+    const float mean = static_cast<float>(row_total / dim);
+    uint16_t* hi = planes + row * ld;
+    uint16_t* lo = hi + plane_stride;
+#pragma unroll
+    for (int j = 0; j < kRhoPrepPer; ++j) {
+        const int i = tid + j * kRhoPrepThreads;
+        if (i >= dim) continue;
+        uint16_t h, l;
+        split_bf16_pair(rho[j] - mean, h, l);
+        hi[i] = h;
+        lo[i] = l;
     }
     over = block_sum(over);
     put_partial(p, SLOT_OVERFLOW, over);
@@ -232,6 +317,13 @@ void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_
     const int grid = work_grid(reinterpret_cast<const void*>(rho_overflow_kernel),
                                static_cast<int64_t>(p.geom.dim) * p.geom.dim, RED_THREADS);
     launch_pdl(rho_overflow_kernel, dim3(grid), dim3(RED_THREADS), 0, s, p, write_maps, zero);
+}
+
+void launch_rho_prep(const DevPtrs& p, uint16_t* planes, int64_t plane_stride, int64_t ld, float* sums,
+                     cudaStream_t s) {
+    SPG_REQUIRE(p.geom.dim <= kRhoPrepThreads * kRhoPrepPer && p.geom.dim <= RED_CAP, SPG_E_INVALID,
+                "rho_prep: grid too large");
+    launch_pdl(rho_prep_kernel, dim3(p.geom.dim), dim3(kRhoPrepThreads), 0, s, p, planes, plane_stride, ld, sums);
 }
 
 void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s) {

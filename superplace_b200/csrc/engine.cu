@@ -973,6 +973,18 @@ void stage_setup(Context& c, int stage) {
 // The WA pass 1 depends only on the positions, so it runs on a side stream, overlapping
 // the density -> Poisson chain; the assembly joins both.
 // `stepped`: the step kernel already added the opt nodes' charge (loop evaluations).
+// rho and tau partials from the fixed-point maps (clearing them); with a tensor-core plan
+// the same launch also writes the solve's first operand. Returns whether it did.
+bool rho_and_split(Context& c, const DevPtrs& p, cudaStream_t s) {
+    RhoOperand op{};
+    if (tc_rho_operand(*c.plan, &op)) {
+        launch_rho_prep(p, op.planes, op.plane_stride, op.ld, op.sums, s);
+        return true;
+    }
+    launch_rho_overflow(p, 0, 1, s);
+    return false;
+}
+
 void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count, bool fused_reduce = false,
               bool stepped = false, cudaGraphConditionalHandle loop_cond = 0) {
     cudaStream_t s = c.stream;
@@ -991,8 +1003,8 @@ void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int cou
     }
     if (stepped) launch_density_rest(p, s);
     else launch_density_accumulate(p, s);
-    launch_rho_overflow(p, 0, 1, s);
-    poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s);
+    const bool fused = rho_and_split(c, p, s);
+    poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s, fused);
     launch_gather_opt_large(p, s);
     if (!wa_serial) SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
     if (fused_reduce) launch_assemble_reduce(p, s, loop_cond);
@@ -2278,8 +2290,9 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     spg::launch_scatter(p, spg::R_POS, s);  // the delivered positions again
     t[1] = time([&] { spg::launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s); }, nothing);
     t[2] = (c.n_rest_small + c.n_rest_large) > 0 ? time([&] { spg::launch_density_rest(p, s); }, zero_maps) : 0.0;
-    t[3] = time([&] { spg::launch_rho_overflow(p, 0, 1, s); }, [&] { spg::launch_density_accumulate(p, s); });
-    t[4] = time([&] { spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s); }, nothing);
+    bool fused = false;
+    t[3] = time([&] { fused = spg::rho_and_split(c, p, s); }, [&] { spg::launch_density_accumulate(p, s); });
+    t[4] = time([&] { spg::poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s, fused); }, nothing);
     // the loop's assembly carries the norms and decisions of the reduce step (part 6 = 0)
     t[5] = time([&] {
         spg::launch_gather_opt_large(p, s);

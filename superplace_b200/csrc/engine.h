@@ -242,6 +242,10 @@ void launch_density_accumulate(const DevPtrs& p, cudaStream_t s);
 void launch_density_rest(const DevPtrs& p, cudaStream_t s);
 // rho + tau partials; write_maps also stores the float maps, zero clears the fixed maps
 void launch_rho_overflow(const DevPtrs& p, int write_maps, int zero, cudaStream_t s);
+// rho + tau partials (clearing the fixed maps) and the first operand of a one-grid
+// tensor-core Poisson solve: the split planes of rho's rows minus their means, and the sums
+void launch_rho_prep(const DevPtrs& p, uint16_t* planes, int64_t plane_stride, int64_t ld, float* sums,
+                     cudaStream_t s);
 // force of the large (block-per-node) opt nodes; cells are gathered inside the assembly
 void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s);
 // gather for every density node into a node-indexed 2*total array (parity hook)

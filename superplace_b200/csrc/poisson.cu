@@ -371,10 +371,12 @@ void poisson_plan_destroy(PoissonPlan& pl) {
 }
 
 void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool rho_split_ready) {
     SPG_REQUIRE(batch >= 1 && batch <= pl.batch_cap, SPG_E_CAPACITY, "Poisson: batch exceeds plan");
+    SPG_REQUIRE(!rho_split_ready || (pl.precision == SPG_POISSON_BF16X3 && batch == 1), SPG_E_INVALID,
+                "Poisson: a prepared density operand needs a one-grid tensor-core solve");
     if (pl.precision == SPG_POISSON_BF16X3) {
-        tc_solve(pl, batch, rho, phi, ex, ey, s);
+        tc_solve(pl, batch, rho, phi, ex, ey, s, rho_split_ready);
         return;
     }
     const int X = pl.nx, Y = pl.ny;

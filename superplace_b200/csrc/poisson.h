@@ -59,8 +59,10 @@ void poisson_plan_destroy(PoissonPlan& pl);
 // plan's buffers on its stream (no allocation; the tensor maps stay valid).
 void poisson_plan_set_steps(PoissonPlan& pl, float step_x, float step_y);
 // Device solve of `batch` grids stored back to back.
+// rho_split_ready (tensor-core plans, one grid): the caller already wrote rho's RhoOperand
+// (tc_rho_operand), so the solve starts at its first GEMM
 void poisson_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
-                   cudaStream_t s);
+                   cudaStream_t s, bool rho_split_ready = false);
 
 // ---- FP32 SIMT GEMM "TN": C[m][n] = sum_k A[m*lda+k] * (B[n*ldb+k] - boff[n])
 // (optionally * S[m][n]). Rows m >= split go to C2 (row m - split) so one launch can fill
@@ -107,10 +109,21 @@ void tc_plan_destroy(PoissonPlan& pl);
 // The plan's device error flag (0, or SPG_E_CUDA after a tensor-core solve gave up a bounded
 // pipeline wait), or nullptr for plans without tensor-core GEMMs.
 const int* tc_error_flag(const PoissonPlan& pl);
+// Where a one-grid tensor-core solve takes its first operand: the split BF16 planes of the
+// density rows minus their means (hi plane, lo plane at + plane_stride, row r at r * ld) and
+// the exact FP32 row sums. False for plans without tensor-core GEMMs.
+struct RhoOperand {
+    uint16_t* planes;
+    int64_t plane_stride;
+    int64_t ld;
+    float* sums;
+};
+bool tc_rho_operand(const PoissonPlan& pl, RhoOperand* out);
 // rewrite the split-BF16 planes of the step-dependent rows in place: Sy (rows ny..2ny of
 // [Ay; Sy]) and Sx (rows nx..2nx of [Ax; Sx]); same buffers, same tensor maps
 void tc_plan_refill_sines(PoissonPlan& pl, const std::vector<float>& sy_rows, const std::vector<float>& sx_rows);
+// rho_split_ready: the caller already wrote the RhoOperand of rho (one grid)
 void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
-              cudaStream_t s);
+              cudaStream_t s, bool rho_split_ready = false);
 
 }  // namespace spg

@@ -596,8 +596,18 @@ const int* tc_error_flag(const PoissonPlan& pl) {
     return st ? st->err : nullptr;
 }
 
+bool tc_rho_operand(const PoissonPlan& pl, RhoOperand* out) {
+    if (!pl.tc) return false;
+    const auto* st = static_cast<const TcState*>(pl.tc);
+    out->planes = pl.rho_s;
+    out->plane_stride = static_cast<int64_t>(pl.batch_cap) * pl.nx * pl.ny;
+    out->ld = pl.ny;
+    out->sums = st->sums;
+    return true;
+}
+
 void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
-              cudaStream_t s) {
+              cudaStream_t s, bool rho_split_ready) {
     auto* st = static_cast<TcState*>(pl.tc);
     const int X = pl.nx, Y = pl.ny;
     const int64_t Bc = pl.batch_cap, BX = static_cast<int64_t>(batch) * X, XY = static_cast<int64_t>(X) * Y;
@@ -605,7 +615,7 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
     float* sum_r = st->sums;
     float* sum_t = st->sums + Bc * std::max(X, Y);
     // rho rows minus their means -> split planes (B operand of G1), exact row sums
-    prep_split(rho, static_cast<int>(BX), Y, Y, Y, 1, pl.rho_s, BXc * Y, sum_r, s);
+    if (!rho_split_ready) prep_split(rho, static_cast<int>(BX), Y, Y, Y, 1, pl.rho_s, BXc * Y, sum_r, s);
     // G1: T0t (Y x BX) = Cy . rho'^T in FP32, DC row from the row sums
     TcArgs g1{};
     g1.M = Y; g1.N = static_cast<int>(BX); g1.K = Y;
