@@ -130,9 +130,9 @@ __device__ __forceinline__ void split_bf16_pair(float v, uint16_t& hi, uint16_t&
 // rho and the tau partials (as rho_overflow_kernel, clearing the fixed maps) fused with the
 // first operand split of a one-grid tensor-core Poisson solve (prep_split_kernel with
 // centring): one block per bin row bx. Each thread keeps its bins' rho in registers; the
-// row's FP64 sum is a fixed-order block reduction (thread partials in bin order, warp trees,
-// then the warp sums in order), so the mean, the split planes of rho - mean and the exact
-// row sum are deterministic.
+// row's FP64 sum is the split kernel's fixed-order block reduction (thread partials in bin
+// order, warp trees, then the warp sums in order), so the mean, the split planes of
+// rho - mean and the exact row sum equal the solve's own split bit for bit.
 constexpr int kRhoPrepThreads = 256;
 constexpr int kRhoPrepPer = 4;  // bins per thread: rows up to 1024 bins
 __global__ void __launch_bounds__(kRhoPrepThreads) rho_prep_kernel(DevPtrs p, uint16_t* planes,

@@ -382,28 +382,40 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
 // Row means (FP64) of `seg`-long row segments; writes the split BF16 planes of
 // (value - mean) when `center`, else of the value, and the exact segment sums.
-// One warp per (row, segment); outputs planes[row][col] with lo plane at + plane_stride.
-__global__ void prep_split_kernel(const float* src, int rows, int nseg, int64_t ld, int seg,
-                                  int center, uint16_t* planes, int64_t plane_stride, float* sums) {
+// One block per (row, segment); outputs planes[row][col] with lo plane at + plane_stride.
+// The segment sum is a fixed-order block reduction (each thread's elements in order, warp
+// trees, then the warp sums in order).
+constexpr int kPrepThreads = 256;
+__global__ void __launch_bounds__(kPrepThreads) prep_split_kernel(const float* src, int rows, int nseg, int64_t ld,
+                                                                  int seg, int center, uint16_t* planes,
+                                                                  int64_t plane_stride, float* sums) {
     pdl_wait();
     pdl_trigger();
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= rows * nseg) return;
+    __shared__ double wsum[kPrepThreads / 32];
+    __shared__ float mean_s;
+    const int w = blockIdx.x, tid = threadIdx.x;
     const int r = w % rows, sg = w / rows;
     const float* p = src + r * ld + static_cast<int64_t>(sg) * seg;
     float mean = 0.f;
     if (center) {
         double v = 0.0;
-        for (int i = lane; i < seg; i += 32) v += static_cast<double>(p[i]);
+        for (int i = tid; i < seg; i += kPrepThreads) v += static_cast<double>(p[i]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        mean = static_cast<float>(v / seg);
-        if (lane == 0 && sums) sums[w] = static_cast<float>(v);
+        if ((tid & 31) == 0) wsum[tid >> 5] = v;
+        __syncthreads();
+        if (tid == 0) {
+            double s = 0.0;
+            for (int k = 0; k < kPrepThreads / 32; ++k) s += wsum[k];
+            mean_s = static_cast<float>(s / seg);
+            if (sums) sums[w] = static_cast<float>(s);
+        }
+        __syncthreads();
+        mean = mean_s;
     }
     uint16_t* hi = planes + r * ld + static_cast<int64_t>(sg) * seg;
     uint16_t* lo = hi + plane_stride;
-    for (int i = lane; i < seg; i += 32) {
+    for (int i = tid; i < seg; i += kPrepThreads) {
         uint16_t h, l;
         split_bf16(p[i] - mean, h, l);
         hi[i] = h;
@@ -497,9 +509,8 @@ void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int 
 
 void prep_split(const float* src, int rows, int cols, int64_t ld, int seg, int center, uint16_t* planes,
                 int64_t plane_stride, float* sums, cudaStream_t s) {
-    const int warps = rows * (cols / seg);
-    launch_pdl(prep_split_kernel, dim3(ceil_div(warps, 8)), dim3(256), 0, s, src, rows, cols / seg, ld, seg,
-               center, planes, plane_stride, sums);
+    launch_pdl(prep_split_kernel, dim3(rows * (cols / seg)), dim3(kPrepThreads), 0, s, src, rows, cols / seg, ld,
+               seg, center, planes, plane_stride, sums);
 }
 
 void split_host(const std::vector<float>& v, std::vector<uint16_t>& out) {
