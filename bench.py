@@ -202,8 +202,8 @@ def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision, traffic=None
     """Algorithmic bytes (or flops) of each iteration part per launch, divided by its
     warm-L2 device time. Bytes count every array the part must touch once (FP32/int32);
     fillers share their attributes as launch constants, so only cells read per-node ones:
-      update     48 B per optimised node (u, v, g in; v', u' out; x, y into the node arrays)
-                 + 52 B per cell (meta, geometry, clamp box, node index) + 16 B per bin (the
+      update     40 B per optimised node (u, v, g in; v', u' out) + 60 B per cell (x, y into
+                 the node arrays; meta, geometry, clamp box, node index) + 16 B per bin (the
                  two fixed-point maps it scatters into)
       wa         32 B per pin + 8 B per net (pin ids, offsets, positions in; 2 terms out)
       scatter    25 B per density node outside the opt set + 16 B per bin (only FILLERONLY
@@ -219,7 +219,7 @@ def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision, traffic=None
     cells = db.num_movable
     n_dens = n_opt
     pins, nets, bins = db.num_pins, db.num_nets, dim * dim
-    by = {"update": 48 * n_opt + 52 * cells + 16 * bins, "wa": 32 * pins + 8 * nets,
+    by = {"update": 40 * n_opt + 60 * cells + 16 * bins, "wa": 32 * pins + 8 * nets,
           "scatter": 25 * n_dens + 16 * bins, "rho": 44 * bins,
           "assemble": 32 * n_opt + 40 * cells + 8 * pins + 8 * bins}
     traffic = traffic or {}

@@ -628,9 +628,13 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
                 un[q] = nu[c];
             }
             bad |= !isfinite(nu[0]) || !isfinite(nu[1]);
-            const int i = fill ? p.filler_node0 + k : p.opt_idx[k];
-            p.x[i] = nu[0];
-            p.y[i] = nu[1];
+            // the node arrays: read inside the loop only for cells (WA) and large nodes (their
+            // gather); the fillers' entries are rewritten from R_POS when the stage ends
+            if (!fill || (meta.w & K_LARGE)) {
+                const int i = fill ? p.filler_node0 + k : p.opt_idx[k];
+                p.x[i] = nu[0];
+                p.y[i] = nu[1];
+            }
         } else {
             nu[0] = cur[k];
             nu[1] = cur[n + k];
