@@ -190,10 +190,11 @@ def cpu_baseline_sample(db, workload, iters=8):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each part, from one
 # ncu --set full capture of the 211k-cell workload with the split-BF16 Poisson (caches flushed
 # before each replayed launch, so these are cold-L2 figures; writes that stay in L2 at the end
-# of a launch are not counted). The Poisson part is its six launches of one solve.
+# of a launch are not counted). The Poisson part is its five launches of one solve (its first
+# operand comes from the rho kernel).
 PROFILED_DRAM_BYTES = {
-    ("large", "bf16x3"): {"update": 41.95e6, "wa": 15.52e6, "rho": 6.31e6, "poisson": 14.83e6,
-                          "assemble": 44.49e6,
+    ("large", "bf16x3"): {"update": 41.01e6, "wa": 15.52e6, "rho": 6.31e6, "poisson": 13.77e6,
+                          "assemble": 44.50e6,
                           "source": "profiles/mgp_211k_bf16x3_kernels.md"},
 }
 
