@@ -20,7 +20,10 @@
 // SPG_E_CUDA in the plan's error word, stops issuing, frees its TMEM and returns.
 //
 // DC split (poisson.h): the forward contractions subtract each B row's mean before the
-// split (prep kernels) and restore the DC row exactly in the epilogue.
+// split (prep_split_kernel, one block per row segment; for the engine's one-grid solves the
+// density's split comes from its rho kernel, rho_prep_kernel, with the same reduction order)
+// and restore the DC row exactly in the epilogue. G4 computes phi, xi_x and xi_y in one launch
+// (xi_y as an alternate M region reading its own A and B rows).
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
