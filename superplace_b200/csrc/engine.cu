@@ -387,7 +387,7 @@ struct Context : ContextStreams {
     int n_rest_small = 0, n_rest_large = 0;
     // stage
     int n_opt = 0;
-    DevBuf<int> opt_idx, opt_deg, opt_large, opt_cells;
+    DevBuf<int> opt_idx, opt_large, opt_cells;
     std::vector<int> opt_cells_h;  // the stage's opt cells (host), ascending
     DevBuf<float4> opt_geom;
     DevBuf<int4> opt_meta;
@@ -501,7 +501,6 @@ struct Context : ContextStreams {
         p.filler_hi_y = filler_hi_y;
         p.opt_lo = opt_lo.p;
         p.opt_hi = opt_hi.p;
-        p.opt_deg = opt_deg.p;
         p.opt_area = opt_area.p;
         p.force = force.p;
         p.pool = pool.p;
@@ -822,7 +821,6 @@ struct StageOptArgs {
     float core_lx, core_ly, core_hx, core_hy;
     int* opt_idx;
     float *lo, *hi;
-    int* deg;
     double* area;
     float4* geom;
     int4* meta;
@@ -844,7 +842,6 @@ __global__ void stage_opt_kernel(StageOptArgs a) {
         a.lo[n + k] = ylo;
         a.hi[n + k] = dmax_f(ylo, fsub(fsub(a.core_hy, hh), kBoundaryEps));
         const int d = a.node_start[i + 1] - a.node_start[i];
-        a.deg[k] = d;
         a.area[k] = __dmul_rn(static_cast<double>(w), static_cast<double>(h));
         a.geom[k] = make_float4(a.hw[i], a.hh[i], a.wgt[i], 0.f);
         const bool has_wl = i < a.num_movable;
@@ -918,14 +915,13 @@ void stage_setup(Context& c, int stage) {
     c.opt_idx.alloc(nn);
     c.opt_lo.alloc(2 * nn);
     c.opt_hi.alloc(2 * nn);
-    c.opt_deg.alloc(nn);
     c.opt_area.alloc(nn);
     c.opt_geom.alloc(nn);
     c.opt_meta.alloc(nn);
     if (n > 0) {
         StageOptArgs a{c.opt_cells.p, k0, n, c.num_nodes, c.num_movable, c.dw.p, c.dh.p, c.hw.p, c.hh.p,
                        c.wgt.p, c.node_start_d.p, c.slot_start.p, c.kind.p, c.core_lx, c.core_ly, c.core_hx,
-                       c.core_hy, c.opt_idx.p, c.opt_lo.p, c.opt_hi.p, c.opt_deg.p, c.opt_area.p, c.opt_geom.p,
+                       c.core_hy, c.opt_idx.p, c.opt_lo.p, c.opt_hi.p, c.opt_area.p, c.opt_geom.p,
                        c.opt_meta.p};
         stage_opt_kernel<<<work_grid(reinterpret_cast<const void*>(stage_opt_kernel), n, RED_THREADS),
                            RED_THREADS, 0, s>>>(a);

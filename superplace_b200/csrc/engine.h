@@ -167,7 +167,6 @@ struct DevPtrs {
     const int* opt_idx;
     const float* opt_lo;   // clamp bounds, 2*nOpt (x then y)
     const float* opt_hi;
-    const int* opt_deg;    // nodeDegree of the opt node
     const double* opt_area;
     // stage-static attributes of opt node k packed for one load each:
     //   opt_geom[k] = {hw, hh, wgt, 0} of its node (smoothed half extents, charge weight)
