@@ -49,6 +49,24 @@ def test_mgp_deterministic():
     assert np.array_equal(db1.node_x, db2.node_x) and np.array_equal(db1.node_y, db2.node_y)
 
 
+def test_caller_arrays_are_free_after_the_position_upload():
+    """spg_positions_h2d copies the caller's arrays before it returns: overwriting them right
+    after the upload (before the stage runs) leaves the placement unchanged bit for bit."""
+    db_ref, _, r_ref, _ = run_small()
+    db, _ = golden_small_db(True)
+    ctx = engine.GpContext(db, abi.default_params(gp_bin_dim=64))
+    x, y = db.node_x.copy(), db.node_y.copy()
+    ctx.set_positions(x, y)
+    x[:] = np.nan  # the caller reuses its buffers at once
+    y[:] = -1.0e9
+    ctx.set_flags(db.node_flags)
+    r = ctx.run(abi.STAGE_MGP)
+    px, py = ctx.positions()
+    ctx.close()
+    assert r.converged == 1 and r.iterations == r_ref.iterations and r.hpwl == r_ref.hpwl
+    assert np.array_equal(px, db_ref.node_x) and np.array_equal(py, db_ref.node_y)
+
+
 def test_already_converged_takes_no_step():
     """test/test_eplace.cpp:256-279: tau_0 below target -> zero iterations."""
     db, _ = golden_small_db(False)
