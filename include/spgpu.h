@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SPG_ABI_VERSION 1
+#define SPG_ABI_VERSION 2
 
 /* ---- status codes (map onto the reference's InvariantError kinds, src/util/invariant.h:10-19) */
 #define SPG_OK 0
@@ -152,6 +152,10 @@ typedef struct spg_iter_metrics {
     double delta_hpwl;
     float lambda_mu;
     int64_t evaluations;
+    /* appended in ABI version 2: the reference's max_displacement (its GP never sets it: 0)
+     * and elapsed_ms, the device time since the stage's iteration loop began */
+    float max_displacement;
+    double elapsed_ms;
 } spg_iter_metrics;
 
 /* Filler plan (sp::FillerInfo, src/gp/filler.h:18-25). */

@@ -84,6 +84,7 @@ class IterMetrics(C.Structure):
         ("grad_norm_wl", C.c_float), ("grad_norm_den", C.c_float),
         ("eval_lambda", C.c_float), ("eval_gamma", C.c_float), ("delta_hpwl", C.c_double),
         ("lambda_mu", C.c_float), ("evaluations", C.c_int64),
+        ("max_displacement", C.c_float), ("elapsed_ms", C.c_double),
     ]
 
 

@@ -229,6 +229,8 @@ __device__ void decide_iteration(const DevPtrs& p, DevState* st) {
         m.delta_hpwl = dh;
         m.lambda_mu = mu;
         m.evaluations = st->evals;
+        m.max_displacement = 0.f;  // not set by the reference's GP either
+        m.elapsed_ms = static_cast<double>(global_ns() - st->t0_ns) * 1e-6;
     }
     st->rows = iter + 1;
     const bool filler_only = st->stage == SPG_STAGE_FILLER_ONLY;

@@ -353,10 +353,17 @@ class EPlace:
         self.db = db
         self.ctx = GpContext(db, params)
 
-    def run(self, stage=abi.STAGE_MGP) -> abi.Result:
+    def run(self, stage=abi.STAGE_MGP, metrics: list | None = None) -> abi.Result:
+        """One stage from the PlaceDB's positions and flags. With a `metrics` list, the stage's
+        per-iteration rows are appended to it as (stage name, rows), the input of
+        superplace_b200.metrics.write_metrics_csv (the reference's MetricsSink rows)."""
         self.ctx.set_positions(self.db.node_x, self.db.node_y)
         self.ctx.set_flags(self.db.node_flags)
         r = self.ctx.run(stage)
+        if metrics is not None:
+            from .metrics import STAGE_NAMES
+
+            metrics.append((STAGE_NAMES[stage], self.ctx.metrics(max(r.iterations, 1))))
         x, y = self.db.node_x, self.db.node_y
         if (x.dtype == np.float32 and y.dtype == np.float32 and x.flags.c_contiguous and y.flags.c_contiguous
                 and x.flags.writeable and y.flags.writeable):

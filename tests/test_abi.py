@@ -40,8 +40,8 @@ def test_struct_layouts_match_header():
 int main(void) {
   printf("%zu %zu %zu %zu %zu\n", sizeof(spg_db_view), sizeof(spg_params), sizeof(spg_result),
          sizeof(spg_iter_metrics), sizeof(spg_filler_info));
-  printf("%zu %zu %zu\n", offsetof(spg_db_view, total_row_area), offsetof(spg_params, random_seed),
-         offsetof(spg_iter_metrics, evaluations));
+  printf("%zu %zu %zu %zu\n", offsetof(spg_db_view, total_row_area), offsetof(spg_params, random_seed),
+         offsetof(spg_iter_metrics, evaluations), offsetof(spg_iter_metrics, elapsed_ms));
   return 0;
 }
 """
@@ -55,7 +55,7 @@ int main(void) {
     mine = [C.sizeof(abi.DbView), C.sizeof(abi.Params), C.sizeof(abi.Result),
             C.sizeof(abi.IterMetrics), C.sizeof(abi.FillerInfo),
             abi.DbView.total_row_area.offset, abi.Params.random_seed.offset,
-            abi.IterMetrics.evaluations.offset]
+            abi.IterMetrics.evaluations.offset, abi.IterMetrics.elapsed_ms.offset]
     assert sizes == mine
 
 
@@ -68,7 +68,7 @@ def test_params_defaults_match_reference_config():
 
 
 def test_abi_version():
-    assert engine.lib().spg_abi_version() == 1
+    assert engine.lib().spg_abi_version() == 2
 
 
 @pytest.mark.skipif(engine.device_available(), reason="checks the no-device refusal")

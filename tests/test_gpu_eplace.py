@@ -67,6 +67,28 @@ def test_caller_arrays_are_free_after_the_position_upload():
     assert np.array_equal(px, db_ref.node_x) and np.array_equal(py, db_ref.node_y)
 
 
+def test_metrics_csv_rows_from_the_device(tmp_path):
+    """The stage's metrics rows as metrics.csv (the reference's MetricsSink columns): one row per
+    iteration in order, max_displacement 0 as in the reference's GP, elapsed_ms from the
+    device clock, non-decreasing and positive."""
+    from superplace_b200 import metrics
+
+    db, _ = golden_small_db(True)
+    ep = engine.EPlace(db, abi.default_params(gp_bin_dim=64))
+    collected = []
+    r = ep.run(abi.STAGE_MGP, metrics=collected)
+    assert len(collected) == 1 and collected[0][0] == "mGP"
+    rows = collected[0][1]
+    assert np.array_equal(rows["iter"], np.arange(r.iterations))
+    assert np.all(rows["max_displacement"] == 0.0)
+    assert rows["elapsed_ms"][0] > 0.0 and np.all(np.diff(rows["elapsed_ms"]) >= 0.0)
+    path = tmp_path / "metrics.csv"
+    metrics.write_metrics_csv(str(path), collected)
+    lines = path.read_text().splitlines()
+    assert lines[0] == metrics.HEADER and len(lines) == 1 + r.iterations
+    assert all(ln.startswith("mGP,") for ln in lines[1:])
+
+
 def test_already_converged_takes_no_step():
     """test/test_eplace.cpp:256-279: tau_0 below target -> zero iterations."""
     db, _ = golden_small_db(False)
