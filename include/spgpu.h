@@ -298,6 +298,36 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n);
  * 0 when it ran the host-driven loop (SPG_HOST_LOOP set, or conditional nodes refused). */
 int spg_ctx_graph_loop(const spg_ctx* ctx);
 
+/* ------------------------------------------------------------------ BookShelf files (host)
+ * BookshelfReader::read (src/io/bookshelf_reader.cpp:404-436): the .aux and the .scl, .nodes,
+ * .nets, .pl and .wts files it names, into the PlaceDB layout: nodes reordered stably to
+ * [movable | fixed] (centres; movable nodes taller than 1.5 row heights marked as macros),
+ * pins in file order with offsets from the node centre, both CSR directions, unit net weights
+ * where the .wts gives none. The handle owns the arrays until spg_bookshelf_destroy. */
+typedef struct spg_bookshelf spg_bookshelf;
+int spg_bookshelf_read(const char* aux_path, spg_bookshelf** out);
+/* Message of the calling thread's last failed BookShelf call. */
+const char* spg_bookshelf_last_error(void);
+/* counts[0..6] = num_movable, num_nodes, num_pins, num_nets, num_rows, bytes of the node names
+ * and bytes of the net names (each name NUL-terminated, back to back, in index order). */
+int spg_bookshelf_counts(const spg_bookshelf* b, int64_t* counts);
+/* Copies into caller arrays sized by spg_bookshelf_counts; a NULL pointer skips that array.
+ * orient is the BookShelf orientation code (0..7 = N, E, S, W, FN, FE, FS, FW). */
+int spg_bookshelf_nodes(const spg_bookshelf* b, float* x, float* y, float* w, float* h, uint8_t* flags,
+                        uint8_t* orient, char* names);
+int spg_bookshelf_pins(const spg_bookshelf* b, float* pin_offset_x, float* pin_offset_y, int32_t* pin2node,
+                       int32_t* pin2net, int32_t* net2pin_start, int32_t* flat_net2pin,
+                       int32_t* node2pin_start, int32_t* flat_node2pin);
+int spg_bookshelf_nets(const spg_bookshelf* b, float* weight, char* names);
+int spg_bookshelf_rows(const spg_bookshelf* b, float* ly, float* height, float* lx, float* step,
+                       int32_t* num_sites);
+int spg_bookshelf_destroy(spg_bookshelf* b);
+/* BookshelfWriter::writePl (src/io/bookshelf_writer.cpp:16-37): lower-left corners of the first
+ * num_nodes nodes in index order; names NUL-terminated back to back; orient may be NULL (N). */
+int spg_bookshelf_write_pl(const char* path, int32_t num_nodes, const char* names, const float* x,
+                           const float* y, const float* w, const float* h, const uint8_t* flags,
+                           const uint8_t* orient);
+
 #ifdef __cplusplus
 }
 #endif

@@ -63,6 +63,13 @@ def lib():
         L.spref_set_threads.argtypes = [C.c_int]
         L.spref_max_threads.restype = C.c_int
         L.spref_quiet.argtypes = [C.c_int]
+        L.spref_bookshelf_read.restype = vp
+        L.spref_bookshelf_read.argtypes = [C.c_char_p]
+        L.spref_db_more_counts.argtypes = [vp, C.POINTER(C.c_longlong)]
+        L.spref_db_get_pins.argtypes = [vp, fp, fp, ip, ip, ip, ip, ip, ip]
+        L.spref_db_get_rows.argtypes = [vp, fp, fp, fp, fp, ip]
+        L.spref_db_get_names.argtypes = [vp, vp, vp, C.POINTER(C.c_uint8), fp]
+        L.spref_write_pl.argtypes = [vp, C.c_char_p]
         L.spref_quiet(1)
         _lib = L
     return _lib
@@ -136,6 +143,57 @@ class RefDb:
         keys = ("iterations", "hpwl", "overflow", "converged", "stagnated", "rollback_iter",
                 "evaluations", "elapsed_ms")
         return dict(zip(keys, list(res))), rows[: nrows.value]
+
+
+def bookshelf_read(aux_path):
+    """The reference's BookshelfReader::read (src/io/bookshelf_reader.cpp:433-463) into a RefDb."""
+    h = lib().spref_bookshelf_read(os.fsencode(aux_path))
+    if not h:
+        raise RuntimeError(lib().spref_last_error().decode())
+    r = RefDb.__new__(RefDb)
+    r.h = h
+    return r
+
+
+def bookshelf_arrays(r: RefDb) -> dict:
+    """Every array of a reference PlaceDB that BookShelf reading fills, keyed like PlaceDB."""
+    num_movable, num_nodes, _, num_pins, num_nets = r.counts()
+    more = (C.c_longlong * 3)()
+    lib().spref_db_more_counts(r.h, more)
+    num_rows, node_bytes, net_bytes = (int(v) for v in more)
+    x, y, w, h, flags = r.nodes()
+    out = dict(num_movable=num_movable, num_nodes=num_nodes, node_x=x, node_y=y, node_w=w, node_h=h,
+               node_flags=flags)
+    f32 = lambda n: np.zeros(n, np.float32)  # noqa: E731
+    i32 = lambda n: np.zeros(n, np.int32)  # noqa: E731
+    ox, oy = f32(num_pins), f32(num_pins)
+    p2n, p2net, fn2p, fnd2p = (i32(num_pins) for _ in range(4))
+    n2ps, nd2ps = i32(num_nets + 1), i32(num_nodes + 1)
+    lib().spref_db_get_pins(r.h, abi.fptr(ox), abi.fptr(oy), abi.iptr(p2n), abi.iptr(p2net), abi.iptr(n2ps),
+                            abi.iptr(fn2p), abi.iptr(nd2ps), abi.iptr(fnd2p))
+    out.update(pin_offset_x=ox, pin_offset_y=oy, pin2node=p2n, pin2net=p2net, net2pin_start=n2ps,
+               flat_net2pin=fn2p, node2pin_start=nd2ps, flat_node2pin=fnd2p)
+    ly, hh, lx, st = (f32(num_rows) for _ in range(4))
+    sites = i32(num_rows)
+    lib().spref_db_get_rows(r.h, abi.fptr(ly), abi.fptr(hh), abi.fptr(lx), abi.fptr(st), abi.iptr(sites))
+    out.update(row_ly=ly, row_height=hh, row_lx=lx, row_step=st, row_num_sites=sites)
+    nn, tn = np.zeros(max(node_bytes, 1), np.uint8), np.zeros(max(net_bytes, 1), np.uint8)
+    orient, weight = np.zeros(num_nodes, np.uint8), f32(num_nets)
+    lib().spref_db_get_names(r.h, nn.ctypes.data, tn.ctypes.data, abi.u8ptr(orient), abi.fptr(weight))
+    out.update(node_orient=orient, net_weight=weight,
+               node_names=[s.decode() for s in bytes(nn).split(b"\0")[:num_nodes]],
+               net_names=[s.decode() for s in bytes(tn).split(b"\0")[:num_nets]])
+    core = (C.c_float * 5)()
+    area = C.c_double()
+    lib().spref_db_regions(r.h, core, C.byref(area))
+    out.update(core=tuple(core[:4]), row_height_mode=core[4], total_row_area=area.value)
+    return out
+
+
+def write_pl(r: RefDb, path):
+    """The reference's BookshelfWriter::writePl (src/io/bookshelf_writer.cpp:16-37)."""
+    if lib().spref_write_pl(r.h, os.fsencode(path)):
+        raise RuntimeError(lib().spref_last_error().decode())
 
 
 class RefGrid:

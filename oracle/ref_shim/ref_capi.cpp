@@ -26,6 +26,8 @@
 #include "gp/eplace.h"
 #include "gp/filler.h"
 #include "gp/wa_wirelength.h"
+#include "io/bookshelf_reader.h"
+#include "io/bookshelf_writer.h"
 #include "numeric/optimizer.h"
 #include "numeric/poisson_backend.h"
 #include "spgpu.h"
@@ -410,6 +412,80 @@ int spref_nesterov_quadratic(int n, const float* coef, const float* target, floa
         out[0] = opt->objective();
         out[1] = static_cast<double>(opt->evaluations());
         out[2] = opt->stepSize();
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// ------------------------------------------------------------------ BookShelf
+// sp::BookshelfReader::read (src/io/bookshelf_reader.cpp) into a new PlaceDB handle.
+void* spref_bookshelf_read(const char* aux) {
+    try {
+        auto* r = new RefDb;
+        sp::BookshelfReader reader;
+        reader.read(aux, r->db);
+        return r;
+    } catch (const std::exception& e) {
+        fail(e);
+        return nullptr;
+    }
+}
+
+// counts[0..3] = rows, bytes of node names, bytes of net names (NUL-terminated, back to back)
+void spref_db_more_counts(void* h, long long* counts) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    long long a = 0, b = 0;
+    for (const std::string& s : db.node_name) a += static_cast<long long>(s.size()) + 1;
+    for (const std::string& s : db.net_name) b += static_cast<long long>(s.size()) + 1;
+    counts[0] = static_cast<long long>(db.rows.size());
+    counts[1] = a;
+    counts[2] = b;
+}
+
+void spref_db_get_pins(void* h, float* ox, float* oy, int* pin2node, int* pin2net, int* net2pin_start,
+                       int* flat_net2pin, int* node2pin_start, int* flat_node2pin) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    const size_t p = db.pin2node.size();
+    std::memcpy(ox, db.pin_offset_x.data(), p * sizeof(float));
+    std::memcpy(oy, db.pin_offset_y.data(), p * sizeof(float));
+    std::memcpy(pin2node, db.pin2node.data(), p * sizeof(int));
+    std::memcpy(pin2net, db.pin2net.data(), p * sizeof(int));
+    std::memcpy(net2pin_start, db.net2pin_start.data(), db.net2pin_start.size() * sizeof(int));
+    std::memcpy(flat_net2pin, db.flat_net2pin.data(), p * sizeof(int));
+    std::memcpy(node2pin_start, db.node2pin_start.data(), db.node2pin_start.size() * sizeof(int));
+    std::memcpy(flat_node2pin, db.flat_node2pin.data(), p * sizeof(int));
+}
+
+void spref_db_get_rows(void* h, float* ly, float* height, float* lx, float* step, int* sites) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    for (size_t r = 0; r < db.rows.size(); ++r) {
+        ly[r] = db.rows[r].ly;
+        height[r] = db.rows[r].height;
+        lx[r] = db.rows[r].lx;
+        step[r] = db.rows[r].step;
+        sites[r] = db.rows[r].numSites;
+    }
+}
+
+void spref_db_get_names(void* h, char* node_names, char* net_names, unsigned char* orient, float* weight) {
+    const sp::PlaceDB& db = static_cast<RefDb*>(h)->db;
+    for (const std::string& s : db.node_name) {
+        std::memcpy(node_names, s.c_str(), s.size() + 1);
+        node_names += s.size() + 1;
+    }
+    for (const std::string& s : db.net_name) {
+        std::memcpy(net_names, s.c_str(), s.size() + 1);
+        net_names += s.size() + 1;
+    }
+    std::memcpy(orient, db.node_orient.data(), db.node_orient.size());
+    std::memcpy(weight, db.net_weight.data(), db.net_weight.size() * sizeof(float));
+}
+
+// sp::BookshelfWriter::writePl (src/io/bookshelf_writer.cpp) of the handle's PlaceDB.
+int spref_write_pl(void* h, const char* path) {
+    try {
+        sp::BookshelfWriter::writePl(path, static_cast<RefDb*>(h)->db);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);

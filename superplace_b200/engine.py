@@ -84,6 +84,16 @@ def lib():
         L.spg_ctx_stream.argtypes = [vp]
         L.spg_ctx_graph_loop.argtypes = [vp]
         L.spg_ctx_profile.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int]
+        u8p, cp = C.POINTER(C.c_uint8), C.c_char_p
+        L.spg_bookshelf_read.argtypes = [cp, C.POINTER(vp)]
+        L.spg_bookshelf_last_error.restype = cp
+        L.spg_bookshelf_counts.argtypes = [vp, i64p]
+        L.spg_bookshelf_nodes.argtypes = [vp, fp, fp, fp, fp, u8p, u8p, vp]
+        L.spg_bookshelf_pins.argtypes = [vp, fp, fp, ip, ip, ip, ip, ip, ip]
+        L.spg_bookshelf_nets.argtypes = [vp, fp, vp]
+        L.spg_bookshelf_rows.argtypes = [vp, fp, fp, fp, fp, ip]
+        L.spg_bookshelf_destroy.argtypes = [vp]
+        L.spg_bookshelf_write_pl.argtypes = [cp, C.c_int32, vp, fp, fp, fp, fp, u8p, u8p]
         _lib = L
     return _lib
 
