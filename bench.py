@@ -13,7 +13,8 @@ src/gp/eplace.cpp:310,515).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision bf16x3|fp32] [--workload large|small]
-       python bench.py --poisson-sweep | --precision-study | --serve   (studies: JSON lines of their own)
+       python bench.py --poisson-sweep | --precision-study | --serve | --bookshelf
+                                                                    (studies: JSON lines of their own)
 The default Poisson arithmetic is split-BF16 on tcgen05 (bf16x3); fp32 is the plain FP32 form.
 Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
 """
@@ -568,6 +569,47 @@ def run_serve(args):
     return 0
 
 
+def run_bookshelf(args):
+    """BookShelf I/O on the 211k-cell design written as BookShelf files: the engine library's
+    reader and .pl writer against the reference's own BookshelfReader / BookshelfWriter
+    (oracle/_ref, single-threaded as shipped). Host work only; one JSON line."""
+    import tempfile
+
+    from superplace_b200 import bookshelf
+    db = make_design("large")
+    d = tempfile.mkdtemp(prefix="spg_bookshelf_")
+    aux = bookshelf.write_bookshelf(d, "large", db)
+    size = sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d))
+    reps = max(3, args.steps)
+
+    def med(fn):
+        fn()  # warm the page cache
+        ts = []
+        for _ in range(reps):
+            t = time.perf_counter()
+            fn()
+            ts.append((time.perf_counter() - t) * 1e3)
+        return statistics.median(ts)
+
+    rd = bookshelf.read_bookshelf(aux)
+    line = {"study": "bookshelf", "design": "211k cells, 221k nets, 859k pins (synthetic)",
+            "bytes": size, "threads": len(os.sched_getaffinity(0)), "reps": reps,
+            "read_ms": round(med(lambda: bookshelf.read_bookshelf(aux)), 2),
+            "write_pl_ms": round(med(lambda: bookshelf.write_pl(os.path.join(d, "o.pl"), rd)), 2)}
+    from oracle import ref
+    if ref.available():
+        r = ref.bookshelf_read(aux)
+        line["ref_read_ms"] = round(med(lambda: ref.bookshelf_read(aux)), 2)
+        line["ref_write_pl_ms"] = round(med(lambda: ref.write_pl(r, os.path.join(d, "r.pl"))), 2)
+        line["read_speedup"] = round(line["ref_read_ms"] / line["read_ms"], 2)
+        line["write_pl_speedup"] = round(line["ref_write_pl_ms"] / line["write_pl_ms"], 2)
+    for f in os.listdir(d):
+        os.remove(os.path.join(d, f))
+    os.rmdir(d)
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -584,6 +626,8 @@ def main():
                     help="211k mGP with FP64 / FP32 / BF16x3 Poisson and the CPU reference: one JSON line")
     ap.add_argument("--serve", action="store_true",
                     help="serving loop on Poisson arrival traces: JSON lines, not the bench line")
+    ap.add_argument("--bookshelf", action="store_true",
+                    help="BookShelf read / .pl write on the 211k design against the reference's: one JSON line")
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
     ap.add_argument("--serve-seconds", type=float, default=8.0)
@@ -596,6 +640,8 @@ def main():
         return run_serve(args)
     if args.poisson_sweep:
         return run_poisson_sweep(args)
+    if args.bookshelf:
+        return run_bookshelf(args)
     if args.precision_study:
         return run_precision_study(args)
     if args.impl == "reference":

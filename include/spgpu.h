@@ -322,6 +322,12 @@ int spg_bookshelf_nets(const spg_bookshelf* b, float* weight, char* names);
 int spg_bookshelf_rows(const spg_bookshelf* b, float* ly, float* height, float* lx, float* step,
                        int32_t* num_sites);
 int spg_bookshelf_destroy(spg_bookshelf* b);
+/* BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp:367-401): applies a .pl to nodes
+ * already read, in place. Names are NUL-terminated back to back (the first of equal names
+ * takes the line); x, y become lower-left + half the size, orient takes the code after ':' and
+ * a token containing FIXED sets SPG_F_FIXED in flags (the nodes are not reordered). */
+int spg_bookshelf_apply_pl(const char* path, int32_t num_nodes, const char* names, const float* w, const float* h,
+                           float* x, float* y, uint8_t* flags, uint8_t* orient);
 /* BookshelfWriter::writePl (src/io/bookshelf_writer.cpp:16-37): lower-left corners of the first
  * num_nodes nodes in index order; names NUL-terminated back to back; orient may be NULL (N). */
 int spg_bookshelf_write_pl(const char* path, int32_t num_nodes, const char* names, const float* x,

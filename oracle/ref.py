@@ -70,6 +70,7 @@ def lib():
         L.spref_db_get_rows.argtypes = [vp, fp, fp, fp, fp, ip]
         L.spref_db_get_names.argtypes = [vp, vp, vp, C.POINTER(C.c_uint8), fp]
         L.spref_write_pl.argtypes = [vp, C.c_char_p]
+        L.spref_read_placement.argtypes = [vp, C.c_char_p]
         L.spref_quiet(1)
         _lib = L
     return _lib
@@ -188,6 +189,12 @@ def bookshelf_arrays(r: RefDb) -> dict:
     lib().spref_db_regions(r.h, core, C.byref(area))
     out.update(core=tuple(core[:4]), row_height_mode=core[4], total_row_area=area.value)
     return out
+
+
+def read_placement(r: RefDb, path):
+    """The reference's BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp:367-401)."""
+    if lib().spref_read_placement(r.h, os.fsencode(path)):
+        raise RuntimeError(lib().spref_last_error().decode())
 
 
 def write_pl(r: RefDb, path):

@@ -482,6 +482,17 @@ void spref_db_get_names(void* h, char* node_names, char* net_names, unsigned cha
     std::memcpy(weight, db.net_weight.data(), db.net_weight.size() * sizeof(float));
 }
 
+// sp::BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp) into the handle's PlaceDB.
+int spref_read_placement(void* h, const char* path) {
+    try {
+        sp::BookshelfReader reader;
+        reader.readPlacement(path, static_cast<RefDb*>(h)->db);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
 // sp::BookshelfWriter::writePl (src/io/bookshelf_writer.cpp) of the handle's PlaceDB.
 int spref_write_pl(void* h, const char* path) {
     try {

@@ -1,7 +1,8 @@
 """BookShelf placement files <-> PlaceDB.
 
-`read_bookshelf` is BookshelfReader::read (src/io/bookshelf_reader.cpp:433-463) and `write_pl`
-is BookshelfWriter::writePl (src/io/bookshelf_writer.cpp:16-37); both run in the engine
+`read_bookshelf` is BookshelfReader::read (src/io/bookshelf_reader.cpp:433-463),
+`read_placement` is BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp:367-401) and
+`write_pl` is BookshelfWriter::writePl (src/io/bookshelf_writer.cpp:16-37); all run in the engine
 library's host code (spg_bookshelf_*, no device work). The returned PlaceDB carries the I/O
 side arrays of the reference's PlaceDB (src/db/place_db.h:30-43) as attributes: node_names,
 net_names (lists of str), node_orient (uint8 codes, ORIENTS order) and net_weight (float32).
@@ -98,6 +99,25 @@ def write_pl(path: str, db: PlaceDB, x=None, y=None) -> None:
     _bs_check(lib().spg_bookshelf_write_pl(os.fsencode(path), n, blob.ctypes.data, abi.fptr(x), abi.fptr(y),
                                            abi.fptr(w), abi.fptr(h), abi.u8ptr(flags),
                                            None if orient is None else abi.u8ptr(orient)))
+
+
+def read_placement(path: str, db: PlaceDB) -> None:
+    """Applies a .pl to a PlaceDB read by read_bookshelf, in place (BookshelfReader::readPlacement,
+    src/io/bookshelf_reader.cpp:367-401): centres from the lower-left corners, orientations, and
+    F_FIXED for "/FIXED" lines. Nodes keep their order, so a node fixed here may sit in the
+    movable segment, as after the reference's call."""
+    n = db.num_nodes
+    for k in ("node_x", "node_y", "node_w", "node_h"):
+        setattr(db, k, np.ascontiguousarray(getattr(db, k), np.float32))
+    db.node_flags = np.ascontiguousarray(db.node_flags, np.uint8)
+    if getattr(db, "node_orient", None) is None:
+        db.node_orient = np.zeros(db.node_x.shape[0], np.uint8)
+    db.node_orient = np.ascontiguousarray(db.node_orient, np.uint8)
+    names = getattr(db, "node_names", None) or [f"o{i}" for i in range(n)]
+    blob = _join_names(names[:n])
+    _bs_check(lib().spg_bookshelf_apply_pl(os.fsencode(path), n, blob.ctypes.data, abi.fptr(db.node_w),
+                                           abi.fptr(db.node_h), abi.fptr(db.node_x), abi.fptr(db.node_y),
+                                           abi.u8ptr(db.node_flags), abi.u8ptr(db.node_orient)))
 
 
 def _num(v) -> str:

@@ -22,14 +22,15 @@
 #include <charconv>
 #include <cstdio>
 #include <cstring>
-#include <fstream>
+#include <exception>
+#include <filesystem>
 #include <map>
 #include <memory>
 #include <numeric>
 #include <stdexcept>
 #include <string>
 #include <string_view>
-#include <unordered_map>
+#include <thread>
 #include <vector>
 
 #include "spgpu.h"
@@ -56,23 +57,33 @@ struct BookshelfDb {
 };
 
 std::string slurp(const std::string& path) {
-    std::ifstream in(path, std::ios::binary);
-    if (!in) throw std::runtime_error("cannot open: " + path);
-    return std::string(std::istreambuf_iterator<char>(in), std::istreambuf_iterator<char>());
+    std::FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open: " + path);
+    std::string text;
+    if (std::fseek(f, 0, SEEK_END) == 0) {
+        const long n = std::ftell(f);
+        if (n > 0) text.resize(static_cast<size_t>(n));
+        std::fseek(f, 0, SEEK_SET);
+    }
+    text.resize(text.empty() ? 0 : std::fread(text.data(), 1, text.size(), f));
+    char buf[1 << 16];
+    for (size_t k; (k = std::fread(buf, 1, sizeof buf, f)) > 0;) text.append(buf, k);  // unsized files
+    std::fclose(f);
+    return text;
 }
 
 bool blank(char c) { return c == ' ' || c == '\t' || c == '\r'; }
 
 // Calls fn(tokens) for every line that is not empty, a '#' comment or a "UCLA " header.
 template <typename F>
-void for_each_line(const std::string& text, F&& fn) {
+void for_each_line(std::string_view text, F&& fn) {
     std::vector<std::string_view> tok;
     size_t pos = 0;
     const size_t n = text.size();
     while (pos < n) {
         size_t end = text.find('\n', pos);
-        if (end == std::string::npos) end = n;
-        std::string_view line(text.data() + pos, end - pos);
+        if (end == std::string_view::npos) end = n;
+        std::string_view line = text.substr(pos, end - pos);
         pos = end + 1;
         while (!line.empty() && blank(line.back())) line.remove_suffix(1);  // trailing blanks
         size_t a = 0;
@@ -91,6 +102,129 @@ void for_each_line(const std::string& text, F&& fn) {
     }
 }
 
+// ------------------------------------------------------------------ parallel pieces
+// Large files are parsed in line-aligned pieces on several threads; each piece's results are
+// joined in file order, so the arrays and the first error reported are those of one pass.
+constexpr size_t kPieceBytes = size_t(1) << 20;
+
+int piece_count(size_t bytes) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    return static_cast<int>(std::max<size_t>(1, std::min<size_t>({bytes / kPieceBytes, hw, 32})));
+}
+
+// The first token of `line` (a view into a larger text, starting at a line start).
+std::string_view first_token(std::string_view text, size_t pos) {
+    while (pos < text.size() && blank(text[pos])) ++pos;
+    size_t e = pos;
+    while (e < text.size() && !blank(text[e]) && text[e] != '\n') ++e;
+    return text.substr(pos, e - pos);
+}
+
+// `parts` pieces covering `text`; every piece after the first starts at a line start (at or
+// after an even split point) whose first token satisfies `opens` (any line when null).
+std::vector<std::string_view> split_pieces(std::string_view text, int parts, bool (*opens)(std::string_view)) {
+    std::vector<size_t> cut{0};
+    const size_t n = text.size();
+    for (int k = 1; k < parts; ++k) {
+        size_t pos = std::max(cut.back(), n / static_cast<size_t>(parts) * static_cast<size_t>(k));
+        while (pos < n) {
+            if (pos > 0 && text[pos - 1] != '\n') {
+                const size_t nl = text.find('\n', pos);
+                pos = nl == std::string_view::npos ? n : nl + 1;
+                continue;
+            }
+            if (!opens || opens(first_token(text, pos))) break;
+            const size_t nl = text.find('\n', pos);
+            pos = nl == std::string_view::npos ? n : nl + 1;
+        }
+        if (pos >= n) break;
+        if (pos > cut.back()) cut.push_back(pos);
+    }
+    cut.push_back(n);
+    std::vector<std::string_view> out;
+    for (size_t k = 0; k + 1 < cut.size(); ++k) out.push_back(text.substr(cut[k], cut[k + 1] - cut[k]));
+    return out;
+}
+
+// Runs fn(k) for k in [0, count) on `count` threads and rethrows the lowest k's exception.
+template <typename F>
+void run_pieces(int count, F&& fn) {
+    std::vector<std::exception_ptr> err(static_cast<size_t>(count));
+    auto body = [&](int k) {
+        try {
+            fn(k);
+        } catch (...) {
+            err[static_cast<size_t>(k)] = std::current_exception();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int k = 1; k < count; ++k) pool.emplace_back(body, k);
+    body(0);
+    for (std::thread& t : pool) t.join();
+    for (const std::exception_ptr& e : err)
+        if (e) std::rethrow_exception(e);
+}
+
+// ------------------------------------------------------------------ name index
+// Open-addressing table from a name to the FIRST index that carries it (the reference's
+// unordered_map::emplace keeps the first). Slots hold 32 bits of the hash beside the index so
+// that most probes compare no string.
+class NameIndex {
+public:
+    explicit NameIndex(const std::vector<std::string>& names) : names_(names) {
+        size_t cap = 16;
+        while (cap < names.size() * 2) cap <<= 1;
+        slots_.assign(cap, 0);
+        mask_ = cap - 1;
+        for (size_t i = 0; i < names.size(); ++i) {
+            const uint64_t h = hash(names[i]);
+            size_t s = h & mask_;
+            for (;; s = (s + 1) & mask_) {
+                const uint64_t v = slots_[s];
+                if (v == 0) {
+                    slots_[s] = (h >> 32 << 32) | (static_cast<uint64_t>(i) + 1);
+                    break;
+                }
+                if ((v >> 32) == (h >> 32) && names_[(v & 0xffffffffu) - 1] == names[i]) break;  // duplicate
+            }
+        }
+    }
+    int32_t find(std::string_view name) const {
+        const uint64_t h = hash(name);
+        for (size_t s = h & mask_;; s = (s + 1) & mask_) {
+            const uint64_t v = slots_[s];
+            if (v == 0) return -1;
+            if ((v >> 32) == (h >> 32)) {
+                const int32_t i = static_cast<int32_t>((v & 0xffffffffu) - 1);
+                if (names_[static_cast<size_t>(i)] == name) return i;
+            }
+        }
+    }
+
+private:
+    // 8 bytes per multiply-xorshift round, then a final avalanche (a splitmix64-style mixer)
+    static uint64_t hash(std::string_view s) {
+        uint64_t h = 0x9e3779b97f4a7c15ull ^ (s.size() * 0xff51afd7ed558ccdull);
+        size_t i = 0;
+        for (; i + 8 <= s.size(); i += 8) {
+            uint64_t w;
+            std::memcpy(&w, s.data() + i, 8);
+            h = (h ^ w) * 0xbf58476d1ce4e5b9ull;
+            h ^= h >> 31;
+        }
+        uint64_t w = 0;
+        std::memcpy(&w, s.data() + i, s.size() - i);
+        h = (h ^ w) * 0x94d049bb133111ebull;
+        h ^= h >> 29;
+        h *= 0xbf58476d1ce4e5b9ull;
+        return h ^ (h >> 32);
+    }
+    const std::vector<std::string>& names_;
+    std::vector<uint64_t> slots_;
+    size_t mask_ = 0;
+};
+
+// ------------------------------------------------------------------ numbers
 float parse_float(std::string_view s) {
     float v = 0.f;
     const auto r = std::from_chars(s.data(), s.data() + s.size(), v);
@@ -176,7 +310,7 @@ Files read_aux(const std::string& aux) {
     return f;
 }
 
-void read_scl(const std::string& path, BookshelfDb& db) {
+void read_scl(const std::string& text, const std::string& path, BookshelfDb& db) {
     bool open = false;
     float ly = 0.f, height = 0.f, lx = 0.f, site_w = 1.f, site_sp = 0.f;
     int sites = 0;
@@ -187,7 +321,7 @@ void read_scl(const std::string& path, BookshelfDb& db) {
         db.row_step.push_back(site_sp > 0.f ? site_sp : site_w);
         db.row_sites.push_back(sites);
     };
-    for_each_line(slurp(path), [&](const std::vector<std::string_view>& tok) {
+    for_each_line(text, [&](const std::vector<std::string_view>& tok) {
         const std::string_view key = tok[0];
         if (key == "CoreRow") {
             open = true;
@@ -238,99 +372,149 @@ float mode_row_height(const BookshelfDb& db) {
     return best_h;
 }
 
-void read_nodes(const std::string& path, BookshelfDb& db) {
-    for_each_line(slurp(path), [&](const std::vector<std::string_view>& tok) {
-        if (tok[0] == "NumNodes" || tok[0] == "NumTerminals") return check_declared(tok);
-        if (tok.size() < 3) return;
-        uint8_t f = 0;
-        if (tok.size() >= 4) {
-            if (tok[3] == "terminal") f = SPG_F_FIXED;
-            else if (tok[3] == "terminal_NI") f = SPG_F_FIXED | SPG_F_NI;
-        }
-        db.node_name.emplace_back(tok[0]);
-        db.w.push_back(parse_float(tok[1]));
-        db.h.push_back(parse_float(tok[2]));
-        db.flags.push_back(f);
+void read_nodes(const std::string& text, BookshelfDb& db) {
+    struct Part {
+        std::vector<std::string> name;
+        std::vector<float> w, h;
+        std::vector<uint8_t> flags;
+    };
+    const std::vector<std::string_view> pieces = split_pieces(text, piece_count(text.size()), nullptr);
+    std::vector<Part> parts(pieces.size());
+    run_pieces(static_cast<int>(pieces.size()), [&](int k) {
+        Part& p = parts[static_cast<size_t>(k)];
+        for_each_line(pieces[static_cast<size_t>(k)], [&](const std::vector<std::string_view>& tok) {
+            if (tok[0] == "NumNodes" || tok[0] == "NumTerminals") return check_declared(tok);
+            if (tok.size() < 3) return;
+            uint8_t f = 0;
+            if (tok.size() >= 4) {
+                if (tok[3] == "terminal") f = SPG_F_FIXED;
+                else if (tok[3] == "terminal_NI") f = SPG_F_FIXED | SPG_F_NI;
+            }
+            p.name.emplace_back(tok[0]);
+            p.w.push_back(parse_float(tok[1]));
+            p.h.push_back(parse_float(tok[2]));
+            p.flags.push_back(f);
+        });
     });
+    for (Part& p : parts) {
+        db.node_name.insert(db.node_name.end(), std::make_move_iterator(p.name.begin()),
+                            std::make_move_iterator(p.name.end()));
+        db.w.insert(db.w.end(), p.w.begin(), p.w.end());
+        db.h.insert(db.h.end(), p.h.begin(), p.h.end());
+        db.flags.insert(db.flags.end(), p.flags.begin(), p.flags.end());
+    }
     const size_t n = db.node_name.size();
     db.x.assign(n, 0.f);
     db.y.assign(n, 0.f);
     db.orient.assign(n, 0);
 }
 
-void read_nets(const std::string& path, BookshelfDb& db) {
-    std::unordered_map<std::string_view, int32_t> index;
-    index.reserve(db.node_name.size() * 2);
-    for (size_t i = 0; i < db.node_name.size(); ++i) index.emplace(db.node_name[i], static_cast<int32_t>(i));
-    int remaining = 0;
-    for_each_line(slurp(path), [&](const std::vector<std::string_view>& tok) {
-        if (tok[0] == "NumNets" || tok[0] == "NumPins") return check_declared(tok);
-        if (tok[0] == "NetDegree") {
-            std::string_view v;
-            if (!value_after_colon(tok, 0, v)) throw std::runtime_error("malformed NetDegree line");
-            remaining = parse_int(v);
-            std::string name = "n" + std::to_string(db.net_name.size());
-            for (size_t i = 0; i + 2 < tok.size(); ++i)
+bool opens_net(std::string_view first) { return first == "NetDegree"; }
+
+// Pieces of a .nets file start at NetDegree lines, so every piece holds whole nets; a piece's
+// nets are numbered locally and shifted when the pieces are joined.
+void read_nets(const std::string& text, const NameIndex& index, BookshelfDb& db) {
+    struct Part {
+        std::vector<int32_t> pin2node, pin_net;
+        std::vector<float> ox, oy;
+        std::vector<std::string> name;  // empty: unnamed, "n<global index>"
+    };
+    const std::vector<std::string_view> pieces = split_pieces(text, piece_count(text.size()), opens_net);
+    std::vector<Part> parts(pieces.size());
+    run_pieces(static_cast<int>(pieces.size()), [&](int k) {
+        Part& p = parts[static_cast<size_t>(k)];
+        int remaining = 0;
+        for_each_line(pieces[static_cast<size_t>(k)], [&](const std::vector<std::string_view>& tok) {
+            if (tok[0] == "NumNets" || tok[0] == "NumPins") return check_declared(tok);
+            if (tok[0] == "NetDegree") {
+                std::string_view v;
+                if (!value_after_colon(tok, 0, v)) throw std::runtime_error("malformed NetDegree line");
+                remaining = parse_int(v);
+                std::string name;
+                for (size_t i = 0; i + 2 < tok.size(); ++i)
+                    if (tok[i] == ":") {
+                        name = std::string(tok[i + 2]);
+                        break;
+                    }
+                p.name.push_back(std::move(name));
+                return;
+            }
+            if (p.name.empty() || remaining <= 0) return;
+            const int32_t node = index.find(tok[0]);
+            if (node < 0) throw std::runtime_error("net references unknown node: " + std::string(tok[0]));
+            float px = 0.f, py = 0.f;
+            for (size_t i = 1; i < tok.size(); ++i)
                 if (tok[i] == ":") {
-                    name = std::string(tok[i + 2]);
+                    if (i + 2 < tok.size()) {
+                        px = parse_float(tok[i + 1]);
+                        py = parse_float(tok[i + 2]);
+                    }
                     break;
                 }
-            db.net_name.push_back(std::move(name));
-            return;
-        }
-        if (db.net_name.empty() || remaining <= 0) return;
-        const auto it = index.find(tok[0]);
-        if (it == index.end()) throw std::runtime_error("net references unknown node: " + std::string(tok[0]));
-        float px = 0.f, py = 0.f;
-        for (size_t i = 1; i < tok.size(); ++i)
-            if (tok[i] == ":") {
-                if (i + 2 < tok.size()) {
-                    px = parse_float(tok[i + 1]);
-                    py = parse_float(tok[i + 2]);
+            p.pin2node.push_back(node);
+            p.ox.push_back(px);
+            p.oy.push_back(py);
+            p.pin_net.push_back(static_cast<int32_t>(p.name.size() - 1));
+            --remaining;
+        });
+    });
+    for (Part& p : parts) {
+        const int32_t base = static_cast<int32_t>(db.net_name.size());
+        for (size_t k = 0; k < p.name.size(); ++k)
+            db.net_name.push_back(p.name[k].empty() ? "n" + std::to_string(base + static_cast<int32_t>(k))
+                                                    : std::move(p.name[k]));
+        db.pin2node.insert(db.pin2node.end(), p.pin2node.begin(), p.pin2node.end());
+        db.ox.insert(db.ox.end(), p.ox.begin(), p.ox.end());
+        db.oy.insert(db.oy.end(), p.oy.begin(), p.oy.end());
+        for (int32_t v : p.pin_net) db.pin_net.push_back(v + base);
+    }
+}
+
+// .pl lines are parsed in pieces into records and applied in file order (a later line for the
+// same node wins, as in one pass).
+void read_pl(const std::string& text, const NameIndex& index, BookshelfDb& db) {
+    struct Rec {
+        int32_t node;
+        float llx, lly;
+        int8_t orient;  // -1: the line sets none
+        uint8_t fixed;
+    };
+    const std::vector<std::string_view> pieces = split_pieces(text, piece_count(text.size()), nullptr);
+    std::vector<std::vector<Rec>> parts(pieces.size());
+    run_pieces(static_cast<int>(pieces.size()), [&](int k) {
+        std::vector<Rec>& out = parts[static_cast<size_t>(k)];
+        for_each_line(pieces[static_cast<size_t>(k)], [&](const std::vector<std::string_view>& tok) {
+            if (tok.size() < 3) return;
+            const int32_t i = index.find(tok[0]);
+            if (i < 0) return;
+            Rec r{i, parse_float(tok[1]), parse_float(tok[2]), -1, 0};
+            for (size_t k2 = 3; k2 < tok.size(); ++k2) {
+                if (tok[k2] == ":") {
+                    if (k2 + 1 < tok.size()) r.orient = static_cast<int8_t>(orient_code(tok[k2 + 1]));
+                } else if (tok[k2].find("FIXED") != std::string_view::npos) {
+                    r.fixed = 1;
                 }
-                break;
             }
-        db.pin2node.push_back(it->second);
-        db.ox.push_back(px);
-        db.oy.push_back(py);
-        db.pin_net.push_back(static_cast<int32_t>(db.net_name.size() - 1));
-        --remaining;
+            out.push_back(r);
+        });
     });
-}
-
-void read_pl(const std::string& path, BookshelfDb& db) {
-    std::unordered_map<std::string_view, int32_t> index;
-    index.reserve(db.node_name.size() * 2);
-    for (size_t i = 0; i < db.node_name.size(); ++i) index.emplace(db.node_name[i], static_cast<int32_t>(i));
-    for_each_line(slurp(path), [&](const std::vector<std::string_view>& tok) {
-        if (tok.size() < 3) return;
-        const auto it = index.find(tok[0]);
-        if (it == index.end()) return;
-        const int32_t i = it->second;
-        db.x[i] = parse_float(tok[1]) + 0.5f * db.w[i];
-        db.y[i] = parse_float(tok[2]) + 0.5f * db.h[i];
-        for (size_t k = 3; k < tok.size(); ++k) {
-            if (tok[k] == ":") {
-                if (k + 1 < tok.size()) db.orient[i] = orient_code(tok[k + 1]);
-            } else if (tok[k].find("FIXED") != std::string_view::npos) {
-                db.flags[i] |= SPG_F_FIXED;
-            }
+    for (const std::vector<Rec>& part : parts)
+        for (const Rec& r : part) {
+            db.x[r.node] = r.llx + 0.5f * db.w[r.node];
+            db.y[r.node] = r.lly + 0.5f * db.h[r.node];
+            if (r.orient >= 0) db.orient[r.node] = static_cast<uint8_t>(r.orient);
+            if (r.fixed) db.flags[r.node] |= SPG_F_FIXED;
         }
-    });
 }
 
-void read_wts(const std::string& path, BookshelfDb& db) {
+void read_wts(const std::string& text, BookshelfDb& db) {
     db.net_weight.assign(db.net_name.size(), 1.f);
-    if (path.empty()) return;
-    std::ifstream probe(path);
-    if (!probe) return;  // a missing .wts means unit weights
-    std::unordered_map<std::string_view, int32_t> index;
-    index.reserve(db.net_name.size() * 2);
-    for (size_t k = 0; k < db.net_name.size(); ++k) index.emplace(db.net_name[k], static_cast<int32_t>(k));
-    for_each_line(slurp(path), [&](const std::vector<std::string_view>& tok) {
+    if (text.empty()) return;
+    const NameIndex index(db.net_name);
+    for_each_line(text, [&](const std::vector<std::string_view>& tok) {
         if (tok.size() < 2) return;
-        const auto it = index.find(tok[0]);
-        if (it != index.end()) db.net_weight[it->second] = parse_float(tok[1]);
+        const int32_t k = index.find(tok[0]);
+        if (k >= 0) db.net_weight[static_cast<size_t>(k)] = parse_float(tok[1]);
     });
 }
 
@@ -394,6 +578,22 @@ void copy_names(const std::vector<std::string>& names, char* out) {
     }
 }
 
+// One .pl line, "%s\t%.6f\t%.6f\t: %s%s\n" of BookshelfWriter::writePl; std::to_chars with a
+// precision prints what printf prints for the same conversion.
+void pl_line(std::string& out, const char* name, double llx, double lly, const char* orient, bool fixed) {
+    char num[400];
+    out += name;
+    for (double v : {llx, lly}) {
+        out += '\t';
+        const auto r = std::to_chars(num, num + sizeof num, v, std::chars_format::fixed, 6);
+        out.append(num, r.ptr);
+    }
+    out += "\t: ";
+    out += orient;
+    if (fixed) out += " /FIXED";
+    out += '\n';
+}
+
 int64_t names_bytes(const std::vector<std::string>& names) {
     int64_t b = 0;
     for (const std::string& s : names) b += static_cast<int64_t>(s.size()) + 1;
@@ -414,13 +614,46 @@ int spg_bookshelf_read(const char* aux_path, spg_bookshelf** out) {
     try {
         if (!aux_path || !out) throw std::invalid_argument("null argument");
         auto b = std::make_unique<spg_bookshelf>();
+        BookshelfDb& db = b->db;
         const Files f = read_aux(aux_path);
-        read_scl(f.scl, b->db);
-        read_nodes(f.nodes, b->db);
-        read_nets(f.nets, b->db);
-        read_pl(f.pl, b->db);
-        read_wts(f.wts, b->db);
-        finish(b->db);
+        // The files are loaded on a second thread while the earlier ones parse; a load error
+        // surfaces when its file's turn comes, so the error reported is that of one pass.
+        struct Loaded {
+            std::string text;
+            std::exception_ptr err;
+        };
+        Loaded nodes, nets, pl, wts;
+        auto load = [](const std::string& path, Loaded& out) {
+            try {
+                out.text = slurp(path);
+            } catch (...) {
+                out.err = std::current_exception();
+            }
+        };
+        std::thread loader([&] {
+            load(f.nodes, nodes);
+            load(f.nets, nets);
+            load(f.pl, pl);
+            std::error_code ec;
+            if (!f.wts.empty() && std::filesystem::exists(f.wts, ec)) load(f.wts, wts);  // none: unit weights
+        });
+        auto take = [&](Loaded& l) -> const std::string& {
+            if (l.err) std::rethrow_exception(l.err);
+            return l.text;
+        };
+        try {
+            read_scl(slurp(f.scl), f.scl, db);
+            loader.join();
+        } catch (...) {
+            loader.join();
+            throw;
+        }
+        read_nodes(take(nodes), db);
+        const NameIndex index(db.node_name);
+        read_nets(take(nets), index, db);
+        read_pl(take(pl), index, db);
+        read_wts(take(wts), db);
+        finish(db);
         *out = b.release();
         return SPG_OK;
     } catch (const std::exception& e) {
@@ -498,24 +731,67 @@ int spg_bookshelf_destroy(spg_bookshelf* b) {
     return SPG_OK;
 }
 
+int spg_bookshelf_apply_pl(const char* path, int32_t num_nodes, const char* names, const float* w, const float* h,
+                           float* x, float* y, uint8_t* flags, uint8_t* orient) {
+    try {
+        if (!path || num_nodes < 0 || (num_nodes > 0 && (!names || !w || !h || !x || !y || !flags || !orient)))
+            throw std::invalid_argument("null argument");
+        BookshelfDb db;
+        const char* name = names;
+        for (int32_t i = 0; i < num_nodes; ++i) {
+            db.node_name.emplace_back(name);
+            name += db.node_name.back().size() + 1;
+        }
+        const size_t n = static_cast<size_t>(num_nodes);
+        db.w.assign(w, w + n);
+        db.h.assign(h, h + n);
+        db.x.assign(x, x + n);
+        db.y.assign(y, y + n);
+        db.flags.assign(flags, flags + n);
+        db.orient.assign(orient, orient + n);
+        read_pl(slurp(path), NameIndex(db.node_name), db);
+        std::copy(db.x.begin(), db.x.end(), x);
+        std::copy(db.y.begin(), db.y.end(), y);
+        std::copy(db.flags.begin(), db.flags.end(), flags);
+        std::copy(db.orient.begin(), db.orient.end(), orient);
+        return SPG_OK;
+    } catch (const std::exception& e) {
+        return bs_fail(e);
+    }
+}
+
 int spg_bookshelf_write_pl(const char* path, int32_t num_nodes, const char* names, const float* x, const float* y,
                            const float* w, const float* h, const uint8_t* flags, const uint8_t* orient) {
     try {
         if (!path || num_nodes < 0 || (num_nodes > 0 && (!names || !x || !y || !w || !h || !flags)))
             throw std::invalid_argument("null argument");
+        std::vector<const char*> name(static_cast<size_t>(num_nodes));
+        size_t bytes = 0;
+        for (int32_t i = 0; i < num_nodes; ++i) {
+            name[static_cast<size_t>(i)] = names + bytes;
+            bytes += std::strlen(names + bytes) + 1;
+        }
+        // node ranges formatted on several threads, written in node order
+        const int parts = piece_count(static_cast<size_t>(num_nodes) * 48);
+        std::vector<std::string> text(static_cast<size_t>(parts));
+        run_pieces(parts, [&](int k) {
+            const int32_t a = static_cast<int32_t>(int64_t(num_nodes) * k / parts);
+            const int32_t b = static_cast<int32_t>(int64_t(num_nodes) * (k + 1) / parts);
+            std::string& out = text[static_cast<size_t>(k)];
+            out.reserve(static_cast<size_t>(b - a) * 48);
+            for (int32_t i = a; i < b; ++i) {
+                const double llx = static_cast<double>(x[i]) - 0.5 * w[i];
+                const double lly = static_cast<double>(y[i]) - 0.5 * h[i];
+                const uint8_t o = orient && orient[i] < 8 ? orient[i] : 0;
+                pl_line(out, name[static_cast<size_t>(i)], llx, lly, kOrient[o], (flags[i] & SPG_F_FIXED) != 0);
+            }
+        });
         std::FILE* f = std::fopen(path, "wb");
         if (!f) throw std::runtime_error(std::string("cannot write: ") + path);
-        std::fputs("UCLA pl 1.0\n# Generated by superPlace\n\n", f);
-        const char* name = names;
-        for (int32_t i = 0; i < num_nodes; ++i) {
-            const double llx = static_cast<double>(x[i]) - 0.5 * w[i];
-            const double lly = static_cast<double>(y[i]) - 0.5 * h[i];
-            const uint8_t o = orient && orient[i] < 8 ? orient[i] : 0;
-            std::fprintf(f, "%s\t%.6f\t%.6f\t: %s%s\n", name, llx, lly, kOrient[o],
-                         (flags[i] & SPG_F_FIXED) ? " /FIXED" : "");
-            name += std::strlen(name) + 1;
-        }
-        if (std::fclose(f) != 0) throw std::runtime_error(std::string("write failed: ") + path);
+        static const char kHead[] = "UCLA pl 1.0\n# Generated by superPlace\n\n";
+        bool ok = std::fwrite(kHead, 1, sizeof kHead - 1, f) == sizeof kHead - 1;
+        for (const std::string& t : text) ok = ok && std::fwrite(t.data(), 1, t.size(), f) == t.size();
+        if (std::fclose(f) != 0 || !ok) throw std::runtime_error(std::string("write failed: ") + path);
         return SPG_OK;
     } catch (const std::exception& e) {
         return bs_fail(e);

@@ -94,6 +94,7 @@ def lib():
         L.spg_bookshelf_rows.argtypes = [vp, fp, fp, fp, fp, ip]
         L.spg_bookshelf_destroy.argtypes = [vp]
         L.spg_bookshelf_write_pl.argtypes = [cp, C.c_int32, vp, fp, fp, fp, fp, u8p, u8p]
+        L.spg_bookshelf_apply_pl.argtypes = [cp, C.c_int32, vp, fp, fp, fp, fp, u8p, u8p]
         _lib = L
     return _lib
 

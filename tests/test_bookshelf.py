@@ -5,7 +5,7 @@ built from its sources into oracle/_ref.
 The designs are written here as text: a hand-made one that walks the format's corner cases
 (comments, CRLF, tabs, glued "Key:value", a row without End, unnamed nets, terminal and
 terminal_NI nodes, /FIXED in the .pl, names missing from the .pl, "12.000000" integers, a .wts
-with unknown names, duplicate names) and seeded random ones with non-integer sizes, offsets
+with unknown names, duplicate names, corners that fall half-way between two 6-decimal values) and seeded random ones with non-integer sizes, offsets
 and positions. Every array must match the reference reader bit for bit, and the .pl writer's
 output byte for byte. The round-trip checks restate test/test_roundtrip.cpp.
 """
@@ -69,7 +69,7 @@ CORNER = {
         "UCLA pl 1.0\n\n"
         "a0\t10\t0\t: N\na1 20.5 12 : FS\nbig 40 12 : E\nt0\t60\t30\t: N /FIXED\n"
         "a2 0 0\nni 5 5 : N /FIXED_NI\na3 1 1 : W /FIXED\na4 30 24 :FN\n"
-        "t1 70 0 : S\nunknown 1 2 : N\nshort 1\na5 12.125 36 : FW\ntall 3 3 : FE\n"
+        "t1 70 0 : S\nunknown 1 2 : N\nshort 1\na5 12.0078125 36.0234375 : FW\ntall 3 3 : FE\n"
         "a1 21 12 : S\n"
     ),
     "c.wts": "UCLA wts 1.0\n\nwide 2.5\nnot_a_net 3\nsingle\nglued 0.5\nn1 4\n",
@@ -272,3 +272,72 @@ def test_errors_match_reference(tmp_path, case):
         with pytest.raises(RuntimeError) as r:
             ref.bookshelf_read(aux)
         assert str(e.value).split("] ", 1)[1] == str(r.value)
+
+
+@pytest.fixture(scope="module")
+def large_bookshelf(tmp_path_factory):
+    """The 211k-cell synthetic design written as BookShelf (about 59 MB): every file above the
+    reader's piece size, so it is parsed in pieces on several threads."""
+    from superplace_b200 import generator
+    d = tmp_path_factory.mktemp("large")
+    return bookshelf.write_bookshelf(str(d), "large", generator.large_design(1002))
+
+
+@needs_ref
+def test_reader_matches_reference_full_size(large_bookshelf, tmp_path):
+    db = bookshelf.read_bookshelf(large_bookshelf)
+    r = ref.bookshelf_read(large_bookshelf)
+    assert_same_arrays(db, ref.bookshelf_arrays(r))
+    mine, theirs = str(tmp_path / "mine.pl"), str(tmp_path / "ref.pl")
+    bookshelf.write_pl(mine, db)
+    ref.write_pl(r, theirs)
+    assert open(mine, "rb").read() == open(theirs, "rb").read()
+
+
+def test_first_error_across_pieces(large_bookshelf, tmp_path):
+    """Two bad pin lines far apart in the .nets file: the one earlier in the file is reported,
+    whichever piece reaches its line first."""
+    src = os.path.dirname(large_bookshelf)
+    for ext in (".aux", ".nodes", ".pl", ".scl", ".wts"):
+        with open(os.path.join(src, "large" + ext), "rb") as f:
+            data = f.read()
+        with open(tmp_path / ("large" + ext), "wb") as f:
+            f.write(data)
+    lines = open(os.path.join(src, "large.nets")).read().split("\n")
+    at = (int(len(lines) * 0.3), int(len(lines) * 0.8))
+    for i, bad in zip(at, ("ghost_early", "ghost_late")):
+        while not lines[i].startswith("\t"):
+            i += 1
+        lines[i] = f"\t{bad}\tI : 0 0"
+    with open(tmp_path / "large.nets", "w") as f:
+        f.write("\n".join(lines))
+    aux = str(tmp_path / "large.aux")
+    with pytest.raises(SpgError, match="unknown node: ghost_early"):
+        bookshelf.read_bookshelf(aux)
+    if ref.available():
+        with pytest.raises(RuntimeError, match="unknown node: ghost_early"):
+            ref.bookshelf_read(aux)
+
+
+@needs_ref
+def test_read_placement_matches_reference(tmp_path):
+    """A second .pl over a design already read (main.cpp's --pl): positions, orientations and
+    /FIXED flags as the reference's readPlacement leaves them, nodes not reordered."""
+    for name, aux in design_cases(tmp_path):
+        db = bookshelf.read_bookshelf(aux)
+        r = ref.bookshelf_read(aux)
+        rng = np.random.default_rng(len(name))
+        lines = ["UCLA pl 1.0", "# second placement", ""]
+        for i in rng.permutation(db.num_nodes)[: db.num_nodes * 3 // 4]:
+            fx = " /FIXED" if rng.random() < 0.1 else ""
+            o = f" : {bookshelf.ORIENTS[int(rng.integers(0, 8))]}" if rng.random() < 0.8 else ""
+            lines.append(f"{db.node_names[i]}\t{rng.uniform(-5, 500):.4f}\t{rng.uniform(0, 90):.3f}{o}{fx}")
+        lines += ["nobody 1 2 : N", f"{db.node_names[0]} 7 8 : FE"]
+        pl = str(tmp_path / f"{name}.second.pl")
+        _write(str(tmp_path), f"{name}.second.pl", "\n".join(lines) + "\n")
+        bookshelf.read_placement(pl, db)
+        ref.read_placement(r, pl)
+        want = ref.bookshelf_arrays(r)
+        for k in ("node_x", "node_y", "node_flags", "node_orient"):
+            assert np.array_equal(getattr(db, k).view(np.uint8), want[k].view(np.uint8)), (name, k)
+        assert db.node_orient[0] == 5
