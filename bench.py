@@ -13,7 +13,7 @@ src/gp/eplace.cpp:310,515).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision bf16x3|fp32] [--workload large|small]
-       python bench.py --poisson-sweep | --precision-study | --serve | --bookshelf
+       python bench.py --poisson-sweep | --precision-study | --serve | --bookshelf | --qp
                                                                     (studies: JSON lines of their own)
 The default Poisson arithmetic is split-BF16 on tcgen05 (bf16x3); fp32 is the plain FP32 form.
 Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
@@ -610,6 +610,38 @@ def run_bookshelf(args):
     return 0
 
 
+def run_qp(args):
+    """B2B quadratic initial placement of the 211k-cell design (QuadraticPlacer::place with
+    configs/default.json's QP keys): the system assembled on the host, BiCGSTAB on the host
+    (all threads) and on the GPU. Both give the same bits; one JSON line. The reference's own
+    QP needs Eigen, which is not installed here, so it has no arm."""
+    from superplace_b200 import qp
+    db = make_design("large")
+    line = {"study": "qp", "design": "211k cells, 221k nets, 859k pins (synthetic)",
+            "threads": len(os.sched_getaffinity(0))}
+    # CUDA start-up (context, modules) outside the timed runs: one small device placement first
+    small = make_design("small")
+    qp.QuadraticPlacer(qp.default_params(device=1, max_iter=1)).place(small)
+    res = {}
+    for name, dev in (("host", 0), ("device", 1)):
+        a = db.copy()
+        t = time.perf_counter()
+        rows = qp.QuadraticPlacer(qp.default_params(device=dev)).place(a)
+        res[name] = (a, rows, (time.perf_counter() - t) * 1e3)
+        line[f"{name}_ms"] = round(res[name][2], 1)
+        line[f"{name}_ms_per_outer_iter"] = [round(v, 1) for v in rows["elapsed_ms"]]
+        line[f"{name}_assemble_ms"] = round(float(np.sum(rows["assemble_ms"])), 1)
+        line[f"{name}_solve_ms"] = round(float(np.sum(rows["solve_ms"])), 1)
+    (ha, hr, _), (da, dr, _) = res["host"], res["device"]
+    line["outer_iters"] = int(dr["iter"].shape[0])
+    line["solver_iters"] = [int(v) for v in dr["solver_iters_x"]] + [int(v) for v in dr["solver_iters_y"]]
+    line["final_hpwl"] = float(dr["hpwl"][-1])
+    line["device_equals_host"] = bool(np.array_equal(da.node_x, ha.node_x) and np.array_equal(da.node_y, ha.node_y))
+    line["speedup"] = round(line["host_ms"] / line["device_ms"], 2)
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -628,6 +660,8 @@ def main():
                     help="serving loop on Poisson arrival traces: JSON lines, not the bench line")
     ap.add_argument("--bookshelf", action="store_true",
                     help="BookShelf read / .pl write on the 211k design against the reference's: one JSON line")
+    ap.add_argument("--qp", action="store_true",
+                    help="B2B quadratic initial placement of the 211k design, host vs GPU solver: one JSON line")
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
     ap.add_argument("--serve-seconds", type=float, default=8.0)
@@ -642,6 +676,8 @@ def main():
         return run_poisson_sweep(args)
     if args.bookshelf:
         return run_bookshelf(args)
+    if args.qp:
+        return run_qp(args)
     if args.precision_study:
         return run_precision_study(args)
     if args.impl == "reference":

@@ -322,6 +322,55 @@ int spg_bookshelf_nets(const spg_bookshelf* b, float* weight, char* names);
 int spg_bookshelf_rows(const spg_bookshelf* b, float* ly, float* height, float* lx, float* step,
                        int32_t* num_sites);
 int spg_bookshelf_destroy(spg_bookshelf* b);
+/* ---------------------------------------------------------------------------------------------
+ * B2B (Kraftwerk2) quadratic initial placement: QuadraticPlacer::place
+ * (src/init/quadratic_placer.cpp:153-228), IInitialPlacer "init" (src/init/initial_placer.h:24-38).
+ * The system is assembled on the host; BiCGSTAB runs on the host or, with device = 1, on the
+ * GPU, with the same bits either way. The fields are the Config keys the placer reads
+ * (src/util/config.h:49-83).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct spg_qp_params {
+    int32_t max_iter;          /* qp_max_iter        20   outer iterations                      */
+    float tol;                 /* qp_tol             1e-6 BiCGSTAB relative residual            */
+    int32_t solver_max_iter;   /* qp_solver_max_iter 100  BiCGSTAB iterations per solve         */
+    float outer_tol;           /* qp_outer_tol       1e-4 stop when HPWL moves less (relative)  */
+    float min_distance;        /* qp_min_distance    1.0  floor of the B2B weight denominator   */
+    int32_t ignore_net_degree; /* ignore_net_degree  100  nets above it are left out            */
+    int32_t threads;           /* host threads; 0 = all (results do not depend on it)           */
+    int32_t device;            /* 1: BiCGSTAB on the GPU (same results); 0: on the host         */
+} spg_qp_params;
+
+/* One outer iteration: the reference's IterMetrics row of the QP (iter, hpwl, grad_norm_wl =
+ * max of the two solver errors, elapsed_ms), plus the solver iterations per axis. */
+typedef struct spg_qp_row {
+    int32_t iter;
+    int32_t solver_iters_x;
+    int32_t solver_iters_y;
+    float err;
+    double hpwl;
+    double elapsed_ms;
+    double assemble_ms; /* of elapsed_ms: bound pins and both systems (host)                 */
+    double solve_ms;    /* of elapsed_ms: both BiCGSTAB solves, copies included              */
+} spg_qp_row;
+
+void spg_qp_default_params(spg_qp_params* p);
+/* Message of the calling thread's last failed QP call. */
+const char* spg_qp_last_error(void);
+/* Places the movable nodes: x, y (num_nodes centres) are read for the fixed nodes and written
+ * for the movable ones (they start at the core centre). net_weight may be NULL (all 1). Up to
+ * cap rows go to rows; *num_rows gets their count. Uses db's CSR, pin offsets, sizes and core. */
+int spg_qp_place(const spg_db_view* db, const float* net_weight, const spg_qp_params* p, float* x, float* y,
+                 spg_qp_row* rows, int32_t cap, int32_t* num_rows);
+/* The linear system of one axis (0 = x, 1 = y) at positions x, y, as the reference assembles it
+ * (src/init/quadratic_placer.cpp:43-112): CSR over the movable nodes (row_start num_movable + 1,
+ * columns ascending) and the right-hand side. *nnz gets the entry count; with cap < *nnz
+ * nothing else is written. */
+int spg_qp_assemble(const spg_db_view* db, const float* net_weight, const spg_qp_params* p, int32_t axis,
+                    const float* x, const float* y, int32_t* row_start, int32_t* col, float* val, float* rhs,
+                    int64_t cap, int64_t* nnz);
+/* computeHPWL (src/db/hpwl.cpp:13-39) at positions x, y on the host. */
+int spg_host_hpwl(const spg_db_view* db, const float* x, const float* y, double* out);
+
 /* BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp:367-401): applies a .pl to nodes
  * already read, in place. Names are NUL-terminated back to back (the first of equal names
  * takes the line); x, y become lower-left + half the size, orient takes the code after ':' and

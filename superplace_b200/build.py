@@ -19,7 +19,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SOURCES = ["engine.cu", "density.cu", "wirelength.cu", "optimizer.cu", "poisson.cu",
-           "poisson_tc.cu", "poisson_static.cu", "bookshelf.cpp"]
+           "poisson_tc.cu", "poisson_static.cu", "bookshelf.cpp", "qp.cpp", "qp_device.cu"]
+# host sources parallelised with OpenMP
+OPENMP = {"qp.cpp"}
 
 
 def _stale(target, deps):
@@ -46,12 +48,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for src in srcs:
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         if force or _stale(obj, [src] + deps):
-            cmd = base + ["-c", src, "-o", obj]
+            omp = ["-Xcompiler", "-fopenmp"] if os.path.basename(src) in OPENMP else []
+            cmd = base + omp + ["-c", src, "-o", obj]
             subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
     subprocess.run([NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-ccbin", "/usr/bin/g++",
-                    "-lcudart_static", "-lrt", "-lpthread", "-ldl"], check=True)
+                    "-lcudart_static", "-lgomp", "-lrt", "-lpthread", "-ldl"], check=True)
     os.replace(tmp, LIB)
     return LIB
 
