@@ -371,6 +371,36 @@ int spg_qp_assemble(const spg_db_view* db, const float* net_weight, const spg_qp
 /* computeHPWL (src/db/hpwl.cpp:13-39) at positions x, y on the host. */
 int spg_host_hpwl(const spg_db_view* db, const float* x, const float* y, double* out);
 
+/* ---------------------------------------------------------------------------------------------
+ * Abacus row legalisation of the standard cells on the host: legalizeCells
+ * (src/lg/abacus.cpp:155-284, AbacusResult src/lg/abacus.h:23-34) and buildAbacusSegments
+ * (src/lg/abacus.cpp:107-153). No device work.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct spg_abacus_result {
+    int32_t precondition_ok; /* 0: a movable macro is not fixed yet; nothing was moved      */
+    int32_t cells;           /* cells to legalise                                           */
+    int32_t failed;          /* cells no segment could take (left where they were)          */
+    int32_t rows;
+    int32_t segments;
+    int32_t rounded_widths;  /* cells whose width is not a whole number of sites            */
+    int32_t selfcheck_overlaps;
+    int32_t selfcheck_off_site;
+    double disp_mean;        /* lower-left displacement of the placed cells                 */
+    double disp_max;
+} spg_abacus_result;
+
+/* Message of the calling thread's last failed Abacus call. */
+const char* spg_abacus_last_error(void);
+/* Legalises the cells: x, y (num_nodes centres) are read for every node and written for the
+ * placed cells. area_weight = 1 weighs cells by area (lg_cell_weight "area"). Uses db's node
+ * sizes and flags, rows and core. SPG_E_INVALID for a row with a non-positive step, height or
+ * site count, or non-finite geometry (nothing moved). */
+int spg_abacus_legalize(const spg_db_view* db, int32_t area_weight, float* x, float* y, spg_abacus_result* out);
+/* The free segments of every row at positions x, y: up to cap of (row, lx, hx); *count gets
+ * how many there are. */
+int spg_abacus_segments(const spg_db_view* db, const float* x, const float* y, int32_t* row, float* lx, float* hx,
+                        int32_t cap, int32_t* count);
+
 /* BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp:367-401): applies a .pl to nodes
  * already read, in place. Names are NUL-terminated back to back (the first of equal names
  * takes the line); x, y become lower-left + half the size, orient takes the code after ':' and

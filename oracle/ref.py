@@ -71,6 +71,8 @@ def lib():
         L.spref_db_get_names.argtypes = [vp, vp, vp, C.POINTER(C.c_uint8), fp]
         L.spref_write_pl.argtypes = [vp, C.c_char_p]
         L.spref_read_placement.argtypes = [vp, C.c_char_p]
+        L.spref_abacus.argtypes = [vp, C.c_int, C.c_int, dp]
+        L.spref_abacus_segments.argtypes = [vp, ip, fp, fp, C.c_int]
         L.spref_quiet(1)
         _lib = L
     return _lib
@@ -189,6 +191,25 @@ def bookshelf_arrays(r: RefDb) -> dict:
     lib().spref_db_regions(r.h, core, C.byref(area))
     out.update(core=tuple(core[:4]), row_height_mode=core[4], total_row_area=area.value)
     return out
+
+
+ABACUS_FIELDS = ("precondition_ok", "cells", "failed", "rows", "segments", "rounded_widths",
+                 "selfcheck_overlaps", "selfcheck_off_site", "disp_mean", "disp_max")
+
+
+def abacus(r: RefDb, area_weight=False, reference_trials=False) -> dict:
+    """The reference's legalizeCells (src/lg/abacus.cpp:155-284) on the RefDb, in place."""
+    res = (C.c_double * 10)()
+    if lib().spref_abacus(r.h, int(area_weight), int(reference_trials), res):
+        raise ValueError(lib().spref_last_error().decode())
+    return {k: (res[i] if i >= 8 else int(res[i])) for i, k in enumerate(ABACUS_FIELDS)}
+
+
+def abacus_segments(r: RefDb):
+    n = lib().spref_abacus_segments(r.h, None, None, None, 0)
+    row, lx, hx = np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros(n, np.float32)
+    lib().spref_abacus_segments(r.h, abi.iptr(row), abi.fptr(lx), abi.fptr(hx), n)
+    return row, lx, hx
 
 
 def read_placement(r: RefDb, path):

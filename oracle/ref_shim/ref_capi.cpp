@@ -28,6 +28,7 @@
 #include "gp/wa_wirelength.h"
 #include "io/bookshelf_reader.h"
 #include "io/bookshelf_writer.h"
+#include "lg/abacus.h"
 #include "numeric/optimizer.h"
 #include "numeric/poisson_backend.h"
 #include "spgpu.h"
@@ -480,6 +481,36 @@ void spref_db_get_names(void* h, char* node_names, char* net_names, unsigned cha
     }
     std::memcpy(orient, db.node_orient.data(), db.node_orient.size());
     std::memcpy(weight, db.net_weight.data(), db.net_weight.size() * sizeof(float));
+}
+
+// sp::legalizeCells (src/lg/abacus.cpp) on the handle's PlaceDB. res[0..9] = preconditionOk,
+// cells, failed, rows, segments, roundedWidths, selfcheckOverlaps, selfcheckOffSite, dispMean,
+// dispMax.
+int spref_abacus(void* h, int area_weight, int reference_trials, double* res) {
+    try {
+        sp::AbacusOptions o;
+        o.areaWeight = area_weight != 0;
+        o.referenceTrials = reference_trials != 0;
+        const sp::AbacusResult r = sp::legalizeCells(static_cast<RefDb*>(h)->db, o);
+        const double v[10] = {double(r.preconditionOk), double(r.cells), double(r.failed), double(r.rows),
+                              double(r.segments), double(r.roundedWidths), double(r.selfcheckOverlaps),
+                              double(r.selfcheckOffSite), r.dispMean, r.dispMax};
+        std::memcpy(res, v, sizeof v);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// sp::buildAbacusSegments: up to cap of (row, lx, hx); returns how many there are.
+int spref_abacus_segments(void* h, int* row, float* lx, float* hx, int cap) {
+    const auto segs = sp::buildAbacusSegments(static_cast<RefDb*>(h)->db);
+    for (int k = 0; k < std::min<int>(cap, static_cast<int>(segs.size())); ++k) {
+        row[k] = segs[static_cast<size_t>(k)].row;
+        lx[k] = segs[static_cast<size_t>(k)].lx;
+        hx[k] = segs[static_cast<size_t>(k)].hx;
+    }
+    return static_cast<int>(segs.size());
 }
 
 // sp::BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp) into the handle's PlaceDB.
