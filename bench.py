@@ -13,7 +13,7 @@ src/gp/eplace.cpp:310,515).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision bf16x3|fp32] [--workload large|small]
-       python bench.py --poisson-sweep | --precision-study | --serve | --bookshelf | --qp
+       python bench.py --poisson-sweep | --precision-study | --serve | --bookshelf | --qp | --flow
                                                                     (studies: JSON lines of their own)
 The default Poisson arithmetic is split-BF16 on tcgen05 (bf16x3); fp32 is the plain FP32 form.
 Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
@@ -642,6 +642,61 @@ def run_qp(args):
     return 0
 
 
+def run_flow(args):
+    """The whole pipeline on the 211k design written as BookShelf files: parse, QP init, mGP
+    (fillers and the device loop), Abacus and the .pl write, through superplace_b200.flow; and
+    the reference's own stages on the same files (oracle/_ref: its reader, initializeFillers,
+    EPlace mGP, legalizeCells, writePl; its QP needs Eigen, so it starts from our QP result).
+    Wall times per stage and HPWL after each; one JSON line."""
+    import tempfile
+
+    from oracle import ref
+    from superplace_b200 import bookshelf, flow
+    db0 = make_design("large")
+    d = tempfile.mkdtemp(prefix="spg_flow_")
+    aux = bookshelf.write_bookshelf(d, "large", db0)
+    # CUDA start-up outside the timed runs
+    flow.place(db=make_design("small"), stages=("init", "gp"))
+    params = abi.default_params(gp_bin_dim=WORKLOADS["large"]["bin_dim"], poisson_precision=abi.POISSON_BF16X3)
+    db, rep = flow.place(aux, out_pl=os.path.join(d, "ours.pl"), params=params)
+    ours = {s["stage"]: {k: (round(v, 3) if isinstance(v, float) else v) for k, v in s.items() if k != "stage"}
+            for s in rep["stages"]}
+    line = {"study": "flow", "design": "211k cells, 221k nets, 859k pins (synthetic), 512x512 bins",
+            "threads": len(os.sched_getaffinity(0)), "ours": ours,
+            "ours_total_ms": round(sum(s["ms"] for s in rep["stages"]), 1)}
+    if ref.available():
+        theirs = {}
+        t = time.perf_counter()
+        r = ref.bookshelf_read(aux)
+        theirs["parse"] = {"ms": round((time.perf_counter() - t) * 1e3, 1)}
+        x = np.zeros(r.counts()[1], np.float32)
+        y = np.zeros_like(x)
+        x[:], y[:] = rep["init_x"], rep["init_y"]
+        r.set_xy(x, y)
+        t = time.perf_counter()
+        r.fillers_init(1.0, 1002)
+        ref.lib().spref_set_threads(len(os.sched_getaffinity(0)))
+        res, _ = r.eplace(abi.default_params(gp_bin_dim=WORKLOADS["large"]["bin_dim"]), abi.STAGE_MGP)
+        theirs["gp"] = {"ms": round((time.perf_counter() - t) * 1e3, 1), "iterations": int(res["iterations"]),
+                        "hpwl": res["hpwl"], "overflow": res["overflow"]}
+        t = time.perf_counter()
+        lg = ref.abacus(r)
+        theirs["lg"] = {"ms": round((time.perf_counter() - t) * 1e3, 1), "hpwl": r.hpwl(), "failed": lg["failed"],
+                        "disp_mean": lg["disp_mean"]}
+        t = time.perf_counter()
+        ref.write_pl(r, os.path.join(d, "ref.pl"))
+        theirs["write"] = {"ms": round((time.perf_counter() - t) * 1e3, 1)}
+        line["reference"] = theirs
+        line["reference_note"] = "init: the reference's QP needs Eigen (absent); it starts from our QP placement"
+        line["reference_total_ms_without_init"] = round(sum(v["ms"] for v in theirs.values()), 1)
+        line["ours_total_ms_without_init"] = round(line["ours_total_ms"] - ours["init"]["ms"], 1)
+    for f in os.listdir(d):
+        os.remove(os.path.join(d, f))
+    os.rmdir(d)
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -662,6 +717,8 @@ def main():
                     help="BookShelf read / .pl write on the 211k design against the reference's: one JSON line")
     ap.add_argument("--qp", action="store_true",
                     help="B2B quadratic initial placement of the 211k design, host vs GPU solver: one JSON line")
+    ap.add_argument("--flow", action="store_true",
+                    help="parse, QP init, mGP, Abacus and .pl write on the 211k design, ours and the reference's: one JSON line")
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
     ap.add_argument("--serve-seconds", type=float, default=8.0)
@@ -678,6 +735,8 @@ def main():
         return run_bookshelf(args)
     if args.qp:
         return run_qp(args)
+    if args.flow:
+        return run_flow(args)
     if args.precision_study:
         return run_precision_study(args)
     if args.impl == "reference":
