@@ -34,7 +34,7 @@ def test_flow_without_gp(small_aux, tmp_path):
 def test_flow_with_gp(small_aux, tmp_path):
     from superplace_b200 import abi
     db, rep = flow.place(small_aux, out_pl=str(tmp_path / "out.pl"),
-                         params=abi.default_params(gp_bin_dim=64, poisson_precision=abi.POISSON_BF16X3))
+                         params=abi.default_params(gp_bin_dim=64))  # split-BF16 needs 128-multiples
     st = {s["stage"]: s for s in rep["stages"]}
     assert "stopped" not in rep and list(st) == ["parse", "init", "gp", "lg", "write"]
     assert st["init"]["device"] == 1
