@@ -200,12 +200,12 @@ void assemble(const Problem& P, const Axis& a, const std::vector<int32_t>& lo, c
         for (int c = 0; c < kChunks; ++c)
             for (const Entry& en : bucket[static_cast<size_t>(c) * kChunks + rb]) sorted[next[en.row - r0]++] = en;
         std::vector<Entry>& out = block_rows[rb];
-        std::vector<Entry> row;
+        out.resize(total + static_cast<size_t>(r1 - r0));  // at most every entry plus a diagonal per row
+        size_t o = 0;
         for (int32_t r = r0; r < r1; ++r) {
-            row.clear();
-            row.push_back(Entry{r, r, 0.f});  // the seeded diagonal precedes every emitted entry
-            row.insert(row.end(), sorted.begin() + cnt[r - r0], sorted.begin() + cnt[r - r0 + 1]);
-            for (size_t j = 1; j < row.size(); ++j) {  // stable insertion sort by column
+            Entry* row = sorted.data() + cnt[r - r0];
+            const size_t len = static_cast<size_t>(cnt[r - r0 + 1] - cnt[r - r0]);
+            for (size_t j = 1; j < len; ++j) {  // stable insertion sort by column, in place
                 const Entry en = row[j];
                 size_t h = j;
                 for (; h > 0 && row[h - 1].col > en.col; --h) row[h] = row[h - 1];
@@ -213,21 +213,34 @@ void assemble(const Problem& P, const Axis& a, const std::vector<int32_t>& lo, c
             }
             float rhs = 0.f;
             size_t i = 0;
-            for (; i < row.size() && row[i].col == kRhs; ++i) rhs += row[i].val;
-            const size_t before = out.size();
-            while (i < row.size()) {
-                const int32_t c = row[i].col;
-                float v = row[i].val;
-                for (++i; i < row.size() && row[i].col == c; ++i) v += row[i].val;
+            for (; i < len && row[i].col == kRhs; ++i) rhs += row[i].val;
+            const size_t before = o;
+            // the reference seeds a zero diagonal before every emitted entry: the diagonal's sum
+            // starts from 0 (0 + w is w exactly), and the slot exists even with nothing emitted
+            bool diag = false;
+            auto put = [&](int32_t c, float v) {
                 if (c == r && v == 0.f) {  // a movable node with no connection: a tiny pull to where it is
                     v = 1e-6f;
                     rhs += 1e-6f * a.pos[r];
                 }
-                out.push_back(Entry{r, c, v});
+                out[o++] = Entry{r, c, v};
+            };
+            while (i < len) {
+                const int32_t c = row[i].col;
+                if (!diag && c > r) {
+                    put(r, 0.f);
+                    diag = true;
+                }
+                float v = c == r ? 0.f + row[i].val : row[i].val;
+                for (++i; i < len && row[i].col == c; ++i) v += row[i].val;
+                if (c == r) diag = true;
+                put(c, v);
             }
+            if (!diag) put(r, 0.f);
             m.rhs[r] = rhs;
-            row_nnz[r] = static_cast<int32_t>(out.size() - before);
+            row_nnz[r] = static_cast<int32_t>(o - before);
         }
+        out.resize(o);
     }
     m.start.assign(static_cast<size_t>(n) + 1, 0);
     for (int32_t r = 0; r < n; ++r) m.start[r + 1] = m.start[r] + row_nnz[r];
