@@ -686,6 +686,9 @@ def run_flow(args):
         t = time.perf_counter()
         ref.write_pl(r, os.path.join(d, "ref.pl"))
         theirs["write"] = {"ms": round((time.perf_counter() - t) * 1e3, 1)}
+        if os.path.exists(ref.CHECK_PATH):  # the reference's legality checker on both outputs
+            line["ours_check"] = "PASS" if ref.check_placement(aux, os.path.join(d, "ours.pl"))[0] == 0 else "FAIL"
+            theirs["check"] = "PASS" if ref.check_placement(aux, os.path.join(d, "ref.pl"))[0] == 0 else "FAIL"
         line["reference"] = theirs
         line["reference_note"] = "init: the reference's QP needs Eigen (absent); it starts from our QP placement"
         line["reference_total_ms_without_init"] = round(sum(v["ms"] for v in theirs.values()), 1)

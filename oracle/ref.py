@@ -212,6 +212,18 @@ def abacus_segments(r: RefDb):
     return row, lx, hx
 
 
+CHECK_PATH = os.path.join(_HERE, "_ref", "superplace-check")
+
+
+def check_placement(aux, pl=None):
+    """The reference's legality checker (tools/check/main.cpp, built by oracle/Makefile) on a
+    design and a placement: (exit code, report text). 0 = PASS, 1 = FAIL, 2 = bad input."""
+    import subprocess
+    args = [CHECK_PATH, str(aux)] + ([str(pl)] if pl else [])
+    out = subprocess.run(args, capture_output=True, text=True, timeout=600)
+    return out.returncode, out.stdout
+
+
 def read_placement(r: RefDb, path):
     """The reference's BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp:367-401)."""
     if lib().spref_read_placement(r.h, os.fsencode(path)):

@@ -5,6 +5,7 @@ import os
 import numpy as np
 import pytest
 
+from oracle import ref
 from superplace_b200 import bookshelf, flow, generator, qp
 
 
@@ -30,6 +31,21 @@ def test_flow_without_gp(small_aux, tmp_path):
     assert np.array_equal(back.node_x, db.node_x[: db.num_nodes])
 
 
+@pytest.mark.skipif(not os.path.exists(ref.CHECK_PATH), reason="oracle/_ref/superplace-check not built")
+def test_flow_output_passes_the_reference_checker(small_aux, tmp_path):
+    """The reference's own legality checker (tools/check/main.cpp) passes the legalised .pl
+    and fails the overlapping start; its HPWL agrees with ours."""
+    out = str(tmp_path / "out.pl")
+    db, rep = flow.place(small_aux, out_pl=out, stages=("parse", "init", "lg", "write"),
+                         qp_params=qp.default_params(device=0))
+    rc, text = ref.check_placement(small_aux, out)
+    assert rc == 0 and "Result:         PASS" in text, text
+    hpwl = float(text.split("HPWL:")[1].split()[0])
+    assert hpwl == pytest.approx(rep["stages"][-1]["hpwl"], rel=1e-6)
+    rc, text = ref.check_placement(small_aux)  # the design's own, overlapping .pl
+    assert rc == 1 and "Result:         FAIL" in text
+
+
 @pytest.mark.gpu
 def test_flow_with_gp(small_aux, tmp_path):
     from superplace_b200 import abi
@@ -41,3 +57,6 @@ def test_flow_with_gp(small_aux, tmp_path):
     assert st["gp"]["overflow"] <= 0.10 and st["gp"]["iterations"] > 0
     assert st["lg"]["failed"] == 0 and st["lg"]["selfcheck_overlaps"] == 0
     assert st["lg"]["hpwl"] < 1.2 * st["gp"]["hpwl"]
+    if os.path.exists(ref.CHECK_PATH):
+        rc, text = ref.check_placement(small_aux, str(tmp_path / "out.pl"))
+        assert rc == 0, text
