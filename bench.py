@@ -691,7 +691,7 @@ def run_flow(args):
             theirs["check"] = "PASS" if ref.check_placement(aux, os.path.join(d, "ref.pl"))[0] == 0 else "FAIL"
         line["reference"] = theirs
         line["reference_note"] = "init: the reference's QP needs Eigen (absent); it starts from our QP placement"
-        line["reference_total_ms_without_init"] = round(sum(v["ms"] for v in theirs.values()), 1)
+        line["reference_total_ms_without_init"] = round(sum(v["ms"] for v in theirs.values() if isinstance(v, dict)), 1)
         line["ours_total_ms_without_init"] = round(line["ours_total_ms"] - ours["init"]["ms"], 1)
     for f in os.listdir(d):
         os.remove(os.path.join(d, f))
