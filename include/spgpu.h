@@ -372,6 +372,21 @@ int spg_qp_assemble(const spg_db_view* db, const float* net_weight, const spg_qp
 int spg_host_hpwl(const spg_db_view* db, const float* x, const float* y, double* out);
 
 /* ---------------------------------------------------------------------------------------------
+ * The other initial placers of the init stage (makeInitialPlacer, src/init/initial_placer.cpp:15-23),
+ * on the host: "random" (RandomPlacer, src/init/random_placer.cpp:15-38) and "cluster_fc" /
+ * "cluster_bc" (ClusterPlacer, src/init/cluster_common.cpp). x, y (num_nodes centres) are
+ * written for the movable nodes. No device work.
+ * ------------------------------------------------------------------------------------------- */
+const char* spg_init_last_error(void);
+/* seed: Config::random_seed. */
+int spg_random_place(const spg_db_view* db, uint64_t seed, float* x, float* y);
+/* best_choice 0 = first-choice matching (cluster_fc), 1 = best-choice (cluster_bc);
+ * target_count: Config::cluster_target_count (0 = num_movable / 25); clusters and levels, when
+ * not NULL, get the final cluster count and the coarsening levels run. */
+int spg_cluster_place(const spg_db_view* db, int32_t best_choice, int32_t target_count, int32_t ignore_net_degree,
+                      float* x, float* y, int32_t* clusters, int32_t* levels);
+
+/* ---------------------------------------------------------------------------------------------
  * Abacus row legalisation of the standard cells on the host: legalizeCells
  * (src/lg/abacus.cpp:155-284, AbacusResult src/lg/abacus.h:23-34) and buildAbacusSegments
  * (src/lg/abacus.cpp:107-153). No device work.

@@ -72,6 +72,7 @@ def lib():
         L.spref_write_pl.argtypes = [vp, C.c_char_p]
         L.spref_read_placement.argtypes = [vp, C.c_char_p]
         L.spref_abacus.argtypes = [vp, C.c_int, C.c_int, dp]
+        L.spref_init_place.argtypes = [vp, C.c_int, C.c_ulonglong, C.c_int, C.c_int]
         L.spref_abacus_segments.argtypes = [vp, ip, fp, fp, C.c_int]
         L.spref_quiet(1)
         _lib = L
@@ -203,6 +204,13 @@ def abacus(r: RefDb, area_weight=False, reference_trials=False) -> dict:
     if lib().spref_abacus(r.h, int(area_weight), int(reference_trials), res):
         raise ValueError(lib().spref_last_error().decode())
     return {k: (res[i] if i >= 8 else int(res[i])) for i, k in enumerate(ABACUS_FIELDS)}
+
+
+def init_place(r: RefDb, method: str, seed=1002, target_count=0, ignore_net_degree=100):
+    """The reference's "random", "cluster_fc" or "cluster_bc" initial placer on the RefDb."""
+    code = {"random": 0, "cluster_fc": 1, "cluster_bc": 2}[method]
+    if lib().spref_init_place(r.h, code, seed, target_count, ignore_net_degree):
+        raise ValueError(lib().spref_last_error().decode())
 
 
 def abacus_segments(r: RefDb):

@@ -29,6 +29,8 @@
 #include "io/bookshelf_reader.h"
 #include "io/bookshelf_writer.h"
 #include "lg/abacus.h"
+#include "init/cluster_common.h"
+#include "init/random_placer.h"
 #include "numeric/optimizer.h"
 #include "numeric/poisson_backend.h"
 #include "spgpu.h"
@@ -496,6 +498,26 @@ int spref_abacus(void* h, int area_weight, int reference_trials, double* res) {
                               double(r.segments), double(r.roundedWidths), double(r.selfcheckOverlaps),
                               double(r.selfcheckOffSite), r.dispMean, r.dispMax};
         std::memcpy(res, v, sizeof v);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// The reference's RandomPlacer (method 0) or ClusterPlacer with first-choice (1) or best-choice
+// (2) matching on the handle's PlaceDB (src/init/random_placer.cpp, src/init/cluster_common.cpp).
+int spref_init_place(void* h, int method, unsigned long long seed, int target_count, int ignore_net_degree) {
+    try {
+        sp::Config cfg;
+        cfg.random_seed = seed;
+        cfg.cluster_target_count = target_count;
+        cfg.ignore_net_degree = ignore_net_degree;
+        sp::MetricsSink sink;
+        std::unique_ptr<sp::IInitialPlacer> p;
+        if (method == 0) p = std::make_unique<sp::RandomPlacer>();
+        else if (method == 1) p = std::make_unique<sp::ClusterPlacer>(sp::makeFirstChoiceMatcher(), "cluster_fc");
+        else p = std::make_unique<sp::ClusterPlacer>(sp::makeBestChoiceMatcher(), "cluster_bc");
+        p->place(static_cast<RefDb*>(h)->db, cfg, sink);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);

@@ -2,7 +2,8 @@
 .pl write) over this package:
 
   parse  read_bookshelf                 BookshelfReader::read
-  init   QuadraticPlacer (B2B QP)       makeInitialPlacer("quadratic"), the default init_method
+  init   QuadraticPlacer (B2B QP)       makeInitialPlacer("quadratic"), the default init_method;
+                                        "random", "cluster_fc", "cluster_bc" by init_method
   gp     fillers + the device mGP loop  GlobalPlaceStage::run (src/stages/gp_stage.cpp)
   lg     Abacus                         LegalizeStage::run (src/stages/lg_stage.cpp:12-41)
   write  write_pl                       BookshelfWriter::writePl
@@ -17,7 +18,7 @@ import time
 
 import numpy as np
 
-from . import abi, bookshelf, engine, legalize, qp
+from . import abi, bookshelf, engine, initial, legalize, qp
 from .placedb import F_FIXED, F_MACRO, PlaceDB
 
 STAGES = ("parse", "init", "gp", "lg", "write")
@@ -28,7 +29,8 @@ def _hpwl(db: PlaceDB) -> float:
 
 
 def place(aux: str | None = None, db: PlaceDB | None = None, out_pl: str | None = None,
-          stages=STAGES, params: abi.Params | None = None, qp_params=None) -> tuple[PlaceDB, dict]:
+          stages=STAGES, params: abi.Params | None = None, qp_params=None,
+          init_method: str = "quadratic") -> tuple[PlaceDB, dict]:
     """Runs `stages` in order on the design of `aux` (or on `db`) and returns the PlaceDB and a
     report: per stage its wall time in ms and the HPWL after it, the GP and legalisation
     results, and `stopped` when a stage could not run."""
@@ -45,9 +47,13 @@ def place(aux: str | None = None, db: PlaceDB | None = None, out_pl: str | None 
         raise ValueError("no design: give aux with the parse stage, or db")
     if "init" in stages:
         t0 = time.perf_counter()
-        qp_params = qp_params or qp.default_params(device=1 if engine.device_available() else 0)
-        rows = qp.QuadraticPlacer(qp_params).place(db)
-        done("init", t0, outer_iters=int(rows["iter"].shape[0]), device=int(qp_params.device))
+        if init_method == "quadratic":
+            qp_params = qp_params or qp.default_params(device=1 if engine.device_available() else 0)
+            rows = qp.QuadraticPlacer(qp_params).place(db)
+            done("init", t0, outer_iters=int(rows["iter"].shape[0]), device=int(qp_params.device))
+        else:
+            seed = (params or abi.default_params()).random_seed
+            done("init", t0, **initial.make_initial_placer(init_method, seed=seed).place(db))
         report["init_x"], report["init_y"] = db.node_x[: db.num_nodes].copy(), db.node_y[: db.num_nodes].copy()
     movable_macros = int(np.sum((db.node_flags[: db.num_movable] & F_MACRO != 0) &
                                 (db.node_flags[: db.num_movable] & F_FIXED == 0)))

@@ -60,3 +60,11 @@ def test_flow_with_gp(small_aux, tmp_path):
     if os.path.exists(ref.CHECK_PATH):
         rc, text = ref.check_placement(small_aux, str(tmp_path / "out.pl"))
         assert rc == 0, text
+
+
+@pytest.mark.parametrize("method", ["random", "cluster_fc", "cluster_bc"])
+def test_flow_with_the_other_initial_placers(small_aux, tmp_path, method):
+    db, rep = flow.place(small_aux, out_pl=str(tmp_path / "out.pl"), stages=("parse", "init", "lg", "write"),
+                         init_method=method)
+    st = {s["stage"]: s for s in rep["stages"]}
+    assert st["init"]["method"] == method and st["lg"]["failed"] == 0 and st["lg"]["selfcheck_overlaps"] == 0
