@@ -372,6 +372,24 @@ int spg_qp_assemble(const spg_db_view* db, const float* net_weight, const spg_qp
 int spg_host_hpwl(const spg_db_view* db, const float* x, const float* y, double* out);
 
 /* ---------------------------------------------------------------------------------------------
+ * The parse stage's design summary: DbStats (src/db/db_stats.h:17-86, src/db/db_stats.cpp). Host
+ * code; fields as the reference's, degree_count[d] for d <= 100 and degree_over above.
+ * ------------------------------------------------------------------------------------------- */
+typedef struct spg_db_stats {
+    double core_lx, core_ly, core_hx, core_hy, row_height;
+    int32_t row_count;
+    double site_step, core_area, movable_area, fixed_area, fixed_area_in_core, total_row_area;
+    int32_t node_count, object_count, fixed_count, macro_count, net_count, pin_count, max_net_degree;
+    int32_t degree_histogram[5]; /* 1, 2, 3-9, 10-99, >= 100 */
+    int32_t degree_count[101];
+    int32_t degree_over;
+} spg_db_stats;
+int spg_db_stats_compute(const spg_db_view* db, spg_db_stats* out);
+/* DbStats::toString's "DATABASE SUMMARY" text into buf (NUL-terminated, cut at cap - 1); returns
+ * its full length. */
+int64_t spg_db_stats_text(const spg_db_stats* s, char* buf, int64_t cap);
+
+/* ---------------------------------------------------------------------------------------------
  * The other initial placers of the init stage (makeInitialPlacer, src/init/initial_placer.cpp:15-23),
  * on the host: "random" (RandomPlacer, src/init/random_placer.cpp:15-38) and "cluster_fc" /
  * "cluster_bc" (ClusterPlacer, src/init/cluster_common.cpp). x, y (num_nodes centres) are

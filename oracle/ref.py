@@ -73,6 +73,7 @@ def lib():
         L.spref_read_placement.argtypes = [vp, C.c_char_p]
         L.spref_abacus.argtypes = [vp, C.c_int, C.c_int, dp]
         L.spref_init_place.argtypes = [vp, C.c_int, C.c_ulonglong, C.c_int, C.c_int]
+        L.spref_db_stats.argtypes = [vp, dp, ip, C.c_char_p, C.c_int]
         L.spref_abacus_segments.argtypes = [vp, ip, fp, fp, C.c_int]
         L.spref_quiet(1)
         _lib = L
@@ -211,6 +212,13 @@ def init_place(r: RefDb, method: str, seed=1002, target_count=0, ignore_net_degr
     code = {"random": 0, "cluster_fc": 1, "cluster_bc": 2}[method]
     if lib().spref_init_place(r.h, code, seed, target_count, ignore_net_degree):
         raise ValueError(lib().spref_last_error().decode())
+
+
+def db_stats(r: RefDb):
+    """The reference's DbStats::compute and toString: (values, histogram, text)."""
+    v, hist, text = (C.c_double * 14)(), (C.c_int * 5)(), C.create_string_buffer(8192)
+    lib().spref_db_stats(r.h, v, hist, text, 8192)
+    return list(v), list(hist), text.value.decode()
 
 
 def abacus_segments(r: RefDb):

@@ -29,6 +29,7 @@
 #include "io/bookshelf_reader.h"
 #include "io/bookshelf_writer.h"
 #include "lg/abacus.h"
+#include "db/db_stats.h"
 #include "init/cluster_common.h"
 #include "init/random_placer.h"
 #include "numeric/optimizer.h"
@@ -522,6 +523,20 @@ int spref_init_place(void* h, int method, unsigned long long seed, int target_co
     } catch (const std::exception& e) {
         return fail(e);
     }
+}
+
+// sp::DbStats::compute of the handle's PlaceDB: v[0..13] = coreLx, coreLy, coreHx, coreHy,
+// rowHeight, rowCount, siteStep, coreArea, movableArea, fixedArea, fixedAreaInCore, totalRowArea,
+// maxNetDegree, degreeOver; hist[0..4] the histogram; text (up to cap) toString's text.
+void spref_db_stats(void* h, double* v, int* hist, char* text, int cap) {
+    const sp::DbStats s = sp::DbStats::compute(static_cast<RefDb*>(h)->db);
+    const double a[14] = {s.coreLx, s.coreLy, s.coreHx, s.coreHy, s.rowHeight, double(s.rowCount), s.siteStep,
+                          s.coreArea, s.movableArea, s.fixedArea, s.fixedAreaInCore, s.totalRowArea,
+                          double(s.maxNetDegree), double(s.degreeOver)};
+    std::memcpy(v, a, sizeof a);
+    for (int k = 0; k < 5; ++k) hist[k] = s.degreeHistogram[static_cast<size_t>(k)];
+    const std::string t = s.toString();
+    std::snprintf(text, static_cast<size_t>(cap), "%s", t.c_str());
 }
 
 // sp::buildAbacusSegments: up to cap of (row, lx, hx); returns how many there are.

@@ -18,7 +18,7 @@ import time
 
 import numpy as np
 
-from . import abi, bookshelf, engine, initial, legalize, qp
+from . import abi, bookshelf, engine, initial, legalize, qp, stats
 from .placedb import F_FIXED, F_MACRO, PlaceDB
 
 STAGES = ("parse", "init", "gp", "lg", "write")
@@ -42,7 +42,10 @@ def place(aux: str | None = None, db: PlaceDB | None = None, out_pl: str | None 
     if "parse" in stages:
         t0 = time.perf_counter()
         db = bookshelf.read_bookshelf(aux)
-        done("parse", t0)
+        st = stats.db_stats(db)
+        done("parse", t0, nodes=st.node_count, fixed=st.fixed_count, macros=st.macro_count, nets=st.net_count,
+             pins=st.pin_count)
+        report["summary"] = stats.summary_text(st)
     if db is None:
         raise ValueError("no design: give aux with the parse stage, or db")
     if "init" in stages:
