@@ -202,41 +202,43 @@ void assemble(const Problem& P, const Axis& a, const std::vector<int32_t>& lo, c
         std::vector<Entry>& out = block_rows[rb];
         out.resize(total + static_cast<size_t>(r1 - r0));  // at most every entry plus a diagonal per row
         size_t o = 0;
+        std::vector<Entry> off;
         for (int32_t r = r0; r < r1; ++r) {
-            Entry* row = sorted.data() + cnt[r - r0];
+            const Entry* row = sorted.data() + cnt[r - r0];
             const size_t len = static_cast<size_t>(cnt[r - r0 + 1] - cnt[r - r0]);
-            for (size_t j = 1; j < len; ++j) {  // stable insertion sort by column, in place
-                const Entry en = row[j];
+            // the right-hand side and the diagonal are summed in emission order as they come
+            // (the diagonal from the zero the reference seeds first); only the off-diagonal
+            // entries need ordering by column (stable, so equal columns keep emission order)
+            float rhs = 0.f, diag = 0.f;
+            off.clear();
+            for (size_t j = 0; j < len; ++j) {
+                if (row[j].col == kRhs) rhs += row[j].val;
+                else if (row[j].col == r) diag += row[j].val;
+                else off.push_back(row[j]);
+            }
+            for (size_t j = 1; j < off.size(); ++j) {  // stable insertion sort by column
+                const Entry en = off[j];
                 size_t h = j;
-                for (; h > 0 && row[h - 1].col > en.col; --h) row[h] = row[h - 1];
-                row[h] = en;
+                for (; h > 0 && off[h - 1].col > en.col; --h) off[h] = off[h - 1];
+                off[h] = en;
             }
-            float rhs = 0.f;
-            size_t i = 0;
-            for (; i < len && row[i].col == kRhs; ++i) rhs += row[i].val;
+            if (diag == 0.f) {  // a movable node with no connection: a tiny pull to where it is
+                diag = 1e-6f;
+                rhs += 1e-6f * a.pos[r];
+            }
             const size_t before = o;
-            // the reference seeds a zero diagonal before every emitted entry: the diagonal's sum
-            // starts from 0 (0 + w is w exactly), and the slot exists even with nothing emitted
-            bool diag = false;
-            auto put = [&](int32_t c, float v) {
-                if (c == r && v == 0.f) {  // a movable node with no connection: a tiny pull to where it is
-                    v = 1e-6f;
-                    rhs += 1e-6f * a.pos[r];
+            bool diag_out = false;
+            for (size_t i = 0; i < off.size();) {
+                const int32_t c = off[i].col;
+                if (!diag_out && c > r) {
+                    out[o++] = Entry{r, r, diag};
+                    diag_out = true;
                 }
+                float v = off[i].val;
+                for (++i; i < off.size() && off[i].col == c; ++i) v += off[i].val;
                 out[o++] = Entry{r, c, v};
-            };
-            while (i < len) {
-                const int32_t c = row[i].col;
-                if (!diag && c > r) {
-                    put(r, 0.f);
-                    diag = true;
-                }
-                float v = c == r ? 0.f + row[i].val : row[i].val;
-                for (++i; i < len && row[i].col == c; ++i) v += row[i].val;
-                if (c == r) diag = true;
-                put(c, v);
             }
-            if (!diag) put(r, 0.f);
+            if (!diag_out) out[o++] = Entry{r, r, diag};
             m.rhs[r] = rhs;
             row_nnz[r] = static_cast<int32_t>(o - before);
         }
