@@ -205,3 +205,20 @@ def test_device_solver_fails_loudly_without_a_gpu():
     with pytest.raises(engine.SpgError) as e:
         qp.QuadraticPlacer(qp.default_params(device=1)).place(qp_design())
     assert e.value.code == -2  # SPG_E_NO_DEVICE, no host fallback
+
+
+@pytest.mark.parametrize("ignore,min_distance", [(5, 1.0), (6, 10.0), (2, 0.25)])
+def test_assembly_degree_cap_and_distance_floor(ignore, min_distance):
+    """Nets of degree exactly ignore_net_degree are kept and one above is dropped
+    (src/init/quadratic_placer.cpp:84); a large qp_min_distance floors the weight denominator."""
+    db = big_net_db(qp_design(seed=11))
+    p = qp.default_params(ignore_net_degree=ignore, min_distance=min_distance)
+    degs = np.diff(db.net2pin_start)
+    assert np.any(degs == ignore) and np.any(degs == ignore + 1)
+    for axis in (0, 1):
+        start, col, val, rhs = qp.assemble(db, axis, params=p)
+        o = oqp.assemble(db, axis, db.node_x, db.node_y, db.net_weight, min_distance=min_distance,
+                         ignore_net_degree=ignore)
+        assert np.array_equal(start, o[0]) and np.array_equal(col, o[1])
+        assert np.array_equal(val.view(np.uint32), o[2].view(np.uint32))
+        assert np.array_equal(rhs.view(np.uint32), o[3].view(np.uint32))
