@@ -122,6 +122,15 @@ def peaks():
 
 
 # ------------------------------------------------------------------ reference arm
+def ref_fillers(db, ref):
+    """The reference's own initializeFillers (src/gp/filler.cpp:47-139) on a copy of db, its
+    fillers appended to db (no library of this package is loaded)."""
+    r = ref.RefDb(db)
+    info = r.fillers_init(1.0, 1002)
+    x, y, _, _, _ = r.nodes()
+    db.set_fillers(int(info[0]), info[1], info[2], x[db.num_nodes:], y[db.num_nodes:])
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -132,33 +141,35 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libspref.so not built"}))
         return 0
     db = make_design(args.workload)
-    from superplace_b200 import engine  # host-only filler routines (no device needed)
-
-    engine.initialize_fillers(db, 1.0, 1002)
+    ref_fillers(db, ref)
     threads = os.cpu_count() or 1
     ref.lib().spref_set_threads(threads)
     sample_iters = args.ref_iters
     params = abi.default_params(gp_bin_dim=WORKLOADS[args.workload]["bin_dim"],
-                                gp_max_iter=sample_iters)
+                                gp_max_iter=sample_iters if sample_iters > 0 else 2000)
+    # the CPU run needs no warm-up: one untimed stage at most, so the arm ends in minutes
     iters, ms = [], []
-    for k in range(args.warmup + args.steps):
+    for k in range(min(args.warmup, 1) + args.steps):
         r = ref.RefDb(db)
         res, rows = r.eplace(params)
-        if k >= args.warmup:
-            iters.append(len(rows))
-            ms.append(rows[-1, 7] if len(rows) else res["elapsed_ms"])
+        if k >= min(args.warmup, 1):
+            iters.append(int(res["iterations"]))
+            ms.append(res["elapsed_ms"])
     value = sum(iters) / (sum(ms) / 1e3)
-    sample = (f"first {sample_iters} mGP iterations of the same instance (reference CPU "
-              f"EPlace built from its sources, FFT stand-in for FFTW)")
+    what = (f"first {sample_iters} mGP iterations" if sample_iters > 0 else
+            "full mGP stages (lambda_0 probe, initial step, iterations to tau<0.10)")
+    sample = (f"{what} of the same instance, each from the same start, on the reference's CPU "
+              f"EPlace built from its sources (FFT stand-in for FFTW), {threads} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "iter/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": min(args.warmup, 1),
         "ms_per_step": sum(ms) / len(ms), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "cells": int(db.num_movable),
                    "fillers": int(db.num_fillers), "pins": int(db.num_pins),
                    "nets": int(db.num_nets), "bins": WORKLOADS[args.workload]["bin_dim"],
-                   "sample_iterations": sample_iters},
+                   "step": "one full mGP stage run" if sample_iters <= 0 else f"{sample_iters}-iteration sample",
+                   "iterations_per_step": iters},
         "cpu_baseline": {"value": value, "unit": "iter/s", "cores": threads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -168,8 +179,9 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ our arm
-def cpu_baseline_sample(db, workload, iters=8):
-    """The reference's CPU EPlace on the same instance, bounded sample, all host cores."""
+def cpu_baseline_sample(db, workload):
+    """The reference's CPU EPlace on the same instance: one full mGP stage (the same work as
+    one step of this arm), all host cores."""
     try:
         from oracle import ref
 
@@ -178,14 +190,34 @@ def cpu_baseline_sample(db, workload, iters=8):
         threads = os.cpu_count() or 1
         ref.lib().spref_set_threads(threads)
         r = ref.RefDb(db)
-        _, rows = r.eplace(abi.default_params(gp_bin_dim=WORKLOADS[workload]["bin_dim"], gp_max_iter=iters))
-        v = len(rows) / (rows[-1, 7] / 1e3)
+        res, _ = r.eplace(abi.default_params(gp_bin_dim=WORKLOADS[workload]["bin_dim"]))
+        v = res["iterations"] / (res["elapsed_ms"] / 1e3)
         return {"value": v, "unit": "iter/s", "cores": threads, "kind": "reference",
-                "sample": f"first {iters} mGP iterations of this instance on the reference CPU "
+                "sample": f"one full mGP stage ({int(res['iterations'])} iterations, "
+                          f"{res['elapsed_ms'] / 1e3:.1f} s) of this instance on the reference's CPU "
                           f"EPlace built from its sources (FFT stand-in for FFTW)"}
     except Exception as e:  # the baseline must not hide our number
         return {"value": None, "unit": "iter/s", "cores": 0, "kind": "reference",
                 "sample": f"failed: {e}"}
+
+
+def fp32_arm(db, workload, init_x, init_y, steps):
+    """The plain FP32 GPU form (FP32 SIMT cosine contractions) on the same instance and start,
+    timed the same way as the headline arm: mGP iterations per second of loop time."""
+    from superplace_b200 import engine
+
+    params = abi.default_params(gp_bin_dim=WORKLOADS[workload]["bin_dim"], poisson_precision=abi.POISSON_FP32)
+    ep = engine.EPlace(db, params)
+    iters, ms = [], []
+    for k in range(1 + steps):
+        db.node_x[:] = init_x
+        db.node_y[:] = init_y
+        r = ep.run(abi.STAGE_MGP)
+        if k:
+            iters.append(r.iterations)
+            ms.append(r.elapsed_ms)
+    ep.ctx.close()
+    return sum(iters) / (sum(ms) / 1e3), iters
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each part, from one
@@ -369,6 +401,11 @@ def run_ours(args):
             "kernels": kern,
             "clocks": clk.summary(),
         }
+        if precision == abi.POISSON_BF16X3 and args.fp32_steps > 0:
+            v32, it32 = fp32_arm(db, args.workload, init_x, init_y, args.fp32_steps)
+            line["fp32_value"] = v32
+            line["fp32_iterations_per_step"] = it32
+            line["bf16x3_over_fp32"] = value / world / v32
         if args.cpu_baseline:
             db.node_x[:] = init_x
             db.node_y[:] = init_y
@@ -708,8 +745,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="bf16x3", choices=["fp32", "bf16x3"])
     ap.add_argument("--workload", default="large", choices=list(WORKLOADS))
-    ap.add_argument("--ref-iters", type=int, default=8)
+    ap.add_argument("--ref-iters", type=int, default=0,
+                    help="reference arm: time only the first N mGP iterations of each stage (0: full stages)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--fp32-steps", type=int, default=3,
+                    help="stages of the plain FP32 form timed after the headline arm (fp32_value)")
     ap.add_argument("--poisson-sweep", action="store_true",
                     help="operator sweep (grids 128..2048, batch 1 and 64): JSON lines, not the bench line")
     ap.add_argument("--precision-study", action="store_true",

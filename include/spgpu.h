@@ -203,12 +203,15 @@ int spg_poisson_destroy(spg_poisson* h);
 /* Poisson solve that allocates nothing. No counterpart in the reference: it exists for
  * callers that cannot call cudaMalloc (hosts that reserve all device memory up front in
  * their own pool and forbid later driver allocations), which therefore cannot create a
- * spg_poisson plan. Same plain-FP32 solve as a plan's, device arrays in and out, work
- * enqueued on `stream`. Its bases and work buffers live in one static device array of
- * 11 MB that every GPU loading this library holds until the process exits; nx and ny must
- * be at most 512 (larger sizes return SPG_E_CAPACITY). All calls on a device share that
- * array, so calls that overlap on the GPU race: serialise them. The first call on a device
- * looks up the array's address (cudaGetSymbolAddress); make it before any stream capture. */
+ * spg_poisson plan. The plain-FP32 solve of a plan, device arrays in and out, work enqueued
+ * on `stream`; its basis tables are built on the device, so it agrees with a plan's solve to
+ * 1e-5 of max|result| rather than bit for bit. Its bases and work buffers live in one static
+ * device array of 11 MB that every GPU loading this library holds until the process exits;
+ * nx and ny must be at most 512 (larger sizes return SPG_E_CAPACITY). All calls on a device
+ * share that array, so calls that overlap on the GPU race: serialise them. Each call made
+ * outside a stream capture looks the array's address up again (cudaGetSymbolAddress), so a
+ * device reset leaves no stale address; a call on a capturing stream reuses the last one,
+ * so make the first call on a device before any stream capture. */
 int spg_poisson_solve_static(int nx, int ny, float step_x, float step_y, const float* d_rho,
                              float* d_phi, float* d_field_x, float* d_field_y, void* stream);
 
@@ -298,6 +301,30 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n);
  * 0 when it ran the host-driven loop (SPG_HOST_LOOP set, or conditional nodes refused). */
 int spg_ctx_graph_loop(const spg_ctx* ctx);
 
+/* EPlace::Impl::objAndGrad (src/gp/eplace.cpp:136-203) at caller positions, through the
+ * stage loop's own kernels (the loop body with no step applied): the grid and opt set are
+ * rebuilt for `stage` from the context's positions and flags (as constructing EPlace does),
+ * the opt nodes are placed at pos (2*nOpt floats, x then y, in buildOptSet's order:
+ * movable non-fixed non-NI nodes, minus the macros in cGP, none in FILLERONLY, then the
+ * fillers, eplace.cpp:82-94), and one evaluation runs with the given lambda and gamma.
+ * grad gets the preconditioned gradient precond * (dWL - lambda * q xi) (2*nOpt floats);
+ * out[0..4] = WA wirelength (the objective), overflow tau, HPWL, sum|dWL|, sum|q xi|;
+ * *n_opt = nOpt. With pos = NULL only *n_opt is set. The opt nodes stay at pos. */
+int spg_eval_grad(spg_ctx* ctx, int stage, float lambda, float gamma, const float* pos, float* grad,
+                  double* out, int32_t* n_opt);
+
+/* The stage loop's optimizer on a test objective: NesterovOptimizer::step
+ * (src/numeric/cpu/nesterov.cpp:51-122) called `steps` times from pos, as the reference's
+ * optimizer tests drive it (test/test_nesterov.cpp), on f(x) = 0.5 * sum c_i (x_i - t_i)^2,
+ * with the device loop's step kernel, backtracking test (redoIfOvershot, :146-169), step
+ * decisions (estimateStep with BB, :221-240) and, when init_step <= 0, estimateInitialStep
+ * (:190-218). n must be even and >= 2 (the vectors are kept as n/2 x-y pairs). No
+ * constraint. pos gets the current solution v; out[0..3] = objective at the last counted
+ * evaluation, evaluations, step size, backtracking re-evaluations. */
+int spg_nesterov_quadratic(int32_t n, const float* coef, const float* target, float* pos, int32_t steps,
+                           int32_t use_bb, int32_t backtrack, int32_t max_backtrack, float init_step,
+                           double* out);
+
 /* ------------------------------------------------------------------ BookShelf files (host)
  * BookshelfReader::read (src/io/bookshelf_reader.cpp:404-436): the .aux and the .scl, .nodes,
  * .nets, .pl and .wts files it names, into the PlaceDB layout: nodes reordered stably to
@@ -370,69 +397,6 @@ int spg_qp_assemble(const spg_db_view* db, const float* net_weight, const spg_qp
                     int64_t cap, int64_t* nnz);
 /* computeHPWL (src/db/hpwl.cpp:13-39) at positions x, y on the host. */
 int spg_host_hpwl(const spg_db_view* db, const float* x, const float* y, double* out);
-
-/* ---------------------------------------------------------------------------------------------
- * The parse stage's design summary: DbStats (src/db/db_stats.h:17-86, src/db/db_stats.cpp). Host
- * code; fields as the reference's, degree_count[d] for d <= 100 and degree_over above.
- * ------------------------------------------------------------------------------------------- */
-typedef struct spg_db_stats {
-    double core_lx, core_ly, core_hx, core_hy, row_height;
-    int32_t row_count;
-    double site_step, core_area, movable_area, fixed_area, fixed_area_in_core, total_row_area;
-    int32_t node_count, object_count, fixed_count, macro_count, net_count, pin_count, max_net_degree;
-    int32_t degree_histogram[5]; /* 1, 2, 3-9, 10-99, >= 100 */
-    int32_t degree_count[101];
-    int32_t degree_over;
-} spg_db_stats;
-int spg_db_stats_compute(const spg_db_view* db, spg_db_stats* out);
-/* DbStats::toString's "DATABASE SUMMARY" text into buf (NUL-terminated, cut at cap - 1); returns
- * its full length. */
-int64_t spg_db_stats_text(const spg_db_stats* s, char* buf, int64_t cap);
-
-/* ---------------------------------------------------------------------------------------------
- * The other initial placers of the init stage (makeInitialPlacer, src/init/initial_placer.cpp:15-23),
- * on the host: "random" (RandomPlacer, src/init/random_placer.cpp:15-38) and "cluster_fc" /
- * "cluster_bc" (ClusterPlacer, src/init/cluster_common.cpp). x, y (num_nodes centres) are
- * written for the movable nodes. No device work.
- * ------------------------------------------------------------------------------------------- */
-const char* spg_init_last_error(void);
-/* seed: Config::random_seed. */
-int spg_random_place(const spg_db_view* db, uint64_t seed, float* x, float* y);
-/* best_choice 0 = first-choice matching (cluster_fc), 1 = best-choice (cluster_bc);
- * target_count: Config::cluster_target_count (0 = num_movable / 25); clusters and levels, when
- * not NULL, get the final cluster count and the coarsening levels run. */
-int spg_cluster_place(const spg_db_view* db, int32_t best_choice, int32_t target_count, int32_t ignore_net_degree,
-                      float* x, float* y, int32_t* clusters, int32_t* levels);
-
-/* ---------------------------------------------------------------------------------------------
- * Abacus row legalisation of the standard cells on the host: legalizeCells
- * (src/lg/abacus.cpp:155-284, AbacusResult src/lg/abacus.h:23-34) and buildAbacusSegments
- * (src/lg/abacus.cpp:107-153). No device work.
- * ------------------------------------------------------------------------------------------- */
-typedef struct spg_abacus_result {
-    int32_t precondition_ok; /* 0: a movable macro is not fixed yet; nothing was moved      */
-    int32_t cells;           /* cells to legalise                                           */
-    int32_t failed;          /* cells no segment could take (left where they were)          */
-    int32_t rows;
-    int32_t segments;
-    int32_t rounded_widths;  /* cells whose width is not a whole number of sites            */
-    int32_t selfcheck_overlaps;
-    int32_t selfcheck_off_site;
-    double disp_mean;        /* lower-left displacement of the placed cells                 */
-    double disp_max;
-} spg_abacus_result;
-
-/* Message of the calling thread's last failed Abacus call. */
-const char* spg_abacus_last_error(void);
-/* Legalises the cells: x, y (num_nodes centres) are read for every node and written for the
- * placed cells. area_weight = 1 weighs cells by area (lg_cell_weight "area"). Uses db's node
- * sizes and flags, rows and core. SPG_E_INVALID for a row with a non-positive step, height or
- * site count, or non-finite geometry (nothing moved). */
-int spg_abacus_legalize(const spg_db_view* db, int32_t area_weight, float* x, float* y, spg_abacus_result* out);
-/* The free segments of every row at positions x, y: up to cap of (row, lx, hx); *count gets
- * how many there are. */
-int spg_abacus_segments(const spg_db_view* db, const float* x, const float* y, int32_t* row, float* lx, float* hx,
-                        int32_t cap, int32_t* count);
 
 /* BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp:367-401): applies a .pl to nodes
  * already read, in place. Names are NUL-terminated back to back (the first of equal names

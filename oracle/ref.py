@@ -72,9 +72,9 @@ def lib():
         L.spref_write_pl.argtypes = [vp, C.c_char_p]
         L.spref_read_placement.argtypes = [vp, C.c_char_p]
         L.spref_abacus.argtypes = [vp, C.c_int, C.c_int, dp]
-        L.spref_init_place.argtypes = [vp, C.c_int, C.c_ulonglong, C.c_int, C.c_int]
-        L.spref_db_stats.argtypes = [vp, dp, ip, C.c_char_p, C.c_int]
-        L.spref_abacus_segments.argtypes = [vp, ip, fp, fp, C.c_int]
+        L.spref_obj_and_grad.argtypes = [vp, C.POINTER(abi.Params), C.c_int, C.c_float, C.c_float, fp, fp, dp, ip]
+        L.spref_legalize_macros.argtypes = [vp, C.POINTER(abi.Params), dp]
+        L.spref_gp_four_stage.argtypes = [vp, C.POINTER(abi.Params), dp]
         L.spref_quiet(1)
         _lib = L
     return _lib
@@ -136,18 +136,61 @@ class RefDb:
         return wl, g
 
     def eplace(self, params, stage=abi.STAGE_MGP, cap=4000):
+        """EPlace(db, cfg, sink).run(stage): the result dict and the stage's metrics rows, one
+        row of ROW_FIELDS per iteration."""
         res = (C.c_double * 8)()
         init = (C.c_double * 3)()
-        rows = np.zeros((cap, 8), np.float64)
+        rows = np.zeros((cap, len(ROW_FIELDS)), np.float64)
         nrows = C.c_int(0)
         rc = lib().spref_eplace_run(self.h, C.byref(params), stage, res, init,
                                     rows.ctypes.data_as(C.POINTER(C.c_double)), cap,
                                     C.byref(nrows))
         if rc:
             raise RuntimeError(f"{rc}: " + lib().spref_last_error().decode())
-        keys = ("iterations", "hpwl", "overflow", "converged", "stagnated", "rollback_iter",
-                "evaluations", "elapsed_ms")
-        return dict(zip(keys, list(res))), rows[: nrows.value]
+        return dict(zip(RESULT_FIELDS, list(res))), rows[: nrows.value]
+
+    def n_opt(self, params, stage=abi.STAGE_MGP):
+        n = C.c_int(0)
+        lib().spref_obj_and_grad(self.h, C.byref(params), stage, 1.0, 1.0, None, None, None, C.byref(n))
+        return n.value
+
+    def obj_and_grad(self, params, stage, lam, gamma, pos):
+        """EPlace::Impl::objAndGrad (src/gp/eplace.cpp:136-203) at opt-set positions pos (x then
+        y), composed from the reference's operators: (grad, {obj, tau, hpwl, sum_wl, sum_den})."""
+        pos = _f(pos)
+        grad = np.zeros_like(pos)
+        out = (C.c_double * 5)()
+        n = C.c_int(0)
+        if lib().spref_obj_and_grad(self.h, C.byref(params), stage, lam, gamma, abi.fptr(pos), abi.fptr(grad),
+                                    out, C.byref(n)):
+            raise RuntimeError(lib().spref_last_error().decode())
+        return grad, dict(zip(("obj", "tau", "hpwl", "sum_wl", "sum_den"), list(out)))
+
+    def legalize_macros(self, params):
+        """legalizeMacros (src/lg/macro_sa.cpp:493) in place; the macros end F_FIXED."""
+        res = (C.c_double * 6)()
+        if lib().spref_legalize_macros(self.h, C.byref(params), res):
+            raise RuntimeError(lib().spref_last_error().decode())
+        return dict(zip(MLG_FIELDS, list(res)))
+
+    def gp_four_stage(self, params):
+        """GlobalPlaceStage's sequence for movable macros (src/stages/gp_stage.cpp:99-201): mGP,
+        mLG, scatterFillers(seed offset 1), FILLERONLY, cGP. Per stage its result dict, and mLG's."""
+        res = (C.c_double * 30)()
+        if lib().spref_gp_four_stage(self.h, C.byref(params), res):
+            raise RuntimeError(lib().spref_last_error().decode())
+        out = {name: dict(zip(RESULT_FIELDS, list(res)[8 * k: 8 * k + 8]))
+               for k, name in enumerate(("mGP", "FILLERONLY", "cGP"))}
+        out["mLG"] = dict(zip(MLG_FIELDS, list(res)[24:30]))
+        return out
+
+
+RESULT_FIELDS = ("iterations", "hpwl", "overflow", "converged", "stagnated", "rollback_iter",
+                 "evaluations", "elapsed_ms")
+# sp::IterMetrics (src/util/metrics.h:12-28) as the shim writes it
+ROW_FIELDS = ("iter", "hpwl", "overflow", "lambda", "gamma", "step_size", "evaluations", "elapsed_ms",
+              "grad_norm_wl", "grad_norm_den", "eval_lambda", "eval_gamma", "delta_hpwl", "lambda_mu")
+MLG_FIELDS = ("num_macros", "overlap_before", "overlap_after", "hpwl_before", "hpwl_after", "repaired")
 
 
 def bookshelf_read(aux_path):
@@ -205,27 +248,6 @@ def abacus(r: RefDb, area_weight=False, reference_trials=False) -> dict:
     if lib().spref_abacus(r.h, int(area_weight), int(reference_trials), res):
         raise ValueError(lib().spref_last_error().decode())
     return {k: (res[i] if i >= 8 else int(res[i])) for i, k in enumerate(ABACUS_FIELDS)}
-
-
-def init_place(r: RefDb, method: str, seed=1002, target_count=0, ignore_net_degree=100):
-    """The reference's "random", "cluster_fc" or "cluster_bc" initial placer on the RefDb."""
-    code = {"random": 0, "cluster_fc": 1, "cluster_bc": 2}[method]
-    if lib().spref_init_place(r.h, code, seed, target_count, ignore_net_degree):
-        raise ValueError(lib().spref_last_error().decode())
-
-
-def db_stats(r: RefDb):
-    """The reference's DbStats::compute and toString: (values, histogram, text)."""
-    v, hist, text = (C.c_double * 14)(), (C.c_int * 5)(), C.create_string_buffer(8192)
-    lib().spref_db_stats(r.h, v, hist, text, 8192)
-    return list(v), list(hist), text.value.decode()
-
-
-def abacus_segments(r: RefDb):
-    n = lib().spref_abacus_segments(r.h, None, None, None, 0)
-    row, lx, hx = np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros(n, np.float32)
-    lib().spref_abacus_segments(r.h, abi.iptr(row), abi.fptr(lx), abi.fptr(hx), n)
-    return row, lx, hx
 
 
 CHECK_PATH = os.path.join(_HERE, "_ref", "superplace-check")

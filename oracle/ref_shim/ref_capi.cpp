@@ -9,6 +9,7 @@
 //   sp::initializeFillers (src/gp/filler.h), sp::EPlace (src/gp/eplace.h),
 //   sp::makeNesterov (src/numeric/optimizer.h), sp::makePoissonBackend
 //   (src/numeric/poisson_backend.h; CPU backend = oracle/ref_shim/poisson_shim.cpp).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -29,9 +30,8 @@
 #include "io/bookshelf_reader.h"
 #include "io/bookshelf_writer.h"
 #include "lg/abacus.h"
-#include "db/db_stats.h"
-#include "init/cluster_common.h"
-#include "init/random_placer.h"
+#include "lg/macro_sa.h"
+#include "numeric/reduction.h"
 #include "numeric/optimizer.h"
 #include "numeric/poisson_backend.h"
 #include "spgpu.h"
@@ -339,11 +339,45 @@ double spref_poisson_bench(int n, int warm, int rounds, int fftwThreads, const f
 }
 
 // ------------------------------------------------------------------ EPlace
+// One metrics row as the doubles the tests read (sp::IterMetrics, src/util/metrics.h:12-28).
+constexpr int kRowWidth = 14;
+void putRow(const sp::IterMetrics& row, double* o) {
+    o[0] = row.iter;
+    o[1] = row.hpwl;
+    o[2] = row.overflow;
+    o[3] = row.lambda;
+    o[4] = row.gamma;
+    o[5] = row.step_size;
+    o[6] = static_cast<double>(row.evaluations);
+    o[7] = row.elapsed_ms;
+    o[8] = row.grad_norm_wl;
+    o[9] = row.grad_norm_den;
+    o[10] = row.eval_lambda;
+    o[11] = row.eval_gamma;
+    o[12] = row.delta_hpwl;
+    o[13] = row.lambda_mu;
+}
+
+sp::GpStage toStage(int stage) {
+    return stage == SPG_STAGE_MGP ? sp::GpStage::kMGP
+         : stage == SPG_STAGE_FILLER_ONLY ? sp::GpStage::kFillerOnly
+                                          : sp::GpStage::kCGP;
+}
+
+void putResult(const sp::GpResult& r, double ms, double* result) {
+    result[0] = r.iterations;
+    result[1] = r.hpwl;
+    result[2] = r.overflow;
+    result[3] = r.converged;
+    result[4] = r.stagnated;
+    result[5] = r.rollbackIter;
+    result[6] = static_cast<double>(r.evaluations);
+    result[7] = ms;
+}
+
 // result[0..7] = iterations, hpwl, overflow, converged, stagnated, rollbackIter,
 //                evaluations, elapsed_ms
-// init[0..2]   = initial hpwl, initial overflow, initial lambda (summary keys)
-// rows: up to cap metrics rows, 8 doubles each:
-//       iter, hpwl, overflow, lambda, gamma, step, evaluations, elapsed_ms
+// rows: up to cap metrics rows, kRowWidth doubles each (putRow)
 int spref_eplace_run(void* dbh, const spg_params* p, int stage, double* result, double* init,
                      double* rows, int cap, int* nRows) {
     try {
@@ -351,39 +385,143 @@ int spref_eplace_run(void* dbh, const spg_params* p, int stage, double* result, 
         const sp::Config cfg = makeConfig(p);
         sp::MetricsSink sink;
         sp::EPlace engine(db, cfg, sink);
-        const sp::GpStage st = stage == SPG_STAGE_MGP ? sp::GpStage::kMGP
-                             : stage == SPG_STAGE_FILLER_ONLY ? sp::GpStage::kFillerOnly
-                                                              : sp::GpStage::kCGP;
+        const sp::GpStage st = toStage(stage);
         const double t0 = omp_get_wtime();
         const sp::GpResult r = engine.run(st);
-        const double ms = (omp_get_wtime() - t0) * 1e3;
-        result[0] = r.iterations;
-        result[1] = r.hpwl;
-        result[2] = r.overflow;
-        result[3] = r.converged;
-        result[4] = r.stagnated;
-        result[5] = r.rollbackIter;
-        result[6] = static_cast<double>(r.evaluations);
-        result[7] = ms;
-        const std::string prefix = std::string(sp::toString(st)) + "_";
+        putResult(r, (omp_get_wtime() - t0) * 1e3, result);
         const auto& m = sink.stageMetrics(sp::toString(st));
         int n = 0;
         for (const auto& row : m) {
             if (n >= cap) break;
-            double* o = rows + 8 * n;
-            o[0] = row.iter;
-            o[1] = row.hpwl;
-            o[2] = row.overflow;
-            o[3] = row.lambda;
-            o[4] = row.gamma;
-            o[5] = row.step_size;
-            o[6] = static_cast<double>(row.evaluations);
-            o[7] = row.elapsed_ms;
+            putRow(row, rows + kRowWidth * n);
             ++n;
         }
         *nRows = n;
         (void)init;
-        (void)prefix;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// EPlace::Impl::objAndGrad (src/gp/eplace.cpp:136-203) at opt-set positions pos (x then y, opt
+// order of buildOptSet, eplace.cpp:82-94) for the given lambda and gamma, composed from the
+// reference's own operators the way objAndGrad composes them: BinGrid built as the EPlace
+// constructor builds it (eplace.cpp:207-215), accumulate, overflow, solveField, gatherForce,
+// WaWirelength::compute, computeHPWL, then the preconditioned assembly of eplace.cpp:166-189
+// and its two fixed-chunk sums. The positions of the opt nodes stay written into the handle.
+// out[0..4] = WA value (the objective), tau, HPWL, sum|grad WL|, sum|q xi|. n_out gets nOpt.
+int spref_obj_and_grad(void* dbh, const spg_params* p, int stage, float lambda, float gamma, const float* pos,
+                       float* grad, double* out, int* n_out) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(dbh)->db;
+        const sp::Config cfg = makeConfig(p);
+        std::vector<int> opt;
+        if (stage != SPG_STAGE_FILLER_ONLY) {
+            for (int i = 0; i < db.numMovable; ++i) {
+                if (db.isFixed(i) || db.isNI(i)) continue;
+                if (stage == SPG_STAGE_CGP && db.isMacro(i)) continue;
+                opt.push_back(i);
+            }
+        }
+        for (int i = db.numNodes; i < db.totalNodes(); ++i) opt.push_back(i);
+        const int n = static_cast<int>(opt.size());
+        *n_out = n;
+        if (!pos) return 0;
+        const int total = db.totalNodes();
+        for (int k = 0; k < n; ++k) {
+            db.node_x[static_cast<size_t>(opt[static_cast<size_t>(k)])] = pos[k];
+            db.node_y[static_cast<size_t>(opt[static_cast<size_t>(k)])] = pos[n + k];
+        }
+        sp::BinGrid grid;
+        grid.initialize(db, cfg.target_density, cfg.gp_bin_dim, cfg.density_chunks, false, cfg.fftw_threads);
+        sp::WaWirelength wl;
+        wl.prepare(db);
+        std::vector<float> force(static_cast<size_t>(2 * total), 0.f);
+        std::vector<float> gradWl(static_cast<size_t>(2 * db.numMovable), 0.f);
+        grid.accumulate(db);
+        const float tau = grid.overflow();
+        grid.solveField();
+        grid.gatherForce(db, force.data());
+        double wlObj = 0.0;
+        wl.compute(db, gamma, cfg.ignore_net_degree, &wlObj, gradWl.data());
+        const double hpwl = sp::computeHPWL(db);
+        const int nMov = db.numMovable;
+        const double sumWl = sp::deterministicSumWithWork(n, [&](int64_t kk, double& accWl) {
+            const int k = static_cast<int>(kk);
+            const int i = opt[static_cast<size_t>(k)];
+            const bool hasWl = i < nMov;
+            const float wlx = hasWl ? gradWl[static_cast<size_t>(i)] : 0.f;
+            const float wly = hasWl ? gradWl[static_cast<size_t>(nMov + i)] : 0.f;
+            const float fx = force[static_cast<size_t>(i)];
+            const float fy = force[static_cast<size_t>(total + i)];
+            const double degree = static_cast<double>(db.nodeDegree(i));
+            const float precond =
+                static_cast<float>(1.0 / std::max(1.0, degree + static_cast<double>(lambda) * db.area(i)));
+            grad[k] = precond * (wlx - lambda * fx);
+            grad[n + k] = precond * (wly - lambda * fy);
+            if (hasWl) accWl += std::fabs(wlx) + std::fabs(wly);
+        });
+        const double sumDen = sp::deterministicSum(n, [&](int64_t kk) -> double {
+            const int i = opt[static_cast<size_t>(kk)];
+            return std::fabs(force[static_cast<size_t>(i)]) + std::fabs(force[static_cast<size_t>(total + i)]);
+        });
+        out[0] = wlObj;
+        out[1] = tau;
+        out[2] = hpwl;
+        out[3] = sumWl;
+        out[4] = sumDen;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// sp::legalizeMacros (src/lg/macro_sa.cpp:493): the SA macro legalisation GlobalPlaceStage runs
+// between mGP and FILLERONLY (src/stages/gp_stage.cpp:128-132); it leaves the macros F_FIXED.
+// res[0..5] = numMacros, overlapBefore, overlapAfter, hpwlBefore, hpwlAfter, repaired.
+int spref_legalize_macros(void* dbh, const spg_params* p, double* res) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(dbh)->db;
+        const sp::Config cfg = makeConfig(p);
+        sp::MetricsSink sink;
+        const sp::MacroSaResult r = sp::legalizeMacros(db, cfg, sink);
+        const double v[6] = {double(r.numMacros), r.overlapBefore, r.overlapAfter, r.hpwlBefore, r.hpwlAfter,
+                             double(r.repaired)};
+        std::memcpy(res, v, sizeof v);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// The GP stage sequence of GlobalPlaceStage::run for a design with movable macros
+// (src/stages/gp_stage.cpp:99-201), on a handle whose fillers are already initialised:
+// mGP, legalizeMacros, scatterFillers with seed offset 1, FILLERONLY, cGP, each EPlace built
+// anew. res = 3 stage results of 8 (putResult: mGP, FILLERONLY, cGP) then the 6 values of
+// spref_legalize_macros.
+int spref_gp_four_stage(void* dbh, const spg_params* p, double* res) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(dbh)->db;
+        const sp::Config cfg = makeConfig(p);
+        sp::MetricsSink sink;
+        const sp::GpStage order[3] = {sp::GpStage::kMGP, sp::GpStage::kFillerOnly, sp::GpStage::kCGP};
+        for (int s = 0; s < 3; ++s) {
+            if (s == 1) {
+                const sp::MacroSaResult r = sp::legalizeMacros(db, cfg, sink);
+                const double v[6] = {double(r.numMacros), r.overlapBefore, r.overlapAfter, r.hpwlBefore,
+                                     r.hpwlAfter, double(r.repaired)};
+                std::memcpy(res + 24, v, sizeof v);
+                sp::scatterFillers(db, cfg, 1);
+            }
+            const double t0 = omp_get_wtime();
+            sp::GpResult r;
+            {
+                sp::EPlace engine(db, cfg, sink);
+                r = engine.run(order[s]);
+            }
+            putResult(r, (omp_get_wtime() - t0) * 1e3, res + 8 * s);
+        }
         return 0;
     } catch (const std::exception& e) {
         return fail(e);
@@ -503,51 +641,6 @@ int spref_abacus(void* h, int area_weight, int reference_trials, double* res) {
     } catch (const std::exception& e) {
         return fail(e);
     }
-}
-
-// The reference's RandomPlacer (method 0) or ClusterPlacer with first-choice (1) or best-choice
-// (2) matching on the handle's PlaceDB (src/init/random_placer.cpp, src/init/cluster_common.cpp).
-int spref_init_place(void* h, int method, unsigned long long seed, int target_count, int ignore_net_degree) {
-    try {
-        sp::Config cfg;
-        cfg.random_seed = seed;
-        cfg.cluster_target_count = target_count;
-        cfg.ignore_net_degree = ignore_net_degree;
-        sp::MetricsSink sink;
-        std::unique_ptr<sp::IInitialPlacer> p;
-        if (method == 0) p = std::make_unique<sp::RandomPlacer>();
-        else if (method == 1) p = std::make_unique<sp::ClusterPlacer>(sp::makeFirstChoiceMatcher(), "cluster_fc");
-        else p = std::make_unique<sp::ClusterPlacer>(sp::makeBestChoiceMatcher(), "cluster_bc");
-        p->place(static_cast<RefDb*>(h)->db, cfg, sink);
-        return 0;
-    } catch (const std::exception& e) {
-        return fail(e);
-    }
-}
-
-// sp::DbStats::compute of the handle's PlaceDB: v[0..13] = coreLx, coreLy, coreHx, coreHy,
-// rowHeight, rowCount, siteStep, coreArea, movableArea, fixedArea, fixedAreaInCore, totalRowArea,
-// maxNetDegree, degreeOver; hist[0..4] the histogram; text (up to cap) toString's text.
-void spref_db_stats(void* h, double* v, int* hist, char* text, int cap) {
-    const sp::DbStats s = sp::DbStats::compute(static_cast<RefDb*>(h)->db);
-    const double a[14] = {s.coreLx, s.coreLy, s.coreHx, s.coreHy, s.rowHeight, double(s.rowCount), s.siteStep,
-                          s.coreArea, s.movableArea, s.fixedArea, s.fixedAreaInCore, s.totalRowArea,
-                          double(s.maxNetDegree), double(s.degreeOver)};
-    std::memcpy(v, a, sizeof a);
-    for (int k = 0; k < 5; ++k) hist[k] = s.degreeHistogram[static_cast<size_t>(k)];
-    const std::string t = s.toString();
-    std::snprintf(text, static_cast<size_t>(cap), "%s", t.c_str());
-}
-
-// sp::buildAbacusSegments: up to cap of (row, lx, hx); returns how many there are.
-int spref_abacus_segments(void* h, int* row, float* lx, float* hx, int cap) {
-    const auto segs = sp::buildAbacusSegments(static_cast<RefDb*>(h)->db);
-    for (int k = 0; k < std::min<int>(cap, static_cast<int>(segs.size())); ++k) {
-        row[k] = segs[static_cast<size_t>(k)].row;
-        lx[k] = segs[static_cast<size_t>(k)].lx;
-        hx[k] = segs[static_cast<size_t>(k)].hx;
-    }
-    return static_cast<int>(segs.size());
 }
 
 // sp::BookshelfReader::readPlacement (src/io/bookshelf_reader.cpp) into the handle's PlaceDB.

@@ -1405,6 +1405,22 @@ bool graph_loop(Context& c, const DevPtrs& p) {
     return true;
 }
 
+// What constructing EPlace and buildOptSet do for a stage (gp_stage.cpp:175-177,
+// eplace.cpp:82-133): the grid rebuilt with the current flags, then the stage's opt set.
+void prepare_stage(Context& c, int stage, HostTimer* ht) {
+    if (!c.mirror_valid) {
+        c.x_mirror.resize(c.num_nodes);
+        c.y_mirror.resize(c.num_nodes);
+        download_bytes(c.x_mirror.data(), c.x.p, c.num_nodes * sizeof(float), c.stream);
+        download_bytes(c.y_mirror.data(), c.y.p, c.num_nodes * sizeof(float), c.stream);
+    }
+    grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, c.x_mirror, c.y_mirror);
+    c.mirror_valid = false;  // the stage moves the positions
+    if (ht) ht->mark("grid_init");
+    stage_setup(c, stage);
+    if (ht) ht->mark("stage_setup");
+}
+
 // EPlace::run (eplace.cpp:223-526) for one stage, device-resident.
 void stage_run(Context& c, int stage, spg_result* res) {
     SPG_REQUIRE(stage >= SPG_STAGE_MGP && stage <= SPG_STAGE_CGP, SPG_E_INVALID, "unknown stage");
@@ -1412,20 +1428,7 @@ void stage_run(Context& c, int stage, spg_result* res) {
     std::memset(res, 0, sizeof(*res));
     res->rollback_iter = -1;
     cudaStream_t s = c.stream;
-    // constructing EPlace rebuilds the grid with the current flags (gp_stage.cpp:175-177)
-    {
-        if (!c.mirror_valid) {
-            c.x_mirror.resize(c.num_nodes);
-            c.y_mirror.resize(c.num_nodes);
-            download_bytes(c.x_mirror.data(), c.x.p, c.num_nodes * sizeof(float), s);
-            download_bytes(c.y_mirror.data(), c.y.p, c.num_nodes * sizeof(float), s);
-        }
-        grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, c.x_mirror, c.y_mirror);
-        c.mirror_valid = false;  // the stage moves the positions
-    }
-    ht.mark("grid_init");
-    stage_setup(c, stage);
-    ht.mark("stage_setup");
+    prepare_stage(c, stage, &ht);
     if (c.n_opt == 0) return;  // "no nodes to optimise" (eplace.cpp:232-236)
     const bool filler_only = stage == SPG_STAGE_FILLER_ONLY;
     const float target_tau = stage == SPG_STAGE_CGP ? c.prm.cgp_target_overflow : c.prm.target_overflow;
@@ -1508,6 +1511,144 @@ void stage_run(Context& c, int stage, spg_result* res) {
               std::fabs(res->hpwl - row.hpwl) <= 1e-6 + 1e-10 * std::fabs(row.hpwl)))
             throw Error(SPG_E_ROLLBACK, "delivered metrics disagree with rollback point");
     }
+}
+
+// lambda and gamma of an evaluation outside the loop; `done` set, so the loop body's step
+// kernel applies no step (it rasterizes the current u) and its decisions are skipped.
+__global__ void set_eval_kernel(DevState* st, float lambda, float gamma) {
+    st->lambda = lambda;
+    st->gamma = gamma;
+    st->done = 1;
+}
+
+// EPlace::Impl::objAndGrad (eplace.cpp:136-203) at opt-set positions pos (x then y, the opt
+// order of buildOptSet) for the given lambda and gamma, through the GP loop body's own kernels
+// (enqueue_iteration): the step kernel's fixed-point scatter of u, the WA pass 1 with HPWL,
+// the rest-list scatter, rho and tau, the Poisson solve, the large nodes' gather, and the
+// fused assembly (cell gather, WA pass 2, preconditioned gradient). grad gets 2*nOpt floats;
+// out[0..4] = WA value, tau, HPWL, sum|grad WL|, sum|q xi|; *n_opt the opt-set size. With
+// pos = NULL only *n_opt is set. The grid and opt set are rebuilt for `stage` from the
+// context's positions and flags first, as constructing EPlace does.
+void eval_grad(Context& c, int stage, float lambda, float gamma, const float* pos, float* grad, double* out,
+               int* n_opt) {
+    SPG_REQUIRE(stage >= SPG_STAGE_MGP && stage <= SPG_STAGE_CGP, SPG_E_INVALID, "unknown stage");
+    prepare_stage(c, stage, nullptr);
+    *n_opt = c.n_opt;
+    if (!pos || c.n_opt == 0) return;
+    SPG_REQUIRE(grad && out, SPG_E_INVALID, "eval_grad: null output");
+    cudaStream_t s = c.stream;
+    DevPtrs p = c.ptrs();
+    init_state_kernel<<<1, 1, 0, s>>>(p, stage, 1, 0.f);
+    set_eval_kernel<<<1, 1, 0, s>>>(p.st, lambda, gamma);
+    count_launch(2);
+    SPG_CHECK_LAUNCH();
+    const size_t n2 = 2 * static_cast<size_t>(c.n_opt);
+    // the roles start as the identity, so role R_U is pool slot R_U
+    upload_bytes(c.pool.p + static_cast<size_t>(R_U) * c.vec_stride, pos, n2 * sizeof(float), s);
+    launch_scatter(p, R_U, s);  // node positions for the WA pass and the large nodes
+    enqueue_iteration(c, p);
+    read_state(c);
+    download_bytes(grad, c.pool.p + static_cast<size_t>(c.hst->role[R_G]) * c.vec_stride, n2 * sizeof(float), s);
+    const DevState& h = *c.hst;
+    out[0] = h.wl_obj;
+    out[1] = h.tau;
+    out[2] = h.hpwl;
+    out[3] = h.sum_wl;
+    out[4] = h.sum_den;
+}
+
+__global__ void set_alpha0_kernel(DevState* st, float a) { st->alpha0 = a; }
+
+// NesterovOptimizer::step called `steps` times (src/numeric/cpu/nesterov.cpp:51-122) on the
+// quadratic test objective of quad_eval_kernel, with the GP loop's own step kernel, redo test
+// and step decisions: the optimizer vectors in the role pool, estimateInitialStep's two
+// uncounted evaluations (or alpha0 = init_step when positive), then one counted evaluation
+// per pass. n coordinates (even: the pool holds them as n/2 x-y pairs); no constraint, as in
+// the reference's optimizer tests. pos: the start in, the current solution v out.
+// out[0..3] = objective of the last counted evaluation, evaluations, step size, re-evaluations.
+void nesterov_quadratic(int n, const float* coef, const float* target, float* pos, int steps, int use_bb,
+                        int backtrack, int max_backtrack, float init_step, double* out) {
+    SPG_REQUIRE(n >= 2 && n % 2 == 0 && steps >= 0 && max_backtrack >= 1, SPG_E_INVALID,
+                "nesterov_quadratic: n must be even and >= 2, steps >= 0, max_backtrack >= 1");
+    SPG_REQUIRE(coef && target && pos && out, SPG_E_INVALID, "nesterov_quadratic: null pointer");
+    cudaStream_t s = nullptr;
+    SPG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() {
+            host_wait(s);
+            cudaStreamDestroy(s);
+        }
+    } guard{s};
+    const size_t nn = static_cast<size_t>(n);
+    const size_t stride = (nn + 63) / 64 * 64;
+    DevBuf<float> pool, lo, hi, c, t;
+    DevBuf<DevState> st;
+    DevBuf<double> partials;
+    pool.alloc(stride * NUM_ROLES);
+    pool.zero(s);
+    lo.upload(std::vector<float>(nn, -INFINITY), s);
+    hi.upload(std::vector<float>(nn, INFINITY), s);
+    c.upload(coef, nn, s);
+    t.upload(target, nn, s);
+    st.alloc(1);
+    partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_CAP);
+    partials.zero(s);
+    DevPtrs p{};
+    p.n_opt = n / 2;
+    p.pool = pool.p;
+    p.vec_stride = stride;
+    p.st = st.p;
+    p.partials = partials.p;
+    p.opt_lo = lo.p;
+    p.opt_hi = hi.p;
+    p.filler_k0 = p.n_opt;
+    p.use_bb = use_bb;
+    p.backtrack = backtrack;
+    p.max_backtrack = max_backtrack;
+    init_state_kernel<<<1, 1, 0, s>>>(p, SPG_STAGE_MGP, steps, 0.f);
+    count_launch();
+    SPG_CHECK_LAUNCH();
+    upload_bytes(pool.p + static_cast<size_t>(R_POS) * stride, pos, nn * sizeof(float), s);
+    DevState h{};
+    auto read = [&] {
+        SPG_CUDA(cudaMemcpyAsync(&h, st.p, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+        SPG_CUDA(host_wait(s));
+        if (h.error) throw Error(h.error, "nesterov_quadratic: non-finite coordinate or gradient");
+    };
+    if (steps > 0) {
+        // NesterovOptimizer::init (nesterov.cpp:173-186)
+        for (int r : {R_U, R_V, R_UPREV, R_VPREV}) launch_copy_role(p, r, R_POS, s);
+        if (init_step > 0.f) {
+            set_alpha0_kernel<<<1, 1, 0, s>>>(st.p, init_step);
+            count_launch();
+            SPG_CHECK_LAUNCH();
+        } else {
+            launch_quad_eval(p, c.p, t.p, R_U, R_GA, 0, s);
+            launch_init_norms(p, s);
+            launch_ctl_init_scale(p, 0.1f, s);
+            launch_init_perturb(p, s);
+            launch_quad_eval(p, c.p, t.p, R_PROBE, R_GB, 0, s);
+            launch_init_diff(p, s);
+            launch_ctl_init_finish(p, s);
+        }
+        launch_quad_eval(p, c.p, t.p, R_U, R_G, 1, s);
+        read();
+        // each pass is a step or a re-evaluation: at most max_backtrack per step
+        const int64_t bound = static_cast<int64_t>(steps + 1) * max_backtrack + 2;
+        int64_t passes = 0;
+        while (!h.done) {
+            SPG_REQUIRE(++passes <= bound, SPG_E_STATE, "nesterov_quadratic: pass bound exceeded");
+            launch_quad_step(p, s);
+            launch_quad_eval(p, c.p, t.p, R_U, R_G, 1, s);
+            read();
+        }
+        download_bytes(pos, pool.p + static_cast<size_t>(h.role[R_V]) * stride, nn * sizeof(float), s);
+    }
+    out[0] = h.wl_obj;
+    out[1] = static_cast<double>(h.evals);
+    out[2] = steps > 0 ? h.alpha : 0.0;
+    out[3] = static_cast<double>(h.redos);
 }
 
 int fail(const std::exception& e) {
@@ -2228,6 +2369,28 @@ int64_t spg_ctx_launch_count(const spg_ctx* ctx) {
 void* spg_ctx_stream(const spg_ctx* ctx) { return ctx ? static_cast<void*>(ctx->c.stream) : nullptr; }
 
 int spg_ctx_graph_loop(const spg_ctx* ctx) { return ctx && ctx->c.last_run_graph ? 1 : 0; }
+
+int spg_eval_grad(spg_ctx* ctx, int stage, float lambda, float gamma, const float* pos, float* grad, double* out,
+                  int32_t* n_opt) {
+    API_TRY
+    SPG_REQUIRE(ctx && n_opt, SPG_E_INVALID, "null argument");
+    spg::CtxScope scope(ctx->c);
+    spg::eval_grad(ctx->c, stage, lambda, gamma, pos, grad, out, n_opt);
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_nesterov_quadratic(int32_t n, const float* coef, const float* target, float* pos, int32_t steps,
+                           int32_t use_bb, int32_t backtrack, int32_t max_backtrack, float init_step,
+                           double* out) {
+    try {
+        if (!spg::device_ok()) return spg::fail(Error(SPG_E_NO_DEVICE, "no sm_100 device"));
+        spg::nesterov_quadratic(n, coef, target, pos, steps, use_bb, backtrack, max_backtrack, init_step, out);
+        return SPG_OK;
+    } catch (const std::exception& e) {
+        return spg::fail(e);
+    }
+}
 
 int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     API_TRY

@@ -268,6 +268,14 @@ void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, cudaGraphCondition
 // decisions asked for one) with the density scatter of the new positions fused in; the
 // evaluation that follows accumulates only the rest list
 void launch_update(const DevPtrs& p, cudaStream_t s);
+// the same step over the optimizer vectors alone (no node arrays, no density), clamped into
+// opt_lo / opt_hi: the optimizer run on the quadratic test objective
+void launch_quad_step(const DevPtrs& p, cudaStream_t s);
+// the quadratic test objective 0.5 sum c (x - t)^2 over the 2*nOpt coordinates: fused = the
+// counted evaluation of the iteration with its norms and decisions, else an uncounted one of
+// pos_role into grad_role
+void launch_quad_eval(const DevPtrs& p, const float* coef, const float* target, int pos_role, int grad_role,
+                      int fused, cudaStream_t s);
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s);
 void launch_init_norms(const DevPtrs& p, cudaStream_t s);
 void launch_ctl_init_scale(const DevPtrs& p, float init_perturb, cudaStream_t s);

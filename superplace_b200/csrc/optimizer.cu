@@ -305,8 +305,6 @@ __global__ void scatter_kernel(DevPtrs p, int role) {
 }
 
 // force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it
-// (bin_grid.cpp:287-318).
-// force = sum over the footprint of q * xi, bx outer, by inner, as gatherForce sums it
 // (bin_grid.cpp:287-318), for a node at (x, y) with smoothed half extents hw, hh and charge
 // weight w. Footprints of at most 2x2 bins (every cell no wider than one bin) issue their
 // eight field loads before the sums, which keep the reference's order.
@@ -412,7 +410,10 @@ __device__ void finish_evaluation(const DevPtrs& p, DevState* st, const double* 
 }
 
 // The decisions after a counted evaluation, on the state `st` (a shared-memory copy): the
-// redo test and, when no re-evaluation is due, the step and iteration decisions.
+// redo test and, when no re-evaluation is due, the step decisions and then, for the EPlace
+// loop (EPLACE), the iteration decisions of eplace.cpp; a plain optimizer run (the quadratic
+// test objective) only marks its last step.
+template <bool EPLACE = true>
 __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, double sy2, double gn2) {
     st->tk_reduce = 0;
     st->dx = sqrt(dx2);
@@ -435,7 +436,8 @@ __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, d
         }
         if (!st->redo) {
             decide_step(p, st);
-            decide_iteration(p, st);
+            if (EPLACE) decide_iteration(p, st);
+            else if (st->iter + 1 >= st->max_iter) st->last = 1;
         }
     }
 }
@@ -575,6 +577,17 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
     state_copy_out(p.st, &sst);
 }
 
+// One coordinate of the Nesterov point (nesterov.cpp:97-107, and the redoIfOvershot body
+// :158-163 with uPrev, gPrevTmp, vPrev and momentumPrev in place of u, g, v and momentum):
+//   v' = u - alpha g ; u' = v' + m (v' - v) ; both clamped into [lo, hi] afterwards.
+__device__ __forceinline__ void nesterov_point(float u, float v, float g, float alpha, float m, float lo,
+                                               float hi, float& vn, float& un) {
+    const float vk = fsub(u, fmul(alpha, g));
+    const float uk = fadd(vk, fmul(m, fsub(vk, v)));
+    vn = clamp_box(vk, lo, hi);
+    un = clamp_box(uk, lo, hi);
+}
+
 // The loop's position step with the density scatter of the new positions fused in. One
 // launch per loop pass; the pass applies whichever step the last decisions asked for:
 //
@@ -586,20 +599,23 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
 //     The role rotation uPrev <- u <- u' ; vPrev <- v <- v' ; gPrevTmp <- g and the loop
 //     counter follow in the next assembly's last block (apply_pending_step).
 //
-// The new u is written into the node positions (for the WA pass) and its fixed-point charge
-// is added to the density maps right here (BinGrid::accumulate, bin_grid.cpp:191-251), so
-// the evaluation needs no separate pass over the cells; nodes whose footprint may exceed 16
-// bins are left to the block-per-node kernel of the rest list. When no step applies (the
-// stage is done) the current u is rasterized unchanged.
+// PLACE (the GP loop): the new u is written into the node positions (for the WA pass) and
+// its fixed-point charge is added to the density maps right here (BinGrid::accumulate,
+// bin_grid.cpp:191-251), so the evaluation needs no separate pass over the cells; nodes whose
+// footprint may exceed 16 bins are left to the block-per-node kernel of the rest list. When
+// no step applies (the stage is done) the current u is rasterized unchanged. Without PLACE
+// (a plain optimizer run over a test objective) only the optimizer vectors are written, with
+// the per-coordinate clamp bounds opt_lo / opt_hi.
 // 40 registers (6 blocks of 256 per SM, no spills): the kernel is latency-bound, one node
 // per thread, so occupancy is what hides its loads and atomics
+template <bool PLACE>
 __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
     pdl_wait();
     pdl_trigger();
     DevState* st = p.st;
     const bool redo = st->redo != 0;
     const int apply = redo ? 1 : !st->done;
-    const int slot = redo ? -1 : st->snap_copy_to;
+    const int slot = (redo || !PLACE) ? -1 : st->snap_copy_to;
     const float* u = role_ptr(p, redo ? R_UPREV : R_U);
     const float* v = role_ptr(p, redo ? R_VPREV : R_V);
     const float* g = role_ptr(p, redo ? R_GPREVTMP : R_G);
@@ -611,9 +627,13 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
     const int n = p.n_opt;
     bool bad = false;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const bool fill = k >= p.filler_k0;  // a filler: attributes are the shared constants
-        const int4 meta = fill ? p.filler_meta : p.opt_meta[k];
-        const float4 geo = fill ? p.filler_geom : p.opt_geom[k];
+        const bool fill = PLACE && k >= p.filler_k0;  // a filler: attributes are the shared constants
+        int4 meta{};
+        float4 geo{};
+        if (PLACE) {
+            meta = fill ? p.filler_meta : p.opt_meta[k];
+            geo = fill ? p.filler_geom : p.opt_geom[k];
+        }
         float nu[2];
         if (apply) {
 #pragma unroll
@@ -621,18 +641,15 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
                 const int q = c * n + k;
                 const float uq = u[q];
                 if (snap) snap[q] = uq;
-                const float vk = fsub(uq, fmul(alpha, g[q]));
-                const float uk = fadd(vk, fmul(m, fsub(vk, v[q])));
                 const float lo = fill ? (c ? p.filler_lo_y : p.filler_lo_x) : p.opt_lo[q];
                 const float hi = fill ? (c ? p.filler_hi_y : p.filler_hi_x) : p.opt_hi[q];
-                vn[q] = clamp_box(vk, lo, hi);
-                nu[c] = clamp_box(uk, lo, hi);
+                nesterov_point(uq, v[q], g[q], alpha, m, lo, hi, vn[q], nu[c]);
                 un[q] = nu[c];
             }
             bad |= !isfinite(nu[0]) || !isfinite(nu[1]);
             // the node arrays: read inside the loop only for cells (WA) and large nodes (their
             // gather); the fillers' entries are rewritten from R_POS when the stage ends
-            if (!fill || (meta.w & K_LARGE)) {
+            if (PLACE && (!fill || (meta.w & K_LARGE))) {
                 const int i = fill ? p.filler_node0 + k : p.opt_idx[k];
                 p.x[i] = nu[0];
                 p.y[i] = nu[1];
@@ -645,12 +662,83 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
                 snap[n + k] = nu[1];
             }
         }
-        if (!(meta.w & K_LARGE)) rasterize(p, nu[0], nu[1], geo.x, geo.y, geo.z, (meta.w & K_FILLER) != 0);
+        if (PLACE && !(meta.w & K_LARGE)) rasterize(p, nu[0], nu[1], geo.x, geo.y, geo.z, (meta.w & K_FILLER) != 0);
     }
     if (bad) raise_error(st, SPG_E_NON_FINITE);
     // the rest of the step (apply_pending_step) runs in the next assembly's last block; every
     // block read the state above before this store can matter to anyone
     if (!redo && blockIdx.x == 0 && threadIdx.x == 0) st->step_pending = apply ? 2 : 1;
+}
+
+// ------------------------------------------------------------------ quadratic test objective
+// f(x) = 0.5 * sum_i c_i (x_i - t_i)^2 over the 2*nOpt optimizer coordinates, with gradient
+// (float)(c_i (x_i - t_i)) and the objective summed in FP64: the objective of the reference's
+// optimizer tests (test/test_nesterov.cpp:14-27). It drives the loop's own step kernel,
+// redo test and step decisions without a placement, so the optimizer can be checked against
+// the reference's NesterovOptimizer on its known answers.
+//
+// FUSE: an evaluation of the iteration (at u = R_U into g = R_G, counted) with the step's four
+// norms, whose last block applies the pending step, records the objective and decides;
+// otherwise an uncounted evaluation of pos_role into grad_role (estimateInitialStep).
+template <bool FUSE>
+__global__ void __launch_bounds__(RED_THREADS) quad_eval_kernel(DevPtrs p, const float* __restrict__ coef,
+                                                                const float* __restrict__ target, int pos_role,
+                                                                int grad_role) {
+    pdl_wait();
+    pdl_trigger();
+    const int pending = p.st->step_pending;
+    const float* __restrict__ pos = role_ptr_pending(p, FUSE ? R_U : pos_role, pending);
+    float* __restrict__ grad = role_ptr_pending(p, FUSE ? R_G : grad_role, pending);
+    const float* __restrict__ up = FUSE ? role_ptr_pending(p, R_UPREV, pending) : nullptr;
+    const float* __restrict__ gp = FUSE ? role_ptr_pending(p, R_GPREVTMP, pending) : nullptr;
+    const int n = 2 * p.n_opt;
+    double obj = 0.0, dx = 0.0, dg = 0.0, sy = 0.0, gn = 0.0;
+    bool bad = false;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float x = pos[k];
+        const double c = static_cast<double>(coef[k]);
+        const double d = static_cast<double>(x) - static_cast<double>(target[k]);
+        obj += __dmul_rn(__dmul_rn(0.5 * c, d), d);
+        const float gk = static_cast<float>(__dmul_rn(c, d));
+        grad[k] = gk;
+        bad |= !isfinite(x) || !isfinite(gk);
+        if (FUSE) {
+            const double sd = static_cast<double>(x) - static_cast<double>(up[k]);
+            const double yd = static_cast<double>(gk) - static_cast<double>(gp[k]);
+            dx += __dmul_rn(sd, sd);
+            dg += __dmul_rn(yd, yd);
+            sy += __dmul_rn(sd, yd);
+            gn += __dmul_rn(static_cast<double>(gk), static_cast<double>(gk));
+        }
+    }
+    if (bad) raise_error(p.st, SPG_E_NON_FINITE);
+    if (!FUSE) return;
+    double v5[5] = {obj, dx, dg, sy, gn};
+    block_sums(v5);
+    put_partial(p, SLOT_WL, v5[0]);
+    put_partial(p, SLOT_DX, v5[1]);
+    put_partial(p, SLOT_DG, v5[2]);
+    put_partial(p, SLOT_SY, v5[3]);
+    put_partial(p, SLOT_GN, v5[4]);
+    if (!last_block(&p.st->tk_assemble)) return;
+    constexpr int kSlots[5] = {SLOT_WL, SLOT_DX, SLOT_DG, SLOT_SY, SLOT_GN};
+    double sums[5];
+    finalize_n(p, kSlots, sums);
+    __shared__ DevState sst;
+    state_copy_in(&sst, p.st);
+    if (threadIdx.x == 0) {
+        DevState* q = &sst;
+        apply_pending_step(q);
+        q->tk_assemble = 0;
+        if (!isfinite(sums[0])) raise_error(q, SPG_E_NON_FINITE);
+        // the objective of the last counted evaluation (NesterovOptimizer::objective)
+        if (!q->done) {
+            q->evals += 1;
+            q->wl_obj = sums[0];
+        }
+        decide<false>(p, q, sums[1], sums[2], sums[3], sums[4]);
+    }
+    state_copy_out(p.st, &sst);
 }
 
 __global__ void copy_role_kernel(DevPtrs p, int dst, int src) {
@@ -870,7 +958,20 @@ inline int node_blocks(const DevPtrs& p) {
     return b < 1 ? 1 : b;
 }
 void launch_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(step_kernel, node_blocks(p), RED_THREADS, p);
+    LAUNCH(step_kernel<true>, node_blocks(p), RED_THREADS, p);
+}
+void launch_quad_step(const DevPtrs& p, cudaStream_t s) {
+    LAUNCH(step_kernel<false>, node_blocks(p), RED_THREADS, p);
+}
+void launch_quad_eval(const DevPtrs& p, const float* coef, const float* target, int pos_role, int grad_role,
+                      int fused, cudaStream_t s) {
+    const int64_t n = 2 * static_cast<int64_t>(p.n_opt);
+    if (fused)
+        LAUNCH(quad_eval_kernel<true>, work_grid(reinterpret_cast<const void*>(quad_eval_kernel<true>), n, RED_THREADS),
+               RED_THREADS, p, coef, target, pos_role, grad_role);
+    else
+        LAUNCH(quad_eval_kernel<false>, work_grid(reinterpret_cast<const void*>(quad_eval_kernel<false>), n, RED_THREADS),
+               RED_THREADS, p, coef, target, pos_role, grad_role);
 }
 void launch_ctl_lambda_init(const DevPtrs& p, cudaStream_t s) {
     LAUNCH(ctl_lambda_init_kernel, 1, 1, p);

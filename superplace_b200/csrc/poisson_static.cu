@@ -7,12 +7,14 @@
 // caller cannot create a spg_poisson plan, because a plan allocates its basis tables and
 // work buffers with cudaMalloc.
 //
-// spg_poisson_solve_static() is the same plain-FP32 cosine-contraction solve as a plan's
-// solve (poisson.cu; the same kernels run through the same poisson_solve()), but its bases
-// and work buffers live in one file-scope device array, g_static_scratch, whose size is
-// fixed when the library is loaded: every GPU that loads the library holds those
-// kStaticScratchFloats floats (11 MB) until the process exits. The caller passes the
-// input and output grids.
+// spg_poisson_solve_static() is the plain-FP32 cosine-contraction solve of a plan (poisson.cu;
+// the same kernels run through the same poisson_solve()), but its bases and work buffers live
+// in one file-scope device array, g_static_scratch, whose size is fixed when the library is
+// loaded: every GPU that loads the library holds those kStaticScratchFloats floats (11 MB)
+// until the process exits. The caller passes the input and output grids. Its basis tables
+// are computed on the device (cospi / sinpi in FP64, rounded once to float) where a plan
+// computes them on the host, so a table entry may differ from the plan's by one float ulp:
+// the results agree with a plan's solve to 1e-5 of max|result|, not bit for bit.
 //
 // Limits and sharing:
 //   * nx, ny in [2, 512]; anything larger is rejected with SPG_E_CAPACITY.
@@ -22,9 +24,10 @@
 //     to start at zero. Calls whose work overlaps on the GPU (on different streams, or
 //     from different host threads) race on the array and corrupt each other's results;
 //     serialise them.
-//   * The first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress and caches it per device. Make that first call before any
-//     stream capture on that device.
+//   * Every call made outside a stream capture looks up the array's device address with
+//     cudaGetSymbolAddress (so a device reset cannot leave a stale address); a call on a
+//     stream being captured reuses the address of the last uncaptured call on its device.
+//     Make the first call on a device before any stream capture on that device.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -52,13 +55,18 @@ constexpr int kMaxDevices = 64;
 float* g_scratch_ptr[kMaxDevices] = {};
 std::mutex g_scratch_mutex;
 
-// Device address of g_static_scratch for the current device (looked up once per device).
-float* scratch_for_current_device() {
+// Device address of g_static_scratch for the current device. It is looked up again on every
+// call made outside a stream capture, so a device reset (which reloads the module and may move
+// the array) never leaves a stale address behind; a call made while `s` is being captured
+// uses the address of the last uncaptured call on that device, and fails when there was none.
+float* scratch_for_current_device(cudaStream_t s) {
     int dev = 0;
     SPG_CUDA(cudaGetDevice(&dev));
     SPG_REQUIRE(dev >= 0 && dev < kMaxDevices, SPG_E_INVALID, "device ordinal out of range");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    SPG_CUDA(cudaStreamIsCapturing(s, &cap));
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess)
@@ -66,6 +74,8 @@ float* scratch_for_current_device() {
                                         cudaGetErrorString(e));
         g_scratch_ptr[dev] = static_cast<float*>(p);
     }
+    SPG_REQUIRE(g_scratch_ptr[dev], SPG_E_STATE,
+                "spg_poisson_solve_static: the first call on a device must come before any stream capture");
     return g_scratch_ptr[dev];
 }
 
@@ -125,7 +135,8 @@ extern "C" int spg_poisson_solve_static(int nx, int ny, float step_x, float step
         SPG_REQUIRE(step_x > 0.f && step_y > 0.f, SPG_E_INVALID, "Poisson: bin step must be positive");
         SPG_REQUIRE(d_rho && d_phi && d_field_x && d_field_y, SPG_E_INVALID, "null argument");
         const int64_t X = nx, Y = ny;
-        float* base = scratch_for_current_device();
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+        float* base = scratch_for_current_device(s);
         int64_t off = 0;
         auto take = [&](int64_t n) {
             float* p = base + off;
@@ -150,7 +161,6 @@ extern "C" int spg_poisson_solve_static(int nx, int ny, float step_x, float step
         pl.dc = take(4 * std::max(X, Y));
         SPG_REQUIRE(off <= kStaticScratchFloats, SPG_E_CAPACITY,
                     "spg_poisson_solve_static: layout exceeds the static scratch array");
-        cudaStream_t s = static_cast<cudaStream_t>(stream);
         const int64_t work = Y * Y + X * X + X * Y;
         const int blocks = static_cast<int>(std::min<int64_t>((work + 255) / 256, 4096));
         static_bases_kernel<<<blocks, 256, 0, s>>>(nx, ny, step_x, step_y, pl.cy, pl.cx, pl.bcat,

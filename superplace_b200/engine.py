@@ -84,6 +84,9 @@ def lib():
         L.spg_ctx_stream.argtypes = [vp]
         L.spg_ctx_graph_loop.argtypes = [vp]
         L.spg_ctx_profile.argtypes = [vp, C.c_int, C.POINTER(C.c_double), C.c_int]
+        L.spg_eval_grad.argtypes = [vp, C.c_int, C.c_float, C.c_float, fp, fp, dp, ip]
+        L.spg_nesterov_quadratic.argtypes = [C.c_int32, fp, fp, fp, C.c_int32, C.c_int32, C.c_int32,
+                                             C.c_int32, C.c_float, dp]
         u8p, cp = C.POINTER(C.c_uint8), C.c_char_p
         L.spg_bookshelf_read.argtypes = [cp, C.POINTER(vp)]
         L.spg_bookshelf_last_error.restype = cp
@@ -161,6 +164,19 @@ def poisson_solve_static(nx, ny, step_x, step_y, rho_ptr, phi_ptr, fx_ptr, fy_pt
     check(lib().spg_poisson_solve_static(int(nx), int(ny), step_x, step_y, C.c_void_p(rho_ptr),
                                          C.c_void_p(phi_ptr), C.c_void_p(fx_ptr),
                                          C.c_void_p(fy_ptr), C.c_void_p(stream)))
+
+
+# ------------------------------------------------------------------ optimizer test hook
+def nesterov_quadratic(coef, target, pos, steps, use_bb=True, backtrack=False, init_step=0.0, max_backtrack=10):
+    """The stage loop's Nesterov optimizer on 0.5 * sum c (x - t)^2 (spg_nesterov_quadratic),
+    `steps` calls of NesterovOptimizer::step: (v, objective, evaluations, step size, redos)."""
+    coef = np.ascontiguousarray(coef, np.float32)
+    target = np.ascontiguousarray(target, np.float32)
+    pos = np.array(pos, np.float32)
+    out = (C.c_double * 4)()
+    check(lib().spg_nesterov_quadratic(pos.size, abi.fptr(coef), abi.fptr(target), abi.fptr(pos), steps,
+                                       int(use_bb), int(backtrack), max_backtrack, init_step, out))
+    return pos, out[0], int(out[1]), out[2], int(out[3])
 
 
 # ------------------------------------------------------------------ fillers
@@ -341,6 +357,24 @@ class GpContext:
         v = C.c_double()
         check(lib().spg_hpwl(self.h, C.byref(v)))
         return v.value
+
+    def n_opt(self, stage=abi.STAGE_MGP) -> int:
+        """Size of the stage's optimisation set (buildOptSet) at the context's flags."""
+        n = C.c_int()
+        check(lib().spg_eval_grad(self.h, stage, 1.0, 1.0, None, None, None, C.byref(n)))
+        return n.value
+
+    def eval_grad(self, stage, lam, gamma, pos):
+        """EPlace::Impl::objAndGrad (src/gp/eplace.cpp:136-203) at opt-set positions pos (x then
+        y) through the stage loop's own kernels: (grad, {obj, tau, hpwl, sum_wl, sum_den})."""
+        pos = np.ascontiguousarray(pos, np.float32)
+        grad = np.zeros_like(pos)
+        out = (C.c_double * 5)()
+        n = C.c_int()
+        check(lib().spg_eval_grad(self.h, stage, lam, gamma, abi.fptr(pos), abi.fptr(grad), out, C.byref(n)))
+        if pos.size != 2 * n.value:
+            raise ValueError(f"eval_grad: {pos.size} coordinates for an opt set of {n.value} nodes")
+        return grad, dict(zip(("obj", "tau", "hpwl", "sum_wl", "sum_den"), list(out)))
 
     # EPlace
     def run(self, stage=abi.STAGE_MGP) -> abi.Result:

@@ -1,36 +1,77 @@
-"""The reference's placement pipeline (src/main.cpp:55-115; stages parse, init, gp, lg and the
-.pl write) over this package:
+"""The GP stage and the reference's placement pipeline (src/main.cpp:55-115) over this package.
 
   parse  read_bookshelf                 BookshelfReader::read
-  init   QuadraticPlacer (B2B QP)       makeInitialPlacer("quadratic"), the default init_method;
-                                        "random", "cluster_fc", "cluster_bc" by init_method
-  gp     fillers + the device mGP loop  GlobalPlaceStage::run (src/stages/gp_stage.cpp)
-  lg     Abacus                         LegalizeStage::run (src/stages/lg_stage.cpp:12-41)
+  init   QuadraticPlacer (B2B QP)       makeInitialPlacer("quadratic"), the default init_method
+  gp     global_place                   GlobalPlaceStage::run (src/stages/gp_stage.cpp:59-244)
+  lg     the caller's cell legaliser    LegalizeStage::run (src/stages/lg_stage.cpp:12-41)
   write  write_pl                       BookshelfWriter::writePl
 
-GlobalPlaceStage runs only mGP when no movable macro exists (src/stages/gp_stage.cpp:114-117).
-With movable macros it needs macro legalisation (mLG), which this package does not provide:
-the flow stops after mGP and says so in the report.
+Macro legalisation (mLG, the reference's simulated annealing, src/lg/macro_sa.cpp:493) and
+cell legalisation (Abacus, src/lg/abacus.cpp:155) stay host code on the reference's side of
+the boundary: the caller passes them in as callables over the PlaceDB, the way
+GlobalPlaceStage and the pipeline call them between the device stages. Without an mLG
+callable a design with movable macros stops after mGP; without a cell legaliser the lg stage
+is skipped.
 """
 from __future__ import annotations
 
 import time
+from typing import Callable
 
 import numpy as np
 
-from . import abi, bookshelf, engine, initial, legalize, qp, stats
+from . import abi, bookshelf, engine, qp
 from .placedb import F_FIXED, F_MACRO, PlaceDB
 
 STAGES = ("parse", "init", "gp", "lg", "write")
+
+Legaliser = Callable[[PlaceDB], dict]
 
 
 def _hpwl(db: PlaceDB) -> float:
     return qp.host_hpwl(db)
 
 
+def movable_macros(db: PlaceDB) -> np.ndarray:
+    """Indices of the movable macros not yet fixed (GlobalPlaceStage's count, gp_stage.cpp:80-84)."""
+    f = db.node_flags[: db.num_movable]
+    return np.nonzero(((f & F_MACRO) != 0) & ((f & F_FIXED) == 0))[0]
+
+
+def global_place(db: PlaceDB, params: abi.Params | None = None, legalize_macros: Legaliser | None = None,
+                 metrics: list | None = None) -> dict:
+    """GlobalPlaceStage::run (src/stages/gp_stage.cpp:59-244) on the device: fillers, mGP, then
+    for designs with movable macros mLG (the caller's `legalize_macros`, which must leave every
+    macro F_FIXED), fillers re-scattered with seed offset 1, FILLERONLY and cGP. The positions
+    of the frozen macros are checked bit for bit after cGP (gp_stage.cpp:205-225). Returns each
+    stage's result (abi.Result) and, with mLG, the legaliser's report; `stopped` says why the
+    sequence ended early."""
+    p = params or abi.default_params()
+    out: dict = {}
+    engine.initialize_fillers(db, p.target_density, p.random_seed)
+    ep = engine.EPlace(db, p)
+    out["mGP"] = ep.run(abi.STAGE_MGP, metrics)
+    macros = movable_macros(db)
+    if macros.size == 0:
+        return out
+    if legalize_macros is None:
+        out["stopped"] = f"{macros.size} movable macros need mLG and no macro legaliser was given; stopped after mGP"
+        return out
+    out["mLG"] = legalize_macros(db)
+    if np.any((db.node_flags[macros] & F_FIXED) == 0):
+        raise engine.SpgError(abi.SPG_E_STATE, "mLG left a movable macro unfixed")
+    mx, my = db.node_x[macros].copy(), db.node_y[macros].copy()
+    engine.scatter_fillers(db, p.random_seed, seed_offset=1)
+    out["FILLERONLY"] = ep.run(abi.STAGE_FILLER_ONLY, metrics)
+    out["cGP"] = ep.run(abi.STAGE_CGP, metrics)
+    if not (np.array_equal(db.node_x[macros], mx) and np.array_equal(db.node_y[macros], my)):
+        raise engine.SpgError(abi.SPG_E_STATE, "a frozen macro changed position during cGP")
+    return out
+
+
 def place(aux: str | None = None, db: PlaceDB | None = None, out_pl: str | None = None,
           stages=STAGES, params: abi.Params | None = None, qp_params=None,
-          init_method: str = "quadratic") -> tuple[PlaceDB, dict]:
+          legalize_macros: Legaliser | None = None, legalize_cells: Legaliser | None = None) -> tuple[PlaceDB, dict]:
     """Runs `stages` in order on the design of `aux` (or on `db`) and returns the PlaceDB and a
     report: per stage its wall time in ms and the HPWL after it, the GP and legalisation
     results, and `stopped` when a stage could not run."""
@@ -42,39 +83,27 @@ def place(aux: str | None = None, db: PlaceDB | None = None, out_pl: str | None 
     if "parse" in stages:
         t0 = time.perf_counter()
         db = bookshelf.read_bookshelf(aux)
-        st = stats.db_stats(db)
-        done("parse", t0, nodes=st.node_count, fixed=st.fixed_count, macros=st.macro_count, nets=st.net_count,
-             pins=st.pin_count)
-        report["summary"] = stats.summary_text(st)
+        done("parse", t0, nodes=db.num_nodes, movable=db.num_movable, nets=db.num_nets, pins=db.num_pins)
     if db is None:
         raise ValueError("no design: give aux with the parse stage, or db")
     if "init" in stages:
         t0 = time.perf_counter()
-        if init_method == "quadratic":
-            qp_params = qp_params or qp.default_params(device=1 if engine.device_available() else 0)
-            rows = qp.QuadraticPlacer(qp_params).place(db)
-            done("init", t0, outer_iters=int(rows["iter"].shape[0]), device=int(qp_params.device))
-        else:
-            seed = (params or abi.default_params()).random_seed
-            done("init", t0, **initial.make_initial_placer(init_method, seed=seed).place(db))
+        qp_params = qp_params or qp.default_params(device=1 if engine.device_available() else 0)
+        rows = qp.QuadraticPlacer(qp_params).place(db)
+        done("init", t0, outer_iters=int(rows["iter"].shape[0]), device=int(qp_params.device))
         report["init_x"], report["init_y"] = db.node_x[: db.num_nodes].copy(), db.node_y[: db.num_nodes].copy()
-    movable_macros = int(np.sum((db.node_flags[: db.num_movable] & F_MACRO != 0) &
-                                (db.node_flags[: db.num_movable] & F_FIXED == 0)))
     if "gp" in stages:
         t0 = time.perf_counter()
-        p = params or abi.default_params()
-        engine.initialize_fillers(db, p.target_density, p.random_seed)
-        ep = engine.EPlace(db, p)
-        r = ep.run(abi.STAGE_MGP)
-        del ep
-        done("gp", t0, iterations=r.iterations, overflow=r.overflow, loop_ms=r.elapsed_ms)
-        if movable_macros:
-            report["stopped"] = f"{movable_macros} movable macros need mLG, which is not built; stopped after mGP"
+        res = global_place(db, params, legalize_macros)
+        last = res.get("cGP", res["mGP"])
+        done("gp", t0, iterations=sum(r.iterations for k, r in res.items() if k in ("mGP", "FILLERONLY", "cGP")),
+             overflow=last.overflow, loop_ms=sum(r.elapsed_ms for k, r in res.items() if k in ("mGP", "FILLERONLY", "cGP")))
+        if "stopped" in res:
+            report["stopped"] = res["stopped"]
             return db, report
-    if "lg" in stages:
+    if "lg" in stages and legalize_cells is not None:
         t0 = time.perf_counter()
-        res = legalize.legalize_cells(db)
-        done("lg", t0, **res)
+        done("lg", t0, **legalize_cells(db))
     if "write" in stages and out_pl:
         t0 = time.perf_counter()
         bookshelf.write_pl(out_pl, db)

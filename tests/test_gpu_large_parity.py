@@ -55,3 +55,22 @@ def test_final_hpwl_within_half_percent_of_cpu(instance, reference, precision):
     # iteration 0 sees the same instance at the same positions
     assert abs(m["hpwl"][0] - rows[0, 1]) <= 1e-9 * rows[0, 1]
     assert abs(m["overflow"][0] - rows[0, 2]) <= 1e-5
+
+
+def test_first_rows_match_reference_build_at_full_size(instance, reference):
+    """The first ten metrics rows at 211k cells against the reference's own run (the rows of
+    the full-stage run above), field by field, with the tolerances of the 2k-cell check."""
+    from oracle import ref
+
+    from .test_gpu_eplace import ROW_TOL
+
+    _, rr = reference
+    _, m = run_device(instance, abi.POISSON_FP32)
+    col = {f: i for i, f in enumerate(ref.ROW_FIELDS)}
+    for f, (t0, t1) in ROW_TOL.items():
+        got = m[f][:10].astype(np.float64)
+        want = rr[:10, col[f]]
+        rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-30)
+        assert rel[0] <= t0, (f, rel)
+        assert np.all(rel[1:] <= t1), (f, rel)
+    assert np.array_equal(m["evaluations"][:10], rr[:10, col["evaluations"]].astype(np.int64))

@@ -1,0 +1,93 @@
+"""The stagnation guard and its rollback point on the device (eplace.cpp:421-473), on the
+overfull design of tests/checks.py (the reference's fixture for these checks, rebuilt), with
+the reference's own assertions and a run of the reference build beside it.
+
+  * testStagnationGuard (test/test_eplace.cpp:288-323): with window 40 the stage stops early
+    without converging, tau stays near its floor, and against the unguarded run (window 0,
+    which runs all 500 iterations) tau is no worse than 5% and HPWL is below half;
+  * testStagnationRollbackPoint (:333-388): the delivered tau and HPWL are the rollback
+    row's (G3), the rollback row is within the tolerance line of the best tau and no worse in
+    HPWL than the best-tau row (G8), and no worse than any snapshot of the tau ladder
+    rebuilt from the rows by eplace.cpp's rule.
+The reference build runs the same design and window: both stagnate, at iteration counts and
+rollback points within 25% of each other, with final tau within 3% and HPWL within 10%.
+"""
+import numpy as np
+import pytest
+
+from superplace_b200 import abi, engine
+
+from .checks import overfull_design
+
+pytestmark = pytest.mark.gpu
+
+MAX_ITER = 500
+
+
+def params(window):
+    return abi.default_params(gp_max_iter=MAX_ITER, gp_stagnation_window=window)
+
+
+@pytest.fixture(scope="module")
+def runs():
+    out = {}
+    for w in (40, 0):
+        db = overfull_design()
+        engine.initialize_fillers(db, 1.0, 1002)  # negative whitespace: no fillers
+        ep = engine.EPlace(db, params(w))
+        r = ep.run(abi.STAGE_MGP)
+        out[w] = (db, r, ep.ctx.metrics())
+    return out
+
+
+def test_stagnation_guard(runs):
+    _, g, _ = runs[40]
+    _, u, _ = runs[0]
+    assert not g.converged and g.stagnated
+    assert g.overflow > 0.2
+    assert g.iterations < u.iterations
+    assert u.iterations == MAX_ITER and not u.stagnated
+    assert g.overflow <= u.overflow * 1.05
+    assert g.hpwl < u.hpwl * 0.5
+
+
+def test_rollback_point(runs):
+    _, r, rows = runs[40]
+    assert r.stagnated and len(rows["iter"]) == r.iterations
+    k = int(np.nonzero(rows["iter"] == r.rollback_iter)[0][0])
+    best = int(np.argmin(rows["overflow"]))
+    min_gain = np.float32(abi.default_params().gp_stagnation_min_gain)
+    tol = np.float32(rows["overflow"][best]) * (np.float32(1) + min_gain)
+    # G3: the delivered point is the one whose tau and HPWL the row recorded
+    assert np.float32(r.overflow) == np.float32(rows["overflow"][k])
+    assert r.hpwl == rows["hpwl"][k]
+    # G8
+    assert np.float32(rows["overflow"][k]) <= tol
+    assert rows["hpwl"][k] <= rows["hpwl"][best]
+    ladder = []
+    best_so_far = np.float32(np.inf)
+    for i in range(len(rows["iter"])):
+        t = np.float32(rows["overflow"][i])
+        best_so_far = min(best_so_far, t)
+        while ladder and np.float32(rows["overflow"][ladder[0]]) > best_so_far * (np.float32(1) + min_gain):
+            ladder.pop(0)
+        if not ladder or t * (np.float32(1) + np.float32(0.5) * min_gain) <= np.float32(rows["overflow"][ladder[-1]]):
+            ladder.append(i)
+    assert len(ladder) >= 2
+    assert rows["hpwl"][k] <= min(rows["hpwl"][i] for i in ladder)
+
+
+def test_stagnation_against_reference_build(runs):
+    from oracle import ref
+
+    if not ref.available():
+        pytest.skip("oracle/_ref/libspref.so not built")
+    db = overfull_design()
+    engine.initialize_fillers(db, 1.0, 1002)
+    res, _ = ref.RefDb(db).eplace(params(40))
+    _, r, _ = runs[40]
+    assert res["stagnated"] == 1 and res["converged"] == 0
+    assert abs(r.iterations - res["iterations"]) <= 0.25 * res["iterations"]
+    assert abs(r.rollback_iter - res["rollback_iter"]) <= 0.25 * res["rollback_iter"]
+    assert r.overflow == pytest.approx(res["overflow"], rel=0.03)
+    assert r.hpwl == pytest.approx(res["hpwl"], rel=0.10)

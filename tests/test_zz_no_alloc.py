@@ -24,7 +24,8 @@ def rel_err(ref, got):
     return np.abs(ref - got).max() / max(np.abs(ref).max(), 1e-300)
 
 
-@pytest.mark.parametrize("nx,ny,sx,sy", [(512, 512, 20.88, 20.86), (64, 128, 2.5, 1.7)])
+@pytest.mark.parametrize("nx,ny,sx,sy", [(512, 512, 20.88, 20.86), (64, 128, 2.5, 1.7), (128, 64, 1.7, 2.5),
+                                         (37, 50, 3.1, 2.2)])
 def test_static_solve_matches_plan_solve_twice(nx, ny, sx, sy):
     import torch
 
@@ -44,6 +45,26 @@ def test_static_solve_matches_plan_solve_twice(nx, ny, sx, sy):
             w, g = w.cpu().numpy(), g.cpu().numpy()
             assert np.all(np.isfinite(g)), f"call {call}: non-finite output"
             assert rel_err(w, g) < TOL, f"call {call}: {rel_err(w, g):.3e}"
+
+
+@pytest.mark.parametrize("nx,ny,sx,sy", [(64, 64, 2.5, 2.5), (128, 64, 1.7, 2.5), (37, 50, 3.1, 2.2)])
+def test_static_solve_matches_fp64_oracle(nx, ny, sx, sy):
+    """Directly against the FP64 oracle (oracle/oracle.py: the reference's transforms by
+    their definitions), within the same 1e-5 of max|ref|."""
+    import torch
+
+    from oracle import oracle as orc
+
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(nx * 7 + ny)
+    rho_h = rng.random((nx, ny), dtype=np.float32)
+    rho = torch.from_numpy(rho_h).to(dev)
+    got = [torch.full_like(rho, float("nan")) for _ in range(3)]
+    engine.poisson_solve_static(nx, ny, sx, sy, rho.data_ptr(), *(t.data_ptr() for t in got),
+                                stream=torch.cuda.current_stream(dev).cuda_stream)
+    torch.cuda.synchronize(dev)
+    for w, g in zip(orc.poisson_f64(rho_h, sx, sy), got):
+        assert rel_err(w, g.cpu().numpy()) < TOL
 
 
 def test_static_solve_rejects_sizes_beyond_its_maximum():
