@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define SPG_ABI_VERSION 2
+#define SPG_ABI_VERSION 3
 
 /* ---- status codes (map onto the reference's InvariantError kinds, src/util/invariant.h:10-19) */
 #define SPG_OK 0
@@ -117,6 +117,11 @@ typedef struct spg_params {
     uint64_t random_seed;          /* 1002 */
     int32_t poisson_precision;     /* SPG_POISSON_* */
     int32_t verbose;               /* log every iteration instead of every 20th */
+    /* appended in ABI version 3: the diagnostic run options GpRunOptions::freezeLambda and
+     * freezeGamma (src/gp/eplace.h:45-52; eplace.cpp:374-380): lambda keeps its initial
+     * value (mu = 1) and gamma its value from the lambda_0 probe. Off (0) in production. */
+    int32_t freeze_lambda;
+    int32_t freeze_gamma;
 } spg_params;
 
 /* Defaults identical to configs/default.json of the reference. */

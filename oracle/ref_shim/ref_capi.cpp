@@ -386,8 +386,11 @@ int spref_eplace_run(void* dbh, const spg_params* p, int stage, double* result, 
         sp::MetricsSink sink;
         sp::EPlace engine(db, cfg, sink);
         const sp::GpStage st = toStage(stage);
+        sp::GpRunOptions o;
+        o.freezeLambda = p->freeze_lambda != 0;
+        o.freezeGamma = p->freeze_gamma != 0;
         const double t0 = omp_get_wtime();
-        const sp::GpResult r = engine.run(st);
+        const sp::GpResult r = engine.run(st, o);
         putResult(r, (omp_get_wtime() - t0) * 1e3, result);
         const auto& m = sink.stageMetrics(sp::toString(st));
         int n = 0;

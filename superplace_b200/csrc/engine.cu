@@ -523,6 +523,8 @@ struct Context : ContextStreams {
         p.max_backtrack = prm.max_backtrack;
         p.min_gain = std::min(std::max(prm.gp_stagnation_min_gain, 0.f), 0.5f);
         p.stagnation_window = prm.gp_stagnation_window;
+        p.freeze_lambda = prm.freeze_lambda != 0;
+        p.freeze_gamma = prm.freeze_gamma != 0;
         p.step_x_gamma = step_x_gamma;
         return p;
     }
@@ -1916,6 +1918,8 @@ void spg_params_default(spg_params* p) {
     p->random_seed = 1002;
     p->poisson_precision = SPG_POISSON_FP32;
     p->verbose = 0;
+    p->freeze_lambda = 0;
+    p->freeze_gamma = 0;
 }
 
 // ------------------------------------------------------------------ Poisson

@@ -201,6 +201,7 @@ struct DevPtrs {
     float min_gain;
     int stagnation_window;
     float step_x_gamma;   // grid.stepX() used by computeGamma
+    int freeze_lambda, freeze_gamma;  // GpRunOptions diagnostics (eplace.cpp:374-380)
 };
 
 __device__ __forceinline__ float* role_ptr(const DevPtrs& p, int role) {

@@ -204,11 +204,12 @@ __device__ void decide_iteration(const DevPtrs& p, DevState* st) {
     }
     const float eval_lambda = st->lambda, eval_gamma = st->gamma;
     const double dh = st->have_prev ? st->hpwl - st->prev_hpwl : 0.0;
-    const float mu = st->have_prev ? lambda_multiplier(dh, st->hpwl_ref) : 1.f;
-    if (st->have_prev) st->lambda = fmul(st->lambda, mu);
+    const bool schedule = st->have_prev && !p.freeze_lambda;
+    const float mu = schedule ? lambda_multiplier(dh, st->hpwl_ref) : 1.f;
+    if (schedule) st->lambda = fmul(st->lambda, mu);
     st->prev_hpwl = st->hpwl;
     st->have_prev = 1;
-    st->gamma = compute_gamma(st->tau, p.step_x_gamma);
+    if (!p.freeze_gamma) st->gamma = compute_gamma(st->tau, p.step_x_gamma);
     if (!isfinite(st->lambda) || !isfinite(st->gamma)) {
         raise_error(st, SPG_E_NON_FINITE);
         st->done = 1;

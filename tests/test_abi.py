@@ -68,7 +68,7 @@ def test_params_defaults_match_reference_config():
 
 
 def test_abi_version():
-    assert engine.lib().spg_abi_version() == 2
+    assert engine.lib().spg_abi_version() == 3
 
 
 @pytest.mark.skipif(engine.device_available(), reason="checks the no-device refusal")

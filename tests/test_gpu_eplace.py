@@ -174,6 +174,7 @@ ROW_TOL = {  # field: (row-0 relative tolerance, rows 1..9 relative tolerance)
     "eval_lambda": (1e-4, 5e-3),
     "eval_gamma": (1e-5, 5e-3),
 }
+DEVICE_KEY = {"lambda": "lambda_"}  # the ctypes field name (lambda is a Python keyword)
 
 
 def compare_first_rows(db, params, k=10):
@@ -191,7 +192,7 @@ def compare_first_rows(db, params, k=10):
     col = {f: i for i, f in enumerate(ref.ROW_FIELDS)}
     worst = {}
     for f, (t0, t1) in ROW_TOL.items():
-        got = rows[f].astype(np.float64)
+        got = rows[DEVICE_KEY.get(f, f)].astype(np.float64)
         want = rr[:, col[f]]
         rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-30)
         worst[f] = (float(rel[0]), float(rel[1:].max()))

@@ -67,6 +67,8 @@ def compare(db, stage, precision, lam=None, gamma=None, tol_grad=1e-5):
         g1 = ref.gamma(1.0, ctx.grid_info()["step_x"])
         _, probe = rdb.obj_and_grad(params, stage, 1.0, g1, pos)
         lam = probe["sum_wl"] / probe["sum_den"] if probe["sum_den"] > 0 else 1.0
+        if not lam > 0:  # eplace.cpp:257 (FILLERONLY: no wirelength term)
+            lam = 1.0
         gamma = ref.gamma(probe["tau"], ctx.grid_info()["step_x"])
     got, gs = ctx.eval_grad(stage, lam, gamma, pos)
     want, ws = rdb.obj_and_grad(params, stage, lam, gamma, pos)

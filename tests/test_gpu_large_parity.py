@@ -62,13 +62,13 @@ def test_first_rows_match_reference_build_at_full_size(instance, reference):
     the full-stage run above), field by field, with the tolerances of the 2k-cell check."""
     from oracle import ref
 
-    from .test_gpu_eplace import ROW_TOL
+    from .test_gpu_eplace import DEVICE_KEY, ROW_TOL
 
     _, rr = reference
     _, m = run_device(instance, abi.POISSON_FP32)
     col = {f: i for i, f in enumerate(ref.ROW_FIELDS)}
     for f, (t0, t1) in ROW_TOL.items():
-        got = m[f][:10].astype(np.float64)
+        got = m[DEVICE_KEY.get(f, f)][:10].astype(np.float64)
         want = rr[:10, col[f]]
         rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-30)
         assert rel[0] <= t0, (f, rel)

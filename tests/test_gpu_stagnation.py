@@ -8,7 +8,10 @@ the reference's own assertions and a run of the reference build beside it.
   * testStagnationRollbackPoint (:333-388): the delivered tau and HPWL are the rollback
     row's (G3), the rollback row is within the tolerance line of the best tau and no worse in
     HPWL than the best-tau row (G8), and no worse than any snapshot of the tau ladder
-    rebuilt from the rows by eplace.cpp's rule.
+    rebuilt from the rows by eplace.cpp's rule. How many snapshots the ladder holds at the
+    end depends on the trajectory (the reference build itself ends with one on some seeds of
+    this fixture), so the checks run on three seeds and at least one must leave a choice of
+    two or more.
 The reference build runs the same design and window: both stagnate, at iteration counts and
 rollback points within 25% of each other, with final tau within 3% and HPWL within 10%.
 """
@@ -28,15 +31,22 @@ def params(window):
     return abi.default_params(gp_max_iter=MAX_ITER, gp_stagnation_window=window)
 
 
+SEEDS = (7, 8, 11)
+
+
+def run(seed, window):
+    db = overfull_design(seed)
+    engine.initialize_fillers(db, 1.0, 1002)  # negative whitespace: no fillers
+    ep = engine.EPlace(db, params(window))
+    r = ep.run(abi.STAGE_MGP)
+    return db, r, ep.ctx.metrics()
+
+
 @pytest.fixture(scope="module")
 def runs():
-    out = {}
-    for w in (40, 0):
-        db = overfull_design()
-        engine.initialize_fillers(db, 1.0, 1002)  # negative whitespace: no fillers
-        ep = engine.EPlace(db, params(w))
-        r = ep.run(abi.STAGE_MGP)
-        out[w] = (db, r, ep.ctx.metrics())
+    out = {w: run(SEEDS[0], w) for w in (40, 0)}
+    for seed in SEEDS[1:]:
+        out[(seed, 40)] = run(seed, 40)
     return out
 
 
@@ -51,8 +61,8 @@ def test_stagnation_guard(runs):
     assert g.hpwl < u.hpwl * 0.5
 
 
-def test_rollback_point(runs):
-    _, r, rows = runs[40]
+def rollback_checks(r, rows):
+    """G3 and G8 of testStagnationRollbackPoint; returns the tau ladder's final size."""
     assert r.stagnated and len(rows["iter"]) == r.iterations
     k = int(np.nonzero(rows["iter"] == r.rollback_iter)[0][0])
     best = int(np.argmin(rows["overflow"]))
@@ -73,8 +83,14 @@ def test_rollback_point(runs):
             ladder.pop(0)
         if not ladder or t * (np.float32(1) + np.float32(0.5) * min_gain) <= np.float32(rows["overflow"][ladder[-1]]):
             ladder.append(i)
-    assert len(ladder) >= 2
     assert rows["hpwl"][k] <= min(rows["hpwl"][i] for i in ladder)
+    return len(ladder)
+
+
+def test_rollback_point(runs):
+    sizes = [rollback_checks(*runs[40][1:])]
+    sizes += [rollback_checks(*runs[(seed, 40)][1:]) for seed in SEEDS[1:]]
+    assert max(sizes) >= 2, sizes
 
 
 def test_stagnation_against_reference_build(runs):
