@@ -13,7 +13,8 @@ src/gp/eplace.cpp:310,515).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision bf16x3|fp32] [--workload large|small]
-       python bench.py --poisson-sweep | --precision-study | --serve | --bookshelf | --qp | --flow
+       python bench.py --poisson-sweep | --precision-study | --mixed-study | --serve | --bookshelf | --qp
+                       | --flow
                                                                     (studies: JSON lines of their own)
 The default Poisson arithmetic is split-BF16 on tcgen05 (bf16x3); fp32 is the plain FP32 form.
 Multi-GPU: replicas only (each rank places its own copy; "scaling": "weak").
@@ -535,6 +536,73 @@ def run_precision_study(args):
     return 0
 
 
+def ref_macro_legaliser(params):
+    """The reference's own legalizeMacros (oracle/_ref; src/lg/macro_sa.cpp:493) as the mLG
+    callable of superplace_b200.flow.global_place: host code on the reference's side of the
+    boundary, run between the device stages as GlobalPlaceStage runs it (gp_stage.cpp:128-132)."""
+    from oracle import ref
+
+    def run(db):
+        r = ref.RefDb(db)
+        t = time.perf_counter()
+        res = r.legalize_macros(params)
+        res["ms"] = (time.perf_counter() - t) * 1e3
+        x, y, _, _, flags = r.nodes()
+        n = db.total_nodes
+        db.node_x[:n], db.node_y[:n], db.node_flags[:n] = x[:n], y[:n], flags[:n]
+        return res
+
+    return run
+
+
+def run_mixed_study(args):
+    """Config C3: the mixed-size four-stage GP (mGP -> mLG -> FILLERONLY -> cGP) on the 211k-cell
+    design with 63 movable macros (56.9% of movable area) and 200 fixed macros, 1024x1024 bins,
+    with the FP64, FP32 and split-BF16 Poisson forms on the device (mLG: the reference's own SA on
+    the host) and the reference's whole four-stage run on the CPU: per stage iterations, device
+    loop time, HPWL and tau, and the final HPWL of each form against FP64 and the CPU run."""
+    from oracle import ref
+    from superplace_b200 import flow
+
+    bins = 1024
+    db0 = generator.mixed_design(1002, n_cells=args.mixed_cells)
+    ref.lib().spref_set_threads(os.cpu_count() or 1)
+    out = {}
+    for name in args.mixed_forms:
+        prec = {"fp64": abi.POISSON_FP64, "fp32": abi.POISSON_FP32, "bf16x3": abi.POISSON_BF16X3}[name]
+        params = abi.default_params(gp_bin_dim=bins, poisson_precision=prec)
+        db = db0.copy()
+        t = time.perf_counter()
+        res = flow.global_place(db, params, legalize_macros=ref_macro_legaliser(params))
+        wall = (time.perf_counter() - t) * 1e3
+        o = {k: {"iterations": r.iterations, "hpwl": r.hpwl, "tau": r.overflow, "converged": r.converged,
+                 "loop_ms": r.elapsed_ms} for k, r in res.items() if k in ("mGP", "FILLERONLY", "cGP")}
+        o["mLG"] = res.get("mLG")
+        o["stopped"] = res.get("stopped")
+        o["wall_ms"] = wall
+        o["final_hpwl"] = res.get("cGP", res["mGP"]).hpwl
+        o["final_tau"] = res.get("cGP", res["mGP"]).overflow
+        out[name] = o
+        print(json.dumps({"study": "mixed-partial", "form": name, **o}), flush=True)
+    cpu = None
+    if args.mixed_cpu:
+        db = db0.copy()
+        ref_fillers(db, ref)
+        t = time.perf_counter()
+        res = ref.RefDb(db).gp_four_stage(abi.default_params(gp_bin_dim=bins))
+        cpu = {**res, "wall_ms": (time.perf_counter() - t) * 1e3, "final_hpwl": res["cGP"]["hpwl"],
+               "final_tau": res["cGP"]["overflow"]}
+    for name, v in out.items():
+        if "fp64" in out:
+            v["final_hpwl_vs_fp64"] = v["final_hpwl"] / out["fp64"]["final_hpwl"] - 1.0
+        if cpu:
+            v["final_hpwl_vs_cpu"] = v["final_hpwl"] / cpu["final_hpwl"] - 1.0
+    print(json.dumps({"study": "mixed", "workload": f"{db0.num_movable - 63} cells + 63 movable macros, "
+                      f"200 fixed macros, {db0.num_nets} nets, {bins}x{bins} bins", "device": out,
+                      "cpu_reference": cpu, "cpu_cores": os.cpu_count()}), flush=True)
+    return 0
+
+
 def run_serve(args):
     """The serving loop on arrival traces: requests from the small generator (cells log-uniform
     in 1k..100k, nets 1.05x cells, grid the next power of two in 64..512 at ~4 cells per bin),
@@ -681,10 +749,12 @@ def run_qp(args):
 
 def run_flow(args):
     """The whole pipeline on the 211k design written as BookShelf files: parse, QP init, mGP
-    (fillers and the device loop), Abacus and the .pl write, through superplace_b200.flow; and
-    the reference's own stages on the same files (oracle/_ref: its reader, initializeFillers,
-    EPlace mGP, legalizeCells, writePl; its QP needs Eigen, so it starts from our QP result).
-    Wall times per stage and HPWL after each; one JSON line."""
+    (fillers and the device loop) and the .pl write through superplace_b200.flow, with the lg
+    stage the reference's own legalizeCells on its side of the boundary (oracle/_ref, passed to
+    the flow as its cell legaliser); and the reference's own stages on the same files
+    (oracle/_ref: its reader, initializeFillers, EPlace mGP, legalizeCells, writePl; its QP needs
+    Eigen, so it starts from our QP result). Wall times per stage and HPWL after each; one JSON
+    line."""
     import tempfile
 
     from oracle import ref
@@ -695,7 +765,14 @@ def run_flow(args):
     # CUDA start-up outside the timed runs
     flow.place(db=make_design("small"), stages=("init", "gp"))
     params = abi.default_params(gp_bin_dim=WORKLOADS["large"]["bin_dim"], poisson_precision=abi.POISSON_BF16X3)
-    db, rep = flow.place(aux, out_pl=os.path.join(d, "ours.pl"), params=params)
+    def legalize_cells(pdb):
+        r = ref.RefDb(pdb)
+        res = ref.abacus(r)
+        x, y, _, _, _ = r.nodes()
+        pdb.node_x[: pdb.total_nodes], pdb.node_y[: pdb.total_nodes] = x, y
+        return res
+
+    db, rep = flow.place(aux, out_pl=os.path.join(d, "ours.pl"), params=params, legalize_cells=legalize_cells)
     ours = {s["stage"]: {k: (round(v, 3) if isinstance(v, float) else v) for k, v in s.items() if k != "stage"}
             for s in rep["stages"]}
     line = {"study": "flow", "design": "211k cells, 221k nets, 859k pins (synthetic), 512x512 bins",
@@ -762,6 +839,11 @@ def main():
                     help="B2B quadratic initial placement of the 211k design, host vs GPU solver: one JSON line")
     ap.add_argument("--flow", action="store_true",
                     help="parse, QP init, mGP, Abacus and .pl write on the 211k design, ours and the reference's: one JSON line")
+    ap.add_argument("--mixed-study", action="store_true",
+                    help="C3 four-stage mixed-size GP at 1024x1024 bins, FP64/FP32/BF16x3 and the CPU run: JSON lines")
+    ap.add_argument("--mixed-cells", type=int, default=211_000)
+    ap.add_argument("--mixed-forms", nargs="+", default=["fp64", "fp32", "bf16x3"])
+    ap.add_argument("--no-mixed-cpu", dest="mixed_cpu", action="store_false")
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
     ap.add_argument("--serve-seconds", type=float, default=8.0)
@@ -782,6 +864,8 @@ def main():
         return run_flow(args)
     if args.precision_study:
         return run_precision_study(args)
+    if args.mixed_study:
+        return run_mixed_study(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -222,11 +222,15 @@ def large_design(seed=1002, n_cells=211_000, n_nets=221_000) -> PlaceDB:
                         fixed_cover=0.35, name="large_211k")
 
 
-def mixed_design(seed=1002, n_cells=211_000, n_nets=221_000) -> PlaceDB:
-    """large_design + 63 movable macros (56.9% of movable area), 200 fixed macros."""
+def mixed_design(seed=1002, n_cells=211_000, n_nets=None) -> PlaceDB:
+    """large_design + 63 movable macros (56.9% of movable area), 200 fixed macros. Fewer cells
+    shrink the die with the square root of the count (same utilisation); nets default to
+    1.047 x cells (221k at 211k)."""
     rng = np.random.default_rng(seed + 17)
     w = np.clip(np.round(np.exp(rng.normal(np.log(6.0), 0.55, n_cells))), 1, 40)
-    return build_design(seed=seed, die=11600.0, row_h=12.0, n_cells=n_cells,
+    n_nets = int(round(n_cells * 221_000 / 211_000)) if n_nets is None else n_nets
+    die = 11600.0 if n_cells == 211_000 else float(np.ceil(11600.0 * np.sqrt(n_cells / 211_000) / 12.0) * 12.0)
+    return build_design(seed=seed, die=die, row_h=12.0, n_cells=n_cells,
                         cell_w=w.astype(np.float32), n_nets=n_nets, n_fixed_macros=200,
                         fixed_cover=0.12, n_movable_macros=63, movable_macro_frac=0.569,
                         name="mixed_211k")

@@ -1,0 +1,78 @@
+"""Config C3 at a reduced size (GPU only): the mixed-size stage sequence with split-BF16 Poisson
+against the reference build.
+
+The design is the C3 generator scaled to 20k cells (63 movable macros at 56.9% of movable area,
+200 fixed macros, the die shrunk to keep the utilisation) at 256x256 bins. The reference's macro
+legaliser (SA) takes about a minute on this instance, so the sequence here freezes the macros
+where mGP left them, as the reference's own cGP regression test does to stand in for mLG
+(test/test_eplace.cpp:445-483); bench.py --mixed-study runs the full four stages with the
+reference's SA at the full C3 size.
+
+  * mGP: the device (BF16x3) and the reference build from the same start converge, with final
+    HPWL within 0.5%;
+  * FILLERONLY and cGP from the same frozen state (fillers re-scattered with seed offset 1, as
+    gp_stage.cpp:168-186 does): cGP converges on both sides with final HPWL within 0.5%, and no
+    macro moves on the device.
+"""
+import numpy as np
+import pytest
+
+from superplace_b200 import abi, engine, generator
+from superplace_b200.placedb import F_FIXED, F_MACRO
+
+pytestmark = pytest.mark.gpu
+
+BINS = 256
+TOL = 0.005
+
+
+def params():
+    return abi.default_params(gp_bin_dim=BINS, poisson_precision=abi.POISSON_BF16X3)
+
+
+@pytest.fixture(scope="module")
+def design():
+    db = generator.mixed_design(1002, n_cells=20_000)
+    engine.initialize_fillers(db, 1.0, 1002)
+    return db
+
+
+@pytest.fixture(scope="module")
+def after_mgp(design):
+    from oracle import ref
+
+    if not ref.available():
+        pytest.skip("oracle/_ref/libspref.so not built")
+    dev = design.copy()
+    r = engine.EPlace(dev, params()).run(abi.STAGE_MGP)
+    res, _ = ref.RefDb(design).eplace(abi.default_params(gp_bin_dim=BINS))
+    return dev, r, res
+
+
+def test_mixed_mgp_within_half_percent(after_mgp):
+    _, r, res = after_mgp
+    assert r.converged and res["converged"]
+    assert r.overflow < 0.10
+    assert abs(r.hpwl - res["hpwl"]) <= TOL * res["hpwl"], (r.hpwl, res["hpwl"])
+
+
+def test_mixed_filler_only_and_cgp_within_half_percent(after_mgp):
+    from oracle import ref
+
+    dev, _, _ = after_mgp
+    db = dev.copy()
+    macros = np.nonzero((db.node_flags[: db.num_movable] & F_MACRO) != 0)[0]
+    assert macros.size == 63
+    db.node_flags[macros] |= F_FIXED
+    engine.scatter_fillers(db, 1002, seed_offset=1)
+    mx, my = db.node_x[macros].copy(), db.node_y[macros].copy()
+    rdb = ref.RefDb(db)
+    rfo, _ = rdb.eplace(abi.default_params(gp_bin_dim=BINS), stage=abi.STAGE_FILLER_ONLY)
+    rcg, _ = rdb.eplace(abi.default_params(gp_bin_dim=BINS), stage=abi.STAGE_CGP)
+    ep = engine.EPlace(db, params())
+    fo = ep.run(abi.STAGE_FILLER_ONLY)
+    cg = ep.run(abi.STAGE_CGP)
+    assert fo.iterations == rfo["iterations"] == abi.default_params().filler_only_iters
+    assert cg.converged and rcg["converged"] and cg.overflow < 0.10
+    assert abs(cg.hpwl - rcg["hpwl"]) <= TOL * rcg["hpwl"], (cg.hpwl, rcg["hpwl"])
+    assert np.array_equal(db.node_x[macros], mx) and np.array_equal(db.node_y[macros], my)
