@@ -562,7 +562,7 @@ def run_mixed_study(args):
     the host) and the reference's whole four-stage run on the CPU: per stage iterations, device
     loop time, HPWL and tau, and the final HPWL of each form against FP64 and the CPU run."""
     from oracle import ref
-    from superplace_b200 import flow
+    from superplace_b200 import engine, flow
 
     bins = 1024
     db0 = generator.mixed_design(1002, n_cells=args.mixed_cells)
@@ -572,8 +572,16 @@ def run_mixed_study(args):
         prec = {"fp64": abi.POISSON_FP64, "fp32": abi.POISSON_FP32, "bf16x3": abi.POISSON_BF16X3}[name]
         params = abi.default_params(gp_bin_dim=bins, poisson_precision=prec)
         db = db0.copy()
+        mlg = ref_macro_legaliser(params)
+        after_mlg = {}
+
+        def legalise(pdb):
+            out = mlg(pdb)
+            after_mlg["db"] = pdb.copy()
+            return out
+
         t = time.perf_counter()
-        res = flow.global_place(db, params, legalize_macros=ref_macro_legaliser(params))
+        res = flow.global_place(db, params, legalize_macros=legalise)
         wall = (time.perf_counter() - t) * 1e3
         o = {k: {"iterations": r.iterations, "hpwl": r.hpwl, "tau": r.overflow, "converged": r.converged,
                  "loop_ms": r.elapsed_ms} for k, r in res.items() if k in ("mGP", "FILLERONLY", "cGP")}
@@ -582,6 +590,18 @@ def run_mixed_study(args):
         o["wall_ms"] = wall
         o["final_hpwl"] = res.get("cGP", res["mGP"]).hpwl
         o["final_tau"] = res.get("cGP", res["mGP"]).overflow
+        if name == args.mixed_forms[-1] and "db" in after_mlg and args.mixed_cpu:
+            # FILLERONLY and cGP of the reference build from this form's own post-mLG state (the
+            # same macro layout): isolates the device stages from the SA's input differences
+            sdb = after_mlg["db"]
+            engine.scatter_fillers(sdb, params.random_seed, seed_offset=1)
+            rdb = ref.RefDb(sdb)
+            same = {}
+            for st, sname in ((abi.STAGE_FILLER_ONLY, "FILLERONLY"), (abi.STAGE_CGP, "cGP")):
+                r_, _ = rdb.eplace(abi.default_params(gp_bin_dim=bins), stage=st)
+                same[sname] = {k: r_[k] for k in ("iterations", "hpwl", "overflow", "converged", "stagnated")}
+            same["cgp_hpwl_device_vs_reference"] = o["cGP"]["hpwl"] / same["cGP"]["hpwl"] - 1.0
+            o["reference_from_same_mlg_state"] = same
         out[name] = o
         print(json.dumps({"study": "mixed-partial", "form": name, **o}), flush=True)
     cpu = None

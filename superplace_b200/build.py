@@ -19,7 +19,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 SOURCES = ["engine.cu", "density.cu", "wirelength.cu", "optimizer.cu", "poisson.cu",
-           "poisson_tc.cu", "poisson_static.cu", "bookshelf.cpp", "qp.cpp", "qp_device.cu"]
+           "poisson_tc.cu", "poisson_static.cu", "filler_order.cu", "bookshelf.cpp", "qp.cpp", "qp_device.cu"]
 # host sources parallelised with OpenMP
 OPENMP = {"qp.cpp"}
 

@@ -112,6 +112,10 @@ struct DevState {
     int max_iter;
     int role[NUM_ROLES];
     unsigned long long t0_ns;
+    // the loop stops (without finishing the stage) once iter reaches pause_iter, so the host
+    // can reorder the fillers between two passes (filler_order.cu); INT_MAX: never
+    int pause_iter;
+    int pause_pad;
 };
 
 // Nets of at most this degree get one thread each in WA pass 1 (SPG_WA_THREAD_DEGREE
@@ -250,6 +254,20 @@ void launch_rho_prep(const DevPtrs& p, uint16_t* planes, int64_t plane_stride, i
 void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s);
 // gather for every density node into a node-indexed 2*total array (parity hook)
 void launch_gather_all(const DevPtrs& p, float* force_nodes, cudaStream_t s);
+
+// ---- filler_order.cu
+// Device buffers of the fillers' spatial reorder: n_keys = filler_order_keys(dim) tile keys,
+// nf fillers, NUM_ROLES + SNAP_MAX pool vectors.
+struct FillerOrderBufs {
+    int *key_of, *tmp, *perm, *fid, *fid_tmp;  // nf each; fid = filler id of each filler slot
+    int *count, *offset, *cursor;               // n_keys each
+    int* skip;                                  // 1 when a tile exceeds the segment capacity
+    float* scratch;                             // 2 * nf * (NUM_ROLES + SNAP_MAX)
+    int* opt_idx;                               // the opt set's node ids (the fillers' are rewritten)
+};
+int filler_order_keys(int dim);
+// Reorders the filler segment of the opt set by tile of the current u (see filler_order.cu).
+void launch_filler_order(const DevPtrs& p, const FillerOrderBufs& b, cudaStream_t s);
 
 // ---- wirelength.cu
 void launch_wa_nets(const DevPtrs& p, const WaClasses& wa, const float* gamma_dev, float gamma_host, int use_dev_gamma,

@@ -22,6 +22,7 @@
 // fixed owner; the "last block" (an atomic ticket) reduces the partials in a fixed tree, so
 // every reduction is deterministic. The host never computes a schedule value.
 #include <cfloat>
+#include <climits>
 
 #include "engine.h"
 
@@ -573,7 +574,9 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
         apply_pending_step(&sst);
         finish_evaluation(p, &sst, sums, count_eval);
         decide(p, &sst, sums[5], sums[6], sums[7], sums[8]);
-        if (loop_cond) cudaGraphSetConditional(loop_cond, (sst.done || sst.error) ? 0u : 1u);
+        // continue while the stage is neither done nor failed nor at a pause (filler reorder)
+        if (loop_cond)
+            cudaGraphSetConditional(loop_cond, (sst.done || sst.error || sst.iter >= sst.pause_iter) ? 0u : 1u);
     }
     state_copy_out(p.st, &sst);
 }
@@ -590,7 +593,8 @@ __device__ __forceinline__ void nesterov_point(float u, float v, float g, float 
 }
 
 // The loop's position step with the density scatter of the new positions fused in. One
-// launch per loop pass; the pass applies whichever step the last decisions asked for:
+// launch per loop pass, one node per thread; the pass applies whichever step the last
+// decisions asked for:
 //
 //   a re-evaluation (st->redo; redoIfOvershot body, nesterov.cpp:158-163):
 //     v = uPrev - alpha gPrevTmp ; u = v + momentumPrev (v - vPrev) ; clamp v, u.
@@ -607,8 +611,8 @@ __device__ __forceinline__ void nesterov_point(float u, float v, float g, float 
 // no step applies (the stage is done) the current u is rasterized unchanged. Without PLACE
 // (a plain optimizer run over a test objective) only the optimizer vectors are written, with
 // the per-coordinate clamp bounds opt_lo / opt_hi.
-// 40 registers (6 blocks of 256 per SM, no spills): the kernel is latency-bound, one node
-// per thread, so occupancy is what hides its loads and atomics
+// 6 blocks of 256 per SM: the kernel is latency-bound, so occupancy is what hides its loads
+// and atomics. The grid covers the opt set (node_blocks), one node per thread.
 template <bool PLACE>
 __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
     pdl_wait();
@@ -626,16 +630,17 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
     float* snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
     const float alpha = st->alpha, m = redo ? st->momentum_prev : st->momentum;
     const int n = p.n_opt;
-    bool bad = false;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const bool fill = PLACE && k >= p.filler_k0;  // a filler: attributes are the shared constants
-        int4 meta{};
-        float4 geo{};
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool have = k < n;
+    const bool fill = PLACE && k >= p.filler_k0;  // a filler: attributes are the shared constants
+    int4 meta{};
+    float4 geo{};
+    float nu[2] = {0.f, 0.f};
+    if (have) {
         if (PLACE) {
             meta = fill ? p.filler_meta : p.opt_meta[k];
             geo = fill ? p.filler_geom : p.opt_geom[k];
         }
-        float nu[2];
         if (apply) {
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
@@ -647,11 +652,11 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
                 nesterov_point(uq, v[q], g[q], alpha, m, lo, hi, vn[q], nu[c]);
                 un[q] = nu[c];
             }
-            bad |= !isfinite(nu[0]) || !isfinite(nu[1]);
+            if (!isfinite(nu[0]) || !isfinite(nu[1])) raise_error(st, SPG_E_NON_FINITE);
             // the node arrays: read inside the loop only for cells (WA) and large nodes (their
             // gather); the fillers' entries are rewritten from R_POS when the stage ends
             if (PLACE && (!fill || (meta.w & K_LARGE))) {
-                const int i = fill ? p.filler_node0 + k : p.opt_idx[k];
+                const int i = p.opt_idx[k];
                 p.x[i] = nu[0];
                 p.y[i] = nu[1];
             }
@@ -663,9 +668,9 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
                 snap[n + k] = nu[1];
             }
         }
-        if (PLACE && !(meta.w & K_LARGE)) rasterize(p, nu[0], nu[1], geo.x, geo.y, geo.z, (meta.w & K_FILLER) != 0);
     }
-    if (bad) raise_error(st, SPG_E_NON_FINITE);
+    if (PLACE && have && !(meta.w & K_LARGE))
+        rasterize(p, nu[0], nu[1], geo.x, geo.y, geo.z, (meta.w & K_FILLER) != 0);
     // the rest of the step (apply_pending_step) runs in the next assembly's last block; every
     // block read the state above before this store can matter to anyone
     if (!redo && blockIdx.x == 0 && threadIdx.x == 0) st->step_pending = apply ? 2 : 1;

@@ -11,8 +11,10 @@ reference's SA at the full C3 size.
   * mGP: the device (BF16x3) and the reference build from the same start converge, with final
     HPWL within 0.5%;
   * FILLERONLY and cGP from the same frozen state (fillers re-scattered with seed offset 1, as
-    gp_stage.cpp:168-186 does): cGP converges on both sides with final HPWL within 0.5%, and no
-    macro moves on the device.
+    gp_stage.cpp:168-186 does). Frozen where mGP left them, the macros still overlap, so tau
+    has a floor near 0.25 and cGP ends by its stagnation guard on both sides (the reference
+    build's run stagnates too): the device and the reference agree on how the stage ends, the
+    delivered HPWL within 0.5% and tau within 2%, and no macro moves on the device.
 """
 import numpy as np
 import pytest
@@ -73,6 +75,7 @@ def test_mixed_filler_only_and_cgp_within_half_percent(after_mgp):
     fo = ep.run(abi.STAGE_FILLER_ONLY)
     cg = ep.run(abi.STAGE_CGP)
     assert fo.iterations == rfo["iterations"] == abi.default_params().filler_only_iters
-    assert cg.converged and rcg["converged"] and cg.overflow < 0.10
+    assert (cg.converged, cg.stagnated) == (rcg["converged"], rcg["stagnated"])
     assert abs(cg.hpwl - rcg["hpwl"]) <= TOL * rcg["hpwl"], (cg.hpwl, rcg["hpwl"])
+    assert cg.overflow == pytest.approx(rcg["overflow"], rel=0.02)
     assert np.array_equal(db.node_x[macros], mx) and np.array_equal(db.node_y[macros], my)
