@@ -122,6 +122,12 @@ typedef struct spg_params {
      * value (mu = 1) and gamma its value from the lambda_0 probe. Off (0) in production. */
     int32_t freeze_lambda;
     int32_t freeze_gamma;
+    /* 1: the context's one-grid split-BF16 solves run as one persistent launch (G1, the split
+     * of its output, G2, G3, G4 with grid barriers between them), with the same results as the
+     * separate launches. Its barriers need all of its CTAs resident at once, so it is only for
+     * a context that runs alone on its device. 0 (default): separate launches, which measured
+     * faster at 512x512. No counterpart in the reference. */
+    int32_t poisson_single_launch;
 } spg_params;
 
 /* Defaults identical to configs/default.json of the reference. */
@@ -203,6 +209,12 @@ int spg_poisson_solve_batch_device(spg_poisson* h, int batch, const float* d_rho
                                    float* d_phi, float* d_field_x, float* d_field_y,
                                    void* stream);
 const char* spg_poisson_name(const spg_poisson* h);
+/* 1: this handle's one-grid split-BF16 solves run as one persistent launch, with the same
+ * results as the separate launches (off by default). Its grid barriers need all of its CTAs
+ * resident at once: only for a handle whose solves do not overlap another such launch on the
+ * device (the reference allows independent handles to run concurrently). No counterpart in
+ * the reference. */
+int spg_poisson_set_single_launch(spg_poisson* h, int on);
 int spg_poisson_destroy(spg_poisson* h);
 
 /* Poisson solve that allocates nothing. No counterpart in the reference: it exists for

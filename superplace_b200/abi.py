@@ -65,7 +65,7 @@ class Params(C.Structure):
         ("use_bb", C.c_int32), ("gp_backtrack", C.c_int32), ("max_backtrack", C.c_int32),
         ("gp_stagnation_window", C.c_int32), ("gp_stagnation_min_gain", C.c_float),
         ("random_seed", C.c_uint64), ("poisson_precision", C.c_int32), ("verbose", C.c_int32),
-        ("freeze_lambda", C.c_int32), ("freeze_gamma", C.c_int32),
+        ("freeze_lambda", C.c_int32), ("freeze_gamma", C.c_int32), ("poisson_single_launch", C.c_int32),
     ]
 
 
@@ -105,7 +105,7 @@ def default_params(**overrides) -> Params:
         delta_hpwl_ref=3.5e5, lambda_schedule_relative=0, delta_hpwl_relative=0.01,
         use_bb=1, gp_backtrack=1, max_backtrack=10, gp_stagnation_window=200,
         gp_stagnation_min_gain=0.02, random_seed=1002, poisson_precision=POISSON_FP32,
-        verbose=0, freeze_lambda=0, freeze_gamma=0,
+        verbose=0, freeze_lambda=0, freeze_gamma=0, poisson_single_launch=0,
     )
     for k, v in overrides.items():
         if not hasattr(p, k):

@@ -815,6 +815,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         }
     }
     poisson_plan_set_steps(*c.plan, g.step_x, g.step_y);
+    c.plan->single_launch = c.prm.poisson_single_launch != 0;
     ht.mark("plan");
     c.partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_CAP);
     c.partials.zero(st);
@@ -1995,6 +1996,7 @@ void spg_params_default(spg_params* p) {
     p->verbose = 0;
     p->freeze_lambda = 0;
     p->freeze_gamma = 0;
+    p->poisson_single_launch = 0;
 }
 
 // ------------------------------------------------------------------ Poisson
@@ -2055,6 +2057,12 @@ int spg_poisson_solve_device(spg_poisson* h, const float* rho, float* phi, float
 }
 
 const char* spg_poisson_name(const spg_poisson* h) { return h ? h->h.plan.name.c_str() : "none"; }
+
+int spg_poisson_set_single_launch(spg_poisson* h, int on) {
+    if (!h) return spg::fail(Error(SPG_E_INVALID, "null argument"));
+    h->h.plan.single_launch = on != 0;
+    return SPG_OK;
+}
 
 int spg_poisson_destroy(spg_poisson* h) {
     delete h;

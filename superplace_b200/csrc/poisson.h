@@ -49,6 +49,10 @@ struct PoissonPlan {
     std::vector<double> sin_x, sin_y;  // host sine tables, for new bin steps (set_steps)
     size_t bytes = 0;    // device memory held
     cudaStream_t stream = nullptr;  // the stream its buffers' frees are ordered on
+    // a one-grid split-BF16 solve may run as one persistent launch (tc_fused_kernel). Its grid
+    // barriers need all its CTAs resident at once, so it is only for a plan whose solves do not
+    // run beside another such launch on the device; off unless the owner asks for it
+    bool single_launch = false;
 };
 
 // Allocates bases and work buffers for up to batch_cap grids. precision: SPG_POISSON_*.

@@ -30,6 +30,8 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdlib>
+#include <mutex>
 #include <cstring>
 #include <vector>
 
@@ -194,19 +196,69 @@ __device__ __forceinline__ float4 ld_dsmem4(uint32_t addr) {
     return v;
 }
 
-// Grid (S, N/BN, (M/128) * batch), cluster (S, 1, 1): the S CTAs of a cluster share one
-// 128 x BN output tile and split its K/64 K slabs evenly (split-K). A ring stage holds one K
-// slab of all four operand planes (A hi, A lo, B hi, B lo), from which the MMA thread issues
-// the three products, so every plane crosses L2 once per slab. Each CTA accumulates its slice
-// in TMEM and stages it in shared memory; then CTA r reduces rows [r*128/S, (r+1)*128/S)
-// over the cluster's S partials through distributed shared memory, in rank order
-// (deterministic), with all of its remote loads in flight at once, and runs the epilogue for
-// those rows with consecutive threads on consecutive columns (coalesced stores).
+// Per-CTA pipeline state, carried across the tiles one CTA computes: a standalone GEMM launch
+// computes one tile per CTA, the fused solve several (tc_fused_kernel).
+struct TileState {
+    uint8_t* base;             // the 1024-aligned stage ring
+    uint32_t full0, empty0, accb;
+    uint32_t tmem;
+    uint32_t it;               // ring slabs this CTA has streamed so far
+    uint32_t acc_n;            // accumulator phases completed
+};
+
+template <int BN, int STAGES>
+__device__ __forceinline__ void tile_setup(uint8_t* smem_raw, TileState& t) {
+    constexpr uint32_t STAGE_BYTES = 2 * TC_BM * TC_BK * 2 + 2 * BN * TC_BK * 2;
+    t.base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(t.base + STAGES * STAGE_BYTES);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
+    t.full0 = smem_u32(bars);
+    t.empty0 = smem_u32(bars + STAGES);
+    t.accb = smem_u32(bars + 2 * STAGES);
+    t.it = 0;
+    t.acc_n = 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < STAGES; ++i) {
+            mbar_init(t.full0 + 8 * i, 1);
+            mbar_init(t.empty0 + 8 * i, 1);
+        }
+        mbar_init(t.accb, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if ((threadIdx.x >> 5) == 0) {  // TMEM accumulator: BN fp32 columns x 128 lanes
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(static_cast<uint32_t>(BN)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    t.tmem = *tmem_slot;
+}
+
+template <int BN>
+__device__ __forceinline__ void tile_teardown(const TileState& t) {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(t.tmem), "r"(static_cast<uint32_t>(BN)));
+}
+
+// One 128 x BN output tile (rows m0.., columns n0.., grid z) of the contraction g, of which
+// this CTA computes K slabs [rank*nk/S, (rank+1)*nk/S): the tile's S CTAs are cluster ranks
+// group0 .. group0+S-1. A ring stage holds one K slab of all four operand planes (A hi, A lo,
+// B hi, B lo), from which the MMA thread issues the three products, so every plane crosses L2
+// once per slab. Each CTA accumulates its slice in TMEM and stages it in shared memory (over
+// the ring, which is idle by then); then CTA r reduces rows [r*128/S, (r+1)*128/S) over the S
+// partials through distributed shared memory, in rank order (deterministic), with all of its
+// remote loads in flight at once, and runs the epilogue for those rows with consecutive
+// threads on consecutive columns (coalesced stores). All threads of the CTA call it. With
+// active = false (a CTA without a tile in this round) or after an earlier failure (*g.err set)
+// the CTA streams and writes nothing but still takes the tile's cluster barriers.
 template <int BN, int STAGES, int S>
-__global__ void __launch_bounds__(TC_THREADS, 1)
-    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                   const TcArgs g) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
+__device__ __forceinline__ void gemm_tile(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& g, int m0,
+                                          int n0, int z, int rank, int group0, bool active, TileState& t) {
     constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;  // one plane
     constexpr uint32_t B_BYTES = BN * TC_BK * 2;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
@@ -215,82 +267,56 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     constexpr int GPT = R * (BN / 4) / TC_THREADS;  // float4 groups per thread
     static_assert(GPT >= 1 && R * (BN / 4) % TC_THREADS == 0, "reduction must split evenly");
     static_assert(TC_BM * RED_LD * 4 <= STAGES * STAGE_BYTES, "partial tile must fit the ring");
-    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + STAGES * STAGE_BYTES);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 1);
-    float* red = reinterpret_cast<float*>(base);  // reuses the ring after the main loop
-
+    float* red = reinterpret_cast<float*>(t.base);  // reuses the ring after the main loop
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rank = blockIdx.x;
-    const int tiles_m = g.M / TC_BM;
-    const int n0 = blockIdx.y * BN, m0 = (blockIdx.z % tiles_m) * TC_BM, z = blockIdx.z / tiles_m;
-    const uint32_t full0 = smem_u32(bars), empty0 = smem_u32(bars + STAGES), accb = smem_u32(bars + 2 * STAGES);
-
-    if (threadIdx.x == 0) {
-        for (int i = 0; i < STAGES; ++i) {
-            mbar_init(full0 + 8 * i, 1);
-            mbar_init(empty0 + 8 * i, 1);
-        }
-        mbar_init(accb, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    }
-    if (warp == 0) {  // TMEM accumulator: BN fp32 columns x 128 lanes
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(static_cast<uint32_t>(BN)));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __shared__ int run_s;
+    if (threadIdx.x == 0) run_s = active && __ldcg(g.err) == 0;
     __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    // everything above touched only this CTA's shared memory and TMEM: wait for the kernel
-    // that produced the operands only now
-    pdl_wait();
-    pdl_trigger();
+    const bool run = run_s != 0;
 
     const int nk = g.K / TC_BK;
     const int s0 = rank * nk / S, s1 = (rank + 1) * nk / S;
-    if (warp == 0 && lane == 0) {
+    if (run && warp == 0 && lane == 0) {
         // producer: one stage = K slab kk of A hi, A lo, B hi, B lo
         for (int s = s0; s < s1; ++s) {
-            const int i = s - s0, st = i % STAGES;
+            const uint32_t i = t.it + static_cast<uint32_t>(s - s0), st = i % STAGES;
             const uint32_t ph = (i / STAGES) & 1;
-            if (!mbar_wait(empty0 + 8 * st, ph ^ 1)) break;
+            if (!mbar_wait(t.empty0 + 8 * st, ph ^ 1)) break;
             const int kk = s * TC_BK;
-            const uint32_t sa = smem_u32(base + st * STAGE_BYTES);
+            const uint32_t sa = smem_u32(t.base + st * STAGE_BYTES);
             const bool alt = g.m_alt > 0 && m0 >= g.m_alt;
             const int arow = alt ? g.a_alt_row0 + (m0 - g.m_alt) : g.a_row0 + m0;
             const int brow = (alt ? g.b_alt_row0 : g.b_row0) + n0, bcol = kk + z * g.b_col_z;
-            mbar_expect_tx(full0 + 8 * st, STAGE_BYTES);
-            tma_load_2d(sa, &tmA, kk, arow, full0 + 8 * st);
-            tma_load_2d(sa + A_BYTES, &tmA, kk, arow + g.a_lo, full0 + 8 * st);
-            tma_load_2d(sa + 2 * A_BYTES, &tmB, bcol, brow, full0 + 8 * st);
-            tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tmB, bcol, brow + g.b_lo, full0 + 8 * st);
+            mbar_expect_tx(t.full0 + 8 * st, STAGE_BYTES);
+            tma_load_2d(sa, &tmA, kk, arow, t.full0 + 8 * st);
+            tma_load_2d(sa + A_BYTES, &tmA, kk, arow + g.a_lo, t.full0 + 8 * st);
+            tma_load_2d(sa + 2 * A_BYTES, &tmB, bcol, brow, t.full0 + 8 * st);
+            tma_load_2d(sa + 2 * A_BYTES + B_BYTES, &tmB, bcol, brow + g.b_lo, t.full0 + 8 * st);
         }
-    } else if (warp == 1 && lane == 0) {
+    } else if (run && warp == 1 && lane == 0) {
         constexpr uint32_t idesc = idesc_bf16(TC_BM, BN);
         bool ok = true;
         for (int s = s0; s < s1; ++s) {
-            const int i = s - s0, st = i % STAGES;
+            const uint32_t i = t.it + static_cast<uint32_t>(s - s0), st = i % STAGES;
             const uint32_t ph = (i / STAGES) & 1;
-            if (!mbar_wait(full0 + 8 * st, ph)) {
+            if (!mbar_wait(t.full0 + 8 * st, ph)) {
                 ok = false;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t ahi = smem_u32(base + st * STAGE_BYTES), alo = ahi + A_BYTES;
+            const uint32_t ahi = smem_u32(t.base + st * STAGE_BYTES), alo = ahi + A_BYTES;
             const uint32_t bhi = ahi + 2 * A_BYTES, blo = bhi + B_BYTES;
+            const bool first = s == s0;
 #pragma unroll
             for (int k = 0; k < TC_BK / 16; ++k) {  // 16 bf16 = 32 bytes per MMA along K
                 const uint32_t o = 32 * k;
-                umma_bf16(tmem, sw128_desc(ahi + o), sw128_desc(bhi + o), idesc, (i > 0 || k > 0) ? 1u : 0u);
-                umma_bf16(tmem, sw128_desc(ahi + o), sw128_desc(blo + o), idesc, 1u);
-                umma_bf16(tmem, sw128_desc(alo + o), sw128_desc(bhi + o), idesc, 1u);
+                umma_bf16(t.tmem, sw128_desc(ahi + o), sw128_desc(bhi + o), idesc, (!first || k > 0) ? 1u : 0u);
+                umma_bf16(t.tmem, sw128_desc(ahi + o), sw128_desc(blo + o), idesc, 1u);
+                umma_bf16(t.tmem, sw128_desc(alo + o), sw128_desc(bhi + o), idesc, 1u);
             }
-            umma_commit(empty0 + 8 * st);
+            umma_commit(t.empty0 + 8 * st);
         }
-        if (ok) umma_commit(accb);
+        if (ok) umma_commit(t.accb);
     }
     __syncwarp();
 
@@ -304,32 +330,35 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         grow[j] = rank * R + e / (BN / 4);
         gcol[j] = (e % (BN / 4)) * 4;
         const int m = m0 + grow[j], n = n0 + gcol[j];
-        sc[j] = g.scale ? __ldg(reinterpret_cast<const float4*>(g.scale + m * g.lds + n)) : make_float4(1.f, 1.f, 1.f, 1.f);
-        if (m == 0 && g.row0) {
+        sc[j] = make_float4(1.f, 1.f, 1.f, 1.f);
+        if (run && g.scale) sc[j] = __ldg(reinterpret_cast<const float4*>(g.scale + m * g.lds + n));
+        if (run && m == 0 && g.row0) {
             const float4 r0 = __ldg(reinterpret_cast<const float4*>(g.row0 + z * g.row0_z + n));
             sc[j] = make_float4(r0.x * sc[j].x, r0.y * sc[j].y, r0.z * sc[j].z, r0.w * sc[j].w);
         }
     }
 
     // stage this CTA's partial tile (TMEM lane = tile row; warp w owns rows 32w..32w+31)
-    const bool acc_ok = __all_sync(0xffffffffu, mbar_wait(accb, 0) ? 1 : 0) != 0;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (acc_ok) {
-        const int r = 32 * warp + lane;
+    bool acc_ok = false;
+    if (run) {
+        acc_ok = __all_sync(0xffffffffu, mbar_wait(t.accb, t.acc_n & 1) ? 1 : 0) != 0;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (acc_ok) {
+            const int r = 32 * warp + lane;
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 32) {
-            float v[32];
-            tmem_ld32(tmem + (static_cast<uint32_t>(32 * warp) << 16) + c, v);
+            for (int c = 0; c < BN; c += 32) {
+                float v[32];
+                tmem_ld32(t.tmem + (static_cast<uint32_t>(32 * warp) << 16) + c, v);
 #pragma unroll
-            for (int i = 0; i < 32; i += 4)
-                *reinterpret_cast<float4*>(red + r * RED_LD + c + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+                for (int i = 0; i < 32; i += 4)
+                    *reinterpret_cast<float4*>(red + r * RED_LD + c + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+            }
+        } else if (threadIdx.x == 0) {
+            atomicCAS(g.err, 0, SPG_E_CUDA);
         }
-    } else if (threadIdx.x == 0) {
-        atomicCAS(g.err, 0, SPG_E_CUDA);
     }
     const int ok_cta = __syncthreads_and(acc_ok ? 1 : 0);
-    cluster_sync_all();  // every CTA of the cluster has staged its partial
-
+    if (S > 1) cluster_sync_all();  // every CTA of the cluster has staged its partial
     if (ok_cta) {
         const uint32_t red_addr = smem_u32(red);
         float4 parts[GPT][S];
@@ -337,7 +366,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int j = 0; j < GPT; ++j) {
             const uint32_t off = 4u * static_cast<uint32_t>(grow[j] * RED_LD + gcol[j]);
 #pragma unroll
-            for (int q = 0; q < S; ++q) parts[j][q] = ld_dsmem4(map_rank(red_addr, static_cast<uint32_t>(q)) + off);
+            for (int q = 0; q < S; ++q)
+                parts[j][q] = S > 1 ? ld_dsmem4(map_rank(red_addr, static_cast<uint32_t>(group0 + q)) + off)
+                                    : *reinterpret_cast<const float4*>(red + grow[j] * RED_LD + gcol[j]);
         }
 #pragma unroll
         for (int j = 0; j < GPT; ++j) {
@@ -376,11 +407,184 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
         }
     }
-    cluster_sync_all();  // no CTA leaves while another may still read its shared memory
+    if (S > 1) cluster_sync_all();  // no CTA reuses its ring while another may still read it
+    if (run) {
+        t.it += static_cast<uint32_t>(s1 - s0);
+        t.acc_n += 1;
+    }
+    // the TMEM reads above are done before the next tile's MMAs overwrite the accumulator
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(static_cast<uint32_t>(BN)));
+}
+
+// Grid (S, N/BN, (M/128) * batch), cluster (S, 1, 1): the S CTAs of a cluster share one
+// 128 x BN output tile and split its K/64 K slabs evenly (split-K), one tile per CTA.
+template <int BN, int STAGES, int S>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const TcArgs g) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    TileState t;
+    tile_setup<BN, STAGES>(smem_raw, t);
+    // everything above touched only this CTA's shared memory and TMEM: wait for the kernel
+    // that produced the operands only now
+    pdl_wait();
+    pdl_trigger();
+    const int tiles_m = g.M / TC_BM;
+    gemm_tile<BN, STAGES, S>(tmA, tmB, g, (blockIdx.z % tiles_m) * TC_BM, blockIdx.y * BN, blockIdx.z / tiles_m,
+                             blockIdx.x, 0, true, t);
+    tile_teardown<BN>(t);
+}
+
+// ------------------------------------------------------------------ the fused one-grid solve
+// tc_fused_kernel runs a one-grid solve's chain in one launch: G1, the split of G1's output
+// (its rows minus their means into BF16 planes, with the exact row sums), G2, G3 and G4, with a
+// grid-wide barrier between phases. Every phase computes what the separate launches compute,
+// with the same tiles, the same split-K factors and the same reduction orders, so the results
+// are the same bits; what goes away is four launches and their drains. The grid is kFusedClusters
+// clusters of kFusedCluster CTAs, one CTA per SM, all resident at once (the host checks the
+// cluster occupancy first); a phase's tiles go round-robin over the clusters, S CTAs per tile.
+// The barrier is a counter in global memory: each CTA arrives once per phase and waits until all
+// have, at most kWaitNs, then records SPG_E_CUDA and goes on without waiting (later phases skip
+// their work once the flag is set). The last CTA to finish zeroes the counter for the next launch. Writes made by one phase reach the next phase's TMA loads
+// through release / acquire at GPU scope and async-proxy fences on both sides.
+constexpr int kFusedCluster = 4;
+constexpr int kFusedClusters = 32;
+constexpr int kPrepThreads = 256;  // prep_split_kernel's block (its reduction order is the split's)
+
+struct FusedMaps {
+    CUtensorMap a[4], b[4];  // G1..G4: A (bases) and B (data planes)
+};
+
+struct FusedArgs {
+    TcArgs g[4];
+    int split[4];               // split-K factor of each contraction (pick_splits)
+    const float* t0t32;         // G1's FP32 output, rows of `len` at stride ld
+    int rows, len;
+    int64_t ld;
+    uint16_t* t0t_s;            // its split planes (lo plane at + plane_stride), row r at r * ld
+    int64_t plane_stride;
+    float* sum_t;               // exact row sums
+    unsigned int* bar;          // [0] arrivals, [1] exits: zero at launch, zeroed again by the last CTA
+    int* err;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// All CTAs of the grid: arrive on *bar and wait until `target` arrivals (bounded).
+__device__ void grid_sync(unsigned int* bar, unsigned int target, int* err) {
+    asm volatile("fence.proxy.async.global;" ::: "memory");  // this thread's stores, for the async proxy
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(bar, 1u);
+        const unsigned long long t0 = gtime();
+        while (ld_acquire_u32(bar) < target) {
+            if (__ldcg(err) != 0) break;
+            if (gtime() - t0 > kWaitNs) {
+                atomicCAS(err, 0, SPG_E_CUDA);
+                break;
+            }
+        }
+        __threadfence();
+        asm volatile("fence.proxy.async.global;" ::: "memory");  // before this thread's next TMA loads
+    }
+    __syncthreads();
+}
+
+// The split of G1's output, one warp per row, with exactly the arithmetic of prep_split_kernel
+// (center = 1, one segment per row): its 256 threads' partial sums (elements t, t+256, ... in
+// order), the warp trees of lane 0, and the eight warp sums in order.
+__device__ void fused_split(const FusedArgs& a) {
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (TC_THREADS / 32) + (threadIdx.x >> 5), nw = gridDim.x * (TC_THREADS / 32);
+    for (int r = gw; r < a.rows; r += nw) {
+        const float* p = a.t0t32 + r * a.ld;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < kPrepThreads / 32; ++w) {
+            const int t = 32 * w + lane;  // the prep kernel's thread t
+            double v = 0.0;
+            for (int i = t; i < a.len; i += kPrepThreads) v += static_cast<double>(p[i]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            s += __shfl_sync(0xffffffffu, v, 0);
+        }
+        const float mean = static_cast<float>(s / a.len);
+        if (lane == 0) a.sum_t[r] = static_cast<float>(s);
+        uint16_t* hi = a.t0t_s + r * a.ld;
+        uint16_t* lo = hi + a.plane_stride;
+        for (int i = lane; i < a.len; i += 32) {
+            uint16_t h, l;
+            split_bf16(p[i] - mean, h, l);
+            hi[i] = h;
+            lo[i] = l;
+        }
+    }
+}
+
+// One contraction of the fused solve: its tiles round-robin over the clusters, 4/S tiles per
+// cluster and round; every CTA of a cluster takes the same number of rounds.
+template <int BN, int STAGES, int S>
+__device__ void fused_gemm(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& g, TileState& t) {
+    const int tiles_m = g.M / TC_BM, tiles = tiles_m * (g.N / BN);
+    const int crank = static_cast<int>(blockIdx.x % kFusedCluster), cid = static_cast<int>(blockIdx.x / kFusedCluster);
+    const int per = kFusedCluster / S, ncl = static_cast<int>(gridDim.x) / kFusedCluster;
+    const int group = crank / S, rank = crank % S;
+    const int rounds = (tiles + ncl * per - 1) / (ncl * per);
+    for (int rd = 0; rd < rounds; ++rd) {
+        const int tile = (rd * ncl + cid) * per + group;
+        const bool active = tile < tiles;
+        const int tt = active ? tile : 0;
+        gemm_tile<BN, STAGES, S>(tmA, tmB, g, (tt % tiles_m) * TC_BM, (tt / tiles_m) * BN, 0, rank, group * S, active,
+                                 t);
+    }
+}
+
+template <int BN, int STAGES, int S>
+__device__ __forceinline__ void fused_phase(const FusedMaps& mp, const FusedArgs& a, int k, TileState& t) {
+    fused_gemm<BN, STAGES, S>(mp.a[k], mp.b[k], a.g[k], t);
+}
+
+template <int BN, int STAGES>
+__device__ void fused_phase_any(const FusedMaps& mp, const FusedArgs& a, int k, TileState& t) {
+    switch (a.split[k]) {  // uniform over the grid
+        case 4: fused_phase<BN, STAGES, 4>(mp, a, k, t); break;
+        case 2: fused_phase<BN, STAGES, 2>(mp, a, k, t); break;
+        default: fused_phase<BN, STAGES, 1>(mp, a, k, t); break;
+    }
+}
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    tc_fused_kernel(const __grid_constant__ FusedMaps mp, const __grid_constant__ FusedArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    TileState t;
+    tile_setup<BN, STAGES>(smem_raw, t);
+    pdl_wait();
+    pdl_trigger();
+    const unsigned int n = gridDim.x;
+    fused_phase_any<BN, STAGES>(mp, a, 0, t);  // G1
+    grid_sync(a.bar, n, a.err);
+    if (__ldcg(a.err) == 0) fused_split(a);
+    grid_sync(a.bar, 2 * n, a.err);
+    fused_phase_any<BN, STAGES>(mp, a, 1, t);  // G2
+    grid_sync(a.bar, 3 * n, a.err);
+    fused_phase_any<BN, STAGES>(mp, a, 2, t);  // G3
+    grid_sync(a.bar, 4 * n, a.err);
+    fused_phase_any<BN, STAGES>(mp, a, 3, t);  // G4
+    // the last CTA out (every CTA has left its last barrier by then) zeroes the counters for
+    // the next launch
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(a.bar + 1, 1u) == n - 1) {
+        atomicExch(a.bar, 0u);
+        atomicExch(a.bar + 1, 0u);
+    }
+    tile_teardown<BN>(t);
 }
 
 // Row means (FP64) of `seg`-long row segments; writes the split BF16 planes of
@@ -388,7 +592,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // One block per (row, segment); outputs planes[row][col] with lo plane at + plane_stride.
 // The segment sum is a fixed-order block reduction (each thread's elements in order, warp
 // trees, then the warp sums in order).
-constexpr int kPrepThreads = 256;
 __global__ void __launch_bounds__(kPrepThreads) prep_split_kernel(const float* src, int rows, int nseg, int64_t ld,
                                                                   int seg, int center, uint16_t* planes,
                                                                   int64_t plane_stride, float* sums) {
@@ -468,6 +671,7 @@ struct TcState {
     float* t0t32 = nullptr;                 // FP32 T0t (G1 output, before its DC split)
     float* sums = nullptr;                  // DC row sums (rho rows, T0t rows per grid)
     int* err = nullptr;
+    unsigned int* bar = nullptr;            // the fused solve's grid barrier counter
 };
 
 // Split-K factor: the largest S in {8, 4, 2} (S divides the 128 tile rows, which the
@@ -507,6 +711,58 @@ void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int 
         case 2: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 2>, a, b, g)); break;
         default: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 1>, a, b, g)); break;
     }
+    count_launch();
+}
+
+// Whether kFusedClusters clusters of the fused kernel fit on the device at once (checked once
+// per device); SPG_POISSON_FUSED=0 turns the fused solve off.
+bool fused_resident() {
+    const char* off = std::getenv("SPG_POISSON_FUSED");
+    if (off && off[0] == '0') return false;
+    static std::mutex mu;
+    static std::vector<std::pair<int, bool>> seen;
+    int dev = 0;
+    SPG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto& e : seen)
+        if (e.first == dev) return e.second;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kFusedCluster * kFusedClusters);
+    cfg.blockDim = dim3(TC_THREADS);
+    cfg.dynamicSmemBytes = tc_smem_bytes();
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kFusedCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    const bool ok = cudaOccupancyMaxActiveClusters(&clusters, tc_fused_kernel<TC_BN, TC_STAGES>, &cfg) == cudaSuccess &&
+                    clusters >= kFusedClusters;
+    cudaGetLastError();
+    seen.emplace_back(dev, ok);
+    return ok;
+}
+
+void launch_fused(const FusedMaps& mp, const FusedArgs& a, cudaStream_t s) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kFusedCluster * kFusedClusters);
+    cfg.blockDim = dim3(TC_THREADS);
+    cfg.dynamicSmemBytes = tc_smem_bytes();
+    cfg.stream = s;
+    cudaLaunchAttribute attr[3];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = kFusedCluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[1].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    attr[2].id = cudaLaunchAttributePriority;
+    attr[2].val.priority = launch_priority(true);
+    cfg.attrs = attr;
+    cfg.numAttrs = 3;
+    SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_fused_kernel<TC_BN, TC_STAGES>, mp, a));
     count_launch();
 }
 
@@ -562,6 +818,8 @@ void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::ve
     st->sums = static_cast<float*>(dev_alloc(2 * B * std::max(X, Y) * 4, &pl.stream));
     st->err = static_cast<int*>(dev_alloc(4, &pl.stream));
     SPG_CUDA(cudaMemsetAsync(st->err, 0, 4, pl.stream));
+    st->bar = static_cast<unsigned int*>(dev_alloc(16, &pl.stream));
+    SPG_CUDA(cudaMemsetAsync(st->bar, 0, 16, pl.stream));
     pl.bytes += B * X * Y * 4 + 2 * B * std::max(X, Y) * 4 + 4;
     st->cy = make_map(pl.cy_s, 2 * Y, Y, TC_BM);
     st->cx = make_map(pl.cx_s, 2 * X, X, TC_BM);
@@ -577,6 +835,7 @@ void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::ve
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    SPG_CUDA(cudaFuncSetAttribute(tc_fused_kernel<TC_BN, TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 }
 
 void tc_plan_refill_sines(PoissonPlan& pl, const std::vector<float>& sy_rows, const std::vector<float>& sx_rows) {
@@ -600,6 +859,7 @@ void tc_plan_destroy(PoissonPlan& pl) {
         dev_free(st->t0t32, pl.stream);
         dev_free(st->sums, pl.stream);
         dev_free(st->err, pl.stream);
+        dev_free(st->bar, pl.stream);
         delete st;
         pl.tc = nullptr;
     }
@@ -636,23 +896,19 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
     g1.a_row0 = 0; g1.a_lo = Y; g1.b_row0 = 0; g1.b_lo = static_cast<int>(BXc); g1.b_col_z = 0;
     g1.mode = TC_F32; g1.out = st->t0t32; g1.out2 = st->t0t32; g1.split = Y; g1.ldc = BXc; g1.out_z = 0;
     g1.row0 = sum_r; g1.row0_z = 0; g1.err = st->err;
-    launch_tc(st->cy, st->rho_b, g1, 1, (X / TC_BN) * (Y / TC_BM), s);
     // T0t rows minus their per-grid means -> split planes (B operand of G2), segment sums
-    prep_split(st->t0t32, Y, static_cast<int>(BX), BXc, X, 1, pl.t0t_s, static_cast<int64_t>(Y) * BXc, sum_t, s);
     // G2: P_z (X x Y) = Cx . T0t'[:, z]^T, times the spectral scale, DC row from the sums
     TcArgs g2{};
     g2.M = X; g2.N = Y; g2.K = X;
     g2.a_row0 = 0; g2.a_lo = X; g2.b_row0 = 0; g2.b_lo = Y; g2.b_col_z = X;
     g2.mode = TC_SPLIT; g2.planes = pl.p_s; g2.plane_stride = BXc * Y; g2.plane_z = XY; g2.ldc = Y;
     g2.scale = pl.scale; g2.lds = Y; g2.row0 = sum_t; g2.row0_z = Y; g2.err = st->err;
-    launch_tc(st->cx, st->t0t_b, g2, batch, (Y / TC_BN) * (X / TC_BM), s);
     // G3: T12t (2Y x BX) = [Ay; Sy] . P^T  -> split planes
     TcArgs g3{};
     g3.M = 2 * Y; g3.N = static_cast<int>(BX); g3.K = Y;
     g3.a_row0 = 0; g3.a_lo = 2 * Y; g3.b_row0 = 0; g3.b_lo = static_cast<int>(BXc); g3.b_col_z = 0;
     g3.mode = TC_SPLIT; g3.planes = pl.t12t_s; g3.plane_stride = 2 * static_cast<int64_t>(Y) * BXc;
     g3.plane_z = 0; g3.ldc = BXc; g3.err = st->err;
-    launch_tc(st->bcat, st->p_b, g3, 1, (X / TC_BN) * (2 * Y / TC_BM), s);
     // G4 in one launch of 3X rows: [phi; xi_x]_z = [Ax; Sx] . T1t[:, z]^T (rows < 2X) and
     // xi_y_z = Ax . T2t[:, z]^T (the alternate region, rows >= 2X)
     TcArgs g4{};
@@ -660,7 +916,49 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
     g4.a_row0 = 0; g4.a_lo = 2 * X; g4.b_row0 = 0; g4.b_lo = 2 * Y; g4.b_col_z = X;
     g4.mode = TC_F32; g4.out = phi; g4.out2 = ex; g4.split = X; g4.ldc = Y; g4.out_z = XY; g4.err = st->err;
     g4.m_alt = 2 * X; g4.a_alt_row0 = 0; g4.b_alt_row0 = Y; g4.out3 = ey;
-    launch_tc(st->acat, st->t12t_b, g4, batch, (Y / TC_BN) * (3 * X / TC_BM), s);
+    const int tiles[4] = {(X / TC_BN) * (Y / TC_BM), (Y / TC_BN) * (X / TC_BM), (X / TC_BN) * (2 * Y / TC_BM),
+                          (Y / TC_BN) * (3 * X / TC_BM)};
+    const int slabs[4] = {Y / TC_BK, X / TC_BK, Y / TC_BK, X / TC_BK};
+    int split[4];
+    bool fusable = batch == 1;
+    for (int k = 0; k < 4; ++k) {
+        split[k] = pick_splits(tiles[k], slabs[k]);
+        fusable = fusable && split[k] <= kFusedCluster;
+    }
+    if (fusable && pl.single_launch && fused_resident()) {
+        // one launch: G1, the split of T0t, G2, G3, G4 (same tiles, splits and orders as below)
+        FusedMaps mp;
+        mp.a[0] = st->cy;
+        mp.b[0] = st->rho_b;
+        mp.a[1] = st->cx;
+        mp.b[1] = st->t0t_b;
+        mp.a[2] = st->bcat;
+        mp.b[2] = st->p_b;
+        mp.a[3] = st->acat;
+        mp.b[3] = st->t12t_b;
+        FusedArgs fa{};
+        fa.g[0] = g1;
+        fa.g[1] = g2;
+        fa.g[2] = g3;
+        fa.g[3] = g4;
+        for (int k = 0; k < 4; ++k) fa.split[k] = split[k];
+        fa.t0t32 = st->t0t32;
+        fa.rows = Y;
+        fa.len = X;
+        fa.ld = BXc;
+        fa.t0t_s = pl.t0t_s;
+        fa.plane_stride = static_cast<int64_t>(Y) * BXc;
+        fa.sum_t = sum_t;
+        fa.bar = st->bar;
+        fa.err = st->err;
+        launch_fused(mp, fa, s);
+        return;
+    }
+    launch_tc(st->cy, st->rho_b, g1, 1, tiles[0], s);
+    prep_split(st->t0t32, Y, static_cast<int>(BX), BXc, X, 1, pl.t0t_s, static_cast<int64_t>(Y) * BXc, sum_t, s);
+    launch_tc(st->cx, st->t0t_b, g2, batch, tiles[1], s);
+    launch_tc(st->bcat, st->p_b, g3, 1, tiles[2], s);
+    launch_tc(st->acat, st->t12t_b, g4, batch, tiles[3], s);
 }
 
 }  // namespace spg

@@ -53,6 +53,7 @@ def lib():
         L.spg_poisson_solve_device.argtypes = [vp, vp, vp, vp, vp, vp]
         L.spg_poisson_solve_batch_device.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp]
         L.spg_poisson_destroy.argtypes = [vp]
+        L.spg_poisson_set_single_launch.argtypes = [vp, C.c_int]
         L.spg_poisson_solve_static.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, vp, vp, vp,
                                                vp, vp]
         L.spg_fillers_plan.argtypes = [C.POINTER(abi.DbView), C.c_float, C.POINTER(abi.FillerInfo)]
@@ -122,12 +123,14 @@ class PoissonBackend:
     ``solve(density, phi, field_x, field_y)`` takes and fills host arrays of shape
     (nx, ny) (row-major, y fast), as the reference's spans."""
 
-    def __init__(self, nx, ny, step_x, step_y, precision=abi.POISSON_FP32, batch=1):
+    def __init__(self, nx, ny, step_x, step_y, precision=abi.POISSON_FP32, batch=1, single_launch=False):
         self.nx, self.ny = int(nx), int(ny)
         h = C.c_void_p()
         check(lib().spg_poisson_create_batched(self.nx, self.ny, step_x, step_y, precision, batch,
                                                C.byref(h)))
         self.h = h
+        if single_launch:  # one persistent launch per one-grid split-BF16 solve (spg_poisson_set_single_launch)
+            check(lib().spg_poisson_set_single_launch(self.h, 1))
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -93,7 +93,9 @@ class _Slot:
         from . import engine
 
         t = [time.perf_counter()]
-        params = abi.default_params(gp_bin_dim=req.bin_dim, poisson_precision=req.precision)
+        # the slots' solves run side by side on the device: separate launches (no grid barriers)
+        params = abi.default_params(gp_bin_dim=req.bin_dim, poisson_precision=req.precision,
+                                    poisson_single_launch=0)
         if self.ctx is None:
             self.ctx = engine.GpContext(req.db, params)
         else:

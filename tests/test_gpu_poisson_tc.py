@@ -71,3 +71,31 @@ def test_poisson_bf16x3_rejects_untiled_grid():
     with pytest.raises(engine.SpgError) as e:
         engine.PoissonBackend(64, 64, 1.0, 1.0, abi.POISSON_BF16X3)
     assert e.value.code == abi.SPG_E_INVALID
+
+
+@pytest.mark.parametrize("nx,ny", [(128, 128), (256, 256), (512, 512), (1024, 1024)])
+def test_fused_solve_matches_separate_launches(nx, ny, monkeypatch):
+    """A one-grid solve runs as one persistent launch (G1, the split of its output, G2, G3, G4
+    with grid barriers between them) where the device holds its clusters at once; it computes
+    the same tiles with the same split-K factors and reduction orders as the separate launches,
+    so the results are the same bits. SPG_POISSON_FUSED=0 selects the separate launches. (Grids
+    whose contractions split K over more than four CTAs, such as 256 x 512, keep the separate
+    launches.)"""
+    monkeypatch.setenv("SPG_POISSON_FUSED", "1")
+    rng = np.random.default_rng(nx * 31 + ny)
+    rho = rng.random((nx, ny)).astype(np.float32)
+    be = engine.PoissonBackend(nx, ny, 1.3, 2.1, abi.POISSON_BF16X3, single_launch=True)
+    n0 = engine.launch_count()
+    fused = be.solve(rho)
+    n_fused = engine.launch_count() - n0
+    monkeypatch.setenv("SPG_POISSON_FUSED", "0")
+    n0 = engine.launch_count()
+    sep = be.solve(rho)
+    n_sep = engine.launch_count() - n0
+    assert n_sep - n_fused == 4, (n_fused, n_sep)  # G1, split, G2, G3, G4 in one launch or five
+    for f, s in zip(fused, sep):
+        assert np.array_equal(f, s)
+    monkeypatch.setenv("SPG_POISSON_FUSED", "1")
+    again = be.solve(rho)  # the barrier counters were left zeroed for the next launch
+    for f, a in zip(fused, again):
+        assert np.array_equal(f, a)
