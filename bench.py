@@ -407,6 +407,9 @@ def run_ours(args):
             line["fp32_value"] = v32
             line["fp32_iterations_per_step"] = it32
             line["bf16x3_over_fp32"] = value / world / v32
+        if args.serve_leg and args.workload == "large":
+            ep.ctx.close()
+            line["serving"] = serve_leg()
         if args.cpu_baseline:
             db.node_x[:] = init_x
             db.node_y[:] = init_y
@@ -621,6 +624,53 @@ def run_mixed_study(args):
                       f"200 fixed macros, {db0.num_nets} nets, {bins}x{bins} bins", "device": out,
                       "cpu_reference": cpu, "cpu_cores": os.cpu_count()}), flush=True)
     return 0
+
+
+def serve_leg(rate=200.0, seconds=1.5, n_designs=16, slots=8):
+    """A short leg of the serving study for the bench line (BASELINE config C4's highest rate):
+    requests from the serving generator (cells log-uniform in 1k..100k) arriving as a Poisson
+    process at `rate` per second for about `seconds`, served by `slots` slots, against the same
+    trace placed one at a time with plain-FP32 solves. placements/s, p50/p99 latency from
+    arrival to the converged placement, and p99 against the median single plain-FP32 solve on
+    an idle device."""
+    from superplace_b200 import engine, generator, serving
+
+    rng = np.random.default_rng(11)
+    designs = []
+    for i in range(n_designs):
+        n = int(round(np.exp(rng.uniform(np.log(1e3), np.log(1e5)))))
+        db, grid = generator.scaled_design(5000 + i, n)
+        engine.initialize_fillers(db, 1.0, 1002)
+        designs.append((db, grid))
+    by_grid = {}
+    for d in designs:
+        by_grid.setdefault(d[1], d)
+
+    def warm(srv, k):
+        for req in by_grid.values():
+            for f in [srv.submit(*req) for _ in range(k)]:
+                f.result()
+
+    with serving.PlacementServer(slots=1, precision="fp32") as srv:
+        warm(srv, 1)
+        single = [srv.submit(db, g).result().latency for db, g in designs]
+    n = max(16, int(rate * seconds))
+    arrivals = serving.poisson_arrivals(rate, n, seed=int(rate))
+    reqs = [designs[i % n_designs] for i in range(n)]
+    with serving.PlacementServer(slots=slots, hbm_budget_bytes=150e9) as srv:
+        warm(srv, slots)
+        ours = serving.summarize(serving.replay(srv, reqs, arrivals))
+    with serving.PlacementServer(slots=1, precision="fp32") as srv:
+        warm(srv, 1)
+        base = serving.summarize(serving.replay(srv, reqs, arrivals))
+    single_ms = float(np.median(single) * 1e3)
+    return {"rate_per_s": rate, "requests": n, "slots": slots, "designs": n_designs,
+            "placements_per_s": ours["placements_per_s"], "p50_ms": ours["p50_ms"], "p99_ms": ours["p99_ms"],
+            "one_at_a_time_fp32_placements_per_s": base["placements_per_s"],
+            "one_at_a_time_fp32_p99_ms": base["p99_ms"],
+            "throughput_ratio": ours["placements_per_s"] / base["placements_per_s"],
+            "single_fp32_solve_median_ms": single_ms, "p99_over_single_solve": ours["p99_ms"] / single_ms,
+            "converged": ours["converged"]}
 
 
 def run_serve(args):
@@ -845,6 +895,8 @@ def main():
     ap.add_argument("--ref-iters", type=int, default=0,
                     help="reference arm: time only the first N mGP iterations of each stage (0: full stages)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-serve-leg", dest="serve_leg", action="store_false",
+                    help="leave out the short serving leg (200 req/s) of the bench line")
     ap.add_argument("--fp32-steps", type=int, default=3,
                     help="stages of the plain FP32 form timed after the headline arm (fp32_value)")
     ap.add_argument("--poisson-sweep", action="store_true",
@@ -869,10 +921,11 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=8.0)
     ap.add_argument("--serve-designs", type=int, default=48)
     args = ap.parse_args()
+    # the serving study and the bench line's serving leg run 8 slots of two streams each: give
+    # the device as many hardware work queues (read when the CUDA context is created, which has
+    # not happened yet in this process)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "16")
     if args.serve:
-        # two streams per slot: give the device as many hardware work queues (read when the
-        # CUDA context is created, which has not happened yet in this process)
-        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "16")
         return run_serve(args)
     if args.poisson_sweep:
         return run_poisson_sweep(args)
