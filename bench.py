@@ -632,7 +632,7 @@ def serve_leg(rate=200.0, seconds=1.5, n_designs=16, slots=8):
     process at `rate` per second for about `seconds`, served by `slots` slots, against the same
     trace placed one at a time with plain-FP32 solves. placements/s, p50/p99 latency from
     arrival to the converged placement, and p99 against the median single plain-FP32 solve on
-    an idle device."""
+    an idle device and against the p99 of the same requests placed alone."""
     from superplace_b200 import engine, generator, serving
 
     rng = np.random.default_rng(11)
@@ -654,6 +654,9 @@ def serve_leg(rate=200.0, seconds=1.5, n_designs=16, slots=8):
     with serving.PlacementServer(slots=1, precision="fp32") as srv:
         warm(srv, 1)
         single = [srv.submit(db, g).result().latency for db, g in designs]
+    with serving.PlacementServer(slots=1) as srv:  # the server's own form, alone on the device
+        warm(srv, 1)
+        alone = [srv.submit(db, g).result().latency for db, g in designs]
     n = max(16, int(rate * seconds))
     arrivals = serving.poisson_arrivals(rate, n, seed=int(rate))
     reqs = [designs[i % n_designs] for i in range(n)]
@@ -664,12 +667,14 @@ def serve_leg(rate=200.0, seconds=1.5, n_designs=16, slots=8):
         warm(srv, 1)
         base = serving.summarize(serving.replay(srv, reqs, arrivals))
     single_ms = float(np.median(single) * 1e3)
+    solo_p99_ms = float(np.percentile([alone[i % n_designs] for i in range(n)], 99) * 1e3)
     return {"rate_per_s": rate, "requests": n, "slots": slots, "designs": n_designs,
             "placements_per_s": ours["placements_per_s"], "p50_ms": ours["p50_ms"], "p99_ms": ours["p99_ms"],
             "one_at_a_time_fp32_placements_per_s": base["placements_per_s"],
             "one_at_a_time_fp32_p99_ms": base["p99_ms"],
             "throughput_ratio": ours["placements_per_s"] / base["placements_per_s"],
             "single_fp32_solve_median_ms": single_ms, "p99_over_single_solve": ours["p99_ms"] / single_ms,
+            "solo_p99_ms": solo_p99_ms, "p99_over_solo_p99": ours["p99_ms"] / solo_p99_ms,
             "converged": ours["converged"]}
 
 

@@ -1,6 +1,5 @@
-"""The QP's BiCGSTAB on the GPU (qp_device.cu) against the host solver, which the CPU tests
-check against the oracle: the same summation order on both sides, so the placements agree
-bit for bit."""
+"""The QP's BiCGSTAB on the GPU (qp_device.cu) against the host solver (the same summation
+order on both sides, so the placements agree bit for bit) and directly against the oracle."""
 import numpy as np
 import pytest
 
@@ -41,3 +40,20 @@ def test_device_qp_is_deterministic_and_handles_trivial_systems():
     c, rc = run(db, device=1, ignore_net_degree=1)
     h, rh = run(db, device=0, ignore_net_degree=1)
     assert np.array_equal(c.node_x, h.node_x) and np.array_equal(rc["hpwl"], rh["hpwl"])
+
+
+def test_device_qp_matches_oracle():
+    """The device solver directly against oracle/qp.py (numpy float32, the reference's order;
+    its dot products are numpy's, so the bar is a tolerance): HPWL of every outer iteration
+    within 1e-4 relative and positions within 1e-3 of the core size, as the host solver's CPU
+    test holds them."""
+    from oracle import qp as oqp
+
+    db = qp_design()
+    dev, rows = run(db, device=1)
+    x, y, hist = oqp.place(db, db.net_weight)
+    n = db.num_movable
+    assert rows["iter"].shape[0] == len(hist)
+    assert np.allclose(rows["hpwl"], hist, rtol=1e-4)
+    assert np.abs(dev.node_x[:n] - x[:n]).max() < 1e-3 * (db.core[2] - db.core[0])
+    assert np.abs(dev.node_y[:n] - y[:n]).max() < 1e-3 * (db.core[3] - db.core[1])
