@@ -1004,7 +1004,7 @@ void stage_setup(Context& c, int stage) {
             for (DevBuf<int>* b : {&c.fo_key, &c.fo_tmp, &c.fo_perm, &c.fo_fid, &c.fo_fid_tmp}) b->alloc(nfs);
             for (DevBuf<int>* b : {&c.fo_count, &c.fo_offset, &c.fo_cursor}) b->alloc(keys);
             c.fo_skip.alloc(1);
-            c.fo_scratch.alloc(2 * nfs * (NUM_ROLES + SNAP_MAX));
+            c.fo_scratch.alloc(2 * nfs * static_cast<size_t>(filler_order_vectors()));
             iota_kernel<<<work_grid(reinterpret_cast<const void*>(iota_kernel), nf, RED_THREADS), RED_THREADS, 0, s>>>(
                 c.fo_fid.p, nf);
             count_launch();

@@ -262,10 +262,11 @@ struct FillerOrderBufs {
     int *key_of, *tmp, *perm, *fid, *fid_tmp;  // nf each; fid = filler id of each filler slot
     int *count, *offset, *cursor;               // n_keys each
     int* skip;                                  // 1 when a tile exceeds the segment capacity
-    float* scratch;                             // 2 * nf * (NUM_ROLES + SNAP_MAX)
+    float* scratch;                             // 2 * nf * filler_order_vectors()
     int* opt_idx;                               // the opt set's node ids (the fillers' are rewritten)
 };
 int filler_order_keys(int dim);
+int filler_order_vectors();
 // Reorders the filler segment of the opt set by tile of the current u (see filler_order.cu).
 void launch_filler_order(const DevPtrs& p, const FillerOrderBufs& b, cudaStream_t s);
 

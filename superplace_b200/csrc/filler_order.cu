@@ -14,8 +14,9 @@
 // atomics are fire-and-forget reductions, and the staging's block barriers cost more than the
 // L2 atomic traffic they saved.)
 //
-// The reorder is a permutation of the filler segment of every optimizer vector (all roles and
-// snapshots, x and y halves), of the fillers' node ids (opt_idx), and of the filler id table
+// The reorder is a permutation of the filler segment of every optimizer vector the loop still
+// reads (its live roles and the snapshots, x and y halves), of the fillers' node ids (opt_idx),
+// and of the filler id table
 // that maps the permuted slots back to the fillers. It changes no value, only the order of the
 // FP64 sums over the opt set, and it is deterministic: tile counts are order-free, and each
 // tile's fillers are ranked by their previous index.
@@ -26,7 +27,7 @@
 //          reorder as skipped (the order then stays as it is)
 //   place  each filler into its tile's segment (any order within the segment)
 //   rank   each segment sorted by previous index (one warp per tile, rank by comparison)
-//   apply  gather every pool vector's filler segment into a scratch copy; commit copies it
+//   apply  gather those vectors' filler segments into a scratch copy; commit copies them
 //          back and rewrites opt_idx
 #include <algorithm>
 
@@ -143,6 +144,24 @@ __global__ void __launch_bounds__(32 * kRankWarps) fsort_rank_kernel(const int* 
     }
 }
 
+// The pool vectors whose filler segments the reorder permutes: the six roles the loop reads
+// before it writes them (u, v, uPrev, vPrev, g, gPrevTmp) and every snapshot slot. The other
+// roles are written whole before they are next read (u', v' by the step kernel, the delivered
+// positions by the deliver kernel) or serve only the stage's set-up (probe, gA, gB).
+constexpr int kOrderVectors = 6 + SNAP_MAX;
+
+__device__ __forceinline__ int order_slot(const DevPtrs& p, int v) {
+    switch (v) {
+        case 0: return p.st->role[R_U];
+        case 1: return p.st->role[R_V];
+        case 2: return p.st->role[R_UPREV];
+        case 3: return p.st->role[R_VPREV];
+        case 4: return p.st->role[R_G];
+        case 5: return p.st->role[R_GPREVTMP];
+        default: return NUM_ROLES + (v - 6);
+    }
+}
+
 // scratch[(v * 2 + h) * nf + j] = pool vector v, half h, filler perm[j]; fid_new[j] = fid[perm[j]]
 __global__ void fsort_apply_kernel(DevPtrs p, const int* perm, const int* fid, int* fid_new, float* scratch,
                                    const int* skip) {
@@ -151,7 +170,7 @@ __global__ void fsort_apply_kernel(DevPtrs p, const int* perm, const int* fid, i
     if (*skip) return;
     const int n = p.n_opt, k0 = p.filler_k0, nf = n - k0;
     const int v = blockIdx.y;
-    const float* src = p.pool + static_cast<size_t>(v) * p.vec_stride;
+    const float* src = p.pool + static_cast<size_t>(order_slot(p, v)) * p.vec_stride;
     float* dst = scratch + static_cast<size_t>(v) * 2 * nf;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nf; j += gridDim.x * blockDim.x) {
         const int q = perm[j];
@@ -168,7 +187,7 @@ __global__ void fsort_commit_kernel(DevPtrs p, const float* scratch, const int* 
     if (*skip) return;
     const int n = p.n_opt, k0 = p.filler_k0, nf = n - k0;
     const int v = blockIdx.y;
-    float* dst = p.pool + static_cast<size_t>(v) * p.vec_stride;
+    float* dst = p.pool + static_cast<size_t>(order_slot(p, v)) * p.vec_stride;
     const float* src = scratch + static_cast<size_t>(v) * 2 * nf;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < nf; j += gridDim.x * blockDim.x) {
         dst[k0 + j] = src[j];
@@ -183,6 +202,8 @@ __global__ void fsort_commit_kernel(DevPtrs p, const float* scratch, const int* 
 
 }  // namespace
 
+int filler_order_vectors() { return kOrderVectors; }
+
 int filler_order_keys(int dim) {
     int t = (dim + kTileBins - 1) / kTileBins, side = 1;
     while (side < t) side <<= 1;
@@ -193,7 +214,7 @@ void launch_filler_order(const DevPtrs& p, const FillerOrderBufs& b, cudaStream_
     const int nf = p.n_opt - p.filler_k0;
     if (nf <= 0) return;
     const int n_keys = filler_order_keys(p.geom.dim);
-    const int n_vec = NUM_ROLES + SNAP_MAX;
+    const int n_vec = kOrderVectors;
     SPG_CUDA(cudaMemsetAsync(b.count, 0, static_cast<size_t>(n_keys) * sizeof(int), s));
     const int blocks = std::min(ceil_div(nf, 256), 148 * 8);
     launch_pdl(fsort_key_kernel, dim3(blocks), dim3(256), 0, s, p, b.key_of, b.count);
