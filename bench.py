@@ -7,9 +7,10 @@ the reference's own definition (mGP_iterations / durations_ms["mGP"],
 src/gp/eplace.cpp:310,515).
 
   value  loop time from CUDA events on the engine's stream (inputs resident in HBM)
-  e2e    the same metric through the public API (EPlace.run on a host PlaceDB): H2D of
-         positions/flags, stage set-up, the loop and the D2H of the delivered positions,
-         bracketed by CUDA events on the engine's stream
+  e2e    the same metric through the public API (EPlace.run on a host PlaceDB whose positions
+         and flags sit in page-locked memory): H2D of positions/flags, stage set-up, the loop
+         and the D2H of the delivered positions, bracketed by CUDA events on the engine's
+         stream
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision bf16x3|fp32] [--workload large|small]
@@ -316,6 +317,7 @@ def run_ours(args):
     precision = abi.POISSON_BF16X3 if args.precision == "bf16x3" else abi.POISSON_FP32
     db = make_design(args.workload)
     engine.initialize_fillers(db, 1.0, 1002)
+    engine.pin_positions(db)  # the step's inputs and result in page-locked host memory
     init_x, init_y = db.node_x.copy(), db.node_y.copy()
     params = abi.default_params(gp_bin_dim=WORKLOADS[args.workload]["bin_dim"],
                                 poisson_precision=precision)

@@ -256,12 +256,19 @@ int spg_ctx_create(const spg_db_view* db, const spg_params* params, spg_ctx** ou
 int spg_ctx_load(spg_ctx* ctx, const spg_db_view* db, const spg_params* params);
 int spg_ctx_destroy(spg_ctx* ctx);
 
-/* Upload new centre positions for all num_nodes + num_fillers nodes. The arrays are copied
- * before the call returns (into the context's pinned staging memory); the device copy runs
- * on the context's stream ahead of its next work. */
+/* Upload new centre positions for all num_nodes + num_fillers nodes. The arrays may be reused
+ * once the call returns: page-locked arrays (spg_host_alloc) are copied by DMA and waited
+ * for; pageable ones are copied into the context's pinned staging memory and their device
+ * copy runs on the context's stream ahead of its next work. */
 int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y);
-/* Download the current centre positions of all nodes. */
+/* Download the current centre positions of all nodes (complete on return; direct DMA into
+ * page-locked arrays, through the staging memory into pageable ones). */
 int spg_positions_d2h(spg_ctx* ctx, float* x, float* y);
+/* Page-locked host memory for the position arrays of spg_positions_h2d / _d2h, so that their
+ * copies skip the host-side staging copy. No counterpart in the reference, which keeps its
+ * PlaceDB in ordinary host memory. */
+int spg_host_alloc(size_t bytes, void** out);
+int spg_host_free(void* p);
 /* Replace node flags (e.g. macros frozen by mLG get SPG_F_FIXED, gp_stage.cpp:130-177). */
 int spg_flags_h2d(spg_ctx* ctx, const uint8_t* flags);
 

@@ -251,10 +251,42 @@ void upload_bytes(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     SPG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
 }
 
+// Whether [p, p + bytes) lies in page-locked host memory (cudaHostAlloc'd or registered), which
+// the copy engines read and write directly: a caller's array there needs no staging.
+bool host_pinned(const void* p, size_t bytes) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();  // pageable memory on an older driver reports an error
+        return false;
+    }
+    if (a.type != cudaMemoryTypeHost) return false;
+    const char* last = static_cast<const char*>(p) + bytes - 1;
+    if (cudaPointerGetAttributes(&a, last) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Two host -> device copies of `bytes` each from a caller's arrays, which are free again once
+// this returns: from page-locked arrays, direct DMA on `s` and one wait for both; from
+// pageable ones, copies into the context's staging memory (no wait).
+void upload_pair(void* dst0, const void* src0, void* dst1, const void* src1, size_t bytes, cudaStream_t s) {
+    if (!bytes) return;
+    if (host_pinned(src0, bytes) && host_pinned(src1, bytes)) {
+        SPG_CUDA(cudaMemcpyAsync(dst0, src0, bytes, cudaMemcpyHostToDevice, s));
+        SPG_CUDA(cudaMemcpyAsync(dst1, src1, bytes, cudaMemcpyHostToDevice, s));
+        SPG_CUDA(host_wait(s));
+        return;
+    }
+    upload_bytes(dst0, src0, bytes, s);
+    upload_bytes(dst1, src1, bytes, s);
+}
+
 // Two device -> host copies of `bytes` each, complete on return, with one wait.
 void download_pair(void* dst0, const void* src0, void* dst1, const void* src1, size_t bytes, cudaStream_t s) {
     if (!bytes) return;
-    if (t_staging && t_staging->s == s) {
+    if (t_staging && t_staging->s == s && !(host_pinned(dst0, bytes) && host_pinned(dst1, bytes))) {
         // one region for both (a second reservation could recycle the first's memory)
         const size_t half = (bytes + 255) & ~static_cast<size_t>(255);
         char* d0 = static_cast<char*>(t_staging->reserve(2 * half));
@@ -676,25 +708,30 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     c.step_x_gamma = g.step_x;
     const size_t n = static_cast<size_t>(dim) * dim;
 
-    // terminal density (bin_grid.cpp:120-137)
+    // terminal density (bin_grid.cpp:120-137): every bin adds its fixed nodes' overlaps in
+    // node order; thread `part` of the pass below takes the bin columns bx = part (mod 4)
+    std::vector<int> fixed_nodes;
+    for (int i = 0; i < c.num_nodes; ++i)
+        if (c.fixed(i) && !c.ni(i)) fixed_nodes.push_back(i);
     std::vector<float> term(n, 0.f), base(n, 0.f);
-    for (int i = 0; i < c.num_nodes; ++i) {
-        if (!c.fixed(i) || c.ni(i)) continue;
-        const float lx = hx_pos[i] - 0.5f * c.w[i], hx = hx_pos[i] + 0.5f * c.w[i];
-        const float ly = hy_pos[i] - 0.5f * c.h[i], hy = hy_pos[i] + 0.5f * c.h[i];
-        const int bx0 = clampi_h(static_cast<int>((lx - g.origin_x) / g.step_x), 0, dim - 1);
-        const int bx1 = clampi_h(static_cast<int>((hx - g.origin_x) / g.step_x), 0, dim - 1);
-        const int by0 = clampi_h(static_cast<int>((ly - g.origin_y) / g.step_y), 0, dim - 1);
-        const int by1 = clampi_h(static_cast<int>((hy - g.origin_y) / g.step_y), 0, dim - 1);
-        for (int bx = bx0; bx <= bx1; ++bx) {
-            const float blx = g.origin_x + bx * g.step_x;
-            for (int by = by0; by <= by1; ++by) {
-                const float bly = g.origin_y + by * g.step_y;
-                term[static_cast<size_t>(bx) * dim + by] +=
-                    target * overlap_area(blx, bly, blx + g.step_x, bly + g.step_y, lx, ly, hx, hy);
+    auto terminal_part = [&](int part) {
+        for (int i : fixed_nodes) {
+            const float lx = hx_pos[i] - 0.5f * c.w[i], hx = hx_pos[i] + 0.5f * c.w[i];
+            const float ly = hy_pos[i] - 0.5f * c.h[i], hy = hy_pos[i] + 0.5f * c.h[i];
+            const int bx0 = clampi_h(static_cast<int>((lx - g.origin_x) / g.step_x), 0, dim - 1);
+            const int bx1 = clampi_h(static_cast<int>((hx - g.origin_x) / g.step_x), 0, dim - 1);
+            const int by0 = clampi_h(static_cast<int>((ly - g.origin_y) / g.step_y), 0, dim - 1);
+            const int by1 = clampi_h(static_cast<int>((hy - g.origin_y) / g.step_y), 0, dim - 1);
+            for (int bx = bx0 + ((part - bx0) % 4 + 4) % 4; bx <= bx1; bx += 4) {
+                const float blx = g.origin_x + bx * g.step_x;
+                for (int by = by0; by <= by1; ++by) {
+                    const float bly = g.origin_y + by * g.step_y;
+                    term[static_cast<size_t>(bx) * dim + by] +=
+                        target * overlap_area(blx, bly, blx + g.step_x, bly + g.step_y, lx, ly, hx, hy);
+                }
             }
         }
-    }
+    };
     // base density: non-row area of each bin (bin_grid.cpp:144-173)
     const int nr = static_cast<int>(c.row_ly.size());
     std::vector<int> order(nr);
@@ -708,8 +745,9 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         rlx[t] = c.row_lx[r];
         rhx[t] = c.row_lx[r] + c.row_step[r] * static_cast<float>(c.row_sites[r]);
     }
-    // bin rows are independent: four threads take every fourth one
+    // bin rows are independent: four threads take every fourth one (after their terminal part)
     run_parts(4, [&](int part) {
+    terminal_part(part);
     for (int by = part; by < dim; by += 4) {
         const float bly = g.origin_y + by * g.step_y;
         const float bhy = bly + g.step_y;
@@ -739,16 +777,29 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     // large nodes (only nodes at least a bin wide or tall can be) and the small-node count
     std::vector<int>& dlarge = c.dens_large_h;
     dlarge.clear();
-    int n_small = 0;
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};  // bound partials: node i adds into acc[i % 4]
-    for (int i = 0; i < c.total; ++i) {
-        if (c.fixed(i) || c.ni(i)) continue;
-        const float w = c.w[i], h = c.h[i];
-        acc[i & 3] += static_cast<double>(w) * static_cast<double>(h);
-        const bool large = !(w < g.step_x && h < g.step_y) && (node_footprint(c, g, target, i).kind & K_LARGE);
-        if (large) dlarge.push_back(i);
-        else ++n_small;
-    }
+    // bound partials: node i adds into acc[i % 4], in ascending i; thread t owns partial t (the
+    // same sums in the same order as one pass), its large nodes and its small-node count
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    int small_t[4] = {0, 0, 0, 0};
+    std::vector<int> large_t[4];
+    run_parts(4, [&](int t) {
+        double a = 0.0;
+        int ns = 0;
+        std::vector<int>& lg = large_t[t];
+        for (int i = t; i < c.total; i += 4) {
+            if (c.fixed(i) || c.ni(i)) continue;
+            const float w = c.w[i], h = c.h[i];
+            a += static_cast<double>(w) * static_cast<double>(h);
+            const bool large = !(w < g.step_x && h < g.step_y) && (node_footprint(c, g, target, i).kind & K_LARGE);
+            if (large) lg.push_back(i);
+            else ++ns;
+        }
+        acc[t] = a;
+        small_t[t] = ns;
+    });
+    const int n_small = (small_t[0] + small_t[1]) + (small_t[2] + small_t[3]);
+    for (const std::vector<int>& lg : large_t) dlarge.insert(dlarge.end(), lg.begin(), lg.end());
+    std::sort(dlarge.begin(), dlarge.end());
     double bound = (acc[0] + acc[1]) + (acc[2] + acc[3]);
     // fixed-point scale: largest s <= 40 with (total charge bound) * 2^s < 2^62
     bound *= target > 1.f ? static_cast<double>(target) : 1.0;
@@ -915,7 +966,9 @@ void stage_setup(Context& c, int stage) {
     {
         const int f0 = c.num_nodes;
         same = same && c.fillers_alike;  // sizes, degrees and pin slots: fixed per netlist
-        for (int i = f0; same && i < c.total; ++i) same = c.flags[i] == c.flags[f0];
+        // all flags equal: the run equals itself shifted by one
+        same = same && (c.total - f0 < 2 ||
+                        std::memcmp(c.flags.data() + f0, c.flags.data() + f0 + 1, c.total - f0 - 1) == 0);
         if (same) {
             const NodeFootprint fp = node_footprint(c, c.geom, c.geom.target_density, f0);
             c.filler_k0 = k0;
@@ -1974,6 +2027,22 @@ int spg_device_check(void) {
     return SPG_OK;
 }
 
+int spg_host_alloc(size_t bytes, void** out) {
+    API_TRY
+    SPG_REQUIRE(out, SPG_E_INVALID, "null argument");
+    *out = nullptr;
+    SPG_CUDA(cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_host_free(void* p) {
+    API_TRY
+    if (p) SPG_CUDA(cudaFreeHost(p));
+    return SPG_OK;
+    API_CATCH
+}
+
 void spg_params_default(spg_params* p) {
     std::memset(p, 0, sizeof(*p));
     p->target_density = 1.0f;
@@ -2205,10 +2274,9 @@ int spg_positions_h2d(spg_ctx* ctx, const float* x, const float* y) {
     SPG_REQUIRE(ctx && x && y, SPG_E_INVALID, "null argument");
     Context& c = ctx->c;
     spg::CtxScope scope(c);
-    // staged copies: the caller's arrays are free once this returns, and the copies run on
-    // the context's stream ahead of its next work (no wait here)
-    spg::upload_bytes(c.x.p, x, c.total * sizeof(float), c.stream);
-    spg::upload_bytes(c.y.p, y, c.total * sizeof(float), c.stream);
+    // the caller's arrays are free once this returns: page-locked ones are copied by DMA and
+    // waited for, pageable ones are staged and their copies run ahead of the context's next work
+    spg::upload_pair(c.x.p, x, c.y.p, y, c.total * sizeof(float), c.stream);
     c.x_mirror.assign(x, x + c.num_nodes);
     c.y_mirror.assign(y, y + c.num_nodes);
     c.mirror_valid = true;

@@ -65,6 +65,8 @@ def lib():
         L.spg_positions_h2d.argtypes = [vp, fp, fp]
         L.spg_positions_d2h.argtypes = [vp, fp, fp]
         L.spg_flags_h2d.argtypes = [vp, C.POINTER(C.c_uint8)]
+        L.spg_host_alloc.argtypes = [C.c_size_t, C.POINTER(vp)]
+        L.spg_host_free.argtypes = [vp]
         L.spg_grid_init.argtypes = [vp, C.c_float, C.c_int]
         L.spg_grid_info.argtypes = [vp, ip, fp, fp, fp, fp, dp]
         L.spg_grid_read.argtypes = [vp, C.c_int, fp]
@@ -114,6 +116,43 @@ def device_available() -> bool:
 
 def launch_count() -> int:
     return int(lib().spg_ctx_launch_count(None))
+
+
+class _PinnedBlock:
+    """Page-locked host memory from spg_host_alloc, freed with the last array viewing it."""
+
+    def __init__(self, nbytes):
+        self.ptr = C.c_void_p()
+        check(lib().spg_host_alloc(max(int(nbytes), 1), C.byref(self.ptr)))
+        self.nbytes = int(nbytes)
+        self.__array_interface__ = {"shape": (self.nbytes,), "typestr": "|u1", "version": 3,
+                                    "data": (self.ptr.value, False)}
+
+    def __del__(self):
+        if self.ptr:
+            try:
+                lib().spg_host_free(self.ptr)
+            except Exception:  # interpreter shutdown: the process frees it
+                pass
+            self.ptr = C.c_void_p()
+
+
+def pinned_empty(n, dtype) -> np.ndarray:
+    """A 1-D array of n elements in page-locked host memory: the context's position copies
+    from and into such arrays are direct DMA, with no staging copy on the host."""
+    dtype = np.dtype(dtype)
+    return np.asarray(_PinnedBlock(n * dtype.itemsize)).view(dtype)
+
+
+def pin_positions(db: PlaceDB) -> PlaceDB:
+    """Move the PlaceDB's node positions and flags into page-locked memory (values kept), so
+    that EPlace.run's uploads and its read-back of the result are direct DMA."""
+    for k, dt in (("node_x", np.float32), ("node_y", np.float32), ("node_flags", np.uint8)):
+        a = np.ascontiguousarray(getattr(db, k), dt)
+        p = pinned_empty(a.size, dt)
+        p[:] = a
+        setattr(db, k, p)
+    return db
 
 
 # ------------------------------------------------------------------ Poisson operator

@@ -67,6 +67,32 @@ def test_caller_arrays_are_free_after_the_position_upload():
     assert np.array_equal(px, db_ref.node_x) and np.array_equal(py, db_ref.node_y)
 
 
+def test_page_locked_positions_place_the_same():
+    """Positions and flags in page-locked memory (engine.pin_positions) take the direct DMA
+    path of spg_positions_h2d / _d2h: the same placement bit for bit as from pageable arrays,
+    the caller's arrays free again once the upload returns, the result read back in place."""
+    db_ref, _, r_ref, _ = run_small()
+    db, _ = golden_small_db(True)
+    engine.pin_positions(db)
+    x, y = db.node_x, db.node_y
+    ctx = engine.GpContext(db, abi.default_params(gp_bin_dim=64))
+    ctx.set_positions(x, y)
+    keep = x.copy(), y.copy()
+    x[:] = np.nan  # the upload has completed: reusing the arrays changes nothing
+    y[:] = -1.0e9
+    ctx.set_flags(db.node_flags)
+    r = ctx.run(abi.STAGE_MGP)
+    ctx.positions(out=(x, y))
+    ctx.close()
+    assert r.converged == 1 and r.iterations == r_ref.iterations and r.hpwl == r_ref.hpwl
+    assert np.array_equal(x, db_ref.node_x) and np.array_equal(y, db_ref.node_y)
+    # and through EPlace.run, which reads the result back into the same page-locked arrays
+    db.node_x[:], db.node_y[:] = keep
+    r2 = engine.EPlace(db, abi.default_params(gp_bin_dim=64)).run(abi.STAGE_MGP)
+    assert r2.iterations == r_ref.iterations and r2.hpwl == r_ref.hpwl
+    assert db.node_x is x and np.array_equal(db.node_x, db_ref.node_x)
+
+
 def test_metrics_csv_rows_from_the_device(tmp_path):
     """The stage's metrics rows as metrics.csv (the reference's MetricsSink columns): one row per
     iteration in order, max_displacement 0 as in the reference's GP, elapsed_ms from the
