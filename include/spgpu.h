@@ -269,6 +269,11 @@ int spg_positions_d2h(spg_ctx* ctx, float* x, float* y);
  * PlaceDB in ordinary host memory. */
 int spg_host_alloc(size_t bytes, void** out);
 int spg_host_free(void* p);
+/* Self-check of the bin-index arithmetic of the density kernels: for each a[i], q_div[i] =
+ * int(a[i] / step) with the float division of BinGrid::footprintOf (src/gp/bin_grid.cpp:49-52)
+ * and q_mul[i] = the same index formed as the double product a[i] * (1/step) rounded to float,
+ * which the kernels use; the two must agree everywhere. */
+int spg_bin_index_check(float step, const float* a, int32_t n, int32_t* q_div, int32_t* q_mul);
 /* Replace node flags (e.g. macros frozen by mLG get SPG_F_FIXED, gp_stage.cpp:130-177). */
 int spg_flags_h2d(spg_ctx* ctx, const uint8_t* flags);
 

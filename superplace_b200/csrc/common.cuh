@@ -169,6 +169,9 @@ struct GridGeom {
     int shift;            // fixed-point scale 2^shift
     double scale;         // 2^shift
     double inv_scale;     // 2^-shift
+    double inv_step_x;    // 1 / step_x and 1 / step_y, rounded to double (bin_index)
+    double inv_step_y;
+    float scale_f;        // 2^shift as a float when shift >= 0, else 0 (to_fixed)
 };
 
 // Per density node data fixed for a stage: half extents after local smoothing and the
@@ -180,6 +183,18 @@ struct Footprint {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
+// The bin index int(a / step) of bin_grid.cpp:49-52, with a / step the float quotient,
+// formed as the double product a * (1/step) rounded once to float. This is the float quotient
+// bit for bit: the double product is within 2^-52 (relative) of the exact quotient a/step,
+// and the exact quotient of two floats with 24-bit significands is either a float or at least
+// 2^-49 (relative) away from every midpoint between consecutive floats (a = mid * step would
+// need an odd 25-bit significand times a 24-bit one to fit in 24 bits), so both round to the
+// same float; the truncation to int follows as before. Checked against the float division
+// over bin-boundary neighbourhoods and random operands (tests/test_gpu_parity.py).
+__device__ __forceinline__ int bin_index(float a, double inv_step) {
+    return static_cast<int>(__double2float_rn(__dmul_rn(static_cast<double>(a), inv_step)));
+}
+
 // Bin range and smoothed rectangle of a node at centre (x, y). hw/hh are the half extents
 // 0.5f*max(w, step) exactly as footprintOf forms lx = x - 0.5f*W.
 __device__ __forceinline__ Footprint footprint(const GridGeom& g, float x, float y, float hw,
@@ -190,10 +205,10 @@ __device__ __forceinline__ Footprint footprint(const GridGeom& g, float x, float
     f.ly = fsub(y, hh);
     f.hy = fadd(y, hh);
     const int d = g.dim - 1;
-    f.bx0 = clampi(static_cast<int>(fdiv(fsub(f.lx, g.origin_x), g.step_x)), 0, d);
-    f.bx1 = clampi(static_cast<int>(fdiv(fsub(f.hx, g.origin_x), g.step_x)), 0, d);
-    f.by0 = clampi(static_cast<int>(fdiv(fsub(f.ly, g.origin_y), g.step_y)), 0, d);
-    f.by1 = clampi(static_cast<int>(fdiv(fsub(f.hy, g.origin_y), g.step_y)), 0, d);
+    f.bx0 = clampi(bin_index(fsub(f.lx, g.origin_x), g.inv_step_x), 0, d);
+    f.bx1 = clampi(bin_index(fsub(f.hx, g.origin_x), g.inv_step_x), 0, d);
+    f.by0 = clampi(bin_index(fsub(f.ly, g.origin_y), g.inv_step_y), 0, d);
+    f.by1 = clampi(bin_index(fsub(f.hy, g.origin_y), g.inv_step_y), 0, d);
     return f;
 }
 
@@ -210,10 +225,12 @@ __device__ __forceinline__ float bin_contribution(const GridGeom& g, int bx, int
     return fmul(a, w);
 }
 
-// Fixed-point image of one contribution: round-to-nearest-even of c * 2^shift.
-// (c * 2^shift is exact in double, so this is one rounding.)
-__device__ __forceinline__ unsigned long long to_fixed(float c, double scale) {
-    return static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(c) * scale));
+// Fixed-point image of one contribution: round-to-nearest-even of c * 2^shift. The product
+// is exact in double, and in float too when shift >= 0 (a power-of-two scale of a float that
+// stays below the float range), so the float form is the same single rounding.
+__device__ __forceinline__ unsigned long long to_fixed(float c, const GridGeom& g) {
+    if (g.scale_f > 0.f) return static_cast<unsigned long long>(__float2ll_rn(fmul(c, g.scale_f)));
+    return static_cast<unsigned long long>(__double2ll_rn(static_cast<double>(c) * g.scale));
 }
 
 }  // namespace spg

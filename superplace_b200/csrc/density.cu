@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(kThreads) acc_large_kernel(DevPtrs p, const in
         const int bx = f.bx0 + j / ny, by = f.by0 + j % ny;
         const float c = bin_contribution(g, bx, by, f, w);
         if (c <= 0.f) continue;
-        atomicAdd(map + static_cast<size_t>(bx) * g.dim + by, to_fixed(c, g.scale));
+        atomicAdd(map + static_cast<size_t>(bx) * g.dim + by, to_fixed(c, g));
     }
 }
 
@@ -330,6 +330,19 @@ void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s) {
     if (p.n_opt_large > 0) {
         launch_pdl(gather_opt_large_kernel, dim3(p.n_opt_large), dim3(kThreads), 0, s, p);
     }
+}
+
+// Self-check of bin_index: the truncated float quotient a / step and bin_index's product form.
+__global__ void bin_index_check_kernel(const float* a, int n, float step, double inv, int* q_div, int* q_mul) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    q_div[i] = static_cast<int>(fdiv(a[i], step));
+    q_mul[i] = bin_index(a[i], inv);
+}
+
+void launch_bin_index_check(const float* a, int n, float step, double inv, int* q_div, int* q_mul, cudaStream_t s) {
+    if (n > 0)
+        bin_index_check_kernel<<<ceil_div(n, kThreads), kThreads, 0, s>>>(a, n, step, inv, q_div, q_mul);
 }
 
 void launch_gather_all(const DevPtrs& p, float* out, cudaStream_t s) {

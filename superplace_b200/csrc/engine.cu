@@ -704,6 +704,8 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     g.origin_y = c.core_ly;
     g.step_x = (c.core_hx - c.core_lx) / static_cast<float>(dim);
     g.step_y = (c.core_hy - c.core_ly) / static_cast<float>(dim);
+    g.inv_step_x = 1.0 / static_cast<double>(g.step_x);
+    g.inv_step_y = 1.0 / static_cast<double>(g.step_y);
     g.target_density = target;
     c.step_x_gamma = g.step_x;
     const size_t n = static_cast<size_t>(dim) * dim;
@@ -811,6 +813,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     }
     g.shift = s;
     g.scale = std::ldexp(1.0, s);
+    g.scale_f = s >= 0 ? std::ldexp(1.0f, s) : 0.f;
     g.inv_scale = std::ldexp(1.0, -s);
 
     ht.mark("footprints");
@@ -1090,28 +1093,36 @@ bool rho_and_split(Context& c, const DevPtrs& p, cudaStream_t s) {
     return false;
 }
 
-void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count, bool fused_reduce = false,
-              bool stepped = false, cudaGraphConditionalHandle loop_cond = 0) {
-    cudaStream_t s = c.stream;
-    if (pos_role >= 0) launch_scatter(p, pos_role, s);
-    static const bool wa_serial = [] {
+bool wa_serial() {
+    static const bool on = [] {
         const char* e = std::getenv("SPG_WA_SERIAL");
         return e && e[0] == '1';
     }();
-    if (wa_serial) {
-        launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s);
-    } else {
-        SPG_CUDA(cudaEventRecord(c.ev_fork, s));
-        SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
-        launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, c.side);
-        SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
-    }
+    return on;
+}
+
+// The WA pass of an evaluation on the side stream, after the work queued on the main stream
+// so far (it reads the cells' node positions); the assembly joins it.
+void fork_wa(Context& c, const DevPtrs& p) {
+    SPG_CUDA(cudaEventRecord(c.ev_fork, c.stream));
+    SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+    launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, c.side);
+    SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
+}
+
+// wa_forked: the loop's step already forked the WA pass (after the cells' step launch).
+void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int count, bool fused_reduce = false,
+              bool stepped = false, cudaGraphConditionalHandle loop_cond = 0, bool wa_forked = false) {
+    cudaStream_t s = c.stream;
+    if (pos_role >= 0) launch_scatter(p, pos_role, s);
+    if (wa_serial()) launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s);
+    else if (!wa_forked) fork_wa(c, p);
     if (stepped) launch_density_rest(p, s);
     else launch_density_accumulate(p, s);
     const bool fused = rho_and_split(c, p, s);
     poisson_solve(*c.plan, 1, c.rho.p, c.phi.p, c.ex.p, c.ey.p, s, fused);
     launch_gather_opt_large(p, s);
-    if (!wa_serial) SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
+    if (!wa_serial()) SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join, 0));
     if (fused_reduce) launch_assemble_reduce(p, s, loop_cond);
     else launch_assemble(p, pos_role >= 0 ? pos_role : R_U, grad_role, count, s);
 }
@@ -1241,6 +1252,21 @@ void final_metrics(Context& c, const DevPtrs& p, float* overflow, double* hpwl) 
 // condition (loop_cond), so the body needs no kernel of its own for it.
 void enqueue_iteration(Context& c, const DevPtrs& p, cudaGraphConditionalHandle loop_cond = 0) {
     cudaStream_t s = c.stream;
+    // The cells' step, the WA pass forked after it (WA reads only cell positions), then the
+    // fillers' step beside WA: WA then overlaps the fillers' step instead of holding the SMs
+    // that the density -> Poisson chain needs (the chain started up to 22 us late behind it).
+    // 6426-6491 iter/s at 211k cells against 6212-6368 as one launch. SPG_SPLIT_STEP=0: one launch.
+    static const bool split = [] {
+        const char* e = std::getenv("SPG_SPLIT_STEP");
+        return !(e && e[0] == '0');
+    }();
+    if (split && !wa_serial() && p.filler_k0 > 0 && p.filler_k0 < p.n_opt) {
+        launch_update_range(p, 0, p.filler_k0, s);
+        fork_wa(c, p);
+        launch_update_range(p, p.filler_k0, p.n_opt, s);
+        evaluate(c, p, -1, R_G, 1, true, true, loop_cond, true);
+        return;
+    }
     launch_update(p, s);
     evaluate(c, p, -1, R_G, 1, true, true, loop_cond);
 }
@@ -2039,6 +2065,30 @@ int spg_host_alloc(size_t bytes, void** out) {
 int spg_host_free(void* p) {
     API_TRY
     if (p) SPG_CUDA(cudaFreeHost(p));
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_bin_index_check(float step, const float* a, int32_t n, int32_t* q_div, int32_t* q_mul) {
+    API_TRY
+    SPG_REQUIRE(a && q_div && q_mul && n >= 0 && step > 0.f, SPG_E_INVALID, "bad argument");
+    SPG_REQUIRE(spg::device_ok(), SPG_E_NO_DEVICE, "no usable sm_100 device");
+    if (n == 0) return SPG_OK;
+    const size_t bytes = static_cast<size_t>(n) * 4;
+    float* da = nullptr;
+    int *dq = nullptr, *dm = nullptr;
+    SPG_CUDA(cudaMalloc(&da, bytes));
+    SPG_CUDA(cudaMalloc(&dq, bytes));
+    SPG_CUDA(cudaMalloc(&dm, bytes));
+    SPG_CUDA(cudaMemcpy(da, a, bytes, cudaMemcpyHostToDevice));
+    // the same double reciprocal as grid_init's
+    spg::launch_bin_index_check(da, n, step, 1.0 / static_cast<double>(step), dq, dm, nullptr);
+    SPG_CUDA(cudaGetLastError());
+    SPG_CUDA(cudaMemcpy(q_div, dq, bytes, cudaMemcpyDeviceToHost));
+    SPG_CUDA(cudaMemcpy(q_mul, dm, bytes, cudaMemcpyDeviceToHost));
+    cudaFree(da);
+    cudaFree(dq);
+    cudaFree(dm);
     return SPG_OK;
     API_CATCH
 }

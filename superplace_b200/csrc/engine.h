@@ -226,7 +226,7 @@ __device__ __forceinline__ void rasterize(const DevPtrs& p, float x, float y, fl
         for (int by = f.by0; by <= f.by1; ++by) {
             const float c = bin_contribution(g, bx, by, f, w);
             if (c <= 0.f) continue;
-            atomicAdd(row + by, to_fixed(c, g.scale));
+            atomicAdd(row + by, to_fixed(c, g));
         }
     }
 }
@@ -254,6 +254,8 @@ void launch_rho_prep(const DevPtrs& p, uint16_t* planes, int64_t plane_stride, i
 void launch_gather_opt_large(const DevPtrs& p, cudaStream_t s);
 // gather for every density node into a node-indexed 2*total array (parity hook)
 void launch_gather_all(const DevPtrs& p, float* force_nodes, cudaStream_t s);
+// the float quotients int(a[i] / step) and bin_index's form of them, for the self-check
+void launch_bin_index_check(const float* a, int n, float step, double inv, int* q_div, int* q_mul, cudaStream_t s);
 
 // ---- filler_order.cu
 // Device buffers of the fillers' spatial reorder: n_keys = filler_order_keys(dim) tile keys,
@@ -288,6 +290,8 @@ void launch_assemble_reduce(const DevPtrs& p, cudaStream_t s, cudaGraphCondition
 // decisions asked for one) with the density scatter of the new positions fused in; the
 // evaluation that follows accumulates only the rest list
 void launch_update(const DevPtrs& p, cudaStream_t s);
+// the same step over the opt positions [k_begin, k_end) only
+void launch_update_range(const DevPtrs& p, int k_begin, int k_end, cudaStream_t s);
 // the same step over the optimizer vectors alone (no node arrays, no density), clamped into
 // opt_lo / opt_hi: the optimizer run on the quadratic test objective
 void launch_quad_step(const DevPtrs& p, cudaStream_t s);

@@ -446,8 +446,17 @@ __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, d
 
 // One node of the assembly (see assemble_kernel). FILL: a filler, whose attributes are the
 // shared constants (no pins, so no WA term).
+// precondition 1 / max(1, deg + lambda * area) (eplace.cpp:166-189) of one node.
+__device__ __forceinline__ float precondition(int deg, float lambda, double area) {
+    const double den = __dadd_rn(static_cast<double>(deg), __dmul_rn(static_cast<double>(lambda), area));
+    return static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
+}
+
+// filler_pre: the fillers' common preconditioner (their degree and area are the shared
+// constants), formed once per thread.
 template <bool FUSE, bool FILL>
-__device__ __forceinline__ void assemble_node(const DevPtrs& p, int k, float lambda, const float* __restrict__ pos,
+__device__ __forceinline__ void assemble_node(const DevPtrs& p, int k, float lambda, float filler_pre,
+                                              const float* __restrict__ pos,
                                               float* __restrict__ grad, const float* __restrict__ up,
                                               const float* __restrict__ gp, double& acc_wl, double& acc_den,
                                               double& dx, double& dg, double& sy, double& gn) {
@@ -477,8 +486,7 @@ __device__ __forceinline__ void assemble_node(const DevPtrs& p, int k, float lam
     } else {
         gather_at(p, x, y, geo.x, geo.y, geo.z, fx, fy);
     }
-    const double den = __dadd_rn(static_cast<double>(meta.z), __dmul_rn(static_cast<double>(lambda), area));
-    const float precond = static_cast<float>(__ddiv_rn(1.0, fmax(1.0, den)));
+    const float precond = FILL ? filler_pre : precondition(meta.z, lambda, area);
     const float ox = fmul(precond, fsub(gx, fmul(lambda, fx)));
     const float oy = fmul(precond, fsub(gy, fmul(lambda, fy)));
     grad[k] = ox;
@@ -535,9 +543,12 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
     const int k0 = p.filler_k0 < n ? p.filler_k0 : n;
     int k = t0;
     for (; k < k0; k += stride)
-        assemble_node<FUSE, false>(p, k, lambda, pos, grad, up, gp, acc_wl, acc_den, dx, dg, sy, gn);
-    for (; k < n; k += stride)
-        assemble_node<FUSE, true>(p, k, lambda, pos, grad, up, gp, acc_wl, acc_den, dx, dg, sy, gn);
+        assemble_node<FUSE, false>(p, k, lambda, 0.f, pos, grad, up, gp, acc_wl, acc_den, dx, dg, sy, gn);
+    if (k < n) {
+        const float filler_pre = precondition(p.filler_meta.z, lambda, p.filler_area);
+        for (; k < n; k += stride)
+            assemble_node<FUSE, true>(p, k, lambda, filler_pre, pos, grad, up, gp, acc_wl, acc_den, dx, dg, sy, gn);
+    }
     if (FUSE) {
         double v6[6] = {acc_wl, acc_den, dx, dg, sy, gn};
         block_sums(v6);
@@ -613,8 +624,11 @@ __device__ __forceinline__ void nesterov_point(float u, float v, float g, float 
 // the per-coordinate clamp bounds opt_lo / opt_hi.
 // 6 blocks of 256 per SM: the kernel is latency-bound, so occupancy is what hides its loads
 // and atomics. The grid covers the opt set (node_blocks), one node per thread.
+// One launch covers the opt positions [k_begin, k_end): the whole set, or the cells and the
+// fillers as two launches (the WA pass, which reads only cell positions, then starts after the
+// cells' launch).
 template <bool PLACE>
-__global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
+__global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p, int k_begin, int k_end) {
     pdl_wait();
     pdl_trigger();
     DevState* st = p.st;
@@ -630,8 +644,8 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p) {
     float* snap = slot >= 0 ? snap_ptr(p, slot) : nullptr;
     const float alpha = st->alpha, m = redo ? st->momentum_prev : st->momentum;
     const int n = p.n_opt;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool have = k < n;
+    const int k = k_begin + blockIdx.x * blockDim.x + threadIdx.x;
+    const bool have = k < k_end;
     const bool fill = PLACE && k >= p.filler_k0;  // a filler: attributes are the shared constants
     int4 meta{};
     float4 geo{};
@@ -964,10 +978,14 @@ inline int node_blocks(const DevPtrs& p) {
     return b < 1 ? 1 : b;
 }
 void launch_update(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(step_kernel<true>, node_blocks(p), RED_THREADS, p);
+    LAUNCH(step_kernel<true>, node_blocks(p), RED_THREADS, p, 0, p.n_opt);
+}
+void launch_update_range(const DevPtrs& p, int k_begin, int k_end, cudaStream_t s) {
+    const int b = ceil_div(static_cast<int64_t>(k_end - k_begin), RED_THREADS);
+    LAUNCH(step_kernel<true>, b < 1 ? 1 : b, RED_THREADS, p, k_begin, k_end);
 }
 void launch_quad_step(const DevPtrs& p, cudaStream_t s) {
-    LAUNCH(step_kernel<false>, node_blocks(p), RED_THREADS, p);
+    LAUNCH(step_kernel<false>, node_blocks(p), RED_THREADS, p, 0, p.n_opt);
 }
 void launch_quad_eval(const DevPtrs& p, const float* coef, const float* target, int pos_role, int grad_role,
                       int fused, cudaStream_t s) {

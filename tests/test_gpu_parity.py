@@ -200,3 +200,39 @@ def test_total_charge_gpu(small):
     ctx.grid_init(1.0, 64)
     ctx.accumulate()
     assert abs(ctx.total_charge() - float(g["d64_charge"])) < 1e-6
+
+
+def bin_index_operands(step, dim, rng):
+    """Operands of int(a / step): every float within 64 ulps of each bin boundary k * step
+    (k = 0..dim, the products rounded both ways), and random values over the grid and beyond."""
+    s = np.float32(step)
+    k = np.arange(dim + 1, dtype=np.float64)
+    centres = np.concatenate([(k * float(s)).astype(np.float32), np.float32(k) * s,
+                              np.nextafter((k * float(s)).astype(np.float32), np.float32(np.inf))])
+    offs = np.arange(-64, 65, dtype=np.int64)
+    bits = centres.view(np.int32).astype(np.int64)[:, None] + offs[None, :]
+    near = bits[(bits >= 0) & (bits < 0x7F800000)].astype(np.int32).view(np.float32)
+    rand = (rng.random(200_000) * (dim + 2) * float(s)).astype(np.float32)
+    tiny = rng.random(1000).astype(np.float32) * np.float32(1e-30)
+    return np.concatenate([near, rand, -rand[:1000], tiny, np.float32([0.0, -0.0])])
+
+
+@pytest.mark.parametrize("step", [22.65625, 20.88, 0.1, 1.0 / 3.0, 3.0, 7.3e-3, 1234.567, 11600.0 / 512])
+def test_bin_index_equals_float_division(step):
+    """The density kernels form int(a / step) (bin_grid.cpp:49-52) as the double product
+    a * (1/step) rounded to float: the same index as the float division for every operand,
+    checked on the device at every bin boundary's neighbourhood and on random operands."""
+    import ctypes as C
+
+    L = engine.lib()
+    L.spg_bin_index_check.argtypes = [C.c_float, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
+    a = bin_index_operands(step, 2048, np.random.default_rng(7))
+    qd = np.zeros(a.size, np.int32)
+    qm = np.zeros(a.size, np.int32)
+    engine.check(L.spg_bin_index_check(np.float32(step), a.ctypes.data, a.size, qd.ctypes.data, qm.ctypes.data))
+    bad = np.nonzero(qd != qm)[0]
+    assert bad.size == 0, (a[bad[:5]], qd[bad[:5]], qm[bad[:5]])
+    # and the float division itself, as numpy forms it on the host
+    host = np.trunc(a / np.float32(step)).astype(np.int64)
+    ok = np.abs(host) < 2**31
+    assert np.array_equal(host[ok], qd[ok])
