@@ -312,6 +312,25 @@ int spg_stage_run(spg_ctx* ctx, int stage, spg_result* result);
 /* Per-iteration metrics of the last stage run (up to `cap` rows). */
 int spg_metrics_d2h(const spg_ctx* ctx, spg_iter_metrics* rows, int cap, int* n_rows);
 
+/* Iteration callback: EPlace::setIterCallback (src/gp/eplace.h:71-72), which the reference calls
+ * after each iteration's metrics row with the PlaceDB at that iteration's evaluation point
+ * (eplace.cpp:405-409); GlobalPlaceStage's frame hook samples it every frame_stride iterations
+ * (gp_stage.cpp:87-93). Here fn(user, stage, iter, x, y) runs for every iteration with
+ * iter % stride == 0, with x and y the positions of all num_nodes + num_fillers nodes at that
+ * evaluation point (arrays owned by the context, valid during the call). Each call pauses the
+ * device loop for a host round trip; the placement is the same bit for bit with and without
+ * the callback. fn NULL or stride <= 0 turns it off. */
+typedef void (*spg_iter_fn)(void* user, int32_t stage, int32_t iter, const float* x, const float* y);
+int spg_set_iter_callback(spg_ctx* ctx, spg_iter_fn fn, void* user, int32_t stride);
+/* Called once per stage (mGP, cGP), like the iteration callback, at the iteration where the
+ * stagnation guard's counter of iterations without enough overflow gain first reaches half its
+ * window: the reference's stagnation_mid GP diagnostic point (eplace.cpp:428-433). fn NULL: off. */
+int spg_set_stagnation_callback(spg_ctx* ctx, spg_iter_fn fn, void* user);
+/* After a stage run: the positions of all nodes at its last evaluation point (which = 0) or at
+ * the evaluation point before it (which = 1), the inputs of the reference's last_eval GP
+ * diagnostic (writeGpDiagnostic, src/gp/diagnostics.h:13-17; eplace.cpp:476-479). */
+int spg_eval_positions(spg_ctx* ctx, int32_t which, float* x, float* y);
+
 /* Number of kernels this library launched (process-wide) so far. */
 int64_t spg_ctx_launch_count(const spg_ctx* ctx);
 /* The cudaStream_t every call on this context enqueues on (for caller-side CUDA events). */

@@ -75,6 +75,9 @@ def lib():
         L.spref_obj_and_grad.argtypes = [vp, C.POINTER(abi.Params), C.c_int, C.c_float, C.c_float, fp, fp, dp, ip]
         L.spref_legalize_macros.argtypes = [vp, C.POINTER(abi.Params), dp]
         L.spref_gp_four_stage.argtypes = [vp, C.POINTER(abi.Params), dp]
+        L.spref_eplace_run_diagnostics.argtypes = [vp, C.POINTER(abi.Params), C.c_int, C.c_char_p, dp]
+        L.spref_diagnose_delivered.argtypes = [vp, C.POINTER(abi.Params), C.c_int, C.c_char_p, C.c_int, C.c_float,
+                                               C.c_float, C.c_int, fp, C.c_int]
         L.spref_quiet(1)
         _lib = L
     return _lib
@@ -148,6 +151,24 @@ class RefDb:
         if rc:
             raise RuntimeError(f"{rc}: " + lib().spref_last_error().decode())
         return dict(zip(RESULT_FIELDS, list(res))), rows[: nrows.value]
+
+    def eplace_diagnostics(self, params, root, stage=abi.STAGE_MGP):
+        """EPlace::run with gp_diagnostics on, its sink writing under root: the reference's own GP
+        diagnostics of the stage; returns the result dict."""
+        res = (C.c_double * 8)()
+        rc = lib().spref_eplace_run_diagnostics(self.h, C.byref(params), stage, str(root).encode(), res)
+        if rc:
+            raise RuntimeError(f"{rc}: " + lib().spref_last_error().decode())
+        return dict(zip(RESULT_FIELDS, list(res)))
+
+    def diagnose_delivered(self, params, root, stage, it, lam, gamma, dim, previous=None):
+        """diagnoseDelivered (src/gp/diagnostics.cpp:175-191) at the handle's positions."""
+        prev = _f(previous) if previous is not None else None
+        rc = lib().spref_diagnose_delivered(self.h, C.byref(params), stage, str(root).encode(), int(it), float(lam),
+                                            float(gamma), int(dim), prev.ctypes.data_as(C.POINTER(C.c_float))
+                                            if prev is not None else None, 0 if prev is None else prev.size)
+        if rc:
+            raise RuntimeError(f"{rc}: " + lib().spref_last_error().decode())
 
     def n_opt(self, params, stage=abi.STAGE_MGP):
         n = C.c_int(0)

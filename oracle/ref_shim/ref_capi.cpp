@@ -24,6 +24,7 @@
 #include "db/hpwl.h"
 #include "db/place_db.h"
 #include "gp/bin_grid.h"
+#include "gp/diagnostics.h"
 #include "gp/eplace.h"
 #include "gp/filler.h"
 #include "gp/wa_wirelength.h"
@@ -401,6 +402,52 @@ int spref_eplace_run(void* dbh, const spg_params* p, int stage, double* result, 
         }
         *nRows = n;
         (void)init;
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// EPlace::run with Config::gp_diagnostics on and the sink writing under `root`: the reference's
+// own GP diagnostics of the stage (first_eval, stagnation_mid, last_eval, delivered). result as
+// spref_eplace_run's.
+int spref_eplace_run_diagnostics(void* dbh, const spg_params* p, int stage, const char* root, double* result) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(dbh)->db;
+        sp::Config cfg = makeConfig(p);
+        cfg.gp_diagnostics = true;
+        sp::MetricsSink sink;
+        sink.setOutputDir(root);
+        sp::EPlace engine(db, cfg, sink);
+        const double t0 = omp_get_wtime();
+        const sp::GpResult r = engine.run(toStage(stage));
+        putResult(r, (omp_get_wtime() - t0) * 1e3, result);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
+}
+
+// diagnoseDelivered (src/gp/diagnostics.cpp:175-191) at the handle's positions: the reference's
+// "delivered" GP diagnostic for the stage's opt set (buildOptSet, eplace.cpp:82-94), with the
+// opt nodes' previous positions (x then y, opt order; n_prev = 0 for none).
+int spref_diagnose_delivered(void* dbh, const spg_params* p, int stage, const char* root, int iter, float lambda,
+                             float gamma, int grid_dim, const float* previous, int n_prev) {
+    try {
+        sp::PlaceDB& db = static_cast<RefDb*>(dbh)->db;
+        const sp::Config cfg = makeConfig(p);
+        const sp::GpStage st = toStage(stage);
+        std::vector<int> opt;
+        if (st != sp::GpStage::kFillerOnly)
+            for (int i = 0; i < db.numMovable; ++i) {
+                if (db.isFixed(i) || db.isNI(i)) continue;
+                if (st == sp::GpStage::kCGP && db.isMacro(i)) continue;
+                opt.push_back(i);
+            }
+        for (int i = db.numNodes; i < db.totalNodes(); ++i) opt.push_back(i);
+        std::vector<float> prev;
+        if (previous && n_prev > 0) prev.assign(previous, previous + n_prev);
+        sp::diagnoseDelivered(root, sp::toString(st), iter, lambda, gamma, db, cfg, grid_dim, opt, prev);
         return 0;
     } catch (const std::exception& e) {
         return fail(e);

@@ -441,6 +441,16 @@ struct Context : ContextStreams {
     // share their attributes and are numerous; the loop pauses at the listed iterations
     bool fo_active = false;
     std::vector<int> fo_pauses;
+    // the iteration callback (spg_set_iter_callback) and the evaluation-point snapshots
+    spg_iter_fn iter_fn = nullptr;
+    void* iter_user = nullptr;
+    int iter_stride = 0;
+    spg_iter_fn mid_fn = nullptr;  // spg_set_stagnation_callback
+    void* mid_user = nullptr;
+    bool have_eval = false;  // a stage ran: its last evaluation point is on the device
+    int eval_role = 0, eval_prev_role = 0;  // the roles that hold it and the point before it
+    DevBuf<float> frame_x, frame_y;
+    std::vector<float> frame_hx, frame_hy;
     DevBuf<int> fo_key, fo_tmp, fo_perm, fo_fid, fo_fid_tmp, fo_count, fo_offset, fo_cursor, fo_skip;
     DevBuf<float> fo_scratch;
     DevBuf<double> opt_area;
@@ -1190,6 +1200,9 @@ __global__ void init_state_kernel(DevPtrs p, int stage, int max_iter, float targ
     st->rollback_iter = -1;
     st->deliver = 0;
     st->pause_iter = INT_MAX;
+    st->pause_row = INT_MAX;
+    st->diag_mid = 0;
+    st->diag_mid_hit = 0;
 }
 
 __global__ void gamma_init_kernel(DevPtrs p) {
@@ -1202,7 +1215,44 @@ __global__ void gamma_init_kernel(DevPtrs p) {
 
 __global__ void set_hpwl_ref_kernel(DevPtrs p, double ref) { p.st->hpwl_ref = ref; }
 
-__global__ void set_pause_kernel(DevState* st, int at) { st->pause_iter = at; }
+__global__ void set_pause_kernel(DevState* st, int at_iter, int at_row, int diag_mid) {
+    st->pause_iter = at_iter;
+    st->pause_row = at_row;
+    st->diag_mid = diag_mid;
+}
+
+// The opt nodes' positions at the evaluation point held by `role` (R_U: the last evaluated
+// point) written over a copy of the node arrays (whose filler entries are only rewritten when
+// the stage ends): every node's position at that point.
+__global__ void eval_positions_opt_kernel(DevPtrs p, int role, float* out_x, float* out_y) {
+    const float* u = role_ptr(p, role);
+    const int n = p.n_opt;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const int i = p.opt_idx[k];
+        out_x[i] = u[k];
+        out_y[i] = u[n + k];
+    }
+}
+
+// Every node's position at the evaluation point of `role` into the host arrays x, y (total
+// entries each); complete on return.
+void download_eval_positions(Context& c, const DevPtrs& p, int role, float* x, float* y) {
+    const size_t n = static_cast<size_t>(c.total);
+    if (n == 0) return;
+    cudaStream_t s = c.stream;
+    c.frame_x.alloc(n);
+    c.frame_y.alloc(n);
+    SPG_CUDA(cudaMemcpyAsync(c.frame_x.p, c.x.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    SPG_CUDA(cudaMemcpyAsync(c.frame_y.p, c.y.p, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    if (p.n_opt > 0) {
+        eval_positions_opt_kernel<<<work_grid(reinterpret_cast<const void*>(eval_positions_opt_kernel), p.n_opt,
+                                              RED_THREADS),
+                                    RED_THREADS, 0, s>>>(p, role, c.frame_x.p, c.frame_y.p);
+        count_launch();
+        SPG_CHECK_LAUNCH();
+    }
+    download_pair(x, c.frame_x.p, y, c.frame_y.p, n * sizeof(float), s);
+}
 
 // Final metrics at the delivered positions: overflow and HPWL (eplace.cpp:484-488).
 __global__ void final_metrics_kernel(DevPtrs p, double* out) {
@@ -1277,7 +1327,8 @@ void host_loop(Context& c, const DevPtrs& p, int max_iter) {
     // the device sets `done` by max_iter; this bound guards the host loop itself
     const int64_t pass_bound = static_cast<int64_t>(max_iter + 2) * std::max(c.prm.max_backtrack, 1);
     int64_t passes = 0;
-    while (!c.hst->done && c.hst->iter < c.hst->pause_iter) {
+    while (!c.hst->done && c.hst->iter < c.hst->pause_iter && c.hst->rows <= c.hst->pause_row &&
+           !(c.hst->diag_mid && c.hst->diag_mid_hit)) {
         if (++passes > pass_bound) throw Error(SPG_E_STATE, "GP loop exceeded its iteration bound");
         enqueue_iteration(c, p);
         read_state(c);
@@ -1567,6 +1618,7 @@ void stage_run(Context& c, int stage, spg_result* res) {
     std::memset(res, 0, sizeof(*res));
     res->rollback_iter = -1;
     cudaStream_t s = c.stream;
+    c.have_eval = false;
     prepare_stage(c, stage, &ht);
     if (c.n_opt == 0) return;  // "no nodes to optimise" (eplace.cpp:232-236)
     const bool filler_only = stage == SPG_STAGE_FILLER_ONLY;
@@ -1595,6 +1647,8 @@ void stage_run(Context& c, int stage, spg_result* res) {
 
     if (!filler_only && c.hst->tau < target_tau) {
         // already converged: take no step (eplace.cpp:278-296)
+        c.have_eval = true;
+        c.eval_role = c.eval_prev_role = R_POS;
         final_metrics(c, p, &res->overflow, &res->hpwl);
         res->converged = 1;
         return;
@@ -1620,27 +1674,74 @@ void stage_run(Context& c, int stage, spg_result* res) {
     c.last_run_graph = false;
     c.last_graph_build_ms = 0.0;
     if (max_iter > 0) {
-        // the loop runs in segments: it pauses at the filler-reorder iterations, the fillers are
-        // reordered (filler_order.cu) and the loop resumes where it stopped
+        // the loop runs in segments: it pauses at the filler-reorder iterations (the fillers are
+        // reordered, filler_order.cu) and after the metrics rows of the iteration callback's
+        // iterations (the callback runs at that evaluation point), and resumes where it stopped
         size_t next = 0;
+        const bool callback = c.iter_fn && c.iter_stride > 0;
+        int next_row = callback ? 0 : INT_MAX;
+        bool mid_pending = c.mid_fn && stage != SPG_STAGE_FILLER_ONLY && c.prm.gp_stagnation_window > 0;
         auto arm = [&] {
             const int at = (c.fo_active && next < c.fo_pauses.size()) ? c.fo_pauses[next] : INT_MAX;
-            set_pause_kernel<<<1, 1, 0, s>>>(c.st.p, at);
+            set_pause_kernel<<<1, 1, 0, s>>>(c.st.p, at, next_row, mid_pending ? 1 : 0);
             count_launch();
             SPG_CHECK_LAUNCH();
         };
+        // every node's position at the evaluation point u, with the metrics rows so far readable
+        auto frame = [&] {
+            c.metrics_rows = std::min(c.hst->rows, max_iter);
+            c.have_eval = true;  // spg_eval_positions inside the callback: u and the point before
+            c.eval_role = R_U;
+            c.eval_prev_role = R_UPREV;
+            c.frame_hx.resize(c.total);
+            c.frame_hy.resize(c.total);
+            download_eval_positions(c, p, R_U, c.frame_hx.data(), c.frame_hy.data());
+        };
+        // the callbacks due at the current state (the loop has paused right after their row)
+        auto service = [&] {
+            bool any = false;
+            if (callback && c.hst->rows > next_row && !c.hst->error) {
+                // the row of iteration next_row is written and u is its evaluation point
+                frame();
+                c.iter_fn(c.iter_user, stage, next_row, c.frame_hx.data(), c.frame_hy.data());
+                next_row = next_row > INT_MAX - c.iter_stride ? INT_MAX : next_row + c.iter_stride;
+                any = true;
+            }
+            if (mid_pending && c.hst->diag_mid_hit && !c.hst->error) {
+                // the stagnation counter reached half the window at iteration rows - 1
+                frame();
+                c.mid_fn(c.mid_user, stage, c.hst->rows - 1, c.frame_hx.data(), c.frame_hy.data());
+                mid_pending = false;
+                any = true;
+            }
+            return any;
+        };
         arm();
-        read_state(c);  // the state the first segment starts from (iter 0, before any pass)
+        read_state(c);  // the state the first segment starts from: iteration 0 evaluated, its row written
+        if (service() && !c.hst->done) arm();
         c.last_run_graph = c.use_graph;
         for (;;) {
+            if (c.hst->done || c.hst->error) break;
             if (c.last_run_graph) c.last_run_graph = graph_loop(c, p);
             if (!c.last_run_graph) host_loop(c, p, max_iter);
-            if (c.hst->done || c.hst->iter < c.hst->pause_iter) break;
-            launch_filler_order(p, c.filler_order_bufs(), s);
-            ++next;
+            bool resume = service();
+            if (c.hst->done || c.hst->error) break;
+            if (c.fo_active && next < c.fo_pauses.size() && c.hst->iter >= c.fo_pauses[next]) {
+                launch_filler_order(p, c.filler_order_bufs(), s);
+                ++next;
+                resume = true;
+            }
+            if (!resume) break;
             arm();
         }
     }
+    // the last evaluation point: u, unless the loop ran to max_iter, which takes the last step
+    // (v is delivered) and evaluates its u once more without counting it: then the point is
+    // uPrev and the one before it was rotated into the spare slot uNew
+    c.have_eval = true;
+    const bool ran_out = max_iter > 0 && !c.hst->converged && !c.hst->stagnated;
+    c.eval_role = ran_out ? R_UPREV : R_U;
+    c.eval_prev_role = ran_out ? R_UNEW : R_UPREV;
     ht.mark("loop");
     if (ht.on) ht.line += " (graph_build=" + std::to_string(c.last_graph_build_ms).substr(0, 6) + ")";
     SPG_CUDA(cudaEventRecord(e1, s));
@@ -1865,6 +1966,7 @@ void load_netlist(Context& c, const spg_db_view* v, const spg_params* prm) {
                     v->num_pins >= 0 && v->num_nets >= 0,
                 SPG_E_INVALID, "inconsistent db counts");
     c.prm = *prm;
+    c.have_eval = false;
     c.grid_ready = false;
     c.metrics_rows = 0;
     c.num_movable = v->num_movable;
@@ -2550,6 +2652,37 @@ int spg_stage_run(spg_ctx* ctx, int stage, spg_result* result) {
     SPG_REQUIRE(ctx && result, SPG_E_INVALID, "null argument");
     spg::CtxScope scope(ctx->c);
     spg::stage_run(ctx->c, stage, result);
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_set_iter_callback(spg_ctx* ctx, spg_iter_fn fn, void* user, int32_t stride) {
+    API_TRY
+    SPG_REQUIRE(ctx, SPG_E_INVALID, "null argument");
+    spg::Context& c = ctx->c;
+    c.iter_fn = stride > 0 ? fn : nullptr;
+    c.iter_user = user;
+    c.iter_stride = fn ? stride : 0;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_set_stagnation_callback(spg_ctx* ctx, spg_iter_fn fn, void* user) {
+    API_TRY
+    SPG_REQUIRE(ctx, SPG_E_INVALID, "null argument");
+    ctx->c.mid_fn = fn;
+    ctx->c.mid_user = user;
+    return SPG_OK;
+    API_CATCH
+}
+
+int spg_eval_positions(spg_ctx* ctx, int32_t which, float* x, float* y) {
+    API_TRY
+    SPG_REQUIRE(ctx && x && y && (which == 0 || which == 1), SPG_E_INVALID, "bad argument");
+    spg::Context& c = ctx->c;
+    SPG_REQUIRE(c.have_eval, SPG_E_STATE, "no stage has evaluated a point yet");
+    spg::CtxScope scope(c);
+    spg::download_eval_positions(c, c.ptrs(), which == 0 ? c.eval_role : c.eval_prev_role, x, y);
     return SPG_OK;
     API_CATCH
 }

@@ -113,9 +113,15 @@ struct DevState {
     int role[NUM_ROLES];
     unsigned long long t0_ns;
     // the loop stops (without finishing the stage) once iter reaches pause_iter, so the host
-    // can reorder the fillers between two passes (filler_order.cu); INT_MAX: never
+    // can reorder the fillers between two passes (filler_order.cu), and once the metrics row
+    // of iteration pause_row is written (rows > pause_row), so the host can run the iteration
+    // callback at that evaluation point; INT_MAX: never
     int pause_iter;
-    int pause_pad;
+    int pause_row;
+    // diag_mid = 1: the loop also stops once, when the stagnation counter first reaches half
+    // the window (the reference's stagnation_mid diagnostic point); diag_mid_hit records it
+    int diag_mid;
+    int diag_mid_hit;
 };
 
 // Nets of at most this degree get one thread each in WA pass 1 (SPG_WA_THREAD_DEGREE

@@ -252,6 +252,9 @@ __device__ void decide_iteration(const DevPtrs& p, DevState* st) {
             st->since_improve += 1;
         }
         st->best_tau = fmin_(st->best_tau, st->tau);
+        // the stagnation_mid diagnostic point (eplace.cpp:428-433)
+        if (st->diag_mid && !st->diag_mid_hit && st->since_improve >= max(1, p.stagnation_window / 2))
+            st->diag_mid_hit = 1;
         const float tol = fmul(st->best_tau, fadd(1.f, g));
         while (st->snap_count > 0 && st->snap_tau[st->snap_head] > tol) {
             st->snap_head = (st->snap_head + 1) % SNAP_MAX;
@@ -585,9 +588,13 @@ __global__ void __launch_bounds__(RED_THREADS) assemble_kernel(DevPtrs p, int po
         apply_pending_step(&sst);
         finish_evaluation(p, &sst, sums, count_eval);
         decide(p, &sst, sums[5], sums[6], sums[7], sums[8]);
-        // continue while the stage is neither done nor failed nor at a pause (filler reorder)
+        // continue while the stage is neither done nor failed nor at a pause (filler reorder,
+        // iteration callback, stagnation-midpoint callback)
         if (loop_cond)
-            cudaGraphSetConditional(loop_cond, (sst.done || sst.error || sst.iter >= sst.pause_iter) ? 0u : 1u);
+            cudaGraphSetConditional(loop_cond, (sst.done || sst.error || sst.iter >= sst.pause_iter ||
+                                                sst.rows > sst.pause_row || (sst.diag_mid && sst.diag_mid_hit))
+                                                   ? 0u
+                                                   : 1u);
     }
     state_copy_out(p.st, &sst);
 }

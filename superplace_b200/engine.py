@@ -23,6 +23,8 @@ from .placedb import PlaceDB
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libspgpu.so")
 _lib = None
+# spg_iter_fn: (user, stage, iter, x, y)
+ITER_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float))
 
 
 class SpgError(RuntimeError):
@@ -66,6 +68,9 @@ def lib():
         L.spg_positions_d2h.argtypes = [vp, fp, fp]
         L.spg_flags_h2d.argtypes = [vp, C.POINTER(C.c_uint8)]
         L.spg_host_alloc.argtypes = [C.c_size_t, C.POINTER(vp)]
+        L.spg_set_iter_callback.argtypes = [vp, ITER_FN, vp, C.c_int32]
+        L.spg_eval_positions.argtypes = [vp, C.c_int32, fp, fp]
+        L.spg_set_stagnation_callback.argtypes = [vp, ITER_FN, vp]
         L.spg_host_free.argtypes = [vp]
         L.spg_grid_init.argtypes = [vp, C.c_float, C.c_int]
         L.spg_grid_info.argtypes = [vp, ip, fp, fp, fp, fp, dp]
@@ -424,6 +429,48 @@ class GpContext:
         check(lib().spg_stage_run(self.h, stage, C.byref(r)))
         return r
 
+    def set_iter_callback(self, fn, stride=1):
+        """EPlace::setIterCallback (src/gp/eplace.h:71-72): fn(stage, iter, x, y) after the
+        metrics row of every iteration with iter % stride == 0, with every node's position at
+        that iteration's evaluation point (copies). fn None turns it off."""
+        total = self.db.total_nodes
+        if fn is None or stride <= 0:
+            self._iter_cb = None
+            check(lib().spg_set_iter_callback(self.h, ITER_FN(), None, 0))
+            return
+
+        def tramp(_user, stage, it, x, y):
+            fn(int(stage), int(it), np.ctypeslib.as_array(x, (total,)).copy(),
+               np.ctypeslib.as_array(y, (total,)).copy())
+
+        self._iter_cb = ITER_FN(tramp)  # kept alive while registered
+        check(lib().spg_set_iter_callback(self.h, self._iter_cb, None, int(stride)))
+
+    def set_stagnation_callback(self, fn):
+        """fn(stage, iter, x, y) once per mGP / cGP stage, at the iteration where the stagnation
+        counter first reaches half its window (the reference's stagnation_mid diagnostic point,
+        eplace.cpp:428-433), with every node's position there. None turns it off."""
+        total = self.db.total_nodes
+        if fn is None:
+            self._mid_cb = None
+            check(lib().spg_set_stagnation_callback(self.h, ITER_FN(), None))
+            return
+
+        def tramp(_user, stage, it, x, y):
+            fn(int(stage), int(it), np.ctypeslib.as_array(x, (total,)).copy(),
+               np.ctypeslib.as_array(y, (total,)).copy())
+
+        self._mid_cb = ITER_FN(tramp)
+        check(lib().spg_set_stagnation_callback(self.h, self._mid_cb, None))
+
+    def eval_positions(self, which=0):
+        """Every node's position at the last stage's last evaluation point (which 0) or at the
+        evaluation point before it (which 1)."""
+        n = self.db.total_nodes
+        x, y = np.empty(n, np.float32), np.empty(n, np.float32)
+        check(lib().spg_eval_positions(self.h, int(which), abi.fptr(x), abi.fptr(y)))
+        return x, y
+
     def metrics(self, cap=100000):
         rows = (abi.IterMetrics * cap)()
         n = C.c_int()
@@ -440,13 +487,30 @@ class EPlace:
         self.db = db
         self.ctx = GpContext(db, params)
 
-    def run(self, stage=abi.STAGE_MGP, metrics: list | None = None) -> abi.Result:
+    def set_iter_callback(self, fn, stride=1):
+        """EPlace::setIterCallback (src/gp/eplace.h:71-72): fn(stage, iter, x, y) with every
+        node's position at the evaluation point of each iteration with iter % stride == 0."""
+        self._user_cb = (fn, stride) if fn is not None and stride > 0 else None
+        self.ctx.set_iter_callback(fn, stride)
+
+    def run(self, stage=abi.STAGE_MGP, metrics: list | None = None, diagnostics: str | None = None) -> abi.Result:
         """One stage from the PlaceDB's positions and flags. With a `metrics` list, the stage's
         per-iteration rows are appended to it as (stage name, rows), the input of
-        superplace_b200.metrics.write_metrics_csv (the reference's MetricsSink rows)."""
+        superplace_b200.metrics.write_metrics_csv (the reference's MetricsSink rows). With a
+        `diagnostics` directory (Config::gp_diagnostics with the sink's output directory), mGP
+        and cGP write the reference's GP diagnostics there (superplace_b200.diagnostics)."""
+        diag = diagnostics is not None and stage != abi.STAGE_FILLER_ONLY
+        if diag:
+            hooks = self._diagnostic_hooks(stage, diagnostics)
         self.ctx.set_positions(self.db.node_x, self.db.node_y)
         self.ctx.set_flags(self.db.node_flags)
-        r = self.ctx.run(stage)
+        try:
+            r = self.ctx.run(stage)
+        finally:
+            if diag:
+                self.ctx.set_stagnation_callback(None)
+                user = getattr(self, "_user_cb", None)
+                self.ctx.set_iter_callback(*(user if user else (None, 0)))
         if metrics is not None:
             from .metrics import STAGE_NAMES
 
@@ -457,4 +521,66 @@ class EPlace:
             self.ctx.positions(out=(x, y))
         else:
             x[:], y[:] = self.ctx.positions()
+        if diag:
+            hooks(r)
         return r
+
+    def _diagnostic_hooks(self, stage, root):
+        """Registers the first_eval and stagnation_mid points of a stage's GP diagnostics and
+        returns the writer of its last_eval and delivered points (eplace.cpp:284-288,365-369,
+        428-433,476-479,505-507)."""
+        from . import diagnostics as D
+
+        db, ctx, params = self.db, self.ctx, self.ctx.params
+        state = {}
+
+        def evaluation():
+            if "ev" not in state:
+                state["ev"] = D.Evaluation(db, params, ctx.grid_info()["dim"])
+            return state["ev"]
+
+        def point(name, it, x, y, previous, row=None, lam=None, gamma=None, step=0.0):
+            if row is not None:
+                rows = ctx.metrics(row + 1)
+                lam, gamma, step = rows["eval_lambda"][row], rows["eval_gamma"][row], rows["step_size"][row]
+            D.write_gp_diagnostic(root, stage, name, it, lam, gamma, step, db, params, ctx.grid_info()["dim"],
+                                  x, y, previous, evaluation())
+
+        def opt_positions(px, py):
+            idx = D.opt_index(db, stage)
+            return np.concatenate([px[idx], py[idx]])
+
+        user = getattr(self, "_user_cb", None)
+
+        def on_iter(st, it, x, y):
+            if it == 0:
+                point("first_eval", 0, x, y, None, row=0)
+            if user and it % user[1] == 0:
+                user[0](st, it, x, y)
+
+        def on_mid(st, it, x, y):
+            point("stagnation_mid", it, x, y, opt_positions(*ctx.eval_positions(1)), row=it)
+
+        ctx.set_iter_callback(on_iter, user[1] if user else 1 << 30)
+        ctx.set_stagnation_callback(on_mid)
+
+        def after(r):
+            try:
+                delivered = (db.node_x.copy(), db.node_y.copy())
+                if r.iterations > 0:
+                    last = r.iterations - 1
+                    lx, ly = ctx.eval_positions(0)
+                    point("last_eval", last, lx, ly, opt_positions(*ctx.eval_positions(1)), row=last)
+                    it = r.rollback_iter if r.stagnated else last
+                    rows = ctx.metrics(last + 1)
+                    point("delivered", it, delivered[0], delivered[1], opt_positions(lx, ly),
+                          lam=rows["eval_lambda"][it], gamma=rows["eval_gamma"][it])
+                elif r.converged:  # converged before any step (eplace.cpp:284-288)
+                    g = ctx.grid_info()
+                    point("delivered", -1, delivered[0], delivered[1], opt_positions(*delivered),
+                          lam=r.initial_lambda, gamma=D.compute_gamma(r.initial_overflow, g["step_x"]))
+            finally:
+                if "ev" in state:
+                    state["ev"].close()
+
+        return after
