@@ -16,6 +16,7 @@ is skipped.
 from __future__ import annotations
 
 import time
+from dataclasses import dataclass
 from typing import Callable
 
 import numpy as np
@@ -26,6 +27,23 @@ from .placedb import F_FIXED, F_MACRO, PlaceDB
 STAGES = ("parse", "init", "gp", "lg", "write")
 
 Legaliser = Callable[[PlaceDB], dict]
+
+
+@dataclass
+class FrameMark:
+    """FrameMark (src/util/metrics.h:31-37): a moment of the run worth a frame. `t` is the GP
+    iteration count accumulated over mGP, FILLERONLY and cGP (the playback clock), `iter` -1 marks
+    a stage milestone, `break_before` a jump the player must not interpolate across."""
+    stage: str
+    iter: int
+    t: float
+    break_before: bool
+    label: str
+
+
+# the frame hook: (mark, x, y) with every node's position at that moment (MetricsSink's
+# FrameHook, src/util/metrics.h:67-71; the PlaceDB itself is not updated inside a stage)
+FrameHook = Callable[[FrameMark, np.ndarray, np.ndarray], None]
 
 
 def _hpwl(db: PlaceDB) -> float:
@@ -39,18 +57,39 @@ def movable_macros(db: PlaceDB) -> np.ndarray:
 
 
 def global_place(db: PlaceDB, params: abi.Params | None = None, legalize_macros: Legaliser | None = None,
-                 metrics: list | None = None) -> dict:
+                 metrics: list | None = None, frame_hook: FrameHook | None = None, frame_stride: int = 0,
+                 diagnostics: str | None = None) -> dict:
     """GlobalPlaceStage::run (src/stages/gp_stage.cpp:59-244) on the device: fillers, mGP, then
     for designs with movable macros mLG (the caller's `legalize_macros`, which must leave every
     macro F_FIXED), fillers re-scattered with seed offset 1, FILLERONLY and cGP. The positions
     of the frozen macros are checked bit for bit after cGP (gp_stage.cpp:205-225). Returns each
     stage's result (abi.Result) and, with mLG, the legaliser's report; `stopped` says why the
-    sequence ended early."""
+    sequence ended early.
+
+    frame_hook with frame_stride > 0 gets the reference's frame marks (gp_stage.cpp:73-93,136):
+    every frame_stride-th iteration of each stage, the end of mGP and of cGP (a break when the
+    stage rolled back), and mLG. `diagnostics`: the output directory of the GP diagnostics of
+    mGP and cGP (Config::gp_diagnostics)."""
     p = params or abi.default_params()
     out: dict = {}
+    t_offset = [0.0]
+    hook = frame_hook if frame_hook is not None and frame_stride > 0 else None
     engine.initialize_fillers(db, p.target_density, p.random_seed)
     ep = engine.EPlace(db, p)
-    out["mGP"] = ep.run(abi.STAGE_MGP, metrics)
+    if hook:
+        names = {abi.STAGE_MGP: "mGP", abi.STAGE_FILLER_ONLY: "FILLERONLY", abi.STAGE_CGP: "cGP"}
+        ep.set_iter_callback(lambda st, it, x, y: hook(
+            FrameMark(names[st], it, t_offset[0] + it, False, f"{names[st]} iter {it}"), x, y), frame_stride)
+
+    def mark_end(name, r):
+        if hook:
+            label = (f"{name} end (tau stagnated, rolled back to iteration {r.rollback_iter})" if r.stagnated
+                     else f"{name} end")
+            hook(FrameMark(name, r.iterations, t_offset[0], bool(r.stagnated), label), db.node_x, db.node_y)
+
+    out["mGP"] = ep.run(abi.STAGE_MGP, metrics, diagnostics)
+    t_offset[0] = float(out["mGP"].iterations)
+    mark_end("mGP", out["mGP"])
     macros = movable_macros(db)
     if macros.size == 0:
         return out
@@ -60,10 +99,16 @@ def global_place(db: PlaceDB, params: abi.Params | None = None, legalize_macros:
     out["mLG"] = legalize_macros(db)
     if np.any((db.node_flags[macros] & F_FIXED) == 0):
         raise engine.SpgError(abi.SPG_E_STATE, "mLG left a movable macro unfixed")
+    if hook:
+        hook(FrameMark("mLG", -1, t_offset[0], True, "mLG macro legalisation (macros moved to legal sites)"),
+             db.node_x, db.node_y)
     mx, my = db.node_x[macros].copy(), db.node_y[macros].copy()
     engine.scatter_fillers(db, p.random_seed, seed_offset=1)
-    out["FILLERONLY"] = ep.run(abi.STAGE_FILLER_ONLY, metrics)
-    out["cGP"] = ep.run(abi.STAGE_CGP, metrics)
+    out["FILLERONLY"] = ep.run(abi.STAGE_FILLER_ONLY, metrics, diagnostics)
+    t_offset[0] += out["FILLERONLY"].iterations
+    out["cGP"] = ep.run(abi.STAGE_CGP, metrics, diagnostics)
+    t_offset[0] += out["cGP"].iterations
+    mark_end("cGP", out["cGP"])
     if not (np.array_equal(db.node_x[macros], mx) and np.array_equal(db.node_y[macros], my)):
         raise engine.SpgError(abi.SPG_E_STATE, "a frozen macro changed position during cGP")
     return out

@@ -99,3 +99,31 @@ def test_eval_positions_needs_a_stage():
     with pytest.raises(engine.SpgError):
         ctx.eval_positions(0)
     ctx.close()
+
+
+def test_global_place_frame_marks():
+    """GlobalPlaceStage's frame marks (gp_stage.cpp:73-93,136) through flow.global_place: every
+    frame_stride-th iteration of mGP, FILLERONLY and cGP on the accumulated clock t, the ends of
+    mGP and cGP, and the mLG jump (here a stand-in legaliser that freezes the macros in place)."""
+    from superplace_b200 import flow, generator
+    from superplace_b200.placedb import F_FIXED
+
+    db = generator.mixed_design(1002, n_cells=3000)
+
+    def freeze(d):
+        m = flow.movable_macros(d)
+        d.node_flags[m] |= F_FIXED
+        return {"macros": int(m.size)}
+
+    marks = []
+    res = flow.global_place(db, abi.default_params(gp_bin_dim=64), legalize_macros=freeze,
+                            frame_hook=lambda m, x, y: marks.append((m, x.size)), frame_stride=10)
+    n_mgp, n_fo, n_cgp = res["mGP"].iterations, res["FILLERONLY"].iterations, res["cGP"].iterations
+    want = [("mGP", i, float(i), False) for i in range(0, n_mgp, 10)]
+    want.append(("mGP", n_mgp, float(n_mgp), bool(res["mGP"].stagnated)))
+    want.append(("mLG", -1, float(n_mgp), True))
+    want += [("FILLERONLY", i, float(n_mgp + i), False) for i in range(0, n_fo, 10)]
+    want += [("cGP", i, float(n_mgp + n_fo + i), False) for i in range(0, n_cgp, 10)]
+    want.append(("cGP", n_cgp, float(n_mgp + n_fo + n_cgp), bool(res["cGP"].stagnated)))
+    assert [(m.stage, m.iter, m.t, m.break_before) for m, _ in marks] == want
+    assert all(n == db.total_nodes for _, n in marks)
