@@ -13,10 +13,13 @@
 // macro freeze, the quality band) run against the device engine.
 //
 // Differences from the CPU engine, by design of the device loop:
-//   * the per-iteration callback (setIterCallback) is called once per stage, after it, with
-//     the delivered placement: the loop runs on the device and reports its rows afterwards;
+//   * the per-iteration callback (setIterCallback) runs at every iteration with the PlaceDB's
+//     positions at that iteration's evaluation point, through the engine's iteration callback
+//     (each call pauses the device loop); the sink receives the stage's metrics rows when the
+//     stage ends, so a callback does not see them in the sink yet;
 //   * of the diagnostic GpRunOptions only freezeLambda and freezeGamma are supported; the
 //     others (noMomentum, stepScale, adaptiveRestart, gradientRestart) throw.
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <stdexcept>
@@ -148,6 +151,21 @@ GpResult EPlace::run(GpStage stage, GpRunOptions options) {
     spg_ctx* ctx = nullptr;
     check(spg_ctx_create(&v, &p, &ctx));
     std::unique_ptr<spg_ctx, int (*)(spg_ctx*)> guard(ctx, spg_ctx_destroy);
+    // the iteration callback: the evaluation point's positions written into the PlaceDB
+    struct Hook {
+        Impl* s;
+        GpStage stage;
+    } hook{&s, stage};
+    if (s.onIter) {
+        spg_iter_fn fn = [](void* user, int32_t, int32_t iter, const float* x, const float* y) {
+            Hook& h = *static_cast<Hook*>(user);
+            PlaceDB& d = h.s->db;
+            std::copy(x, x + d.totalNodes(), d.node_x.begin());
+            std::copy(y, y + d.totalNodes(), d.node_y.begin());
+            h.s->onIter(h.stage, iter, d);
+        };
+        check(spg_set_iter_callback(ctx, fn, &hook, 1));
+    }
     spg_result r{};
     check(spg_stage_run(ctx, static_cast<int>(stage), &r));
     check(spg_positions_d2h(ctx, db.node_x.data(), db.node_y.data()));
@@ -195,7 +213,6 @@ GpResult EPlace::run(GpStage stage, GpRunOptions options) {
     s.sink.setSummary(prefix + "converged", out.converged ? 1 : 0);
     s.sink.setSummary(prefix + "stagnated", out.stagnated ? 1 : 0);
     s.sink.setSummary(prefix + "rollback_iter", out.rollbackIter);
-    if (s.onIter) s.onIter(stage, std::max(out.iterations - 1, 0), db);
     return out;
 }
 
