@@ -228,8 +228,8 @@ def fp32_arm(db, workload, init_x, init_y, steps):
 # of a launch are not counted). The Poisson part is its five launches of one solve (its first
 # operand comes from the rho kernel).
 PROFILED_DRAM_BYTES = {
-    ("large", "bf16x3"): {"update": 40.70e6, "wa": 15.52e6, "rho": 6.31e6, "poisson": 13.77e6,
-                          "assemble": 44.97e6,
+    ("large", "bf16x3"): {"update": 40.15e6, "wa": 15.52e6, "rho": 6.31e6, "poisson": 13.77e6,
+                          "assemble": 44.73e6,
                           "source": "profiles/mgp_211k_bf16x3_kernels.md"},
 }
 
