@@ -376,17 +376,15 @@ struct LoopGraph;
 struct ContextStreams {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;   // WA pass 1 overlaps the density -> Poisson chain
-    cudaStream_t side2 = nullptr;  // the fillers' step beside the cells' step
     ~ContextStreams() {
         if (stream) host_wait(stream);
-        if (side2) cudaStreamDestroy(side2);
         if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
 };
 
 struct Context : ContextStreams {
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_fork2 = nullptr, ev_join2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;  // the stage loop's timing events
     spg_params prm{};
     // host copy of the db (flags and sizes change with mLG; positions live on the device)
@@ -487,13 +485,10 @@ struct Context : ContextStreams {
 
     ~Context() {
         if (side) host_wait(side);
-        if (side2) host_wait(side2);
         if (stream) host_wait(stream);
         loop_graphs.clear();
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
-        if (ev_fork2) cudaEventDestroy(ev_fork2);
-        if (ev_join2) cudaEventDestroy(ev_join2);
         if (ev_t0) cudaEventDestroy(ev_t0);
         if (ev_t1) cudaEventDestroy(ev_t1);
         if (plan) poisson_plan_destroy(*plan);
@@ -1315,25 +1310,10 @@ void enqueue_iteration(Context& c, const DevPtrs& p, cudaGraphConditionalHandle 
         const char* e = std::getenv("SPG_SPLIT_STEP");
         return !(e && e[0] == '0');
     }();
-    static const bool beside = [] {
-        const char* e = std::getenv("SPG_STEP_STREAMS");
-        return e && e[0] == '1';
-    }();
     if (split && !wa_serial() && p.filler_k0 > 0 && p.filler_k0 < p.n_opt) {
-        if (beside) {
-            // the fillers' step on a stream of its own beside the cells' step
-            SPG_CUDA(cudaEventRecord(c.ev_fork2, s));
-            SPG_CUDA(cudaStreamWaitEvent(c.side2, c.ev_fork2, 0));
-            launch_update_range(p, p.filler_k0, p.n_opt, c.side2);
-            SPG_CUDA(cudaEventRecord(c.ev_join2, c.side2));
-            launch_update_range(p, 0, p.filler_k0, s);
-            fork_wa(c, p);
-            SPG_CUDA(cudaStreamWaitEvent(s, c.ev_join2, 0));
-        } else {
-            launch_update_range(p, 0, p.filler_k0, s);
-            fork_wa(c, p);
-            launch_update_range(p, p.filler_k0, p.n_opt, s);
-        }
+        launch_update_range(p, 0, p.filler_k0, s);
+        fork_wa(c, p);
+        launch_update_range(p, p.filler_k0, p.n_opt, s);
         evaluate(c, p, -1, R_G, 1, true, true, loop_cond, true);
         return;
     }
@@ -2412,11 +2392,8 @@ int spg_ctx_create(const spg_db_view* v, const spg_params* prm, spg_ctx** out) {
     SPG_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
     SPG_CUDA(cudaStreamCreateWithPriority(&c.stream, cudaStreamNonBlocking, prio_high));
     SPG_CUDA(cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, prio_low));
-    SPG_CUDA(cudaStreamCreateWithPriority(&c.side2, cudaStreamNonBlocking, prio_high));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
     SPG_CUDA(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
-    SPG_CUDA(cudaEventCreateWithFlags(&c.ev_fork2, cudaEventDisableTiming));
-    SPG_CUDA(cudaEventCreateWithFlags(&c.ev_join2, cudaEventDisableTiming));
     SPG_CUDA(cudaEventCreate(&c.ev_t0));
     SPG_CUDA(cudaEventCreate(&c.ev_t1));
     spg::CtxScope scope(c);

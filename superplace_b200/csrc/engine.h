@@ -227,6 +227,22 @@ __device__ __forceinline__ void rasterize(const DevPtrs& p, float x, float y, fl
     const GridGeom& g = p.geom;
     const Footprint f = footprint(g, x, y, hw, hh);
     unsigned long long* map = filler ? p.filler_fix : p.node_fix;
+    if (f.bx1 - f.bx0 <= 1 && f.by1 - f.by0 <= 1) {
+        // at most 2 x 2 bins (a node no larger than a bin after smoothing): unrolled, so the
+        // bins' corners are formed once per column and row; the same contributions
+        const bool x2 = f.bx1 > f.bx0, y2 = f.by1 > f.by0;
+#pragma unroll
+        for (int a = 0; a < 2; ++a) {
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                if ((a && !x2) || (b && !y2)) continue;
+                const int bx = f.bx0 + a, by = f.by0 + b;
+                const float c = bin_contribution(g, bx, by, f, w);
+                if (c > 0.f) atomicAdd(map + static_cast<size_t>(bx) * g.dim + by, to_fixed(c, g));
+            }
+        }
+        return;
+    }
     for (int bx = f.bx0; bx <= f.bx1; ++bx) {
         unsigned long long* row = map + static_cast<size_t>(bx) * g.dim;
         for (int by = f.by0; by <= f.by1; ++by) {

@@ -663,23 +663,34 @@ __global__ void __launch_bounds__(RED_THREADS, 6) step_kernel(DevPtrs p, int k_b
             geo = fill ? p.filler_geom : p.opt_geom[k];
         }
         if (apply) {
+            // every load first (the stores below go to other vectors, so both coordinates'
+            // loads are in flight together), then the two Nesterov points, then the stores
+            float uq[2], vq[2], gq[2], lo[2], hi[2], vk[2];
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
                 const int q = c * n + k;
-                const float uq = u[q];
-                if (snap) snap[q] = uq;
-                const float lo = fill ? (c ? p.filler_lo_y : p.filler_lo_x) : p.opt_lo[q];
-                const float hi = fill ? (c ? p.filler_hi_y : p.filler_hi_x) : p.opt_hi[q];
-                nesterov_point(uq, v[q], g[q], alpha, m, lo, hi, vn[q], nu[c]);
+                uq[c] = u[q];
+                vq[c] = v[q];
+                gq[c] = g[q];
+                lo[c] = fill ? (c ? p.filler_lo_y : p.filler_lo_x) : p.opt_lo[q];
+                hi[c] = fill ? (c ? p.filler_hi_y : p.filler_hi_x) : p.opt_hi[q];
+            }
+            // the node arrays: read inside the loop only for cells (WA) and large nodes (their
+            // gather); the fillers' entries are rewritten from R_POS when the stage ends
+            const int node = (PLACE && (!fill || (meta.w & K_LARGE))) ? p.opt_idx[k] : -1;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) nesterov_point(uq[c], vq[c], gq[c], alpha, m, lo[c], hi[c], vk[c], nu[c]);
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int q = c * n + k;
+                if (snap) snap[q] = uq[c];
+                vn[q] = vk[c];
                 un[q] = nu[c];
             }
             if (!isfinite(nu[0]) || !isfinite(nu[1])) raise_error(st, SPG_E_NON_FINITE);
-            // the node arrays: read inside the loop only for cells (WA) and large nodes (their
-            // gather); the fillers' entries are rewritten from R_POS when the stage ends
-            if (PLACE && (!fill || (meta.w & K_LARGE))) {
-                const int i = p.opt_idx[k];
-                p.x[i] = nu[0];
-                p.y[i] = nu[1];
+            if (node >= 0) {
+                p.x[node] = nu[0];
+                p.y[node] = nu[1];
             }
         } else {
             nu[0] = cur[k];
