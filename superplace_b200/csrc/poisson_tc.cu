@@ -187,6 +187,17 @@ __device__ __forceinline__ uint32_t map_rank(uint32_t local_addr, uint32_t rank)
     return remote;
 }
 
+// 16-byte store into another CTA's shared memory (a shared::cluster address from mapa).
+__device__ __forceinline__ void st_dsmem4(uint32_t addr, float a, float b, float c, float d) {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
+
 // 16-byte load from another CTA's shared memory (volatile keeps it after the cluster barrier).
 __device__ __forceinline__ float4 ld_dsmem4(uint32_t addr) {
     float4 v;
@@ -194,6 +205,36 @@ __device__ __forceinline__ float4 ld_dsmem4(uint32_t addr) {
                  : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
                  : "r"(addr));
     return v;
+}
+
+// The epilogue of four reduced outputs at (m, n..n+3) of grid z: the spectral scale (sc) or,
+// on row 0 with row0 set, the exact DC row held in sc; then an FP32 store or the split store of
+// the next contraction's BF16 hi/lo planes.
+__device__ __forceinline__ void tile_store(const TcArgs& g, int m, int n, int z, float4 sc, float* v) {
+    if (m == 0 && g.row0) {  // the DC row: the exact sums (times the scale), in sc
+        v[0] = sc.x;
+        v[1] = sc.y;
+        v[2] = sc.z;
+        v[3] = sc.w;
+    } else if (g.scale) {
+        v[0] *= sc.x;
+        v[1] *= sc.y;
+        v[2] *= sc.z;
+        v[3] *= sc.w;
+    }
+    if (g.mode == TC_F32) {
+        float* dst = (g.m_alt > 0 && m >= g.m_alt) ? g.out3 + z * g.out_z + (m - g.m_alt) * g.ldc
+                     : (m < g.split) ? g.out + z * g.out_z + m * g.ldc
+                                     : g.out2 + z * g.out_z + (m - g.split) * g.ldc;
+        *reinterpret_cast<float4*>(dst + n) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        uint16_t h[4], l[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) split_bf16(v[i], h[i], l[i]);
+        uint16_t* hi = g.planes + z * g.plane_z + m * g.ldc + n;
+        *reinterpret_cast<uint2*>(hi) = *reinterpret_cast<const uint2*>(h);
+        *reinterpret_cast<uint2*>(hi + g.plane_stride) = *reinterpret_cast<const uint2*>(l);
+    }
 }
 
 // Per-CTA pipeline state, carried across the tiles one CTA computes: a standalone GEMM launch
@@ -256,7 +297,16 @@ __device__ __forceinline__ void tile_teardown(const TileState& t) {
 // threads on consecutive columns (coalesced stores). All threads of the CTA call it. With
 // active = false (a CTA without a tile in this round) or after an earlier failure (*g.err set)
 // the CTA streams and writes nothing but still takes the tile's cluster barriers.
-template <int BN, int STAGES, int S>
+//
+// PUSH (a CTA that computes one tile in its launch, S > 1): instead of staging its partial in
+// its own ring for the others to pull, each CTA stores the rows that CTA r reduces straight
+// into r's receive area (past the ring and its barriers, so a store cannot land on a ring the
+// MMAs still read), slot = the sender's rank; one cluster barrier makes them visible and each
+// CTA sums its S slots locally in rank order: the same sums as the pull form, with one cluster
+// barrier fewer and local instead of remote loads. The caller has arrived on the cluster barrier
+// once after tile_setup (cluster_arrive_relaxed), so every CTA of the cluster is running before
+// the first remote store.
+template <int BN, int STAGES, int S, bool PUSH = false>
 __device__ __forceinline__ void gemm_tile(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& g, int m0,
                                           int n0, int z, int rank, int group0, bool active, TileState& t) {
     constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;  // one plane
@@ -338,6 +388,57 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap& tmA, const CUtensor
         }
     }
 
+    static_assert(!PUSH || S > 1, "the push form reduces over S > 1 partials");
+    // the receive area of the push form: S slots of R rows at RED_LD floats
+    float* recv = reinterpret_cast<float*>(t.base + STAGES * STAGE_BYTES + 256);
+    if (PUSH) {
+        bool acc_ok = false;
+        if (run) {
+            acc_ok = __all_sync(0xffffffffu, mbar_wait(t.accb, t.acc_n & 1) ? 1 : 0) != 0;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        }
+        cluster_wait();  // every CTA of the cluster has started (arrived after its set-up)
+        if (run && acc_ok) {
+            const int r = 32 * warp + lane;  // this thread's tile row
+            const int dst = r / R, rr = r % R;
+            const uint32_t remote = map_rank(smem_u32(recv + (rank * R + rr) * RED_LD), static_cast<uint32_t>(group0 + dst));
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 32) {
+                float v[32];
+                tmem_ld32(t.tmem + (static_cast<uint32_t>(32 * warp) << 16) + c, v);
+#pragma unroll
+                for (int i = 0; i < 32; i += 4) st_dsmem4(remote + 4u * static_cast<uint32_t>(c + i), v[i], v[i + 1], v[i + 2], v[i + 3]);
+            }
+        } else if (run && threadIdx.x == 0) {
+            atomicCAS(g.err, 0, SPG_E_CUDA);
+        }
+        const int ok_cta = __syncthreads_and(!run || acc_ok ? 1 : 0);
+        cluster_sync_all();  // every CTA's rows are in their reducers' slots
+        if (run && ok_cta) {
+#pragma unroll
+            for (int j = 0; j < GPT; ++j) {
+                const int rr = grow[j] - rank * R;
+                float v[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+                for (int q = 0; q < S; ++q) {
+                    const float4 a = *reinterpret_cast<const float4*>(recv + (q * R + rr) * RED_LD + gcol[j]);
+                    v[0] += a.x;
+                    v[1] += a.y;
+                    v[2] += a.z;
+                    v[3] += a.w;
+                }
+                tile_store(g, m0 + grow[j], n0 + gcol[j], z, sc[j], v);
+            }
+        }
+        if (run) {
+            t.it += static_cast<uint32_t>(s1 - s0);
+            t.acc_n += 1;
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        return;
+    }
+
     // stage this CTA's partial tile (TMEM lane = tile row; warp w owns rows 32w..32w+31)
     bool acc_ok = false;
     if (run) {
@@ -380,31 +481,7 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap& tmA, const CUtensor
                 v[2] += parts[j][q].z;
                 v[3] += parts[j][q].w;
             }
-            const int m = m0 + grow[j], n = n0 + gcol[j];
-            if (m == 0 && g.row0) {  // the DC row: the exact sums (times the scale), in sc
-                v[0] = sc[j].x;
-                v[1] = sc[j].y;
-                v[2] = sc[j].z;
-                v[3] = sc[j].w;
-            } else if (g.scale) {
-                v[0] *= sc[j].x;
-                v[1] *= sc[j].y;
-                v[2] *= sc[j].z;
-                v[3] *= sc[j].w;
-            }
-            if (g.mode == TC_F32) {
-                float* dst = (g.m_alt > 0 && m >= g.m_alt) ? g.out3 + z * g.out_z + (m - g.m_alt) * g.ldc
-                             : (m < g.split) ? g.out + z * g.out_z + m * g.ldc
-                                             : g.out2 + z * g.out_z + (m - g.split) * g.ldc;
-                *reinterpret_cast<float4*>(dst + n) = make_float4(v[0], v[1], v[2], v[3]);
-            } else {
-                uint16_t h[4], l[4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) split_bf16(v[i], h[i], l[i]);
-                uint16_t* hi = g.planes + z * g.plane_z + m * g.ldc + n;
-                *reinterpret_cast<uint2*>(hi) = *reinterpret_cast<const uint2*>(h);
-                *reinterpret_cast<uint2*>(hi + g.plane_stride) = *reinterpret_cast<const uint2*>(l);
-            }
+            tile_store(g, m0 + grow[j], n0 + gcol[j], z, sc[j], v);
         }
     }
     if (S > 1) cluster_sync_all();  // no CTA reuses its ring while another may still read it
@@ -419,20 +496,22 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap& tmA, const CUtensor
 
 // Grid (S, N/BN, (M/128) * batch), cluster (S, 1, 1): the S CTAs of a cluster share one
 // 128 x BN output tile and split its K/64 K slabs evenly (split-K), one tile per CTA.
-template <int BN, int STAGES, int S>
+// PUSH: the partials are reduced in the push form (gemm_tile).
+template <int BN, int STAGES, int S, bool PUSH = false>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                    const TcArgs g) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     TileState t;
     tile_setup<BN, STAGES>(smem_raw, t);
+    if (PUSH) cluster_arrive_relaxed();  // waited for before the first store into a peer
     // everything above touched only this CTA's shared memory and TMEM: wait for the kernel
     // that produced the operands only now
     pdl_wait();
     pdl_trigger();
     const int tiles_m = g.M / TC_BM;
-    gemm_tile<BN, STAGES, S>(tmA, tmB, g, (blockIdx.z % tiles_m) * TC_BM, blockIdx.y * BN, blockIdx.z / tiles_m,
-                             blockIdx.x, 0, true, t);
+    gemm_tile<BN, STAGES, S, PUSH>(tmA, tmB, g, (blockIdx.z % tiles_m) * TC_BM, blockIdx.y * BN,
+                                   blockIdx.z / tiles_m, blockIdx.x, 0, true, t);
     tile_teardown<BN>(t);
 }
 
@@ -663,6 +742,22 @@ constexpr size_t tc_smem_bytes() {
     return 1024 + TC_STAGES * 2 * (TC_BM * TC_BK * 2 + TC_BN * TC_BK * 2) + (2 * TC_STAGES + 1) * 8 + 128;
 }
 static_assert(tc_smem_bytes() <= 227 * 1024, "ring exceeds the shared memory of one CTA");
+// The push form's launches (S > 1): each CTA streams at most K/64/2 slabs, so a 3-deep ring,
+// then 256 bytes of barriers and the receive area of S slots x (128/S) rows x (TC_BN + 4) floats.
+constexpr int TC_PUSH_STAGES = 3;
+constexpr size_t tc_push_smem_bytes() {
+    return 1024 + TC_PUSH_STAGES * 2 * (TC_BM * TC_BK * 2 + TC_BN * TC_BK * 2) + 256 + TC_BM * (TC_BN + 4) * 4;
+}
+static_assert(tc_push_smem_bytes() <= 227 * 1024, "push form exceeds the shared memory of one CTA");
+
+// SPG_TC_PUSH=0: the pull form for every launch (the receive area unused).
+bool tc_push() {
+    static const bool on = [] {
+        const char* e = std::getenv("SPG_TC_PUSH");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 struct TcState {
     // tensor maps: bases (A operands) and data planes (B operands)
@@ -690,9 +785,10 @@ void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int 
                 "tensor-core GEMM dims must be tile multiples");
     const int S = pick_splits(grid_tiles, g.K / TC_BK);
     cudaLaunchConfig_t cfg = {};
+    const bool push = S > 1 && tc_push();
     cfg.gridDim = dim3(S, g.N / TC_BN, (g.M / TC_BM) * batch);
     cfg.blockDim = dim3(TC_THREADS);
-    cfg.dynamicSmemBytes = tc_smem_bytes();
+    cfg.dynamicSmemBytes = push ? tc_push_smem_bytes() : tc_smem_bytes();
     cfg.stream = s;
     cudaLaunchAttribute attr[3];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -706,9 +802,18 @@ void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int 
     cfg.attrs = attr;
     cfg.numAttrs = 3;
     switch (S) {
-        case 8: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 8>, a, b, g)); break;
-        case 4: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 4>, a, b, g)); break;
-        case 2: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 2>, a, b, g)); break;
+        case 8:
+            if (push) SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_PUSH_STAGES, 8, true>, a, b, g));
+            else SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 8>, a, b, g));
+            break;
+        case 4:
+            if (push) SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_PUSH_STAGES, 4, true>, a, b, g));
+            else SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 4>, a, b, g));
+            break;
+        case 2:
+            if (push) SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_PUSH_STAGES, 2, true>, a, b, g));
+            else SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 2>, a, b, g));
+            break;
         default: SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_BN, TC_STAGES, 1>, a, b, g)); break;
     }
     count_launch();
@@ -836,6 +941,13 @@ void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::ve
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPG_CUDA(cudaFuncSetAttribute(tc_fused_kernel<TC_BN, TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    const int push_bytes = static_cast<int>(tc_push_smem_bytes());
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_PUSH_STAGES, 2, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes));
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_PUSH_STAGES, 4, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes));
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_PUSH_STAGES, 8, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes));
 }
 
 void tc_plan_refill_sines(PoissonPlan& pl, const std::vector<float>& sy_rows, const std::vector<float>& sx_rows) {
