@@ -207,6 +207,18 @@ __device__ __forceinline__ float4 ld_dsmem4(uint32_t addr) {
     return v;
 }
 
+// The epilogue's factors for the outputs at (m, n..n+3) of grid z: the spectral scale, and on
+// row 0 with row0 set the exact DC row times it (ones when the CTA does not run).
+__device__ __forceinline__ float4 epi_scale(const TcArgs& g, int m, int n, int z, bool run) {
+    float4 sc = make_float4(1.f, 1.f, 1.f, 1.f);
+    if (run && g.scale) sc = __ldg(reinterpret_cast<const float4*>(g.scale + m * g.lds + n));
+    if (run && m == 0 && g.row0) {
+        const float4 r0 = __ldg(reinterpret_cast<const float4*>(g.row0 + z * g.row0_z + n));
+        sc = make_float4(r0.x * sc.x, r0.y * sc.y, r0.z * sc.z, r0.w * sc.w);
+    }
+    return sc;
+}
+
 // The epilogue of four reduced outputs at (m, n..n+3) of grid z: the spectral scale (sc) or,
 // on row 0 with row0 set, the exact DC row held in sc; then an FP32 store or the split store of
 // the next contraction's BF16 hi/lo planes.
@@ -371,20 +383,20 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap& tmA, const CUtensor
     __syncwarp();
 
     // epilogue inputs that do not depend on the partials, fetched while the MMAs run: this
-    // thread's output groups (row, 4 columns), the spectral scale and the exact DC row
-    int grow[GPT], gcol[GPT];
-    float4 sc[GPT];
+    // thread's output groups (row, 4 columns), the spectral scale and the exact DC row. A
+    // 128 x 128 tile reduced by one CTA (BIG: 32 groups per thread) forms them group by group
+    // in its epilogue instead, to stay within its registers.
+    constexpr bool BIG = GPT > 16;
+    static_assert(!BIG || (S == 1 && !PUSH), "a 128-wide tile is reduced by its own CTA");
+    int grow[BIG ? 1 : GPT], gcol[BIG ? 1 : GPT];
+    float4 sc[BIG ? 1 : GPT];
+    if constexpr (!BIG) {
 #pragma unroll
-    for (int j = 0; j < GPT; ++j) {
-        const int e = threadIdx.x + j * TC_THREADS;
-        grow[j] = rank * R + e / (BN / 4);
-        gcol[j] = (e % (BN / 4)) * 4;
-        const int m = m0 + grow[j], n = n0 + gcol[j];
-        sc[j] = make_float4(1.f, 1.f, 1.f, 1.f);
-        if (run && g.scale) sc[j] = __ldg(reinterpret_cast<const float4*>(g.scale + m * g.lds + n));
-        if (run && m == 0 && g.row0) {
-            const float4 r0 = __ldg(reinterpret_cast<const float4*>(g.row0 + z * g.row0_z + n));
-            sc[j] = make_float4(r0.x * sc[j].x, r0.y * sc[j].y, r0.z * sc[j].z, r0.w * sc[j].w);
+        for (int j = 0; j < GPT; ++j) {
+            const int e = threadIdx.x + j * TC_THREADS;
+            grow[j] = rank * R + e / (BN / 4);
+            gcol[j] = (e % (BN / 4)) * 4;
+            sc[j] = epi_scale(g, m0 + grow[j], n0 + gcol[j], z, run);
         }
     }
 
@@ -460,7 +472,22 @@ __device__ __forceinline__ void gemm_tile(const CUtensorMap& tmA, const CUtensor
     }
     const int ok_cta = __syncthreads_and(acc_ok ? 1 : 0);
     if (S > 1) cluster_sync_all();  // every CTA of the cluster has staged its partial
-    if (ok_cta) {
+    if constexpr (BIG) {
+        if (ok_cta) {
+#pragma unroll 4
+            for (int j = 0; j < GPT; ++j) {
+                const int e = threadIdx.x + j * TC_THREADS;
+                const int row = e / (BN / 4), col = (e % (BN / 4)) * 4;
+                const float4 a = *reinterpret_cast<const float4*>(red + row * RED_LD + col);
+                float v[4] = {0.f, 0.f, 0.f, 0.f};  // the sum of the one partial, as below
+                v[0] += a.x;
+                v[1] += a.y;
+                v[2] += a.z;
+                v[3] += a.w;
+                tile_store(g, m0 + row, n0 + col, z, epi_scale(g, m0 + row, n0 + col, z, run), v);
+            }
+        }
+    } else if (ok_cta) {
         const uint32_t red_addr = smem_u32(red);
         float4 parts[GPT][S];
 #pragma unroll
@@ -750,6 +777,25 @@ constexpr size_t tc_push_smem_bytes() {
 }
 static_assert(tc_push_smem_bytes() <= 227 * 1024, "push form exceeds the shared memory of one CTA");
 
+// Wide launches: 128 x 128 tiles, one CTA each (no split-K), for contractions whose one grid
+// has at least a full wave of them (2048^2 grids, and G4 from 1024^2): each K slab then brings
+// 64 KB for twice the MMAs of a 128 x 64 tile's 48 KB, where the L2 -> shared-memory fill
+// bounds the large grids. Chosen from one grid's problem, so a grid's result does not depend
+// on the batch it is solved in. SPG_TC_WIDE=0 keeps 64-wide tiles everywhere.
+constexpr int TC_WIDE_BN = 128;
+constexpr int TC_WIDE_STAGES = 3;
+constexpr size_t tc_wide_smem_bytes() {
+    return 1024 + TC_WIDE_STAGES * 2 * (TC_BM * TC_BK * 2 + TC_WIDE_BN * TC_BK * 2) + (2 * TC_WIDE_STAGES + 1) * 8 + 128;
+}
+static_assert(tc_wide_smem_bytes() <= 227 * 1024, "wide ring exceeds the shared memory of one CTA");
+bool tc_wide() {
+    static const bool on = [] {
+        const char* e = std::getenv("SPG_TC_WIDE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 // SPG_TC_PUSH=0: the pull form for every launch (the receive area unused).
 bool tc_push() {
     static const bool on = [] {
@@ -763,6 +809,7 @@ struct TcState {
     // tensor maps: bases (A operands) and data planes (B operands)
     CUtensorMap cy, cx, bcat, acat;         // A: box rows 128
     CUtensorMap rho_b, t0t_b, p_b, t12t_b;  // B: box rows TC_BN
+    CUtensorMap rho_w, t0t_w, p_w, t12t_w;  // B: box rows TC_WIDE_BN (the wide launches)
     float* t0t32 = nullptr;                 // FP32 T0t (G1 output, before its DC split)
     float* sums = nullptr;                  // DC row sums (rho rows, T0t rows per grid)
     int* err = nullptr;
@@ -779,10 +826,27 @@ int pick_splits(int tiles, int slabs) {
     return 1;
 }
 
-void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const TcArgs& g, int batch, int grid_tiles,
-               cudaStream_t s) {
+void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& b_wide, const TcArgs& g, int batch,
+               int grid_tiles, cudaStream_t s) {
     SPG_REQUIRE(g.M % TC_BM == 0 && g.N % TC_BN == 0 && g.K % TC_BK == 0, SPG_E_INVALID,
                 "tensor-core GEMM dims must be tile multiples");
+    if (tc_wide() && g.N % TC_WIDE_BN == 0 && grid_tiles / 2 >= 148) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(1, g.N / TC_WIDE_BN, (g.M / TC_BM) * batch);
+        cfg.blockDim = dim3(TC_THREADS);
+        cfg.dynamicSmemBytes = tc_wide_smem_bytes();
+        cfg.stream = s;
+        cudaLaunchAttribute attr[2];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+        attr[1].id = cudaLaunchAttributePriority;
+        attr[1].val.priority = launch_priority(true);
+        cfg.attrs = attr;
+        cfg.numAttrs = 2;
+        SPG_CUDA(cudaLaunchKernelEx(&cfg, tc_gemm_kernel<TC_WIDE_BN, TC_WIDE_STAGES, 1>, a, b_wide, g));
+        count_launch();
+        return;
+    }
     const int S = pick_splits(grid_tiles, g.K / TC_BK);
     cudaLaunchConfig_t cfg = {};
     const bool push = S > 1 && tc_push();
@@ -934,6 +998,10 @@ void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::ve
     st->t0t_b = make_map(pl.t0t_s, 2 * Y, B * X, TC_BN);
     st->p_b = make_map(pl.p_s, 2 * B * X, Y, TC_BN);
     st->t12t_b = make_map(pl.t12t_s, 4 * Y, B * X, TC_BN);
+    st->rho_w = make_map(pl.rho_s, 2 * B * X, Y, TC_WIDE_BN);
+    st->t0t_w = make_map(pl.t0t_s, 2 * Y, B * X, TC_WIDE_BN);
+    st->p_w = make_map(pl.p_s, 2 * B * X, Y, TC_WIDE_BN);
+    st->t12t_w = make_map(pl.t12t_s, 4 * Y, B * X, TC_WIDE_BN);
     // per device (the attribute is a property of the kernel on the current device)
     const int bytes = static_cast<int>(tc_smem_bytes());
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
@@ -941,6 +1009,8 @@ void tc_plan_create(PoissonPlan& pl, const std::vector<float>& cy, const std::ve
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_STAGES, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     SPG_CUDA(cudaFuncSetAttribute(tc_fused_kernel<TC_BN, TC_STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_WIDE_BN, TC_WIDE_STAGES, 1>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tc_wide_smem_bytes())));
     const int push_bytes = static_cast<int>(tc_push_smem_bytes());
     SPG_CUDA(cudaFuncSetAttribute(tc_gemm_kernel<TC_BN, TC_PUSH_STAGES, 2, true>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes));
@@ -1066,11 +1136,11 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
         launch_fused(mp, fa, s);
         return;
     }
-    launch_tc(st->cy, st->rho_b, g1, 1, tiles[0], s);
+    launch_tc(st->cy, st->rho_b, st->rho_w, g1, 1, tiles[0], s);
     prep_split(st->t0t32, Y, static_cast<int>(BX), BXc, X, 1, pl.t0t_s, static_cast<int64_t>(Y) * BXc, sum_t, s);
-    launch_tc(st->cx, st->t0t_b, g2, batch, tiles[1], s);
-    launch_tc(st->bcat, st->p_b, g3, 1, tiles[2], s);
-    launch_tc(st->acat, st->t12t_b, g4, batch, tiles[3], s);
+    launch_tc(st->cx, st->t0t_b, st->t0t_w, g2, batch, tiles[1], s);
+    launch_tc(st->bcat, st->p_b, st->p_w, g3, 1, tiles[2], s);
+    launch_tc(st->acat, st->t12t_b, st->t12t_w, g4, batch, tiles[3], s);
 }
 
 }  // namespace spg

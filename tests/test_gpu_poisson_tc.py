@@ -17,8 +17,11 @@ from .test_gpu_parity import gaussians, rel_err
 pytestmark = pytest.mark.gpu
 
 BF16X3_TOL = 3e-5
+# the split-BF16 error grows with the contraction length (every output sums n terms, each with
+# the dropped lo*lo term and the planes' rounding): at 2048 the bar is 5e-5 of max|ref|
+BF16X3_TOL_2048 = 5e-5
 TC_GRIDS = [(128, 128, 2.5, 2.5), (512, 512, 20.88, 20.86), (1024, 1024, 10.44, 10.43),
-            (256, 512, 3.0, 1.7), (512, 256, 1.7, 3.0)]
+            (256, 512, 3.0, 1.7), (512, 256, 1.7, 3.0), (2048, 2048, 5.22, 5.21)]
 
 
 @pytest.mark.parametrize("nx,ny,sx,sy", TC_GRIDS)
@@ -31,7 +34,7 @@ def test_poisson_bf16x3_parity(nx, ny, sx, sy):
         want = orc.poisson_f64(rho, sx, sy)
         errs = [rel_err(w, g) for g, w in zip(got, want)]
         print(f"bf16x3 {nx}x{ny}: phi {errs[0]:.2e} xi_x {errs[1]:.2e} xi_y {errs[2]:.2e}")
-        assert max(errs) < BF16X3_TOL
+        assert max(errs) < (BF16X3_TOL_2048 if max(nx, ny) >= 2048 else BF16X3_TOL)
         again = be.solve(rho.copy())
         for g, h in zip(got, again):
             assert np.array_equal(g, h)
@@ -55,6 +58,27 @@ def test_poisson_bf16x3_batched_matches_single():
     n, b = 256, 3
     be = engine.PoissonBackend(n, n, 3.0, 3.0, abi.POISSON_BF16X3, batch=b)
     rng = np.random.default_rng(3)
+    rho = rng.random((b, n, n), dtype=np.float32)
+    d_rho = torch.from_numpy(rho).cuda()
+    outs = [torch.empty_like(d_rho) for _ in range(3)]
+    s = torch.cuda.current_stream().cuda_stream
+    be.solve_device(d_rho.data_ptr(), *(o.data_ptr() for o in outs), stream=s, batch=b)
+    torch.cuda.synchronize()
+    for i in range(b):
+        single = be.solve(rho[i])
+        for o, sgl in zip(outs, single):
+            assert np.array_equal(o[i].cpu().numpy(), sgl)
+
+
+def test_poisson_bf16x3_wide_batched_matches_single():
+    """2048 x 2048 grids run every contraction as 128 x 128 tiles (a full wave per grid): the
+    choice follows one grid's problem, so a batch of two gives each grid the bits it gets
+    alone."""
+    import torch
+
+    n, b = 2048, 2
+    be = engine.PoissonBackend(n, n, 5.2, 5.2, abi.POISSON_BF16X3, batch=b)
+    rng = np.random.default_rng(5)
     rho = rng.random((b, n, n), dtype=np.float32)
     d_rho = torch.from_numpy(rho).cuda()
     outs = [torch.empty_like(d_rho) for _ in range(3)]
