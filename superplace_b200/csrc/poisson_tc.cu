@@ -29,7 +29,9 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <mutex>
 #include <cstring>
@@ -814,6 +816,7 @@ struct TcState {
     float* sums = nullptr;                  // DC row sums (rho rows, T0t rows per grid)
     int* err = nullptr;
     unsigned int* bar = nullptr;            // the fused solve's grid barrier counter
+    int8_t wide[4] = {-1, -1, -1, -1};      // G1..G4 as wide tiles (tc_tune); -1 not chosen yet
 };
 
 // Split-K factor: the largest S in {8, 4, 2} (S divides the 128 tile rows, which the
@@ -826,11 +829,16 @@ int pick_splits(int tiles, int slabs) {
     return 1;
 }
 
+// Whether contraction g may run as wide tiles, and whether its one grid (grid_tiles 64-wide
+// tiles) has the full wave of them that makes the wide form the default.
+bool wide_valid(const TcArgs& g) { return tc_wide() && g.N % TC_WIDE_BN == 0 && g.M % TC_BM == 0; }
+bool wide_default(const TcArgs& g, int grid_tiles) { return wide_valid(g) && grid_tiles / 2 >= 148; }
+
 void launch_tc(const CUtensorMap& a, const CUtensorMap& b, const CUtensorMap& b_wide, const TcArgs& g, int batch,
-               int grid_tiles, cudaStream_t s) {
+               int grid_tiles, bool wide, cudaStream_t s) {
     SPG_REQUIRE(g.M % TC_BM == 0 && g.N % TC_BN == 0 && g.K % TC_BK == 0, SPG_E_INVALID,
                 "tensor-core GEMM dims must be tile multiples");
-    if (tc_wide() && g.N % TC_WIDE_BN == 0 && grid_tiles / 2 >= 148) {
+    if (wide && wide_valid(g)) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(1, g.N / TC_WIDE_BN, (g.M / TC_BM) * batch);
         cfg.blockDim = dim3(TC_THREADS);
@@ -1062,6 +1070,62 @@ bool tc_rho_operand(const PoissonPlan& pl, RhoOperand* out) {
     return true;
 }
 
+// The tile-shape tuner. For each contraction whose tiles may be either 128 x 64 or 128 x 128,
+// both with one CTA per tile (pick_splits gives no split-K), it times both on the plan's buffers
+// (3 launches each after one warm-up, CUDA events on the solve's stream) and keeps the faster;
+// the choices are kept per device, grid and batch size for the process, so later plans of the
+// same shape skip the measurement. Both forms add the same products in the same order for every
+// output, so the choice changes the time of a solve, never its bits. A solve enqueued while its
+// stream is being captured (a CUDA graph) takes the default choice (wide_default) instead, and
+// so does every solve with SPG_TC_TUNE=0.
+void tc_tune(TcState* st, const CUtensorMap* const maps[4][3], const TcArgs* const gs[4], const int batches[4],
+             const int tiles[4], cudaStream_t s) {
+    int dev = 0;
+    SPG_CUDA(cudaGetDevice(&dev));
+    const std::array<int64_t, 6> key = {dev, gs[0]->M, gs[1]->M, gs[0]->N, gs[1]->N, batches[1]};
+    static std::mutex mu;
+    static std::vector<std::pair<std::array<int64_t, 6>, std::array<int8_t, 4>>> known;
+    std::lock_guard<std::mutex> lock(mu);
+    for (const auto& k : known)
+        if (k.first == key) {
+            for (int i = 0; i < 4; ++i) st->wide[i] = k.second[i];
+            return;
+        }
+    for (int i = 0; i < 4; ++i) st->wide[i] = wide_default(*gs[i], tiles[i]) ? 1 : 0;
+    const char* e = std::getenv("SPG_TC_TUNE");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    SPG_CUDA(cudaStreamIsCapturing(s, &cap));
+    if ((e && e[0] == '0') || cap != cudaStreamCaptureStatusNone) return;  // defaults, not kept
+    cudaEvent_t e0, e1;
+    SPG_CUDA(cudaEventCreate(&e0));
+    SPG_CUDA(cudaEventCreate(&e1));
+    std::array<int8_t, 4> pick{};
+    for (int i = 0; i < 4; ++i) {
+        pick[i] = st->wide[i];
+        // only where the 64-wide form splits no K either, so both add the same products in order
+        if (!wide_valid(*gs[i]) || pick_splits(tiles[i], gs[i]->K / TC_BK) != 1) continue;
+        float ms[2] = {0.f, 0.f};
+        for (int w = 0; w < 2; ++w) {
+            launch_tc(*maps[i][0], *maps[i][1], *maps[i][2], *gs[i], batches[i], tiles[i], w != 0, s);
+            SPG_CUDA(cudaEventRecord(e0, s));
+            for (int r = 0; r < 3; ++r)
+                launch_tc(*maps[i][0], *maps[i][1], *maps[i][2], *gs[i], batches[i], tiles[i], w != 0, s);
+            SPG_CUDA(cudaEventRecord(e1, s));
+            SPG_CUDA(cudaEventSynchronize(e1));
+            SPG_CUDA(cudaEventElapsedTime(&ms[w], e0, e1));
+        }
+        pick[i] = ms[1] < ms[0] ? 1 : 0;
+        st->wide[i] = pick[i];
+        if (const char* log = std::getenv("SPG_TC_TUNE_LOG"); log && log[0] == '1')
+            std::fprintf(stderr, "[spg tc tune] G%d %dx%dx%d batch %d: 64-wide %.1f us, 128-wide %.1f us -> %s\n", i + 1,
+                         gs[i]->M, gs[i]->N, gs[i]->K, batches[i], 1e3 * ms[0] / 3, 1e3 * ms[1] / 3,
+                         pick[i] ? "128-wide" : "64-wide");
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    known.emplace_back(key, pick);
+}
+
 void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* ex, float* ey,
               cudaStream_t s, bool rho_split_ready) {
     auto* st = static_cast<TcState*>(pl.tc);
@@ -1136,11 +1200,16 @@ void tc_solve(PoissonPlan& pl, int batch, const float* rho, float* phi, float* e
         launch_fused(mp, fa, s);
         return;
     }
-    launch_tc(st->cy, st->rho_b, st->rho_w, g1, 1, tiles[0], s);
+    const CUtensorMap* maps[4][3] = {{&st->cy, &st->rho_b, &st->rho_w}, {&st->cx, &st->t0t_b, &st->t0t_w},
+                                     {&st->bcat, &st->p_b, &st->p_w}, {&st->acat, &st->t12t_b, &st->t12t_w}};
+    const TcArgs* gs[4] = {&g1, &g2, &g3, &g4};
+    const int batches[4] = {1, batch, 1, batch};
+    if (st->wide[0] < 0) tc_tune(st, maps, gs, batches, tiles, s);
+    launch_tc(st->cy, st->rho_b, st->rho_w, g1, 1, tiles[0], st->wide[0] > 0, s);
     prep_split(st->t0t32, Y, static_cast<int>(BX), BXc, X, 1, pl.t0t_s, static_cast<int64_t>(Y) * BXc, sum_t, s);
-    launch_tc(st->cx, st->t0t_b, st->t0t_w, g2, batch, tiles[1], s);
-    launch_tc(st->bcat, st->p_b, st->p_w, g3, 1, tiles[2], s);
-    launch_tc(st->acat, st->t12t_b, st->t12t_w, g4, batch, tiles[3], s);
+    launch_tc(st->cx, st->t0t_b, st->t0t_w, g2, batch, tiles[1], st->wide[1] > 0, s);
+    launch_tc(st->bcat, st->p_b, st->p_w, g3, 1, tiles[2], st->wide[2] > 0, s);
+    launch_tc(st->acat, st->t12t_b, st->t12t_w, g4, batch, tiles[3], st->wide[3] > 0, s);
 }
 
 }  // namespace spg
