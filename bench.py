@@ -372,7 +372,9 @@ def run_ours(args):
         parts = ep.ctx.profile(reps=20)
         traffic = PROFILED_DRAM_BYTES.get((args.workload, args.precision), {})
         kern = part_rooflines(parts, db, dim, hbm, bf16, precision, traffic)
-        dom = max((k for k in kern if k != "evaluation"), key=lambda k: kern[k]["us"])
+        # the dominant kernel: the longest part of the iteration's critical chain (WA runs on the
+        # side stream beside the fillers' step, so it is listed under `kernels` but not chosen)
+        dom = max((k for k in kern if k not in ("evaluation", "wa")), key=lambda k: kern[k]["us"])
         d = kern[dom]
         total = db.total_nodes
         h2d = 2 * 4 * total + total  # positions x, y and flags
