@@ -757,8 +757,38 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         rlx[t] = c.row_lx[r];
         rhx[t] = c.row_lx[r] + c.row_step[r] * static_cast<float>(c.row_sites[r]);
     }
-    // bin rows are independent: four threads take every fourth one (after their terminal part)
-    run_parts(4, [&](int part) {
+    // footprint data (half extents after local smoothing, charge weight, kernel class) is
+    // written on the device by footprint_kernel; the host keeps the fixed-point bound, the
+    // large nodes (only nodes at least a bin wide or tall can be) and the small-node count
+    std::vector<int>& dlarge = c.dens_large_h;
+    dlarge.clear();
+    // bound partials: node i adds into acc[i % 4], in ascending i; thread t owns partial t (the
+    // same sums in the same order as one pass), its large nodes and its small-node count
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    int small_t[4] = {0, 0, 0, 0};
+    std::vector<int> large_t[4];
+    auto footprint_part = [&](int t) {
+        double a = 0.0;
+        int ns = 0;
+        std::vector<int>& lg = large_t[t];
+        for (int i = t; i < c.total; i += 4) {
+            if (c.fixed(i) || c.ni(i)) continue;
+            const float w = c.w[i], h = c.h[i];
+            a += static_cast<double>(w) * static_cast<double>(h);
+            const bool large = !(w < g.step_x && h < g.step_y) && (node_footprint(c, g, target, i).kind & K_LARGE);
+            if (large) lg.push_back(i);
+            else ++ns;
+        }
+        acc[t] = a;
+        small_t[t] = ns;
+    };
+    // eight threads: 0-3 the statics (each its terminal columns, then every fourth bin row of
+    // the base map; bin rows are independent), 4-7 the footprint scan's four partials
+    run_parts(8, [&](int part) {
+    if (part >= 4) {
+        footprint_part(part - 4);
+        return;
+    }
     terminal_part(part);
     for (int by = part; by < dim; by += 4) {
         const float bly = g.origin_y + by * g.step_y;
@@ -782,33 +812,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         }
     }
     });
-
-    ht.mark("statics");
-    // footprint data (half extents after local smoothing, charge weight, kernel class) is
-    // written on the device by footprint_kernel; the host keeps the fixed-point bound, the
-    // large nodes (only nodes at least a bin wide or tall can be) and the small-node count
-    std::vector<int>& dlarge = c.dens_large_h;
-    dlarge.clear();
-    // bound partials: node i adds into acc[i % 4], in ascending i; thread t owns partial t (the
-    // same sums in the same order as one pass), its large nodes and its small-node count
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    int small_t[4] = {0, 0, 0, 0};
-    std::vector<int> large_t[4];
-    run_parts(4, [&](int t) {
-        double a = 0.0;
-        int ns = 0;
-        std::vector<int>& lg = large_t[t];
-        for (int i = t; i < c.total; i += 4) {
-            if (c.fixed(i) || c.ni(i)) continue;
-            const float w = c.w[i], h = c.h[i];
-            a += static_cast<double>(w) * static_cast<double>(h);
-            const bool large = !(w < g.step_x && h < g.step_y) && (node_footprint(c, g, target, i).kind & K_LARGE);
-            if (large) lg.push_back(i);
-            else ++ns;
-        }
-        acc[t] = a;
-        small_t[t] = ns;
-    });
+    ht.mark("statics+footprints");
     const int n_small = (small_t[0] + small_t[1]) + (small_t[2] + small_t[3]);
     for (const std::vector<int>& lg : large_t) dlarge.insert(dlarge.end(), lg.begin(), lg.end());
     std::sort(dlarge.begin(), dlarge.end());
@@ -826,7 +830,6 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     g.scale_f = s >= 0 ? std::ldexp(1.0f, s) : 0.f;
     g.inv_scale = std::ldexp(1.0, -s);
 
-    ht.mark("footprints");
     cudaStream_t st = c.stream;
     c.terminal.upload(term, st);
     c.base.upload(base, st);
