@@ -222,14 +222,14 @@ def fp32_arm(db, workload, init_x, init_y, steps):
     return sum(iters) / (sum(ms) / 1e3), iters
 
 
-# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each part, from one
-# ncu --set full capture of the 211k-cell workload with the split-BF16 Poisson (caches flushed
-# before each replayed launch, so these are cold-L2 figures; writes that stay in L2 at the end
-# of a launch are not counted). The Poisson part is its five launches of one solve (its first
-# operand comes from the rho kernel).
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of each part, from ncu
+# captures of the 211k-cell workload with the split-BF16 Poisson (caches flushed before each
+# replayed launch, so these are cold-L2 figures; writes that stay in L2 at the end of a launch
+# are not counted). The Poisson part is its five launches of one solve (its first operand comes
+# from the rho kernel); the WA part is the nets pass and the cells' pass 2.
 PROFILED_DRAM_BYTES = {
-    ("large", "bf16x3"): {"update": 40.15e6, "wa": 15.52e6, "rho": 6.31e6, "poisson": 13.77e6,
-                          "assemble": 44.73e6,
+    ("large", "bf16x3"): {"update": 40.15e6, "wa": 25.76e6, "rho": 6.31e6, "poisson": 13.77e6,
+                          "assemble": 39.18e6,
                           "source": "profiles/mgp_211k_bf16x3_kernels.md"},
 }
 
@@ -241,23 +241,24 @@ def part_rooflines(parts, db, dim, hbm_gbs, bf16_tflops, precision, traffic=None
       update     40 B per optimised node (u, v, g in; v', u' out) + 60 B per cell (x, y into
                  the node arrays; meta, geometry, clamp box, node index) + 16 B per bin (the
                  two fixed-point maps it scatters into)
-      wa         32 B per pin + 8 B per net (pin ids, offsets, positions in; 2 terms out)
+      wa         32 B per pin + 8 B per net (pass 1: pin ids, offsets, positions in; 2 terms
+                 out) + 8 B per pin + 24 B per cell (pass 2: terms and meta in; 2 sums out)
       scatter    25 B per density node outside the opt set + 16 B per bin (only FILLERONLY
                  and cGP have such nodes)
       rho        44 B per bin (maps, terminal, base in; rho out; maps cleared)
       poisson    14 M^3 flops (16 B per bin of I/O)
-      assemble   32 B per optimised node (u, uPrev, gPrevTmp in; g out) + 40 B per cell
-                 (meta, geometry, area) + 8 B per pin (the WA pass-1 terms) + 8 B per bin
-                 (the field maps it gathers from)
+      assemble   32 B per optimised node (u, uPrev, gPrevTmp in; g out) + 48 B per cell
+                 (meta, geometry, area, the WA pass-2 sums) + 8 B per bin (the field maps it
+                 gathers from)
     traffic: measured DRAM bytes per launch by part (PROFILED_DRAM_BYTES), when known.
     """
     n_opt = db.num_movable + db.num_fillers
     cells = db.num_movable
     n_dens = n_opt
     pins, nets, bins = db.num_pins, db.num_nets, dim * dim
-    by = {"update": 40 * n_opt + 60 * cells + 16 * bins, "wa": 32 * pins + 8 * nets,
+    by = {"update": 40 * n_opt + 60 * cells + 16 * bins, "wa": 40 * pins + 8 * nets + 24 * cells,
           "scatter": 25 * n_dens + 16 * bins, "rho": 44 * bins,
-          "assemble": 32 * n_opt + 40 * cells + 8 * pins + 8 * bins}
+          "assemble": 32 * n_opt + 48 * cells + 8 * bins}
     traffic = traffic or {}
     out = {}
     for k, us in parts.items():

@@ -8,17 +8,22 @@
 // updated by control kernels. Per iteration it reads a 16-byte status to learn whether
 // to launch a backtracking re-evaluation or the next iteration.
 #include <cuda_runtime.h>
+#include <pthread.h>
 
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
+#include <functional>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <numeric>
 #include <random>
 #include <string>
@@ -43,6 +48,16 @@ bool pdl_enabled() {
 thread_local cudaStream_t t_alloc_stream = nullptr;
 
 namespace {
+// The opt cells' WA pass 2 runs on the WA stream ahead of the assembly (wl_cells_kernel);
+// SPG_WL_AHEAD=0 leaves it inside the assembly. Same sums either way.
+bool wl_ahead() {
+    static const bool on = [] {
+        const char* e = std::getenv("SPG_WL_AHEAD");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
 cudaMemPool_t library_pool(int dev) {
     static std::mutex mu;
     static std::vector<std::pair<int, cudaMemPool_t>> pools;
@@ -179,15 +194,123 @@ constexpr float kBoundaryEps = 1e-3f;  // eplace.cpp:38
 
 }  // namespace
 
-// Runs fn(t) for t = 0..n-1, t = 0 on the calling thread and the others on threads of their
-// own; returns once all have finished. Used for host passes whose parts write disjoint data.
+// A process-wide pool of host worker threads for run_parts. The host passes of a stage run
+// as parts at once (grid statics, the footprint scan, large copies); a pool spares each part a
+// thread start. Any number of callers (contexts on threads of their own) may submit at once,
+// and a caller runs parts of its own batch as well, so its call completes even when every
+// worker is busy elsewhere. Every access to a batch is under the pool's lock, and a caller
+// returns only after the last part of its batch has been accounted for there, so no worker
+// touches a batch after its call ends. The pool is never destroyed (its workers idle until the
+// process exits); a forked child, which has none of the parent's workers, starts a pool of its
+// own on first use.
+class HostPool {
+public:
+    static HostPool& get() {
+        HostPool* p = g_pool.load(std::memory_order_acquire);
+        if (p) return *p;
+        std::lock_guard<std::mutex> lock(*g_pool_mu);
+        p = g_pool.load(std::memory_order_relaxed);
+        if (!p) {
+            static const int registered = pthread_atfork(nullptr, nullptr, [] {
+                g_pool_mu = new (g_pool_mu_store) std::mutex();  // the child's first and only thread
+                g_pool.store(nullptr, std::memory_order_relaxed);
+            });
+            (void)registered;
+            p = new HostPool();
+            g_pool.store(p, std::memory_order_release);
+        }
+        return *p;
+    }
+
+    template <typename F>
+    void run(int n, F& fn) {
+        if (n <= 0) return;
+        Batch b;
+        b.fn = [&fn](int t) { fn(t); };
+        b.n = n;
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            queue_.push_back(&b);
+        }
+        work_.notify_all();
+        for (;;) {  // the caller takes parts until none is left unclaimed
+            int t;
+            {
+                std::lock_guard<std::mutex> lock(mu_);
+                if (!claim(&b, &t)) break;
+            }
+            execute(&b, t);
+        }
+        std::unique_lock<std::mutex> lock(mu_);
+        done_.wait(lock, [&] { return b.finished == b.n; });
+        lock.unlock();
+        if (b.err) std::rethrow_exception(b.err);
+    }
+
+private:
+    struct Batch {
+        std::function<void(int)> fn;
+        int n = 0, next = 0, finished = 0;
+        std::exception_ptr err;
+    };
+
+    HostPool() {
+        const unsigned hc = std::thread::hardware_concurrency();
+        const int workers = static_cast<int>(std::min(15u, hc > 1 ? hc - 1 : 0u));
+        for (int i = 0; i < workers; ++i) std::thread([this] { loop(); }).detach();
+    }
+
+    // under mu_: the next unclaimed part of b (the batch leaves the queue with its last part)
+    bool claim(Batch* b, int* t) {
+        if (b->next >= b->n) return false;
+        *t = b->next++;
+        if (b->next == b->n) queue_.erase(std::find(queue_.begin(), queue_.end(), b));
+        return true;
+    }
+
+    void execute(Batch* b, int t) {
+        std::exception_ptr err;
+        try {
+            b->fn(t);
+        } catch (...) {
+            err = std::current_exception();
+        }
+        std::lock_guard<std::mutex> lock(mu_);
+        if (err && !b->err) b->err = err;
+        if (++b->finished == b->n) done_.notify_all();
+    }
+
+    void loop() {
+        for (;;) {
+            Batch* b;
+            int t;
+            {
+                std::unique_lock<std::mutex> lock(mu_);
+                work_.wait(lock, [&] { return !queue_.empty(); });
+                b = queue_.front();
+                claim(b, &t);
+            }
+            execute(b, t);
+        }
+    }
+
+    std::mutex mu_;
+    std::condition_variable work_, done_;
+    std::vector<Batch*> queue_;
+
+    static std::atomic<HostPool*> g_pool;
+    alignas(std::mutex) static unsigned char g_pool_mu_store[sizeof(std::mutex)];
+    static std::mutex* g_pool_mu;
+};
+std::atomic<HostPool*> HostPool::g_pool{nullptr};
+alignas(std::mutex) unsigned char HostPool::g_pool_mu_store[sizeof(std::mutex)];
+std::mutex* HostPool::g_pool_mu = new (HostPool::g_pool_mu_store) std::mutex();
+
+// Runs fn(t) for t = 0..n-1 at once on the host pool and the calling thread; returns once all
+// have finished. Used for host passes whose parts write disjoint data.
 template <typename F>
 void run_parts(int n, F&& fn) {
-    std::vector<std::thread> th;
-    th.reserve(static_cast<size_t>(n > 1 ? n - 1 : 0));
-    for (int t = 1; t < n; ++t) th.emplace_back(fn, t);
-    fn(0);
-    for (auto& x : th) x.join();
+    HostPool::get().run(n, fn);
 }
 
 // memcpy of a large host buffer split over four threads (a single thread copies a few GB/s,
@@ -436,7 +559,7 @@ struct Context : ContextStreams {
     // host copy of the node positions as last uploaded, while the device copy is unchanged
     std::vector<float> x_mirror, y_mirror;  // host copy of the non-filler positions (fixed nodes' terminal density)
     bool mirror_valid = false;
-    DevBuf<float> opt_lo, opt_hi, force, pool;
+    DevBuf<float> opt_lo, opt_hi, force, wlg, pool;
     // the fillers' spatial reorder (filler_order.cu): active for the stage when the fillers
     // share their attributes and are numerous; the loop pauses at the listed iterations
     bool fo_active = false;
@@ -556,6 +679,7 @@ struct Context : ContextStreams {
         p.opt_hi = opt_hi.p;
         p.opt_area = opt_area.p;
         p.force = force.p;
+        p.wlg = wl_ahead() ? wlg.p : nullptr;
         p.pool = pool.p;
         p.vec_stride = vec_stride;
         p.dens_large = dens_large.p;
@@ -721,7 +845,8 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     const size_t n = static_cast<size_t>(dim) * dim;
 
     // terminal density (bin_grid.cpp:120-137): every bin adds its fixed nodes' overlaps in
-    // node order; thread `part` of the pass below takes the bin columns bx = part (mod 4)
+    // node order; thread `part` of the pass below takes the bin columns bx = part (mod kParts)
+    constexpr int kParts = 4;
     std::vector<int> fixed_nodes;
     for (int i = 0; i < c.num_nodes; ++i)
         if (c.fixed(i) && !c.ni(i)) fixed_nodes.push_back(i);
@@ -734,7 +859,7 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
             const int bx1 = clampi_h(static_cast<int>((hx - g.origin_x) / g.step_x), 0, dim - 1);
             const int by0 = clampi_h(static_cast<int>((ly - g.origin_y) / g.step_y), 0, dim - 1);
             const int by1 = clampi_h(static_cast<int>((hy - g.origin_y) / g.step_y), 0, dim - 1);
-            for (int bx = bx0 + ((part - bx0) % 4 + 4) % 4; bx <= bx1; bx += 4) {
+            for (int bx = bx0 + ((part - bx0) % kParts + kParts) % kParts; bx <= bx1; bx += kParts) {
                 const float blx = g.origin_x + bx * g.step_x;
                 for (int by = by0; by <= by1; ++by) {
                     const float bly = g.origin_y + by * g.step_y;
@@ -782,35 +907,38 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         acc[t] = a;
         small_t[t] = ns;
     };
-    // eight threads: 0-3 the statics (each its terminal columns, then every fourth bin row of
-    // the base map; bin rows are independent), 4-7 the footprint scan's four partials
-    run_parts(8, [&](int part) {
-    if (part >= 4) {
-        footprint_part(part - 4);
-        return;
-    }
-    terminal_part(part);
-    for (int by = part; by < dim; by += 4) {
-        const float bly = g.origin_y + by * g.step_y;
-        const float bhy = bly + g.step_y;
-        size_t lo = 0, hi = static_cast<size_t>(nr);
-        while (lo < hi) {
-            const size_t mid = (lo + hi) / 2;
-            if (rhy[mid] <= bly) lo = mid + 1;
-            else hi = mid;
+    // eight parts: 0-3 the statics (each its terminal columns, then one contiguous block of bin
+    // rows of the base map, so no two threads write into one cache line; bin rows are
+    // independent), 4-7 the footprint scan's four partials (more statics parts measured no
+    // faster on a 16-core host)
+    run_parts(kParts + 4, [&](int part) {
+        if (part >= kParts) {
+            footprint_part(part - kParts);
+            return;
         }
-        for (int bx = 0; bx < dim; ++bx) {
-            const float blx = g.origin_x + bx * g.step_x;
-            const float bhx = blx + g.step_x;
-            float covered = 0.f;
-            for (size_t t = lo; t < static_cast<size_t>(nr); ++t) {
-                if (rly[t] >= bhy) break;
-                covered += overlap_area(blx, bly, bhx, bhy, rlx[t], rly[t], rhx[t], rhy[t]);
+        terminal_part(part);
+        const int by_end = (part + 1) * dim / kParts;
+        for (int by = part * dim / kParts; by < by_end; ++by) {
+            const float bly = g.origin_y + by * g.step_y;
+            const float bhy = bly + g.step_y;
+            size_t lo = 0, hi = static_cast<size_t>(nr);
+            while (lo < hi) {
+                const size_t mid = (lo + hi) / 2;
+                if (rhy[mid] <= bly) lo = mid + 1;
+                else hi = mid;
             }
-            const float area = (bhx - blx) * (bhy - bly);
-            base[static_cast<size_t>(bx) * dim + by] = target * hmax(0.f, area - covered);
+            for (int bx = 0; bx < dim; ++bx) {
+                const float blx = g.origin_x + bx * g.step_x;
+                const float bhx = blx + g.step_x;
+                float covered = 0.f;
+                for (size_t t = lo; t < static_cast<size_t>(nr); ++t) {
+                    if (rly[t] >= bhy) break;
+                    covered += overlap_area(blx, bly, bhx, bhy, rlx[t], rly[t], rhx[t], rhy[t]);
+                }
+                const float area = (bhx - blx) * (bhy - bly);
+                base[static_cast<size_t>(bx) * dim + by] = target * hmax(0.f, area - covered);
+            }
         }
-    }
     });
     ht.mark("statics+footprints");
     const int n_small = (small_t[0] + small_t[1]) + (small_t[2] + small_t[3]);
@@ -1038,6 +1166,7 @@ void stage_setup(Context& c, int stage) {
     c.opt_large.upload(olarge, s);
     c.n_opt_large = static_cast<int>(olarge.size());
     c.force.alloc(2 * static_cast<size_t>(std::max(n, 1)));
+    if (wl_ahead()) c.wlg.alloc(2 * static_cast<size_t>(std::max(n, 1)));
     // vectors padded to 64 floats so every role starts 256-byte aligned
     c.vec_stride = (2 * static_cast<size_t>(std::max(n, 1)) + 63) / 64 * 64;
     c.pool.alloc(c.vec_stride * (NUM_ROLES + SNAP_MAX));
@@ -1120,6 +1249,7 @@ void fork_wa(Context& c, const DevPtrs& p) {
     SPG_CUDA(cudaEventRecord(c.ev_fork, c.stream));
     SPG_CUDA(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
     launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, c.side);
+    launch_wl_cells(p, c.side);
     SPG_CUDA(cudaEventRecord(c.ev_join, c.side));
 }
 
@@ -1128,8 +1258,12 @@ void evaluate(Context& c, const DevPtrs& p, int pos_role, int grad_role, int cou
               bool stepped = false, cudaGraphConditionalHandle loop_cond = 0, bool wa_forked = false) {
     cudaStream_t s = c.stream;
     if (pos_role >= 0) launch_scatter(p, pos_role, s);
-    if (wa_serial()) launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s);
-    else if (!wa_forked) fork_wa(c, p);
+    if (wa_serial()) {
+        launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s);
+        launch_wl_cells(p, s);
+    } else if (!wa_forked) {
+        fork_wa(c, p);
+    }
     if (stepped) launch_density_rest(p, s);
     else launch_density_accumulate(p, s);
     const bool fused = rho_and_split(c, p, s);
@@ -1785,11 +1919,11 @@ __global__ void set_eval_kernel(DevState* st, float lambda, float gamma) {
 // EPlace::Impl::objAndGrad (eplace.cpp:136-203) at opt-set positions pos (x then y, the opt
 // order of buildOptSet) for the given lambda and gamma, through the GP loop body's own kernels
 // (enqueue_iteration): the step kernel's fixed-point scatter of u, the WA pass 1 with HPWL,
-// the rest-list scatter, rho and tau, the Poisson solve, the large nodes' gather, and the
-// fused assembly (cell gather, WA pass 2, preconditioned gradient). grad gets 2*nOpt floats;
-// out[0..4] = WA value, tau, HPWL, sum|grad WL|, sum|q xi|; *n_opt the opt-set size. With
-// pos = NULL only *n_opt is set. The grid and opt set are rebuilt for `stage` from the
-// context's positions and flags first, as constructing EPlace does.
+// WA pass 2 of the cells, the rest-list scatter, rho and tau, the Poisson solve, the large
+// nodes' gather, and the fused assembly (cell gather, preconditioned gradient). grad gets
+// 2*nOpt floats; out[0..4] = WA value, tau, HPWL, sum|grad WL|, sum|q xi|; *n_opt the opt-set
+// size. With pos = NULL only *n_opt is set. The grid and opt set are rebuilt for `stage` from
+// the context's positions and flags first, as constructing EPlace does.
 void eval_grad(Context& c, int stage, float lambda, float gamma, const float* pos, float* grad, double* out,
                int* n_opt) {
     SPG_REQUIRE(stage >= SPG_STAGE_MGP && stage <= SPG_STAGE_CGP, SPG_E_INVALID, "unknown stage");
@@ -2788,7 +2922,10 @@ int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n) {
     t[0] = time([&] { spg::launch_update(p, s); }, zero_maps);
     set_state(probe);
     spg::launch_scatter(p, spg::R_POS, s);  // the delivered positions again
-    t[1] = time([&] { spg::launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s); }, nothing);
+    t[1] = time([&] {
+        spg::launch_wa_nets(p, c.wa_classes, &p.st->gamma, 0.f, 1, s);
+        spg::launch_wl_cells(p, s);
+    }, nothing);
     t[2] = (c.n_rest_small + c.n_rest_large) > 0 ? time([&] { spg::launch_density_rest(p, s); }, zero_maps) : 0.0;
     bool fused = false;
     t[3] = time([&] { fused = spg::rho_and_split(c, p, s); }, [&] { spg::launch_density_accumulate(p, s); });

@@ -192,6 +192,9 @@ struct DevPtrs {
     double filler_area;
     float filler_lo_x, filler_hi_x, filler_lo_y, filler_hi_y;
     float* force;          // 2*nOpt, density force q*xi (not gradient)
+    // 2*nOpt: the opt cells' WA gradient (pass 2, wl_cells_kernel) formed beside the density
+    // chain; null when the assembly sums the pin terms itself (SPG_WL_AHEAD=0)
+    float* wlg;
     float* pool;           // NUM_ROLES + SNAP_MAX vectors of 2*nOpt
     size_t vec_stride;
     // density work lists (node ids): every density node, and the "rest" the loop's step
@@ -302,7 +305,10 @@ void launch_wa_node_grad(const DevPtrs& p, float* grad, cudaStream_t s);
 
 // ---- optimizer.cu
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s);
-// WA pass 2 + cell gather + gradient assembly; its last block finalizes the evaluation
+// WA pass 2 of the opt cells into p.wlg (after the WA nets pass, before the assembly)
+void launch_wl_cells(const DevPtrs& p, cudaStream_t s);
+// cell gather + gradient assembly (with wl_cells_kernel's WA sums); its last block finalizes
+// the evaluation
 void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s);
 // the loop's evaluation tail: the assembly at u = R_U into g = R_G with the step's norms
 // and the per-iteration decisions in the same launch

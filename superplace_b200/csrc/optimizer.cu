@@ -12,8 +12,11 @@
 //   step_kernel     v' = u - alpha g, u' = v' + m (v' - v), clamp (or the re-evaluation step
 //                   when the last decisions asked for one), u' into the node positions and
 //                   its fixed-point charge into the density maps; stagnation snapshot copy
-//   assemble_kernel WA pass 2 + cell gather + gradient assembly and, in the same pass, the
-//                   norms |u-uPrev|, |g-gPrevTmp|, their dot and |g|^2; its last block applies
+//   wl_cells_kernel WA pass 2 of the opt cells (per-cell sum of its pin terms), on the WA
+//                   stream after the nets pass, beside the density -> Poisson chain
+//   assemble_kernel cell gather + gradient assembly (pass 2's sums read back) and, in the
+//                   same pass, the norms |u-uPrev|, |g-gPrevTmp|, their dot and |g|^2; its last
+//                   block applies
 //                   the step's role rotation, finalizes the evaluation (tau, HPWL, WA value,
 //                   force sums) and runs the backtracking test and every per-iteration decision
 //                   of the reference (step size, momentum, lambda/gamma, metrics row, stop test,
@@ -447,6 +450,27 @@ __device__ void decide(const DevPtrs& p, DevState* st, double dx2, double dg2, d
     }
 }
 
+// WA pass 2 of the opt cells (k < filler_k0): wlg[k], wlg[n + k] = the sums of cell k's pin
+// terms in node->pin order (wa_wirelength.cpp:137-179), the fadd sequence the assembly would
+// run itself. It runs on the WA stream after the nets pass, beside the density -> Poisson
+// chain, so the assembly on that chain reads two values per cell instead of walking its pins.
+__global__ void __launch_bounds__(RED_THREADS) wl_cells_kernel(DevPtrs p) {
+    pdl_wait();
+    pdl_trigger();
+    const int n = p.n_opt;
+    const int k0 = p.filler_k0 < n ? p.filler_k0 : n;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < k0; k += gridDim.x * blockDim.x) {
+        const int4 meta = p.opt_meta[k];
+        float gx = 0.f, gy = 0.f;
+        for (int t = meta.x; t < meta.y; ++t) {
+            gx = fadd(gx, p.gpx[t]);
+            gy = fadd(gy, p.gpy[t]);
+        }
+        p.wlg[k] = gx;
+        p.wlg[n + k] = gy;
+    }
+}
+
 // One node of the assembly (see assemble_kernel). FILL: a filler, whose attributes are the
 // shared constants (no pins, so no WA term).
 // precondition 1 / max(1, deg + lambda * area) (eplace.cpp:166-189) of one node.
@@ -477,9 +501,14 @@ __device__ __forceinline__ void assemble_node(const DevPtrs& p, int k, float lam
     }
     float gx = 0.f, gy = 0.f;
     if (!FILL) {
-        for (int t = meta.x; t < meta.y; ++t) {
-            gx = fadd(gx, p.gpx[t]);
-            gy = fadd(gy, p.gpy[t]);
+        if (p.wlg) {
+            gx = p.wlg[k];
+            gy = p.wlg[n + k];
+        } else {
+            for (int t = meta.x; t < meta.y; ++t) {
+                gx = fadd(gx, p.gpx[t]);
+                gy = fadd(gy, p.gpy[t]);
+            }
         }
     }
     float fx, fy;
@@ -512,9 +541,10 @@ __device__ __forceinline__ void assemble_node(const DevPtrs& p, int k, float lam
 }
 
 // grad_k = precond * (dWL - lambda * q*xi), precond = 1 / max(1, deg + lambda*area)
-// (eplace.cpp:166-189), with the WA pass 2 (per-node sum of per-pin contributions in
-// node->pin order, wa_wirelength.cpp:137-179) and the field gather of cells fused in (large
-// nodes' force comes from gather_opt_large). The last block finalizes the evaluation
+// (eplace.cpp:166-189), with the field gather of cells fused in (large nodes' force comes from
+// gather_opt_large) and the cells' WA gradient read from wl_cells_kernel's sums (WA pass 2:
+// per-node sum of per-pin contributions in node->pin order, wa_wirelength.cpp:137-179; with
+// SPG_WL_AHEAD=0 the assembly forms those sums itself). The last block finalizes the evaluation
 // (eplace.cpp:149,154-155,190-197).
 //
 // FUSE (the iteration loop's evaluations, at u = R_U into g = R_G): the same pass also forms
@@ -977,6 +1007,23 @@ inline int vec_blocks(const DevPtrs& p, K kernel) {
 
 void launch_scatter(const DevPtrs& p, int role, cudaStream_t s) {
     LAUNCH(scatter_kernel, vec_blocks(p, scatter_kernel), RED_THREADS, p, role);
+}
+void launch_wl_cells(const DevPtrs& p, cudaStream_t s) {
+    const int k0 = p.filler_k0 < p.n_opt ? p.filler_k0 : p.n_opt;
+    if (!p.wlg || k0 <= 0) return;
+    // no programmatic early start: blocks resident ahead of the WA pass's end would only wait
+    // there, holding SM room the chain's kernels need; the WA stream's low priority
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ceil_div(k0, RED_THREADS));
+    cfg.blockDim = dim3(RED_THREADS);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = launch_priority(false);
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    SPG_CUDA(cudaLaunchKernelEx(&cfg, wl_cells_kernel, p));
+    count_launch();
 }
 void launch_assemble(const DevPtrs& p, int pos_role, int grad_role, int count_eval, cudaStream_t s) {
     LAUNCH(assemble_kernel<false>, work_grid(reinterpret_cast<const void*>(assemble_kernel<false>), p.n_opt, RED_THREADS),
