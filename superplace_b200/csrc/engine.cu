@@ -194,13 +194,13 @@ constexpr float kBoundaryEps = 1e-3f;  // eplace.cpp:38
 
 }  // namespace
 
-// A process-wide pool of host worker threads for run_parts. The host passes of a stage run
-// as parts at once (grid statics, the footprint scan, large copies); a pool spares each part a
-// thread start. Any number of callers (contexts on threads of their own) may submit at once,
-// and a caller runs parts of its own batch as well, so its call completes even when every
-// worker is busy elsewhere. Every access to a batch is under the pool's lock, and a caller
-// returns only after the last part of its batch has been accounted for there, so no worker
-// touches a batch after its call ends. The pool is never destroyed (its workers idle until the
+// A process-wide pool of host worker threads for run_parts and PartsTask. The host passes of a
+// stage run as parts at once (grid statics, the footprint scan, large copies); a pool spares
+// each part a thread start. Any number of callers (contexts on threads of their own) may submit
+// at once, and a waiting caller runs parts of its own batch as well, so its wait completes even
+// when every worker is busy elsewhere. Every access to a batch is under the pool's lock, and
+// wait returns only after the last part of its batch has been accounted for there, so no worker
+// touches a batch after its wait ends. The pool is never destroyed (its workers idle until the
 // process exits); a forked child, which has none of the parent's workers, starts a pool of its
 // own on first use.
 class HostPool {
@@ -222,18 +222,28 @@ public:
         return *p;
     }
 
-    template <typename F>
-    void run(int n, F& fn) {
-        if (n <= 0) return;
-        Batch b;
-        b.fn = [&fn](int t) { fn(t); };
-        b.n = n;
+    // One submission: fn(t) for t = 0..n-1. It must stay in place (and fn alive) from submit
+    // to the end of wait.
+    struct Batch {
+        std::function<void(int)> fn;
+        int n = 0, next = 0, finished = 0;
+        std::exception_ptr err;
+    };
+
+    void submit(Batch& b) {
+        if (b.n <= 0) return;
         {
             std::lock_guard<std::mutex> lock(mu_);
             queue_.push_back(&b);
         }
         work_.notify_all();
-        for (;;) {  // the caller takes parts until none is left unclaimed
+    }
+
+    // Runs the batch's unclaimed parts on the calling thread, waits for the others, then
+    // rethrows the first exception a part raised.
+    void wait(Batch& b) {
+        if (b.n <= 0) return;
+        for (;;) {
             int t;
             {
                 std::lock_guard<std::mutex> lock(mu_);
@@ -247,13 +257,16 @@ public:
         if (b.err) std::rethrow_exception(b.err);
     }
 
-private:
-    struct Batch {
-        std::function<void(int)> fn;
-        int n = 0, next = 0, finished = 0;
-        std::exception_ptr err;
-    };
+    template <typename F>
+    void run(int n, F& fn) {
+        Batch b;
+        b.fn = [&fn](int t) { fn(t); };
+        b.n = n;
+        submit(b);
+        wait(b);
+    }
 
+private:
     HostPool() {
         const unsigned hc = std::thread::hardware_concurrency();
         const int workers = static_cast<int>(std::min(15u, hc > 1 ? hc - 1 : 0u));
@@ -312,6 +325,36 @@ template <typename F>
 void run_parts(int n, F&& fn) {
     HostPool::get().run(n, fn);
 }
+
+// run_parts in the background: the parts start on the pool at construction, and wait() runs
+// what is left on the calling thread and waits for the rest (the destructor does the same on an
+// exception's way out, dropping the parts' own errors). fn must outlive the task.
+class PartsTask {
+public:
+    template <typename F>
+    PartsTask(int n, F& fn) {
+        b_.fn = [&fn](int t) { fn(t); };
+        b_.n = n;
+        HostPool::get().submit(b_);
+    }
+    PartsTask(const PartsTask&) = delete;
+    PartsTask& operator=(const PartsTask&) = delete;
+    void wait() {
+        waited_ = true;
+        HostPool::get().wait(b_);
+    }
+    ~PartsTask() {
+        if (waited_) return;
+        try {
+            HostPool::get().wait(b_);
+        } catch (...) {
+        }
+    }
+
+private:
+    HostPool::Batch b_;
+    bool waited_ = false;
+};
 
 // memcpy of a large host buffer split over four threads (a single thread copies a few GB/s,
 // well below what the host link and the host's memory sustain).
@@ -810,8 +853,12 @@ __global__ void footprint_kernel(FootprintArgs a) {
     }
 }
 
+// BinGrid::initialize (bin_grid.cpp:64-189) for the context's nodes at hx_pos / hy_pos: the
+// grid, its static maps, the footprints and the fixed-point scale. `meanwhile` (optional) runs
+// on the calling thread after the device set-up and before the static maps are uploaded, while
+// the pool still builds them; it may enqueue work that needs no static map.
 void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& hx_pos,
-               const std::vector<float>& hy_pos) {
+               const std::vector<float>& hy_pos, const std::function<void()>& meanwhile = nullptr) {
     HostTimer ht(" grid");
     double cell_area = 0.0, macro_area = 0.0;
     for (int i = 0; i < c.num_movable; ++i) {
@@ -907,15 +954,11 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
         acc[t] = a;
         small_t[t] = ns;
     };
-    // eight parts: 0-3 the statics (each its terminal columns, then one contiguous block of bin
-    // rows of the base map, so no two threads write into one cache line; bin rows are
-    // independent), 4-7 the footprint scan's four partials (more statics parts measured no
-    // faster on a 16-core host)
-    run_parts(kParts + 4, [&](int part) {
-        if (part >= kParts) {
-            footprint_part(part - kParts);
-            return;
-        }
+    // The statics run in the background on the pool: four parts, each its terminal columns,
+    // then one contiguous block of bin rows of the base map (so no two threads write into one
+    // cache line; bin rows are independent). Meanwhile the footprint scan's four partials run,
+    // then the device set-up and the caller's `meanwhile` work, which need no static map.
+    auto statics_part = [&](int part) {
         terminal_part(part);
         const int by_end = (part + 1) * dim / kParts;
         for (int by = part * dim / kParts; by < by_end; ++by) {
@@ -939,8 +982,10 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
                 base[static_cast<size_t>(bx) * dim + by] = target * hmax(0.f, area - covered);
             }
         }
-    });
-    ht.mark("statics+footprints");
+    };
+    PartsTask statics(kParts, statics_part);
+    run_parts(4, footprint_part);
+    ht.mark("footprints");
     const int n_small = (small_t[0] + small_t[1]) + (small_t[2] + small_t[3]);
     for (const std::vector<int>& lg : large_t) dlarge.insert(dlarge.end(), lg.begin(), lg.end());
     std::sort(dlarge.begin(), dlarge.end());
@@ -959,8 +1004,6 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     g.inv_scale = std::ldexp(1.0, -s);
 
     cudaStream_t st = c.stream;
-    c.terminal.upload(term, st);
-    c.base.upload(base, st);
     c.flags_d.upload(c.flags, st);
     c.hw.alloc(c.total);
     c.hh.alloc(c.total);
@@ -1014,6 +1057,14 @@ void grid_init(Context& c, float target, int bin_dim, const std::vector<float>& 
     ht.mark("plan");
     c.partials.alloc(static_cast<size_t>(RED_SLOTS) * RED_CAP);
     c.partials.zero(st);
+    if (meanwhile) {
+        meanwhile();
+        ht.mark("meanwhile");
+    }
+    statics.wait();
+    ht.mark("statics");
+    c.terminal.upload(term, st);
+    c.base.upload(base, st);
     c.grid_ready = true;
 }
 
@@ -1741,11 +1792,10 @@ void prepare_stage(Context& c, int stage, HostTimer* ht) {
         download_bytes(c.x_mirror.data(), c.x.p, c.num_nodes * sizeof(float), c.stream);
         download_bytes(c.y_mirror.data(), c.y.p, c.num_nodes * sizeof(float), c.stream);
     }
-    grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, c.x_mirror, c.y_mirror);
+    // the opt set is built while the pool builds the grid's static maps
+    grid_init(c, c.prm.target_density, c.prm.gp_bin_dim, c.x_mirror, c.y_mirror, [&] { stage_setup(c, stage); });
     c.mirror_valid = false;  // the stage moves the positions
-    if (ht) ht->mark("grid_init");
-    stage_setup(c, stage);
-    if (ht) ht->mark("stage_setup");
+    if (ht) ht->mark("grid_init+stage_setup");
 }
 
 // EPlace::run (eplace.cpp:223-526) for one stage, device-resident.
