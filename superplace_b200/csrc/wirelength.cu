@@ -24,9 +24,11 @@ namespace spg {
 
 namespace {
 
-// WA blocks per SM (0: one full wave, 4 at 64 registers); SPG_WA_BLOCKS_PER_SM overrides it.
-// Three leave a quarter of each SM's registers to the fillers' step that runs beside WA:
-// 6441-6491 iter/s at 211k cells against 6357-6399 with the full wave.
+// WA blocks per SM (0: one full wave, 5 at 48 registers); SPG_WA_BLOCKS_PER_SM overrides it.
+// WA's blocks are resident before the fillers' step that runs beside it, so the registers they
+// leave decide how many of the step's blocks fit: three blocks of 48 registers leave room for
+// two (6822-6857 iter/s at 211k cells, against 6661-6668 at 64 registers, which left room for
+// one; 2 blocks of 48: 6545-6576, 4: 6756-6788; 40 registers spill: 6457-6498).
 constexpr int kWaBlocksPerSm = 3;
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -229,7 +231,7 @@ static_assert(kWaThreadNetDegree == 5, "wa_thread_class_net covers degrees up to
 // butterflies, and every lane writes its own pin's gradient term. Those sums are formed in
 // butterfly order rather than the reference's pin order, so values differ from the
 // reference's sequential float sums in the last bits only.
-__global__ void __launch_bounds__(RED_THREADS, 4) wa_net_kernel(DevPtrs p, WaClasses wa, const float* gamma_dev,
+__global__ void __launch_bounds__(RED_THREADS, 5) wa_net_kernel(DevPtrs p, WaClasses wa, const float* gamma_dev,
                                                                 float gamma_host, int use_dev) {
     pdl_wait();
     pdl_trigger();
@@ -308,8 +310,8 @@ __global__ void wa_node_grad_kernel(DevPtrs p, float* grad) {
 void launch_wa_nets(const DevPtrs& p, const WaClasses& wa, const float* gamma_dev, float gamma_host, int use_dev,
                     cudaStream_t s) {
     // A fixed grid per device, so the FP64 partials keep a fixed owner per block. WA runs
-    // beside the scatter -> rho -> Poisson chain; at most kWaBlocksPerSm blocks per SM leave
-    // each SM room for a Poisson GEMM block (its registers and ~150 KB of shared memory).
+    // beside the fillers' step and the rho -> Poisson chain; at most kWaBlocksPerSm blocks per
+    // SM leave each SM room for the step's blocks and a Poisson GEMM block.
     int per_sm = kWaBlocksPerSm;
     if (const char* e = std::getenv("SPG_WA_BLOCKS_PER_SM")) per_sm = std::atoi(e);
     int dev = 0, sms = 0;
