@@ -8,7 +8,10 @@
  *
  * Threading: one host thread per context / Poisson handle (the reference's contract,
  * src/numeric/poisson_backend.h:20-46 and src/gp/eplace.h:56-77). Independent handles
- * may be used concurrently from different threads.
+ * may be used concurrently from different threads. The host passes of a stage (the grid's
+ * static maps, the footprint scan, large host copies) run on a process-wide pool of worker
+ * threads (one fewer than the hardware threads, at most 15), started on first use and idle
+ * between calls; results do not depend on how many there are.
  *
  * Ownership: the caller owns every host array passed in; the library owns every device
  * buffer and releases it in the matching *_destroy call.
