@@ -228,7 +228,7 @@ def fp32_arm(db, workload, init_x, init_y, steps):
 # are not counted). The Poisson part is its five launches of one solve (its first operand comes
 # from the rho kernel); the WA part is the nets pass and the cells' pass 2.
 PROFILED_DRAM_BYTES = {
-    ("large", "bf16x3"): {"update": 40.15e6, "wa": 25.76e6, "rho": 6.31e6, "poisson": 13.77e6,
+    ("large", "bf16x3"): {"update": 40.17e6, "wa": 25.76e6, "rho": 6.31e6, "poisson": 13.77e6,
                           "assemble": 39.18e6,
                           "source": "profiles/mgp_211k_bf16x3_kernels.md"},
 }
@@ -894,6 +894,22 @@ def run_flow(args):
     return 0
 
 
+def run_stage_once(args):
+    """One mGP stage of the workload (its instance, fillers and grid) through the public API,
+    for profilers: the loop's kernels in their order, nothing else timed or printed but one
+    line. Under ncu, set SPG_HOST_LOOP=1 (ncu does not profile kernels inside conditional graphs)
+    and SPG_TC_TUNE=0 (the tile-shape tuner's timing is distorted under the profiler)."""
+    from superplace_b200 import engine
+
+    db = make_design(args.workload)
+    engine.initialize_fillers(db, 1.0, 1002)
+    precision = abi.POISSON_BF16X3 if args.precision == "bf16x3" else abi.POISSON_FP32
+    params = abi.default_params(gp_bin_dim=WORKLOADS[args.workload]["bin_dim"], poisson_precision=precision)
+    r = engine.EPlace(db, params).run(abi.STAGE_MGP)
+    print(json.dumps({"stage": "mGP", "iterations": r.iterations, "hpwl": r.hpwl, "overflow": r.overflow}))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -926,6 +942,8 @@ def main():
     ap.add_argument("--mixed-cells", type=int, default=211_000)
     ap.add_argument("--mixed-forms", nargs="+", default=["fp64", "fp32", "bf16x3"])
     ap.add_argument("--no-mixed-cpu", dest="mixed_cpu", action="store_false")
+    ap.add_argument("--stage-once", action="store_true",
+                    help="one mGP stage of the workload at --precision, no timing (the profiles' command)")
     ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[10.0, 50.0, 200.0])
     ap.add_argument("--serve-seconds", type=float, default=8.0)
@@ -935,6 +953,8 @@ def main():
     # the device as many hardware work queues (read when the CUDA context is created, which has
     # not happened yet in this process)
     os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "16")
+    if args.stage_once:
+        return run_stage_once(args)
     if args.serve:
         return run_serve(args)
     if args.poisson_sweep:
