@@ -341,10 +341,11 @@ void* spg_ctx_stream(const spg_ctx* ctx);
 /* Per-kernel device time (microseconds, CUDA events on the context's stream, averaged
  * over `reps` back-to-back launches, L2 warm as inside the loop) of the iteration's parts
  * at the current positions, after a stage run. us[] receives up to n values in this order:
- *   0 update + density scatter of the opt nodes   1 WA pass 1 + HPWL
+ *   0 update + density scatter of the opt nodes
+ *   1 WA pass 1 + HPWL, then the cells' WA pass 2
  *   2 density scatter of the other density nodes (0 when there are none)
  *   3 rho + overflow   4 Poisson solve
- *   5 assembly (gather + WA pass 2 + gradient + the step's norms and decisions)
+ *   5 assembly (gather + gradient + the step's norms and decisions)
  *   6 unused (0: the norms run inside the assembly)   7 one evaluation
  * The stage's results are left unchanged (state and delivered positions are restored). */
 int spg_ctx_profile(spg_ctx* ctx, int reps, double* us, int n);

@@ -10,9 +10,10 @@
 // centred c'+- sums (wa_wirelength.cpp:73-127), the WA value and the HPWL term, and every
 // lane writes its pin's gradient contribution termMax - termMin (wa_wirelength.cpp:192-221)
 // to a per-pin array.
-// Pass 2 (fused into the gradient assembly) sums those contributions per node in
-// node->pin CSR order, which is exactly the reference's accumulation order, so the node
-// gradient equals the reference's whenever the exponentials agree.
+// Pass 2 (wl_cells_kernel in optimizer.cu, on the same stream after this pass; the assembly
+// reads its sums) adds those contributions per node in node->pin CSR order, which is exactly
+// the reference's accumulation order, so the node gradient equals the reference's whenever the
+// exponentials agree.
 // HPWL is fused into pass 1 (the reference re-walks all pins for it every evaluation).
 #include <algorithm>
 #include <cfloat>
