@@ -1,8 +1,9 @@
 """EPlace::Impl::objAndGrad (src/gp/eplace.cpp:136-203) on the device against the reference.
 
 spg_eval_grad runs the stage loop's own kernels (the loop body with no step applied: the step
-kernel's fixed-point scatter, WA pass 1 with HPWL, rho and tau, the Poisson solve, the large
-nodes' gather, and the fused assembly with the cell gather, WA pass 2 and preconditioning) at
+kernel's fixed-point scatter, WA pass 1 with HPWL and the cells' WA pass 2, rho and tau, the
+Poisson solve, the large nodes' gather, and the fused assembly with the cell gather and
+preconditioning) at
 caller positions. The reference side is objAndGrad's composition of the reference's own
 operators (oracle/_ref: BinGrid, WaWirelength, computeHPWL and the assembly of
 eplace.cpp:166-189). Both evaluate the same opt set at the same positions with the same
