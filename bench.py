@@ -59,6 +59,19 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(values, world, device):
+    """The elementwise maximum of per-rank times over the job's ranks (one all-reduce on the
+    job's process group, on `device`); the values themselves when the job has one rank."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -359,10 +372,7 @@ def run_ours(args):
         dist.barrier()
     t_loop = sum(loop_ms) / 1e3
     t_e2e = sum(e2e_ms) / 1e3
-    if world > 1:
-        tl = torch.tensor([t_loop, t_e2e], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tl, op=dist.ReduceOp.MAX)
-        t_loop, t_e2e = float(tl[0]), float(tl[1])
+    t_loop, t_e2e = max_over_ranks([t_loop, t_e2e], world, "cuda")
     total_iters = sum(iters) * world
     value = total_iters / t_loop
     e2e = total_iters / t_e2e
@@ -407,15 +417,17 @@ def run_ours(args):
             "kernels": kern,
             "clocks": clk.summary(),
         }
-        if precision == abi.POISSON_BF16X3 and args.fp32_steps > 0:
+        # the FP32 arm, the serving leg and the CPU baseline are one-GPU records: a job of
+        # several ranks reports its throughput only (the other ranks wait at the barrier)
+        if precision == abi.POISSON_BF16X3 and args.fp32_steps > 0 and world == 1:
             v32, it32 = fp32_arm(db, args.workload, init_x, init_y, args.fp32_steps)
             line["fp32_value"] = v32
             line["fp32_iterations_per_step"] = it32
             line["bf16x3_over_fp32"] = value / world / v32
-        if args.serve_leg and args.workload == "large":
+        if args.serve_leg and args.workload == "large" and world == 1:
             ep.ctx.close()
             line["serving"] = serve_leg()
-        if args.cpu_baseline:
+        if args.cpu_baseline and world == 1:
             db.node_x[:] = init_x
             db.node_y[:] = init_y
             line["cpu_baseline"] = cpu_baseline_sample(db, args.workload)
