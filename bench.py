@@ -644,7 +644,7 @@ def run_mixed_study(args):
 
 
 def serve_leg(rate=200.0, seconds=1.5, n_designs=16, slots=8):
-    """A short leg of the serving study for the bench line (BASELINE config C4's highest rate):
+    """A short leg of the serving study for the bench line (the study's highest rate, 200 req/s):
     requests from the serving generator (cells log-uniform in 1k..100k) arriving as a Poisson
     process at `rate` per second for about `seconds`, served by `slots` slots, against the same
     trace placed one at a time with plain-FP32 solves. placements/s, p50/p99 latency from
