@@ -576,7 +576,7 @@ def ref_macro_legaliser(params):
 
 
 def run_mixed_study(args):
-    """Config C3: the mixed-size four-stage GP (mGP -> mLG -> FILLERONLY -> cGP) on the 211k-cell
+    """The mixed-size four-stage GP (mGP -> mLG -> FILLERONLY -> cGP) on the 211k-cell
     design with 63 movable macros (56.9% of movable area) and 200 fixed macros, 1024x1024 bins,
     with the FP64, FP32 and split-BF16 Poisson forms on the device (mLG: the reference's own SA on
     the host) and the reference's whole four-stage run on the CPU: per stage iterations, device
@@ -950,7 +950,8 @@ def main():
     ap.add_argument("--flow", action="store_true",
                     help="parse, QP init, mGP, Abacus and .pl write on the 211k design, ours and the reference's: one JSON line")
     ap.add_argument("--mixed-study", action="store_true",
-                    help="C3 four-stage mixed-size GP at 1024x1024 bins, FP64/FP32/BF16x3 and the CPU run: JSON lines")
+                    help="four-stage mixed-size GP (211k cells + 63 movable macros) at 1024x1024 bins, "
+                         "FP64/FP32/BF16x3 and the CPU run: JSON lines")
     ap.add_argument("--mixed-cells", type=int, default=211_000)
     ap.add_argument("--mixed-forms", nargs="+", default=["fp64", "fp32", "bf16x3"])
     ap.add_argument("--no-mixed-cpu", dest="mixed_cpu", action="store_false")

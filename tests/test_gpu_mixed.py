@@ -1,12 +1,12 @@
-"""Config C3 at a reduced size (GPU only): the mixed-size stage sequence with split-BF16 Poisson
-against the reference build.
+"""The mixed-size stage sequence at a reduced size (GPU only), split-BF16 Poisson against the
+reference build.
 
-The design is the C3 generator scaled to 20k cells (63 movable macros at 56.9% of movable area,
+The design is the mixed-size generator (211k cells + 63 movable macros at full size) scaled to 20k cells (63 movable macros at 56.9% of movable area,
 200 fixed macros, the die shrunk to keep the utilisation) at 256x256 bins. The reference's macro
 legaliser (SA) takes about a minute on this instance, so the sequence here freezes the macros
 where mGP left them, as the reference's own cGP regression test does to stand in for mLG
 (test/test_eplace.cpp:445-483); bench.py --mixed-study runs the full four stages with the
-reference's SA at the full C3 size.
+reference's SA at the full size (211k cells, 1024x1024 bins).
 
   * mGP: the device (BF16x3) and the reference build from the same start converge, with final
     HPWL within 0.5%;
