@@ -1,8 +1,9 @@
 """The mixed-size stage sequence at a reduced size (GPU only), split-BF16 Poisson against the
 reference build.
 
-The design is the mixed-size generator (211k cells + 63 movable macros at full size) scaled to 20k cells (63 movable macros at 56.9% of movable area,
-200 fixed macros, the die shrunk to keep the utilisation) at 256x256 bins. The reference's macro
+The design is the mixed-size generator (211k cells + 63 movable macros at full size) scaled
+to 20k cells (63 movable macros at 56.9% of movable area, 200 fixed macros, the die shrunk to
+keep the utilisation) at 256x256 bins. The reference's macro
 legaliser (SA) takes about a minute on this instance, so the sequence here freezes the macros
 where mGP left them, as the reference's own cGP regression test does to stand in for mLG
 (test/test_eplace.cpp:445-483); bench.py --mixed-study runs the full four stages with the
